@@ -1,0 +1,664 @@
+// ElmGMR on the device: diffusive-flux reconstruction (AsIq/qpbc), interior
+// residual + tangent (AsIGMR/e3/e3LHS + fillsparseI), boundary residual
+// (AsBMFG/e3b), outlet coupling (ElmpvsQ) and bc3Res.
+//
+// Reference: flowsolver/src/elmgmr.f90:82-555 and the e3* routines it calls.
+//
+// Element kernels use four lanes per linear tet.  In the quadrature phase lane
+// q evaluates quadrature point q (e3ivar/e3stab/e3Res at that point); in the
+// output phase lane a owns row a of the element: rl(a,:) and the four 3x3 +
+// 4 blocks (a, b).  Per-point quantities are exchanged through shared memory.
+// On a linear tet the metrics, gradients and div q are element constants, so
+// they are computed once per element (the reference recomputes them per
+// point with identical inputs), and the sums over quadrature points of the
+// tangent terms are formed algebraically:
+//   K_ij(a,b) = d_ij [ tsFct M_ab + tlW (rho sum_q N_a(q) uBar_q.dN_b
+//                       + 4 mu dN_a.dN_b
+//                       + sum_q (tauM_q rho (u_q.dN_a)(u_q.dN_b)
+//                                + tauBar_q (L_q.dN_a)(L_q.dN_b))) ]
+//               + tlW ( (sum_q tauC_q) dN_b,i dN_a,j + 4 mu dN_b,j dN_a,i )
+//   G_i(a,b)  = tlW dN_b,i sum_q N_a(q)
+//   C(a,b)    = tlW/rho (sum_q tauM_q) dN_a.dN_b
+// which equals the reference's per-point accumulation (e3lhs.f90:171-402) in
+// exact arithmetic; the FP64 results agree to rounding (~1e-15 relative).
+// Scatter into the CSR blocks uses FP64 atomics at slots precomputed by the
+// pattern pass (no binary search per element, fillsparse.f90:29-60).
+#include "common.cuh"
+
+namespace crimson {
+
+struct ElmConst {
+    double shp[4][4];   // shp[q][n]: shape value of node n at quadrature point q
+    double shgl[3][4];  // local gradients (halved), identical at every point
+    double Qwt;         // quadrature weight (1/4 * 4/3)
+    double M[4][4];     // sum_q N_a(q) N_b(q)
+    double SN[4];       // sum_q N_a(q)
+    double shpb[3][4];  // boundary rule: shape values at the 3 face points
+    double Qwtb;        // boundary weight (2 * 1/3)
+};
+
+__constant__ ElmConst c_el;
+
+struct ElmParams {
+    double rho, mu, alfi, almi, gami, Delt, Dtgl, dtsfct, taucfct, stabflux;
+    int idiff;
+};
+
+static ElmConst make_consts() {
+    // 4-point rule of flowsolver/src/symtet.c:22-23,72-74; shapes of uniformP.c:22-40
+    const double A4 = 0.5854101966249685, B4 = 0.1381966011250150;
+    const double rstw4[4][3] = {{A4, B4, B4}, {B4, A4, B4}, {B4, B4, A4}, {B4, B4, B4}};
+    ElmConst k{};
+    for (int q = 0; q < 4; ++q) {
+        const double* par = rstw4[q];
+        k.shp[q][0] = par[0];
+        k.shp[q][1] = par[1];
+        k.shp[q][2] = par[2];
+        k.shp[q][3] = 1.0e0 - par[0] - par[1] - par[2];
+    }
+    for (int n = 0; n < 4; ++n)
+        for (int j = 0; j < 3; ++j) k.shgl[j][n] = (n == 3 ? -1.0 : (n == j ? 1.0 : 0.0)) / 2.0;
+    k.Qwt = (4.0 / 3.0) * 0.25;
+    for (int a = 0; a < 4; ++a) {
+        k.SN[a] = 0.0;
+        for (int b = 0; b < 4; ++b) {
+            k.M[a][b] = 0.0;
+            for (int q = 0; q < 4; ++q) k.M[a][b] += k.shp[q][a] * k.shp[q][b];
+        }
+        for (int q = 0; q < 4; ++q) k.SN[a] += k.shp[q][a];
+    }
+    // boundary 3-point rule (symtri.c rst3/wt3, genshpb.f90:31-36, genint.f90:86)
+    const double B3 = 0.666666666666667, C3 = 0.166666666666667, A3 = 0.3333333333333330000000000000000000;
+    const double rst3[3][3] = {{B3, C3, C3}, {C3, B3, C3}, {C3, C3, B3}};
+    for (int q = 0; q < 3; ++q) {
+        k.shpb[q][0] = rst3[q][0];
+        k.shpb[q][1] = rst3[q][1];
+        k.shpb[q][2] = rst3[q][2];
+        k.shpb[q][3] = 1.0e0 - rst3[q][0] - rst3[q][1] - rst3[q][2];
+    }
+    k.Qwtb = 2.0 * A3;
+    return k;
+}
+
+int upload_elm_consts(cudaStream_t s) {
+    static bool done = false;
+    if (done) return CRIMSON_OK;
+    ElmConst k = make_consts();
+    CR_CUDA(cudaMemcpyToSymbolAsync(c_el, &k, sizeof(k), 0, cudaMemcpyHostToDevice, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    done = true;
+    return CRIMSON_OK;
+}
+
+static ElmParams elm_params(const crimson_params& p) {
+    ElmParams e;
+    e.rho = p.rho;
+    e.mu = p.mu;
+    e.alfi = p.alfi;
+    e.almi = p.almi;
+    e.gami = p.gami;
+    e.Delt = p.Delt;
+    e.Dtgl = p.Dtgl;
+    e.dtsfct = p.dtsfct;
+    e.taucfct = p.taucfct;
+    e.stabflux = p.stabflux_coeff;
+    e.idiff = p.idiff;
+    return e;
+}
+
+// ---------------------------------------------------------------------------
+// Element metrics (e3metric.f90:26-81) from the four vertex coordinates.
+// dxidx[i][j] = d xi_i / d x_j ; shg[n][k] = d N_n / d x_k.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void elem_metric(const double xl[4][3], double dxidx[3][3], double shg[4][3],
+                                            double* WdetJ) {
+    double d[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) d[i][j] = 0.5 * xl[j][i] - 0.5 * xl[3][i];
+    dxidx[0][0] = d[1][1] * d[2][2] - d[2][1] * d[1][2];
+    dxidx[0][1] = d[2][1] * d[0][2] - d[0][1] * d[2][2];
+    dxidx[0][2] = d[0][1] * d[1][2] - d[0][2] * d[1][1];
+    double tmp = 1.0 / (dxidx[0][0] * d[0][0] + dxidx[0][1] * d[1][0] + dxidx[0][2] * d[2][0]);
+    dxidx[0][0] *= tmp;
+    dxidx[0][1] *= tmp;
+    dxidx[0][2] *= tmp;
+    dxidx[1][0] = (d[1][2] * d[2][0] - d[1][0] * d[2][2]) * tmp;
+    dxidx[1][1] = (d[0][0] * d[2][2] - d[2][0] * d[0][2]) * tmp;
+    dxidx[1][2] = (d[1][0] * d[0][2] - d[0][0] * d[1][2]) * tmp;
+    dxidx[2][0] = (d[1][0] * d[2][1] - d[1][1] * d[2][0]) * tmp;
+    dxidx[2][1] = (d[2][0] * d[0][1] - d[0][0] * d[2][1]) * tmp;
+    dxidx[2][2] = (d[0][0] * d[1][1] - d[0][1] * d[1][0]) * tmp;
+    *WdetJ = c_el.Qwt / tmp;
+    // shgl = (e_j/2) for nodes 0..2 and -(1,1,1)/2 for node 3
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        shg[0][k] = 0.5 * dxidx[0][k];
+        shg[1][k] = 0.5 * dxidx[1][k];
+        shg[2][k] = 0.5 * dxidx[2][k];
+        shg[3][k] = -0.5 * dxidx[0][k] - 0.5 * dxidx[1][k] - 0.5 * dxidx[2][k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// AsIq + e3q: lumped projection of the viscous flux q = mu (grad u + grad u^T)
+// (asiq.f90:52-70, e3q.f90:58-145).  On a linear tet qdi is constant, so
+// ql(a,k) = WdetJ qdi(k) sum_q N_a(q) and rmassl(a) = WdetJ sum_q N_a(q).
+// One thread per element; q node-major (9, nshg).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_asiq(const int4* __restrict__ ien, const double4* __restrict__ x,
+                                              const double4* __restrict__ y, int nelem, ElmParams P,
+                                              double* __restrict__ qres, double* __restrict__ rmass) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
+        int4 nn = ien[e];
+        int nd[4] = {nn.x, nn.y, nn.z, nn.w};
+        double xl[4][3], ul[4][3];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            double4 xv = x[nd[a]];
+            double4 yv = y[nd[a]];
+            xl[a][0] = xv.x;
+            xl[a][1] = xv.y;
+            xl[a][2] = xv.z;
+            ul[a][0] = yv.x;
+            ul[a][1] = yv.y;
+            ul[a][2] = yv.z;
+        }
+        double dxidx[3][3], shg[4][3], W;
+        elem_metric(xl, dxidx, shg, &W);
+        double g[3][3];  // g[k][i] = d u_i / d x_k
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                g[k][i] = shg[0][k] * ul[0][i] + shg[1][k] * ul[1][i] + shg[2][k] * ul[2][i] + shg[3][k] * ul[3][i];
+        const double mu = P.mu;
+        double qdi[9];
+        qdi[0] = 2.0 * mu * g[0][0];
+        qdi[3] = mu * (g[0][1] + g[1][0]);
+        qdi[6] = mu * (g[0][2] + g[2][0]);
+        qdi[1] = qdi[3];
+        qdi[4] = 2.0 * mu * g[1][1];
+        qdi[7] = mu * (g[1][2] + g[2][1]);
+        qdi[2] = qdi[6];
+        qdi[5] = qdi[7];
+        qdi[8] = 2.0 * mu * g[2][2];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            double wa = W * c_el.SN[a];
+            double* qa = qres + 9 * (size_t)nd[a];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) atomicAdd(qa + k, wa * qdi[k]);
+            atomicAdd(rmass + nd[a], wa);
+        }
+    }
+}
+
+// qpbc (qpbc.f90:67-71): rmass <- 1/rmass, q <- q * rmass
+__global__ void k_qpbc(double* __restrict__ qres, double* __restrict__ rmass, int nshg) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
+        double r = 1.0 / rmass[i];
+        rmass[i] = r;
+        double* q = qres + 9 * (size_t)i;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) q[k] = r * q[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// AsIGMR / e3 / e3LHS / fillsparseI, four lanes per element.
+// ---------------------------------------------------------------------------
+constexpr int kQ = 28;   // doubles of per-point data exchanged in shared memory
+
+template <bool kLhs>
+__global__ void __launch_bounds__(128) k_asigmr(const int4* __restrict__ ien, const double4* __restrict__ x,
+                                                const double4* __restrict__ y, const double4* __restrict__ ac,
+                                                const double* __restrict__ qres, const int* __restrict__ epos,
+                                                int nelem, ElmParams P, double* __restrict__ res,
+                                                double* __restrict__ lhsK, double* __restrict__ lhsP) {
+    __shared__ double sq[128][kQ];
+    const int lane4 = threadIdx.x & 3;
+    const int gbase = threadIdx.x & ~3;   // first thread of this element's group
+    const long long ngroups = (long long)gridDim.x * (blockDim.x >> 2);
+    for (long long e0 = (long long)blockIdx.x * (blockDim.x >> 2); e0 < nelem; e0 += ngroups) {
+        const long long e = e0 + (threadIdx.x >> 2);
+        const bool live = e < nelem;
+        int nd[4] = {0, 0, 0, 0};
+        double xl[4][3], yl[4][4];
+        if (live) {
+            int4 nn = ien[e];
+            nd[0] = nn.x;
+            nd[1] = nn.y;
+            nd[2] = nn.z;
+            nd[3] = nn.w;
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            double4 xv = live ? x[nd[a]] : make_double4(0, 0, 0, 0);
+            double4 yv = live ? y[nd[a]] : make_double4(0, 0, 0, 0);
+            xl[a][0] = xv.x;
+            xl[a][1] = xv.y;
+            xl[a][2] = xv.z;
+            // element-local dof order (p, u, v, w) as localy gathers it
+            yl[a][0] = yv.w;
+            yl[a][1] = yv.x;
+            yl[a][2] = yv.y;
+            yl[a][3] = yv.z;
+        }
+        double dxidx[3][3], shg[4][3], WdetJ;
+        elem_metric(xl, dxidx, shg, &WdetJ);
+        if (!live) WdetJ = 0.0;
+        // global gradients g[k][d] of (p, u, v, w)
+        double g[3][4];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int d = 0; d < 4; ++d)
+                g[k][d] = shg[0][k] * yl[0][d] + shg[1][k] * yl[1][d] + shg[2][k] * yl[2][d] + shg[3][k] * yl[3][d];
+        // div q (e3ivar.f90:354-368)
+        double divq[3] = {0.0, 0.0, 0.0};
+        if (P.idiff >= 1 && live) {
+#pragma unroll
+            for (int n = 0; n < 4; ++n) {
+                const double* q = qres + 9 * (size_t)nd[n];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    divq[i] += shg[n][0] * q[i] + shg[n][1] * q[3 + i] + shg[n][2] * q[6 + i];
+            }
+        }
+        // metric tensor, tet branch (e3stab.f90:487-528)
+        double gij[6];
+        {
+            const double c1 = 1.259921049894873e+00, c2 = 6.299605249474365e-01;
+            double t1, t2, t3;
+            t1 = c1 * dxidx[0][0] + c2 * (dxidx[1][0] + dxidx[2][0]);
+            t2 = c1 * dxidx[1][0] + c2 * (dxidx[0][0] + dxidx[2][0]);
+            t3 = c1 * dxidx[2][0] + c2 * (dxidx[0][0] + dxidx[1][0]);
+            gij[0] = dxidx[0][0] * t1 + dxidx[1][0] * t2 + dxidx[2][0] * t3;
+            t1 = c1 * dxidx[0][1] + c2 * (dxidx[1][1] + dxidx[2][1]);
+            t2 = c1 * dxidx[1][1] + c2 * (dxidx[0][1] + dxidx[2][1]);
+            t3 = c1 * dxidx[2][1] + c2 * (dxidx[0][1] + dxidx[1][1]);
+            gij[1] = dxidx[0][1] * t1 + dxidx[1][1] * t2 + dxidx[2][1] * t3;
+            gij[3] = dxidx[0][0] * t1 + dxidx[1][0] * t2 + dxidx[2][0] * t3;
+            t1 = c1 * dxidx[0][2] + c2 * (dxidx[1][2] + dxidx[2][2]);
+            t2 = c1 * dxidx[1][2] + c2 * (dxidx[0][2] + dxidx[2][2]);
+            t3 = c1 * dxidx[2][2] + c2 * (dxidx[0][2] + dxidx[1][2]);
+            gij[2] = dxidx[0][2] * t1 + dxidx[1][2] * t2 + dxidx[2][2] * t3;
+            gij[4] = dxidx[0][1] * t1 + dxidx[1][1] * t2 + dxidx[2][1] * t3;
+            gij[5] = dxidx[0][0] * t1 + dxidx[1][0] * t2 + dxidx[2][0] * t3;
+        }
+        // ---- quadrature point q = lane4: e3ivar / e3stab / e3Res ----
+        const int q = lane4;
+        double pres = 0.0, u[3] = {0.0, 0.0, 0.0}, aci[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            double N = c_el.shp[q][n];
+            pres += N * yl[n][0];
+            u[0] += N * yl[n][1];
+            u[1] += N * yl[n][2];
+            u[2] += N * yl[n][3];
+            double4 av = live ? ac[nd[n]] : make_double4(0, 0, 0, 0);
+            aci[0] += N * av.x;
+            aci[1] += N * av.y;
+            aci[2] += N * av.z;
+        }
+        const double rho = P.rho, mu = P.mu;
+        double rL[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            rL[i] = (aci[i] + u[0] * g[0][i + 1] + u[1] * g[1][i + 1] + u[2] * g[2][i + 1]) * rho + g[i][0] - divq[i];
+        const double rnu = mu / rho;
+        const double dts = P.Dtgl * P.dtsfct;
+        double uGu = u[0] * (gij[0] * u[0] + gij[3] * u[1] + gij[5] * u[2]) +
+                     u[1] * (gij[3] * u[0] + gij[1] * u[1] + gij[4] * u[2]) +
+                     u[2] * (gij[5] * u[0] + gij[4] * u[1] + gij[2] * u[2]);
+        double gg = gij[0] * gij[0] + gij[1] * gij[1] + gij[2] * gij[2] +
+                    2.0 * (gij[3] * gij[3] + gij[4] * gij[4] + gij[5] * gij[5]);
+        double tauM = (2.0 * dts) * (2.0 * dts) + uGu + 36.0 * (rnu * rnu) * gg;
+        double fact = sqrt(tauM);
+        double tauC = rho * 0.125 * fact / (gij[0] + gij[1] + gij[2]) * (P.taucfct / P.dtsfct);
+        tauM = 1.0 / fact;
+        double tauBar = rL[0] * (gij[0] * rL[0] + gij[3] * rL[1] + gij[5] * rL[2]) +
+                        rL[1] * (gij[3] * rL[0] + gij[1] * rL[1] + gij[4] * rL[2]) +
+                        rL[2] * (gij[5] * rL[0] + gij[4] * rL[1] + gij[2] * rL[2]);
+        if (tauBar != 0.0) tauBar = tauM / sqrt(tauBar);
+        double uBar[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) uBar[i] = u[i] - tauM * rL[i] / rho;
+        // e3Res, advective form (e3res.f90:104-284)
+        double rNa[3], rGNa[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            rNa[i] = (aci[i] + uBar[0] * g[0][i + 1] + uBar[1] * g[1][i + 1] + uBar[2] * g[2][i + 1]) * rho;
+        {
+            double divu = g[0][1] + g[1][2] + g[2][3];
+            double tmp = -pres + tauC * divu;
+            double lg[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) lg[i] = tauBar * (rL[0] * g[0][i + 1] + rL[1] * g[1][i + 1] + rL[2] * g[2][i + 1]);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    rGNa[i][j] = mu * (g[j][i + 1] + g[i][j + 1]) + (i == j ? tmp : 0.0) + tauM * rL[i] * u[j] +
+                                 lg[i] * rL[j];
+        }
+        double* s = sq[threadIdx.x];
+        // per-point dot products with every node gradient (reused by all rows)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            s[c] = u[0] * shg[c][0] + u[1] * shg[c][1] + u[2] * shg[c][2];              // alpha_qc
+            s[4 + c] = rL[0] * shg[c][0] + rL[1] * shg[c][1] + rL[2] * shg[c][2];       // beta_qc
+            s[8 + c] = uBar[0] * shg[c][0] + uBar[1] * shg[c][1] + uBar[2] * shg[c][2]; // gamma_qc
+        }
+        s[12] = tauM;
+        s[13] = tauBar;
+        s[14] = tauC;
+        s[15] = rNa[0];
+        s[16] = rNa[1];
+        s[17] = rNa[2];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) s[18 + 3 * i + j] = rGNa[i][j];
+        s[27] = 0.0;
+        __syncwarp();
+        // ---- row a = lane4 ----
+        const int a = lane4;
+        const double* S0 = sq[gbase];
+        const double* S1 = sq[gbase + 1];
+        const double* S2 = sq[gbase + 2];
+        const double* S3 = sq[gbase + 3];
+        const double* Sq[4] = {S0, S1, S2, S3};
+        double Na[4];
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) Na[qq] = c_el.shp[qq][a];
+        if (live) {
+            // residual row a
+            double sub[3] = {0.0, 0.0, 0.0}, sG[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, sN[3] = {0, 0, 0};
+            double div_ub = 0.0;
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) {
+                const double* Sx = Sq[qq];
+                div_ub += Sx[8 + a];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    sN[i] += Na[qq] * Sx[15 + i];
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) sG[i][j] += Sx[18 + 3 * i + j];
+                }
+            }
+            (void)sub;
+            double* r = res + 4 * (size_t)nd[a];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                double v = sN[i] + shg[a][0] * sG[i][0] + shg[a][1] * sG[i][1] + shg[a][2] * sG[i][2];
+                atomicAdd(r + i, -WdetJ * v);
+            }
+            atomicAdd(r + 3, WdetJ * div_ub);
+            if (kLhs) {
+                const double lhsFct = P.alfi * P.gami * P.Delt;
+                const double tlW = lhsFct * WdetJ;
+                const double tsFct = P.almi * WdetJ * rho;
+                double TC = 0.0, TM = 0.0, aqa[4], bqa[4], tMq[4], tBq[4];
+#pragma unroll
+                for (int qq = 0; qq < 4; ++qq) {
+                    const double* Sx = Sq[qq];
+                    aqa[qq] = Sx[a];
+                    bqa[qq] = Sx[4 + a];
+                    tMq[qq] = Sx[12];
+                    tBq[qq] = Sx[13];
+                    TC += Sx[14];
+                    TM += Sx[12];
+                }
+                const int* ep = epos + 16 * e + 4 * a;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    double conv = 0.0, sym = 0.0;
+#pragma unroll
+                    for (int qq = 0; qq < 4; ++qq) {
+                        const double* Sx = Sq[qq];
+                        conv += Na[qq] * Sx[8 + b];
+                        sym += tMq[qq] * rho * aqa[qq] * Sx[b] + tBq[qq] * bqa[qq] * Sx[4 + b];
+                    }
+                    double grad = shg[a][0] * shg[b][0] + shg[a][1] * shg[b][1] + shg[a][2] * shg[b][2];
+                    double Kd = tsFct * c_el.M[a][b] + tlW * (rho * conv + 4.0 * mu * grad + sym);
+                    const double tc = tlW * TC, tm = tlW * 4.0 * mu;
+                    double K[9];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j)
+                            K[3 * i + j] = (i == j ? Kd : 0.0) + tc * shg[b][i] * shg[a][j] + tm * shg[b][j] * shg[a][i];
+                    const size_t k = (size_t)ep[b];
+                    double* Kp = lhsK + 9 * k;
+#pragma unroll
+                    for (int t = 0; t < 9; ++t) atomicAdd(Kp + t, K[t]);
+                    double* Pp = lhsP + 4 * k;
+                    const double sn = tlW * c_el.SN[a];
+                    atomicAdd(Pp + 0, sn * shg[b][0]);
+                    atomicAdd(Pp + 1, sn * shg[b][1]);
+                    atomicAdd(Pp + 2, sn * shg[b][2]);
+                    atomicAdd(Pp + 3, tlW / rho * TM * grad);
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// AsBMFG / e3b / e3bvar, rigid wall, one thread per boundary face
+// (e3b.f90:112-470, e3bvar.f90:140-460).  Residual only: for rigid walls the
+// boundary tangent is zero (e3b.f90:338-343).
+// ---------------------------------------------------------------------------
+__global__ void k_asbmfg(const int4* __restrict__ ienb, const int* __restrict__ iBCB, const double* __restrict__ BCB,
+                         const double4* __restrict__ x, const double4* __restrict__ y, int nface, ElmParams P,
+                         double* __restrict__ res) {
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nface; f += gridDim.x * blockDim.x) {
+        int4 nn = ienb[f];
+        int nd[4] = {nn.x, nn.y, nn.z, nn.w};
+        double xl[4][3], yl[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            double4 xv = x[nd[a]];
+            double4 yv = y[nd[a]];
+            xl[a][0] = xv.x;
+            xl[a][1] = xv.y;
+            xl[a][2] = xv.z;
+            yl[a][0] = yv.w;
+            yl[a][1] = yv.x;
+            yl[a][2] = yv.y;
+            yl[a][3] = yv.z;
+        }
+        const int bits = iBCB[f];
+        const double* bcb = BCB + 18 * (size_t)f;
+        double dxidx[3][3], shg[4][3], Wtmp;
+        elem_metric(xl, dxidx, shg, &Wtmp);
+        double g[3][4];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int d = 1; d < 4; ++d)
+                g[k][d] = shg[0][k] * yl[0][d] + shg[1][k] * yl[1][d] + shg[2][k] * yl[2][d] + shg[3][k] * yl[3][d];
+        double v1[3], v2[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            v1[i] = xl[1][i] - xl[0][i];
+            v2[i] = xl[2][i] - xl[0][i];
+        }
+        double t1 = v1[1] * v2[2] - v2[1] * v1[2];
+        double t2 = v2[0] * v1[2] - v1[0] * v2[2];
+        double t3 = v1[0] * v2[1] - v2[0] * v1[1];
+        double temp = 1.0 / sqrt(t1 * t1 + t2 * t2 + t3 * t3);
+        double bn[3] = {t1 * temp, t2 * temp, t3 * temp};
+        double WdetJb = c_el.Qwtb / (4.0 * temp);
+        const double mu = P.mu, rho = P.rho;
+        double tau[3];
+        tau[0] = bn[0] * 2.0 * mu * g[0][1] + bn[1] * (mu * (g[1][1] + g[0][2])) + bn[2] * (mu * (g[2][1] + g[0][3]));
+        tau[1] = bn[0] * (mu * (g[1][1] + g[0][2])) + bn[1] * 2.0 * mu * g[1][2] + bn[2] * (mu * (g[2][2] + g[1][3]));
+        tau[2] = bn[0] * (mu * (g[2][1] + g[0][3])) + bn[1] * (mu * (g[2][2] + g[1][3])) + bn[2] * 2.0 * mu * g[2][3];
+        double tn = bn[0] * tau[0] + bn[1] * tau[1] + bn[2] * tau[2];
+        double rl[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+        for (int q = 0; q < 3; ++q) {
+            const double* Nb = c_el.shpb[q];
+            double pres = 0.0, u[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int n = 0; n < 3; ++n) {
+                pres += Nb[n] * yl[n][0];
+                u[0] += Nb[n] * yl[n][1];
+                u[1] += Nb[n] * yl[n][2];
+                u[2] += Nb[n] * yl[n][3];
+            }
+            double unm = bn[0] * u[0] + bn[1] * u[1] + bn[2] * u[2];
+            pres = pres - tn;
+            double tt[3] = {tau[0] - bn[0] * tn, tau[1] - bn[1] * tn, tau[2] - bn[2] * tn};
+            double unm_copy = 0.0;
+            if ((bits >> 1) & 1)
+                if (unm < 0.0) unm_copy = unm;
+            if (bits & 1) {
+                unm = 0.0;
+                for (int n = 0; n < 3; ++n) unm += Nb[n] * bcb[6 * n + 0];
+            }
+            if ((bits >> 1) & 1) {
+                pres = 0.0;
+                for (int n = 0; n < 3; ++n) pres += Nb[n] * bcb[6 * n + 1];
+            }
+            if ((bits >> 2) & 1) {
+                tt[0] = tt[1] = tt[2] = 0.0;
+                for (int n = 0; n < 3; ++n) {
+                    tt[0] += Nb[n] * bcb[6 * n + 2];
+                    tt[1] += Nb[n] * bcb[6 * n + 3];
+                    tt[2] += Nb[n] * bcb[6 * n + 4];
+                }
+            }
+            if ((bits >> 4) & 1) {
+                pres = 0.0;
+                tt[0] = tt[1] = tt[2] = 0.0;
+            }
+            double rNa[4];
+            const double rou_copy = rho * unm_copy;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) rNa[i] = (-tt[i] + bn[i] * pres - P.stabflux * rou_copy * u[i]) * WdetJb;
+            rNa[3] = unm * WdetJb;
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+#pragma unroll
+                for (int d = 0; d < 4; ++d) rl[n][d] -= Nb[n] * rNa[d];
+        }
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            double* r = res + 4 * (size_t)nd[n];
+#pragma unroll
+            for (int d = 0; d < 4; ++d) atomicAdd(r + d, rl[n][d]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ElmpvsQ, GRCR branch (elmgmr.f90:1271-1330) with GetFlowQ
+// (boundarydata.f90:1157-1196).  One block per coupled surface reduces
+// Q_k = sum NABI.u over its nodes (fixed order: deterministic).
+// ---------------------------------------------------------------------------
+__global__ void k_flowq(const int* __restrict__ onodes, const int* __restrict__ off, const double4* __restrict__ onabi,
+                        const double4* __restrict__ y, double* __restrict__ q) {
+    __shared__ double sm[32];
+    const int k = blockIdx.x;
+    double s = 0.0;
+    for (int t = off[k] + threadIdx.x; t < off[k + 1]; t += blockDim.x) {
+        double4 nb = onabi[t];
+        double4 yv = y[onodes[t]];
+        s += nb.x * yv.x + nb.y * yv.y + nb.z * yv.z;
+    }
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) q[k] = s;
+}
+
+__global__ void k_pvsq_add(const int* __restrict__ onodes, const int* __restrict__ off, const double4* __restrict__ onabi,
+                           const double* __restrict__ q, const double* __restrict__ coefs, int ncoupled,
+                           double* __restrict__ res) {
+    const int k = blockIdx.y;
+    const double pk = -1.0 * (q[k] * coefs[k]) - coefs[ncoupled + k];
+    for (int t = off[k] + blockIdx.x * blockDim.x + threadIdx.x; t < off[k + 1]; t += gridDim.x * blockDim.x) {
+        double4 nb = onabi[t];
+        double* r = res + 4 * (size_t)onodes[t];
+        r[0] += pk * nb.x;
+        r[1] += pk * nb.y;
+        r[2] += pk * nb.z;
+    }
+}
+
+// bc3Res (bc3res.f90:30-124) for no or all three velocity components
+__global__ void k_bc3res(const int* __restrict__ iBC, int nshg, double* __restrict__ res) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
+        int b = iBC[i];
+        double* r = res + 4 * (size_t)i;
+        if ((b >> 2) & 1) r[3] = 0.0;
+        if (((b >> 3) & 7) == 7 || ((b >> 11) & 1)) {
+            r[0] = 0.0;
+            r[1] = 0.0;
+            r[2] = 0.0;
+        }
+    }
+}
+
+// device-side offsets for the outlet node groups
+static int upload_offsets(crimson_ctx* c, DBuf<int>& doff) {
+    return doff.upload(c->onode_off.data(), c->onode_off.size(), c->stream);
+}
+
+int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1, const double* coef2,
+                  double* d_res, double* d_lhsK, double* d_lhsP, int lhs) {
+    cudaStream_t s = c->stream;
+    CR_CHECK(upload_elm_consts(s));
+    const ElmParams P = elm_params(c->p);
+    const double4* y4 = reinterpret_cast<const double4*>(d_y);
+    const double4* a4 = reinterpret_cast<const double4*>(d_ac);
+    // diffusive flux reconstruction
+    if (c->p.idiff == 1) {
+        CR_CHECK(c->qres.alloc((size_t)c->nshg * 9));
+        CR_CHECK(c->rmass.alloc((size_t)c->nshg));
+        CR_CUDA(cudaMemsetAsync(c->qres.p, 0, sizeof(double) * 9 * (size_t)c->nshg, s));
+        CR_CUDA(cudaMemsetAsync(c->rmass.p, 0, sizeof(double) * (size_t)c->nshg, s));
+        k_asiq<<<grid_for(c->nelem, 256, 16), 256, 0, s>>>(c->ien.p, c->x.p, y4, c->nelem, P, c->qres.p, c->rmass.p);
+        k_qpbc<<<grid_for(c->nshg, 256), 256, 0, s>>>(c->qres.p, c->rmass.p, c->nshg);
+    }
+    CR_CUDA(cudaMemsetAsync(d_res, 0, sizeof(double) * 4 * (size_t)c->nshg, s));
+    if (lhs) {
+        CR_CUDA(cudaMemsetAsync(d_lhsK, 0, sizeof(double) * 9 * (size_t)c->nnz, s));
+        CR_CUDA(cudaMemsetAsync(d_lhsP, 0, sizeof(double) * 4 * (size_t)c->nnz, s));
+    }
+    const int blk = 128;
+    const int grid = grid_for((long long)c->nelem * 4, blk, 16);
+    if (lhs)
+        k_asigmr<true><<<grid, blk, 0, s>>>(c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
+                                            d_lhsK, d_lhsP);
+    else
+        k_asigmr<false><<<grid, blk, 0, s>>>(c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
+                                             nullptr, nullptr);
+    CR_CUDA(cudaGetLastError());
+    if (c->nface > 0)
+        k_asbmfg<<<grid_for(c->nface, 128), 128, 0, s>>>(c->ienb.p, c->iBCB.p, c->BCB.p, c->x.p, y4, c->nface, P,
+                                                        d_res);
+    if (c->ncoupled > 0) {
+        std::vector<double> hc(2 * (size_t)c->ncoupled);
+        for (int k = 0; k < c->ncoupled; ++k) {
+            hc[k] = coef1 ? coef1[k] : 0.0;
+            hc[c->ncoupled + k] = coef2 ? coef2[k] : 0.0;
+        }
+        CR_CHECK(c->coefs.upload(hc.data(), hc.size(), s));
+        DBuf<int> doff;
+        CR_CHECK(upload_offsets(c, doff));
+        CR_CHECK(c->flowq.alloc((size_t)c->ncoupled));
+        k_flowq<<<c->ncoupled, 256, 0, s>>>(c->onodes.p, doff.p, c->onabi.p, y4, c->flowq.p);
+        dim3 g2(8, c->ncoupled);
+        k_pvsq_add<<<g2, 256, 0, s>>>(c->onodes.p, doff.p, c->onabi.p, c->flowq.p, c->coefs.p, c->ncoupled, d_res);
+        CR_CUDA(cudaStreamSynchronize(s));   // doff is released at scope exit
+    }
+    k_bc3res<<<grid_for(c->nshg, 256), 256, 0, s>>>(c->iBC.p, c->nshg, d_res);
+    CR_CUDA(cudaGetLastError());
+    return CRIMSON_OK;
+}
+
+}  // namespace crimson

@@ -1,0 +1,689 @@
+// extern "C" entry points of crimson_b200 (declared in include/crimson_b200.h).
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "memls.cuh"
+
+namespace crimson {
+
+thread_local std::string g_last_error;
+void set_last_error(const std::string& s) { g_last_error = s; }
+
+int sm_count() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    }
+    return n;
+}
+
+int build_pattern(crimson_ctx* c);
+int pattern_aux(crimson_lhs* L);
+int pattern_to_host(crimson_ctx* c, int* colm, int* rowp, long long cap);
+int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1, const double* coef2,
+                  double* d_res, double* d_lhsK, double* d_lhsP, int lhs);
+int memls_solve_val(crimson_lhs* L, crimson_ls* ls, double* Ri, double* Val, const int* incL, const double* res,
+                    crimson_ls_stats* st);
+int memls_solve_lhs_device(crimson_lhs* L, crimson_ls* ls, const double* d_res, const double* d_lhsK,
+                           const double* d_lhsP, const int* incL, const double* faceRes, double* d_sol,
+                           crimson_ls_stats* st);
+
+// ---- layout conversion kernels ----
+__global__ void k_soa_to_node4(const double* __restrict__ a, int n, int ld, double* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int d = 0; d < 4; ++d) out[4 * (size_t)i + d] = a[(size_t)d * ld + i];
+}
+__global__ void k_node4_to_soa(const double* __restrict__ a, int n, double* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int d = 0; d < 4; ++d) out[(size_t)d * n + i] = a[4 * (size_t)i + d];
+}
+
+// ---- time stepping kernels (itrPC.f90, itrbc.f90) ----
+__global__ void k_predict(const double* __restrict__ yold, const double* __restrict__ acold, double* __restrict__ y,
+                          double* __restrict__ ac, long long n4, double fct) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += (long long)gridDim.x * blockDim.x) {
+        y[t] = yold[t];
+        ac[t] = acold[t] * fct;
+    }
+}
+__global__ void k_yalpha(const double* __restrict__ yold, const double* __restrict__ acold,
+                         const double* __restrict__ y, const double* __restrict__ ac, double* __restrict__ ya,
+                         double* __restrict__ aa, int n, double alfi, double almi) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const size_t b = 4 * (size_t)i;
+        for (int d = 0; d < 3; ++d) {
+            ya[b + d] = yold[b + d] + alfi * (y[b + d] - yold[b + d]);
+            aa[b + d] = acold[b + d] + almi * (ac[b + d] - acold[b + d]);
+        }
+        ya[b + 3] = y[b + 3];
+        aa[b + 3] = 0.0;
+    }
+}
+__global__ void k_correct(double* __restrict__ y, double* __restrict__ ac, const double* __restrict__ sol, int n,
+                          double fct1, double fct2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const size_t b = 4 * (size_t)i;
+        for (int d = 0; d < 3; ++d) y[b + d] = y[b + d] + fct1 * sol[b + d];
+        y[b + 3] = y[b + 3] + fct2 * sol[b + 3];
+        for (int d = 0; d < 3; ++d) ac[b + d] = ac[b + d] + sol[b + d];
+    }
+}
+// BC node-major (ndofBC per node)
+__global__ void k_itrbc(const int* __restrict__ iBC, const double* __restrict__ BC, int ndofBC, int n,
+                        double* __restrict__ y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int b = iBC[i];
+        const double* bc = BC + (size_t)ndofBC * i;
+        if (((b >> 3) & 7) == 7) {
+            y[4 * (size_t)i + 0] = bc[2];
+            y[4 * (size_t)i + 1] = bc[3];
+            y[4 * (size_t)i + 2] = bc[4];
+        }
+        if ((b >> 2) & 1) y[4 * (size_t)i + 3] = bc[0];
+    }
+}
+__global__ void k_inflow(const int* __restrict__ nodes, const double* __restrict__ prof, int m, double scale,
+                         int ndofBC, double* __restrict__ BC) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        double* bc = BC + (size_t)ndofBC * nodes[t];
+        bc[2] = prof[3 * (size_t)t + 0] * scale;
+        bc[3] = prof[3 * (size_t)t + 1] * scale;
+        bc[4] = prof[3 * (size_t)t + 2] * scale;
+    }
+}
+__global__ void k_flowq_step(const int* __restrict__ onodes, int beg, int end, const double4* __restrict__ onabi,
+                             const double4* __restrict__ y, double* __restrict__ q) {
+    __shared__ double sm[32];
+    double s = 0.0;
+    for (int t = beg + threadIdx.x; t < end; t += blockDim.x) {
+        double4 nb = onabi[t];
+        double4 yv = y[onodes[t]];
+        s += nb.x * yv.x + nb.y * yv.y + nb.z * yv.z;
+    }
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) *q = s;
+}
+
+static void rcr_coeffs(double Rp, double C, double Rd, double Pdn, double Pdn1, double Pn, double Qn,
+                       double alfi_delt, double* slope, double* offset) {
+    // RCR::computeImplicitCoefficients (flowsolver/src/RCR.cxx:49-81)
+    double denominator = 1.0 + ((C * Rd) / alfi_delt);
+    double num = Rd + Rp * (1.0 + ((C * Rd) / alfi_delt));
+    *slope = num / denominator;
+    double temp2 = Pn + Pdn1 - Pdn - Rp * Qn;
+    temp2 = ((C * Rd) / alfi_delt) * temp2 + Pdn1;
+    *offset = temp2 / denominator;
+}
+
+static int check_params(const crimson_params* p) {
+    if (!p) return CRIMSON_ERR_ARG;
+    if (p->itau != 0 || p->flmpl != 0.0 || p->flmpr != 0.0 || p->iconvflow != 2 || (p->idiff != 0 && p->idiff != 1)) {
+        set_last_error("unsupported settings: need itau=0, flmpl=flmpr=0, iconvflow=2, idiff in {0,1}");
+        return CRIMSON_ERR_UNSUPPORTED;
+    }
+    return CRIMSON_OK;
+}
+
+}  // namespace crimson
+
+using namespace crimson;
+
+extern "C" {
+
+const char* crimson_version(void) { return "crimson_b200 0.1 sm_100a"; }
+void* crimson_ctx_stream(crimson_ctx* c) { return c ? (void*)c->stream : nullptr; }
+const char* crimson_last_error(void) { return g_last_error.c_str(); }
+
+int crimson_ctx_create(crimson_ctx** out, const crimson_params* p, int nshg, int numnp, int nelem, const int* ien,
+                       const double* x) {
+    if (!out || !ien || !x || nshg <= 0 || numnp < nshg || nelem <= 0) return CRIMSON_ERR_ARG;
+    CR_CHECK(check_params(p));
+    crimson_ctx* c = new crimson_ctx();
+    c->p = *p;
+    c->nshg = nshg;
+    c->numnp = numnp;
+    c->nelem = nelem;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        set_last_error(cudaGetErrorString(e));
+        delete c;
+        return CRIMSON_ERR_CUDA;
+    }
+    std::vector<int4> hien(nelem);
+    for (int i = 0; i < nelem; ++i) {
+        int v[4];
+        for (int a = 0; a < 4; ++a) {
+            v[a] = std::abs(ien[(size_t)a * nelem + i]) - 1;
+            if (v[a] < 0 || v[a] >= nshg) {
+                set_last_error("ien out of range");
+                crimson_ctx_destroy(c);
+                return CRIMSON_ERR_ARG;
+            }
+        }
+        hien[i] = make_int4(v[0], v[1], v[2], v[3]);
+    }
+    std::vector<double4> hx(numnp);
+    for (int i = 0; i < numnp; ++i)
+        hx[i] = make_double4(x[i], x[(size_t)numnp + i], x[2 * (size_t)numnp + i], 0.0);
+    int rc = c->ien.upload(hien.data(), hien.size(), c->stream);
+    if (rc == CRIMSON_OK) rc = c->x.upload(hx.data(), hx.size(), c->stream);
+    std::vector<int> zi(nshg, 0);
+    if (rc == CRIMSON_OK) rc = c->iBC.upload(zi.data(), zi.size(), c->stream);
+    int nbc = p->ndofBC > 0 ? p->ndofBC : 7;
+    c->p.ndofBC = nbc;
+    std::vector<double> zb((size_t)nshg * nbc, 0.0);
+    c->h_BC.assign(zb.begin(), zb.end());
+    c->h_iBC.assign(nshg, 0);
+    if (rc == CRIMSON_OK) rc = c->BC.upload(zb.data(), zb.size(), c->stream);
+    if (rc == CRIMSON_OK) {
+        cudaError_t e2 = cudaStreamSynchronize(c->stream);
+        if (e2 != cudaSuccess) {
+            set_last_error(cudaGetErrorString(e2));
+            rc = CRIMSON_ERR_CUDA;
+        }
+    }
+    if (rc != CRIMSON_OK) {
+        crimson_ctx_destroy(c);
+        return rc;
+    }
+    *out = c;
+    return CRIMSON_OK;
+}
+
+int crimson_ctx_destroy(crimson_ctx* c) {
+    if (!c) return CRIMSON_ERR_ARG;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaStream_t s = c->stream;
+    delete c;
+    if (s) cudaStreamDestroy(s);
+    return CRIMSON_OK;
+}
+
+int crimson_set_params(crimson_ctx* c, const crimson_params* p) {
+    if (!c) return CRIMSON_ERR_ARG;
+    CR_CHECK(check_params(p));
+    int nbc = c->p.ndofBC;
+    c->p = *p;
+    c->p.ndofBC = nbc;
+    return CRIMSON_OK;
+}
+
+int crimson_set_bc(crimson_ctx* c, const int* iBC, const double* BC) {
+    if (!c || !iBC || !BC) return CRIMSON_ERR_ARG;
+    const int n = c->nshg, nb = c->p.ndofBC;
+    for (int i = 0; i < n; ++i) {
+        int v = (iBC[i] >> 3) & 7;
+        if (v != 0 && v != 7) {
+            // bc3LHS only acts on partially constrained nodes (bc3lhs.f90:48-49)
+            set_last_error("partially constrained velocity nodes (bc3LHS projection) are not supported");
+            return CRIMSON_ERR_UNSUPPORTED;
+        }
+    }
+    std::vector<double> nm((size_t)n * nb);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < nb; ++k) nm[(size_t)nb * i + k] = BC[(size_t)k * n + i];
+    c->h_iBC.assign(iBC, iBC + n);
+    c->h_BC.assign(BC, BC + (size_t)n * nb);
+    CR_CHECK(c->iBC.upload(iBC, n, c->stream));
+    CR_CHECK(c->BC.upload(nm.data(), nm.size(), c->stream));
+    CR_CUDA(cudaStreamSynchronize(c->stream));
+    return CRIMSON_OK;
+}
+
+int crimson_set_boundary(crimson_ctx* c, int nface, const int* ienb, const int* iBCB, const double* BCB) {
+    if (!c || nface < 0 || (nface > 0 && (!ienb || !iBCB))) return CRIMSON_ERR_ARG;
+    c->nface = nface;
+    if (nface == 0) return CRIMSON_OK;
+    std::vector<int4> hb(nface);
+    std::vector<int> hbits(nface);
+    std::vector<double> hbcb((size_t)nface * 18, 0.0);
+    for (int f = 0; f < nface; ++f) {
+        int v[4];
+        for (int a = 0; a < 4; ++a) {
+            v[a] = std::abs(ienb[(size_t)a * nface + f]) - 1;
+            if (v[a] < 0 || v[a] >= c->nshg) return CRIMSON_ERR_ARG;
+        }
+        hb[f] = make_int4(v[0], v[1], v[2], v[3]);
+        hbits[f] = iBCB[f];
+        if (BCB)
+            for (int n = 0; n < 3; ++n)
+                for (int k = 0; k < 6; ++k) hbcb[18 * (size_t)f + 6 * n + k] = BCB[((size_t)k * 3 + n) * nface + f];
+    }
+    CR_CHECK(c->ienb.upload(hb.data(), hb.size(), c->stream));
+    CR_CHECK(c->iBCB.upload(hbits.data(), hbits.size(), c->stream));
+    CR_CHECK(c->BCB.upload(hbcb.data(), hbcb.size(), c->stream));
+    CR_CUDA(cudaStreamSynchronize(c->stream));
+    return CRIMSON_OK;
+}
+
+int crimson_set_outlets(crimson_ctx* c, int ncoupled, const int* srflist, const int* ndsurf, const double* NABI) {
+    if (!c || ncoupled < 0 || (ncoupled > 0 && (!srflist || !ndsurf || !NABI))) return CRIMSON_ERR_ARG;
+    if (ncoupled > 8) return CRIMSON_ERR_UNSUPPORTED;
+    c->ncoupled = ncoupled;
+    c->srflist.assign(srflist, srflist + ncoupled);
+    std::vector<int> nodes;
+    std::vector<double4> nab;
+    c->onode_off.assign(1, 0);
+    const int n = c->nshg;
+    for (int k = 0; k < ncoupled; ++k) {
+        for (int i = 0; i < n; ++i)
+            if (ndsurf[i] == srflist[k]) {
+                nodes.push_back(i);
+                nab.push_back(make_double4(NABI[i], NABI[(size_t)n + i], NABI[2 * (size_t)n + i], 0.0));
+            }
+        c->onode_off.push_back((int)nodes.size());
+    }
+    CR_CHECK(c->onodes.upload(nodes.data(), nodes.size(), c->stream));
+    CR_CHECK(c->onabi.upload(nab.data(), nab.size(), c->stream));
+    CR_CUDA(cudaStreamSynchronize(c->stream));
+    c->rcr_Pn.assign(ncoupled, 0.0);
+    c->rcr_Qn.assign(ncoupled, 0.0);
+    return CRIMSON_OK;
+}
+
+int crimson_genadj(crimson_ctx* c, int* colm, int* rowp, long long cap, long long* nnz_tot) {
+    if (!c) return CRIMSON_ERR_ARG;
+    if (c->nnz == 0) CR_CHECK(build_pattern(c));
+    if (nnz_tot) *nnz_tot = c->nnz;
+    return pattern_to_host(c, colm, rowp, cap);
+}
+
+int crimson_elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1,
+                          const double* coef2, double* d_res, double* d_lhsK, double* d_lhsP, int lhs) {
+    if (!c || !d_y || !d_ac || !d_res) return CRIMSON_ERR_ARG;
+    if (lhs && (!d_lhsK || !d_lhsP)) return CRIMSON_ERR_ARG;
+    if (c->nnz == 0) CR_CHECK(build_pattern(c));
+    return elmgmr_device(c, d_y, d_ac, coef1, coef2, d_res, d_lhsK, d_lhsP, lhs);
+}
+
+int crimson_elmgmr(crimson_ctx* c, const double* y, const double* ac, const double* coef1, const double* coef2,
+                   double* res, double* lhsK, double* lhsP, int lhs) {
+    if (!c || !y || !ac || !res) return CRIMSON_ERR_ARG;
+    if (lhs && (!lhsK || !lhsP)) return CRIMSON_ERR_ARG;
+    if (c->nnz == 0) CR_CHECK(build_pattern(c));
+    cudaStream_t s = c->stream;
+    const int n = c->nshg;
+    DBuf<double> tmp;
+    CR_CHECK(tmp.alloc(4 * (size_t)n));
+    CR_CHECK(c->y4.alloc(4 * (size_t)n));
+    CR_CHECK(c->ac4.alloc(4 * (size_t)n));
+    CR_CHECK(c->res4.alloc(4 * (size_t)n));
+    if (lhs) {
+        CR_CHECK(c->lhsK.alloc(9 * (size_t)c->nnz));
+        CR_CHECK(c->lhsP.alloc(4 * (size_t)c->nnz));
+    }
+    CR_CUDA(cudaMemcpyAsync(tmp.p, y, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s));
+    k_soa_to_node4<<<grid_for(n, 256), 256, 0, s>>>(tmp.p, n, n, c->y4.p);
+    CR_CUDA(cudaStreamSynchronize(s));
+    CR_CUDA(cudaMemcpyAsync(tmp.p, ac, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s));
+    k_soa_to_node4<<<grid_for(n, 256), 256, 0, s>>>(tmp.p, n, n, c->ac4.p);
+    CR_CHECK(elmgmr_device(c, c->y4.p, c->ac4.p, coef1, coef2, c->res4.p, lhs ? c->lhsK.p : nullptr,
+                           lhs ? c->lhsP.p : nullptr, lhs));
+    k_node4_to_soa<<<grid_for(n, 256), 256, 0, s>>>(c->res4.p, n, tmp.p);
+    CR_CUDA(cudaMemcpyAsync(res, tmp.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
+    if (lhs) {
+        CR_CUDA(cudaMemcpyAsync(lhsK, c->lhsK.p, sizeof(double) * 9 * (size_t)c->nnz, cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaMemcpyAsync(lhsP, c->lhsP.p, sizeof(double) * 4 * (size_t)c->nnz, cudaMemcpyDeviceToHost, s));
+    }
+    CR_CUDA(cudaStreamSynchronize(s));
+    return CRIMSON_OK;
+}
+
+// ---------------------------------------------------------------------------
+// memLS objects
+// ---------------------------------------------------------------------------
+int crimson_memls_ls_create(crimson_ls** out, int LS_type, int present_mask, double relTol, double absTol, int maxItr,
+                            int dimKry, const double* relTolIn, const double* absTolIn, const int* maxItrIn) {
+    if (!out) return CRIMSON_ERR_ARG;
+    if (LS_type != CRIMSON_LS_TYPE_NS) return CRIMSON_ERR_UNSUPPORTED;
+    crimson_ls* ls = new crimson_ls();
+    // memLS_LS_CREATE defaults (flowsolver/src/memLS.f90:1395-1414)
+    ls->RI.relTol = 4e-1;
+    ls->GM.relTol = 1e-2;
+    ls->CG.relTol = 1e-1;
+    ls->RI.mItr = 10;
+    ls->GM.mItr = 3;
+    ls->CG.mItr = 500;
+    ls->GM.sD = 50;
+    ls->RI.absTol = 1e-10;
+    ls->GM.absTol = 1e-10;
+    ls->CG.absTol = 1e-10;
+    if (present_mask & 1) ls->RI.relTol = relTol;
+    if (present_mask & 2) ls->RI.absTol = absTol;
+    if (present_mask & 4) ls->RI.mItr = maxItr;
+    if (present_mask & 8) {
+        ls->RI.sD = dimKry;
+        ls->GM.sD = dimKry;
+    }
+    if ((present_mask & 16) && relTolIn) {
+        ls->GM.relTol = relTolIn[0];
+        ls->CG.relTol = relTolIn[1];
+    }
+    if ((present_mask & 32) && absTolIn) {
+        ls->GM.absTol = absTolIn[0];
+        ls->CG.absTol = absTolIn[1];
+    }
+    if ((present_mask & 64) && maxItrIn) {
+        ls->GM.mItr = maxItrIn[0];
+        ls->CG.mItr = maxItrIn[1];
+    }
+    *out = ls;
+    return CRIMSON_OK;
+}
+
+int crimson_memls_ls_free(crimson_ls* ls) {
+    delete ls;
+    return CRIMSON_OK;
+}
+
+__global__ void k_one_to_zero(const int* __restrict__ in, int* __restrict__ out, long long n) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        out[t] = in[t] - 1;
+}
+
+int crimson_memls_lhs_create(crimson_lhs** out, int gnNo, int nNo, long long nnz, const int* gNodes,
+                             const int* rowPtr, const int* colPtr, int nFaces) {
+    if (!out || nNo <= 0 || nnz <= 0 || !rowPtr || !colPtr || nFaces < 0) return CRIMSON_ERR_ARG;
+    crimson_lhs* L = new crimson_lhs();
+    L->gnNo = gnNo;
+    L->nNo = nNo;
+    L->nnz = nnz;
+    L->nFaces = nFaces;
+    L->face.resize(nFaces);
+    (void)gNodes;
+    if (cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete L;
+        return CRIMSON_ERR_CUDA;
+    }
+    L->own_stream = true;
+    int rc = CRIMSON_OK;
+    DBuf<int> t1, t2;
+    rc = t1.upload(rowPtr, (size_t)nNo + 1, L->stream);
+    if (rc == CRIMSON_OK) rc = t2.upload(colPtr, (size_t)nnz, L->stream);
+    if (rc == CRIMSON_OK) rc = L->own_rowptr.alloc((size_t)nNo + 1);
+    if (rc == CRIMSON_OK) rc = L->own_col.alloc((size_t)nnz);
+    if (rc == CRIMSON_OK) {
+        k_one_to_zero<<<grid_for(nNo + 1, 256), 256, 0, L->stream>>>(t1.p, L->own_rowptr.p, nNo + 1);
+        k_one_to_zero<<<grid_for(nnz, 256), 256, 0, L->stream>>>(t2.p, L->own_col.p, nnz);
+        L->rowptr = L->own_rowptr.p;
+        L->col = L->own_col.p;
+        rc = crimson::pattern_aux(L);
+        cudaStreamSynchronize(L->stream);
+    }
+    if (rc != CRIMSON_OK) {
+        crimson_memls_lhs_free(L);
+        return rc;
+    }
+    *out = L;
+    return CRIMSON_OK;
+}
+
+int crimson_memls_lhs_create_from_ctx(crimson_lhs** out, crimson_ctx* c, int nFaces) {
+    if (!out || !c || nFaces < 0) return CRIMSON_ERR_ARG;
+    if (c->nnz == 0) CR_CHECK(build_pattern(c));
+    crimson_lhs* L = new crimson_lhs();
+    L->gnNo = c->nshg;
+    L->nNo = c->nshg;
+    L->nnz = c->nnz;
+    L->nFaces = nFaces;
+    L->face.resize(nFaces);
+    L->stream = c->stream;
+    L->own_stream = false;
+    L->rowptr = c->rowptr.p;
+    L->col = c->col.p;
+    L->diag = c->diag.p;
+    L->trans = c->trans.p;
+    *out = L;
+    return CRIMSON_OK;
+}
+
+int crimson_memls_lhs_free(crimson_lhs* L) {
+    if (!L) return CRIMSON_ERR_ARG;
+    if (L->stream) cudaStreamSynchronize(L->stream);
+    if (L->hscal) cudaFreeHost(L->hscal);
+    cudaStream_t s = L->own_stream ? L->stream : nullptr;
+    delete L;
+    if (s) cudaStreamDestroy(s);
+    return CRIMSON_OK;
+}
+
+int crimson_memls_bc_create(crimson_lhs* L, int faIn, int nNo, int dof, int BC_type, const int* gNodes,
+                            const double* Val) {
+    if (!L) return CRIMSON_ERR_ARG;
+    if (faIn > L->nFaces || faIn < 1) {
+        set_last_error("faIn exceeds the lhs structure's number of faces");
+        return CRIMSON_ERR_ARG;
+    }
+    if (nNo < 0 || dof <= 0 || dof > 4 || (nNo > 0 && !gNodes)) return CRIMSON_ERR_ARG;
+    MemlsFace& f = L->face[faIn - 1];
+    f.nNo = nNo;
+    f.dof = dof;
+    f.bGrp = BC_type;
+    f.created = true;
+    std::vector<int> g(nNo);
+    for (int a = 0; a < nNo; ++a) {
+        g[a] = gNodes[a] - 1;
+        if (g[a] < 0 || g[a] >= L->nNo) return CRIMSON_ERR_ARG;
+    }
+    std::vector<double> v((size_t)dof * nNo, 0.0);
+    if (Val) std::memcpy(v.data(), Val, sizeof(double) * v.size());
+    CR_CHECK(f.glob.upload(g.data(), g.size(), L->stream));
+    CR_CHECK(f.val.upload(v.data(), v.size(), L->stream));
+    CR_CHECK(f.valM.alloc(v.size()));
+    CR_CUDA(cudaMemsetAsync(f.valM.p, 0, sizeof(double) * v.size(), L->stream));
+    CR_CUDA(cudaStreamSynchronize(L->stream));
+    return CRIMSON_OK;
+}
+
+int crimson_memls_solve(crimson_lhs* L, crimson_ls* ls, int dof, double* Ri, double* Val, const int* incL,
+                        const double* res, crimson_ls_stats* stats) {
+    if (!L || !ls || !Ri || !Val) return CRIMSON_ERR_ARG;
+    if (dof != 4 || ls->LS_type != CRIMSON_LS_TYPE_NS) return CRIMSON_ERR_UNSUPPORTED;
+    return memls_solve_val(L, ls, Ri, Val, incL, res, stats);
+}
+
+int crimson_solflow_device(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const double* d_res, const double* d_lhsK,
+                           const double* d_lhsP, const int* incL, const double* faceRes, double* d_solinc,
+                           crimson_ls_stats* stats) {
+    if (!c || !L || !ls || !d_res || !d_lhsK || !d_lhsP || !d_solinc) return CRIMSON_ERR_ARG;
+    if (L->diag == nullptr || L->trans == nullptr) return CRIMSON_ERR_STATE;
+    return memls_solve_lhs_device(L, ls, d_res, d_lhsK, d_lhsP, incL, faceRes, d_solinc, stats);
+}
+
+// ---------------------------------------------------------------------------
+// Time stepping
+// ---------------------------------------------------------------------------
+int crimson_set_inflow(crimson_ctx* c, int ninlet, const int* nodes, const double* profile) {
+    if (!c || ninlet < 0 || (ninlet > 0 && (!nodes || !profile))) return CRIMSON_ERR_ARG;
+    std::vector<int> g(ninlet);
+    for (int t = 0; t < ninlet; ++t) {
+        g[t] = nodes[t] - 1;
+        if (g[t] < 0 || g[t] >= c->nshg) return CRIMSON_ERR_ARG;
+    }
+    c->ninlet = ninlet;
+    CR_CHECK(c->inlet_nodes.upload(g.data(), g.size(), c->stream));
+    CR_CHECK(c->inlet_profile.upload(profile, 3 * (size_t)ninlet, c->stream));
+    CR_CUDA(cudaStreamSynchronize(c->stream));
+    return CRIMSON_OK;
+}
+
+int crimson_set_rcr(crimson_ctx* c, int n, const double* Rp, const double* C, const double* Rd, const double* Pd) {
+    if (!c || n != c->ncoupled) return CRIMSON_ERR_ARG;
+    c->rcr_Rp.assign(Rp, Rp + n);
+    c->rcr_C.assign(C, C + n);
+    c->rcr_Rd.assign(Rd, Rd + n);
+    c->rcr_Pd.assign(Pd, Pd + n);
+    c->rcr_Pn.assign(n, 0.0);
+    c->rcr_Qn.assign(n, 0.0);
+    return CRIMSON_OK;
+}
+
+int crimson_state_set(crimson_ctx* c, const double* y, const double* ac) {
+    if (!c || !y || !ac) return CRIMSON_ERR_ARG;
+    const int n = c->nshg;
+    cudaStream_t s = c->stream;
+    for (DBuf<double>* b : {&c->yold, &c->acold, &c->ycur, &c->accur, &c->yalpha, &c->acalpha, &c->solinc, &c->res4})
+        CR_CHECK(b->alloc(4 * (size_t)n));
+    DBuf<double> tmp;
+    CR_CHECK(tmp.alloc(4 * (size_t)n));
+    CR_CUDA(cudaMemcpyAsync(tmp.p, y, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s));
+    k_soa_to_node4<<<grid_for(n, 256), 256, 0, s>>>(tmp.p, n, n, c->yold.p);
+    CR_CUDA(cudaStreamSynchronize(s));
+    CR_CUDA(cudaMemcpyAsync(tmp.p, ac, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s));
+    k_soa_to_node4<<<grid_for(n, 256), 256, 0, s>>>(tmp.p, n, n, c->acold.p);
+    CR_CUDA(cudaStreamSynchronize(s));
+    c->istep = 0;
+    return CRIMSON_OK;
+}
+
+int crimson_state_get(crimson_ctx* c, double* y, double* ac) {
+    if (!c || !c->yold.p) return CRIMSON_ERR_STATE;
+    const int n = c->nshg;
+    cudaStream_t s = c->stream;
+    DBuf<double> tmp;
+    CR_CHECK(tmp.alloc(4 * (size_t)n));
+    if (y) {
+        k_node4_to_soa<<<grid_for(n, 256), 256, 0, s>>>(c->yold.p, n, tmp.p);
+        CR_CUDA(cudaMemcpyAsync(y, tmp.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+    }
+    if (ac) {
+        k_node4_to_soa<<<grid_for(n, 256), 256, 0, s>>>(c->acold.p, n, tmp.p);
+        CR_CUDA(cudaMemcpyAsync(ac, tmp.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+    }
+    return CRIMSON_OK;
+}
+
+int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_step_args* args,
+                 crimson_step_stats* st) {
+    if (!c || !L || !ls || !args) return CRIMSON_ERR_ARG;
+    if (!c->yold.p) return CRIMSON_ERR_STATE;
+    if (args->nitr < 1 || args->nitr > 16) return CRIMSON_ERR_ARG;
+    if (L->nFaces != 1 + c->ncoupled) return CRIMSON_ERR_STATE;
+    cudaStream_t s = c->stream;
+    const crimson_params& P = c->p;
+    const int n = c->nshg;
+    if (c->nnz == 0) CR_CHECK(build_pattern(c));
+    CR_CHECK(c->lhsK.alloc(9 * (size_t)c->nnz));
+    CR_CHECK(c->lhsP.alloc(4 * (size_t)c->nnz));
+    const int nb = P.ndofBC;
+    if (c->ninlet > 0)
+        k_inflow<<<grid_for(c->ninlet, 256), 256, 0, s>>>(c->inlet_nodes.p, c->inlet_profile.p, c->ninlet,
+                                                          args->inflow_scale, nb, c->BC.p);
+    const double fct = (P.gami - 1.0) / P.gami;
+    k_predict<<<grid_for(4LL * n, 256), 256, 0, s>>>(c->yold.p, c->acold.p, c->ycur.p, c->accur.p, 4LL * n, fct);
+    k_itrbc<<<grid_for(n, 256), 256, 0, s>>>(c->iBC.p, c->BC.p, nb, n, c->ycur.p);
+    const int nc = c->ncoupled;
+    std::vector<double> c1(nc), c2(nc), faceRes(1 + nc, 0.0);
+    for (int k = 0; k < nc; ++k)
+        rcr_coeffs(c->rcr_Rp[k], c->rcr_C[k], c->rcr_Rd[k], c->rcr_Pd[k], c->rcr_Pd[k], c->rcr_Pn[k], c->rcr_Qn[k],
+                   P.alfi * P.Delt, &c1[k], &c2[k]);
+    for (int k = 0; k < nc; ++k) faceRes[1 + k] = c1[k] * P.alfi * P.gami * P.Delt;
+    std::vector<int> incL(1 + nc, 1);
+    if (st) std::memset(st, 0, sizeof(*st));
+    for (int it = 0; it < args->nitr; ++it) {
+        k_yalpha<<<grid_for(n, 256), 256, 0, s>>>(c->yold.p, c->acold.p, c->ycur.p, c->accur.p, c->yalpha.p,
+                                                  c->acalpha.p, n, P.alfi, P.almi);
+        CR_CHECK(elmgmr_device(c, c->yalpha.p, c->acalpha.p, c1.data(), c2.data(), c->res4.p, c->lhsK.p, c->lhsP.p, 1));
+        crimson_ls_stats lst;
+        CR_CHECK(memls_solve_lhs_device(L, ls, c->res4.p, c->lhsK.p, c->lhsP.p, incL.data(), faceRes.data(),
+                                        c->solinc.p, &lst));
+        k_correct<<<grid_for(n, 256), 256, 0, s>>>(c->ycur.p, c->accur.p, c->solinc.p, n, P.gami * P.Delt,
+                                                   P.gami * P.alfi * P.Delt);
+        k_itrbc<<<grid_for(n, 256), 256, 0, s>>>(c->iBC.p, c->BC.p, nb, n, c->ycur.p);
+        if (st) {
+            st->ri_itr[it] = lst.RI.itr;
+            st->gm_itr[it] = lst.GM.itr;
+            st->cg_itr[it] = lst.CG.itr;
+            st->ri_inorm[it] = lst.RI.iNorm;
+            st->ri_fnorm[it] = lst.RI.fNorm;
+            st->nsolves = it + 1;
+        }
+    }
+    // RCR history update at t_{n+1} (AbstractBoundaryCondition.cxx:55-91)
+    if (nc > 0) {
+        DBuf<double> q;
+        CR_CHECK(q.alloc(nc));
+        for (int k = 0; k < nc; ++k)
+            k_flowq_step<<<1, 256, 0, s>>>(c->onodes.p, c->onode_off[k], c->onode_off[k + 1], c->onabi.p,
+                                           reinterpret_cast<const double4*>(c->ycur.p), q.p + k);
+        std::vector<double> hq(nc);
+        CR_CUDA(cudaMemcpyAsync(hq.data(), q.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+        for (int k = 0; k < nc; ++k) {
+            double d1, h1;
+            rcr_coeffs(c->rcr_Rp[k], c->rcr_C[k], c->rcr_Rd[k], c->rcr_Pd[k], c->rcr_Pd[k], c->rcr_Pn[k], c->rcr_Qn[k],
+                       P.Delt, &d1, &h1);
+            c->rcr_Pn[k] = d1 * hq[k] + h1;
+            c->rcr_Qn[k] = hq[k];
+            if (st && k < 8) {
+                st->q_out[k] = hq[k];
+                st->p_out[k] = c->rcr_Pn[k];
+            }
+        }
+    }
+    CR_CUDA(cudaMemcpyAsync(c->yold.p, c->ycur.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToDevice, s));
+    CR_CUDA(cudaMemcpyAsync(c->acold.p, c->accur.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToDevice, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    CR_CUDA(cudaGetLastError());
+    c->istep += 1;
+    return CRIMSON_OK;
+}
+
+}  // extern "C"
+
+namespace crimson {
+
+__global__ void k_diag_trans_only(const int* __restrict__ rowptr, const int* __restrict__ col, int n,
+                                  int* __restrict__ diag, int* __restrict__ trans, int* __restrict__ bad) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int d = -1;
+        for (int j = rowptr[i]; j < rowptr[i + 1]; ++j) {
+            if (col[j] == i) d = j;
+            const int c = col[j];
+            int t = -1, lo = rowptr[c], hi = rowptr[c + 1];
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if (col[mid] < i)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            if (lo < rowptr[c + 1] && col[lo] == i) t = lo;
+            trans[j] = t;
+            if (t < 0) atomicAdd(bad, 1);
+        }
+        diag[i] = d;
+        if (d < 0) atomicAdd(bad, 1);
+    }
+}
+
+// diagPtr (memLS.f90:1121-1131) and the transpose map for a caller-given pattern
+int pattern_aux(crimson_lhs* L) {
+    CR_CHECK(L->own_diag.alloc((size_t)L->nNo));
+    CR_CHECK(L->own_trans.alloc((size_t)L->nnz));
+    DBuf<int> bad;
+    CR_CHECK(bad.alloc(1));
+    CR_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), L->stream));
+    k_diag_trans_only<<<grid_for(L->nNo, 128), 128, 0, L->stream>>>(L->rowptr, L->col, L->nNo, L->own_diag.p,
+                                                                     L->own_trans.p, bad.p);
+    int hb = 0;
+    CR_CUDA(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, L->stream));
+    CR_CUDA(cudaStreamSynchronize(L->stream));
+    if (hb) {
+        set_last_error("pattern without diagonal or not structurally symmetric");
+        return CRIMSON_ERR_PATTERN;
+    }
+    L->diag = L->own_diag.p;
+    L->trans = L->own_trans.p;
+    return CRIMSON_OK;
+}
+
+}  // namespace crimson

@@ -1,0 +1,62 @@
+// memLS handles shared by memls.cu and capi.cu.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace crimson {
+
+struct RedScratch {
+    DBuf<double> part;          // partial sums, kMaxBlocks per concurrent slot
+    DBuf<unsigned int> ticket;  // one counter per slot
+    static constexpr int kMaxBlocks = 1184;   // 148 SMs x 8
+    static constexpr int kSlots = 4;
+    int init() {
+        CR_CHECK(part.alloc((size_t)kMaxBlocks * kSlots));
+        CR_CHECK(ticket.alloc(kSlots));
+        CR_CUDA(cudaMemset(ticket.p, 0, sizeof(unsigned int) * kSlots));
+        return CRIMSON_OK;
+    }
+};
+
+}  // namespace crimson
+
+using crimson::DBuf;
+using crimson::RedScratch;
+
+struct MemlsFace {
+    int nNo = 0, dof = 0, bGrp = CRIMSON_BC_TYPE_DIR;
+    bool incFlag = true, coupledFlag = false, created = false;
+    double res = 0.0, nS = 0.0;
+    DBuf<int> glob;
+    DBuf<double> val, valM;
+};
+
+struct crimson_lhs {
+    int gnNo = 0, nNo = 0, nFaces = 0;
+    long long nnz = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    // pattern (owned or borrowed from a ctx)
+    DBuf<int> own_rowptr, own_col, own_diag, own_trans;
+    const int* rowptr = nullptr;
+    const int* col = nullptr;
+    const int* diag = nullptr;
+    const int* trans = nullptr;
+    std::vector<MemlsFace> face;
+    // work space
+    DBuf<double> W, R, Val, mK, mG, mD, mL, Gt;
+    DBuf<double> Rm, Rc, Rmi, Rci, U, P, MU, MP, X3, basis, w3;
+    DBuf<double> cgX, cgP, cgSP, cgGP, cgR;
+    DBuf<double> scal;      // device scalars
+    RedScratch red;
+    double* hscal = nullptr;   // pinned host mirror of scal
+    int sD = 0, iBcap = 0;
+};
+
+struct crimson_ls {
+    crimson_subls GM{}, CG{}, RI{};
+    int LS_type = CRIMSON_LS_TYPE_NS, Resm = 0, Resc = 0;
+};
+

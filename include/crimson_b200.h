@@ -1,0 +1,207 @@
+/*
+ * crimson_b200 -- B200 (sm_100a) implementation of the CRIMSON flow solver's
+ * element assembly (ElmGMR) and memLS Navier-Stokes linear solve.
+ *
+ * C ABI: plain pointers and sizes only.  Every entry point returns an int
+ * status (CRIMSON_OK = 0) instead of the reference's PRINT + STOP.
+ *
+ * Array conventions follow the reference's Fortran arrays (column-major,
+ * 1-based node and CSR indices) on every host-pointer entry point:
+ *   ien   (nelem, 4)     int    ien[a*nelem + e], 1-based node numbers
+ *   x     (numnp, 3)     double x[d*numnp + i]
+ *   y, ac, res (nshg, 4) double y[d*nshg + i], dofs (u, v, w, p)
+ *   iBC   (nshg)         int    bit 2 pressure, bits 3,4,5 velocity, bit 11 plane
+ *   BC    (nshg, ndofBC) double BC[c*nshg + i]
+ *   colm  (nshg+1)       int    row pointer, 1-based   (the reference's naming)
+ *   rowp  (nnz)          int    column indices, 1-based, sorted in each row
+ *   lhsK  (9, nnz)       double row-major 3x3 momentum blocks
+ *   lhsP  (4, nnz)       double (G^T row D, PSPG C) per block
+ *   ienb  (nface, 4)     int    boundary face nodes first, opposite node last
+ *   iBCB  (nface, 2)     int    (flag bits, surface id)
+ *   BCB   (nface, 3, 6)  double BCB[(c*3 + n)*nface + f]
+ *   NABI  (nshg, 3)      double integral of N_a n over coupled outlets
+ *   Ri    (dof, nNo)     double memLS right-hand side / solution
+ *   Val   (dof*dof, nnz) double memLS block matrix, row-major blocks
+ *
+ * Entry points with the suffix _device take device pointers in the solver's
+ * node-major layout (dof, nshg) -- the layout of memLS's R(dof, nNo) -- and
+ * launch on the context's CUDA stream.
+ *
+ * Threading: one host thread per context; calls on a context are ordered on
+ * its stream.  No global mutable state.
+ */
+#ifndef CRIMSON_B200_H
+#define CRIMSON_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CRIMSON_OK 0
+#define CRIMSON_ERR_ARG 1
+#define CRIMSON_ERR_UNSUPPORTED 2
+#define CRIMSON_ERR_CUDA 3
+#define CRIMSON_ERR_OOM 4
+#define CRIMSON_ERR_PATTERN 5
+#define CRIMSON_ERR_SINGULAR 6
+#define CRIMSON_ERR_NONFINITE 7
+#define CRIMSON_ERR_STATE 8
+
+/* Precision of the element quadrature and inner Krylov arithmetic. */
+#define CRIMSON_FP64 0
+#define CRIMSON_MIXED 1
+
+typedef struct crimson_ctx crimson_ctx;
+typedef struct crimson_lhs crimson_lhs;
+typedef struct crimson_ls crimson_ls;
+
+/* Flow / time-integration / stabilisation settings.  The fields are the
+ * module variables ElmGMR reads implicitly (phcommonvars: datmat, alfi, almi,
+ * gami, Delt, Dtgl, dtsfct, taucfct, flmpl, flmpr, stabflux_coeff, idiff,
+ * iconvflow, itau, ibksiz) -- flowsolver/src/elmgmr.f90:21-30. */
+typedef struct {
+    double rho, mu;
+    double alfi, almi, gami;
+    double Delt, Dtgl;
+    double dtsfct, taucfct;
+    double flmpl, flmpr;
+    double stabflux_coeff;
+    int idiff, iconvflow, itau, ibksiz, ndofBC, nthreads;
+} crimson_params;
+
+/* memLS statistics, field for field memLS_subLsType
+ * (flowsolver/src/memLS.f90:159-188). */
+typedef struct {
+    double absTol, relTol, iNorm, fNorm, dB, callD;
+    int suc, mItr, sD, itr, cM, cN, cD, reserve;
+} crimson_subls;
+
+typedef struct {
+    crimson_subls GM, CG, RI;
+    int LS_type, Resm, Resc;
+} crimson_ls_stats;
+
+/* ---------------------------------------------------------------------------
+ * Context: mesh, boundary data and device work space.
+ * Replaces the state the reference builds in input/proces/genblk and keeps in
+ * pointer_data (mien blocks, x) -- flowsolver/src/genblk.f90:33-62,
+ * flowsolver/src/readnblk.f90:33.
+ * ------------------------------------------------------------------------- */
+int crimson_ctx_create(crimson_ctx** ctx, const crimson_params* p, int nshg, int numnp, int nelem,
+                       const int* ien, const double* x);
+int crimson_ctx_destroy(crimson_ctx* ctx);
+int crimson_set_params(crimson_ctx* ctx, const crimson_params* p);
+/* iBC / BC as passed to ElmGMR (flowsolver/src/elmgmr.f90:1-8) */
+int crimson_set_bc(crimson_ctx* ctx, const int* iBC, const double* BC);
+/* boundary element blocks mienb / miBCB / mBCB used by AsBMFG
+ * (flowsolver/src/elmgmr.f90:325-460) */
+int crimson_set_boundary(crimson_ctx* ctx, int nface, const int* ienb, const int* iBCB, const double* BCB);
+/* coupled outlet surfaces: nsrflistGRCR, ndsurf, NABI (flowsolver/src/pvsqbi.f90:28,
+ * flowsolver/src/elmgmr.f90:1271-1330) */
+int crimson_set_outlets(crimson_ctx* ctx, int ncoupled, const int* srflist, const int* ndsurf, const double* NABI);
+
+/* ---------------------------------------------------------------------------
+ * Sparse pattern: genadj(colm, rowp, icnt) -- flowsolver/src/genadj.f90:1.
+ * Builds the node-graph CSR pattern on the device (bit-identical to genadj:
+ * sorted columns, diagonal included, 1-based).  colm/rowp may be NULL to only
+ * build it and query nnz_tot; rowp needs room for cap entries.
+ * ------------------------------------------------------------------------- */
+int crimson_genadj(crimson_ctx* ctx, int* colm, int* rowp, long long cap, long long* nnz_tot);
+
+/* ---------------------------------------------------------------------------
+ * Assembly: ElmGMR(u, y, ac, x, ..., iBC, BC, ..., res, ..., rowp, colm, lhsK,
+ * lhsP, ...) -- flowsolver/src/elmgmr.f90:1-8, called from SolFlow
+ * (flowsolver/src/solfar.f90:148).  Host arrays in the reference layout.
+ * coef1/coef2 are the implicit coefficients (dp/dq, Hop) of the coupled
+ * surfaces (callCppGetImplicitCoeff_rcr, flowsolver/src/elmgmr.f90:1298).
+ * lhs = 1 forms lhsK/lhsP (the reference's lhs flag).
+ * ------------------------------------------------------------------------- */
+int crimson_elmgmr(crimson_ctx* ctx, const double* y, const double* ac, const double* coef1, const double* coef2,
+                   double* res, double* lhsK, double* lhsP, int lhs);
+/* Device-resident ElmGMR: y, ac, res node-major (4, nshg); lhsK (9, nnz),
+ * lhsP (4, nnz) on the device. */
+int crimson_elmgmr_device(crimson_ctx* ctx, const double* d_y, const double* d_ac, const double* coef1,
+                          const double* coef2, double* d_res, double* d_lhsK, double* d_lhsP, int lhs);
+
+/* ---------------------------------------------------------------------------
+ * memLS (flowsolver/src/memLS.f90): NS solver type only.
+ * ------------------------------------------------------------------------- */
+#define CRIMSON_LS_TYPE_NS 3
+#define CRIMSON_BC_TYPE_DIR 0
+#define CRIMSON_BC_TYPE_NEU 1
+/* memLS_LS_CREATE(ls, LS_type, relTol, absTol, maxItr, dimKry, relTolIn,
+ * absTolIn, maxItrIn) -- flowsolver/src/memLS.f90:1379.  present_mask bits mark
+ * the optional arguments given: 1 relTol, 2 absTol, 4 maxItr, 8 dimKry,
+ * 16 relTolIn, 32 absTolIn, 64 maxItrIn. */
+int crimson_memls_ls_create(crimson_ls** ls, int LS_type, int present_mask, double relTol, double absTol,
+                            int maxItr, int dimKry, const double* relTolIn, const double* absTolIn,
+                            const int* maxItrIn);
+int crimson_memls_ls_free(crimson_ls* ls);
+/* memLS_LHS_CREATE(lhs, commu, gnNo, nNo, nnz, gNodes, rowPtr, colPtr, nFaces)
+ * -- flowsolver/src/memLS.f90:1080 (single task; rowPtr = colm, colPtr = rowp) */
+int crimson_memls_lhs_create(crimson_lhs** lhs, int gnNo, int nNo, long long nnz, const int* gNodes,
+                             const int* rowPtr, const int* colPtr, int nFaces);
+/* Same, sharing the pattern already built on the device by crimson_genadj. */
+int crimson_memls_lhs_create_from_ctx(crimson_lhs** lhs, crimson_ctx* ctx, int nFaces);
+int crimson_memls_lhs_free(crimson_lhs* lhs);
+/* memLS_BC_CREATE(lhs, faIn, nNo, dof, BC_type, gNodes, Val) -- memLS.f90:272 */
+int crimson_memls_bc_create(crimson_lhs* lhs, int faIn, int nNo, int dof, int BC_type, const int* gNodes,
+                            const double* Val);
+/* memLS_SOLVE(lhs, ls, dof, Ri, Val, incL, res) -- flowsolver/src/memLS.f90:1947.
+ * Host arrays.  As in the reference, Ri returns the solution and Val returns
+ * scaled in place by the diagonal preconditioner. */
+int crimson_memls_solve(crimson_lhs* lhs, crimson_ls* ls, int dof, double* Ri, double* Val, const int* incL,
+                        const double* res, crimson_ls_stats* stats);
+
+/* ---------------------------------------------------------------------------
+ * SolFlow's pack + solve on the device (flowsolver/src/solfar.f90:210-280):
+ * Res4 = res, Val4 from lhsK/lhsP (with the transposed -G blocks found by a
+ * precomputed transpose map instead of the search), memLS_SOLVE, solinc.
+ * d_res (4, nshg) node-major in, d_solinc (4, nshg) out.  lhs must come from
+ * crimson_memls_lhs_create_from_ctx.  faceRes has nFaces entries.
+ * ------------------------------------------------------------------------- */
+int crimson_solflow_device(crimson_ctx* ctx, crimson_lhs* lhs, crimson_ls* ls, const double* d_res,
+                           const double* d_lhsK, const double* d_lhsP, const int* incL, const double* faceRes,
+                           double* d_solinc, crimson_ls_stats* stats);
+
+/* ---------------------------------------------------------------------------
+ * Device-resident time step: itrdrv_iter_step (flowsolver/src/itrdrv.f90:1239)
+ * = itrPredict, itrBC, nitr x [itrYAlpha, ElmGMR, SolFlow pack + memLS_SOLVE,
+ * itrCorrect, itrBC], with RCR outlets (flowsolver/src/RCR.cxx:49-81).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    int nitr;               /* solve/update pairs per step (Step Construction) */
+    double inflow_scale;    /* multiplies the registered inlet profile at t_{n+1} */
+} crimson_step_args;
+
+typedef struct {
+    int nsolves;
+    int ri_itr[16], gm_itr[16], cg_itr[16];
+    double ri_inorm[16], ri_fnorm[16];
+    double q_out[8], p_out[8];   /* outlet flow and pressure at t_{n+1} */
+} crimson_step_stats;
+
+/* register the inlet profile: BC(node, 3:5) = profile * inflow_scale */
+int crimson_set_inflow(crimson_ctx* ctx, int ninlet, const int* nodes, const double* profile);
+/* RCR outlets on the coupled surfaces, in srflist order */
+int crimson_set_rcr(crimson_ctx* ctx, int n, const double* Rp, const double* C, const double* Rd, const double* Pd);
+/* yold/acold in the reference layout (nshg, 4) */
+int crimson_state_set(crimson_ctx* ctx, const double* y, const double* ac);
+int crimson_state_get(crimson_ctx* ctx, double* y, double* ac);
+int crimson_step(crimson_ctx* ctx, crimson_lhs* lhs, crimson_ls* ls, const crimson_step_args* args,
+                 crimson_step_stats* stats);
+
+/* The CUDA stream (cudaStream_t) every call on this context launches on. */
+void* crimson_ctx_stream(crimson_ctx* ctx);
+
+/* Library version and build target, for diagnostics. */
+const char* crimson_version(void);
+/* Last CUDA error string seen by this library (diagnostics). */
+const char* crimson_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1393,6 +1393,9 @@ int NSSOLVER(int dof, Lhs& L, Ls& ls, const double* Val, double* Ri) {
         double sxb = 0.0;
         for (int t = 0; t < iBB; ++t) sxb = sxb + xB[t] * B[t];
         ls.RI.fNorm = std::sqrt(std::pow(ls.RI.iNorm, 2.0) - sxb);
+        if (std::getenv("CRIMSON_ORACLE_VERBOSE"))
+            std::fprintf(stderr, "NSSOLVER i=%d fNorm/iNorm=%.6e GM.itr=%d CG.itr=%d\n", i, ls.RI.fNorm / ls.RI.iNorm,
+                         ls.GM.itr, ls.CG.itr);
         if (ls.RI.fNorm < eps) {
             ls.RI.suc = 1;
             break;
