@@ -1,0 +1,353 @@
+"""Benchmark: s/timestep of the ElmGMR + memLS hot path on a 4M-tet cylinder.
+
+Workload (one "step" = one time step, itrdrv_iter_step): a 4.0M-tet jittered
+cylinder (R = 1 cm, L = 10 cm, 80x80 cross-section masked to the disc, 133
+layers, 6 tets per hex), pulsatile parabolic inflow 10 + 5 sin(2 pi t / 0.8)
+cm/s, one RCR outlet (Rp = 100, C = 1e-4, Rd = 1000), rho = 1.06, mu = 0.04,
+dt = 1e-3 s, 3 nonlinear iterations (ElmGMR + memLS NS solve + correct) per
+step, FP64 throughout.  Inputs are synthetic and seeded.
+
+Multi-GPU: the path does not shard (one GPU, no domain decomposition), so
+``--gpus N`` under torchrun runs N independent replicas; time is the max over
+ranks and ``value`` counts every rank's time steps (weak scaling).
+
+``--impl reference`` times the CPU oracle (the reference algorithm restated
+in C++, all host threads) on a bounded sample of the same workload and scales
+it to one time step using the solver's per-iteration costs.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s/timestep @4M tets (mixed vs FP64 GPU, ≤1e-6 rel err); Melem/s assembly"
+NCROSS, NAXIAL = 80, 133
+NITR = 3
+# Outer NS iterations and inner GMRES / CG iteration totals per memLS solve on
+# this workload, as counted by the solver on steps 2-5 (identical algorithm
+# and counts on CPU and GPU, see tests/test_gpu_parity.py).  Used only to
+# scale the CPU sample of --impl reference when it runs without a GPU.
+SOLVE_ITERS = {"ri": 5.7, "gm": 77.0, "cg": 2330.0}
+
+
+def _inflow(t: float) -> float:
+    return 10.0 + 5.0 * np.sin(2.0 * np.pi * t / 0.8)
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    return ws, rank
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int = 0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([v.strip() for v in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 4 + i and "Active" in s[4 + i]
+                          and "Not" not in s[4 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def make_problem(ncross: int, naxial: int):
+    from crimsonflowsolver_b200 import FlowParams, RCR, mesh
+
+    m = mesh.cylinder(ncross=ncross, naxial=naxial, seed=1)
+    P = FlowParams(rcr=[RCR(srfid=3, Rp=100.0, C=1e-4, Rd=1000.0)], nitr=NITR)
+    return m, P
+
+
+def cpu_sample(m, P, nthreads: int, iters=None):
+    """Time the oracle on one bounded sample of a time step and scale to a step.
+
+    Sample: one ElmGMR (residual + tangent), the SolFlow pack, and one memLS
+    solve cut to a single NSSOLVER outer iteration, at the full workload size.
+    Per-iteration GMRES and CG costs come from the oracle's own callD timers;
+    a full step = nitr x (ElmGMR + pack + outer iterations x (per-outer
+    overhead) + GMRES its x t_gm + CG its x t_cg).
+    """
+    from oracle import pyoracle as po
+
+    iters = iters or SOLVE_ITERS
+    colm, rowp = po.genadj(m.ien, m.nshg)
+    elm = po.Elm(m, P, colm, rowp, nthreads=nthreads)
+    m.set_inflow(_inflow(P.Delt))
+    y = np.zeros((m.nshg, 4))
+    full = ((m.iBC >> 3) & 7) == 7
+    y[full, 0:3] = m.BC[full, 2:5]
+    ac = np.zeros_like(y)
+    c1, c2 = po.rcr_coeffs(100.0, 1e-4, 1000.0, 0.0, 0.0, 0.0, 0.0, P.alfi * P.Delt)
+    t0 = time.perf_counter()
+    out = elm(y, ac, srflist=[3], coef1=[c1], coef2=[c2])
+    t_elm = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    Res4, Val4 = po.solflow_pack(m.nshg, colm, rowp, out["res"], out["lhsK"], out["lhsP"])
+    t_pack = time.perf_counter() - t0
+    from crimsonflowsolver_b200 import FlowParams
+
+    P1 = FlowParams(**{**P.__dict__, "nprjs": 1})
+    ms = po.MemLS(m.nshg, colm, rowp, 2, P1, nthreads=nthreads)
+    nodes, sv = po.dirichlet_face(m)
+    ms.bc_create(1, nodes, 3, 0, sv)
+    nn, vv = po.neumann_face(m, 3)
+    ms.bc_create(2, nn, 3, 1, vv)
+    t0 = time.perf_counter()
+    _, st = ms.solve(Res4, Val4, [0.0, c1 * P.alfi * P.gami * P.Delt])
+    t_solve = time.perf_counter() - t0
+    t_gm = st.GM.callD / max(st.GM.itr, 1)
+    t_cg = st.CG.callD / max(st.CG.itr, 1)
+    t_outer = max(t_solve - st.GM.callD - st.CG.callD, 0.0)
+    t_step = P.nitr * (t_elm + t_pack + iters["ri"] * t_outer + iters["gm"] * t_gm + iters["cg"] * t_cg)
+    sample = (f"full-size ElmGMR {t_elm:.2f}s + pack {t_pack:.2f}s + 1 NSSOLVER outer iteration {t_solve:.2f}s "
+              f"(GM {st.GM.itr} its, CG {st.CG.itr} its); scaled to {P.nitr} solves x ({iters['ri']:.1f} outer, "
+              f"{iters['gm']:.0f} GMRES, {iters['cg']:.0f} CG its)")
+    return t_step, sample, t_elm + t_pack + t_solve
+
+
+def run_reference(args):
+    ws, rank = _dist()
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    m, P = make_problem(args.ncross, args.naxial)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, sample, wall = cpu_sample(m, P, nthreads)
+        if i >= args.warmup:
+            vals.append(v)
+    value = float(np.median(vals))
+    line = {"metric": METRIC, "value": value, "unit": "s/timestep", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"4.0M-tet cylinder ({m.nelem} tets, {m.nshg} nodes), pulsatile inflow, RCR "
+                                   "outlet, dt=1e-3, 3 nonlinear iterations/step, FP64",
+                       "parallelism": "replicas"},
+            "cpu_baseline": {"value": value, "unit": "s/timestep", "cores": nthreads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "s/timestep", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    from crimsonflowsolver_b200 import _native as N
+    from crimsonflowsolver_b200 import solver
+
+    ws, rank = _dist()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    m, P = make_problem(args.ncross, args.naxial)
+    F = solver.FlowSolver(m, P, inflow=_inflow)
+    stream = torch.cuda.ExternalStream(F.elm.stream_handle)
+    L = N.lib()
+    iters = []
+    for _ in range(args.warmup):
+        F.step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = L.crimson_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            st = F.step()
+            iters.append([(st.ri_itr[i], st.gm_itr[i], st.cg_itr[i]) for i in range(st.nsolves)])
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = L.crimson_launch_count() - l0
+    t_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+        dist.barrier()
+    t_s = t_ms / 1e3
+    value = t_s / (args.steps * ws)
+    # ---- end to end through the host-buffer API: state in from pinned host, step, state out ----
+    n = m.nshg
+    y_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
+    ac_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
+    y0, a0 = F.state()
+    y_h.copy_(torch.from_numpy(np.ascontiguousarray(y0.T)))
+    ac_h.copy_(torch.from_numpy(np.ascontiguousarray(a0.T)))
+    import ctypes
+
+    yp = ctypes.cast(y_h.data_ptr(), N.c_dbl_p)
+    ap = ctypes.cast(ac_h.data_ptr(), N.c_dbl_p)
+    e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e_steps):
+        N.check(L.crimson_state_set(F.elm.h, yp, ap), "crimson_state_set")
+        F.step()
+        N.check(L.crimson_state_get(F.elm.h, yp, ap), "crimson_state_get")
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e = f0.elapsed_time(f1) / 1e3 / e_steps
+    # ---- assembly throughput and the dominant solver kernel, timed live on the library stream ----
+    dres = torch.zeros((n, 4), dtype=torch.float64, device="cuda")
+    nnz = F.elm._nnz()
+    dK = torch.empty((nnz, 9), dtype=torch.float64, device="cuda")
+    dP = torch.empty((nnz, 4), dtype=torch.float64, device="cuda")
+    dy = torch.tensor(F.state()[0], device="cuda")
+    dac = torch.tensor(F.state()[1], device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(2):
+        F.elm.device(dy, dac, dres, dK, dP, [100.0], [0.0])
+    a0e = torch.cuda.Event(enable_timing=True)
+    a1e = torch.cuda.Event(enable_timing=True)
+    a0e.record(stream)
+    reps = 5
+    for _ in range(reps):
+        F.elm.device(dy, dac, dres, dK, dP, [100.0], [0.0])
+    a1e.record(stream)
+    torch.cuda.synchronize()
+    t_asm = a0e.elapsed_time(a1e) / reps / 1e3
+    kt = {}
+    for which, name in ((0, "spmv_K"), (1, "cg_op"), (2, "spmv_G"), (3, "mgs")):
+        ms = ctypes_double()
+        N.check(L.crimson_memls_kernel_time(F.memls.lhs, which, 20, ctypes_ref(ms)), "kernel_time")
+        kt[name] = ms.value
+    peaks = _peaks()
+    # algorithmic bytes per launch (per block / per row)
+    nrow = n
+    cg_bytes = nnz * (8 + 24 + 4) + nrow * (4 + 8 + 24 + 8)
+    achieved = cg_bytes / (kt["cg_op"] / 1e3) / 1e9
+    it = np.array([s for step in iters for s in step], dtype=float)
+    line = {
+        "metric": METRIC, "value": value, "unit": "s/timestep", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"4.0M-tet cylinder ({m.nelem} tets, {n} nodes, {nnz} blocks), pulsatile inflow, "
+                               "RCR outlet, dt=1e-3, 3 nonlinear iterations/step, plain FP64",
+                   "parallelism": "replicas" if ws > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (matrices 1.3 GB per solve)"},
+        "assembly_melem_s": m.nelem / t_asm / 1e6,
+        "assembly_ms": t_asm * 1e3,
+        "solver_iters_per_solve": {"ri": float(it[:, 0].mean()), "gm": float(it[:, 1].mean()),
+                                   "cg": float(it[:, 2].mean())} if len(it) else None,
+        "kernel_ms": kt,
+        "roofline": {"kernel": "k_cg_op (SPARMULSS L + SPARMULVS Gt + DOTS)", "bound": "hbm",
+                     "achieved": achieved, "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
+                     "traffic": None, "peak_source": peaks[1]},
+        "e2e": {"value": e2e, "unit": "s/timestep", "h2d_bytes_per_step": 2 * 4 * n * 8,
+                "d2h_bytes_per_step": 2 * 4 * n * 8},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            cpu_v, sample, _ = cpu_sample(m, P, os.cpu_count() or 1,
+                                          {"ri": float(it[:, 0].mean()), "gm": float(it[:, 1].mean()),
+                                           "cg": float(it[:, 2].mean())})
+            line["cpu_baseline"] = {"value": cpu_v, "unit": "s/timestep", "cores": os.cpu_count(), "kind": "port",
+                                    "sample": sample}
+        except Exception as ex:  # the CPU baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": "s/timestep", "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"failed: {ex}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def ctypes_double():
+    import ctypes
+
+    return ctypes.c_double()
+
+
+def ctypes_ref(x):
+    import ctypes
+
+    return ctypes.byref(x)
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ncross", type=int, default=NCROSS)
+    ap.add_argument("--naxial", type=int, default=NAXIAL)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -621,8 +621,8 @@ int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const d
         CR_CHECK(c->rmass.alloc((size_t)c->nshg));
         CR_CUDA(cudaMemsetAsync(c->qres.p, 0, sizeof(double) * 9 * (size_t)c->nshg, s));
         CR_CUDA(cudaMemsetAsync(c->rmass.p, 0, sizeof(double) * (size_t)c->nshg, s));
-        k_asiq<<<grid_for(c->nelem, 256, 16), 256, 0, s>>>(c->ien.p, c->x.p, y4, c->nelem, P, c->qres.p, c->rmass.p);
-        k_qpbc<<<grid_for(c->nshg, 256), 256, 0, s>>>(c->qres.p, c->rmass.p, c->nshg);
+        launch(k_asiq, grid_for(c->nelem, 256, 16), 256, 0, s, c->ien.p, c->x.p, y4, c->nelem, P, c->qres.p, c->rmass.p);
+        launch(k_qpbc, grid_for(c->nshg, 256), 256, 0, s, c->qres.p, c->rmass.p, c->nshg);
     }
     CR_CUDA(cudaMemsetAsync(d_res, 0, sizeof(double) * 4 * (size_t)c->nshg, s));
     if (lhs) {
@@ -632,14 +632,14 @@ int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const d
     const int blk = 128;
     const int grid = grid_for((long long)c->nelem * 4, blk, 16);
     if (lhs)
-        k_asigmr<true><<<grid, blk, 0, s>>>(c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
+        launch(k_asigmr<true>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
                                             d_lhsK, d_lhsP);
     else
-        k_asigmr<false><<<grid, blk, 0, s>>>(c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
+        launch(k_asigmr<false>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
                                              nullptr, nullptr);
     CR_CUDA(cudaGetLastError());
     if (c->nface > 0)
-        k_asbmfg<<<grid_for(c->nface, 128), 128, 0, s>>>(c->ienb.p, c->iBCB.p, c->BCB.p, c->x.p, y4, c->nface, P,
+        launch(k_asbmfg, grid_for(c->nface, 128), 128, 0, s, c->ienb.p, c->iBCB.p, c->BCB.p, c->x.p, y4, c->nface, P,
                                                         d_res);
     if (c->ncoupled > 0) {
         std::vector<double> hc(2 * (size_t)c->ncoupled);
@@ -651,12 +651,12 @@ int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const d
         DBuf<int> doff;
         CR_CHECK(upload_offsets(c, doff));
         CR_CHECK(c->flowq.alloc((size_t)c->ncoupled));
-        k_flowq<<<c->ncoupled, 256, 0, s>>>(c->onodes.p, doff.p, c->onabi.p, y4, c->flowq.p);
+        launch(k_flowq, c->ncoupled, 256, 0, s, c->onodes.p, doff.p, c->onabi.p, y4, c->flowq.p);
         dim3 g2(8, c->ncoupled);
-        k_pvsq_add<<<g2, 256, 0, s>>>(c->onodes.p, doff.p, c->onabi.p, c->flowq.p, c->coefs.p, c->ncoupled, d_res);
+        launch(k_pvsq_add, g2, 256, 0, s, c->onodes.p, doff.p, c->onabi.p, c->flowq.p, c->coefs.p, c->ncoupled, d_res);
         CR_CUDA(cudaStreamSynchronize(s));   // doff is released at scope exit
     }
-    k_bc3res<<<grid_for(c->nshg, 256), 256, 0, s>>>(c->iBC.p, c->nshg, d_res);
+    launch(k_bc3res, grid_for(c->nshg, 256), 256, 0, s, c->iBC.p, c->nshg, d_res);
     CR_CUDA(cudaGetLastError());
     return CRIMSON_OK;
 }

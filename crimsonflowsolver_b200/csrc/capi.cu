@@ -1,6 +1,7 @@
 // extern "C" entry points of crimson_b200 (declared in include/crimson_b200.h).
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -11,6 +12,8 @@
 namespace crimson {
 
 thread_local std::string g_last_error;
+static std::atomic<unsigned long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void set_last_error(const std::string& s) { g_last_error = s; }
 
 int sm_count() {
@@ -25,6 +28,7 @@ int sm_count() {
 
 int build_pattern(crimson_ctx* c);
 int pattern_aux(crimson_lhs* L);
+int memls_kernel_time(crimson_lhs* L, int which, int reps, double* ms);
 int pattern_to_host(crimson_ctx* c, int* colm, int* rowp, long long cap);
 int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1, const double* coef2,
                   double* d_res, double* d_lhsK, double* d_lhsP, int lhs);
@@ -138,6 +142,11 @@ extern "C" {
 
 const char* crimson_version(void) { return "crimson_b200 0.1 sm_100a"; }
 void* crimson_ctx_stream(crimson_ctx* c) { return c ? (void*)c->stream : nullptr; }
+unsigned long long crimson_launch_count(void) { return g_launches.load(); }
+int crimson_memls_kernel_time(crimson_lhs* L, int which, int reps, double* ms) {
+    if (!L || !ms) return CRIMSON_ERR_ARG;
+    return memls_kernel_time(L, which, reps, ms);
+}
 const char* crimson_last_error(void) { return g_last_error.c_str(); }
 
 int crimson_ctx_create(crimson_ctx** out, const crimson_params* p, int nshg, int numnp, int nelem, const int* ien,
@@ -319,13 +328,13 @@ int crimson_elmgmr(crimson_ctx* c, const double* y, const double* ac, const doub
         CR_CHECK(c->lhsP.alloc(4 * (size_t)c->nnz));
     }
     CR_CUDA(cudaMemcpyAsync(tmp.p, y, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s));
-    k_soa_to_node4<<<grid_for(n, 256), 256, 0, s>>>(tmp.p, n, n, c->y4.p);
+    launch(k_soa_to_node4, grid_for(n, 256), 256, 0, s, tmp.p, n, n, c->y4.p);
     CR_CUDA(cudaStreamSynchronize(s));
     CR_CUDA(cudaMemcpyAsync(tmp.p, ac, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s));
-    k_soa_to_node4<<<grid_for(n, 256), 256, 0, s>>>(tmp.p, n, n, c->ac4.p);
+    launch(k_soa_to_node4, grid_for(n, 256), 256, 0, s, tmp.p, n, n, c->ac4.p);
     CR_CHECK(elmgmr_device(c, c->y4.p, c->ac4.p, coef1, coef2, c->res4.p, lhs ? c->lhsK.p : nullptr,
                            lhs ? c->lhsP.p : nullptr, lhs));
-    k_node4_to_soa<<<grid_for(n, 256), 256, 0, s>>>(c->res4.p, n, tmp.p);
+    launch(k_node4_to_soa, grid_for(n, 256), 256, 0, s, c->res4.p, n, tmp.p);
     CR_CUDA(cudaMemcpyAsync(res, tmp.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
     if (lhs) {
         CR_CUDA(cudaMemcpyAsync(lhsK, c->lhsK.p, sizeof(double) * 9 * (size_t)c->nnz, cudaMemcpyDeviceToHost, s));
@@ -409,8 +418,8 @@ int crimson_memls_lhs_create(crimson_lhs** out, int gnNo, int nNo, long long nnz
     if (rc == CRIMSON_OK) rc = L->own_rowptr.alloc((size_t)nNo + 1);
     if (rc == CRIMSON_OK) rc = L->own_col.alloc((size_t)nnz);
     if (rc == CRIMSON_OK) {
-        k_one_to_zero<<<grid_for(nNo + 1, 256), 256, 0, L->stream>>>(t1.p, L->own_rowptr.p, nNo + 1);
-        k_one_to_zero<<<grid_for(nnz, 256), 256, 0, L->stream>>>(t2.p, L->own_col.p, nnz);
+        launch(k_one_to_zero, grid_for(nNo + 1, 256), 256, 0, L->stream, t1.p, L->own_rowptr.p, nNo + 1);
+        launch(k_one_to_zero, grid_for(nnz, 256), 256, 0, L->stream, t2.p, L->own_col.p, nnz);
         L->rowptr = L->own_rowptr.p;
         L->col = L->own_col.p;
         rc = crimson::pattern_aux(L);
@@ -528,34 +537,30 @@ int crimson_state_set(crimson_ctx* c, const double* y, const double* ac) {
     if (!c || !y || !ac) return CRIMSON_ERR_ARG;
     const int n = c->nshg;
     cudaStream_t s = c->stream;
-    for (DBuf<double>* b : {&c->yold, &c->acold, &c->ycur, &c->accur, &c->yalpha, &c->acalpha, &c->solinc, &c->res4})
+    for (DBuf<double>* b :
+         {&c->yold, &c->acold, &c->ycur, &c->accur, &c->yalpha, &c->acalpha, &c->solinc, &c->res4, &c->stage})
         CR_CHECK(b->alloc(4 * (size_t)n));
-    DBuf<double> tmp;
-    CR_CHECK(tmp.alloc(4 * (size_t)n));
-    CR_CUDA(cudaMemcpyAsync(tmp.p, y, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s));
-    k_soa_to_node4<<<grid_for(n, 256), 256, 0, s>>>(tmp.p, n, n, c->yold.p);
+    CR_CUDA(cudaMemcpyAsync(c->stage.p, y, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s));
+    launch(k_soa_to_node4, grid_for(n, 256), 256, 0, s, c->stage.p, n, n, c->yold.p);
     CR_CUDA(cudaStreamSynchronize(s));
-    CR_CUDA(cudaMemcpyAsync(tmp.p, ac, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s));
-    k_soa_to_node4<<<grid_for(n, 256), 256, 0, s>>>(tmp.p, n, n, c->acold.p);
+    CR_CUDA(cudaMemcpyAsync(c->stage.p, ac, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s));
+    launch(k_soa_to_node4, grid_for(n, 256), 256, 0, s, c->stage.p, n, n, c->acold.p);
     CR_CUDA(cudaStreamSynchronize(s));
-    c->istep = 0;
     return CRIMSON_OK;
 }
 
 int crimson_state_get(crimson_ctx* c, double* y, double* ac) {
-    if (!c || !c->yold.p) return CRIMSON_ERR_STATE;
+    if (!c || !c->yold.p || !c->stage.p) return CRIMSON_ERR_STATE;
     const int n = c->nshg;
     cudaStream_t s = c->stream;
-    DBuf<double> tmp;
-    CR_CHECK(tmp.alloc(4 * (size_t)n));
     if (y) {
-        k_node4_to_soa<<<grid_for(n, 256), 256, 0, s>>>(c->yold.p, n, tmp.p);
-        CR_CUDA(cudaMemcpyAsync(y, tmp.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
+        launch(k_node4_to_soa, grid_for(n, 256), 256, 0, s, c->yold.p, n, c->stage.p);
+        CR_CUDA(cudaMemcpyAsync(y, c->stage.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
     }
     if (ac) {
-        k_node4_to_soa<<<grid_for(n, 256), 256, 0, s>>>(c->acold.p, n, tmp.p);
-        CR_CUDA(cudaMemcpyAsync(ac, tmp.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
+        launch(k_node4_to_soa, grid_for(n, 256), 256, 0, s, c->acold.p, n, c->stage.p);
+        CR_CUDA(cudaMemcpyAsync(ac, c->stage.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
     }
     return CRIMSON_OK;
@@ -575,11 +580,11 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
     CR_CHECK(c->lhsP.alloc(4 * (size_t)c->nnz));
     const int nb = P.ndofBC;
     if (c->ninlet > 0)
-        k_inflow<<<grid_for(c->ninlet, 256), 256, 0, s>>>(c->inlet_nodes.p, c->inlet_profile.p, c->ninlet,
+        launch(k_inflow, grid_for(c->ninlet, 256), 256, 0, s, c->inlet_nodes.p, c->inlet_profile.p, c->ninlet,
                                                           args->inflow_scale, nb, c->BC.p);
     const double fct = (P.gami - 1.0) / P.gami;
-    k_predict<<<grid_for(4LL * n, 256), 256, 0, s>>>(c->yold.p, c->acold.p, c->ycur.p, c->accur.p, 4LL * n, fct);
-    k_itrbc<<<grid_for(n, 256), 256, 0, s>>>(c->iBC.p, c->BC.p, nb, n, c->ycur.p);
+    launch(k_predict, grid_for(4LL * n, 256), 256, 0, s, c->yold.p, c->acold.p, c->ycur.p, c->accur.p, 4LL * n, fct);
+    launch(k_itrbc, grid_for(n, 256), 256, 0, s, c->iBC.p, c->BC.p, nb, n, c->ycur.p);
     const int nc = c->ncoupled;
     std::vector<double> c1(nc), c2(nc), faceRes(1 + nc, 0.0);
     for (int k = 0; k < nc; ++k)
@@ -589,15 +594,15 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
     std::vector<int> incL(1 + nc, 1);
     if (st) std::memset(st, 0, sizeof(*st));
     for (int it = 0; it < args->nitr; ++it) {
-        k_yalpha<<<grid_for(n, 256), 256, 0, s>>>(c->yold.p, c->acold.p, c->ycur.p, c->accur.p, c->yalpha.p,
+        launch(k_yalpha, grid_for(n, 256), 256, 0, s, c->yold.p, c->acold.p, c->ycur.p, c->accur.p, c->yalpha.p,
                                                   c->acalpha.p, n, P.alfi, P.almi);
         CR_CHECK(elmgmr_device(c, c->yalpha.p, c->acalpha.p, c1.data(), c2.data(), c->res4.p, c->lhsK.p, c->lhsP.p, 1));
         crimson_ls_stats lst;
         CR_CHECK(memls_solve_lhs_device(L, ls, c->res4.p, c->lhsK.p, c->lhsP.p, incL.data(), faceRes.data(),
                                         c->solinc.p, &lst));
-        k_correct<<<grid_for(n, 256), 256, 0, s>>>(c->ycur.p, c->accur.p, c->solinc.p, n, P.gami * P.Delt,
+        launch(k_correct, grid_for(n, 256), 256, 0, s, c->ycur.p, c->accur.p, c->solinc.p, n, P.gami * P.Delt,
                                                    P.gami * P.alfi * P.Delt);
-        k_itrbc<<<grid_for(n, 256), 256, 0, s>>>(c->iBC.p, c->BC.p, nb, n, c->ycur.p);
+        launch(k_itrbc, grid_for(n, 256), 256, 0, s, c->iBC.p, c->BC.p, nb, n, c->ycur.p);
         if (st) {
             st->ri_itr[it] = lst.RI.itr;
             st->gm_itr[it] = lst.GM.itr;
@@ -612,7 +617,7 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
         DBuf<double> q;
         CR_CHECK(q.alloc(nc));
         for (int k = 0; k < nc; ++k)
-            k_flowq_step<<<1, 256, 0, s>>>(c->onodes.p, c->onode_off[k], c->onode_off[k + 1], c->onabi.p,
+            launch(k_flowq_step, 1, 256, 0, s, c->onodes.p, c->onode_off[k], c->onode_off[k + 1], c->onabi.p,
                                            reinterpret_cast<const double4*>(c->ycur.p), q.p + k);
         std::vector<double> hq(nc);
         CR_CUDA(cudaMemcpyAsync(hq.data(), q.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s));
@@ -672,7 +677,7 @@ int pattern_aux(crimson_lhs* L) {
     DBuf<int> bad;
     CR_CHECK(bad.alloc(1));
     CR_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), L->stream));
-    k_diag_trans_only<<<grid_for(L->nNo, 128), 128, 0, L->stream>>>(L->rowptr, L->col, L->nNo, L->own_diag.p,
+    launch(k_diag_trans_only, grid_for(L->nNo, 128), 128, 0, L->stream, L->rowptr, L->col, L->nNo, L->own_diag.p,
                                                                      L->own_trans.p, bad.p);
     int hb = 0;
     CR_CUDA(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, L->stream));

@@ -84,6 +84,16 @@ struct DBuf {
     }
 };
 
+// Count of kernels this library has launched (diagnostics: crimson_launch_count).
+void note_launch();
+
+// Every kernel launch of the library goes through here.
+template <typename... KArgs, typename... Args>
+inline void launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+    note_launch();
+    k<<<grid, block, smem, s>>>(static_cast<KArgs>(args)...);
+}
+
 // Number of SMs of the current device (148 on B200).
 int sm_count();
 
@@ -170,7 +180,7 @@ struct crimson_ctx {
     crimson::DBuf<double> lhsK, lhsP;      // (9, nnz), (4, nnz)
 
     // time stepping state (crimson_step)
-    crimson::DBuf<double> yold, acold, ycur, accur, yalpha, acalpha, solinc;
+    crimson::DBuf<double> yold, acold, ycur, accur, yalpha, acalpha, solinc, stage;
     crimson::DBuf<int> inlet_nodes;
     crimson::DBuf<double> inlet_profile;   // (ninlet, 3)
     int ninlet = 0;

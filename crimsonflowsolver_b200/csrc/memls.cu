@@ -480,16 +480,16 @@ struct Ctx {
         return CRIMSON_OK;
     }
     void dot(const double* u, const double* v, long long n, int slot) {
-        k_dot<<<red_grid(n), 256, 0, s>>>(u, v, n, L->red.part.p, L->red.ticket.p, sc(slot));
+        launch(k_dot, red_grid(n), 256, 0, s, u, v, n, L->red.part.p, L->red.ticket.p, sc(slot));
     }
     void spmv_vv3(const double* K, const double* U, double* KU) {
-        k_spmv_vv3<<<grid_for((long long)L->nNo * kLanes, 256, 8), 256, 0, s>>>(L->rowptr, L->col, K, U, KU, L->nNo);
+        launch(k_spmv_vv3, grid_for((long long)L->nNo * kLanes, 256, 8), 256, 0, s, L->rowptr, L->col, K, U, KU, L->nNo);
     }
     void spmv_vs3(const double* K, const double* U, double* KU) {
-        k_spmv_vs3<<<grid_for((long long)L->nNo * kLanes, 256, 8), 256, 0, s>>>(L->rowptr, L->col, K, U, KU, L->nNo);
+        launch(k_spmv_vs3, grid_for((long long)L->nNo * kLanes, 256, 8), 256, 0, s, L->rowptr, L->col, K, U, KU, L->nNo);
     }
     void spmv_sv3(const double* K, const double* U, double* KU) {
-        k_spmv_sv3<<<grid_for((long long)L->nNo * kLanes, 256, 8), 256, 0, s>>>(L->rowptr, L->col, K, U, KU, L->nNo);
+        launch(k_spmv_sv3, grid_for((long long)L->nNo * kLanes, 256, 8), 256, 0, s, L->rowptr, L->col, K, U, KU, L->nNo);
     }
     void spmv_ss_into(const double* Kd, const double* U, double* KU);
     bool any_coupled() const {
@@ -503,7 +503,7 @@ struct Ctx {
         for (auto& f : L->face) {
             if (f.coupledFlag) {
                 int nsd = std::min(f.dof, dof);
-                k_face_dot<<<1, 512, 0, s>>>(f.glob.p, f.valM.p, f.dof, nsd, f.nNo, X, dof, sc(kSlotFace + k));
+                launch(k_face_dot, 1, 512, 0, s, f.glob.p, f.valM.p, f.dof, nsd, f.nNo, X, dof, sc(kSlotFace + k));
             }
             ++k;
         }
@@ -512,7 +512,7 @@ struct Ctx {
             if (f.coupledFlag) {
                 int nsd = std::min(f.dof, dof);
                 double coef = (op == 0) ? f.res : -f.res / (1.0 + f.res * f.nS);
-                k_face_axpy<<<grid_for(f.nNo, 256), 256, 0, s>>>(f.glob.p, f.valM.p, f.dof, nsd, f.nNo,
+                launch(k_face_axpy, grid_for(f.nNo, 256), 256, 0, s, f.glob.p, f.valM.p, f.dof, nsd, f.nNo,
                                                                  sc(kSlotFace + k), coef, Y, dof);
             }
             ++k;
@@ -537,7 +537,7 @@ __global__ void k_spmv_ss(const int* __restrict__ rowptr, const int* __restrict_
 }
 
 void Ctx::spmv_ss_into(const double* Kd, const double* U, double* KU) {
-    k_spmv_ss<<<grid_for((long long)L->nNo * kLanes, 256, 8), 256, 0, s>>>(L->rowptr, L->col, Kd, U, KU, L->nNo);
+    launch(k_spmv_ss, grid_for((long long)L->nNo * kLanes, 256, 8), 256, 0, s, L->rowptr, L->col, Kd, U, KU, L->nNo);
 }
 
 // GMRES (memLS.f90:681-788) on dof = 3 with K = mK; X may not alias R.
@@ -564,7 +564,7 @@ static int gmres(Ctx& C, crimson_subls& ls, const double* K, const double* R, do
             ls.itr = ls.itr + 1;
             C.spmv_vv3(K, X, U(0));
             C.addbcmul(0, dof, X, U(0));
-            k_sub<<<grid_for(n, 256), 256, 0, s>>>(R, U(0), U(0), n);
+            launch(k_sub, grid_for(n, 256), 256, 0, s, R, U(0), U(0), n);
         }
         if (coupled) {
             CR_CUDA(cudaMemcpyAsync(L->w3.p, U(0), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
@@ -585,7 +585,7 @@ static int gmres(Ctx& C, crimson_subls& ls, const double* K, const double* R, do
             eps = std::max(ls.absTol, ls.relTol * eps);
         }
         ls.dB = ls.fNorm;
-        k_divide<<<grid_for(n, 256), 256, 0, s>>>(U(0), C.sc(kSlotNrm), U(0), n, 1);
+        launch(k_divide, grid_for(n, 256), 256, 0, s, U(0), C.sc(kSlotNrm), U(0), n, 1);
         for (i = 1; i <= sD; ++i) {
             ls.itr = ls.itr + 1;
             double* w = U(i);
@@ -598,12 +598,12 @@ static int gmres(Ctx& C, crimson_subls& ls, const double* K, const double* R, do
             // fused modified Gram-Schmidt
             for (int j = 1; j <= i; ++j) {
                 const double* uprev = (j == 1) ? nullptr : U(j - 2);
-                k_mgs<<<red_grid(n), 256, 0, s>>>(w, uprev, C.sc(kSlotH + j - 2), U(j - 1), n, L->red.part.p,
+                launch(k_mgs, red_grid(n), 256, 0, s, w, uprev, C.sc(kSlotH + j - 2), U(j - 1), n, L->red.part.p,
                                                   L->red.ticket.p, C.sc(kSlotH + j - 1));
             }
-            k_mgs<<<red_grid(n), 256, 0, s>>>(w, U(i - 1), C.sc(kSlotH + i - 1), w, n, L->red.part.p, L->red.ticket.p,
+            launch(k_mgs, red_grid(n), 256, 0, s, w, U(i - 1), C.sc(kSlotH + i - 1), w, n, L->red.part.p, L->red.ticket.p,
                                               C.sc(kSlotH + i));
-            k_divide<<<grid_for(n, 256), 256, 0, s>>>(w, C.sc(kSlotH + i), w, n, 1);
+            launch(k_divide, grid_for(n, 256), 256, 0, s, w, C.sc(kSlotH + i), w, n, 1);
             CR_CHECK(C.sync_scal(kSlotH, i + 1));
             for (int j = 1; j <= i; ++j) H(j - 1, i - 1) = L->hscal[kSlotH + j - 1];
             H(i, i - 1) = std::sqrt(L->hscal[kSlotH + i]);
@@ -633,7 +633,7 @@ static int gmres(Ctx& C, crimson_subls& ls, const double* K, const double* R, do
         }
         std::memcpy(L->hscal + kSlotY, y.data(), sizeof(double) * i);
         CR_CUDA(cudaMemcpyAsync(C.sc(kSlotY), L->hscal + kSlotY, sizeof(double) * i, cudaMemcpyHostToDevice, s));
-        k_multi_axpy<<<grid_for(n, 256), 256, 0, s>>>(X, u, C.sc(kSlotY), i, n);
+        launch(k_multi_axpy, grid_for(n, 256), 256, 0, s, X, u, C.sc(kSlotY), i, n);
         CR_CUDA(cudaStreamSynchronize(s));   // y staging buffer is reused
         ls.fNorm = std::fabs(err[i]);
         if (ls.suc) break;
@@ -681,16 +681,16 @@ static int cgrad(Ctx& C, crimson_subls& ls, const double* Gt, const double* G, c
             CR_CUDA(cudaMemcpyAsync(L->w3.p, GP, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, s));
             C.addbcmul(1, 3, L->w3.p, GP);
         }
-        k_cg_op<<<red_grid((long long)n * kLanes), 256, 0, s>>>(L->rowptr, L->col, Lm, Gt, P, GP, SP, n,
+        launch(k_cg_op, red_grid((long long)n * kLanes), 256, 0, s, L->rowptr, L->col, Lm, Gt, P, GP, SP, n,
                                                                 L->red.part.p, L->red.ticket.p, C.sc(kSlotDen));
-        k_cg_update<<<red_grid(n), 256, 0, s>>>(X, R, P, SP, n, C.sc(kSlotErrO), C.sc(kSlotDen), L->red.part.p,
+        launch(k_cg_update, red_grid(n), 256, 0, s, X, R, P, SP, n, C.sc(kSlotErrO), C.sc(kSlotDen), L->red.part.p,
                                                 L->red.ticket.p, C.sc(kSlotErr));
         CR_CHECK(C.sync_scal(kSlotErr, 1));
         double e2 = std::sqrt(L->hscal[kSlotErr]);
         err = e2 * e2;
         L->hscal[kSlotErr] = err;
         CR_CUDA(cudaMemcpyAsync(C.sc(kSlotErr), L->hscal + kSlotErr, sizeof(double), cudaMemcpyHostToDevice, s));
-        k_cg_dir<<<grid_for(n, 256), 256, 0, s>>>(P, R, n, C.sc(kSlotErr), C.sc(kSlotErrO));
+        launch(k_cg_dir, grid_for(n, 256), 256, 0, s, P, R, n, C.sc(kSlotErr), C.sc(kSlotErrO));
     }
     CR_CUDA(cudaMemcpyAsync(R, X, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     CR_CUDA(cudaStreamSynchronize(s));
@@ -753,7 +753,7 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
     auto Pcol = [&](int k) { return L->P.p + (size_t)k * nNo; };
     auto MUc = [&](int k) { return L->MU.p + (size_t)k * nv; };
     auto MPc = [&](int k) { return L->MP.p + (size_t)k * nNo; };
-    k_split4<<<grid_for(nNo, 256), 256, 0, s>>>(R, L->Rmi.p, L->Rci.p, nNo);
+    launch(k_split4, grid_for(nNo, 256), 256, 0, s, R, L->Rmi.p, L->Rci.p, nNo);
     CR_CUDA(cudaMemcpyAsync(L->Rm.p, L->Rmi.p, sizeof(double) * nv, cudaMemcpyDeviceToDevice, s));
     CR_CUDA(cudaMemcpyAsync(L->Rc.p, L->Rci.p, sizeof(double) * nNo, cudaMemcpyDeviceToDevice, s));
     std::vector<double> A((size_t)nB * nB, 0.0), B(nB, 0.0), xB(nB, 0.0);
@@ -791,10 +791,10 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
         ls->RI.dB = ls->RI.fNorm;
         CR_CHECK(gmres(C, ls->GM, mK, L->Rm.p, Ucol(i - 1)));
         C.spmv_vs3(mD, Ucol(i - 1), Pcol(i - 1));
-        k_sub<<<grid_for(nNo, 256), 256, 0, s>>>(L->Rc.p, Pcol(i - 1), Pcol(i - 1), nNo);
+        launch(k_sub, grid_for(nNo, 256), 256, 0, s, L->Rc.p, Pcol(i - 1), Pcol(i - 1), nNo);
         CR_CHECK(cgrad(C, ls->CG, Gt, mG, mL, Pcol(i - 1)));
         C.spmv_sv3(mG, Pcol(i - 1), MUc(iB - 1));
-        k_sub<<<grid_for(nv, 256), 256, 0, s>>>(L->Rm.p, MUc(iB - 1), MUc(iBB - 1), nv);
+        launch(k_sub, grid_for(nv, 256), 256, 0, s, L->Rm.p, MUc(iB - 1), MUc(iBB - 1), nv);
         CR_CHECK(gmres(C, ls->GM, mK, MUc(iBB - 1), Ucol(i - 1)));
         C.spmv_vv3(mK, Ucol(i - 1), MUc(iBB - 1));
         C.addbcmul(0, 3, Ucol(i - 1), MUc(iBB - 1));
@@ -841,8 +841,8 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
         CR_CUDA(cudaMemcpyAsync(L->Rm.p, L->Rmi.p, sizeof(double) * nv, cudaMemcpyDeviceToDevice, s));
         CR_CUDA(cudaMemcpyAsync(L->Rc.p, L->Rci.p, sizeof(double) * nNo, cudaMemcpyDeviceToDevice, s));
         for (int j = 1; j <= iBB; ++j) {
-            k_axpy<<<grid_for(nv, 256), 256, 0, s>>>(-xB[j - 1], MUc(j - 1), L->Rm.p, nv);
-            k_axpy<<<grid_for(nNo, 256), 256, 0, s>>>(-xB[j - 1], MPc(j - 1), L->Rc.p, nNo);
+            launch(k_axpy, grid_for(nv, 256), 256, 0, s, -xB[j - 1], MUc(j - 1), L->Rm.p, nv);
+            launch(k_axpy, grid_for(nNo, 256), 256, 0, s, -xB[j - 1], MPc(j - 1), L->Rc.p, nNo);
         }
     }
     if (i > ls->RI.mItr) {
@@ -850,7 +850,7 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
     } else {
         ls->RI.itr = i;
         CR_CUDA(cudaMemcpyAsync(L->Rc.p, L->Rci.p, sizeof(double) * nNo, cudaMemcpyDeviceToDevice, s));
-        for (int j = 1; j <= iBB; ++j) k_axpy<<<grid_for(nNo, 256), 256, 0, s>>>(-xB[j - 1], MPc(j - 1), L->Rc.p, nNo);
+        for (int j = 1; j <= iBB; ++j) launch(k_axpy, grid_for(nNo, 256), 256, 0, s, -xB[j - 1], MPc(j - 1), L->Rc.p, nNo);
     }
     C.dot(L->Rc.p, L->Rc.p, nNo, 0);
     CR_CHECK(C.sync_scal(0, 1));
@@ -859,13 +859,13 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
     // solution: Rmi = xB(2) U_1 + sum xB(2i) U_i ; Rci = xB(1) P_1 + sum xB(2i-1) P_i
     CR_CUDA(cudaMemsetAsync(L->Rmi.p, 0, sizeof(double) * nv, s));
     CR_CUDA(cudaMemsetAsync(L->Rci.p, 0, sizeof(double) * nNo, s));
-    k_axpy<<<grid_for(nv, 256), 256, 0, s>>>(xB[1], Ucol(0), L->Rmi.p, nv);
-    k_axpy<<<grid_for(nNo, 256), 256, 0, s>>>(xB[0], Pcol(0), L->Rci.p, nNo);
+    launch(k_axpy, grid_for(nv, 256), 256, 0, s, xB[1], Ucol(0), L->Rmi.p, nv);
+    launch(k_axpy, grid_for(nNo, 256), 256, 0, s, xB[0], Pcol(0), L->Rci.p, nNo);
     for (i = 2; i <= ls->RI.itr; ++i) {
-        k_axpy<<<grid_for(nv, 256), 256, 0, s>>>(xB[2 * i - 1], Ucol(i - 1), L->Rmi.p, nv);
-        k_axpy<<<grid_for(nNo, 256), 256, 0, s>>>(xB[2 * i - 2], Pcol(i - 1), L->Rci.p, nNo);
+        launch(k_axpy, grid_for(nv, 256), 256, 0, s, xB[2 * i - 1], Ucol(i - 1), L->Rmi.p, nv);
+        launch(k_axpy, grid_for(nNo, 256), 256, 0, s, xB[2 * i - 2], Pcol(i - 1), L->Rci.p, nNo);
     }
-    k_merge4<<<grid_for(nNo, 256), 256, 0, s>>>(R, L->Rmi.p, L->Rci.p, nNo);
+    launch(k_merge4, grid_for(nNo, 256), 256, 0, s, R, L->Rmi.p, L->Rci.p, nNo);
     CR_CUDA(cudaStreamSynchronize(s));
     ls->RI.callD = now_s() - t0;
     ls->RI.dB = 10.0 * std::log(ls->RI.fNorm / ls->RI.dB);
@@ -928,10 +928,10 @@ static int precond_faces(crimson_lhs* L, bool after_scale) {
         if (!f.created || f.nNo == 0) continue;
         if (!after_scale) {
             if (f.incFlag && f.bGrp == CRIMSON_BC_TYPE_DIR)
-                k_w_dirichlet<<<grid_for(f.nNo, 256), 256, 0, s>>>(f.glob.p, f.val.p, f.dof, std::min(f.dof, 4), f.nNo,
+                launch(k_w_dirichlet, grid_for(f.nNo, 256), 256, 0, s, f.glob.p, f.val.p, f.dof, std::min(f.dof, 4), f.nNo,
                                                                    L->W.p);
         } else if (f.coupledFlag) {
-            k_valm<<<grid_for(f.nNo, 256), 256, 0, s>>>(f.glob.p, f.val.p, f.valM.p, f.dof, std::min(f.dof, 4), f.nNo,
+            launch(k_valm, grid_for(f.nNo, 256), 256, 0, s, f.glob.p, f.val.p, f.valM.p, f.dof, std::min(f.dof, 4), f.nNo,
                                                         L->W.p);
         }
     }
@@ -948,15 +948,15 @@ int memls_solve_val(crimson_lhs* L, crimson_ls* ls, double* Ri, double* Val, con
     set_face_flags(L, incL, res);
     CR_CUDA(cudaMemcpyAsync(L->R.p, Ri, sizeof(double) * 4 * (size_t)L->nNo, cudaMemcpyHostToDevice, s));
     CR_CUDA(cudaMemcpyAsync(L->Val.p, Val, sizeof(double) * 16 * (size_t)L->nnz, cudaMemcpyHostToDevice, s));
-    k_w_from_val<<<grid_for(L->nNo, 256), 256, 0, s>>>(L->Val.p, L->diag, L->W.p, L->nNo);
+    launch(k_w_from_val, grid_for(L->nNo, 256), 256, 0, s, L->Val.p, L->diag, L->W.p, L->nNo);
     CR_CHECK(precond_faces(L, false));
-    k_scale_split_val<<<grid_for(L->nNo, 128), 128, 0, s>>>(L->Val.p, L->rowptr, L->col, L->diag, L->trans, L->W.p,
+    launch(k_scale_split_val, grid_for(L->nNo, 128), 128, 0, s, L->Val.p, L->rowptr, L->col, L->diag, L->trans, L->W.p,
                                                            L->nNo, L->mK.p, L->mG.p, L->mD.p, L->mL.p);
-    k_gt<<<grid_for(L->nnz, 256), 256, 0, s>>>(L->mG.p, L->trans, L->nnz, L->Gt.p);
-    k_mul<<<grid_for(4LL * L->nNo, 256), 256, 0, s>>>(L->R.p, L->W.p, 4LL * L->nNo);
+    launch(k_gt, grid_for(L->nnz, 256), 256, 0, s, L->mG.p, L->trans, L->nnz, L->Gt.p);
+    launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, L->W.p, 4LL * L->nNo);
     CR_CHECK(precond_faces(L, true));
     CR_CHECK(nssolver(L, ls, L->mK.p, L->mG.p, L->mD.p, L->mL.p, L->Gt.p, L->R.p));
-    k_mul<<<grid_for(4LL * L->nNo, 256), 256, 0, s>>>(L->R.p, L->W.p, 4LL * L->nNo);
+    launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, L->W.p, 4LL * L->nNo);
     CR_CUDA(cudaMemcpyAsync(Ri, L->R.p, sizeof(double) * 4 * (size_t)L->nNo, cudaMemcpyDeviceToHost, s));
     CR_CUDA(cudaMemcpyAsync(Val, L->Val.p, sizeof(double) * 16 * (size_t)L->nnz, cudaMemcpyDeviceToHost, s));
     CR_CUDA(cudaStreamSynchronize(s));
@@ -978,16 +978,16 @@ int memls_solve_lhs_device(crimson_lhs* L, crimson_ls* ls, const double* d_res, 
     CR_CHECK(lhs_work_alloc(L, ls));
     set_face_flags(L, incL, faceRes);
     CR_CUDA(cudaMemcpyAsync(L->R.p, d_res, sizeof(double) * 4 * (size_t)L->nNo, cudaMemcpyDeviceToDevice, s));
-    k_w_from_lhs<<<grid_for(L->nNo, 256), 256, 0, s>>>(d_lhsK, d_lhsP, L->diag, L->W.p, L->nNo);
+    launch(k_w_from_lhs, grid_for(L->nNo, 256), 256, 0, s, d_lhsK, d_lhsP, L->diag, L->W.p, L->nNo);
     CR_CHECK(precond_faces(L, false));
-    k_scale_split_lhs<<<grid_for(L->nNo, 128), 128, 0, s>>>(d_lhsK, d_lhsP, L->rowptr, L->col, L->diag, L->trans,
+    launch(k_scale_split_lhs, grid_for(L->nNo, 128), 128, 0, s, d_lhsK, d_lhsP, L->rowptr, L->col, L->diag, L->trans,
                                                            L->W.p, L->nNo, L->mK.p, L->mG.p, L->mD.p, L->mL.p);
-    k_mul<<<grid_for(4LL * L->nNo, 256), 256, 0, s>>>(L->R.p, L->W.p, 4LL * L->nNo);
+    launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, L->W.p, 4LL * L->nNo);
     CR_CHECK(precond_faces(L, true));
     // With Val4 built from lhsK/lhsP, Gt = -mG^T equals mD up to the order of
     // the two scaling products, so mD serves as Gt.
     CR_CHECK(nssolver(L, ls, L->mK.p, L->mG.p, L->mD.p, L->mL.p, L->mD.p, L->R.p));
-    k_mul<<<grid_for(4LL * L->nNo, 256), 256, 0, s>>>(L->R.p, L->W.p, 4LL * L->nNo);
+    launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, L->W.p, 4LL * L->nNo);
     CR_CUDA(cudaMemcpyAsync(d_sol, L->R.p, sizeof(double) * 4 * (size_t)L->nNo, cudaMemcpyDeviceToDevice, s));
     CR_CUDA(cudaStreamSynchronize(s));
     if (st) {
@@ -998,6 +998,47 @@ int memls_solve_lhs_device(crimson_lhs* L, crimson_ls* ls, const double* d_res, 
         st->Resm = ls->Resm;
         st->Resc = ls->Resc;
     }
+    return CRIMSON_OK;
+}
+
+}  // namespace crimson
+
+namespace crimson {
+
+// Average device time of one launch of a memLS kernel on the lhs's current
+// split matrices (events recorded on the lhs stream around reps launches).
+int memls_kernel_time(crimson_lhs* L, int which, int reps, double* ms) {
+    if (!L->mK.p || !L->basis.p || reps <= 0) return CRIMSON_ERR_STATE;
+    cudaStream_t s = L->stream;
+    Ctx C{L, s};
+    const long long n3 = 3LL * L->nNo;
+    cudaEvent_t e0, e1;
+    CR_CUDA(cudaEventCreate(&e0));
+    CR_CUDA(cudaEventCreate(&e1));
+    auto run = [&]() {
+        switch (which) {
+            case 0: C.spmv_vv3(L->mK.p, L->basis.p, L->basis.p + n3); break;
+            case 1:
+                launch(k_cg_op, red_grid((long long)L->nNo * kLanes), 256, 0, s, L->rowptr, L->col, L->mL.p, L->mD.p,
+                       L->cgP.p, L->cgGP.p, L->cgSP.p, L->nNo, L->red.part.p, L->red.ticket.p, C.sc(kSlotDen));
+                break;
+            case 2: C.spmv_sv3(L->mG.p, L->cgP.p, L->cgGP.p); break;
+            default:
+                launch(k_mgs, red_grid(n3), 256, 0, s, L->basis.p + 2 * n3, L->basis.p, C.sc(kSlotH),
+                       L->basis.p + n3, n3, L->red.part.p, L->red.ticket.p, C.sc(kSlotH + 1));
+        }
+    };
+    for (int i = 0; i < 2; ++i) run();
+    CR_CUDA(cudaEventRecord(e0, s));
+    for (int i = 0; i < reps; ++i) run();
+    CR_CUDA(cudaEventRecord(e1, s));
+    CR_CUDA(cudaEventSynchronize(e1));
+    float t = 0.f;
+    CR_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    *ms = (double)t / reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CR_CUDA(cudaGetLastError());
     return CRIMSON_OK;
 }
 

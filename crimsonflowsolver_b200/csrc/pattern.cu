@@ -108,7 +108,7 @@ int build_pattern(crimson_ctx* c) {
     CR_CHECK(ukeys.alloc(npair));
     CR_CHECK(dcount.alloc(1));
     CR_CHECK(bad.alloc(1));
-    k_pair_keys<<<grid_for(npair, 256), 256, 0, s>>>(c->ien.p, c->nelem, (unsigned long long)c->nshg, keys.p);
+    launch(k_pair_keys, grid_for(npair, 256), 256, 0, s, c->ien.p, c->nelem, (unsigned long long)c->nshg, keys.p);
     CR_CUDA(cudaGetLastError());
     unsigned long long maxkey = (unsigned long long)c->nshg * (unsigned long long)c->nshg;
     int end_bit = 1;
@@ -131,11 +131,11 @@ int build_pattern(crimson_ctx* c) {
     CR_CHECK(c->trans.alloc((size_t)hnnz));
     CR_CHECK(c->epos.alloc((size_t)npair));
     CR_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
-    k_rowptr_cols<<<grid_for((long long)hnnz + c->nshg + 1, 256), 256, 0, s>>>(ukeys.p, hnnz, c->nshg, c->rowptr.p,
+    launch(k_rowptr_cols, grid_for((long long)hnnz + c->nshg + 1, 256), 256, 0, s, ukeys.p, hnnz, c->nshg, c->rowptr.p,
                                                                               c->col.p);
-    k_diag_trans<<<grid_for(c->nshg, 128), 128, 0, s>>>(c->rowptr.p, c->col.p, c->nshg, c->diag.p, c->trans.p,
+    launch(k_diag_trans, grid_for(c->nshg, 128), 128, 0, s, c->rowptr.p, c->col.p, c->nshg, c->diag.p, c->trans.p,
                                                         bad.p);
-    k_epos<<<grid_for(npair, 256), 256, 0, s>>>(c->ien.p, c->nelem, c->rowptr.p, c->col.p, c->epos.p, bad.p);
+    launch(k_epos, grid_for(npair, 256), 256, 0, s, c->ien.p, c->nelem, c->rowptr.p, c->col.p, c->epos.p, bad.p);
     CR_CUDA(cudaGetLastError());
     int hbad = 0;
     CR_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -153,13 +153,13 @@ int pattern_to_host(crimson_ctx* c, int* colm, int* rowp, long long cap) {
     DBuf<int> tmp;
     if (colm) {
         CR_CHECK(tmp.alloc((size_t)c->nshg + 1));
-        k_to_one_based<<<grid_for(c->nshg + 1, 256), 256, 0, s>>>(c->rowptr.p, tmp.p, c->nshg + 1);
+        launch(k_to_one_based, grid_for(c->nshg + 1, 256), 256, 0, s, c->rowptr.p, tmp.p, c->nshg + 1);
         CR_CUDA(cudaMemcpyAsync(colm, tmp.p, sizeof(int) * ((size_t)c->nshg + 1), cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
     }
     if (rowp) {
         CR_CHECK(tmp.alloc((size_t)c->nnz));
-        k_to_one_based<<<grid_for(c->nnz, 256), 256, 0, s>>>(c->col.p, tmp.p, c->nnz);
+        launch(k_to_one_based, grid_for(c->nnz, 256), 256, 0, s, c->col.p, tmp.p, c->nnz);
         CR_CUDA(cudaMemcpyAsync(rowp, tmp.p, sizeof(int) * (size_t)c->nnz, cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
     }

@@ -196,6 +196,16 @@ int crimson_step(crimson_ctx* ctx, crimson_lhs* lhs, crimson_ls* ls, const crims
 /* The CUDA stream (cudaStream_t) every call on this context launches on. */
 void* crimson_ctx_stream(crimson_ctx* ctx);
 
+/* Diagnostics: average device time (ms) of one launch of a memLS kernel on the
+ * lhs's current split matrices, timed with CUDA events on the lhs stream.
+ * which: 0 = 3x3 block SpMV (SPARMULVV, K), 1 = fused CG operator
+ * (SPARMULSS L + SPARMULVS Gt + DOTS), 2 = SPARMULSV (G), 3 = fused MGS step.
+ * Valid after a solve on the lhs. */
+int crimson_memls_kernel_time(crimson_lhs* lhs, int which, int reps, double* ms);
+
+/* Number of CUDA kernels this library has launched since it was loaded. */
+unsigned long long crimson_launch_count(void);
+
 /* Library version and build target, for diagnostics. */
 const char* crimson_version(void);
 /* Last CUDA error string seen by this library (diagnostics). */

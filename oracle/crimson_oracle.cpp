@@ -16,6 +16,7 @@
 #include "crimson_oracle.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -591,6 +592,11 @@ inline long long sparseloc(const int* list, int n, int target) {
 
 int nthreads_of(const orc_params* p) { return p->nthreads > 0 ? p->nthreads : 1; }
 
+// CPUT (memLS.f90:2382-2400): wall-clock seconds
+double CPUT() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1116,6 +1122,7 @@ void GMRES(int dof, Lhs& L, orc_subls& ls, const double* Val, const double* R, d
     auto H = [&](int i, int j) -> double& { return h[(size_t)j * (sD + 1) + i]; };
     auto U = [&](int k) { return &u[n * k]; };
     double eps = 0.0, tmp;
+    const double time = CPUT();
     ls.suc = 0;
     bool coupled = any_coupled(L);
     std::fill(X, X + n, 0.0);
@@ -1196,6 +1203,7 @@ void GMRES(int dof, Lhs& L, orc_subls& ls, const double* Val, const double* R, d
         ls.fNorm = std::fabs(err[i]);
         if (ls.suc) break;
     }
+    ls.callD = CPUT() - time + ls.callD;
     ls.dB = 10.0 * std::log(ls.fNorm / ls.dB);
 }
 
@@ -1204,6 +1212,7 @@ void CGRAD(int dof, Lhs& L, orc_subls& ls, const double* D, const double* G, con
     const int nNo = L.nNo;
     std::vector<double> X(nNo, 0.0), P(nNo), SP(nNo), DGP(nNo), GP((size_t)dof * nNo), unCondU((size_t)dof * nNo);
     bool coupled = any_coupled(L);
+    const double time = CPUT();
     ls.suc = 0;
     double errO = NORMS(nNo, R);
     ls.iNorm = errO;
@@ -1236,6 +1245,7 @@ void CGRAD(int dof, Lhs& L, orc_subls& ls, const double* D, const double* G, con
     }
     std::memcpy(R, X.data(), nNo * sizeof(double));
     ls.fNorm = std::sqrt(err);
+    ls.callD = CPUT() - time + ls.callD;
     ls.dB = 5.0 * std::log(err / errO);
     ls.itr = ls.itr + i - 1;
 }
@@ -1325,6 +1335,7 @@ int NSSOLVER(int dof, Lhs& L, Ls& ls, const double* Val, double* Ri) {
     ls.GM.callD = 0.0;
     ls.CG.itr = 0;
     ls.GM.itr = 0;
+    ls.RI.callD = CPUT();
     ls.RI.suc = 0;
     eps = std::max(ls.RI.absTol, ls.RI.relTol * eps);
     // DEPART (memLS.f90:1612-1679)
@@ -1425,6 +1436,7 @@ int NSSOLVER(int dof, Lhs& L, Ls& ls, const double* Val, double* Ri) {
         for (size_t t = 0; t < nv; ++t) Rmi[t] = Rmi[t] + xB[iBB - 1] * Ucol(i - 1)[t];
         for (int t = 0; t < nNo; ++t) Rci[t] = Rci[t] + xB[iB - 1] * Pcol(i - 1)[t];
     }
+    ls.RI.callD = CPUT() - ls.RI.callD;
     ls.RI.dB = 10.0 * std::log(ls.RI.fNorm / ls.RI.dB);
     for (int a = 0; a < nNo; ++a) {
         for (int d = 0; d < nsd; ++d) Ri[(size_t)dof * a + d] = Rmi[(size_t)nsd * a + d];
