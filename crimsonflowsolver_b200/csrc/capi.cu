@@ -454,7 +454,9 @@ int crimson_memls_lhs_create_from_ctx(crimson_lhs** out, crimson_ctx* c, int nFa
 
 int crimson_memls_lhs_free(crimson_lhs* L) {
     if (!L) return CRIMSON_ERR_ARG;
-    if (L->stream) cudaStreamSynchronize(L->stream);
+    // An lhs made from a context borrows that context's stream and must be
+    // freed before the context; it never touches the borrowed stream here.
+    if (L->own_stream && L->stream) cudaStreamSynchronize(L->stream);
     if (L->hscal) cudaFreeHost(L->hscal);
     cudaStream_t s = L->own_stream ? L->stream : nullptr;
     delete L;

@@ -128,6 +128,12 @@ class ElmGMR:
             N.lib().crimson_ctx_destroy(self.h)
             self.h = None
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
     def __del__(self):
         try:
             self.close()
@@ -148,6 +154,7 @@ class MemLS:
                                           P.kspace, N.dp(rin), N.dp(ain), N.ip(mit)), "crimson_memls_ls_create")
         self.ls = ls
         lhs = ctypes.c_void_p()
+        self._ctx = ctx   # an lhs made from a context must be freed before it
         if ctx is not None:
             N.check(L.crimson_memls_lhs_create_from_ctx(ctypes.byref(lhs), ctx.h, nfaces),
                     "crimson_memls_lhs_create_from_ctx")
@@ -196,6 +203,7 @@ class MemLS:
         if getattr(self, "ls", None):
             L.crimson_memls_ls_free(self.ls)
             self.ls = None
+        self._ctx = None
 
     def __del__(self):
         try:
@@ -263,6 +271,21 @@ class FlowSolver:
         ac = np.zeros((self.mesh.nshg, 4), order="F")
         N.check(N.lib().crimson_state_get(self.elm.h, N.dp(y), N.dp(ac)), "crimson_state_get")
         return np.ascontiguousarray(y), np.ascontiguousarray(ac)
+
+    def close(self) -> None:
+        """Free the memLS handles, then the context they borrow from."""
+        if getattr(self, "memls", None) is not None:
+            self.memls.close()
+            self.memls = None
+        if getattr(self, "elm", None) is not None:
+            self.elm.close()
+            self.elm = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def step(self) -> N.StepStats:
         t1 = self.P.Delt * (self.istep + 1)
