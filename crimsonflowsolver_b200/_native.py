@@ -88,6 +88,8 @@ SIGNATURES = {
     "crimson_step": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.POINTER(StepArgs),
                                     ctypes.POINTER(StepStats)]),
     "crimson_ctx_stream": (c_void_p, [c_void_p]),
+    "crimson_pvsq_noalloc": (ctypes.c_int, [ctypes.c_int, c_int_p, c_void_p, c_void_p, c_void_p, c_dbl_p, c_dbl_p,
+                                            c_void_p, c_dbl_p, c_void_p]),
     "crimson_launch_count": (ctypes.c_ulonglong, []),
     "crimson_memls_kernel_time": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, c_dbl_p]),
     "crimson_version": (ctypes.c_char_p, []),

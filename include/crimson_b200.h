@@ -143,7 +143,8 @@ int crimson_memls_ls_free(crimson_ls* ls);
  * -- flowsolver/src/memLS.f90:1080 (single task; rowPtr = colm, colPtr = rowp) */
 int crimson_memls_lhs_create(crimson_lhs** lhs, int gnNo, int nNo, long long nnz, const int* gNodes,
                              const int* rowPtr, const int* colPtr, int nFaces);
-/* Same, sharing the pattern already built on the device by crimson_genadj. */
+/* Same, sharing the pattern already built on the device by crimson_genadj and
+ * the context's stream; free such an lhs before its context. */
 int crimson_memls_lhs_create_from_ctx(crimson_lhs** lhs, crimson_ctx* ctx, int nFaces);
 int crimson_memls_lhs_free(crimson_lhs* lhs);
 /* memLS_BC_CREATE(lhs, faIn, nNo, dof, BC_type, gNodes, Val) -- memLS.f90:272 */
@@ -195,6 +196,29 @@ int crimson_step(crimson_ctx* ctx, crimson_lhs* lhs, crimson_ls* ls, const crims
 
 /* The CUDA stream (cudaStream_t) every call on this context launches on. */
 void* crimson_ctx_stream(crimson_ctx* ctx);
+
+/* ---------------------------------------------------------------------------
+ * Outlet coupling without device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc (a stream
+ * being captured into a CUDA graph, a host framework that owns all device
+ * memory through its own pool, a latency-bound coupling loop where an
+ * allocation would synchronise the device).
+ * Computes the flows Q_k = sum NABI . u over each coupled surface and adds
+ * p_k NABI to the momentum rows of res with p_k = -(Q_k coef1_k) - coef2_k,
+ * as ElmGMR's outlet coupling does.  Device inputs: d_nodes (1-based node
+ * numbers of the surfaces, grouped by surface), d_nabi (3, n) NABI of those
+ * nodes, d_y (4, nshg) node-major; d_res (4, nshg) updated in place.  Host
+ * inputs: surf_offsets (nsurf+1) into d_nodes, coef1/coef2 (nsurf).  q_out
+ * (host, nsurf) receives the flows when not NULL (the call then waits for
+ * the stream).  stream is a cudaStream_t (NULL = default stream).
+ * At most 64 surfaces: the flows live in a 512-byte static device array
+ * shared by every call (overlapping calls on the GPU race on it); the first
+ * call on a device looks up that array's address, so make it before any
+ * stream capture.  Returns CRIMSON_ERR_UNSUPPORTED for nsurf > 64.
+ * ------------------------------------------------------------------------- */
+int crimson_pvsq_noalloc(int nsurf, const int* surf_offsets, const int* d_nodes, const double* d_nabi,
+                         const double* d_y, const double* coef1, const double* coef2, double* d_res, double* q_out,
+                         void* stream);
 
 /* Diagnostics: average device time (ms) of one launch of a memLS kernel on the
  * lhs's current split matrices, timed with CUDA events on the lhs stream.
