@@ -5,7 +5,13 @@ cylinder (R = 1 cm, L = 10 cm, 80x80 cross-section masked to the disc, 133
 layers, 6 tets per hex), pulsatile parabolic inflow 10 + 5 sin(2 pi t / 0.8)
 cm/s, one RCR outlet (Rp = 100, C = 1e-4, Rd = 1000), rho = 1.06, mu = 0.04,
 dt = 1e-3 s, 3 nonlinear iterations (ElmGMR + memLS NS solve + correct) per
-step, FP64 throughout.  Inputs are synthetic and seeded.
+step.  Inputs are synthetic and seeded.
+
+Both arithmetic modes run on the same workload from the same initial state:
+plain FP64 (memLS's arithmetic, the ``fp64`` object) and the mixed-precision
+NS solve (FP32 matrices in the inner Krylov matvecs, FP64 refinement), which
+is the headline ``value``; ``mixed_rel_err_vs_fp64`` compares their velocity
+and pressure fields after the same number of steps.
 
 Multi-GPU: the path does not shard (one GPU, no domain decomposition), so
 ``--gpus N`` under torchrun runs N independent replicas; time is the max over
@@ -175,25 +181,12 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args):
+def _timed_steps(F, args, stream, local, dist):
+    """W untimed steps, then K steps timed with CUDA events on the library stream."""
     import torch
 
     from crimsonflowsolver_b200 import _native as N
-    from crimsonflowsolver_b200 import solver
 
-    ws, rank = _dist()
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if ws > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    m, P = make_problem(args.ncross, args.naxial)
-    F = solver.FlowSolver(m, P, inflow=_inflow)
-    stream = torch.cuda.ExternalStream(F.elm.stream_handle)
     L = N.lib()
     iters = []
     for _ in range(args.warmup):
@@ -209,7 +202,8 @@ def run_ours(args):
         e0.record(stream)
         for _ in range(args.steps):
             st = F.step()
-            iters.append([(st.ri_itr[i], st.gm_itr[i], st.cg_itr[i]) for i in range(st.nsolves)])
+            iters.append([(st.ri_itr[i], st.gm_itr[i], st.cg_itr[i], st.refine_steps[i], st.refine_rel[i])
+                          for i in range(st.nsolves)])
         e1.record(stream)
         torch.cuda.synchronize()
     launches = L.crimson_launch_count() - l0
@@ -219,109 +213,160 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_ms = float(t.item())
         dist.barrier()
-    t_s = t_ms / 1e3
-    value = t_s / (args.steps * ws)
-    # ---- end to end through the host-buffer API: state in from pinned host, step, state out ----
-    n = m.nshg
-    y_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
-    ac_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
-    y0, a0 = F.state()
-    y_h.copy_(torch.from_numpy(np.ascontiguousarray(y0.T)))
-    ac_h.copy_(torch.from_numpy(np.ascontiguousarray(a0.T)))
+    it = np.array([s for step in iters for s in step], dtype=float)
+    per_solve = {"ri": float(it[:, 0].mean()), "gm": float(it[:, 1].mean()), "cg": float(it[:, 2].mean())}
+    if it[:, 3].max() > 0:
+        per_solve["refine_sweeps"] = float(it[:, 3].mean())
+        per_solve["max_final_defect"] = float(it[:, 4].max())
+    return t_ms, per_solve, int(launches), clk.summary()
+
+
+def _relerr(a, b):
+    den = float(np.abs(b).max())
+    return float(np.abs(a - b).max() / (den if den > 0 else 1.0))
+
+
+def cg_iter_bytes(nnz: int, n: int, mbytes: int, nface: int) -> int:
+    """Algorithmic HBM bytes of one iteration of the persistent CGRAD kernel.
+
+    Per block: column index (4) + G (3 values) + {Gt, L} (4 values), values of
+    mbytes each.  Per row, once: row pointers (2 x 4), records {R, P_prev}
+    read (16), {GP, P} written (32) and read (32), SP written (8), X read and
+    written (16), {R, P} read and written (32), SP and P read in the update
+    (16), and 2 x 8 per coupled face (w_f, z_f).
+    """
+    return nnz * (8 + 7 * mbytes) + n * (8 + 16 + 32 + 32 + 8 + 16 + 32 + 16 + 16 * nface)
+
+
+def run_ours(args):
     import ctypes
 
+    import torch
+
+    from crimsonflowsolver_b200 import FlowParams
+    from crimsonflowsolver_b200 import _native as N
+    from crimsonflowsolver_b200 import solver
+
+    ws, rank = _dist()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    L = N.lib()
+    m, P = make_problem(args.ncross, args.naxial)
+    n = m.nshg
+    # ---- FP64 (memLS arithmetic) ----
+    F64 = solver.FlowSolver(m, P, inflow=_inflow)
+    s64 = torch.cuda.ExternalStream(F64.elm.stream_handle)
+    t64_ms, it64, l64, clk64 = _timed_steps(F64, args, s64, local, dist)
+    # ---- mixed: FP32 inner matvecs, FP64 refinement ----
+    Pm = FlowParams(**{**P.__dict__, "precision": "mixed"})
+    FM = solver.FlowSolver(m, Pm, inflow=_inflow)
+    sm = torch.cuda.ExternalStream(FM.elm.stream_handle)
+    tm_ms, itm, lm, clkm = _timed_steps(FM, args, sm, local, dist)
+    y64, _ = F64.state()
+    ym, _ = FM.state()
+    acc = {"velocity": _relerr(ym[:, 0:3], y64[:, 0:3]), "pressure": _relerr(ym[:, 3], y64[:, 3]),
+           "after_steps": args.warmup + args.steps}
+    value = tm_ms / 1e3 / (args.steps * ws)
+    v64 = t64_ms / 1e3 / (args.steps * ws)
+    # ---- end to end through the host-buffer API (mixed): state in from pinned host, step, state out ----
+    y_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
+    ac_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
+    y0, a0 = FM.state()
+    y_h.copy_(torch.from_numpy(np.ascontiguousarray(y0.T)))
+    ac_h.copy_(torch.from_numpy(np.ascontiguousarray(a0.T)))
     yp = ctypes.cast(y_h.data_ptr(), N.c_dbl_p)
     ap = ctypes.cast(ac_h.data_ptr(), N.c_dbl_p)
     e_steps = max(1, min(args.steps, 3))
     torch.cuda.synchronize()
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
+    f0.record(sm)
     for _ in range(e_steps):
-        N.check(L.crimson_state_set(F.elm.h, yp, ap), "crimson_state_set")
-        F.step()
-        N.check(L.crimson_state_get(F.elm.h, yp, ap), "crimson_state_get")
-    f1.record(stream)
+        N.check(L.crimson_state_set(FM.elm.h, yp, ap), "crimson_state_set")
+        FM.step()
+        N.check(L.crimson_state_get(FM.elm.h, yp, ap), "crimson_state_get")
+    f1.record(sm)
     torch.cuda.synchronize()
     e2e = f0.elapsed_time(f1) / 1e3 / e_steps
-    # ---- assembly throughput and the dominant solver kernel, timed live on the library stream ----
+    # ---- assembly throughput, timed live on the library stream ----
     dres = torch.zeros((n, 4), dtype=torch.float64, device="cuda")
-    nnz = F.elm._nnz()
+    nnz = FM.elm._nnz()
     dK = torch.empty((nnz, 9), dtype=torch.float64, device="cuda")
     dP = torch.empty((nnz, 4), dtype=torch.float64, device="cuda")
-    dy = torch.tensor(F.state()[0], device="cuda")
-    dac = torch.tensor(F.state()[1], device="cuda")
+    dy = torch.tensor(FM.state()[0], device="cuda")
+    dac = torch.tensor(FM.state()[1], device="cuda")
     torch.cuda.synchronize()
     for _ in range(2):
-        F.elm.device(dy, dac, dres, dK, dP, [100.0], [0.0])
+        FM.elm.device(dy, dac, dres, dK, dP, [100.0], [0.0])
     a0e = torch.cuda.Event(enable_timing=True)
     a1e = torch.cuda.Event(enable_timing=True)
-    a0e.record(stream)
+    a0e.record(sm)
     reps = 5
     for _ in range(reps):
-        F.elm.device(dy, dac, dres, dK, dP, [100.0], [0.0])
-    a1e.record(stream)
+        FM.elm.device(dy, dac, dres, dK, dP, [100.0], [0.0])
+    a1e.record(sm)
     torch.cuda.synchronize()
     t_asm = a0e.elapsed_time(a1e) / reps / 1e3
+    # ---- kernel times: the persistent CG (events around every launch of the timed run) and the SpMVs ----
     kt = {}
-    for which, name in ((0, "spmv_K"), (1, "cg_op"), (2, "spmv_G"), (3, "mgs")):
-        ms = ctypes_double()
-        N.check(L.crimson_memls_kernel_time(F.memls.lhs, which, 20, ctypes_ref(ms)), "kernel_time")
-        kt[name] = ms.value
+    for lhs, which, name in ((FM.memls.lhs, 4, "cg_iter_f32"), (F64.memls.lhs, 1, "cg_iter_f64"),
+                             (FM.memls.lhs, 5, "spmv_K_f32"), (F64.memls.lhs, 0, "spmv_K_f64"),
+                             (F64.memls.lhs, 2, "spmv_G_f64"), (F64.memls.lhs, 3, "mgs_f64")):
+        ms = ctypes.c_double()
+        rc = L.crimson_memls_kernel_time(lhs, which, 20, ctypes.byref(ms))
+        kt[name] = ms.value if rc == 0 else None
     peaks = _peaks()
-    # algorithmic bytes per launch (per block / per row)
-    nrow = n
-    cg_bytes = nnz * (8 + 24 + 4) + nrow * (4 + 8 + 24 + 8)
-    achieved = cg_bytes / (kt["cg_op"] / 1e3) / 1e9
-    it = np.array([s for step in iters for s in step], dtype=float)
+    nface = len(P.rcr)
+    cg_bytes = cg_iter_bytes(nnz, n, 4, nface)
+    achieved = cg_bytes / (kt["cg_iter_f32"] / 1e3) / 1e9 if kt["cg_iter_f32"] else None
     line = {
         "metric": METRIC, "value": value, "unit": "s/timestep", "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "warmup": args.warmup, "ms_per_step": tm_ms / args.steps, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 matrices in inner Krylov matvecs, f64 vectors/reductions/refinement",
+        "data": "synthetic",
         "config": {"workload": f"4.0M-tet cylinder ({m.nelem} tets, {n} nodes, {nnz} blocks), pulsatile inflow, "
-                               "RCR outlet, dt=1e-3, 3 nonlinear iterations/step, plain FP64",
+                               "RCR outlet, dt=1e-3, 3 nonlinear iterations/step, mixed-precision NS solve",
                    "parallelism": "replicas" if ws > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (matrices 1.3 GB per solve)"},
+                   "l2": "inputs larger than L2 (FP32 matrices 0.45 GB, FP64 1.3 GB per solve)"},
+        "fp64": {"value": v64, "unit": "s/timestep", "ms_per_step": t64_ms / args.steps,
+                 "solver_iters_per_solve": it64, "gpu_launches": l64, "clocks": clk64},
+        "mixed_speedup_vs_fp64": v64 / value,
+        "mixed_rel_err_vs_fp64": acc,
+        "solver_iters_per_solve": itm,
         "assembly_melem_s": m.nelem / t_asm / 1e6,
         "assembly_ms": t_asm * 1e3,
-        "solver_iters_per_solve": {"ri": float(it[:, 0].mean()), "gm": float(it[:, 1].mean()),
-                                   "cg": float(it[:, 2].mean())} if len(it) else None,
         "kernel_ms": kt,
-        "roofline": {"kernel": "k_cg_op (SPARMULSS L + SPARMULVS Gt + DOTS)", "bound": "hbm",
-                     "achieved": achieved, "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
-                     "traffic": None, "peak_source": peaks[1]},
+        "roofline": {"kernel": "k_cg_persistent<float> (one CGRAD iteration: G P, L P - Gt G P, updates)",
+                     "bound": "hbm", "achieved": achieved, "peak": peaks[0], "unit": "GB/s",
+                     "frac": achieved / peaks[0] if achieved else None, "traffic": None,
+                     "algorithmic_bytes_per_iter": cg_bytes, "peak_source": peaks[1]},
         "e2e": {"value": e2e, "unit": "s/timestep", "h2d_bytes_per_step": 2 * 4 * n * 8,
                 "d2h_bytes_per_step": 2 * 4 * n * 8},
-        "gpu_launches": int(launches),
-        "clocks": clk.summary(),
+        "gpu_launches": lm,
+        "clocks": clkm,
     }
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
-            cpu_v, sample, _ = cpu_sample(m, P, os.cpu_count() or 1,
-                                          {"ri": float(it[:, 0].mean()), "gm": float(it[:, 1].mean()),
-                                           "cg": float(it[:, 2].mean())})
+            cpu_v, sample, _ = cpu_sample(m, P, os.cpu_count() or 1, it64)
             line["cpu_baseline"] = {"value": cpu_v, "unit": "s/timestep", "cores": os.cpu_count(), "kind": "port",
                                     "sample": sample}
         except Exception as ex:  # the CPU baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "unit": "s/timestep", "cores": os.cpu_count(), "kind": "port",
                                     "sample": f"failed: {ex}"}
+    FM.close()
+    F64.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-
-
-def ctypes_double():
-    import ctypes
-
-    return ctypes.c_double()
-
-
-def ctypes_ref(x):
-    import ctypes
-
-    return ctypes.byref(x)
 
 
 def _peaks():

@@ -49,7 +49,8 @@ class StepArgs(ctypes.Structure):
 class StepStats(ctypes.Structure):
     _fields_ = [("nsolves", ctypes.c_int), ("ri_itr", ctypes.c_int * 16), ("gm_itr", ctypes.c_int * 16),
                 ("cg_itr", ctypes.c_int * 16), ("ri_inorm", ctypes.c_double * 16),
-                ("ri_fnorm", ctypes.c_double * 16), ("q_out", ctypes.c_double * 8), ("p_out", ctypes.c_double * 8)]
+                ("ri_fnorm", ctypes.c_double * 16), ("q_out", ctypes.c_double * 8), ("p_out", ctypes.c_double * 8),
+                ("refine_steps", ctypes.c_int * 16), ("refine_rel", ctypes.c_double * 16)]
 
 
 # name -> (restype, argtypes)
@@ -71,6 +72,8 @@ SIGNATURES = {
                                                ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                                c_dbl_p, c_dbl_p, c_int_p]),
     "crimson_memls_ls_free": (ctypes.c_int, [c_void_p]),
+    "crimson_memls_ls_set_precision": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
+    "crimson_memls_refine_info": (ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_int), c_dbl_p]),
     "crimson_memls_lhs_create": (ctypes.c_int, [ctypes.POINTER(c_void_p), ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_longlong, c_int_p, c_int_p, c_int_p, ctypes.c_int]),
     "crimson_memls_lhs_create_from_ctx": (ctypes.c_int, [ctypes.POINTER(c_void_p), c_void_p, ctypes.c_int]),

@@ -391,6 +391,23 @@ int crimson_memls_ls_free(crimson_ls* ls) {
     return CRIMSON_OK;
 }
 
+int crimson_memls_ls_set_precision(crimson_ls* ls, int precision, int max_refine, double refine_tol) {
+    if (!ls || (precision != CRIMSON_FP64 && precision != CRIMSON_MIXED) || max_refine < 1 || max_refine > 64 ||
+        !(refine_tol < 1.0))
+        return CRIMSON_ERR_ARG;
+    ls->precision = precision;
+    ls->max_refine = max_refine;
+    ls->refine_tol = refine_tol;
+    return CRIMSON_OK;
+}
+
+int crimson_memls_refine_info(const crimson_lhs* L, int* steps, double* rel) {
+    if (!L) return CRIMSON_ERR_ARG;
+    if (steps) *steps = L->refine_steps;
+    if (rel) *rel = L->refine_rel;
+    return CRIMSON_OK;
+}
+
 __global__ void k_one_to_zero(const int* __restrict__ in, int* __restrict__ out, long long n) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
         out[t] = in[t] - 1;
@@ -458,6 +475,8 @@ int crimson_memls_lhs_free(crimson_lhs* L) {
     // freed before the context; it never touches the borrowed stream here.
     if (L->own_stream && L->stream) cudaStreamSynchronize(L->stream);
     if (L->hscal) cudaFreeHost(L->hscal);
+    if (L->ev0) cudaEventDestroy(L->ev0);
+    if (L->ev1) cudaEventDestroy(L->ev1);
     cudaStream_t s = L->own_stream ? L->stream : nullptr;
     delete L;
     if (s) cudaStreamDestroy(s);
@@ -611,6 +630,8 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
             st->cg_itr[it] = lst.CG.itr;
             st->ri_inorm[it] = lst.RI.iNorm;
             st->ri_fnorm[it] = lst.RI.fNorm;
+            st->refine_steps[it] = ls->precision == CRIMSON_FP64 ? 0 : L->refine_steps;
+            st->refine_rel[it] = ls->precision == CRIMSON_FP64 ? 0.0 : L->refine_rel;
             st->nsolves = it + 1;
         }
     }

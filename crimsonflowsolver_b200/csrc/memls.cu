@@ -4,17 +4,27 @@
 // matrices split as DEPART does (memLS.f90:1612-1679) into mK (9, nnz),
 // mG (3, nnz), mD (3, nnz), mL (nnz) and Gt (3, nnz).
 //
-// Kernels are HBM-bound: block SpMVs use 8 lanes per block row with lanes
-// striding the row's blocks, so each warp streams 4 rows' blocks contiguously;
-// dot products and norms use a single-pass grid reduction whose last block
-// sums the per-block partials in a fixed order (deterministic).  The Krylov
-// control flow (Givens rotations, back substitution, the 2i x 2i Gram system
-// solved by GE) runs on the host in FP64 on scalars copied back per step, as
-// the reference's serial code does.
+// Two precisions share one implementation, templated on the matrix storage
+// type M and the GMRES basis type B:
+//   * FP64 (M = B = double): the plain path, same arithmetic as memLS.
+//   * mixed (M = B = float): every inner Krylov matvec reads FP32 matrices
+//     and the GMRES basis is FP32; FP64 is kept for the NSSOLVER outer
+//     vectors and Gram system, every dot product / norm (FP64 accumulation),
+//     the Givens rotations and back substitution, the CG recurrences, and a
+//     final FP64 defect R - A x with iterative refinement.
+//
+// Kernels are HBM-bound: block SpMVs use four lanes per block row with four
+// blocks per lane issued together; dot products and norms use a single-pass
+// grid reduction whose last block sums the per-block partials in a fixed
+// order (deterministic).  CGRAD runs as one persistent cooperative kernel per
+// call.  The Krylov control flow (Givens rotations, back substitution, the
+// 2i x 2i Gram system solved by GE) runs on the host in FP64 on scalars
+// copied back per step, as the reference's serial code does.
 //
 // Modified Gram-Schmidt is fused: kernel j subtracts h(j-1) u_{j-1} from w and
-// accumulates <w, u_j> in the same pass, so orthogonalising against i basis
-// vectors streams w i+1 times instead of 2i times.
+// accumulates <w, u_j> in the same pass.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -26,11 +36,44 @@
 namespace crimson {
 
 // ---------------------------------------------------------------------------
+// Small helpers
+// ---------------------------------------------------------------------------
+template <typename T>
+struct V4;
+template <>
+struct V4<double> {
+    using type = double4;
+};
+template <>
+struct V4<float> {
+    using type = float4;
+};
+
+__device__ __forceinline__ double4 ldg4(const double4* p) {
+    const double2 lo = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 hi = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+__device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ double4 ldcg4(const double4* p) {
+    const double2 lo = __ldcg(reinterpret_cast<const double2*>(p));
+    const double2 hi = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+template <typename T>
+__device__ __forceinline__ typename V4<T>::type mk4(T a, T b, T c, T d);
+template <>
+__device__ __forceinline__ double4 mk4<double>(double a, double b, double c, double d) {
+    return make_double4(a, b, c, d);
+}
+template <>
+__device__ __forceinline__ float4 mk4<float>(float a, float b, float c, float d) {
+    return make_float4(a, b, c, d);
+}
+
+// ---------------------------------------------------------------------------
 // Reductions: partial sums per block -> last block sums them in block order.
 // ---------------------------------------------------------------------------
-
-
-// Finish a grid reduction: every block calls this with its block-summed value.
 __device__ __forceinline__ void grid_reduce_finish(double bsum, double* part, unsigned int* ticket, double* out,
                                                    double* smem) {
     __shared__ bool am_last;
@@ -58,242 +101,450 @@ static int red_grid(long long n) {
     return g > RedScratch::kMaxBlocks ? RedScratch::kMaxBlocks : g;
 }
 
-// out = <u, v>
-__global__ void k_dot(const double* __restrict__ u, const double* __restrict__ v, long long n, double* part,
+// out = <u, v> (FP64 accumulation)
+template <typename U, typename V>
+__global__ void k_dot(const U* __restrict__ u, const V* __restrict__ v, long long n, double* part,
                       unsigned int* ticket, double* out) {
     __shared__ double sm[32];
     double s = 0.0;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-        s += u[t] * v[t];
+        s += (double)u[t] * (double)v[t];
     s = block_sum(s, sm);
     grid_reduce_finish(s, part, ticket, out, sm);
 }
 
 // MGS step: w -= (*hprev) * uprev (if uprev), then out = <w, uj>  (uj may be w -> squared norm)
-__global__ void k_mgs(double* w, const double* __restrict__ uprev, const double* __restrict__ hprev,
-                      const double* uj, long long n, double* part, unsigned int* ticket, double* out) {
+template <typename B>
+__global__ void k_mgs(B* w, const B* __restrict__ uprev, const double* __restrict__ hprev, const B* uj, long long n,
+                      double* part, unsigned int* ticket, double* out) {
     __shared__ double sm[32];
     const double h = uprev ? *hprev : 0.0;
     double s = 0.0;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
-        double wv = w[t];
+        double wv = (double)w[t];
         if (uprev) {
-            wv = wv - h * uprev[t];
-            w[t] = wv;
+            wv = (double)(B)(wv - h * (double)uprev[t]);
+            w[t] = (B)wv;
         }
-        s += wv * (uj == w ? wv : uj[t]);
+        s += wv * (uj == w ? wv : (double)uj[t]);
     }
     s = block_sum(s, sm);
     grid_reduce_finish(s, part, ticket, out, sm);
 }
 
-// y = a*x + y with a from host
-__global__ void k_axpy(double a, const double* __restrict__ x, double* __restrict__ y, long long n) {
+// y = y + a*x
+template <typename X, typename Y>
+__global__ void k_axpy(double a, const X* __restrict__ x, Y* __restrict__ y, long long n) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-        y[t] = y[t] + a * x[t];
+        y[t] = (Y)((double)y[t] + a * (double)x[t]);
 }
 
-// y = x / d (d on device, the reference divides)
-__global__ void k_divide(const double* x, const double* __restrict__ dptr, double* y,
-                         long long n, int take_sqrt) {
+// y = x / d (d on device; the reference divides)
+template <typename B>
+__global__ void k_divide(const B* x, const double* __restrict__ dptr, B* y, long long n, int take_sqrt) {
     double d = *dptr;
     if (take_sqrt) d = sqrt(d);
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-        y[t] = x[t] / d;
+        y[t] = (B)((double)x[t] / d);
 }
 
 // z = x - y
-__global__ void k_sub(const double* x, const double* y, double* z, long long n) {
+template <typename A, typename Bt, typename C>
+__global__ void k_sub(const A* x, const Bt* y, C* z, long long n) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-        z[t] = x[t] - y[t];
+        z[t] = (C)((double)x[t] - (double)y[t]);
 }
 
 // X += sum_j U_j y_j  (U_j at stride n), y on device
-__global__ void k_multi_axpy(double* __restrict__ X, const double* __restrict__ U, const double* __restrict__ yv,
-                             int m, long long n) {
+template <typename B>
+__global__ void k_multi_axpy(double* __restrict__ X, const B* __restrict__ U, const double* __restrict__ yv, int m,
+                             long long n) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         double xv = X[t];
-        for (int j = 0; j < m; ++j) xv = xv + U[(size_t)j * n + t] * yv[j];
+        for (int j = 0; j < m; ++j) xv = xv + (double)U[(size_t)j * n + t] * yv[j];
         X[t] = xv;
     }
 }
 
-// ---------------------------------------------------------------------------
-// Block SpMVs (SPARMULVV/VS/SV/SS, memLS.f90:2024-2236), 8 lanes per row.
-// ---------------------------------------------------------------------------
-constexpr int kLanes = 8;
+__global__ void k_scale(double a, double* __restrict__ x, long long n) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        x[t] = a * x[t];
+}
 
-__device__ __forceinline__ double group_sum8(double v) {
-    v += __shfl_xor_sync(0xffffffffu, v, 4);
+template <typename T, typename S>
+__global__ void k_convert(const S* __restrict__ in, T* __restrict__ out, long long n) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        out[t] = (T)in[t];
+}
+
+// ---------------------------------------------------------------------------
+// Block SpMVs (SPARMULVV/VS/SV/SS, memLS.f90:2024-2236).
+// Four lanes per block row; each lane handles blocks j = s + lane + 4k and
+// issues kUnroll of them together (column index, matrix values, gathered
+// vector entries), so 16 independent loads per row are in flight instead of
+// one dependent col -> x chain.  Matrix data is read through the read-only
+// path (__ldg); evict-first loads measured slower on this pattern.
+// ---------------------------------------------------------------------------
+constexpr int kLanes = 4;
+constexpr int kUnroll = 4;
+
+__device__ __forceinline__ double group_sum(double v) {
     v += __shfl_xor_sync(0xffffffffu, v, 2);
     v += __shfl_xor_sync(0xffffffffu, v, 1);
     return v;
 }
 
+// Rows handled by this thread's lane group: r = r0 + threadIdx.x / kLanes,
+// r0 block-uniform so every lane of a warp reaches the shuffles.
+#define CR_ROW_LOOP(n)                                                                          \
+    const int lane = threadIdx.x & (kLanes - 1);                                                \
+    const long long ngrp = (long long)gridDim.x * (blockDim.x / kLanes);                        \
+    for (long long r0 = (long long)blockIdx.x * (blockDim.x / kLanes); r0 < (n); r0 += ngrp) { \
+        const long long r = r0 + threadIdx.x / kLanes;                                          \
+        const bool rv = r < (n);
+
+// Unrolled visit of the blocks of row r: j and c defined for the body; ok marks valid blocks.
+#define CR_ROW_BLOCKS(rowptr, col, ...)                                              \
+    if (rv) {                                                                         \
+        const int rs_ = (rowptr)[r], re_ = (rowptr)[r + 1];                           \
+        for (int b0_ = rs_ + lane; b0_ < re_; b0_ += kLanes * kUnroll) {              \
+            int cj_[kUnroll];                                                         \
+            _Pragma("unroll") for (int k_ = 0; k_ < kUnroll; ++k_) {                  \
+                const int j_ = b0_ + k_ * kLanes;                                     \
+                cj_[k_] = __ldg((col) + (j_ < re_ ? j_ : b0_));                       \
+            }                                                                         \
+            _Pragma("unroll") for (int k_ = 0; k_ < kUnroll; ++k_) {                  \
+                const int j0_ = b0_ + k_ * kLanes;                                    \
+                const bool ok = j0_ < re_;                                            \
+                const size_t j = (size_t)(ok ? j0_ : b0_);                            \
+                const int c = cj_[k_];                                                \
+                __VA_ARGS__                                                           \
+            }                                                                         \
+        }                                                                             \
+    }
+
 // KU = K U, K (9, nnz), U/KU (3, n)
+template <typename M, typename IN, typename OUT>
 __global__ void __launch_bounds__(256) k_spmv_vv3(const int* __restrict__ rowptr, const int* __restrict__ col,
-                                                  const double* __restrict__ K, const double* __restrict__ U,
-                                                  double* __restrict__ KU, int n) {
-    const int lane = threadIdx.x & (kLanes - 1);
-    const long long ng = (long long)gridDim.x * (blockDim.x / kLanes);
-    for (long long r0 = (long long)blockIdx.x * (blockDim.x / kLanes); r0 < n; r0 += ng) {
-        const long long r = r0 + threadIdx.x / kLanes;
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        if (r < n) {
-            const int s = rowptr[r], e = rowptr[r + 1];
-            for (int j = s + lane; j < e; j += kLanes) {
-                const double* k = K + 9 * (size_t)j;
-                const double* u = U + 3 * (size_t)col[j];
-                const double u0 = u[0], u1 = u[1], u2 = u[2];
-                a0 += k[0] * u0 + k[1] * u1 + k[2] * u2;
-                a1 += k[3] * u0 + k[4] * u1 + k[5] * u2;
-                a2 += k[6] * u0 + k[7] * u1 + k[8] * u2;
-            }
+                                                  const M* __restrict__ K, const IN* __restrict__ U,
+                                                  OUT* __restrict__ KU, int n) {
+    CR_ROW_LOOP(n)
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    CR_ROW_BLOCKS(rowptr, col, {
+        const M* k = K + 9 * j;
+        const IN* u = U + 3 * (size_t)c;
+        const double u0 = (double)u[0], u1 = (double)u[1], u2 = (double)u[2];
+        const double k0 = (double)__ldg(k + 0), k1 = (double)__ldg(k + 1), k2 = (double)__ldg(k + 2),
+                     k3 = (double)__ldg(k + 3), k4 = (double)__ldg(k + 4), k5 = (double)__ldg(k + 5),
+                     k6 = (double)__ldg(k + 6), k7 = (double)__ldg(k + 7), k8 = (double)__ldg(k + 8);
+        if (ok) {
+            a0 += k0 * u0 + k1 * u1 + k2 * u2;
+            a1 += k3 * u0 + k4 * u1 + k5 * u2;
+            a2 += k6 * u0 + k7 * u1 + k8 * u2;
         }
-        a0 = group_sum8(a0);
-        a1 = group_sum8(a1);
-        a2 = group_sum8(a2);
-        if (r < n && lane == 0) {
-            KU[3 * r + 0] = a0;
-            KU[3 * r + 1] = a1;
-            KU[3 * r + 2] = a2;
-        }
+    })
+    a0 = group_sum(a0);
+    a1 = group_sum(a1);
+    a2 = group_sum(a2);
+    if (rv && lane == 0) {
+        KU[3 * r + 0] = (OUT)a0;
+        KU[3 * r + 1] = (OUT)a1;
+        KU[3 * r + 2] = (OUT)a2;
+    }
     }
 }
 
 // KU(i) = sum K(:,j).U(:,col)  (3 -> 1)
+template <typename M, typename IN, typename OUT>
 __global__ void __launch_bounds__(256) k_spmv_vs3(const int* __restrict__ rowptr, const int* __restrict__ col,
-                                                  const double* __restrict__ K, const double* __restrict__ U,
-                                                  double* __restrict__ KU, int n) {
-    const int lane = threadIdx.x & (kLanes - 1);
-    const long long ng = (long long)gridDim.x * (blockDim.x / kLanes);
-    for (long long r0 = (long long)blockIdx.x * (blockDim.x / kLanes); r0 < n; r0 += ng) {
-        const long long r = r0 + threadIdx.x / kLanes;
-        double a = 0.0;
-        if (r < n) {
-            const int s = rowptr[r], e = rowptr[r + 1];
-            for (int j = s + lane; j < e; j += kLanes) {
-                const double* k = K + 3 * (size_t)j;
-                const double* u = U + 3 * (size_t)col[j];
-                a += k[0] * u[0] + k[1] * u[1] + k[2] * u[2];
-            }
-        }
-        a = group_sum8(a);
-        if (r < n && lane == 0) KU[r] = a;
+                                                  const M* __restrict__ K, const IN* __restrict__ U,
+                                                  OUT* __restrict__ KU, int n) {
+    CR_ROW_LOOP(n)
+    double a = 0.0;
+    CR_ROW_BLOCKS(rowptr, col, {
+        const M* k = K + 3 * j;
+        const IN* u = U + 3 * (size_t)c;
+        const double t = (double)__ldg(k) * (double)u[0] + (double)__ldg(k + 1) * (double)u[1] +
+                         (double)__ldg(k + 2) * (double)u[2];
+        if (ok) a += t;
+    })
+    a = group_sum(a);
+    if (rv && lane == 0) KU[r] = (OUT)a;
     }
 }
 
 // KU(:,i) = sum K(:,j) U(col)  (1 -> 3)
+template <typename M, typename IN, typename OUT>
 __global__ void __launch_bounds__(256) k_spmv_sv3(const int* __restrict__ rowptr, const int* __restrict__ col,
-                                                  const double* __restrict__ K, const double* __restrict__ U,
-                                                  double* __restrict__ KU, int n) {
-    const int lane = threadIdx.x & (kLanes - 1);
-    const long long ng = (long long)gridDim.x * (blockDim.x / kLanes);
-    for (long long r0 = (long long)blockIdx.x * (blockDim.x / kLanes); r0 < n; r0 += ng) {
-        const long long r = r0 + threadIdx.x / kLanes;
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        if (r < n) {
-            const int s = rowptr[r], e = rowptr[r + 1];
-            for (int j = s + lane; j < e; j += kLanes) {
-                const double* k = K + 3 * (size_t)j;
-                const double u = U[col[j]];
-                a0 += k[0] * u;
-                a1 += k[1] * u;
-                a2 += k[2] * u;
-            }
+                                                  const M* __restrict__ K, const IN* __restrict__ U,
+                                                  OUT* __restrict__ KU, int n) {
+    CR_ROW_LOOP(n)
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    CR_ROW_BLOCKS(rowptr, col, {
+        const M* k = K + 3 * j;
+        const double u = (double)U[c];
+        const double k0 = (double)__ldg(k), k1 = (double)__ldg(k + 1), k2 = (double)__ldg(k + 2);
+        if (ok) {
+            a0 += k0 * u;
+            a1 += k1 * u;
+            a2 += k2 * u;
         }
-        a0 = group_sum8(a0);
-        a1 = group_sum8(a1);
-        a2 = group_sum8(a2);
-        if (r < n && lane == 0) {
-            KU[3 * r + 0] = a0;
-            KU[3 * r + 1] = a1;
-            KU[3 * r + 2] = a2;
-        }
+    })
+    a0 = group_sum(a0);
+    a1 = group_sum(a1);
+    a2 = group_sum(a2);
+    if (rv && lane == 0) {
+        KU[3 * r + 0] = (OUT)a0;
+        KU[3 * r + 1] = (OUT)a1;
+        KU[3 * r + 2] = (OUT)a2;
+    }
     }
 }
 
-// CG operator: SP = L P - Gt GP, and out = <P, SP> (fused SPARMULSS, SPARMULVS, DOTS)
-__global__ void __launch_bounds__(256) k_cg_op(const int* __restrict__ rowptr, const int* __restrict__ col,
-                                               const double* __restrict__ L, const double* __restrict__ Gt,
-                                               const double* __restrict__ P, const double* __restrict__ GP,
-                                               double* __restrict__ SP, int n, double* part, unsigned int* ticket,
-                                               double* out) {
-    __shared__ double sm[32];
-    const int lane = threadIdx.x & (kLanes - 1);
-    const long long ng = (long long)gridDim.x * (blockDim.x / kLanes);
-    double dsum = 0.0;
-    for (long long r0 = (long long)blockIdx.x * (blockDim.x / kLanes); r0 < n; r0 += ng) {
-        const long long r = r0 + threadIdx.x / kLanes;
-        double a = 0.0, b = 0.0;
-        if (r < n) {
-            const int s = rowptr[r], e = rowptr[r + 1];
-            for (int j = s + lane; j < e; j += kLanes) {
-                const int c = col[j];
-                a += L[j] * P[c];
-                const double* g = Gt + 3 * (size_t)j;
-                const double* gp = GP + 3 * (size_t)c;
-                b += g[0] * gp[0] + g[1] * gp[1] + g[2] * gp[2];
-            }
-        }
-        a = group_sum8(a);
-        b = group_sum8(b);
-        if (r < n && lane == 0) {
-            const double v = a - b;
-            SP[r] = v;
-            dsum += P[r] * v;
-        }
+// KU = K U, scalar
+template <typename M, typename IN, typename OUT>
+__global__ void __launch_bounds__(256) k_spmv_ss(const int* __restrict__ rowptr, const int* __restrict__ col,
+                                                 const M* __restrict__ K, const IN* __restrict__ U,
+                                                 OUT* __restrict__ KU, int n) {
+    CR_ROW_LOOP(n)
+    double a = 0.0;
+    CR_ROW_BLOCKS(rowptr, col, {
+        const double t = (double)__ldg(K + j) * (double)U[c];
+        if (ok) a += t;
+    })
+    a = group_sum(a);
+    if (rv && lane == 0) KU[r] = (OUT)a;
     }
-    dsum = block_sum(dsum, sm);
-    grid_reduce_finish(dsum, part, ticket, out, sm);
 }
 
-// X += alpha P, R -= alpha SP, out = <R, R>, alpha = (*errO)/(*den)
-__global__ void k_cg_update(double* __restrict__ X, double* __restrict__ R, const double* __restrict__ P,
-                            const double* __restrict__ SP, int n, const double* errO, const double* den, double* part,
-                            unsigned int* ticket, double* out) {
-    __shared__ double sm[32];
-    const double alpha = *errO / *den;
+// (G^T v)(c) = sum over row c of G(:, trans j) . v(:, col j)   (transposed SPARMULVS)
+template <typename M>
+__global__ void __launch_bounds__(256) k_spmv_vs3_trans(const int* __restrict__ rowptr, const int* __restrict__ col,
+                                                        const int* __restrict__ trans, const M* __restrict__ G,
+                                                        const double* __restrict__ V, double* __restrict__ out, int n) {
+    CR_ROW_LOOP(n)
+    double acc = 0.0;
+    CR_ROW_BLOCKS(rowptr, col, {
+        const M* g = G + 3 * (size_t)trans[j];
+        const double* v = V + 3 * (size_t)c;
+        const double t = (double)g[0] * v[0] + (double)g[1] * v[1] + (double)g[2] * v[2];
+        if (ok) acc += t;
+    })
+    acc = group_sum(acc);
+    if (rv && lane == 0) out[r] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CGRAD as one persistent cooperative kernel (memLS.f90:367-430).
+//
+// Per iteration three grid-wide barriers: (A) P = R + beta P formed on the
+// fly while computing GP = G P, plus the coupled-face dots w_f . P; (B)
+// SP = L P - Gt GP - sum_f coef_f (w_f . P) z_f and <P, SP>; (C) X += alpha P,
+// R -= alpha SP, |R|^2.  The coupled-face (Sherman-Morrison) term of
+// ADDBCMUL(PRE) is applied through the precomputed vectors w_f = G^T valM_f
+// and z_f = Gt valM_f: Gt (GP + coef valM (valM . GP)) = Gt GP + coef (w.P) z
+// -- exact.  Node records keep every gather to one aligned sector:
+// recA = {R, P_prev} (16 B) read in phase A, recB = {GP, P} (32 B) read in
+// phase B; matrix blocks GL = {Gt, L}.  Partial sums are written per block
+// and summed in block order by every block after the barrier
+// (deterministic, identical in all blocks).  Values written by other blocks
+// earlier in the kernel are read with __ldcg (L2), never from a possibly
+// stale L1 line.  The loop is bounded by mItr.  Vectors and scalars are FP64
+// in both precisions; M is the storage type of G, Gt and L.
+// ---------------------------------------------------------------------------
+constexpr int kMaxCoupled = 8;
+
+template <typename M>
+struct CgArgs {
+    const int* rowptr;
+    const int* col;
+    int n;
+    const M* G;                      // (3, nnz)
+    const typename V4<M>::type* GL;  // (nnz) {Gt0, Gt1, Gt2, L}
+    double* X;
+    double2* recA;  // (n) {R, P of the previous iteration}
+    double4* recB;  // (n) {GP0, GP1, GP2, P}
+    double* SP;
+    int nface;
+    const double* w;  // (nface, n)
+    const double* z;  // (nface, n)
+    double coef[kMaxCoupled];
+    double eps;   // squared tolerance
+    double err0;  // squared initial norm
+    int mItr;
+    double* part;  // 3 regions of kCgPartStride * gridDim
+    double* out;   // err, errO, i, suc
+};
+constexpr int kCgPartStride = kMaxCoupled + 2;
+
+__device__ __forceinline__ double sum_partials(const double* part, int k, double* sm) {
     double s = 0.0;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        X[t] = X[t] + alpha * P[t];
-        double r = R[t] - alpha * SP[t];
-        R[t] = r;
-        s += r * r;
-    }
-    s = block_sum(s, sm);
-    grid_reduce_finish(s, part, ticket, out, sm);
+    for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += __ldcg(part + (size_t)b * kCgPartStride + k);
+    return block_sum(s, sm);
 }
 
-// P = R + (err/errO) P
-__global__ void k_cg_dir(double* __restrict__ P, const double* __restrict__ R, int n, const double* err,
-                         const double* errO) {
-    const double f = *err / *errO;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) P[t] = R[t] + f * P[t];
+template <int NF, typename M>
+__global__ void __launch_bounds__(256, 4) k_cg_persistent(CgArgs<M> a) {
+    namespace cgrp = cooperative_groups;
+    cgrp::grid_group grid = cgrp::this_grid();
+    __shared__ double sm[32];
+    const int n = a.n;
+    double* partA = a.part;
+    double* partB = a.part + (size_t)gridDim.x * kCgPartStride;
+    double* partC = a.part + 2 * (size_t)gridDim.x * kCgPartStride;
+    double err = a.err0, errO = a.err0;
+    int suc = 0, i;
+    for (i = 1; i <= a.mItr; ++i) {
+        if (err < a.eps) {
+            suc = 1;
+            break;
+        }
+        const bool first = (i == 1);
+        const double beta = first ? 0.0 : err / errO;
+        errO = err;
+        // ---- phase A: P = R + beta P_prev (on the fly), GP = G P, w_f . P ----
+        double wp[NF > 0 ? NF : 1];
+#pragma unroll
+        for (int f = 0; f < (NF > 0 ? NF : 1); ++f) wp[f] = 0.0;
+        {
+            CR_ROW_LOOP(n)
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+            CR_ROW_BLOCKS(a.rowptr, a.col, {
+                const double2 rp = __ldcg(a.recA + c);
+                const double pc = first ? rp.x : rp.x + beta * rp.y;
+                const M* g = a.G + 3 * j;
+                const double g0 = (double)__ldg(g), g1 = (double)__ldg(g + 1), g2 = (double)__ldg(g + 2);
+                if (ok) {
+                    a0 += g0 * pc;
+                    a1 += g1 * pc;
+                    a2 += g2 * pc;
+                }
+            })
+            a0 = group_sum(a0);
+            a1 = group_sum(a1);
+            a2 = group_sum(a2);
+            if (rv && lane == 0) {
+                const double2 rr = __ldcg(a.recA + r);
+                const double pr = first ? rr.x : rr.x + beta * rr.y;
+                a.recB[r] = make_double4(a0, a1, a2, pr);
+#pragma unroll
+                for (int f = 0; f < NF; ++f)
+                    if (f < a.nface) wp[f] += a.w[(size_t)f * n + r] * pr;
+            }
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            if (f < a.nface) {
+                double t = block_sum(wp[f], sm);
+                if (threadIdx.x == 0) partA[(size_t)blockIdx.x * kCgPartStride + f] = t;
+            }
+        }
+        grid.sync();
+        double cS[NF > 0 ? NF : 1];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) cS[f] = f < a.nface ? a.coef[f] * sum_partials(partA, f, sm) : 0.0;
+        // ---- phase B: SP = L P - Gt GP - sum_f cS_f z_f ; <P, SP> ----
+        double dsum = 0.0;
+        {
+            CR_ROW_LOOP(n)
+            double lp = 0.0, gg = 0.0;
+            CR_ROW_BLOCKS(a.rowptr, a.col, {
+                const auto gl = ldg4(a.GL + j);
+                const double4 q = ldcg4(a.recB + c);
+                const double tl = (double)gl.w * q.w;
+                const double tg = (double)gl.x * q.x + (double)gl.y * q.y + (double)gl.z * q.z;
+                if (ok) {
+                    lp += tl;
+                    gg += tg;
+                }
+            })
+            lp = group_sum(lp);
+            gg = group_sum(gg);
+            if (rv && lane == 0) {
+#pragma unroll
+                for (int f = 0; f < NF; ++f)
+                    if (f < a.nface) gg += cS[f] * a.z[(size_t)f * n + r];
+                const double v = lp - gg;
+                a.SP[r] = v;
+                dsum += __ldcg(&a.recB[r].w) * v;
+            }
+            }
+        }
+        dsum = block_sum(dsum, sm);
+        if (threadIdx.x == 0) partB[(size_t)blockIdx.x * kCgPartStride] = dsum;
+        grid.sync();
+        const double alpha = errO / sum_partials(partB, 0, sm);
+        // ---- phase C: X += alpha P, R -= alpha SP, |R|^2 ; recA = {R, P} ----
+        double rs = 0.0;
+        for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+             t += (long long)gridDim.x * blockDim.x) {
+            const double pv = __ldcg(&a.recB[t].w);
+            a.X[t] = a.X[t] + alpha * pv;
+            const double rv = __ldcg(&a.recA[t].x) - alpha * __ldcg(a.SP + t);
+            a.recA[t] = make_double2(rv, pv);
+            rs += rv * rv;
+        }
+        rs = block_sum(rs, sm);
+        if (threadIdx.x == 0) partC[(size_t)blockIdx.x * kCgPartStride] = rs;
+        grid.sync();
+        const double e2 = sqrt(sum_partials(partC, 0, sm));
+        err = e2 * e2;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.out[0] = err;
+        a.out[1] = errO;
+        a.out[2] = (double)i;
+        a.out[3] = (double)suc;
+    }
+}
+
+// recA = {R, 0}
+__global__ void k_cg_init(const double* __restrict__ R, double2* __restrict__ recA, int n) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) recA[t] = make_double2(R[t], 0.0);
+}
+
+// GL = {Gt(3), L} per block, in the matrix storage type
+template <typename M>
+__global__ void k_pack_gl(const M* __restrict__ Gt, const M* __restrict__ Lm, typename V4<M>::type* __restrict__ GL,
+                          long long nnz) {
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nnz; j += (long long)gridDim.x * blockDim.x)
+        GL[j] = mk4<M>(Gt[3 * j], Gt[3 * j + 1], Gt[3 * j + 2], Lm[j]);
+}
+
+// ext = valM scattered into a (3, n) vector
+__global__ void k_face_ext(const int* __restrict__ glob, const double* __restrict__ valM, int fdof, int nsd, int nNoF,
+                           double* __restrict__ ext) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nNoF; a += gridDim.x * blockDim.x)
+        for (int i = 0; i < nsd; ++i) ext[3 * (size_t)glob[a] + i] = valM[(size_t)fdof * a + i];
 }
 
 // ---------------------------------------------------------------------------
 // ADDBCMUL pieces (memLS.f90:206-268): S = <valM, X> over face nodes; Y += S*coef*valM
 // ---------------------------------------------------------------------------
+template <typename V>
 __global__ void k_face_dot(const int* __restrict__ glob, const double* __restrict__ valM, int fdof, int nsd,
-                           int nNoF, const double* __restrict__ X, int dof, double* out) {
+                           int nNoF, const V* __restrict__ X, int dof, double* out) {
     __shared__ double sm[32];
     double s = 0.0;
     for (int a = threadIdx.x; a < nNoF; a += blockDim.x) {
         const int Ac = glob[a];
-        for (int i = 0; i < nsd; ++i) s += valM[(size_t)fdof * a + i] * X[(size_t)dof * Ac + i];
+        for (int i = 0; i < nsd; ++i) s += valM[(size_t)fdof * a + i] * (double)X[(size_t)dof * Ac + i];
     }
     s = block_sum(s, sm);
     if (threadIdx.x == 0) *out = s;
 }
 
+template <typename V>
 __global__ void k_face_axpy(const int* __restrict__ glob, const double* __restrict__ valM, int fdof, int nsd,
-                            int nNoF, const double* Sptr, double coef, double* __restrict__ Y, int dof) {
+                            int nNoF, const double* Sptr, double coef, V* __restrict__ Y, int dof) {
     const double S = coef * *Sptr;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nNoF; a += gridDim.x * blockDim.x) {
         const int Ac = glob[a];
-        for (int i = 0; i < nsd; ++i) Y[(size_t)dof * Ac + i] = Y[(size_t)dof * Ac + i] + valM[(size_t)fdof * a + i] * S;
+        for (int i = 0; i < nsd; ++i)
+            Y[(size_t)dof * Ac + i] = (V)((double)Y[(size_t)dof * Ac + i] + valM[(size_t)fdof * a + i] * S);
     }
 }
 
@@ -339,9 +590,9 @@ __global__ void k_w_dirichlet(const int* __restrict__ glob, const double* __rest
 
 // Row then column scaling of Val (16 per block) + zero-diagonal fix + DEPART split
 __global__ void k_scale_split_val(double* __restrict__ Val, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                  const int* __restrict__ diag, const int* __restrict__ trans,
-                                  const double* __restrict__ W, int n, double* __restrict__ mK,
-                                  double* __restrict__ mG, double* __restrict__ mD, double* __restrict__ mL) {
+                                  const int* __restrict__ diag, const double* __restrict__ W, int n,
+                                  double* __restrict__ mK, double* __restrict__ mG, double* __restrict__ mD,
+                                  double* __restrict__ mL) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         const double* wr = W + 4 * (size_t)r;
         for (int j = rowptr[r]; j < rowptr[r + 1]; ++j) {
@@ -448,10 +699,21 @@ __global__ void k_valm(const int* __restrict__ glob, const double* __restrict__ 
             valM[(size_t)fdof * a + i] = val[(size_t)fdof * a + i] * W[4 * (size_t)glob[a] + i];
 }
 
-}  // namespace crimson
+// Defect of the scaled NS system: D4 = R4 - [K u + G p ; D u + L p] given
+// KU = K u (+ coupling), GP = G p, DU = D u, LP = L p (all FP64).
+__global__ void k_defect4(const double* __restrict__ R4, const double* __restrict__ KU,
+                          const double* __restrict__ GPm, const double* __restrict__ DU,
+                          const double* __restrict__ LP, double* __restrict__ D4, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        for (int d = 0; d < 3; ++d)
+            D4[4 * (size_t)i + d] = R4[4 * (size_t)i + d] - (KU[3 * (size_t)i + d] + GPm[3 * (size_t)i + d]);
+        D4[4 * (size_t)i + 3] = R4[4 * (size_t)i + 3] - (DU[i] + LP[i]);
+    }
+}
 
-namespace crimson {
-
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
 static double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -463,7 +725,8 @@ enum {
     kSlotErr = 2,
     kSlotErrO = 3,
     kSlotDen = 4,
-    kSlotFace = 8,      // up to 32 faces
+    kSlotFace = 8,      // up to 16 faces
+    kSlotCg = 24,       // persistent CG outputs (4)
     kSlotH = 64,        // Hessenberg column (sD + 1)
     kSlotY = 64 + 512,  // back-substitution coefficients
     kSlotGram = 64 + 1024,
@@ -479,31 +742,40 @@ struct Ctx {
         CR_CUDA(cudaStreamSynchronize(s));
         return CRIMSON_OK;
     }
-    void dot(const double* u, const double* v, long long n, int slot) {
-        launch(k_dot, red_grid(n), 256, 0, s, u, v, n, L->red.part.p, L->red.ticket.p, sc(slot));
+    template <typename U, typename V>
+    void dot(const U* u, const V* v, long long n, int slot) {
+        launch(k_dot<U, V>, red_grid(n), 256, 0, s, u, v, n, L->red.part.p, L->red.ticket.p, sc(slot));
     }
-    void spmv_vv3(const double* K, const double* U, double* KU) {
-        launch(k_spmv_vv3, grid_for((long long)L->nNo * kLanes, 256, 8), 256, 0, s, L->rowptr, L->col, K, U, KU, L->nNo);
+    int spmv_grid() const { return grid_for((long long)L->nNo * kLanes, 256, 8); }
+    template <typename M, typename IN, typename OUT>
+    void vv3(const M* K, const IN* U, OUT* KU) {
+        launch(k_spmv_vv3<M, IN, OUT>, spmv_grid(), 256, 0, s, L->rowptr, L->col, K, U, KU, L->nNo);
     }
-    void spmv_vs3(const double* K, const double* U, double* KU) {
-        launch(k_spmv_vs3, grid_for((long long)L->nNo * kLanes, 256, 8), 256, 0, s, L->rowptr, L->col, K, U, KU, L->nNo);
+    template <typename M, typename IN, typename OUT>
+    void vs3(const M* K, const IN* U, OUT* KU) {
+        launch(k_spmv_vs3<M, IN, OUT>, spmv_grid(), 256, 0, s, L->rowptr, L->col, K, U, KU, L->nNo);
     }
-    void spmv_sv3(const double* K, const double* U, double* KU) {
-        launch(k_spmv_sv3, grid_for((long long)L->nNo * kLanes, 256, 8), 256, 0, s, L->rowptr, L->col, K, U, KU, L->nNo);
+    template <typename M, typename IN, typename OUT>
+    void sv3(const M* K, const IN* U, OUT* KU) {
+        launch(k_spmv_sv3<M, IN, OUT>, spmv_grid(), 256, 0, s, L->rowptr, L->col, K, U, KU, L->nNo);
     }
-    void spmv_ss_into(const double* Kd, const double* U, double* KU);
+    template <typename M, typename IN, typename OUT>
+    void ss(const M* K, const IN* U, OUT* KU) {
+        launch(k_spmv_ss<M, IN, OUT>, spmv_grid(), 256, 0, s, L->rowptr, L->col, K, U, KU, L->nNo);
+    }
     bool any_coupled() const {
         for (auto& f : L->face)
             if (f.coupledFlag) return true;
         return false;
     }
     // ADDBCMUL on nsd-dof vectors: all face dots first (on X), then all updates of Y
-    void addbcmul(int op, int dof, const double* X, double* Y) {
+    template <typename VX, typename VY>
+    void addbcmul(int op, int dof, const VX* X, VY* Y) {
         int k = 0;
         for (auto& f : L->face) {
             if (f.coupledFlag) {
                 int nsd = std::min(f.dof, dof);
-                launch(k_face_dot, 1, 512, 0, s, f.glob.p, f.valM.p, f.dof, nsd, f.nNo, X, dof, sc(kSlotFace + k));
+                launch(k_face_dot<VX>, 1, 512, 0, s, f.glob.p, f.valM.p, f.dof, nsd, f.nNo, X, dof, sc(kSlotFace + k));
             }
             ++k;
         }
@@ -512,42 +784,24 @@ struct Ctx {
             if (f.coupledFlag) {
                 int nsd = std::min(f.dof, dof);
                 double coef = (op == 0) ? f.res : -f.res / (1.0 + f.res * f.nS);
-                launch(k_face_axpy, grid_for(f.nNo, 256), 256, 0, s, f.glob.p, f.valM.p, f.dof, nsd, f.nNo,
-                                                                 sc(kSlotFace + k), coef, Y, dof);
+                launch(k_face_axpy<VY>, grid_for(f.nNo, 256), 256, 0, s, f.glob.p, f.valM.p, f.dof, nsd, f.nNo,
+                       (const double*)sc(kSlotFace + k), coef, Y, dof);
             }
             ++k;
         }
     }
 };
 
-__global__ void k_spmv_ss(const int* __restrict__ rowptr, const int* __restrict__ col, const double* __restrict__ K,
-                          const double* __restrict__ U, double* __restrict__ KU, int n) {
-    const int lane = threadIdx.x & (kLanes - 1);
-    const long long ng = (long long)gridDim.x * (blockDim.x / kLanes);
-    for (long long r0 = (long long)blockIdx.x * (blockDim.x / kLanes); r0 < n; r0 += ng) {
-        const long long r = r0 + threadIdx.x / kLanes;
-        double a = 0.0;
-        if (r < n) {
-            const int s = rowptr[r], e = rowptr[r + 1];
-            for (int j = s + lane; j < e; j += kLanes) a += K[j] * U[col[j]];
-        }
-        a = group_sum8(a);
-        if (r < n && lane == 0) KU[r] = a;
-    }
-}
-
-void Ctx::spmv_ss_into(const double* Kd, const double* U, double* KU) {
-    launch(k_spmv_ss, grid_for((long long)L->nNo * kLanes, 256, 8), 256, 0, s, L->rowptr, L->col, Kd, U, KU, L->nNo);
-}
-
-// GMRES (memLS.f90:681-788) on dof = 3 with K = mK; X may not alias R.
-static int gmres(Ctx& C, crimson_subls& ls, const double* K, const double* R, double* X) {
+// GMRES (memLS.f90:681-788) on dof = 3; K in M, basis in B, R and X FP64; X may not alias R.
+template <typename M, typename B>
+static int gmres(Ctx& C, crimson_subls& ls, const M* K, const double* R, double* X) {
     crimson_lhs* L = C.L;
     cudaStream_t s = C.s;
     const int dof = 3;
     const long long n = (long long)dof * L->nNo;
     const int sD = ls.sD;
-    double* u = L->basis.p;
+    B* u = reinterpret_cast<B*>(L->basis.p);
+    B* w3 = reinterpret_cast<B*>(L->w3.p);
     auto U = [&](int k) { return u + (size_t)k * n; };
     std::vector<double> h((size_t)(sD + 1) * sD, 0.0), c(sD), sn(sD), err(sD + 1), y(sD);
     auto H = [&](int i, int j) -> double& { return h[(size_t)j * (sD + 1) + i]; };
@@ -559,18 +813,18 @@ static int gmres(Ctx& C, crimson_subls& ls, const double* K, const double* R, do
     int i = 0;
     for (int l = 1; l <= ls.mItr; ++l) {
         if (l == 1) {
-            CR_CUDA(cudaMemcpyAsync(U(0), R, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+            launch(k_convert<B, double>, grid_for(n, 256), 256, 0, s, R, U(0), n);
         } else {
             ls.itr = ls.itr + 1;
-            C.spmv_vv3(K, X, U(0));
-            C.addbcmul(0, dof, X, U(0));
-            launch(k_sub, grid_for(n, 256), 256, 0, s, R, U(0), U(0), n);
+            C.vv3(K, (const double*)X, U(0));
+            C.addbcmul(0, dof, (const double*)X, U(0));
+            launch(k_sub<double, B, B>, grid_for(n, 256), 256, 0, s, R, (const B*)U(0), U(0), n);
         }
         if (coupled) {
-            CR_CUDA(cudaMemcpyAsync(L->w3.p, U(0), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-            C.addbcmul(1, dof, L->w3.p, U(0));
+            CR_CUDA(cudaMemcpyAsync(w3, U(0), sizeof(B) * n, cudaMemcpyDeviceToDevice, s));
+            C.addbcmul(1, dof, (const B*)w3, U(0));
         }
-        C.dot(U(0), U(0), n, kSlotNrm);
+        C.dot((const B*)U(0), (const B*)U(0), n, kSlotNrm);
         CR_CHECK(C.sync_scal(kSlotNrm, 1));
         err[0] = std::sqrt(L->hscal[kSlotNrm]);
         if (l == 1) {
@@ -585,25 +839,25 @@ static int gmres(Ctx& C, crimson_subls& ls, const double* K, const double* R, do
             eps = std::max(ls.absTol, ls.relTol * eps);
         }
         ls.dB = ls.fNorm;
-        launch(k_divide, grid_for(n, 256), 256, 0, s, U(0), C.sc(kSlotNrm), U(0), n, 1);
+        launch(k_divide<B>, grid_for(n, 256), 256, 0, s, (const B*)U(0), (const double*)C.sc(kSlotNrm), U(0), n, 1);
         for (i = 1; i <= sD; ++i) {
             ls.itr = ls.itr + 1;
-            double* w = U(i);
-            C.spmv_vv3(K, U(i - 1), w);
-            C.addbcmul(0, dof, U(i - 1), w);
+            B* w = U(i);
+            C.vv3(K, (const B*)U(i - 1), w);
+            C.addbcmul(0, dof, (const B*)U(i - 1), w);
             if (coupled) {
-                CR_CUDA(cudaMemcpyAsync(L->w3.p, w, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-                C.addbcmul(1, dof, L->w3.p, w);
+                CR_CUDA(cudaMemcpyAsync(w3, w, sizeof(B) * n, cudaMemcpyDeviceToDevice, s));
+                C.addbcmul(1, dof, (const B*)w3, w);
             }
             // fused modified Gram-Schmidt
             for (int j = 1; j <= i; ++j) {
-                const double* uprev = (j == 1) ? nullptr : U(j - 2);
-                launch(k_mgs, red_grid(n), 256, 0, s, w, uprev, C.sc(kSlotH + j - 2), U(j - 1), n, L->red.part.p,
-                                                  L->red.ticket.p, C.sc(kSlotH + j - 1));
+                const B* uprev = (j == 1) ? nullptr : U(j - 2);
+                launch(k_mgs<B>, red_grid(n), 256, 0, s, w, uprev, (const double*)C.sc(kSlotH + j - 2),
+                       (const B*)U(j - 1), n, L->red.part.p, L->red.ticket.p, C.sc(kSlotH + j - 1));
             }
-            launch(k_mgs, red_grid(n), 256, 0, s, w, U(i - 1), C.sc(kSlotH + i - 1), w, n, L->red.part.p, L->red.ticket.p,
-                                              C.sc(kSlotH + i));
-            launch(k_divide, grid_for(n, 256), 256, 0, s, w, C.sc(kSlotH + i), w, n, 1);
+            launch(k_mgs<B>, red_grid(n), 256, 0, s, w, (const B*)U(i - 1), (const double*)C.sc(kSlotH + i - 1),
+                   (const B*)w, n, L->red.part.p, L->red.ticket.p, C.sc(kSlotH + i));
+            launch(k_divide<B>, grid_for(n, 256), 256, 0, s, (const B*)w, (const double*)C.sc(kSlotH + i), w, n, 1);
             CR_CHECK(C.sync_scal(kSlotH, i + 1));
             for (int j = 1; j <= i; ++j) H(j - 1, i - 1) = L->hscal[kSlotH + j - 1];
             H(i, i - 1) = std::sqrt(L->hscal[kSlotH + i]);
@@ -633,8 +887,8 @@ static int gmres(Ctx& C, crimson_subls& ls, const double* K, const double* R, do
         }
         std::memcpy(L->hscal + kSlotY, y.data(), sizeof(double) * i);
         CR_CUDA(cudaMemcpyAsync(C.sc(kSlotY), L->hscal + kSlotY, sizeof(double) * i, cudaMemcpyHostToDevice, s));
-        launch(k_multi_axpy, grid_for(n, 256), 256, 0, s, X, u, C.sc(kSlotY), i, n);
-        CR_CUDA(cudaStreamSynchronize(s));   // y staging buffer is reused
+        launch(k_multi_axpy<B>, grid_for(n, 256), 256, 0, s, X, (const B*)u, (const double*)C.sc(kSlotY), i, n);
+        CR_CUDA(cudaStreamSynchronize(s));  // y staging buffer is reused
         ls.fNorm = std::fabs(err[i]);
         if (ls.suc) break;
     }
@@ -643,19 +897,45 @@ static int gmres(Ctx& C, crimson_subls& ls, const double* K, const double* R, do
     return CRIMSON_OK;
 }
 
-// CGRAD (memLS.f90:367-430) on the Schur-like operator L P - Gt G P; R in/out (n)
-static int cgrad(Ctx& C, crimson_subls& ls, const double* Gt, const double* G, const double* Lm, double* R) {
+// Coupled-face vectors for the CG's ADDBCMUL(PRE) term: w_f = G^T valM_f and
+// z_f = Gt valM_f, with the Sherman-Morrison coefficient -res/(1 + res nS).
+// Built once per NSSOLVER call (valM, G, Gt are fixed during it).
+template <typename M>
+static int cg_faces(Ctx& C, const M* G, const M* Gt, int* nface, double* coef) {
+    crimson_lhs* L = C.L;
+    cudaStream_t s = C.s;
+    const int n = L->nNo;
+    int k = 0;
+    for (auto& f : L->face) {
+        if (!f.coupledFlag) continue;
+        if (k >= kMaxCoupled) return CRIMSON_ERR_UNSUPPORTED;
+        CR_CHECK(L->cgExt.alloc(3 * (size_t)n));
+        CR_CHECK(L->cgW.alloc((size_t)kMaxCoupled * n));
+        CR_CHECK(L->cgZ.alloc((size_t)kMaxCoupled * n));
+        CR_CUDA(cudaMemsetAsync(L->cgExt.p, 0, sizeof(double) * 3 * (size_t)n, s));
+        launch(k_face_ext, grid_for(f.nNo, 256), 256, 0, s, f.glob.p, f.valM.p, f.dof, std::min(f.dof, 3), f.nNo,
+               L->cgExt.p);
+        launch(k_spmv_vs3_trans<M>, C.spmv_grid(), 256, 0, s, L->rowptr, L->col, L->trans, G, (const double*)L->cgExt.p,
+               L->cgW.p + (size_t)k * n, n);
+        C.vs3(Gt, (const double*)L->cgExt.p, L->cgZ.p + (size_t)k * n);
+        coef[k] = -f.res / (1.0 + f.res * f.nS);
+        ++k;
+    }
+    *nface = k;
+    CR_CUDA(cudaGetLastError());
+    return CRIMSON_OK;
+}
+
+// CGRAD (memLS.f90:367-430) on the Schur-like operator L P - Gt G P; R in/out (n).
+// GL (packed {Gt, L}) must be current for this NSSOLVER call.
+template <typename M>
+static int cgrad(Ctx& C, crimson_subls& ls, const M* G, double* R, int nface, const double* coef) {
     crimson_lhs* L = C.L;
     cudaStream_t s = C.s;
     const int n = L->nNo;
     const double time = now_s();
-    const bool coupled = C.any_coupled();
-    double* X = L->cgX.p;
-    double* P = L->cgP.p;
-    double* SP = L->cgSP.p;
-    double* GP = L->cgGP.p;
     ls.suc = 0;
-    C.dot(R, R, n, kSlotErr);
+    C.dot((const double*)R, (const double*)R, n, kSlotErr);
     CR_CHECK(C.sync_scal(kSlotErr, 1));
     double errO = std::sqrt(L->hscal[kSlotErr]);
     ls.iNorm = errO;
@@ -663,36 +943,59 @@ static int cgrad(Ctx& C, crimson_subls& ls, const double* Gt, const double* G, c
     eps = eps * eps;
     double err = errO;
     err = err * err;
-    // the device err slot holds the squared norm; the reference re-squares sqrt(sum)
-    L->hscal[kSlotErr] = err;
-    CR_CUDA(cudaMemcpyAsync(C.sc(kSlotErr), L->hscal + kSlotErr, sizeof(double), cudaMemcpyHostToDevice, s));
-    CR_CUDA(cudaMemsetAsync(X, 0, sizeof(double) * n, s));
-    CR_CUDA(cudaMemcpyAsync(P, R, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-    int i;
-    for (i = 1; i <= ls.mItr; ++i) {
-        if (err < eps) {
-            ls.suc = 1;
-            break;
-        }
-        errO = err;
-        CR_CUDA(cudaMemcpyAsync(C.sc(kSlotErrO), C.sc(kSlotErr), sizeof(double), cudaMemcpyDeviceToDevice, s));
-        C.spmv_sv3(G, P, GP);
-        if (coupled) {
-            CR_CUDA(cudaMemcpyAsync(L->w3.p, GP, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, s));
-            C.addbcmul(1, 3, L->w3.p, GP);
-        }
-        launch(k_cg_op, red_grid((long long)n * kLanes), 256, 0, s, L->rowptr, L->col, Lm, Gt, P, GP, SP, n,
-                                                                L->red.part.p, L->red.ticket.p, C.sc(kSlotDen));
-        launch(k_cg_update, red_grid(n), 256, 0, s, X, R, P, SP, n, C.sc(kSlotErrO), C.sc(kSlotDen), L->red.part.p,
-                                                L->red.ticket.p, C.sc(kSlotErr));
-        CR_CHECK(C.sync_scal(kSlotErr, 1));
-        double e2 = std::sqrt(L->hscal[kSlotErr]);
-        err = e2 * e2;
-        L->hscal[kSlotErr] = err;
-        CR_CUDA(cudaMemcpyAsync(C.sc(kSlotErr), L->hscal + kSlotErr, sizeof(double), cudaMemcpyHostToDevice, s));
-        launch(k_cg_dir, grid_for(n, 256), 256, 0, s, P, R, n, C.sc(kSlotErr), C.sc(kSlotErrO));
+    const void* kfn = nface == 0 ? (const void*)k_cg_persistent<0, M>
+                      : (nface == 1 ? (const void*)k_cg_persistent<1, M> : (const void*)k_cg_persistent<kMaxCoupled, M>);
+    int& grid = std::is_same<M, float>::value ? L->cg_grid32 : L->cg_grid;
+    if (grid == 0) {
+        int nb0 = 0, nb1 = 0, nb8 = 0;
+        CR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb0, k_cg_persistent<0, M>, 256, 0));
+        CR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb1, k_cg_persistent<1, M>, 256, 0));
+        CR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb8, k_cg_persistent<kMaxCoupled, M>, 256, 0));
+        const int nb = std::min(nb0, std::min(nb1, nb8));
+        if (nb < 1) return CRIMSON_ERR_UNSUPPORTED;
+        grid = sm_count() * std::min(nb, 8);
     }
-    CR_CUDA(cudaMemcpyAsync(R, X, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    CR_CHECK(L->cgPart.alloc(3 * (size_t)kCgPartStride * std::max(L->cg_grid, L->cg_grid32)));
+    CR_CHECK(L->cgRecA.alloc(2 * (size_t)n));
+    CR_CHECK(L->cgRecB.alloc(4 * (size_t)n));
+    CR_CUDA(cudaMemsetAsync(L->cgX.p, 0, sizeof(double) * n, s));
+    launch(k_cg_init, grid_for(n, 256), 256, 0, s, (const double*)R, reinterpret_cast<double2*>(L->cgRecA.p), n);
+    CgArgs<M> a;
+    a.rowptr = L->rowptr;
+    a.col = L->col;
+    a.n = n;
+    a.G = G;
+    a.GL = reinterpret_cast<const typename V4<M>::type*>(L->cgGL.p);
+    a.X = L->cgX.p;
+    a.recA = reinterpret_cast<double2*>(L->cgRecA.p);
+    a.recB = reinterpret_cast<double4*>(L->cgRecB.p);
+    a.SP = L->cgSP.p;
+    a.nface = nface;
+    a.w = L->cgW.p;
+    a.z = L->cgZ.p;
+    for (int f = 0; f < kMaxCoupled; ++f) a.coef[f] = f < nface ? coef[f] : 0.0;
+    a.eps = eps;
+    a.err0 = err;
+    a.mItr = ls.mItr;
+    a.part = L->cgPart.p;
+    a.out = C.sc(kSlotCg);
+    void* kargs[] = {&a};
+    note_launch();
+    CR_CUDA(cudaEventRecord(L->ev0, s));
+    CR_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(256), kargs, 0, s));
+    CR_CUDA(cudaEventRecord(L->ev1, s));
+    CR_CHECK(C.sync_scal(kSlotCg, 4));
+    err = L->hscal[kSlotCg + 0];
+    errO = L->hscal[kSlotCg + 1];
+    const int i = (int)L->hscal[kSlotCg + 2];
+    ls.suc = (int)L->hscal[kSlotCg + 3];
+    float ms = 0.f;
+    CR_CUDA(cudaEventElapsedTime(&ms, L->ev0, L->ev1));
+    auto& acc = std::is_same<M, float>::value ? L->cg_acc32 : L->cg_acc64;
+    acc.ms += ms;
+    acc.iters += i - 1;
+    acc.launches += 1;
+    CR_CUDA(cudaMemcpyAsync(R, L->cgX.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     CR_CUDA(cudaStreamSynchronize(s));
     ls.fNorm = std::sqrt(err);
     ls.callD = now_s() - time + ls.callD;
@@ -740,9 +1043,10 @@ static int ge_solve(int N, const double* A, double* B) {
     return CRIMSON_OK;
 }
 
-// NSSOLVER (memLS.f90:1460-1759); R (4, nNo) in/out
-static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const double* mG, const double* mD,
-                    const double* mL, const double* Gt, double* R) {
+// NSSOLVER (memLS.f90:1460-1759); R (4, nNo) FP64 in/out; matrices in M.
+template <typename M, typename B>
+static int nssolver(crimson_lhs* L, crimson_ls* ls, const M* mK, const M* mG, const M* mD, const M* mL, const M* Gt,
+                    double* R) {
     Ctx C{L, L->stream};
     cudaStream_t s = L->stream;
     const int nNo = L->nNo;
@@ -753,13 +1057,13 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
     auto Pcol = [&](int k) { return L->P.p + (size_t)k * nNo; };
     auto MUc = [&](int k) { return L->MU.p + (size_t)k * nv; };
     auto MPc = [&](int k) { return L->MP.p + (size_t)k * nNo; };
-    launch(k_split4, grid_for(nNo, 256), 256, 0, s, R, L->Rmi.p, L->Rci.p, nNo);
+    launch(k_split4, grid_for(nNo, 256), 256, 0, s, (const double*)R, L->Rmi.p, L->Rci.p, nNo);
     CR_CUDA(cudaMemcpyAsync(L->Rm.p, L->Rmi.p, sizeof(double) * nv, cudaMemcpyDeviceToDevice, s));
     CR_CUDA(cudaMemcpyAsync(L->Rc.p, L->Rci.p, sizeof(double) * nNo, cudaMemcpyDeviceToDevice, s));
-    std::vector<double> A((size_t)nB * nB, 0.0), B(nB, 0.0), xB(nB, 0.0);
+    std::vector<double> A((size_t)nB * nB, 0.0), Bv(nB, 0.0), xB(nB, 0.0);
     auto Aa = [&](int i, int j) -> double& { return A[(size_t)j * nB + i]; };
-    C.dot(L->Rm.p, L->Rm.p, nv, 0);
-    C.dot(L->Rc.p, L->Rc.p, nNo, 1);
+    C.dot((const double*)L->Rm.p, (const double*)L->Rm.p, nv, 0);
+    C.dot((const double*)L->Rc.p, (const double*)L->Rc.p, nNo, 1);
     CR_CHECK(C.sync_scal(0, 2));
     double nv1 = std::sqrt(L->hscal[0]), ns1 = std::sqrt(L->hscal[1]);
     double eps = std::sqrt(std::pow(nv1, 2.0) + std::pow(ns1, 2.0));
@@ -784,33 +1088,41 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
         for (int a = 0; a < f.nNo; ++a)
             for (int i = 0; i < nsd; ++i) f.nS = f.nS + std::pow(vm[(size_t)f.dof * a + i], 2.0);
     }
+    int cg_nface = 0;
+    double cg_coef[kMaxCoupled];
+    CR_CHECK(cg_faces(C, mG, Gt, &cg_nface, cg_coef));
+    CR_CHECK(L->cgGL.alloc(4 * (size_t)L->nnz));
+    launch(k_pack_gl<M>, grid_for(L->nnz, 256), 256, 0, s, Gt, mL,
+           reinterpret_cast<typename V4<M>::type*>(L->cgGL.p), L->nnz);
     int i, iBB = 0;
     for (i = 1; i <= ls->RI.mItr; ++i) {
         iB = 2 * i - 1;
         iBB = 2 * i;
         ls->RI.dB = ls->RI.fNorm;
-        CR_CHECK(gmres(C, ls->GM, mK, L->Rm.p, Ucol(i - 1)));
-        C.spmv_vs3(mD, Ucol(i - 1), Pcol(i - 1));
-        launch(k_sub, grid_for(nNo, 256), 256, 0, s, L->Rc.p, Pcol(i - 1), Pcol(i - 1), nNo);
-        CR_CHECK(cgrad(C, ls->CG, Gt, mG, mL, Pcol(i - 1)));
-        C.spmv_sv3(mG, Pcol(i - 1), MUc(iB - 1));
-        launch(k_sub, grid_for(nv, 256), 256, 0, s, L->Rm.p, MUc(iB - 1), MUc(iBB - 1), nv);
-        CR_CHECK(gmres(C, ls->GM, mK, MUc(iBB - 1), Ucol(i - 1)));
-        C.spmv_vv3(mK, Ucol(i - 1), MUc(iBB - 1));
-        C.addbcmul(0, 3, Ucol(i - 1), MUc(iBB - 1));
-        C.spmv_ss_into(mL, Pcol(i - 1), MPc(iB - 1));
-        C.spmv_vs3(mD, Ucol(i - 1), MPc(iBB - 1));
+        CR_CHECK((gmres<M, B>(C, ls->GM, mK, L->Rm.p, Ucol(i - 1))));
+        C.vs3(mD, (const double*)Ucol(i - 1), Pcol(i - 1));
+        launch(k_sub<double, double, double>, grid_for(nNo, 256), 256, 0, s, (const double*)L->Rc.p,
+               (const double*)Pcol(i - 1), Pcol(i - 1), (long long)nNo);
+        CR_CHECK(cgrad<M>(C, ls->CG, mG, Pcol(i - 1), cg_nface, cg_coef));
+        C.sv3(mG, (const double*)Pcol(i - 1), MUc(iB - 1));
+        launch(k_sub<double, double, double>, grid_for(nv, 256), 256, 0, s, (const double*)L->Rm.p,
+               (const double*)MUc(iB - 1), MUc(iBB - 1), nv);
+        CR_CHECK((gmres<M, B>(C, ls->GM, mK, MUc(iBB - 1), Ucol(i - 1))));
+        C.vv3(mK, (const double*)Ucol(i - 1), MUc(iBB - 1));
+        C.addbcmul(0, 3, (const double*)Ucol(i - 1), MUc(iBB - 1));
+        C.ss(mL, (const double*)Pcol(i - 1), MPc(iB - 1));
+        C.vs3(mD, (const double*)Ucol(i - 1), MPc(iBB - 1));
         // Gram matrix entries for columns iB, iBB
         int slot = kSlotGram;
         for (int k = iB; k <= iBB; ++k) {
             for (int j = 1; j <= k - 1; ++j) {
-                C.dot(MUc(j - 1), MUc(k - 1), nv, slot++);
-                C.dot(MPc(j - 1), MPc(k - 1), nNo, slot++);
+                C.dot((const double*)MUc(j - 1), (const double*)MUc(k - 1), nv, slot++);
+                C.dot((const double*)MPc(j - 1), (const double*)MPc(k - 1), nNo, slot++);
             }
-            C.dot(MUc(k - 1), MUc(k - 1), nv, slot++);
-            C.dot(MPc(k - 1), MPc(k - 1), nNo, slot++);
-            C.dot(MUc(k - 1), L->Rmi.p, nv, slot++);
-            C.dot(MPc(k - 1), L->Rci.p, nNo, slot++);
+            C.dot((const double*)MUc(k - 1), (const double*)MUc(k - 1), nv, slot++);
+            C.dot((const double*)MPc(k - 1), (const double*)MPc(k - 1), nNo, slot++);
+            C.dot((const double*)MUc(k - 1), (const double*)L->Rmi.p, nv, slot++);
+            C.dot((const double*)MPc(k - 1), (const double*)L->Rci.p, nNo, slot++);
         }
         CR_CHECK(C.sync_scal(kSlotGram, slot - kSlotGram));
         slot = kSlotGram;
@@ -822,16 +1134,16 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
             }
             Aa(k - 1, k - 1) = std::pow(std::sqrt(L->hscal[slot]), 2.0) + std::pow(std::sqrt(L->hscal[slot + 1]), 2.0);
             slot += 2;
-            B[k - 1] = L->hscal[slot] + L->hscal[slot + 1];
+            Bv[k - 1] = L->hscal[slot] + L->hscal[slot + 1];
             slot += 2;
         }
-        for (int t = 0; t < iBB; ++t) xB[t] = B[t];
+        for (int t = 0; t < iBB; ++t) xB[t] = Bv[t];
         std::vector<double> Asub((size_t)iBB * iBB);
         for (int c = 0; c < iBB; ++c)
             for (int r = 0; r < iBB; ++r) Asub[(size_t)c * iBB + r] = Aa(r, c);
         CR_CHECK(ge_solve(iBB, Asub.data(), xB.data()));
         double sxb = 0.0;
-        for (int t = 0; t < iBB; ++t) sxb = sxb + xB[t] * B[t];
+        for (int t = 0; t < iBB; ++t) sxb = sxb + xB[t] * Bv[t];
         ls->RI.fNorm = std::sqrt(std::pow(ls->RI.iNorm, 2.0) - sxb);
         if (ls->RI.fNorm < eps) {
             ls->RI.suc = 1;
@@ -841,8 +1153,10 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
         CR_CUDA(cudaMemcpyAsync(L->Rm.p, L->Rmi.p, sizeof(double) * nv, cudaMemcpyDeviceToDevice, s));
         CR_CUDA(cudaMemcpyAsync(L->Rc.p, L->Rci.p, sizeof(double) * nNo, cudaMemcpyDeviceToDevice, s));
         for (int j = 1; j <= iBB; ++j) {
-            launch(k_axpy, grid_for(nv, 256), 256, 0, s, -xB[j - 1], MUc(j - 1), L->Rm.p, nv);
-            launch(k_axpy, grid_for(nNo, 256), 256, 0, s, -xB[j - 1], MPc(j - 1), L->Rc.p, nNo);
+            launch(k_axpy<double, double>, grid_for(nv, 256), 256, 0, s, -xB[j - 1], (const double*)MUc(j - 1),
+                   L->Rm.p, nv);
+            launch(k_axpy<double, double>, grid_for(nNo, 256), 256, 0, s, -xB[j - 1], (const double*)MPc(j - 1),
+                   L->Rc.p, (long long)nNo);
         }
     }
     if (i > ls->RI.mItr) {
@@ -850,22 +1164,27 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
     } else {
         ls->RI.itr = i;
         CR_CUDA(cudaMemcpyAsync(L->Rc.p, L->Rci.p, sizeof(double) * nNo, cudaMemcpyDeviceToDevice, s));
-        for (int j = 1; j <= iBB; ++j) launch(k_axpy, grid_for(nNo, 256), 256, 0, s, -xB[j - 1], MPc(j - 1), L->Rc.p, nNo);
+        for (int j = 1; j <= iBB; ++j)
+            launch(k_axpy<double, double>, grid_for(nNo, 256), 256, 0, s, -xB[j - 1], (const double*)MPc(j - 1),
+                   L->Rc.p, (long long)nNo);
     }
-    C.dot(L->Rc.p, L->Rc.p, nNo, 0);
+    C.dot((const double*)L->Rc.p, (const double*)L->Rc.p, nNo, 0);
     CR_CHECK(C.sync_scal(0, 1));
     ls->Resc = (int)std::lround(100.0 * std::pow(std::sqrt(L->hscal[0]) / ls->RI.fNorm, 2.0));
     ls->Resm = 100 - ls->Resc;
     // solution: Rmi = xB(2) U_1 + sum xB(2i) U_i ; Rci = xB(1) P_1 + sum xB(2i-1) P_i
     CR_CUDA(cudaMemsetAsync(L->Rmi.p, 0, sizeof(double) * nv, s));
     CR_CUDA(cudaMemsetAsync(L->Rci.p, 0, sizeof(double) * nNo, s));
-    launch(k_axpy, grid_for(nv, 256), 256, 0, s, xB[1], Ucol(0), L->Rmi.p, nv);
-    launch(k_axpy, grid_for(nNo, 256), 256, 0, s, xB[0], Pcol(0), L->Rci.p, nNo);
+    launch(k_axpy<double, double>, grid_for(nv, 256), 256, 0, s, xB[1], (const double*)Ucol(0), L->Rmi.p, nv);
+    launch(k_axpy<double, double>, grid_for(nNo, 256), 256, 0, s, xB[0], (const double*)Pcol(0), L->Rci.p,
+           (long long)nNo);
     for (i = 2; i <= ls->RI.itr; ++i) {
-        launch(k_axpy, grid_for(nv, 256), 256, 0, s, xB[2 * i - 1], Ucol(i - 1), L->Rmi.p, nv);
-        launch(k_axpy, grid_for(nNo, 256), 256, 0, s, xB[2 * i - 2], Pcol(i - 1), L->Rci.p, nNo);
+        launch(k_axpy<double, double>, grid_for(nv, 256), 256, 0, s, xB[2 * i - 1], (const double*)Ucol(i - 1),
+               L->Rmi.p, nv);
+        launch(k_axpy<double, double>, grid_for(nNo, 256), 256, 0, s, xB[2 * i - 2], (const double*)Pcol(i - 1),
+               L->Rci.p, (long long)nNo);
     }
-    launch(k_merge4, grid_for(nNo, 256), 256, 0, s, R, L->Rmi.p, L->Rci.p, nNo);
+    launch(k_merge4, grid_for(nNo, 256), 256, 0, s, R, (const double*)L->Rmi.p, (const double*)L->Rci.p, nNo);
     CR_CUDA(cudaStreamSynchronize(s));
     ls->RI.callD = now_s() - t0;
     ls->RI.dB = 10.0 * std::log(ls->RI.fNorm / ls->RI.dB);
@@ -878,6 +1197,7 @@ static int lhs_work_alloc(crimson_lhs* L, const crimson_ls* ls) {
     const long long nnz = L->nnz;
     const int iB = ls->RI.mItr;
     const int sD = ls->GM.sD;
+    if (sD + 1 > 512 || 8 * iB * iB + 64 > 4096) return CRIMSON_ERR_UNSUPPORTED;
     CR_CHECK(L->W.alloc(4 * (size_t)nNo));
     CR_CHECK(L->R.alloc(4 * (size_t)nNo));
     CR_CHECK(L->mK.alloc(9 * (size_t)nnz));
@@ -895,15 +1215,14 @@ static int lhs_work_alloc(crimson_lhs* L, const crimson_ls* ls) {
     CR_CHECK(L->basis.alloc(3 * (size_t)nNo * (sD + 1)));
     CR_CHECK(L->w3.alloc(3 * (size_t)nNo));
     CR_CHECK(L->cgX.alloc((size_t)nNo));
-    CR_CHECK(L->cgP.alloc((size_t)nNo));
     CR_CHECK(L->cgSP.alloc((size_t)nNo));
-    CR_CHECK(L->cgGP.alloc(3 * (size_t)nNo));
     if (!L->scal.p) {
         CR_CHECK(L->scal.alloc(kScalTotal));
         CR_CHECK(L->red.init());
         CR_CUDA(cudaMallocHost(&L->hscal, sizeof(double) * kScalTotal));
+        CR_CUDA(cudaEventCreate(&L->ev0));
+        CR_CUDA(cudaEventCreate(&L->ev1));
     }
-    if (sD + 1 > 512 || iB * 8 * iB + 64 > 4096) return CRIMSON_ERR_UNSUPPORTED;
     return CRIMSON_OK;
 }
 
@@ -928,14 +1247,139 @@ static int precond_faces(crimson_lhs* L, bool after_scale) {
         if (!f.created || f.nNo == 0) continue;
         if (!after_scale) {
             if (f.incFlag && f.bGrp == CRIMSON_BC_TYPE_DIR)
-                launch(k_w_dirichlet, grid_for(f.nNo, 256), 256, 0, s, f.glob.p, f.val.p, f.dof, std::min(f.dof, 4), f.nNo,
-                                                                   L->W.p);
+                launch(k_w_dirichlet, grid_for(f.nNo, 256), 256, 0, s, f.glob.p, f.val.p, f.dof, std::min(f.dof, 4),
+                       f.nNo, L->W.p);
         } else if (f.coupledFlag) {
-            launch(k_valm, grid_for(f.nNo, 256), 256, 0, s, f.glob.p, f.val.p, f.valM.p, f.dof, std::min(f.dof, 4), f.nNo,
-                                                        L->W.p);
+            launch(k_valm, grid_for(f.nNo, 256), 256, 0, s, f.glob.p, f.val.p, f.valM.p, f.dof, std::min(f.dof, 4),
+                   f.nNo, L->W.p);
         }
     }
     CR_CUDA(cudaGetLastError());
+    return CRIMSON_OK;
+}
+
+static void copy_stats(const crimson_ls* ls, crimson_ls_stats* st) {
+    if (!st) return;
+    st->GM = ls->GM;
+    st->CG = ls->CG;
+    st->RI = ls->RI;
+    st->LS_type = ls->LS_type;
+    st->Resm = ls->Resm;
+    st->Resc = ls->Resc;
+}
+
+// FP64 defect of the scaled system: D4 = R0 - A x (A with the coupled-face
+// momentum term of ADDBCMUL(ADD)); returns |D4| and |R0|.
+static int defect64(crimson_lhs* L, const double* R0, const double* x4, double* D4, double* nD, double* nR) {
+    Ctx C{L, L->stream};
+    cudaStream_t s = L->stream;
+    const int n = L->nNo;
+    // x split into xu (3, n) in Rmi and xp (n) in Rci; products into MU/MP slots 0
+    launch(k_split4, grid_for(n, 256), 256, 0, s, x4, L->Rmi.p, L->Rci.p, n);
+    double* KU = L->MU.p;
+    double* GPm = L->MU.p + 3 * (size_t)n;
+    double* DU = L->MP.p;
+    double* LP = L->MP.p + (size_t)n;
+    C.vv3((const double*)L->mK.p, (const double*)L->Rmi.p, KU);
+    C.addbcmul(0, 3, (const double*)L->Rmi.p, KU);
+    C.sv3((const double*)L->mG.p, (const double*)L->Rci.p, GPm);
+    C.vs3((const double*)L->mD.p, (const double*)L->Rmi.p, DU);
+    C.ss((const double*)L->mL.p, (const double*)L->Rci.p, LP);
+    launch(k_defect4, grid_for(n, 256), 256, 0, s, R0, (const double*)KU, (const double*)GPm, (const double*)DU,
+           (const double*)LP, D4, n);
+    C.dot(D4, (const double*)D4, 4LL * n, 0);
+    C.dot(R0, R0, 4LL * n, 1);
+    CR_CHECK(C.sync_scal(0, 2));
+    *nD = std::sqrt(L->hscal[0]);
+    *nR = std::sqrt(L->hscal[1]);
+    return CRIMSON_OK;
+}
+
+// NSSOLVER on the scaled system in L->R (in/out).  FP64: the reference's
+// arithmetic.  Mixed: FP32 copies of the scaled split matrices drive every
+// inner matvec; each sweep solves A d = D in FP32-matrix arithmetic, adds d
+// to the FP64 solution and forms the FP64 defect D = R0 - A x, until
+// |D| <= refine_tol |R0| (RI.relTol when refine_tol <= 0) or max_refine
+// sweeps.  Every sweep's NSSOLVER stops at its own relative tolerances, so
+// the sweeps reach a defect below what one NSSOLVER's estimate can resolve.  Iteration counts are summed
+// over the sweeps.  has_gt: Gt is a separate matrix (host Val path),
+// otherwise mD serves as Gt.
+static int solve_scaled(crimson_lhs* L, crimson_ls* ls, bool has_gt) {
+    cudaStream_t s = L->stream;
+    const double* Gt64 = has_gt ? L->Gt.p : L->mD.p;
+    if (ls->precision == CRIMSON_FP64)
+        return nssolver<double, double>(L, ls, L->mK.p, L->mG.p, L->mD.p, L->mL.p, Gt64, L->R.p);
+    const long long nnz = L->nnz;
+    const int n = L->nNo;
+    CR_CHECK(L->mK32.alloc(9 * (size_t)nnz));
+    CR_CHECK(L->mG32.alloc(3 * (size_t)nnz));
+    CR_CHECK(L->mD32.alloc(3 * (size_t)nnz));
+    CR_CHECK(L->mL32.alloc((size_t)nnz));
+    if (has_gt) CR_CHECK(L->Gt32.alloc(3 * (size_t)nnz));
+    CR_CHECK(L->R0.alloc(4 * (size_t)n));
+    CR_CHECK(L->X4.alloc(4 * (size_t)n));
+    launch(k_convert<float, double>, grid_for(9 * nnz, 256), 256, 0, s, (const double*)L->mK.p, L->mK32.p, 9 * nnz);
+    launch(k_convert<float, double>, grid_for(3 * nnz, 256), 256, 0, s, (const double*)L->mG.p, L->mG32.p, 3 * nnz);
+    launch(k_convert<float, double>, grid_for(3 * nnz, 256), 256, 0, s, (const double*)L->mD.p, L->mD32.p, 3 * nnz);
+    launch(k_convert<float, double>, grid_for(nnz, 256), 256, 0, s, (const double*)L->mL.p, L->mL32.p, nnz);
+    if (has_gt)
+        launch(k_convert<float, double>, grid_for(3 * nnz, 256), 256, 0, s, (const double*)L->Gt.p, L->Gt32.p,
+               3 * nnz);
+    const float* Gt32 = has_gt ? L->Gt32.p : L->mD32.p;
+    CR_CUDA(cudaMemcpyAsync(L->R0.p, L->R.p, sizeof(double) * 4 * (size_t)n, cudaMemcpyDeviceToDevice, s));
+    CR_CUDA(cudaMemsetAsync(L->X4.p, 0, sizeof(double) * 4 * (size_t)n, s));
+    crimson_subls gm{}, cg{}, ri{};
+    const double tol = ls->refine_tol > 0.0 ? ls->refine_tol : ls->RI.relTol;
+    double rel = 1.0;
+    L->refine_steps = 0;
+    // Each sweep solves for the defect scaled to the norm of the original
+    // right side, so the Krylov solvers' absolute tolerances and GE's
+    // absolute pivot test see the same magnitudes in every sweep.  A later
+    // sweep only has to bring the defect from nD to tol nR: its outer
+    // relative tolerance is kRefineSafety * tol nR / nD (never tighter than
+    // the first sweep's), so it stops after the reduction it needs.
+    constexpr double kRefineSafety = 0.3;
+    struct RelTolGuard {
+        crimson_subls& ri;
+        double v;
+        ~RelTolGuard() { ri.relTol = v; }
+    } guard{ls->RI, ls->RI.relTol};
+    double sigma = 1.0;
+    for (int ref = 0; ref < std::max(ls->max_refine, 1); ++ref) {
+        CR_CHECK((nssolver<float, float>(L, ls, L->mK32.p, L->mG32.p, L->mD32.p, L->mL32.p, Gt32, L->R.p)));
+        if (ref == 0) {
+            gm = ls->GM;
+            cg = ls->CG;
+            ri = ls->RI;
+        } else {
+            gm.itr += ls->GM.itr;
+            cg.itr += ls->CG.itr;
+            ri.itr += ls->RI.itr;
+            gm.callD += ls->GM.callD;
+            cg.callD += ls->CG.callD;
+            ri.callD += ls->RI.callD;
+        }
+        launch(k_axpy<double, double>, grid_for(4LL * n, 256), 256, 0, s, 1.0 / sigma, (const double*)L->R.p,
+               L->X4.p, 4LL * n);
+        double nD = 0.0, nR = 0.0;
+        CR_CHECK(defect64(L, L->R0.p, L->X4.p, L->R.p, &nD, &nR));
+        rel = nR > 0.0 ? nD / nR : 0.0;
+        L->refine_steps = ref + 1;
+        L->refine_rel = rel;
+        if (!(rel > tol) || nD == 0.0) break;
+        if (!std::isfinite(rel)) return CRIMSON_ERR_NONFINITE;
+        sigma = nR / nD;
+        launch(k_scale, grid_for(4LL * n, 256), 256, 0, s, sigma, L->R.p, 4LL * n);
+        ls->RI.relTol = std::min(0.5, std::max(guard.v, kRefineSafety * tol / rel));
+    }
+    ls->RI.relTol = guard.v;
+    ri.relTol = guard.v;
+    ri.fNorm = rel * ri.iNorm;
+    ri.suc = rel <= tol ? 1 : 0;
+    ls->GM = gm;
+    ls->CG = cg;
+    ls->RI = ri;
+    CR_CUDA(cudaMemcpyAsync(L->R.p, L->X4.p, sizeof(double) * 4 * (size_t)n, cudaMemcpyDeviceToDevice, s));
     return CRIMSON_OK;
 }
 
@@ -950,24 +1394,17 @@ int memls_solve_val(crimson_lhs* L, crimson_ls* ls, double* Ri, double* Val, con
     CR_CUDA(cudaMemcpyAsync(L->Val.p, Val, sizeof(double) * 16 * (size_t)L->nnz, cudaMemcpyHostToDevice, s));
     launch(k_w_from_val, grid_for(L->nNo, 256), 256, 0, s, L->Val.p, L->diag, L->W.p, L->nNo);
     CR_CHECK(precond_faces(L, false));
-    launch(k_scale_split_val, grid_for(L->nNo, 128), 128, 0, s, L->Val.p, L->rowptr, L->col, L->diag, L->trans, L->W.p,
-                                                           L->nNo, L->mK.p, L->mG.p, L->mD.p, L->mL.p);
-    launch(k_gt, grid_for(L->nnz, 256), 256, 0, s, L->mG.p, L->trans, L->nnz, L->Gt.p);
-    launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, L->W.p, 4LL * L->nNo);
+    launch(k_scale_split_val, grid_for(L->nNo, 128), 128, 0, s, L->Val.p, L->rowptr, L->col, L->diag,
+           (const double*)L->W.p, L->nNo, L->mK.p, L->mG.p, L->mD.p, L->mL.p);
+    launch(k_gt, grid_for(L->nnz, 256), 256, 0, s, (const double*)L->mG.p, L->trans, L->nnz, L->Gt.p);
+    launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, (const double*)L->W.p, 4LL * L->nNo);
     CR_CHECK(precond_faces(L, true));
-    CR_CHECK(nssolver(L, ls, L->mK.p, L->mG.p, L->mD.p, L->mL.p, L->Gt.p, L->R.p));
-    launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, L->W.p, 4LL * L->nNo);
+    CR_CHECK(solve_scaled(L, ls, true));
+    launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, (const double*)L->W.p, 4LL * L->nNo);
     CR_CUDA(cudaMemcpyAsync(Ri, L->R.p, sizeof(double) * 4 * (size_t)L->nNo, cudaMemcpyDeviceToHost, s));
     CR_CUDA(cudaMemcpyAsync(Val, L->Val.p, sizeof(double) * 16 * (size_t)L->nnz, cudaMemcpyDeviceToHost, s));
     CR_CUDA(cudaStreamSynchronize(s));
-    if (st) {
-        st->GM = ls->GM;
-        st->CG = ls->CG;
-        st->RI = ls->RI;
-        st->LS_type = ls->LS_type;
-        st->Resm = ls->Resm;
-        st->Resc = ls->Resc;
-    }
+    copy_stats(ls, st);
     return CRIMSON_OK;
 }
 
@@ -981,34 +1418,33 @@ int memls_solve_lhs_device(crimson_lhs* L, crimson_ls* ls, const double* d_res, 
     launch(k_w_from_lhs, grid_for(L->nNo, 256), 256, 0, s, d_lhsK, d_lhsP, L->diag, L->W.p, L->nNo);
     CR_CHECK(precond_faces(L, false));
     launch(k_scale_split_lhs, grid_for(L->nNo, 128), 128, 0, s, d_lhsK, d_lhsP, L->rowptr, L->col, L->diag, L->trans,
-                                                           L->W.p, L->nNo, L->mK.p, L->mG.p, L->mD.p, L->mL.p);
-    launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, L->W.p, 4LL * L->nNo);
+           (const double*)L->W.p, L->nNo, L->mK.p, L->mG.p, L->mD.p, L->mL.p);
+    launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, (const double*)L->W.p, 4LL * L->nNo);
     CR_CHECK(precond_faces(L, true));
     // With Val4 built from lhsK/lhsP, Gt = -mG^T equals mD up to the order of
     // the two scaling products, so mD serves as Gt.
-    CR_CHECK(nssolver(L, ls, L->mK.p, L->mG.p, L->mD.p, L->mL.p, L->mD.p, L->R.p));
-    launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, L->W.p, 4LL * L->nNo);
+    CR_CHECK(solve_scaled(L, ls, false));
+    launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, (const double*)L->W.p, 4LL * L->nNo);
     CR_CUDA(cudaMemcpyAsync(d_sol, L->R.p, sizeof(double) * 4 * (size_t)L->nNo, cudaMemcpyDeviceToDevice, s));
     CR_CUDA(cudaStreamSynchronize(s));
-    if (st) {
-        st->GM = ls->GM;
-        st->CG = ls->CG;
-        st->RI = ls->RI;
-        st->LS_type = ls->LS_type;
-        st->Resm = ls->Resm;
-        st->Resc = ls->Resc;
-    }
+    copy_stats(ls, st);
     return CRIMSON_OK;
 }
 
-}  // namespace crimson
-
-namespace crimson {
-
-// Average device time of one launch of a memLS kernel on the lhs's current
-// split matrices (events recorded on the lhs stream around reps launches).
+// Diagnostics.  which: 0 = 3x3 block SpMV (K), 1 = one CG iteration of the
+// persistent FP64 CGRAD kernel (average over all launches so far, from CUDA
+// events recorded around each launch), 2 = SPARMULSV (G), 3 = fused MGS step,
+// 4 = one CG iteration of the FP32-matrix CGRAD kernel, 5 = 3x3 block SpMV
+// with FP32 K.
 int memls_kernel_time(crimson_lhs* L, int which, int reps, double* ms) {
+    if (which == 1 || which == 4) {
+        const auto& acc = which == 1 ? L->cg_acc64 : L->cg_acc32;
+        if (acc.iters <= 0) return CRIMSON_ERR_STATE;
+        *ms = acc.ms / (double)acc.iters;
+        return CRIMSON_OK;
+    }
     if (!L->mK.p || !L->basis.p || reps <= 0) return CRIMSON_ERR_STATE;
+    if (which == 5 && !L->mK32.p) return CRIMSON_ERR_STATE;
     cudaStream_t s = L->stream;
     Ctx C{L, s};
     const long long n3 = 3LL * L->nNo;
@@ -1017,15 +1453,13 @@ int memls_kernel_time(crimson_lhs* L, int which, int reps, double* ms) {
     CR_CUDA(cudaEventCreate(&e1));
     auto run = [&]() {
         switch (which) {
-            case 0: C.spmv_vv3(L->mK.p, L->basis.p, L->basis.p + n3); break;
-            case 1:
-                launch(k_cg_op, red_grid((long long)L->nNo * kLanes), 256, 0, s, L->rowptr, L->col, L->mL.p, L->mD.p,
-                       L->cgP.p, L->cgGP.p, L->cgSP.p, L->nNo, L->red.part.p, L->red.ticket.p, C.sc(kSlotDen));
-                break;
-            case 2: C.spmv_sv3(L->mG.p, L->cgP.p, L->cgGP.p); break;
+            case 0: C.vv3((const double*)L->mK.p, (const double*)L->basis.p, L->basis.p + n3); break;
+            case 2: C.sv3((const double*)L->mG.p, (const double*)L->cgX.p, L->w3.p); break;
+            case 5: C.vv3((const float*)L->mK32.p, (const double*)L->basis.p, L->basis.p + n3); break;
             default:
-                launch(k_mgs, red_grid(n3), 256, 0, s, L->basis.p + 2 * n3, L->basis.p, C.sc(kSlotH),
-                       L->basis.p + n3, n3, L->red.part.p, L->red.ticket.p, C.sc(kSlotH + 1));
+                launch(k_mgs<double>, red_grid(n3), 256, 0, s, L->basis.p + 2 * n3, (const double*)L->basis.p,
+                       (const double*)C.sc(kSlotH), (const double*)(L->basis.p + n3), n3, L->red.part.p,
+                       L->red.ticket.p, C.sc(kSlotH + 1));
         }
     };
     for (int i = 0; i < 2; ++i) run();

@@ -48,7 +48,23 @@ struct crimson_lhs {
     // work space
     DBuf<double> W, R, Val, mK, mG, mD, mL, Gt;
     DBuf<double> Rm, Rc, Rmi, Rci, U, P, MU, MP, X3, basis, w3;
-    DBuf<double> cgX, cgP, cgSP, cgGP, cgR;
+    DBuf<double> cgX, cgP, cgSP, cgGP, cgR, cgP2;
+    DBuf<double> cgW, cgZ, cgExt;     // coupled-face vectors w = G^T valM, z = Gt valM (per face)
+    DBuf<double> cgPart;              // persistent CG partial sums (3 regions)
+    DBuf<double> cgGL, cgRecA, cgRecB; // packed {Gt, L} blocks; {R, P} and {GP, P} node records
+    int cg_grid = 0, cg_grid32 = 0;
+    // mixed precision: FP32 copies of the scaled split matrices; FP64 right
+    // side and accumulated solution of the iterative refinement
+    DBuf<float> mK32, mG32, mD32, mL32, Gt32;
+    DBuf<double> R0, X4;
+    int refine_steps = 0;
+    double refine_rel = 0.0;
+    // CUDA-event time of the persistent CG launches (per matrix precision)
+    struct CgAcc {
+        double ms = 0.0;
+        long long iters = 0, launches = 0;
+    } cg_acc64, cg_acc32;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DBuf<double> scal;      // device scalars
     RedScratch red;
     double* hscal = nullptr;   // pinned host mirror of scal
@@ -58,5 +74,8 @@ struct crimson_lhs {
 struct crimson_ls {
     crimson_subls GM{}, CG{}, RI{};
     int LS_type = CRIMSON_LS_TYPE_NS, Resm = 0, Resc = 0;
+    int precision = CRIMSON_FP64;  // CRIMSON_FP64 or CRIMSON_MIXED
+    int max_refine = 4;            // FP64 refinement sweeps of the mixed solve
+    double refine_tol = 0.0;       // target |R - A x| / |R|; <= 0: RI.relTol
 };
 

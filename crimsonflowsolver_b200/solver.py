@@ -24,6 +24,9 @@ from . import _native as N
 from .problem import FlowParams
 
 
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+
 def make_params(P: FlowParams) -> N.Params:
     return N.Params(rho=P.rho, mu=P.mu, alfi=P.alfi, almi=P.almi, gami=P.gami, Delt=P.Delt, Dtgl=1.0 / P.Delt,
                     dtsfct=P.dtsfct, taucfct=P.taucfct, flmpl=0.0, flmpr=0.0, stabflux_coeff=P.stabflux_coeff,
@@ -153,6 +156,12 @@ class MemLS:
         N.check(L.crimson_memls_ls_create(ctypes.byref(ls), 3, 1 | 4 | 8 | 16 | 64, P.epstol_ns, 0.0, P.nprjs,
                                           P.kspace, N.dp(rin), N.dp(ain), N.ip(mit)), "crimson_memls_ls_create")
         self.ls = ls
+        if P.precision not in PRECISIONS:
+            L.crimson_memls_ls_free(ls)
+            self.ls = None
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, got {P.precision!r}")
+        N.check(L.crimson_memls_ls_set_precision(ls, PRECISIONS[P.precision], P.max_refine, P.refine_tol),
+                "crimson_memls_ls_set_precision")
         lhs = ctypes.c_void_p()
         self._ctx = ctx   # an lhs made from a context must be freed before it
         if ctx is not None:
@@ -194,6 +203,14 @@ class MemLS:
                                                d_lhsP.data_ptr(), N.ip(inc), N.dp(fr), d_sol.data_ptr(),
                                                ctypes.byref(st)), "crimson_solflow_device")
         return st
+
+    def refine_info(self):
+        """(sweeps, relative FP64 defect) of the last mixed-precision solve."""
+        steps = ctypes.c_int()
+        rel = ctypes.c_double()
+        N.check(N.lib().crimson_memls_refine_info(self.lhs, ctypes.byref(steps), ctypes.byref(rel)),
+                "crimson_memls_refine_info")
+        return steps.value, rel.value
 
     def close(self) -> None:
         L = N.lib()

@@ -139,6 +139,18 @@ int crimson_memls_ls_create(crimson_ls** ls, int LS_type, int present_mask, doub
                             int maxItr, int dimKry, const double* relTolIn, const double* absTolIn,
                             const int* maxItrIn);
 int crimson_memls_ls_free(crimson_ls* ls);
+/* Arithmetic of the NS solve; no counterpart in the reference (memLS is FP64
+ * throughout).  CRIMSON_FP64 (default): memLS's arithmetic.  CRIMSON_MIXED:
+ * FP32 copies of the scaled block matrices in every inner Krylov matvec and an
+ * FP32 GMRES basis; FP64 outer vectors, dot products, Givens rotations, Gram
+ * system and CG recurrences; FP64 iterative refinement on the defect
+ * R - A x until |R - A x| <= refine_tol |R| (relTol of memLS_LS_CREATE when
+ * refine_tol <= 0) or max_refine sweeps (1..64).
+ * Applies to crimson_memls_solve, crimson_solflow_device and crimson_step. */
+int crimson_memls_ls_set_precision(crimson_ls* ls, int precision, int max_refine, double refine_tol);
+/* Refinement sweeps taken by the last mixed solve on lhs and its final
+ * relative FP64 defect |R - A x| / |R| (scaled system). */
+int crimson_memls_refine_info(const crimson_lhs* lhs, int* steps, double* rel);
 /* memLS_LHS_CREATE(lhs, commu, gnNo, nNo, nnz, gNodes, rowPtr, colPtr, nFaces)
  * -- flowsolver/src/memLS.f90:1080 (single task; rowPtr = colm, colPtr = rowp) */
 int crimson_memls_lhs_create(crimson_lhs** lhs, int gnNo, int nNo, long long nnz, const int* gNodes,
@@ -182,6 +194,8 @@ typedef struct {
     int ri_itr[16], gm_itr[16], cg_itr[16];
     double ri_inorm[16], ri_fnorm[16];
     double q_out[8], p_out[8];   /* outlet flow and pressure at t_{n+1} */
+    int refine_steps[16];        /* mixed precision: refinement sweeps per solve */
+    double refine_rel[16];       /* mixed precision: final |R - A x| / |R| per solve */
 } crimson_step_stats;
 
 /* register the inlet profile: BC(node, 3:5) = profile * inflow_scale */
@@ -222,8 +236,11 @@ int crimson_pvsq_noalloc(int nsurf, const int* surf_offsets, const int* d_nodes,
 
 /* Diagnostics: average device time (ms) of one launch of a memLS kernel on the
  * lhs's current split matrices, timed with CUDA events on the lhs stream.
- * which: 0 = 3x3 block SpMV (SPARMULVV, K), 1 = fused CG operator
- * (SPARMULSS L + SPARMULVS Gt + DOTS), 2 = SPARMULSV (G), 3 = fused MGS step.
+ * which: 0 = 3x3 block SpMV (SPARMULVV, K), 2 = SPARMULSV (G), 3 = fused MGS
+ * step, 5 = 3x3 block SpMV with the FP32 copy of K (after a mixed solve).
+ * which 1 / 4: time of one CGRAD iteration of the persistent CG kernel with
+ * FP64 / FP32 matrices, averaged over every launch on this lhs so far (CUDA
+ * events recorded around each cooperative launch; reps is ignored).
  * Valid after a solve on the lhs. */
 int crimson_memls_kernel_time(crimson_lhs* lhs, int which, int reps, double* ms);
 
