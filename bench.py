@@ -318,6 +318,7 @@ def run_ours(args):
     kt = {}
     for lhs, which, name in ((FM.memls.lhs, 4, "cg_iter_f32"), (F64.memls.lhs, 1, "cg_iter_f64"),
                              (FM.memls.lhs, 5, "spmv_K_f32"), (F64.memls.lhs, 0, "spmv_K_f64"),
+                             (F64.memls.lhs, 6, "spmv_K_f64_csr"),
                              (F64.memls.lhs, 2, "spmv_G_f64"), (F64.memls.lhs, 3, "mgs_f64")):
         ms = ctypes.c_double()
         rc = L.crimson_memls_kernel_time(lhs, which, 20, ctypes.byref(ms))

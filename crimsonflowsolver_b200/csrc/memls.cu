@@ -55,11 +55,6 @@ __device__ __forceinline__ double4 ldg4(const double4* p) {
     return make_double4(lo.x, lo.y, hi.x, hi.y);
 }
 __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
-__device__ __forceinline__ double4 ldcg4(const double4* p) {
-    const double2 lo = __ldcg(reinterpret_cast<const double2*>(p));
-    const double2 hi = __ldcg(reinterpret_cast<const double2*>(p) + 1);
-    return make_double4(lo.x, lo.y, hi.x, hi.y);
-}
 template <typename T>
 __device__ __forceinline__ typename V4<T>::type mk4(T a, T b, T c, T d);
 template <>
@@ -337,6 +332,114 @@ __global__ void __launch_bounds__(256) k_spmv_vs3_trans(const int* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
+// Sliced ELL copy of the pattern for the SpMVs inside the Krylov loops
+// (GMRES's K products and the CG's G / {Gt, L} products).
+// Rows are grouped in slices of 32 (one warp); a slice is stored column by
+// column with width w = its longest row, so position of entry k of row r is
+// sp[r / 32] + r % 32 + 32 k.  One thread per row: every load of column
+// indices and matrix values is a fully coalesced 128-byte warp access, with
+// no row-pointer -> column dependency; entries are summed in CSR order.
+// Padding entries carry zero values and a valid column (the row itself;
+// 0 for the rows past n of the last slice), so they add exactly +0.
+// K is stored per component (structure of arrays, stride npad); the CG's
+// operands as one 4-vector per entry: {G0, G1, G2, column} (one load gives
+// the column and the values) and {Gt0, Gt1, Gt2, L}.  Converted once per NSSOLVER call,
+// read ~10^3 times.
+// ---------------------------------------------------------------------------
+constexpr int kSlice = 32;
+constexpr int kSellUnroll = 8;
+
+// Visit the entries of row r, U at a time: pos (size_t) and c (int) defined
+// for the body.
+#define CR_SELL_ROW_U(U, sp, scol, r, ...)                                              \
+    {                                                                                    \
+        const int s_ = (r) >> 5;                                                         \
+        const int p0_ = __ldg((sp) + s_);                                                \
+        const int w_ = (__ldg((sp) + s_ + 1) - p0_) >> 5;                                \
+        const int base_ = p0_ + ((r) & (kSlice - 1));                                    \
+        for (int k0_ = 0; k0_ < w_; k0_ += (U)) {                                        \
+            int cc_[(U)];                                                                \
+            _Pragma("unroll") for (int u_ = 0; u_ < (U); ++u_) cc_[u_] =                 \
+                (k0_ + u_ < w_) ? __ldg((scol) + base_ + kSlice * (k0_ + u_)) : 0;       \
+            _Pragma("unroll") for (int u_ = 0; u_ < (U); ++u_) {                         \
+                if (k0_ + u_ < w_) {                                                     \
+                    const size_t pos = (size_t)base_ + (size_t)kSlice * (k0_ + u_);      \
+                    const int c = cc_[u_];                                               \
+                    __VA_ARGS__                                                          \
+                }                                                                        \
+            }                                                                            \
+        }                                                                                \
+    }
+#define CR_SELL_ROW(sp, scol, r, ...) CR_SELL_ROW_U(kSellUnroll, sp, scol, r, __VA_ARGS__)
+constexpr int kCgUnroll = 4;
+
+// KU = K U on the sliced copy: K (9, npad), U / KU (3, n)
+template <typename M, typename IN, typename OUT>
+__global__ void __launch_bounds__(256) k_sell_vv3(const int* __restrict__ sp, const int* __restrict__ scol,
+                                                  const M* __restrict__ Ks, long long npad,
+                                                  const IN* __restrict__ U, OUT* __restrict__ KU, int n) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        CR_SELL_ROW(sp, scol, r, {
+            const IN* u = U + 3 * (size_t)c;
+            const double u0 = (double)__ldg(u), u1 = (double)__ldg(u + 1), u2 = (double)__ldg(u + 2);
+            const double k0 = (double)__ldg(Ks + pos), k1 = (double)__ldg(Ks + npad + pos),
+                         k2 = (double)__ldg(Ks + 2 * npad + pos), k3 = (double)__ldg(Ks + 3 * npad + pos),
+                         k4 = (double)__ldg(Ks + 4 * npad + pos), k5 = (double)__ldg(Ks + 5 * npad + pos),
+                         k6 = (double)__ldg(Ks + 6 * npad + pos), k7 = (double)__ldg(Ks + 7 * npad + pos),
+                         k8 = (double)__ldg(Ks + 8 * npad + pos);
+            a0 = a0 + k0 * u0 + k1 * u1 + k2 * u2;
+            a1 = a1 + k3 * u0 + k4 * u1 + k5 * u2;
+            a2 = a2 + k6 * u0 + k7 * u1 + k8 * u2;
+        })
+        KU[3 * (size_t)r + 0] = (OUT)a0;
+        KU[3 * (size_t)r + 1] = (OUT)a1;
+        KU[3 * (size_t)r + 2] = (OUT)a2;
+    }
+}
+
+// Column index of every sliced position (pads: the row, or 0 past n).
+__global__ void k_sell_cols(const int* __restrict__ rowptr, const int* __restrict__ col, const int* __restrict__ sp,
+                            int n, int nrows_pad, int* __restrict__ scol) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows_pad; r += gridDim.x * blockDim.x) {
+        const int s = r >> 5;
+        const int w = (sp[s + 1] - sp[s]) >> 5;
+        const int base = sp[s] + (r & (kSlice - 1));
+        const int rs = r < n ? rowptr[r] : 0;
+        const int len = r < n ? rowptr[r + 1] - rs : 0;
+        for (int k = 0; k < w; ++k) scol[base + kSlice * k] = k < len ? col[rs + k] : (r < n ? r : 0);
+    }
+}
+
+// Column index carried in the 4th component of a {G0, G1, G2, col} record
+// (bit pattern, never used in arithmetic).
+__device__ __forceinline__ double col_bits(int c, double) { return __hiloint2double(0, c); }
+__device__ __forceinline__ float col_bits(int c, float) { return __int_as_float(c); }
+__device__ __forceinline__ int bits_col(double w) { return __double2loint(w); }
+__device__ __forceinline__ int bits_col(float w) { return __float_as_int(w); }
+
+// Scaled split matrices (CSR, type M) -> sliced copies: K (9, npad),
+// {G0, G1, G2, col} (npad), {Gt0, Gt1, Gt2, L} (npad).
+template <typename M>
+__global__ void k_to_sell(const int* __restrict__ rowptr, const int* __restrict__ sp, int n, const M* __restrict__ mK,
+                          const M* __restrict__ mG, const M* __restrict__ Gt, const M* __restrict__ mL,
+                          long long npad, M* __restrict__ Ks, typename V4<M>::type* __restrict__ Gs,
+                          typename V4<M>::type* __restrict__ GLs, const int* __restrict__ col) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const size_t base = (size_t)sp[r >> 5] + (r & (kSlice - 1));
+        const int rs = rowptr[r], re = rowptr[r + 1];
+        for (int j = rs; j < re; ++j) {
+            const size_t pos = base + (size_t)kSlice * (j - rs);
+            const size_t jj = (size_t)j;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) Ks[q * npad + pos] = mK[9 * jj + q];
+            Gs[pos] = mk4<M>(mG[3 * jj], mG[3 * jj + 1], mG[3 * jj + 2], col_bits(col[jj], M(0)));
+            GLs[pos] = mk4<M>(Gt[3 * jj], Gt[3 * jj + 1], Gt[3 * jj + 2], mL[jj]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // CGRAD as one persistent cooperative kernel (memLS.f90:367-430).
 //
 // Per iteration three grid-wide barriers: (A) P = R + beta P formed on the
@@ -346,26 +449,35 @@ __global__ void __launch_bounds__(256) k_spmv_vs3_trans(const int* __restrict__ 
 // ADDBCMUL(PRE) is applied through the precomputed vectors w_f = G^T valM_f
 // and z_f = Gt valM_f: Gt (GP + coef valM (valM . GP)) = Gt GP + coef (w.P) z
 // -- exact.  Node records keep every gather to one aligned sector:
-// recA = {R, P_prev} (16 B) read in phase A, recB = {GP, P} (32 B) read in
-// phase B; matrix blocks GL = {Gt, L}.  Partial sums are written per block
+// recA = {R, P_prev} (16 B, FP64) read in phase A, recB = {GP, P} read in
+// phase B, stored in the matrix type M (32 B FP64 / 16 B FP32: with FP32
+// matrices the matvec operands are rounded to FP32 as the matrices are,
+// while P itself stays FP64 for the updates); matrix entries
+// {G0, G1, G2, column} and {Gt0, Gt1, Gt2, L}.  Partial sums are written per block
 // and summed in block order by every block after the barrier
-// (deterministic, identical in all blocks).  Values written by other blocks
-// earlier in the kernel are read with __ldcg (L2), never from a possibly
-// stale L1 line.  The loop is bounded by mItr.  Vectors and scalars are FP64
-// in both precisions; M is the storage type of G, Gt and L.
+// (deterministic, identical in all blocks).  Node records written by other
+// blocks in an earlier phase are read with ordinary (L1-cached) loads: the
+// grid barrier's acquire fence orders them after those writes, and the
+// neighbour gathers of one block hit the same lines many times, which keeps
+// them out of L2.  Only the matrix streams use the read-only path.  The loop
+// is bounded by mItr.  X, R, P, SP, the recurrences and all dot products
+// are FP64 in both precisions; M is the storage type of G, Gt, L and of
+// the gathered copy of {GP, P}.
 // ---------------------------------------------------------------------------
 constexpr int kMaxCoupled = 8;
 
 template <typename M>
 struct CgArgs {
-    const int* rowptr;
-    const int* col;
+    const int* sp;    // sliced pattern: slice offsets
+    const int* scol;  // sliced pattern: columns
+    long long npad;
     int n;
-    const M* G;                      // (3, nnz)
-    const typename V4<M>::type* GL;  // (nnz) {Gt0, Gt1, Gt2, L}
+    const typename V4<M>::type* G;   // sliced (npad) {G0, G1, G2, col}
+    const typename V4<M>::type* GL;  // sliced (npad) {Gt0, Gt1, Gt2, L}
     double* X;
     double2* recA;  // (n) {R, P of the previous iteration}
-    double4* recB;  // (n) {GP0, GP1, GP2, P}
+    typename V4<M>::type* recB;  // (n) {GP0, GP1, GP2, P} rounded to M: the gathered copy
+    double* Pd;                  // (n) P in FP64 for the updates
     double* SP;
     int nface;
     const double* w;  // (nface, n)
@@ -408,32 +520,35 @@ __global__ void __launch_bounds__(256, 4) k_cg_persistent(CgArgs<M> a) {
         double wp[NF > 0 ? NF : 1];
 #pragma unroll
         for (int f = 0; f < (NF > 0 ? NF : 1); ++f) wp[f] = 0.0;
-        {
-            CR_ROW_LOOP(n)
+        for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
             double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-            CR_ROW_BLOCKS(a.rowptr, a.col, {
-                const double2 rp = __ldcg(a.recA + c);
-                const double pc = first ? rp.x : rp.x + beta * rp.y;
-                const M* g = a.G + 3 * j;
-                const double g0 = (double)__ldg(g), g1 = (double)__ldg(g + 1), g2 = (double)__ldg(g + 2);
-                if (ok) {
-                    a0 += g0 * pc;
-                    a1 += g1 * pc;
-                    a2 += g2 * pc;
-                }
-            })
-            a0 = group_sum(a0);
-            a1 = group_sum(a1);
-            a2 = group_sum(a2);
-            if (rv && lane == 0) {
-                const double2 rr = __ldcg(a.recA + r);
-                const double pr = first ? rr.x : rr.x + beta * rr.y;
-                a.recB[r] = make_double4(a0, a1, a2, pr);
+            const int s_ = r >> 5;
+            const int p0 = __ldg(a.sp + s_);
+            const int w = (__ldg(a.sp + s_ + 1) - p0) >> 5;
+            const int base = p0 + (r & (kSlice - 1));
+            for (int k0 = 0; k0 < w; k0 += kCgUnroll) {
+                typename V4<M>::type g[kCgUnroll];
 #pragma unroll
-                for (int f = 0; f < NF; ++f)
-                    if (f < a.nface) wp[f] += a.w[(size_t)f * n + r] * pr;
+                for (int u = 0; u < kCgUnroll; ++u)
+                    g[u] = (k0 + u < w) ? ldg4(a.G + base + kSlice * (k0 + u)) : mk4<M>(M(0), M(0), M(0), M(0));
+#pragma unroll
+                for (int u = 0; u < kCgUnroll; ++u) {
+                    if (k0 + u < w) {
+                        const double2 rp = a.recA[bits_col(g[u].w)];
+                        const double pc = first ? rp.x : rp.x + beta * rp.y;
+                        a0 = a0 + (double)g[u].x * pc;
+                        a1 = a1 + (double)g[u].y * pc;
+                        a2 = a2 + (double)g[u].z * pc;
+                    }
+                }
             }
-            }
+            const double2 rr = a.recA[r];
+            const double pr = first ? rr.x : rr.x + beta * rr.y;
+            a.recB[r] = mk4<M>((M)a0, (M)a1, (M)a2, (M)pr);
+            a.Pd[r] = pr;
+#pragma unroll
+            for (int f = 0; f < NF; ++f)
+                if (f < a.nface) wp[f] += a.w[(size_t)f * n + r] * pr;
         }
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
@@ -448,30 +563,20 @@ __global__ void __launch_bounds__(256, 4) k_cg_persistent(CgArgs<M> a) {
         for (int f = 0; f < NF; ++f) cS[f] = f < a.nface ? a.coef[f] * sum_partials(partA, f, sm) : 0.0;
         // ---- phase B: SP = L P - Gt GP - sum_f cS_f z_f ; <P, SP> ----
         double dsum = 0.0;
-        {
-            CR_ROW_LOOP(n)
+        for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
             double lp = 0.0, gg = 0.0;
-            CR_ROW_BLOCKS(a.rowptr, a.col, {
-                const auto gl = ldg4(a.GL + j);
-                const double4 q = ldcg4(a.recB + c);
-                const double tl = (double)gl.w * q.w;
-                const double tg = (double)gl.x * q.x + (double)gl.y * q.y + (double)gl.z * q.z;
-                if (ok) {
-                    lp += tl;
-                    gg += tg;
-                }
+            CR_SELL_ROW_U(kCgUnroll, a.sp, a.scol, r, {
+                const auto gl = ldg4(a.GL + pos);
+                const auto q = a.recB[c];
+                lp = lp + (double)gl.w * (double)q.w;
+                gg = gg + (double)gl.x * (double)q.x + (double)gl.y * (double)q.y + (double)gl.z * (double)q.z;
             })
-            lp = group_sum(lp);
-            gg = group_sum(gg);
-            if (rv && lane == 0) {
 #pragma unroll
-                for (int f = 0; f < NF; ++f)
-                    if (f < a.nface) gg += cS[f] * a.z[(size_t)f * n + r];
-                const double v = lp - gg;
-                a.SP[r] = v;
-                dsum += __ldcg(&a.recB[r].w) * v;
-            }
-            }
+            for (int f = 0; f < NF; ++f)
+                if (f < a.nface) gg += cS[f] * a.z[(size_t)f * n + r];
+            const double v = lp - gg;
+            a.SP[r] = v;
+            dsum += a.Pd[r] * v;
         }
         dsum = block_sum(dsum, sm);
         if (threadIdx.x == 0) partB[(size_t)blockIdx.x * kCgPartStride] = dsum;
@@ -481,9 +586,9 @@ __global__ void __launch_bounds__(256, 4) k_cg_persistent(CgArgs<M> a) {
         double rs = 0.0;
         for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
              t += (long long)gridDim.x * blockDim.x) {
-            const double pv = __ldcg(&a.recB[t].w);
+            const double pv = a.Pd[t];
             a.X[t] = a.X[t] + alpha * pv;
-            const double rv = __ldcg(&a.recA[t].x) - alpha * __ldcg(a.SP + t);
+            const double rv = a.recA[t].x - alpha * a.SP[t];
             a.recA[t] = make_double2(rv, pv);
             rs += rv * rv;
         }
@@ -504,14 +609,6 @@ __global__ void __launch_bounds__(256, 4) k_cg_persistent(CgArgs<M> a) {
 // recA = {R, 0}
 __global__ void k_cg_init(const double* __restrict__ R, double2* __restrict__ recA, int n) {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) recA[t] = make_double2(R[t], 0.0);
-}
-
-// GL = {Gt(3), L} per block, in the matrix storage type
-template <typename M>
-__global__ void k_pack_gl(const M* __restrict__ Gt, const M* __restrict__ Lm, typename V4<M>::type* __restrict__ GL,
-                          long long nnz) {
-    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nnz; j += (long long)gridDim.x * blockDim.x)
-        GL[j] = mk4<M>(Gt[3 * j], Gt[3 * j + 1], Gt[3 * j + 2], Lm[j]);
 }
 
 // ext = valM scattered into a (3, n) vector
@@ -763,6 +860,11 @@ struct Ctx {
     void ss(const M* K, const IN* U, OUT* KU) {
         launch(k_spmv_ss<M, IN, OUT>, spmv_grid(), 256, 0, s, L->rowptr, L->col, K, U, KU, L->nNo);
     }
+    template <typename M, typename IN, typename OUT>
+    void vv3s(const M* Ks, const IN* U, OUT* KU) {
+        launch(k_sell_vv3<M, IN, OUT>, grid_for(L->nNo, 256, 8), 256, 0, s, (const int*)L->sell_ptr.p,
+               (const int*)L->sell_col.p, Ks, L->npad, U, KU, L->nNo);
+    }
     bool any_coupled() const {
         for (auto& f : L->face)
             if (f.coupledFlag) return true;
@@ -792,9 +894,9 @@ struct Ctx {
     }
 };
 
-// GMRES (memLS.f90:681-788) on dof = 3; K in M, basis in B, R and X FP64; X may not alias R.
+// GMRES (memLS.f90:681-788) on dof = 3; K sliced in M, basis in B, R and X FP64; X may not alias R.
 template <typename M, typename B>
-static int gmres(Ctx& C, crimson_subls& ls, const M* K, const double* R, double* X) {
+static int gmres(Ctx& C, crimson_subls& ls, const M* Ks, const double* R, double* X) {
     crimson_lhs* L = C.L;
     cudaStream_t s = C.s;
     const int dof = 3;
@@ -816,7 +918,7 @@ static int gmres(Ctx& C, crimson_subls& ls, const M* K, const double* R, double*
             launch(k_convert<B, double>, grid_for(n, 256), 256, 0, s, R, U(0), n);
         } else {
             ls.itr = ls.itr + 1;
-            C.vv3(K, (const double*)X, U(0));
+            C.vv3s(Ks, (const double*)X, U(0));
             C.addbcmul(0, dof, (const double*)X, U(0));
             launch(k_sub<double, B, B>, grid_for(n, 256), 256, 0, s, R, (const B*)U(0), U(0), n);
         }
@@ -843,7 +945,7 @@ static int gmres(Ctx& C, crimson_subls& ls, const M* K, const double* R, double*
         for (i = 1; i <= sD; ++i) {
             ls.itr = ls.itr + 1;
             B* w = U(i);
-            C.vv3(K, (const B*)U(i - 1), w);
+            C.vv3s(Ks, (const B*)U(i - 1), w);
             C.addbcmul(0, dof, (const B*)U(i - 1), w);
             if (coupled) {
                 CR_CUDA(cudaMemcpyAsync(w3, w, sizeof(B) * n, cudaMemcpyDeviceToDevice, s));
@@ -927,9 +1029,11 @@ static int cg_faces(Ctx& C, const M* G, const M* Gt, int* nface, double* coef) {
 }
 
 // CGRAD (memLS.f90:367-430) on the Schur-like operator L P - Gt G P; R in/out (n).
-// GL (packed {Gt, L}) must be current for this NSSOLVER call.
+// Gs / GLs: sliced G and {Gt, L} of this NSSOLVER call.
 template <typename M>
-static int cgrad(Ctx& C, crimson_subls& ls, const M* G, double* R, int nface, const double* coef) {
+static int cgrad(Ctx& C, crimson_subls& ls, const typename V4<M>::type* Gs, const typename V4<M>::type* GLs,
+                 double* R, int nface,
+                 const double* coef) {
     crimson_lhs* L = C.L;
     cudaStream_t s = C.s;
     const int n = L->nNo;
@@ -958,17 +1062,20 @@ static int cgrad(Ctx& C, crimson_subls& ls, const M* G, double* R, int nface, co
     CR_CHECK(L->cgPart.alloc(3 * (size_t)kCgPartStride * std::max(L->cg_grid, L->cg_grid32)));
     CR_CHECK(L->cgRecA.alloc(2 * (size_t)n));
     CR_CHECK(L->cgRecB.alloc(4 * (size_t)n));
+    CR_CHECK(L->cgPd.alloc((size_t)n));
     CR_CUDA(cudaMemsetAsync(L->cgX.p, 0, sizeof(double) * n, s));
     launch(k_cg_init, grid_for(n, 256), 256, 0, s, (const double*)R, reinterpret_cast<double2*>(L->cgRecA.p), n);
     CgArgs<M> a;
-    a.rowptr = L->rowptr;
-    a.col = L->col;
+    a.sp = L->sell_ptr.p;
+    a.scol = L->sell_col.p;
+    a.npad = L->npad;
     a.n = n;
-    a.G = G;
-    a.GL = reinterpret_cast<const typename V4<M>::type*>(L->cgGL.p);
+    a.G = Gs;
+    a.GL = GLs;
     a.X = L->cgX.p;
     a.recA = reinterpret_cast<double2*>(L->cgRecA.p);
-    a.recB = reinterpret_cast<double4*>(L->cgRecB.p);
+    a.recB = reinterpret_cast<typename V4<M>::type*>(L->cgRecB.p);
+    a.Pd = L->cgPd.p;
     a.SP = L->cgSP.p;
     a.nface = nface;
     a.w = L->cgW.p;
@@ -1043,6 +1150,67 @@ static int ge_solve(int N, const double* A, double* B) {
     return CRIMSON_OK;
 }
 
+// Sliced matrix buffers of one precision (zeroed at allocation, so the
+// padding entries stay zero: conversions only write real entries).
+template <typename M>
+static int sell_alloc(crimson_lhs* L, DBuf<M>& K, DBuf<M>& G, DBuf<M>& GL) {
+    const size_t np = (size_t)L->npad + (size_t)kSlice * kSellUnroll;
+    if (K.n == 9 * np && G.n == 4 * np && GL.n == 4 * np) return CRIMSON_OK;
+    CR_CHECK(K.alloc(9 * np));
+    CR_CHECK(G.alloc(4 * np));
+    CR_CHECK(GL.alloc(4 * np));
+    CR_CUDA(cudaMemsetAsync(K.p, 0, sizeof(M) * K.n, L->stream));
+    CR_CUDA(cudaMemsetAsync(G.p, 0, sizeof(M) * G.n, L->stream));
+    CR_CUDA(cudaMemsetAsync(GL.p, 0, sizeof(M) * GL.n, L->stream));
+    return CRIMSON_OK;
+}
+static int sell_mats(crimson_lhs* L, double** K, double4** G, double4** GL) {
+    CR_CHECK(sell_alloc(L, L->Ks64, L->Gs64, L->GLs64));
+    *K = L->Ks64.p;
+    *G = reinterpret_cast<double4*>(L->Gs64.p);
+    *GL = reinterpret_cast<double4*>(L->GLs64.p);
+    return CRIMSON_OK;
+}
+static int sell_mats(crimson_lhs* L, float** K, float4** G, float4** GL) {
+    CR_CHECK(sell_alloc(L, L->Ks32, L->Gs32, L->GLs32));
+    *K = L->Ks32.p;
+    *G = reinterpret_cast<float4*>(L->Gs32.p);
+    *GL = reinterpret_cast<float4*>(L->GLs32.p);
+    return CRIMSON_OK;
+}
+
+// Sliced pattern: slice widths from the row lengths (host), columns (device).
+static int sell_pattern(crimson_lhs* L) {
+    if (L->sell_ptr.p) return CRIMSON_OK;
+    const int n = L->nNo;
+    cudaStream_t s = L->stream;
+    std::vector<int> rp((size_t)n + 1);
+    CR_CUDA(cudaMemcpyAsync(rp.data(), L->rowptr, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    const int ns = (n + kSlice - 1) / kSlice;
+    std::vector<int> sp((size_t)ns + 1, 0);
+    long long pos = 0;
+    for (int q = 0; q < ns; ++q) {
+        int w = 0;
+        for (int r = q * kSlice; r < std::min(n, (q + 1) * kSlice); ++r) w = std::max(w, rp[r + 1] - rp[r]);
+        sp[q] = (int)pos;
+        pos += (long long)kSlice * w;
+        if (pos + (long long)kSlice * kSellUnroll > 0x7fffffffLL) return CRIMSON_ERR_UNSUPPORTED;
+    }
+    sp[ns] = (int)pos;
+    L->nslice = ns;
+    L->npad = pos;
+    CR_CHECK(L->sell_ptr.upload(sp.data(), sp.size(), s));
+    const size_t np = (size_t)pos + (size_t)kSlice * kSellUnroll;
+    CR_CHECK(L->sell_col.alloc(np));
+    CR_CUDA(cudaMemsetAsync(L->sell_col.p, 0, sizeof(int) * np, s));
+    launch(k_sell_cols, grid_for((long long)ns * kSlice, 256), 256, 0, s, L->rowptr, L->col,
+           (const int*)L->sell_ptr.p, n, ns * kSlice, L->sell_col.p);
+    CR_CUDA(cudaStreamSynchronize(s));
+    CR_CUDA(cudaGetLastError());
+    return CRIMSON_OK;
+}
+
 // NSSOLVER (memLS.f90:1460-1759); R (4, nNo) FP64 in/out; matrices in M.
 template <typename M, typename B>
 static int nssolver(crimson_lhs* L, crimson_ls* ls, const M* mK, const M* mG, const M* mD, const M* mL, const M* Gt,
@@ -1091,24 +1259,29 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const M* mK, const M* mG, co
     int cg_nface = 0;
     double cg_coef[kMaxCoupled];
     CR_CHECK(cg_faces(C, mG, Gt, &cg_nface, cg_coef));
-    CR_CHECK(L->cgGL.alloc(4 * (size_t)L->nnz));
-    launch(k_pack_gl<M>, grid_for(L->nnz, 256), 256, 0, s, Gt, mL,
-           reinterpret_cast<typename V4<M>::type*>(L->cgGL.p), L->nnz);
+    M* Ks = nullptr;
+    typename V4<M>::type* Gs = nullptr;
+    typename V4<M>::type* GLs = nullptr;
+    CR_CHECK(sell_mats(L, &Ks, &Gs, &GLs));
+    launch(k_to_sell<M>, grid_for(nNo, 256), 256, 0, s, L->rowptr, (const int*)L->sell_ptr.p, nNo, mK, mG, Gt, mL,
+           L->npad, Ks, Gs, GLs, L->col);
     int i, iBB = 0;
     for (i = 1; i <= ls->RI.mItr; ++i) {
         iB = 2 * i - 1;
         iBB = 2 * i;
         ls->RI.dB = ls->RI.fNorm;
-        CR_CHECK((gmres<M, B>(C, ls->GM, mK, L->Rm.p, Ucol(i - 1))));
+        CR_CHECK((gmres<M, B>(C, ls->GM, (const M*)Ks, L->Rm.p, Ucol(i - 1))));
         C.vs3(mD, (const double*)Ucol(i - 1), Pcol(i - 1));
         launch(k_sub<double, double, double>, grid_for(nNo, 256), 256, 0, s, (const double*)L->Rc.p,
                (const double*)Pcol(i - 1), Pcol(i - 1), (long long)nNo);
-        CR_CHECK(cgrad<M>(C, ls->CG, mG, Pcol(i - 1), cg_nface, cg_coef));
+        CR_CHECK(cgrad<M>(C, ls->CG, (const typename V4<M>::type*)Gs, (const typename V4<M>::type*)GLs, Pcol(i - 1),
+                          cg_nface,
+                          cg_coef));
         C.sv3(mG, (const double*)Pcol(i - 1), MUc(iB - 1));
         launch(k_sub<double, double, double>, grid_for(nv, 256), 256, 0, s, (const double*)L->Rm.p,
                (const double*)MUc(iB - 1), MUc(iBB - 1), nv);
-        CR_CHECK((gmres<M, B>(C, ls->GM, mK, MUc(iBB - 1), Ucol(i - 1))));
-        C.vv3(mK, (const double*)Ucol(i - 1), MUc(iBB - 1));
+        CR_CHECK((gmres<M, B>(C, ls->GM, (const M*)Ks, MUc(iBB - 1), Ucol(i - 1))));
+        C.vv3s((const M*)Ks, (const double*)Ucol(i - 1), MUc(iBB - 1));
         C.addbcmul(0, 3, (const double*)Ucol(i - 1), MUc(iBB - 1));
         C.ss(mL, (const double*)Pcol(i - 1), MPc(iB - 1));
         C.vs3(mD, (const double*)Ucol(i - 1), MPc(iBB - 1));
@@ -1216,6 +1389,7 @@ static int lhs_work_alloc(crimson_lhs* L, const crimson_ls* ls) {
     CR_CHECK(L->w3.alloc(3 * (size_t)nNo));
     CR_CHECK(L->cgX.alloc((size_t)nNo));
     CR_CHECK(L->cgSP.alloc((size_t)nNo));
+    CR_CHECK(sell_pattern(L));
     if (!L->scal.p) {
         CR_CHECK(L->scal.alloc(kScalTotal));
         CR_CHECK(L->red.init());
@@ -1431,11 +1605,12 @@ int memls_solve_lhs_device(crimson_lhs* L, crimson_ls* ls, const double* d_res, 
     return CRIMSON_OK;
 }
 
-// Diagnostics.  which: 0 = 3x3 block SpMV (K), 1 = one CG iteration of the
-// persistent FP64 CGRAD kernel (average over all launches so far, from CUDA
-// events recorded around each launch), 2 = SPARMULSV (G), 3 = fused MGS step,
-// 4 = one CG iteration of the FP32-matrix CGRAD kernel, 5 = 3x3 block SpMV
-// with FP32 K.
+// Diagnostics.  which: 0 = 3x3 block SpMV (K, sliced, FP64, as GMRES runs
+// it), 1 = one CG iteration of the persistent FP64 CGRAD kernel (average over
+// all launches so far, from CUDA events recorded around each launch),
+// 2 = SPARMULSV (G), 3 = fused MGS step, 4 = one CG iteration of the
+// FP32-matrix CGRAD kernel, 5 = 3x3 block SpMV with the sliced FP32 K,
+// 6 = 3x3 block SpMV on the CSR FP64 K (four lanes per row).
 int memls_kernel_time(crimson_lhs* L, int which, int reps, double* ms) {
     if (which == 1 || which == 4) {
         const auto& acc = which == 1 ? L->cg_acc64 : L->cg_acc32;
@@ -1444,7 +1619,7 @@ int memls_kernel_time(crimson_lhs* L, int which, int reps, double* ms) {
         return CRIMSON_OK;
     }
     if (!L->mK.p || !L->basis.p || reps <= 0) return CRIMSON_ERR_STATE;
-    if (which == 5 && !L->mK32.p) return CRIMSON_ERR_STATE;
+    if ((which == 5 && !L->Ks32.p) || (which == 0 && !L->Ks64.p)) return CRIMSON_ERR_STATE;
     cudaStream_t s = L->stream;
     Ctx C{L, s};
     const long long n3 = 3LL * L->nNo;
@@ -1453,9 +1628,10 @@ int memls_kernel_time(crimson_lhs* L, int which, int reps, double* ms) {
     CR_CUDA(cudaEventCreate(&e1));
     auto run = [&]() {
         switch (which) {
-            case 0: C.vv3((const double*)L->mK.p, (const double*)L->basis.p, L->basis.p + n3); break;
+            case 0: C.vv3s((const double*)L->Ks64.p, (const double*)L->basis.p, L->basis.p + n3); break;
+            case 6: C.vv3((const double*)L->mK.p, (const double*)L->basis.p, L->basis.p + n3); break;
             case 2: C.sv3((const double*)L->mG.p, (const double*)L->cgX.p, L->w3.p); break;
-            case 5: C.vv3((const float*)L->mK32.p, (const double*)L->basis.p, L->basis.p + n3); break;
+            case 5: C.vv3s((const float*)L->Ks32.p, (const double*)L->basis.p, L->basis.p + n3); break;
             default:
                 launch(k_mgs<double>, red_grid(n3), 256, 0, s, L->basis.p + 2 * n3, (const double*)L->basis.p,
                        (const double*)C.sc(kSlotH), (const double*)(L->basis.p + n3), n3, L->red.part.p,

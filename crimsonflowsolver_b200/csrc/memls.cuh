@@ -51,7 +51,14 @@ struct crimson_lhs {
     DBuf<double> cgX, cgP, cgSP, cgGP, cgR, cgP2;
     DBuf<double> cgW, cgZ, cgExt;     // coupled-face vectors w = G^T valM, z = Gt valM (per face)
     DBuf<double> cgPart;              // persistent CG partial sums (3 regions)
-    DBuf<double> cgGL, cgRecA, cgRecB; // packed {Gt, L} blocks; {R, P} and {GP, P} node records
+    DBuf<double> cgRecA, cgRecB, cgPd; // {R, P} and {GP, P} node records; P (FP64)
+    // sliced ELL copy of the pattern (32 rows per slice) and of the matrices
+    // the Krylov loops multiply by, per storage precision
+    int nslice = 0;
+    long long npad = 0;
+    DBuf<int> sell_ptr, sell_col;
+    DBuf<double> Ks64, Gs64, GLs64;
+    DBuf<float> Ks32, Gs32, GLs32;
     int cg_grid = 0, cg_grid32 = 0;
     // mixed precision: FP32 copies of the scaled split matrices; FP64 right
     // side and accumulated solution of the iterative refinement

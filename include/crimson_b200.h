@@ -236,8 +236,9 @@ int crimson_pvsq_noalloc(int nsurf, const int* surf_offsets, const int* d_nodes,
 
 /* Diagnostics: average device time (ms) of one launch of a memLS kernel on the
  * lhs's current split matrices, timed with CUDA events on the lhs stream.
- * which: 0 = 3x3 block SpMV (SPARMULVV, K), 2 = SPARMULSV (G), 3 = fused MGS
- * step, 5 = 3x3 block SpMV with the FP32 copy of K (after a mixed solve).
+ * which: 0 = 3x3 block SpMV (SPARMULVV, K) on the sliced-ELL copy GMRES
+ * uses, 2 = SPARMULSV (G), 3 = fused MGS step, 5 = the sliced 3x3 block SpMV
+ * with FP32 K (after a mixed solve), 6 = the 3x3 block SpMV on CSR K.
  * which 1 / 4: time of one CGRAD iteration of the persistent CG kernel with
  * FP64 / FP32 matrices, averaged over every launch on this lhs so far (CUDA
  * events recorded around each cooperative launch; reps is ignored).
