@@ -40,6 +40,16 @@ sys.path.insert(0, ROOT)
 METRIC = "s/timestep @4M tets (mixed vs FP64 GPU, ≤1e-6 rel err); Melem/s assembly"
 NCROSS, NAXIAL = 80, 133
 NITR = 3
+EPSTOL_NS = 1e-5      # memLS NSSOLVER relative tolerance (epstol(8))
+REFINE_TOL = 0.0      # mixed precision: FP64 defect target (0: the NSSOLVER tolerance)
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one persistent
+# CG iteration divided by cg_iter_bytes, from ncu captures of one launch of 50
+# iterations on a 2.07M-tet cylinder (5.3M blocks, matrices and vectors
+# larger than L2); the traffic of a launch grows with blocks x iterations, so
+# the ratio scales the full-size algorithmic bytes to full-size traffic.
+TRAFFIC_PER_ALG_F32 = 0.982
+TRAFFIC_PER_ALG_F64 = 1.075
+TRAFFIC_SOURCE = "ncu --set full, k_cg_persistent, 2.07M-tet cylinder, 50 iterations/launch, scaled by blocks"
 # Outer NS iterations and inner GMRES / CG iteration totals per memLS solve on
 # this workload, as counted by the solver on steps 2-5 (identical algorithm
 # and counts on CPU and GPU, see tests/test_gpu_parity.py).  Used only to
@@ -102,11 +112,12 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def make_problem(ncross: int, naxial: int):
+def make_problem(ncross: int, naxial: int, epstol_ns: float = None):
     from crimsonflowsolver_b200 import FlowParams, RCR, mesh
 
     m = mesh.cylinder(ncross=ncross, naxial=naxial, seed=1)
-    P = FlowParams(rcr=[RCR(srfid=3, Rp=100.0, C=1e-4, Rd=1000.0)], nitr=NITR)
+    P = FlowParams(rcr=[RCR(srfid=3, Rp=100.0, C=1e-4, Rd=1000.0)], nitr=NITR,
+                   epstol_ns=EPSTOL_NS if epstol_ns is None else epstol_ns)
     return m, P
 
 
@@ -162,7 +173,7 @@ def run_reference(args):
     if rank != 0:
         return
     nthreads = os.cpu_count() or 1
-    m, P = make_problem(args.ncross, args.naxial)
+    m, P = make_problem(args.ncross, args.naxial, args.epstol_ns)
     vals = []
     for i in range(args.warmup + args.steps):
         v, sample, wall = cpu_sample(m, P, nthreads)
@@ -229,13 +240,14 @@ def _relerr(a, b):
 def cg_iter_bytes(nnz: int, n: int, mbytes: int, nface: int) -> int:
     """Algorithmic HBM bytes of one iteration of the persistent CGRAD kernel.
 
-    Per block: column index (4) + G (3 values) + {Gt, L} (4 values), values of
-    mbytes each.  Per row, once: row pointers (2 x 4), records {R, P_prev}
-    read (16), {GP, P} written (32) and read (32), SP written (8), X read and
-    written (16), {R, P} read and written (32), SP and P read in the update
-    (16), and 2 x 8 per coupled face (w_f, z_f).
+    Per block (nnz real blocks, no padding): G (3 values) + Gt (3) + L (1) of
+    mbytes each, and the column index read by each of the two SpMV phases
+    (2 x 4).  Per row, once: {R, P_prev} read (16), {GP, P} written and
+    gathered (2 x 4 mbytes), P written and read twice (24), SP written and
+    read (16), X read and written (16), {R, P} written (16), and 2 x 8 per
+    coupled face (w_f, z_f).
     """
-    return nnz * (8 + 7 * mbytes) + n * (8 + 16 + 32 + 32 + 8 + 16 + 32 + 16 + 16 * nface)
+    return nnz * (8 + 7 * mbytes) + n * (16 + 8 * mbytes + 24 + 16 + 16 + 16 + 16 * nface)
 
 
 def run_ours(args):
@@ -258,14 +270,14 @@ def run_ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     L = N.lib()
-    m, P = make_problem(args.ncross, args.naxial)
+    m, P = make_problem(args.ncross, args.naxial, args.epstol_ns)
     n = m.nshg
     # ---- FP64 (memLS arithmetic) ----
     F64 = solver.FlowSolver(m, P, inflow=_inflow)
     s64 = torch.cuda.ExternalStream(F64.elm.stream_handle)
     t64_ms, it64, l64, clk64 = _timed_steps(F64, args, s64, local, dist)
     # ---- mixed: FP32 inner matvecs, FP64 refinement ----
-    Pm = FlowParams(**{**P.__dict__, "precision": "mixed"})
+    Pm = FlowParams(**{**P.__dict__, "precision": "mixed", "max_refine": 8, "refine_tol": args.refine_tol})
     FM = solver.FlowSolver(m, Pm, inflow=_inflow)
     sm = torch.cuda.ExternalStream(FM.elm.stream_handle)
     tm_ms, itm, lm, clkm = _timed_steps(FM, args, sm, local, dist)
@@ -327,6 +339,8 @@ def run_ours(args):
     nface = len(P.rcr)
     cg_bytes = cg_iter_bytes(nnz, n, 4, nface)
     achieved = cg_bytes / (kt["cg_iter_f32"] / 1e3) / 1e9 if kt["cg_iter_f32"] else None
+    cg_bytes64 = cg_iter_bytes(nnz, n, 8, nface)
+    achieved64 = cg_bytes64 / (kt["cg_iter_f64"] / 1e3) / 1e9 if kt["cg_iter_f64"] else None
     line = {
         "metric": METRIC, "value": value, "unit": "s/timestep", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tm_ms / args.steps, "higher_is_better": False, "scaling": "weak",
@@ -335,6 +349,8 @@ def run_ours(args):
         "config": {"workload": f"4.0M-tet cylinder ({m.nelem} tets, {n} nodes, {nnz} blocks), pulsatile inflow, "
                                "RCR outlet, dt=1e-3, 3 nonlinear iterations/step, mixed-precision NS solve",
                    "parallelism": "replicas" if ws > 1 else "single GPU",
+                   "epstol_ns": P.epstol_ns, "epstol_gmres_cg": [P.epstol_mom, P.epstol_cont],
+                   "mixed_refine_tol": Pm.refine_tol if Pm.refine_tol > 0 else P.epstol_ns,
                    "l2": "inputs larger than L2 (FP32 matrices 0.45 GB, FP64 1.3 GB per solve)"},
         "fp64": {"value": v64, "unit": "s/timestep", "ms_per_step": t64_ms / args.steps,
                  "solver_iters_per_solve": it64, "gpu_launches": l64, "clocks": clk64},
@@ -346,8 +362,13 @@ def run_ours(args):
         "kernel_ms": kt,
         "roofline": {"kernel": "k_cg_persistent<float> (one CGRAD iteration: G P, L P - Gt G P, updates)",
                      "bound": "hbm", "achieved": achieved, "peak": peaks[0], "unit": "GB/s",
-                     "frac": achieved / peaks[0] if achieved else None, "traffic": None,
-                     "algorithmic_bytes_per_iter": cg_bytes, "peak_source": peaks[1]},
+                     "frac": achieved / peaks[0] if achieved else None,
+                     "traffic": TRAFFIC_PER_ALG_F32 * cg_bytes if TRAFFIC_PER_ALG_F32 else None,
+                     "traffic_source": TRAFFIC_SOURCE,
+                     "algorithmic_bytes_per_iter": cg_bytes, "peak_source": peaks[1],
+                     "fp64_kernel": {"achieved": achieved64, "frac": achieved64 / peaks[0] if achieved64 else None,
+                                     "algorithmic_bytes_per_iter": cg_bytes64,
+                                     "traffic": TRAFFIC_PER_ALG_F64 * cg_bytes64 if TRAFFIC_PER_ALG_F64 else None}},
         "e2e": {"value": e2e, "unit": "s/timestep", "h2d_bytes_per_step": 2 * 4 * n * 8,
                 "d2h_bytes_per_step": 2 * 4 * n * 8},
         "gpu_launches": lm,
@@ -379,6 +400,25 @@ def _peaks():
         return 6650.0, "fallback 6.65 TB/s"
 
 
+def run_cg_capture(args):
+    """Small fixed-work case for profiler captures of the persistent CG kernel.
+
+    One time step with one nonlinear iteration, two NSSOLVER outer iterations
+    and CG maxiters = --cg-iters with an unreachable CG tolerance, so every CG
+    launch runs exactly --cg-iters iterations.
+    """
+    from crimsonflowsolver_b200 import FlowParams, RCR, mesh, solver
+
+    m = mesh.cylinder(ncross=args.ncross, naxial=args.naxial, seed=1)
+    P = FlowParams(rcr=[RCR(srfid=3)], precision=args.precision, maxiters=args.cg_iters, epstol_cont=1e-14,
+                   nprjs=2, nitr=1, max_refine=1)
+    F = solver.FlowSolver(m, P, inflow=lambda t: 10.0)
+    st = F.step()
+    print(json.dumps({"tets": m.nelem, "nodes": m.nshg, "blocks": F.elm._nnz(),
+                      "solves": [(st.ri_itr[i], st.gm_itr[i], st.cg_itr[i]) for i in range(st.nsolves)]}))
+    F.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -388,8 +428,17 @@ def main():
     ap.add_argument("--ncross", type=int, default=NCROSS)
     ap.add_argument("--naxial", type=int, default=NAXIAL)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--epstol-ns", type=float, default=EPSTOL_NS, help="NSSOLVER relative tolerance, both arms")
+    ap.add_argument("--refine-tol", type=float, default=REFINE_TOL,
+                    help="mixed precision FP64 defect target (0: the NSSOLVER tolerance)")
+    ap.add_argument("--cg-capture", action="store_true",
+                    help="run the small fixed-iteration CG case for profiler captures instead of the benchmark")
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"], help="--cg-capture only")
+    ap.add_argument("--cg-iters", type=int, default=50, help="--cg-capture only")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.cg_capture:
+        run_cg_capture(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
