@@ -84,6 +84,11 @@ SIGNATURES = {
                                            ctypes.POINTER(LsStats)]),
     "crimson_solflow_device": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int_p,
                                               c_dbl_p, c_void_p, ctypes.POINTER(LsStats)]),
+    "crimson_solflow_device_transposed": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                                         c_int_p, c_dbl_p, c_void_p, ctypes.POINTER(LsStats)]),
+    "crimson_elmgmr_vjp": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_dbl_p, c_dbl_p, c_void_p, c_void_p,
+                                          c_void_p, c_void_p, c_dbl_p, c_dbl_p, c_dbl_p]),
+    "crimson_rcr_state": (ctypes.c_int, [c_void_p, ctypes.c_int, c_dbl_p, c_dbl_p, ctypes.c_int]),
     "crimson_set_inflow": (ctypes.c_int, [c_void_p, ctypes.c_int, c_int_p, c_dbl_p]),
     "crimson_set_rcr": (ctypes.c_int, [c_void_p, ctypes.c_int, c_dbl_p, c_dbl_p, c_dbl_p, c_dbl_p]),
     "crimson_state_set": (ctypes.c_int, [c_void_p, c_dbl_p, c_dbl_p]),

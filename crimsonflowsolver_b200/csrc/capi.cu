@@ -36,7 +36,10 @@ int memls_solve_val(crimson_lhs* L, crimson_ls* ls, double* Ri, double* Val, con
                     crimson_ls_stats* st);
 int memls_solve_lhs_device(crimson_lhs* L, crimson_ls* ls, const double* d_res, const double* d_lhsK,
                            const double* d_lhsP, const int* incL, const double* faceRes, double* d_sol,
-                           crimson_ls_stats* st);
+                           crimson_ls_stats* st, bool transpose = false);
+int elmgmr_vjp(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1, const double* coef2,
+               const double* d_lam, double* d_res, double* d_ybar, double* d_abar, double* mubar, double* c1bar,
+               double* c2bar);
 
 // ---- layout conversion kernels ----
 __global__ void k_soa_to_node4(const double* __restrict__ a, int n, int ld, double* __restrict__ out) {
@@ -526,6 +529,23 @@ int crimson_solflow_device(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const
     return memls_solve_lhs_device(L, ls, d_res, d_lhsK, d_lhsP, incL, faceRes, d_solinc, stats);
 }
 
+int crimson_solflow_device_transposed(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const double* d_rhs,
+                                      const double* d_lhsK, const double* d_lhsP, const int* incL,
+                                      const double* faceRes, double* d_sol, crimson_ls_stats* stats) {
+    if (!c || !L || !ls || !d_rhs || !d_lhsK || !d_lhsP || !d_sol) return CRIMSON_ERR_ARG;
+    if (L->diag == nullptr || L->trans == nullptr) return CRIMSON_ERR_STATE;
+    return memls_solve_lhs_device(L, ls, d_rhs, d_lhsK, d_lhsP, incL, faceRes, d_sol, stats, true);
+}
+
+int crimson_elmgmr_vjp(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1,
+                       const double* coef2, const double* d_lambda, double* d_res, double* d_ybar, double* d_acbar,
+                       double* mubar, double* coef1bar, double* coef2bar) {
+    if (!c || !d_y || !d_ac || !d_lambda || !d_ybar || !d_acbar) return CRIMSON_ERR_ARG;
+    if (c->ncoupled > 0 && (!coef1 || !coef2)) return CRIMSON_ERR_ARG;
+    CR_CHECK(check_params(&c->p));
+    return elmgmr_vjp(c, d_y, d_ac, coef1, coef2, d_lambda, d_res, d_ybar, d_acbar, mubar, coef1bar, coef2bar);
+}
+
 // ---------------------------------------------------------------------------
 // Time stepping
 // ---------------------------------------------------------------------------
@@ -554,6 +574,20 @@ int crimson_set_rcr(crimson_ctx* c, int n, const double* Rp, const double* C, co
     return CRIMSON_OK;
 }
 
+int crimson_rcr_state(crimson_ctx* c, int n, double* Pn, double* Qn, int set) {
+    if (!c || n != c->ncoupled || (n > 0 && (!Pn || !Qn))) return CRIMSON_ERR_ARG;
+    if ((int)c->rcr_Pn.size() != n) return CRIMSON_ERR_STATE;
+    for (int k = 0; k < n; ++k) {
+        if (set) {
+            c->rcr_Pn[k] = Pn[k];
+            c->rcr_Qn[k] = Qn[k];
+        } else {
+            Pn[k] = c->rcr_Pn[k];
+            Qn[k] = c->rcr_Qn[k];
+        }
+    }
+    return CRIMSON_OK;
+}
 int crimson_state_set(crimson_ctx* c, const double* y, const double* ac) {
     if (!c || !y || !ac) return CRIMSON_ERR_ARG;
     const int n = c->nshg;

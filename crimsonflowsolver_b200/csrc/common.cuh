@@ -181,6 +181,9 @@ struct crimson_ctx {
 
     // time stepping state (crimson_step)
     crimson::DBuf<double> yold, acold, ycur, accur, yalpha, acalpha, solinc, stage;
+
+    // adjoint work space (crimson_elmgmr_vjp)
+    crimson::DBuf<double> adj_res, adj_lam, adj_qbar, adj_scal;
     crimson::DBuf<int> inlet_nodes;
     crimson::DBuf<double> inlet_profile;   // (ninlet, 3)
     int ninlet = 0;

@@ -1582,9 +1582,34 @@ int memls_solve_val(crimson_lhs* L, crimson_ls* ls, double* Ri, double* Val, con
     return CRIMSON_OK;
 }
 
+// K_out(j) = K_in(trans(j))^T: the momentum blocks of the transposed system
+__global__ void k_transpose_k(const double* __restrict__ Kin, const int* __restrict__ trans, long long nnz,
+                              double* __restrict__ Kout) {
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nnz; j += (long long)gridDim.x * blockDim.x) {
+        const double* k = Kin + 9 * (size_t)trans[j];
+        double* o = Kout + 9 * (size_t)j;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) o[3 * a + b] = k[3 * b + a];
+    }
+}
+
+// R(4, i) = -R(4, i)
+__global__ void k_negate_p(double* __restrict__ R, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) R[4 * (size_t)i + 3] = -R[4 * (size_t)i + 3];
+}
+
+// transpose: solve with the transposed matrix.  Val4 = [K G; D L] built from
+// lhsK / lhsP has G = -D^T (both come from lhsP(1:3)) and a symmetric L
+// (the PSPG block is symmetrised per element), so
+//   A^T = [K^T  -G; -D  L]  and  A^T [u; p] = [f; g]  <=>  [K^T G; D L] [u; -p] = [f; -g]:
+// the same NS solve with the momentum blocks transposed and the pressure
+// rows of the right side and of the solution negated.  The diagonal
+// scaling, Dirichlet faces and the (symmetric) coupled-face terms carry over.
 int memls_solve_lhs_device(crimson_lhs* L, crimson_ls* ls, const double* d_res, const double* d_lhsK,
                            const double* d_lhsP, const int* incL, const double* faceRes, double* d_sol,
-                           crimson_ls_stats* st) {
+                           crimson_ls_stats* st, bool transpose) {
     cudaStream_t s = L->stream;
     CR_CHECK(lhs_work_alloc(L, ls));
     set_face_flags(L, incL, faceRes);
@@ -1595,9 +1620,16 @@ int memls_solve_lhs_device(crimson_lhs* L, crimson_ls* ls, const double* d_res, 
            (const double*)L->W.p, L->nNo, L->mK.p, L->mG.p, L->mD.p, L->mL.p);
     launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, (const double*)L->W.p, 4LL * L->nNo);
     CR_CHECK(precond_faces(L, true));
+    if (transpose) {
+        CR_CHECK(L->mKt.alloc(9 * (size_t)L->nnz));
+        launch(k_transpose_k, grid_for(L->nnz, 256), 256, 0, s, (const double*)L->mK.p, L->trans, L->nnz, L->mKt.p);
+        std::swap(L->mK, L->mKt);
+        launch(k_negate_p, grid_for(L->nNo, 256), 256, 0, s, L->R.p, L->nNo);
+    }
     // With Val4 built from lhsK/lhsP, Gt = -mG^T equals mD up to the order of
     // the two scaling products, so mD serves as Gt.
     CR_CHECK(solve_scaled(L, ls, false));
+    if (transpose) launch(k_negate_p, grid_for(L->nNo, 256), 256, 0, s, L->R.p, L->nNo);
     launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, (const double*)L->W.p, 4LL * L->nNo);
     CR_CUDA(cudaMemcpyAsync(d_sol, L->R.p, sizeof(double) * 4 * (size_t)L->nNo, cudaMemcpyDeviceToDevice, s));
     CR_CUDA(cudaStreamSynchronize(s));

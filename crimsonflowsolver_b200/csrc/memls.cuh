@@ -46,7 +46,7 @@ struct crimson_lhs {
     const int* trans = nullptr;
     std::vector<MemlsFace> face;
     // work space
-    DBuf<double> W, R, Val, mK, mG, mD, mL, Gt;
+    DBuf<double> W, R, Val, mK, mG, mD, mL, Gt, mKt;
     DBuf<double> Rm, Rc, Rmi, Rci, U, P, MU, MP, X3, basis, w3;
     DBuf<double> cgX, cgP, cgSP, cgGP, cgR, cgP2;
     DBuf<double> cgW, cgZ, cgExt;     // coupled-face vectors w = G^T valM, z = Gt valM (per face)

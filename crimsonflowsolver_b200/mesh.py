@@ -210,13 +210,16 @@ def _finish_tube(m: Mesh, fb: np.ndarray, srf: np.ndarray, inlet_axis_profile) -
 
 
 def cylinder(ncross: int = 24, naxial: int = 40, radius: float = 1.0, length: float = 10.0,
-             jitter: float = 0.05, seed: int = 1, name: str = "cylinder") -> Mesh:
+             jitter: float = 0.05, seed: int = 1, name: str = "cylinder", n_outlets: int = 1) -> Mesh:
     """Straight tube: ncross x ncross hex cross-section masked to the disc, naxial layers.
 
     Cells whose centre lies inside ``radius`` are kept; each hex is split into
     6 Kuhn tets.  Nodes not on the boundary are jittered uniformly by
     ``jitter`` x the local edge length in every coordinate (seeded).
-    Inlet at z = 0 (parabolic profile, unit mean speed), outlet at z = length.
+    Inlet at z = 0 (parabolic profile, unit mean speed), outlet cap at
+    z = length.  With ``n_outlets`` > 1 the cap is split into that many
+    equal angular sectors (by face centroid), each its own outlet surface
+    (ids 3, 4, ...): outlets branching from the distal cap.
     """
     h = 2.0 * radius / ncross
     hz = length / naxial
@@ -261,7 +264,14 @@ def cylinder(ncross: int = 24, naxial: int = 40, radius: float = 1.0, length: fl
     zc = x[fb[:, :3], 2].mean(axis=1)
     srf = np.full(fb.shape[0], SRF_WALL, dtype=np.int32)
     srf[zc < 1e-9 * length] = SRF_INLET
-    srf[zc > length * (1 - 1e-9)] = SRF_OUTLET0
+    cap = zc > length * (1 - 1e-9)
+    if n_outlets <= 1:
+        srf[cap] = SRF_OUTLET0
+    else:
+        xc = x[fb[:, :3], 0].mean(axis=1)
+        yc = x[fb[:, :3], 1].mean(axis=1)
+        sector = np.floor((np.arctan2(yc, xc) + np.pi) / (2.0 * np.pi) * n_outlets).astype(np.int32)
+        srf[cap] = SRF_OUTLET0 + np.clip(sector[cap], 0, n_outlets - 1)
 
     def profile(nodes):
         r2 = (x[nodes, 0] ** 2 + x[nodes, 1] ** 2) / radius ** 2

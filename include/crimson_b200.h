@@ -180,6 +180,31 @@ int crimson_solflow_device(crimson_ctx* ctx, crimson_lhs* lhs, crimson_ls* ls, c
                            double* d_solinc, crimson_ls_stats* stats);
 
 /* ---------------------------------------------------------------------------
+ * Adjoint building blocks.  No counterpart in the reference (it has no
+ * adjoint).
+ * ------------------------------------------------------------------------- */
+/* Transposed solve: same arguments and preconditioning as
+ * crimson_solflow_device, but solves A^T z = rhs, A the Val4 matrix SolFlow
+ * packs from lhsK/lhsP (plus the coupled-face terms).  d_rhs, d_sol (4, nshg)
+ * node-major on the device. */
+int crimson_solflow_device_transposed(crimson_ctx* ctx, crimson_lhs* lhs, crimson_ls* ls, const double* d_rhs,
+                                      const double* d_lhsK, const double* d_lhsP, const int* incL,
+                                      const double* faceRes, double* d_sol, crimson_ls_stats* stats);
+/* Exact vector-Jacobian product of ElmGMR's residual res(y, ac; mu, coef1,
+ * coef2) -- the same vector crimson_elmgmr_device assembles, with the
+ * viscous-flux projection, boundary faces, outlet coupling and bc3Res --
+ * for a cotangent lambda (4, nshg) node-major on the device:
+ *   d_ybar  = (d res / d y)^T lambda      (4, nshg) node-major (u, v, w, p)
+ *   d_acbar = (d res / d ac)^T lambda     (4, nshg) node-major (pressure slot 0)
+ *   *mubar = lambda . d res / d mu; coef1bar[k], coef2bar[k] likewise (host).
+ * d_res (optional) receives res itself.  Unlike the assembled tangent (the
+ * reference's approximate Jacobian), this differentiates tauM, tauC, tauBar,
+ * uBar and the flux projection as well. */
+int crimson_elmgmr_vjp(crimson_ctx* ctx, const double* d_y, const double* d_ac, const double* coef1,
+                       const double* coef2, const double* d_lambda, double* d_res, double* d_ybar, double* d_acbar,
+                       double* mubar, double* coef1bar, double* coef2bar);
+
+/* ---------------------------------------------------------------------------
  * Device-resident time step: itrdrv_iter_step (flowsolver/src/itrdrv.f90:1239)
  * = itrPredict, itrBC, nitr x [itrYAlpha, ElmGMR, SolFlow pack + memLS_SOLVE,
  * itrCorrect, itrBC], with RCR outlets (flowsolver/src/RCR.cxx:49-81).
@@ -202,6 +227,10 @@ typedef struct {
 int crimson_set_inflow(crimson_ctx* ctx, int ninlet, const int* nodes, const double* profile);
 /* RCR outlets on the coupled surfaces, in srflist order */
 int crimson_set_rcr(crimson_ctx* ctx, int n, const double* Rp, const double* C, const double* Rd, const double* Pd);
+/* RCR history (P_n, Q_n per coupled surface, the AbstractBoundaryCondition
+ * state, flowsolver/src/AbstractBoundaryCondition.cxx:55-91): read (set = 0)
+ * or write (set = 1), e.g. to restart from a checkpoint. */
+int crimson_rcr_state(crimson_ctx* ctx, int n, double* Pn, double* Qn, int set);
 /* yold/acold in the reference layout (nshg, 4) */
 int crimson_state_set(crimson_ctx* ctx, const double* y, const double* ac);
 int crimson_state_get(crimson_ctx* ctx, double* y, double* ac);
