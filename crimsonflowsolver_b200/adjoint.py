@@ -14,12 +14,11 @@ with RCR outlets, flowsolver/src/RCR.cxx:49-81):
   with y = y_n + gamma dt a - (gamma - 1) dt a_n, and the equations are
   res(y_alpha, a_alpha; mu, c1, c2) = 0 on the free rows (res is what ElmGMR
   assembles; c1, c2 the RCR implicit coefficients from P_n, Q_n);
-* the adjoint solve J^T lambda = xbar uses the exact transposed Jacobian
-  product ``crimson_elmgmr_vjp`` and, as its preconditioner, the transposed
-  memLS solve with the assembled (approximate) tangent,
-  ``crimson_solflow_device_transposed``, in a defect-correction loop
-  lambda <- lambda - A^-T (xbar - J^T lambda) (A ~ -J, as the forward Newton
-  step uses it);
+* the adjoint solve J^T lambda = xbar is flexible GMRES on the exact
+  transposed Jacobian product ``crimson_elmgmr_vjp``, right-preconditioned
+  by the transposed memLS solve with the assembled (approximate) tangent,
+  ``crimson_solflow_device_transposed`` (-A^-T ~ J^-T: A ~ -J, as the
+  forward Newton step uses it);
 * the RCR update P_{n+1} = d1 Q_{n+1} + h1(P_n, Q_n) and the coupling
   coefficients are differentiated by hand (``rcr_coeffs``).
 
@@ -319,19 +318,14 @@ class _AdjointContext:
         # assembled tangent at the converged state (the preconditioner)
         self.F.elm.device(ya, aa, self.res, self.lhsK, self.lhsP, list(c1), list(c2), lhs=True)
         t.cuda.synchronize()
-        # 5. J~^T lambda = xbar by defect correction around the transposed solve
+        # 5. J~^T lambda = xbar: flexible GMRES on the exact J~^T, right
+        #    preconditioned by the transposed memLS solve (-A^-T ~ J~^-T)
         bn = float(t.linalg.norm(xbar))
-        lam = t.zeros_like(xbar)
         its = 0
         if bn > 0.0:
-            r_ = xbar.clone()
-            for its in range(1, maxit + 1):
-                delta = self._solve_t(r_, faceRes)
-                lam = lam - delta
-                jt, mub, c1b, c2b = self._jt(ya, aa, c1, c2, lam)
-                r_ = xbar - jt
-                if float(t.linalg.norm(r_)) <= tol * bn:
-                    break
+            lam, its = _fgmres(lambda v: self._jt(ya, aa, c1, c2, v)[0], lambda v: -self._solve_t(v, faceRes),
+                               xbar, tol, maxit, t)
+            jt, mub, c1b, c2b = self._jt(ya, aa, c1, c2, lam)
             # 6. z_bar -= (d G / d z)^T lambda
             yba = self.ybar
             aba = self.abar
@@ -347,6 +341,48 @@ class _AdjointContext:
                 Pb_prev[k] += c2bar * doP
                 Qb_prev[k] += c2bar * doQ
         return yb_prev, ab_prev, Pb_prev, Qb_prev, its
+
+
+def _fgmres(apply_a, apply_m, b, tol, maxit, t):
+    """Flexible GMRES (right preconditioning that may change per step: the
+    preconditioner is itself an iterative solve) for a(x) = b, from x = 0.
+    Orthogonalisation by modified Gram-Schmidt; the small least-squares
+    problem is solved on the host in FP64.  Restarts every 30 steps; stops at
+    |b - a(x)| <= tol |b| or after maxit steps.  Returns (x, steps)."""
+    bn = float(t.linalg.norm(b))
+    x = t.zeros_like(b)
+    steps = 0
+    restart = 30
+    r = b.clone()
+    while steps < maxit:
+        beta = float(t.linalg.norm(r))
+        if beta <= tol * bn:
+            break
+        V = [r / beta]
+        Z = []
+        m = min(restart, maxit - steps)
+        H = np.zeros((m + 1, m))
+        y = None
+        for j in range(m):
+            z = apply_m(V[j])
+            Z.append(z)
+            w = apply_a(z)
+            for i in range(j + 1):
+                H[i, j] = float((w * V[i]).sum())
+                w = w - H[i, j] * V[i]
+            H[j + 1, j] = float(t.linalg.norm(w))
+            steps += 1
+            e1 = np.zeros(j + 2)
+            e1[0] = beta
+            y, *_ = np.linalg.lstsq(H[:j + 2, :j + 1], e1, rcond=None)
+            res = float(np.linalg.norm(e1 - H[:j + 2, :j + 1] @ y))
+            if res <= tol * bn or H[j + 1, j] == 0.0:
+                break
+            V.append(w / H[j + 1, j])
+        for i in range(len(y)):
+            x = x + float(y[i]) * Z[i]
+        r = b - apply_a(x)
+    return x, steps
 
 
 def make_objective_function():
