@@ -419,6 +419,56 @@ def run_cg_capture(args):
     F.close()
 
 
+def run_adjoint(args):
+    """Gradient of the outlet-pressure misfit on a multi-outlet cylinder.
+
+    Workload: cylinder (R 1 cm, L 10 cm) whose distal cap is split into 3 RCR
+    outlets (Rp 100 / 120 / 100, C 1e-4 / 1.2e-4 / 1e-4, Rd 1000 / 1000 /
+    900), pulsatile inflow, --adj-steps steps of dt 1e-3 with 10 nonlinear
+    iterations each (converged), checkpoint every 10 steps; objective
+    sum_k (mean_n P_k(t_n) - T_k)^2 with T = (2, 3, 1.5) x 1e3.  Times the
+    forward pass alone and the full gradient (forward + recomputation +
+    adjoint), and checks --adj-fd components against central differences
+    with relative step 1e-6.
+    """
+    import torch
+
+    from crimsonflowsolver_b200 import FlowParams, RCR, mesh
+    from crimsonflowsolver_b200.adjoint import AdjointProblem
+
+    m = mesh.cylinder(ncross=args.ncross, naxial=args.naxial, seed=1, n_outlets=3)
+    P = FlowParams(rcr=[RCR(srfid=3), RCR(srfid=4, Rp=120.0, C=1.2e-4), RCR(srfid=5, Rd=900.0)], nitr=10)
+    prob = AdjointProblem(m, P, targets=[2.0e3, 3.0e3, 1.5e3], nsteps=args.adj_steps, inflow=_inflow,
+                          checkpoint_every=10)
+    th = prob.theta0()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J0 = prob.objective(th)
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    J, g = prob.gradient(th)
+    t_grad = time.perf_counter() - t0
+    its = prob.last_stats["adjoint_iterations"]
+    comps = [int(c) for c in args.adj_fd.split(",") if c != ""]
+    fd = {}
+    for i in comps:
+        h = 1e-6 * abs(th[i])
+        tp, tm = th.copy(), th.copy()
+        tp[i] += h
+        tm[i] -= h
+        fd[i] = (prob.objective(tp) - prob.objective(tm)) / (2 * h)
+    names = ["mu"] + [f"{p}_{k + 1}" for k in range(3) for p in ("Rp", "C", "Rd")]
+    line = {"workload": f"adjoint: {m.nelem}-tet cylinder, 3 RCR outlets, {args.adj_steps} steps, checkpoint 10, "
+                        "10 nonlinear iterations/step, FP64",
+            "tets": m.nelem, "nodes": m.nshg, "J": J, "J_forward_only": J0,
+            "forward_s": t_fwd, "gradient_s": t_grad, "gradient_over_forward": t_grad / t_fwd,
+            "adjoint_krylov_iterations_per_step": float(np.mean(its)),
+            "gradient": dict(zip(names, g.tolist())),
+            "fd_check": {names[i]: {"adjoint": float(g[i]), "central_fd": float(fd[i]),
+                                    "rel_err": float(abs(g[i] - fd[i]) / abs(fd[i]))} for i in comps}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -435,9 +485,15 @@ def main():
                     help="run the small fixed-iteration CG case for profiler captures instead of the benchmark")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"], help="--cg-capture only")
     ap.add_argument("--cg-iters", type=int, default=50, help="--cg-capture only")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="run the adjoint-gradient workload (multi-outlet cylinder) instead of the benchmark")
+    ap.add_argument("--adj-steps", type=int, default=100, help="--adjoint only")
+    ap.add_argument("--adj-fd", default="0,1", help="--adjoint only: theta components checked by central FD")
     args = ap.parse_args()
     if args.cg_capture:
         run_cg_capture(args)
+    elif args.adjoint:
+        run_adjoint(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
