@@ -112,13 +112,27 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def make_problem(ncross: int, naxial: int, epstol_ns: float = None):
+def make_problem(ncross: int, naxial: int, epstol_ns: float = None, workload: str = "cylinder",
+                 ybif_h: float = 0.036):
     from crimsonflowsolver_b200 import FlowParams, RCR, mesh
 
+    tol = EPSTOL_NS if epstol_ns is None else epstol_ns
+    if workload == "ybif":
+        m = mesh.bifurcation(h=ybif_h, seed=3)
+        P = FlowParams(rcr=[RCR(**d) for d in mesh.bifurcation_rcr(seed=3)], nitr=NITR, epstol_ns=tol)
+        return m, P
     m = mesh.cylinder(ncross=ncross, naxial=naxial, seed=1)
-    P = FlowParams(rcr=[RCR(srfid=3, Rp=100.0, C=1e-4, Rd=1000.0)], nitr=NITR,
-                   epstol_ns=EPSTOL_NS if epstol_ns is None else epstol_ns)
+    P = FlowParams(rcr=[RCR(srfid=3, Rp=100.0, C=1e-4, Rd=1000.0)], nitr=NITR, epstol_ns=tol)
     return m, P
+
+
+def workload_name(args, m) -> str:
+    if args.workload == "ybif":
+        return (f"{m.nelem / 1e6:.1f}M-tet Y-bifurcation ({m.nelem} tets, {m.nshg} nodes; parent R 1 cm, daughters "
+                "R 0.7 cm at +-30 deg, 2 RCR outlets +-20% seeded), pulsatile inflow, dt=1e-3, 3 nonlinear "
+                "iterations/step")
+    return (f"4.0M-tet cylinder ({m.nelem} tets, {m.nshg} nodes), pulsatile inflow, RCR outlet, dt=1e-3, "
+            "3 nonlinear iterations/step")
 
 
 def cpu_sample(m, P, nthreads: int, iters=None):
@@ -140,9 +154,11 @@ def cpu_sample(m, P, nthreads: int, iters=None):
     full = ((m.iBC >> 3) & 7) == 7
     y[full, 0:3] = m.BC[full, 2:5]
     ac = np.zeros_like(y)
-    c1, c2 = po.rcr_coeffs(100.0, 1e-4, 1000.0, 0.0, 0.0, 0.0, 0.0, P.alfi * P.Delt)
+    cc = [po.rcr_coeffs(r.Rp, r.C, r.Rd, r.Pd, r.Pd, 0.0, 0.0, P.alfi * P.Delt) for r in P.rcr]
+    c1 = [c[0] for c in cc]
+    c2 = [c[1] for c in cc]
     t0 = time.perf_counter()
-    out = elm(y, ac, srflist=[3], coef1=[c1], coef2=[c2])
+    out = elm(y, ac, srflist=[r.srfid for r in P.rcr], coef1=c1, coef2=c2)
     t_elm = time.perf_counter() - t0
     t0 = time.perf_counter()
     Res4, Val4 = po.solflow_pack(m.nshg, colm, rowp, out["res"], out["lhsK"], out["lhsP"])
@@ -150,13 +166,14 @@ def cpu_sample(m, P, nthreads: int, iters=None):
     from crimsonflowsolver_b200 import FlowParams
 
     P1 = FlowParams(**{**P.__dict__, "nprjs": 1})
-    ms = po.MemLS(m.nshg, colm, rowp, 2, P1, nthreads=nthreads)
+    ms = po.MemLS(m.nshg, colm, rowp, 1 + len(P.rcr), P1, nthreads=nthreads)
     nodes, sv = po.dirichlet_face(m)
     ms.bc_create(1, nodes, 3, 0, sv)
-    nn, vv = po.neumann_face(m, 3)
-    ms.bc_create(2, nn, 3, 1, vv)
+    for k, r in enumerate(P.rcr):
+        nn, vv = po.neumann_face(m, r.srfid)
+        ms.bc_create(2 + k, nn, 3, 1, vv)
     t0 = time.perf_counter()
-    _, st = ms.solve(Res4, Val4, [0.0, c1 * P.alfi * P.gami * P.Delt])
+    _, st = ms.solve(Res4, Val4, [0.0] + [c * P.alfi * P.gami * P.Delt for c in c1])
     t_solve = time.perf_counter() - t0
     t_gm = st.GM.callD / max(st.GM.itr, 1)
     t_cg = st.CG.callD / max(st.CG.itr, 1)
@@ -173,7 +190,7 @@ def run_reference(args):
     if rank != 0:
         return
     nthreads = os.cpu_count() or 1
-    m, P = make_problem(args.ncross, args.naxial, args.epstol_ns)
+    m, P = make_problem(args.ncross, args.naxial, args.epstol_ns, args.workload, args.ybif_h)
     vals = []
     for i in range(args.warmup + args.steps):
         v, sample, wall = cpu_sample(m, P, nthreads)
@@ -183,8 +200,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": value, "unit": "s/timestep", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"4.0M-tet cylinder ({m.nelem} tets, {m.nshg} nodes), pulsatile inflow, RCR "
-                                   "outlet, dt=1e-3, 3 nonlinear iterations/step, FP64",
+            "config": {"workload": workload_name(args, m) + ", FP64",
                        "parallelism": "replicas"},
             "cpu_baseline": {"value": value, "unit": "s/timestep", "cores": nthreads, "kind": "port",
                              "sample": sample},
@@ -218,18 +234,31 @@ def _timed_steps(F, args, stream, local, dist):
         e1.record(stream)
         torch.cuda.synchronize()
     launches = L.crimson_launch_count() - l0
-    t_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
-        dist.barrier()
+    t_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     it = np.array([s for step in iters for s in step], dtype=float)
     per_solve = {"ri": float(it[:, 0].mean()), "gm": float(it[:, 1].mean()), "cg": float(it[:, 2].mean())}
     if it[:, 3].max() > 0:
         per_solve["refine_sweeps"] = float(it[:, 3].mean())
         per_solve["max_final_defect"] = float(it[:, 4].max())
     return t_ms, per_solve, int(launches), clk.summary()
+
+
+def max_over_ranks(t_ms: float, dist, device: str) -> float:
+    """The slowest rank's time: replicas run independently, so the job's time
+    is the maximum (every rank takes the same collective steps)."""
+    if not dist:
+        return t_ms
+    import torch
+
+    t = torch.tensor([t_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    return float(t.item())
+
+
+def replica_value(t_ms: float, steps: int, world_size: int) -> float:
+    """s/timestep of the whole job: every replica's steps count (weak scaling)."""
+    return t_ms / 1e3 / (steps * world_size)
 
 
 def _relerr(a, b):
@@ -270,7 +299,7 @@ def run_ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     L = N.lib()
-    m, P = make_problem(args.ncross, args.naxial, args.epstol_ns)
+    m, P = make_problem(args.ncross, args.naxial, args.epstol_ns, args.workload, args.ybif_h)
     n = m.nshg
     # ---- FP64 (memLS arithmetic) ----
     F64 = solver.FlowSolver(m, P, inflow=_inflow)
@@ -285,8 +314,8 @@ def run_ours(args):
     ym, _ = FM.state()
     acc = {"velocity": _relerr(ym[:, 0:3], y64[:, 0:3]), "pressure": _relerr(ym[:, 3], y64[:, 3]),
            "after_steps": args.warmup + args.steps}
-    value = tm_ms / 1e3 / (args.steps * ws)
-    v64 = t64_ms / 1e3 / (args.steps * ws)
+    value = replica_value(tm_ms, args.steps, ws)
+    v64 = replica_value(t64_ms, args.steps, ws)
     # ---- end to end through the host-buffer API (mixed): state in from pinned host, step, state out ----
     y_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
     ac_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
@@ -346,8 +375,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": tm_ms / args.steps, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 matrices in inner Krylov matvecs, f64 vectors/reductions/refinement",
         "data": "synthetic",
-        "config": {"workload": f"4.0M-tet cylinder ({m.nelem} tets, {n} nodes, {nnz} blocks), pulsatile inflow, "
-                               "RCR outlet, dt=1e-3, 3 nonlinear iterations/step, mixed-precision NS solve",
+        "config": {"workload": workload_name(args, m) + f", {nnz} blocks, mixed-precision NS solve",
                    "parallelism": "replicas" if ws > 1 else "single GPU",
                    "epstol_ns": P.epstol_ns, "epstol_gmres_cg": [P.epstol_mom, P.epstol_cont],
                    "mixed_refine_tol": Pm.refine_tol if Pm.refine_tol > 0 else P.epstol_ns,
@@ -469,6 +497,93 @@ def run_adjoint(args):
     print(json.dumps(line), flush=True)
 
 
+def run_microbench(args):
+    """Assembly / SpMV microbenchmark on a jittered lattice of linear tets.
+
+    Workload: --lattice n gives 6 n^3 tets on an (n+1)^3-node jittered unit
+    lattice (n = 139: 16.1M tets, 2.74M nodes), nodal y = (u, v, w, p) and ac
+    ~ N(0, 1) (seeded).  Measures ElmGMR residual + tangent assembly (Melem/s)
+    and the 4x4 block SpMV (SPARMULVV, dof 4) on the assembled pattern with
+    N(0, 1) blocks, FP64 and FP32, each against the HBM roofline, with CUDA
+    events on the library stream.
+    """
+    import ctypes
+
+    import torch
+
+    from crimsonflowsolver_b200 import FlowParams
+    from crimsonflowsolver_b200 import _native as N
+    from crimsonflowsolver_b200 import mesh, solver
+
+    L = N.lib()
+    m = mesh.lattice(args.lattice, seed=5)
+    P = FlowParams()
+    elm = solver.ElmGMR(m, P)
+    nnz = elm._nnz()
+    n = m.nshg
+    stream = torch.cuda.ExternalStream(elm.stream_handle)
+    y, ac = mesh.random_state(n, seed=5)
+    dev = "cuda"
+    dy = torch.tensor(y, device=dev)
+    dac = torch.tensor(ac, device=dev)
+    res = torch.empty((n, 4), dtype=torch.float64, device=dev)
+    K = torch.empty((nnz, 9), dtype=torch.float64, device=dev)
+    Pm = torch.empty((nnz, 4), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps / 1e3
+
+    peak, peak_src = _peaks()
+    t_asm = timed(lambda: elm.device(dy, dac, res, K, Pm, lhs=True), 5)
+    t_res = timed(lambda: elm.device(dy, dac, res, None, None, lhs=False), 5)
+    rec = torch.empty((nnz, 16), dtype=torch.float32, device=dev)
+    t_asm32 = timed(lambda: N.check(L.crimson_elmgmr_device_f32(elm.h, ctypes.c_void_p(dy.data_ptr()),
+                                                                ctypes.c_void_p(dac.data_ptr()), None, None,
+                                                                ctypes.c_void_p(res.data_ptr()),
+                                                                ctypes.c_void_p(rec.data_ptr())), "f32"), 5)
+    del rec
+    asm_bytes = (2416 + 560) * m.nelem
+    asm32_bytes = (624 + 128 + 16 * 13 * 4 + 560) * m.nelem
+    out = {"workload": f"lattice {args.lattice}^3 x 6: {m.nelem} tets, {n} nodes, {nnz} blocks; y, ac ~ N(0,1)",
+           "peak_gbs": peak, "peak_source": peak_src,
+           "assembly_fp64": {"ms": t_asm * 1e3, "melem_s": m.nelem / t_asm / 1e6,
+                             "algorithmic_bytes_per_elem": 2976, "achieved_gbs": asm_bytes / t_asm / 1e9,
+                             "frac": asm_bytes / t_asm / 1e9 / peak},
+           "assembly_fp32_tangent": {"ms": t_asm32 * 1e3, "melem_s": m.nelem / t_asm32 / 1e6,
+                                     "algorithmic_bytes_per_elem": 2144,
+                                     "achieved_gbs": asm32_bytes / t_asm32 / 1e9,
+                                     "frac": asm32_bytes / t_asm32 / 1e9 / peak},
+           "residual_only_fp64": {"ms": t_res * 1e3, "melem_s": m.nelem / t_res / 1e6}}
+    g = torch.Generator(device=dev).manual_seed(5)
+    val = torch.randn((nnz, 16), dtype=torch.float64, device=dev, generator=g)
+    u = torch.randn((n, 4), dtype=torch.float64, device=dev, generator=g)
+    for prec, dt, bb, br in ((0, torch.float64, 132, 72), (1, torch.float32, 68, 40)):
+        v = val.to(dt).contiguous()
+        uu = u.to(dt).contiguous()
+        ku = torch.empty_like(uu)
+        torch.cuda.synchronize()
+        N.check(L.crimson_spmv4_prepare(elm.h, prec, ctypes.c_void_p(v.data_ptr())), "crimson_spmv4_prepare")
+        t = timed(lambda: N.check(L.crimson_spmv4_apply(elm.h, ctypes.c_void_p(uu.data_ptr()),
+                                                        ctypes.c_void_p(ku.data_ptr())), "crimson_spmv4_apply"), 20)
+        byt = nnz * bb + n * br
+        out["spmv4_" + ("fp64" if prec == 0 else "fp32")] = {
+            "ms": t * 1e3, "algorithmic_bytes": byt, "achieved_gbs": byt / t / 1e9, "frac": byt / t / 1e9 / peak}
+        del v, uu, ku
+    elm.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -478,22 +593,34 @@ def main():
     ap.add_argument("--ncross", type=int, default=NCROSS)
     ap.add_argument("--naxial", type=int, default=NAXIAL)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--workload", default="cylinder", choices=["cylinder", "ybif"],
+                    help="cylinder: 4.0M-tet tube, 1 RCR outlet (default); ybif: ~3.9M-tet Y-bifurcation, 2 RCR "
+                         "outlets, mixed arm refined to 1e-8")
+    ap.add_argument("--ybif-h", type=float, default=0.036, help="grid spacing of the Y-bifurcation (cm)")
     ap.add_argument("--epstol-ns", type=float, default=EPSTOL_NS, help="NSSOLVER relative tolerance, both arms")
-    ap.add_argument("--refine-tol", type=float, default=REFINE_TOL,
-                    help="mixed precision FP64 defect target (0: the NSSOLVER tolerance)")
+    ap.add_argument("--refine-tol", type=float, default=None,
+                    help="mixed precision FP64 defect target (0: the NSSOLVER tolerance; default 0 for the "
+                         "cylinder, 1e-8 for the Y-bifurcation)")
     ap.add_argument("--cg-capture", action="store_true",
                     help="run the small fixed-iteration CG case for profiler captures instead of the benchmark")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"], help="--cg-capture only")
     ap.add_argument("--cg-iters", type=int, default=50, help="--cg-capture only")
+    ap.add_argument("--microbench", action="store_true",
+                    help="run the lattice assembly / 4x4 SpMV microbenchmark instead of the benchmark")
+    ap.add_argument("--lattice", type=int, default=139, help="--microbench only: lattice cells per side")
     ap.add_argument("--adjoint", action="store_true",
                     help="run the adjoint-gradient workload (multi-outlet cylinder) instead of the benchmark")
     ap.add_argument("--adj-steps", type=int, default=100, help="--adjoint only")
     ap.add_argument("--adj-fd", default="0,1", help="--adjoint only: theta components checked by central FD")
     args = ap.parse_args()
+    if args.refine_tol is None:
+        args.refine_tol = 1e-8 if args.workload == "ybif" else REFINE_TOL
     if args.cg_capture:
         run_cg_capture(args)
     elif args.adjoint:
         run_adjoint(args)
+    elif args.microbench:
+        run_microbench(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -89,6 +89,12 @@ SIGNATURES = {
     "crimson_elmgmr_vjp": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_dbl_p, c_dbl_p, c_void_p, c_void_p,
                                           c_void_p, c_void_p, c_dbl_p, c_dbl_p, c_dbl_p]),
     "crimson_rcr_state": (ctypes.c_int, [c_void_p, ctypes.c_int, c_dbl_p, c_dbl_p, ctypes.c_int]),
+    "crimson_spmv4_prepare": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p]),
+    "crimson_elmgmr_device_f32": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_dbl_p, c_dbl_p, c_void_p,
+                                                 c_void_p]),
+    "crimson_solflow_device_f32": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int_p,
+                                                  c_dbl_p, c_void_p, ctypes.POINTER(LsStats)]),
+    "crimson_spmv4_apply": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
     "crimson_set_inflow": (ctypes.c_int, [c_void_p, ctypes.c_int, c_int_p, c_dbl_p]),
     "crimson_set_rcr": (ctypes.c_int, [c_void_p, ctypes.c_int, c_dbl_p, c_dbl_p, c_dbl_p, c_dbl_p]),
     "crimson_state_set": (ctypes.c_int, [c_void_p, c_dbl_p, c_dbl_p]),

@@ -27,7 +27,7 @@
 namespace crimson {
 
 int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1, const double* coef2,
-                  double* d_res, double* d_lhsK, double* d_lhsP, int lhs);
+                  double* d_res, double* d_lhsK, double* d_lhsP, int lhs, float* d_lhs32 = nullptr);
 
 // ---------------------------------------------------------------------------
 // Forward-mode dual numbers

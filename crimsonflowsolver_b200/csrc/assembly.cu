@@ -211,12 +211,24 @@ __global__ void k_qpbc(double* __restrict__ qres, double* __restrict__ rmass, in
 // ---------------------------------------------------------------------------
 constexpr int kQ = 28;   // doubles of per-point data exchanged in shared memory
 
-template <bool kLhs>
+// FP32 vector reduction (sm_90+): one instruction adds four floats at a
+// 16-byte aligned address.
+__device__ __forceinline__ void red_add_v4(float* p, float a, float b, float c, float d) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
+
+// kLhs: 0 residual only; 1 residual + FP64 tangent (lhsK, lhsP); 2 residual
+// (FP64) + FP32 tangent records (16 floats per block: K(9), P(4), 3 zero
+// pads), whose quadrature sums are formed in FP32 and scattered with 4-wide
+// vector reductions.
+template <int kLhs>
 __global__ void __launch_bounds__(128) k_asigmr(const int4* __restrict__ ien, const double4* __restrict__ x,
                                                 const double4* __restrict__ y, const double4* __restrict__ ac,
                                                 const double* __restrict__ qres, const int* __restrict__ epos,
                                                 int nelem, ElmParams P, double* __restrict__ res,
-                                                double* __restrict__ lhsK, double* __restrict__ lhsP) {
+                                                double* __restrict__ lhsK, double* __restrict__ lhsP,
+                                                float* __restrict__ lhs32) {
     __shared__ double sq[128][kQ];
     const int lane4 = threadIdx.x & 3;
     const int gbase = threadIdx.x & ~3;   // first thread of this element's group
@@ -397,7 +409,53 @@ __global__ void __launch_bounds__(128) k_asigmr(const int4* __restrict__ ien, co
                 atomicAdd(r + i, -WdetJ * v);
             }
             atomicAdd(r + 3, WdetJ * div_ub);
-            if (kLhs) {
+            if (kLhs == 2) {
+                const float rhof = (float)rho, muf = (float)mu;
+                const float lhsFct = (float)(P.alfi * P.gami * P.Delt);
+                const float tlW = lhsFct * (float)WdetJ;
+                const float tsFct = (float)P.almi * (float)WdetJ * rhof;
+                float TC = 0.f, TM = 0.f, aqa[4], bqa[4], tMq[4], tBq[4], Naf[4];
+#pragma unroll
+                for (int qq = 0; qq < 4; ++qq) {
+                    const double* Sx = Sq[qq];
+                    aqa[qq] = (float)Sx[a];
+                    bqa[qq] = (float)Sx[4 + a];
+                    tMq[qq] = (float)Sx[12];
+                    tBq[qq] = (float)Sx[13];
+                    TC += (float)Sx[14];
+                    TM += (float)Sx[12];
+                    Naf[qq] = (float)Na[qq];
+                }
+                float sga[3] = {(float)shg[a][0], (float)shg[a][1], (float)shg[a][2]};
+                const int* ep = epos + 16 * e + 4 * a;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    float conv = 0.f, sym = 0.f;
+#pragma unroll
+                    for (int qq = 0; qq < 4; ++qq) {
+                        const double* Sx = Sq[qq];
+                        conv += Naf[qq] * (float)Sx[8 + b];
+                        sym += tMq[qq] * rhof * aqa[qq] * (float)Sx[b] + tBq[qq] * bqa[qq] * (float)Sx[4 + b];
+                    }
+                    const float sgb[3] = {(float)shg[b][0], (float)shg[b][1], (float)shg[b][2]};
+                    const float grad = sga[0] * sgb[0] + sga[1] * sgb[1] + sga[2] * sgb[2];
+                    const float Kd = tsFct * (float)c_el.M[a][b] + tlW * (rhof * conv + 4.0f * muf * grad + sym);
+                    const float tc = tlW * TC, tm = tlW * 4.0f * muf;
+                    float K[9];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j)
+                            K[3 * i + j] = (i == j ? Kd : 0.f) + tc * sgb[i] * sga[j] + tm * sgb[j] * sga[i];
+                    const float sn = tlW * (float)c_el.SN[a];
+                    float* rec = lhs32 + 16 * (size_t)ep[b];
+                    red_add_v4(rec + 0, K[0], K[1], K[2], K[3]);
+                    red_add_v4(rec + 4, K[4], K[5], K[6], K[7]);
+                    red_add_v4(rec + 8, K[8], sn * sgb[0], sn * sgb[1], sn * sgb[2]);
+                    atomicAdd(rec + 12, tlW / rhof * TM * grad);
+                }
+            }
+            if (kLhs == 1) {
                 const double lhsFct = P.alfi * P.gami * P.Delt;
                 const double tlW = lhsFct * WdetJ;
                 const double tsFct = P.almi * WdetJ * rho;
@@ -609,7 +667,7 @@ static int upload_offsets(crimson_ctx* c, DBuf<int>& doff) {
 }
 
 int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1, const double* coef2,
-                  double* d_res, double* d_lhsK, double* d_lhsP, int lhs) {
+                  double* d_res, double* d_lhsK, double* d_lhsP, int lhs, float* d_lhs32) {
     cudaStream_t s = c->stream;
     CR_CHECK(upload_elm_consts(s));
     const ElmParams P = elm_params(c->p);
@@ -625,18 +683,23 @@ int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const d
         launch(k_qpbc, grid_for(c->nshg, 256), 256, 0, s, c->qres.p, c->rmass.p, c->nshg);
     }
     CR_CUDA(cudaMemsetAsync(d_res, 0, sizeof(double) * 4 * (size_t)c->nshg, s));
-    if (lhs) {
+    if (lhs == 2) {
+        CR_CUDA(cudaMemsetAsync(d_lhs32, 0, sizeof(float) * 16 * (size_t)c->nnz, s));
+    } else if (lhs) {
         CR_CUDA(cudaMemsetAsync(d_lhsK, 0, sizeof(double) * 9 * (size_t)c->nnz, s));
         CR_CUDA(cudaMemsetAsync(d_lhsP, 0, sizeof(double) * 4 * (size_t)c->nnz, s));
     }
     const int blk = 128;
     const int grid = grid_for((long long)c->nelem * 4, blk, 16);
-    if (lhs)
-        launch(k_asigmr<true>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
-                                            d_lhsK, d_lhsP);
+    if (lhs == 2)
+        launch(k_asigmr<2>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
+               nullptr, nullptr, d_lhs32);
+    else if (lhs)
+        launch(k_asigmr<1>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
+               d_lhsK, d_lhsP, nullptr);
     else
-        launch(k_asigmr<false>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
-                                             nullptr, nullptr);
+        launch(k_asigmr<0>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
+               nullptr, nullptr, nullptr);
     CR_CUDA(cudaGetLastError());
     if (c->nface > 0)
         launch(k_asbmfg, grid_for(c->nface, 128), 128, 0, s, c->ienb.p, c->iBCB.p, c->BCB.p, c->x.p, y4, c->nface, P,

@@ -31,12 +31,14 @@ int pattern_aux(crimson_lhs* L);
 int memls_kernel_time(crimson_lhs* L, int which, int reps, double* ms);
 int pattern_to_host(crimson_ctx* c, int* colm, int* rowp, long long cap);
 int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1, const double* coef2,
-                  double* d_res, double* d_lhsK, double* d_lhsP, int lhs);
+                  double* d_res, double* d_lhsK, double* d_lhsP, int lhs, float* d_lhs32 = nullptr);
 int memls_solve_val(crimson_lhs* L, crimson_ls* ls, double* Ri, double* Val, const int* incL, const double* res,
                     crimson_ls_stats* st);
 int memls_solve_lhs_device(crimson_lhs* L, crimson_ls* ls, const double* d_res, const double* d_lhsK,
                            const double* d_lhsP, const int* incL, const double* faceRes, double* d_sol,
-                           crimson_ls_stats* st, bool transpose = false);
+                           crimson_ls_stats* st, bool transpose = false, const float* d_lhs32 = nullptr);
+int spmv4_prepare(crimson_ctx* c, int precision, const void* d_val);
+int spmv4_apply(crimson_ctx* c, const void* d_u, void* d_ku);
 int elmgmr_vjp(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1, const double* coef2,
                const double* d_lam, double* d_res, double* d_ybar, double* d_abar, double* mubar, double* c1bar,
                double* c2bar);
@@ -537,6 +539,35 @@ int crimson_solflow_device_transposed(crimson_ctx* c, crimson_lhs* L, crimson_ls
     return memls_solve_lhs_device(L, ls, d_rhs, d_lhsK, d_lhsP, incL, faceRes, d_sol, stats, true);
 }
 
+int crimson_elmgmr_device_f32(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1,
+                              const double* coef2, double* d_res, float* d_lhs32) {
+    if (!c || !d_y || !d_ac || !d_res || !d_lhs32) return CRIMSON_ERR_ARG;
+    if (c->ncoupled > 0 && (!coef1 || !coef2)) return CRIMSON_ERR_ARG;
+    CR_CHECK(check_params(&c->p));
+    if (c->nnz == 0) CR_CHECK(build_pattern(c));
+    return elmgmr_device(c, d_y, d_ac, coef1, coef2, d_res, nullptr, nullptr, 2, d_lhs32);
+}
+
+int crimson_solflow_device_f32(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const double* d_res,
+                               const float* d_lhs32, const int* incL, const double* faceRes, double* d_solinc,
+                               crimson_ls_stats* stats) {
+    if (!c || !L || !ls || !d_res || !d_lhs32 || !d_solinc) return CRIMSON_ERR_ARG;
+    if (L->diag == nullptr || L->trans == nullptr) return CRIMSON_ERR_STATE;
+    return memls_solve_lhs_device(L, ls, d_res, nullptr, nullptr, incL, faceRes, d_solinc, stats, false, d_lhs32);
+}
+
+int crimson_spmv4_prepare(crimson_ctx* c, int precision, const void* d_val) {
+    if (!c || !d_val || (precision != CRIMSON_FP64 && precision != CRIMSON_MIXED)) return CRIMSON_ERR_ARG;
+    if (c->nnz == 0) CR_CHECK(build_pattern(c));
+    return spmv4_prepare(c, precision, d_val);
+}
+
+int crimson_spmv4_apply(crimson_ctx* c, const void* d_u, void* d_ku) {
+    if (!c || !d_u || !d_ku) return CRIMSON_ERR_ARG;
+    if (!c->s4_ptr.p) return CRIMSON_ERR_STATE;
+    return spmv4_apply(c, d_u, d_ku);
+}
+
 int crimson_elmgmr_vjp(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1,
                        const double* coef2, const double* d_lambda, double* d_res, double* d_ybar, double* d_acbar,
                        double* mubar, double* coef1bar, double* coef2bar) {
@@ -651,10 +682,20 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
     for (int it = 0; it < args->nitr; ++it) {
         launch(k_yalpha, grid_for(n, 256), 256, 0, s, c->yold.p, c->acold.p, c->ycur.p, c->accur.p, c->yalpha.p,
                                                   c->acalpha.p, n, P.alfi, P.almi);
-        CR_CHECK(elmgmr_device(c, c->yalpha.p, c->acalpha.p, c1.data(), c2.data(), c->res4.p, c->lhsK.p, c->lhsP.p, 1));
         crimson_ls_stats lst;
-        CR_CHECK(memls_solve_lhs_device(L, ls, c->res4.p, c->lhsK.p, c->lhsP.p, incL.data(), faceRes.data(),
-                                        c->solinc.p, &lst));
+        if (ls->precision == CRIMSON_MIXED) {
+            // FP32 element quadrature for the tangent, FP64 residual
+            CR_CHECK(c->lhs32.alloc(16 * (size_t)c->nnz));
+            CR_CHECK(elmgmr_device(c, c->yalpha.p, c->acalpha.p, c1.data(), c2.data(), c->res4.p, nullptr, nullptr, 2,
+                                   c->lhs32.p));
+            CR_CHECK(memls_solve_lhs_device(L, ls, c->res4.p, nullptr, nullptr, incL.data(), faceRes.data(),
+                                            c->solinc.p, &lst, false, c->lhs32.p));
+        } else {
+            CR_CHECK(elmgmr_device(c, c->yalpha.p, c->acalpha.p, c1.data(), c2.data(), c->res4.p, c->lhsK.p,
+                                   c->lhsP.p, 1));
+            CR_CHECK(memls_solve_lhs_device(L, ls, c->res4.p, c->lhsK.p, c->lhsP.p, incL.data(), faceRes.data(),
+                                            c->solinc.p, &lst));
+        }
         launch(k_correct, grid_for(n, 256), 256, 0, s, c->ycur.p, c->accur.p, c->solinc.p, n, P.gami * P.Delt,
                                                    P.gami * P.alfi * P.Delt);
         launch(k_itrbc, grid_for(n, 256), 256, 0, s, c->iBC.p, c->BC.p, nb, n, c->ycur.p);

@@ -178,12 +178,20 @@ struct crimson_ctx {
     crimson::DBuf<double> rmass;    // (nshg)
     crimson::DBuf<double> y4, ac4, res4;   // (4, nshg) staging for host-pointer calls
     crimson::DBuf<double> lhsK, lhsP;      // (9, nnz), (4, nnz)
+    crimson::DBuf<float> lhs32;            // (16, nnz) FP32 tangent records (mixed precision)
 
     // time stepping state (crimson_step)
     crimson::DBuf<double> yold, acold, ycur, accur, yalpha, acalpha, solinc, stage;
 
     // adjoint work space (crimson_elmgmr_vjp)
     crimson::DBuf<double> adj_res, adj_lam, adj_qbar, adj_scal;
+
+    // 4x4 block SpMV (crimson_spmv4_*): sliced pattern and values
+    crimson::DBuf<int> s4_ptr, s4_col;
+    long long s4_npad = 0;
+    int s4_nslice = 0, s4_prec = 0;
+    crimson::DBuf<double> s4_val64;
+    crimson::DBuf<float> s4_val32;
     crimson::DBuf<int> inlet_nodes;
     crimson::DBuf<double> inlet_profile;   // (ninlet, 3)
     int ninlet = 0;

@@ -663,12 +663,25 @@ __global__ void k_w_from_val(double* __restrict__ Val, const int* __restrict__ d
     }
 }
 
+// Tangent block j as ElmGMR produced it: FP64 lhsK (9, nnz) / lhsP (4, nnz),
+// or FP32 records of 16 floats (K(9), P(4), pads) when rec is not null.
+struct TangentIn {
+    const double* lhsK;
+    const double* lhsP;
+    const float* rec;
+    __device__ __forceinline__ double K(size_t j, int t) const {
+        return rec ? (double)rec[16 * j + t] : lhsK[9 * j + t];
+    }
+    __device__ __forceinline__ double P(size_t j, int t) const {
+        return rec ? (double)rec[16 * j + 9 + t] : lhsP[4 * j + t];
+    }
+};
+
 // W from lhsK / lhsP diagonals (fused SolFlow path; Val4 diagonal = K11,K22,K33,C)
-__global__ void k_w_from_lhs(const double* __restrict__ lhsK, const double* __restrict__ lhsP,
-                             const int* __restrict__ diag, double* __restrict__ W, int n) {
+__global__ void k_w_from_lhs(TangentIn T, const int* __restrict__ diag, double* __restrict__ W, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const size_t k = (size_t)diag[i];
-        double w[4] = {lhsK[9 * k + 0], lhsK[9 * k + 4], lhsK[9 * k + 8], lhsP[4 * k + 3]};
+        double w[4] = {T.K(k, 0), T.K(k, 4), T.K(k, 8), T.P(k, 3)};
         for (int d = 0; d < 4; ++d) {
             double v = w[d] == 0.0 ? 1.0 : w[d];
             W[4 * (size_t)i + d] = 1.0 / sqrt(fabs(v));
@@ -731,8 +744,7 @@ __global__ void k_gt(const double* __restrict__ mG, const int* __restrict__ tran
 //   Val4 rows 1-3 cols 1-3 = lhsK, col 4 rows 1-3 = -lhsP(1:3) of the
 //   transposed block, row 4 cols 1-3 = lhsP(1:3), (4,4) = lhsP(4)
 //   (solfar.f90:217-232), scaled by W(row) W(col) and split.
-__global__ void k_scale_split_lhs(const double* __restrict__ lhsK, const double* __restrict__ lhsP,
-                                  const int* __restrict__ rowptr, const int* __restrict__ col,
+__global__ void k_scale_split_lhs(TangentIn T, const int* __restrict__ rowptr, const int* __restrict__ col,
                                   const int* __restrict__ diag, const int* __restrict__ trans,
                                   const double* __restrict__ W, int n, double* __restrict__ mK,
                                   double* __restrict__ mG, double* __restrict__ mD, double* __restrict__ mL) {
@@ -741,13 +753,13 @@ __global__ void k_scale_split_lhs(const double* __restrict__ lhsK, const double*
         const int dg = diag[r];
         for (int j = rowptr[r]; j < rowptr[r + 1]; ++j) {
             const double* wc = W + 4 * (size_t)col[j];
-            const double* K = lhsK + 9 * (size_t)j;
-            const double* Pj = lhsP + 4 * (size_t)j;
-            const double* Pt = lhsP + 4 * (size_t)trans[j];
+            const size_t jj = (size_t)j, jt = (size_t)trans[j];
+            const double Pj[4] = {T.P(jj, 0), T.P(jj, 1), T.P(jj, 2), T.P(jj, 3)};
+            const double Pt[3] = {T.P(jt, 0), T.P(jt, 1), T.P(jt, 2)};
             double* k = mK + 9 * (size_t)j;
             for (int a = 0; a < 3; ++a)
                 for (int b = 0; b < 3; ++b) {
-                    double v = K[3 * a + b];
+                    double v = T.K(jj, 3 * a + b);
                     if (j == dg && a == b && v == 0.0) v = 1.0;
                     double t = (v * wr[a]) * wc[b];
                     if (j == dg && a == b && t == 0.0) t = 1.0;
@@ -1179,13 +1191,13 @@ static int sell_mats(crimson_lhs* L, float** K, float4** G, float4** GL) {
     return CRIMSON_OK;
 }
 
-// Sliced pattern: slice widths from the row lengths (host), columns (device).
-static int sell_pattern(crimson_lhs* L) {
-    if (L->sell_ptr.p) return CRIMSON_OK;
-    const int n = L->nNo;
-    cudaStream_t s = L->stream;
+// Sliced pattern of a CSR pattern (rowptr, col on the device): slice widths
+// from the row lengths (host), columns (device).  The column array carries
+// kSlice * kSellUnroll zero entries past npad.
+int sell_build(const int* rowptr, const int* col, int n, cudaStream_t s, DBuf<int>& sell_ptr, DBuf<int>& sell_col,
+               long long* npad_out, int* nslice_out) {
     std::vector<int> rp((size_t)n + 1);
-    CR_CUDA(cudaMemcpyAsync(rp.data(), L->rowptr, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaMemcpyAsync(rp.data(), rowptr, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
     CR_CUDA(cudaStreamSynchronize(s));
     const int ns = (n + kSlice - 1) / kSlice;
     std::vector<int> sp((size_t)ns + 1, 0);
@@ -1198,16 +1210,22 @@ static int sell_pattern(crimson_lhs* L) {
         if (pos + (long long)kSlice * kSellUnroll > 0x7fffffffLL) return CRIMSON_ERR_UNSUPPORTED;
     }
     sp[ns] = (int)pos;
-    L->nslice = ns;
-    L->npad = pos;
-    CR_CHECK(L->sell_ptr.upload(sp.data(), sp.size(), s));
+    CR_CHECK(sell_ptr.upload(sp.data(), sp.size(), s));
     const size_t np = (size_t)pos + (size_t)kSlice * kSellUnroll;
-    CR_CHECK(L->sell_col.alloc(np));
-    CR_CUDA(cudaMemsetAsync(L->sell_col.p, 0, sizeof(int) * np, s));
-    launch(k_sell_cols, grid_for((long long)ns * kSlice, 256), 256, 0, s, L->rowptr, L->col,
-           (const int*)L->sell_ptr.p, n, ns * kSlice, L->sell_col.p);
+    CR_CHECK(sell_col.alloc(np));
+    CR_CUDA(cudaMemsetAsync(sell_col.p, 0, sizeof(int) * np, s));
+    launch(k_sell_cols, grid_for((long long)ns * kSlice, 256), 256, 0, s, rowptr, col, (const int*)sell_ptr.p, n,
+           ns * kSlice, sell_col.p);
     CR_CUDA(cudaStreamSynchronize(s));
     CR_CUDA(cudaGetLastError());
+    *npad_out = pos;
+    *nslice_out = ns;
+    return CRIMSON_OK;
+}
+
+static int sell_pattern(crimson_lhs* L) {
+    if (L->sell_ptr.p) return CRIMSON_OK;
+    CR_CHECK(sell_build(L->rowptr, L->col, L->nNo, L->stream, L->sell_ptr, L->sell_col, &L->npad, &L->nslice));
     return CRIMSON_OK;
 }
 
@@ -1609,14 +1627,15 @@ __global__ void k_negate_p(double* __restrict__ R, int n) {
 // scaling, Dirichlet faces and the (symmetric) coupled-face terms carry over.
 int memls_solve_lhs_device(crimson_lhs* L, crimson_ls* ls, const double* d_res, const double* d_lhsK,
                            const double* d_lhsP, const int* incL, const double* faceRes, double* d_sol,
-                           crimson_ls_stats* st, bool transpose) {
+                           crimson_ls_stats* st, bool transpose, const float* d_lhs32) {
+    const TangentIn T{d_lhsK, d_lhsP, d_lhs32};
     cudaStream_t s = L->stream;
     CR_CHECK(lhs_work_alloc(L, ls));
     set_face_flags(L, incL, faceRes);
     CR_CUDA(cudaMemcpyAsync(L->R.p, d_res, sizeof(double) * 4 * (size_t)L->nNo, cudaMemcpyDeviceToDevice, s));
-    launch(k_w_from_lhs, grid_for(L->nNo, 256), 256, 0, s, d_lhsK, d_lhsP, L->diag, L->W.p, L->nNo);
+    launch(k_w_from_lhs, grid_for(L->nNo, 256), 256, 0, s, T, L->diag, L->W.p, L->nNo);
     CR_CHECK(precond_faces(L, false));
-    launch(k_scale_split_lhs, grid_for(L->nNo, 128), 128, 0, s, d_lhsK, d_lhsP, L->rowptr, L->col, L->diag, L->trans,
+    launch(k_scale_split_lhs, grid_for(L->nNo, 128), 128, 0, s, T, L->rowptr, L->col, L->diag, L->trans,
            (const double*)L->W.p, L->nNo, L->mK.p, L->mG.p, L->mD.p, L->mL.p);
     launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, (const double*)L->W.p, 4LL * L->nNo);
     CR_CHECK(precond_faces(L, true));

@@ -283,6 +283,103 @@ def cylinder(ncross: int = 24, naxial: int = 40, radius: float = 1.0, length: fl
     return _finish_tube(m, fb, srf, profile)
 
 
+def bifurcation(h: float = 0.036, parent_radius: float = 1.0, daughter_radius: float = 0.7,
+                parent_length: float = 5.0, daughter_length: float = 5.0, angle_deg: float = 30.0,
+                jitter: float = 0.05, seed: int = 3, name: str = "bifurcation") -> Mesh:
+    """Y-bifurcation: a parent tube along +z (inlet at z = 0) splitting at
+    B = (0, 0, parent_length) into two daughters along (+-sin a, 0, cos a).
+
+    Built the way :func:`cylinder` is, on one structured grid of spacing h:
+    hex cells whose centre lies inside the union of the three tubes (each a
+    finite cylinder about its centreline; the parent reaches half a radius
+    past B so the junction closes) are kept and split into 6 Kuhn tets; the
+    walls are the grid's staircase approximation of the tubes.  Interior
+    nodes are jittered by ``jitter`` x h (seeded).  A boundary face is an
+    outlet of daughter k (ids 3, 4) when the cell beyond it lies inside
+    daughter k's radius but past its end; the inlet is the z = 0 plane;
+    everything else is wall.  h = 0.036 cm gives about 4M tets.
+    """
+    a = np.deg2rad(angle_deg)
+    Bz = parent_length
+    dirs = [np.array([np.sin(a), 0.0, np.cos(a)]), np.array([-np.sin(a), 0.0, np.cos(a)])]
+    B = np.array([0.0, 0.0, Bz])
+    ends = [B + daughter_length * d for d in dirs]
+    rmax = max(parent_radius, daughter_radius)
+    lo = np.array([min(e[0] for e in ends) - rmax - h, -rmax - h, 0.0])
+    hi = np.array([max(e[0] for e in ends) + rmax + h, rmax + h, max(e[2] for e in ends) + rmax + h])
+    nc = np.ceil((hi - lo) / h).astype(np.int64)
+    # cell centres, z-major order (layer by layer, for locality)
+    ck, cj, ci = np.meshgrid(np.arange(nc[2]), np.arange(nc[1]), np.arange(nc[0]), indexing="ij")
+    ci, cj, ck = ci.ravel(), cj.ravel(), ck.ravel()
+    cen = lo + h * (np.stack([ci, cj, ck], axis=1) + 0.5)
+
+    def inside(p):
+        par = (p[:, 0] ** 2 + p[:, 1] ** 2 < parent_radius ** 2) & (p[:, 2] > 0.0) & \
+              (p[:, 2] < Bz + 0.5 * parent_radius)
+        inn = par.copy()
+        for d in dirs:
+            s = (p - B) @ d
+            r2 = np.sum((p - B - s[:, None] * d) ** 2, axis=1)
+            inn |= (s > 0.0) & (s < daughter_length) & (r2 < daughter_radius ** 2)
+        return inn
+
+    keep = inside(cen)
+    ci, cj, ck = ci[keep], cj[keep], ck[keep]
+    nn = nc + 1
+    gid = lambda i, j, k: (k * nn[1] + j) * nn[0] + i
+    hv = np.zeros((ci.size, 8), dtype=np.int64)
+    for v in range(8):
+        dx, dy, dz = v & 1, (v >> 1) & 1, (v >> 2) & 1
+        hv[:, v] = gid(ci + dx, cj + dy, ck + dz)
+    used, inv = np.unique(hv, return_inverse=True)
+    hexes = inv.reshape(hv.shape)
+    gk = used // (nn[0] * nn[1])
+    gj = (used // nn[0]) % nn[1]
+    gi = used % nn[0]
+    x = lo + h * np.stack([gi, gj, gk], axis=1).astype(np.float64)
+    ien = _hex_to_tets(hexes)
+    fb = _boundary_faces(ien)
+    bnodes = np.unique(fb[:, :3])
+    rng = np.random.default_rng(seed)
+    interior = np.ones(x.shape[0], dtype=bool)
+    interior[bnodes] = False
+    x[interior] += rng.uniform(-jitter * h, jitter * h, size=(int(interior.sum()), 3))
+    ien = _orient(x, ien).astype(np.int32)
+    fb = _boundary_faces(ien)
+    fb = _orient_faces_outward(x, fb)
+    v1 = x[fb[:, 1]] - x[fb[:, 0]]
+    v2 = x[fb[:, 2]] - x[fb[:, 0]]
+    nrm = np.cross(v1, v2)
+    nrm /= np.linalg.norm(nrm, axis=1)[:, None]
+    # centre of the grid cell across the face (faces lie on grid planes; the
+    # jitter moves interior nodes only)
+    beyond = x[fb[:, :3]].mean(axis=1) + 0.5 * h * nrm
+    beyond = lo + h * (np.floor((beyond - lo) / h) + 0.5)
+    srf = np.full(fb.shape[0], SRF_WALL, dtype=np.int32)
+    srf[beyond[:, 2] < 0.0] = SRF_INLET
+    for k, d in enumerate(dirs):
+        s = (beyond - B) @ d
+        r2 = np.sum((beyond - B - s[:, None] * d) ** 2, axis=1)
+        srf[(s >= daughter_length) & (r2 < daughter_radius ** 2)] = SRF_OUTLET0 + k
+
+    def profile(nodes):
+        r2 = (x[nodes, 0] ** 2 + x[nodes, 1] ** 2) / parent_radius ** 2
+        p = np.zeros((len(nodes), 3))
+        p[:, 2] = 2.0 * np.clip(1.0 - r2, 0.0, None)
+        return p
+
+    m = Mesh(x=x, ien=ien, name=name)
+    return _finish_tube(m, fb, srf, profile)
+
+
+def bifurcation_rcr(seed: int = 3, Rp: float = 100.0, C: float = 1e-4, Rd: float = 1000.0, spread: float = 0.2):
+    """RCR values of the two daughters: the nominal values scaled by
+    independent factors uniform in [1 - spread, 1 + spread] (seeded)."""
+    rng = np.random.default_rng(seed)
+    f = rng.uniform(1.0 - spread, 1.0 + spread, size=(2, 3))
+    return [dict(srfid=SRF_OUTLET0 + k, Rp=Rp * f[k, 0], C=C * f[k, 1], Rd=Rd * f[k, 2]) for k in range(2)]
+
+
 def lattice(n: int, jitter: float = 0.05, seed: int = 5, name: str = "lattice") -> Mesh:
     """n^3 hexes on a unit-spaced jittered lattice split into 6n^3 tets (no boundary data)."""
     nn = n + 1

@@ -180,6 +180,32 @@ int crimson_solflow_device(crimson_ctx* ctx, crimson_lhs* lhs, crimson_ls* ls, c
                            double* d_solinc, crimson_ls_stats* stats);
 
 /* ---------------------------------------------------------------------------
+ * FP32 element quadrature for the tangent (mixed precision; no counterpart
+ * in the reference).  crimson_elmgmr_device_f32 forms res exactly as
+ * crimson_elmgmr_device (FP64 arithmetic and scatter) and the tangent in
+ * FP32: d_lhs32 (16, nnz) floats per block = lhsK(1:9), lhsP(1:4), 3 zero
+ * pads (16-byte aligned records scattered with 4-wide vector reductions).
+ * crimson_solflow_device_f32 is crimson_solflow_device taking those
+ * records.  crimson_step uses both when the ls handle is CRIMSON_MIXED.
+ * ------------------------------------------------------------------------- */
+int crimson_elmgmr_device_f32(crimson_ctx* ctx, const double* d_y, const double* d_ac, const double* coef1,
+                              const double* coef2, double* d_res, float* d_lhs32);
+int crimson_solflow_device_f32(crimson_ctx* ctx, crimson_lhs* lhs, crimson_ls* ls, const double* d_res,
+                               const float* d_lhs32, const int* incL, const double* faceRes, double* d_solinc,
+                               crimson_ls_stats* stats);
+
+/* ---------------------------------------------------------------------------
+ * 4x4 block SpMV, SPARMULVV with dof = 4 (flowsolver/src/memLS.f90:2024-2076):
+ * KU(:, i) = sum_j Val(:, :, j) U(:, col(j)) on the context's pattern.
+ * prepare: d_val is memLS's Val (16, nnz), row-major 4x4 blocks, on the
+ * device, FP64 (precision CRIMSON_FP64) or FP32 (CRIMSON_MIXED); it is
+ * copied into a sliced layout.  apply: d_u, d_ku (4, nshg) node-major on the
+ * device, in the prepared precision; launches on the context's stream.
+ * ------------------------------------------------------------------------- */
+int crimson_spmv4_prepare(crimson_ctx* ctx, int precision, const void* d_val);
+int crimson_spmv4_apply(crimson_ctx* ctx, const void* d_u, void* d_ku);
+
+/* ---------------------------------------------------------------------------
  * Adjoint building blocks.  No counterpart in the reference (it has no
  * adjoint).
  * ------------------------------------------------------------------------- */

@@ -127,3 +127,35 @@ def test_mixed_time_steps_track_fp64_oracle():
         assert ev < bv, ev
         assert ep < bp, ep
         assert eo < bp, eo
+
+
+def test_fp32_tangent_records_match_fp64(system):
+    """FP32 element quadrature of the tangent: the 16-float records equal the
+    FP64 lhsK / lhsP to FP32 rounding (1e-6 normwise) and the residual formed
+    alongside is the FP64 one (1e-12)."""
+    import ctypes
+
+    import torch
+
+    from crimsonflowsolver_b200 import _native as N
+
+    m, P, elm, colm, rowp, Res4, Val4, faceRes, (yA, acA, c1, c2), xd, A, f = system
+    dev = torch.device("cuda:0")
+    dy = torch.tensor(yA, device=dev)
+    dac = torch.tensor(acA, device=dev)
+    nnz = len(rowp)
+    r64 = torch.zeros((m.nshg, 4), dtype=torch.float64, device=dev)
+    K = torch.zeros((nnz, 9), dtype=torch.float64, device=dev)
+    Pm = torch.zeros((nnz, 4), dtype=torch.float64, device=dev)
+    elm.device(dy, dac, r64, K, Pm, c1, c2)
+    r32 = torch.zeros_like(r64)
+    rec = torch.zeros((nnz, 16), dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    N.check(N.lib().crimson_elmgmr_device_f32(elm.h, dy.data_ptr(), dac.data_ptr(), N.dp(np.asarray(c1, float)),
+                                              N.dp(np.asarray(c2, float)), r32.data_ptr(), rec.data_ptr()), "f32")
+    torch.cuda.synchronize()
+    rec = rec.double().cpu().numpy()
+    assert relerr(r32.cpu().numpy(), r64.cpu().numpy()) < 1e-12
+    assert relerr(rec[:, 0:9], K.cpu().numpy()) < 1e-6
+    assert relerr(rec[:, 9:13], Pm.cpu().numpy()) < 1e-6
+    assert np.all(rec[:, 13:16] == 0.0)

@@ -158,3 +158,54 @@ def test_time_steps_parity():
     assert relerr(y[:, 0:3], F.y[:, 0:3]) < 1e-10, relerr(y[:, 0:3], F.y[:, 0:3])
     assert relerr(y[:, 3], F.y[:, 3]) < 1e-10, relerr(y[:, 3], F.y[:, 3])
     assert abs(st.p_out[0] - F.Pn[0]) <= 1e-10 * abs(F.Pn[0])
+
+
+def test_bifurcation_time_steps_parity():
+    """Two time steps on a small Y-bifurcation (two RCR outlets, +-20% seeded
+    values) against the oracle: the multi-outlet coupling path."""
+    m = mesh.bifurcation(h=0.25)
+    P = FlowParams(rcr=[RCR(**d) for d in mesh.bifurcation_rcr()])
+    inflow = lambda t: 10.0 + 5.0 * np.sin(2 * np.pi * t / 0.8)
+    F = po.OracleFlow(m, P, inflow=inflow)
+    G = solver.FlowSolver(mesh.bifurcation(h=0.25), P, inflow=inflow)
+    try:
+        for _ in range(2):
+            F.step()
+            st = G.step()
+        y, ac = G.state()
+    finally:
+        G.close()
+    assert relerr(y[:, 0:3], F.y[:, 0:3]) < 1e-10, relerr(y[:, 0:3], F.y[:, 0:3])
+    assert relerr(y[:, 3], F.y[:, 3]) < 1e-10, relerr(y[:, 3], F.y[:, 3])
+    for k in range(2):
+        assert abs(st.p_out[k] - F.Pn[k]) <= 1e-10 * abs(F.Pn[k])
+
+
+@pytest.mark.parametrize("state", ["restart", "seeded"])
+def test_reference_mesh_parity(state):
+    """The reference's own test mesh (testbin/mainTests/basic) with its
+    restart state, and with a seeded velocity field on the same mesh: CSR
+    pattern bit-exact and ElmGMR (its boundary faces and outlets included)
+    within 1e-12 of the oracle."""
+    from tests.fixtures import basic_mesh
+
+    m, y, ac = basic_mesh()
+    if state == "seeded":
+        rng = np.random.default_rng(17)
+        y[:, 0:3] = 10.0 * rng.standard_normal((m.nshg, 3))
+        ac = rng.standard_normal((m.nshg, 4))
+    srf = m.outlets
+    P = FlowParams(rcr=[RCR(srfid=s) for s in srf])
+    elm = solver.ElmGMR(m, P)
+    try:
+        colm, rowp = elm.genadj()
+        oc, orp = po.genadj(m.ien, m.nshg)
+        assert np.array_equal(colm, oc) and np.array_equal(rowp, orp)
+        c1 = [110.0 + 5 * k for k in range(len(srf))]
+        c2 = [-3.0 + k for k in range(len(srf))]
+        g = elm(y, ac, c1, c2)
+        o = po.Elm(m, P, colm, rowp)(y, ac, srflist=srf, coef1=c1, coef2=c2)
+    finally:
+        elm.close()
+    for k in ("res", "lhsK", "lhsP"):
+        assert relerr(g[k], o[k]) < 1e-12, (k, relerr(g[k], o[k]))

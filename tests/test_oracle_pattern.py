@@ -36,3 +36,22 @@ def test_genadj_single_element():
     colm, rowp = po.genadj(ien, 4)
     assert list(colm) == [1, 5, 9, 13, 17]
     assert list(rowp) == [1, 2, 3, 4] * 4
+
+
+def test_reference_mesh_fixture_loads_and_is_oriented():
+    """The reference's own mesh: every tet has det[x1-x4, x2-x4, x3-x4] > 0
+    (the orientation e3metric's WdetJ > 0 needs), and genadj's pattern is
+    symmetric with the diagonal in every row."""
+    from tests.fixtures import basic_mesh
+
+    m, y, ac = basic_mesh()
+    x, ien = m.x, m.ien
+    det = np.einsum("ij,ij->i", x[ien[:, 0]] - x[ien[:, 3]],
+                    np.cross(x[ien[:, 1]] - x[ien[:, 3]], x[ien[:, 2]] - x[ien[:, 3]]))
+    assert np.all(det > 0)
+    colm, rowp = po.genadj(m.ien, m.nshg)
+    rows = np.repeat(np.arange(m.nshg), np.diff(colm))
+    pairs = set(zip(rows.tolist(), (rowp - 1).tolist()))
+    assert all((c, r) in pairs for r, c in pairs)
+    assert all((i, i) in pairs for i in range(m.nshg))
+    assert y.shape == (1072, 4) and np.all(np.isfinite(y))
