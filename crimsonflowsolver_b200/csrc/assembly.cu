@@ -230,6 +230,12 @@ __global__ void __launch_bounds__(128) k_asigmr(const int4* __restrict__ ien, co
                                                 double* __restrict__ lhsK, double* __restrict__ lhsP,
                                                 float* __restrict__ lhs32) {
     __shared__ double sq[128][kQ];
+    // FP64 tangent staging: per warp the 32 (element, row a) blocks of one
+    // column b, so the scatter can be issued with consecutive lanes on
+    // consecutive values of the same block (3-4 sectors per block instead of
+    // one sector per lane).
+    __shared__ double stg[kLhs == 1 ? 128 : 1][13];
+    __shared__ int stg_slot[kLhs == 1 ? 128 : 1];
     const int lane4 = threadIdx.x & 3;
     const int gbase = threadIdx.x & ~3;   // first thread of this element's group
     const long long ngroups = (long long)gridDim.x * (blockDim.x >> 2);
@@ -409,45 +415,49 @@ __global__ void __launch_bounds__(128) k_asigmr(const int4* __restrict__ ien, co
                 atomicAdd(r + i, -WdetJ * v);
             }
             atomicAdd(r + 3, WdetJ * div_ub);
-            if (kLhs == 2) {
-                const float rhof = (float)rho, muf = (float)mu;
-                const float lhsFct = (float)(P.alfi * P.gami * P.Delt);
-                const float tlW = lhsFct * (float)WdetJ;
-                const float tsFct = (float)P.almi * (float)WdetJ * rhof;
-                float TC = 0.f, TM = 0.f, aqa[4], bqa[4], tMq[4], tBq[4], Naf[4];
+        }
+        if (kLhs == 2) {
+            // FP32 tangent row a: each lane scatters its blocks with 4-wide
+            // vector reductions (4 per 16-float record)
+            const float rhof = (float)rho, muf = (float)mu;
+            const float lhsFct = (float)(P.alfi * P.gami * P.Delt);
+            const float tlW = lhsFct * (float)WdetJ;
+            const float tsFct = (float)P.almi * (float)WdetJ * rhof;
+            float TC = 0.f, TM = 0.f, aqa[4], bqa[4], tMq[4], tBq[4], Naf[4];
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) {
+                const double* Sx = Sq[qq];
+                aqa[qq] = (float)Sx[a];
+                bqa[qq] = (float)Sx[4 + a];
+                tMq[qq] = (float)Sx[12];
+                tBq[qq] = (float)Sx[13];
+                TC += (float)Sx[14];
+                TM += (float)Sx[12];
+                Naf[qq] = (float)Na[qq];
+            }
+            float sga[3] = {(float)shg[a][0], (float)shg[a][1], (float)shg[a][2]};
+            const int* ep = epos + 16 * e + 4 * a;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                float conv = 0.f, sym = 0.f;
 #pragma unroll
                 for (int qq = 0; qq < 4; ++qq) {
                     const double* Sx = Sq[qq];
-                    aqa[qq] = (float)Sx[a];
-                    bqa[qq] = (float)Sx[4 + a];
-                    tMq[qq] = (float)Sx[12];
-                    tBq[qq] = (float)Sx[13];
-                    TC += (float)Sx[14];
-                    TM += (float)Sx[12];
-                    Naf[qq] = (float)Na[qq];
+                    conv += Naf[qq] * (float)Sx[8 + b];
+                    sym += tMq[qq] * rhof * aqa[qq] * (float)Sx[b] + tBq[qq] * bqa[qq] * (float)Sx[4 + b];
                 }
-                float sga[3] = {(float)shg[a][0], (float)shg[a][1], (float)shg[a][2]};
-                const int* ep = epos + 16 * e + 4 * a;
+                const float sgb[3] = {(float)shg[b][0], (float)shg[b][1], (float)shg[b][2]};
+                const float grad = sga[0] * sgb[0] + sga[1] * sgb[1] + sga[2] * sgb[2];
+                const float Kd = tsFct * (float)c_el.M[a][b] + tlW * (rhof * conv + 4.0f * muf * grad + sym);
+                const float tc = tlW * TC, tm = tlW * 4.0f * muf;
+                float K[9];
 #pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    float conv = 0.f, sym = 0.f;
+                for (int i = 0; i < 3; ++i)
 #pragma unroll
-                    for (int qq = 0; qq < 4; ++qq) {
-                        const double* Sx = Sq[qq];
-                        conv += Naf[qq] * (float)Sx[8 + b];
-                        sym += tMq[qq] * rhof * aqa[qq] * (float)Sx[b] + tBq[qq] * bqa[qq] * (float)Sx[4 + b];
-                    }
-                    const float sgb[3] = {(float)shg[b][0], (float)shg[b][1], (float)shg[b][2]};
-                    const float grad = sga[0] * sgb[0] + sga[1] * sgb[1] + sga[2] * sgb[2];
-                    const float Kd = tsFct * (float)c_el.M[a][b] + tlW * (rhof * conv + 4.0f * muf * grad + sym);
-                    const float tc = tlW * TC, tm = tlW * 4.0f * muf;
-                    float K[9];
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int j = 0; j < 3; ++j)
-                            K[3 * i + j] = (i == j ? Kd : 0.f) + tc * sgb[i] * sga[j] + tm * sgb[j] * sga[i];
-                    const float sn = tlW * (float)c_el.SN[a];
+                    for (int j = 0; j < 3; ++j)
+                        K[3 * i + j] = (i == j ? Kd : 0.f) + tc * sgb[i] * sga[j] + tm * sgb[j] * sga[i];
+                const float sn = tlW * (float)c_el.SN[a];
+                if (live) {
                     float* rec = lhs32 + 16 * (size_t)ep[b];
                     red_add_v4(rec + 0, K[0], K[1], K[2], K[3]);
                     red_add_v4(rec + 4, K[4], K[5], K[6], K[7]);
@@ -455,51 +465,62 @@ __global__ void __launch_bounds__(128) k_asigmr(const int4* __restrict__ ien, co
                     atomicAdd(rec + 12, tlW / rhof * TM * grad);
                 }
             }
-            if (kLhs == 1) {
-                const double lhsFct = P.alfi * P.gami * P.Delt;
-                const double tlW = lhsFct * WdetJ;
-                const double tsFct = P.almi * WdetJ * rho;
-                double TC = 0.0, TM = 0.0, aqa[4], bqa[4], tMq[4], tBq[4];
+        }
+        if (kLhs == 1) {
+            // tangent row a of this element, one column b at a time: staged,
+            // then scattered by the whole warp
+            const double lhsFct = P.alfi * P.gami * P.Delt;
+            const double tlW = lhsFct * WdetJ;
+            const double tsFct = P.almi * WdetJ * rho;
+            double TC = 0.0, TM = 0.0, aqa[4], bqa[4], tMq[4], tBq[4];
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) {
+                const double* Sx = Sq[qq];
+                aqa[qq] = Sx[a];
+                bqa[qq] = Sx[4 + a];
+                tMq[qq] = Sx[12];
+                tBq[qq] = Sx[13];
+                TC += Sx[14];
+                TM += Sx[12];
+            }
+            const int* ep = epos + 16 * e + 4 * a;
+            const int wbase = threadIdx.x & ~31;
+            const int lane = threadIdx.x & 31;
+#pragma unroll 1
+            for (int b = 0; b < 4; ++b) {
+                double conv = 0.0, sym = 0.0;
 #pragma unroll
                 for (int qq = 0; qq < 4; ++qq) {
                     const double* Sx = Sq[qq];
-                    aqa[qq] = Sx[a];
-                    bqa[qq] = Sx[4 + a];
-                    tMq[qq] = Sx[12];
-                    tBq[qq] = Sx[13];
-                    TC += Sx[14];
-                    TM += Sx[12];
+                    conv += Na[qq] * Sx[8 + b];
+                    sym += tMq[qq] * rho * aqa[qq] * Sx[b] + tBq[qq] * bqa[qq] * Sx[4 + b];
                 }
-                const int* ep = epos + 16 * e + 4 * a;
+                double grad = shg[a][0] * shg[b][0] + shg[a][1] * shg[b][1] + shg[a][2] * shg[b][2];
+                double Kd = tsFct * c_el.M[a][b] + tlW * (rho * conv + 4.0 * mu * grad + sym);
+                const double tc = tlW * TC, tm = tlW * 4.0 * mu;
+                double* st = stg[threadIdx.x];
 #pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    double conv = 0.0, sym = 0.0;
+                for (int i = 0; i < 3; ++i)
 #pragma unroll
-                    for (int qq = 0; qq < 4; ++qq) {
-                        const double* Sx = Sq[qq];
-                        conv += Na[qq] * Sx[8 + b];
-                        sym += tMq[qq] * rho * aqa[qq] * Sx[b] + tBq[qq] * bqa[qq] * Sx[4 + b];
+                    for (int j = 0; j < 3; ++j)
+                        st[3 * i + j] = (i == j ? Kd : 0.0) + tc * shg[b][i] * shg[a][j] + tm * shg[b][j] * shg[a][i];
+                const double sn = tlW * c_el.SN[a];
+                st[9] = sn * shg[b][0];
+                st[10] = sn * shg[b][1];
+                st[11] = sn * shg[b][2];
+                st[12] = tlW / rho * TM * grad;
+                stg_slot[threadIdx.x] = live ? ep[b] : -1;
+                __syncwarp();
+#pragma unroll 1
+                for (int v = lane; v < 32 * 13; v += 32) {
+                    const int blk = v / 13, comp = v - 13 * blk;
+                    const int slot = stg_slot[wbase + blk];
+                    if (slot >= 0) {
+                        double* dst = comp < 9 ? lhsK + 9 * (size_t)slot + comp : lhsP + 4 * (size_t)slot + (comp - 9);
+                        atomicAdd(dst, stg[wbase + blk][comp]);
                     }
-                    double grad = shg[a][0] * shg[b][0] + shg[a][1] * shg[b][1] + shg[a][2] * shg[b][2];
-                    double Kd = tsFct * c_el.M[a][b] + tlW * (rho * conv + 4.0 * mu * grad + sym);
-                    const double tc = tlW * TC, tm = tlW * 4.0 * mu;
-                    double K[9];
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int j = 0; j < 3; ++j)
-                            K[3 * i + j] = (i == j ? Kd : 0.0) + tc * shg[b][i] * shg[a][j] + tm * shg[b][j] * shg[a][i];
-                    const size_t k = (size_t)ep[b];
-                    double* Kp = lhsK + 9 * k;
-#pragma unroll
-                    for (int t = 0; t < 9; ++t) atomicAdd(Kp + t, K[t]);
-                    double* Pp = lhsP + 4 * k;
-                    const double sn = tlW * c_el.SN[a];
-                    atomicAdd(Pp + 0, sn * shg[b][0]);
-                    atomicAdd(Pp + 1, sn * shg[b][1]);
-                    atomicAdd(Pp + 2, sn * shg[b][2]);
-                    atomicAdd(Pp + 3, tlW / rho * TM * grad);
                 }
+                __syncwarp();
             }
         }
         __syncwarp();

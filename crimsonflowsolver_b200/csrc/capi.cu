@@ -397,7 +397,7 @@ int crimson_memls_ls_free(crimson_ls* ls) {
 }
 
 int crimson_memls_ls_set_precision(crimson_ls* ls, int precision, int max_refine, double refine_tol) {
-    if (!ls || (precision != CRIMSON_FP64 && precision != CRIMSON_MIXED) || max_refine < 1 || max_refine > 64 ||
+    if (!ls || precision < CRIMSON_FP64 || precision > CRIMSON_MIXED_F32_TANGENT || max_refine < 1 || max_refine > 64 ||
         !(refine_tol < 1.0))
         return CRIMSON_ERR_ARG;
     ls->precision = precision;
@@ -683,7 +683,7 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
         launch(k_yalpha, grid_for(n, 256), 256, 0, s, c->yold.p, c->acold.p, c->ycur.p, c->accur.p, c->yalpha.p,
                                                   c->acalpha.p, n, P.alfi, P.almi);
         crimson_ls_stats lst;
-        if (ls->precision == CRIMSON_MIXED) {
+        if (ls->precision == CRIMSON_MIXED_F32_TANGENT) {
             // FP32 element quadrature for the tangent, FP64 residual
             CR_CHECK(c->lhs32.alloc(16 * (size_t)c->nnz));
             CR_CHECK(elmgmr_device(c, c->yalpha.p, c->acalpha.p, c1.data(), c2.data(), c->res4.p, nullptr, nullptr, 2,

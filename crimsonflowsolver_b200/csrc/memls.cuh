@@ -81,7 +81,7 @@ struct crimson_lhs {
 struct crimson_ls {
     crimson_subls GM{}, CG{}, RI{};
     int LS_type = CRIMSON_LS_TYPE_NS, Resm = 0, Resc = 0;
-    int precision = CRIMSON_FP64;  // CRIMSON_FP64 or CRIMSON_MIXED
+    int precision = CRIMSON_FP64;  // CRIMSON_FP64, CRIMSON_MIXED or CRIMSON_MIXED_F32_TANGENT
     int max_refine = 4;            // FP64 refinement sweeps of the mixed solve
     double refine_tol = 0.0;       // target |R - A x| / |R|; <= 0: RI.relTol
 };

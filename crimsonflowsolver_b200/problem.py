@@ -76,11 +76,12 @@ class FlowParams:
     maxiters: int = 500
     nprjs: int = 10
     rcr: List[RCR] = field(default_factory=list)
-    # NS solve arithmetic: "fp64" (memLS's) or "mixed" (FP32 matrices in the
+    # NS solve arithmetic: "fp64" (memLS's), "mixed" (FP32 matrices in the
     # inner Krylov matvecs, FP64 outer vectors and iterative refinement of at
     # most max_refine sweeps, until the FP64 defect |R - A x| / |R| is at
-    # most refine_tol, epstol_ns when refine_tol <= 0).  Not reference
-    # settings.
+    # most refine_tol, epstol_ns when refine_tol <= 0) or "mixed_f32_tangent"
+    # (mixed, and FP32 element quadrature of the tangent in the time step).
+    # Not reference settings.
     precision: str = "fp64"
     max_refine: int = 4
     refine_tol: float = 0.0

@@ -24,7 +24,7 @@ from . import _native as N
 from .problem import FlowParams
 
 
-PRECISIONS = {"fp64": 0, "mixed": 1}
+PRECISIONS = {"fp64": 0, "mixed": 1, "mixed_f32_tangent": 2}
 
 
 def make_params(P: FlowParams) -> N.Params:

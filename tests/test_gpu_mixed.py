@@ -159,3 +159,27 @@ def test_fp32_tangent_records_match_fp64(system):
     assert relerr(rec[:, 0:9], K.cpu().numpy()) < 1e-6
     assert relerr(rec[:, 9:13], Pm.cpu().numpy()) < 1e-6
     assert np.all(rec[:, 13:16] == 0.0)
+
+
+def test_f32_tangent_converged_steps_match_fp64():
+    """FP32 element quadrature of the tangent (mixed_f32_tangent) changes the
+    Newton path, not its limit: with the nonlinear iterations converged (8
+    per step) two steps agree with the FP64 path to 1e-6."""
+    inflow = lambda t: 10.0 + 5.0 * np.sin(2 * np.pi * t / 0.8)
+    out = {}
+    for prec, extra in (("fp64", dict(epstol_ns=3e-7, epstol_mom=3e-6, epstol_cont=3e-6)),
+                        ("mixed_f32_tangent", dict(max_refine=8, refine_tol=1e-9))):
+        P = FlowParams(rcr=[RCR(srfid=3)], nitr=8, precision=prec, **extra)
+        G = solver.FlowSolver(mesh.cylinder(ncross=8, naxial=10), P, inflow=inflow)
+        try:
+            for _ in range(2):
+                st = G.step()
+            out[prec] = (G.state()[0], st.p_out[0])
+        finally:
+            G.close()
+    y64, p64 = out["fp64"]
+    y32, p32 = out["mixed_f32_tangent"]
+    ev = relerr(y32[:, 0:3], y64[:, 0:3])
+    ep = relerr(y32[:, 3], y64[:, 3])
+    print(f"f32 tangent, converged steps: vel {ev:.3e} p {ep:.3e} Pout {abs(p32 - p64) / abs(p64):.3e}")
+    assert ev < 1e-6 and ep < 1e-6 and abs(p32 - p64) <= 1e-6 * abs(p64)
