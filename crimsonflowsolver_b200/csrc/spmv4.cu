@@ -22,7 +22,16 @@ int sell_build(const int* rowptr, const int* col, int n, cudaStream_t s, DBuf<in
 namespace {
 
 constexpr int kS4Slice = 32;
-constexpr int kS4Unroll = 4;
+// entries issued together per thread: all their loads are hoisted ahead of
+// the arithmetic (FP64: 160 B per entry in registers, FP32: 80 B)
+template <typename T>
+struct S4Unroll {
+    static constexpr int value = 2;
+};
+template <>
+struct S4Unroll<float> {
+    static constexpr int value = 4;
+};
 
 template <typename T>
 struct Vec4;
@@ -75,23 +84,27 @@ __global__ void __launch_bounds__(256) k_spmv4(const int* __restrict__ sp, const
         const int w = (__ldg(sp + s + 1) - p0) / kS4Slice;
         const int base = p0 + (r % kS4Slice);
         T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
-        for (int k0 = 0; k0 < w; k0 += kS4Unroll) {
-            int c[kS4Unroll];
+        constexpr int UN = S4Unroll<T>::value;
+        for (int k0 = 0; k0 < w; k0 += UN) {
+            // entries past w are re-read from the row's first position (in
+            // bounds) and not accumulated
+            T4 x[UN], b0[UN], b1[UN], b2[UN], b3[UN];
 #pragma unroll
-            for (int u = 0; u < kS4Unroll; ++u) c[u] = (k0 + u < w) ? __ldg(scol + base + kS4Slice * (k0 + u)) : 0;
+            for (int u = 0; u < UN; ++u) {
+                const size_t pos = (size_t)base + (size_t)kS4Slice * ((k0 + u < w) ? (k0 + u) : 0);
+                x[u] = V::load(U + __ldg(scol + pos));
+                b0[u] = V::load(blk + 4 * pos + 0);
+                b1[u] = V::load(blk + 4 * pos + 1);
+                b2[u] = V::load(blk + 4 * pos + 2);
+                b3[u] = V::load(blk + 4 * pos + 3);
+            }
 #pragma unroll
-            for (int u = 0; u < kS4Unroll; ++u) {
+            for (int u = 0; u < UN; ++u) {
                 if (k0 + u < w) {
-                    const size_t pos = (size_t)base + (size_t)kS4Slice * (k0 + u);
-                    const T4 x = V::load(U + c[u]);
-                    const T4 b0 = V::load(blk + 4 * pos + 0);
-                    const T4 b1 = V::load(blk + 4 * pos + 1);
-                    const T4 b2 = V::load(blk + 4 * pos + 2);
-                    const T4 b3 = V::load(blk + 4 * pos + 3);
-                    a0 = a0 + b0.x * x.x + b0.y * x.y + b0.z * x.z + b0.w * x.w;
-                    a1 = a1 + b1.x * x.x + b1.y * x.y + b1.z * x.z + b1.w * x.w;
-                    a2 = a2 + b2.x * x.x + b2.y * x.y + b2.z * x.z + b2.w * x.w;
-                    a3 = a3 + b3.x * x.x + b3.y * x.y + b3.z * x.z + b3.w * x.w;
+                    a0 = a0 + b0[u].x * x[u].x + b0[u].y * x[u].y + b0[u].z * x[u].z + b0[u].w * x[u].w;
+                    a1 = a1 + b1[u].x * x[u].x + b1[u].y * x[u].y + b1[u].z * x[u].z + b1[u].w * x[u].w;
+                    a2 = a2 + b2[u].x * x[u].x + b2[u].y * x[u].y + b2[u].z * x[u].z + b2[u].w * x[u].w;
+                    a3 = a3 + b3[u].x * x[u].x + b3[u].y * x[u].y + b3[u].z * x[u].z + b3[u].w * x[u].w;
                 }
             }
         }
