@@ -26,7 +26,7 @@ constexpr int kS4Slice = 32;
 // the arithmetic (FP64: 160 B per entry in registers, FP32: 80 B)
 template <typename T>
 struct S4Unroll {
-    static constexpr int value = 2;
+    static constexpr int value = 4;
 };
 template <>
 struct S4Unroll<float> {
