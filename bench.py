@@ -240,6 +240,8 @@ def _timed_steps(F, args, stream, local, dist):
     if it[:, 3].max() > 0:
         per_solve["refine_sweeps"] = float(it[:, 3].mean())
         per_solve["max_final_defect"] = float(it[:, 4].max())
+    per_solve["outlet_q"] = [float(st.q_out[k]) for k in range(len(F.P.rcr))]
+    per_solve["outlet_p"] = [float(st.p_out[k]) for k in range(len(F.P.rcr))]
     return t_ms, per_solve, int(launches), clk.summary()
 
 
@@ -313,6 +315,8 @@ def run_ours(args):
     y64, _ = F64.state()
     ym, _ = FM.state()
     acc = {"velocity": _relerr(ym[:, 0:3], y64[:, 0:3]), "pressure": _relerr(ym[:, 3], y64[:, 3]),
+           "outlet_flow": _relerr(np.array(itm["outlet_q"]), np.array(it64["outlet_q"])),
+           "outlet_pressure": _relerr(np.array(itm["outlet_p"]), np.array(it64["outlet_p"])),
            "after_steps": args.warmup + args.steps}
     value = replica_value(tm_ms, args.steps, ws)
     v64 = replica_value(t64_ms, args.steps, ws)
