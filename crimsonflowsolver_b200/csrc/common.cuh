@@ -175,7 +175,8 @@ struct crimson_ctx {
 
     // ElmGMR work space
     crimson::DBuf<double> qres;     // (nshg, 9) node-major: q[9*i + k]
-    crimson::DBuf<double> rmass;    // (nshg)
+    crimson::DBuf<double> rmass;    // (nshg) 1 / lumped mass (geometry only)
+    bool rmass_ready = false;       // rmass holds the inverse lumped mass
     crimson::DBuf<double> y4, ac4, res4;   // (4, nshg) staging for host-pointer calls
     crimson::DBuf<double> lhsK, lhsP;      // (9, nnz), (4, nnz)
     crimson::DBuf<float> lhs32;            // (16, nnz) FP32 tangent records (mixed precision)
