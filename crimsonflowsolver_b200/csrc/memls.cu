@@ -371,7 +371,18 @@ constexpr int kSellUnroll = 8;
         }                                                                                \
     }
 #define CR_SELL_ROW(sp, scol, r, ...) CR_SELL_ROW_U(kSellUnroll, sp, scol, r, __VA_ARGS__)
-constexpr int kCgUnroll = 4;
+// Entries per stage of the CG's software-pipelined row loops: the matrix
+// records of the next stage are loaded while the current stage's gathers are
+// in flight (two stages live: 2 x 4 x 16 B FP32, 2 x 2 x 32 B FP64, within
+// the 64 registers of four 256-thread blocks per SM).
+template <typename M>
+struct CgStage {
+    static constexpr int value = 4;
+};
+template <>
+struct CgStage<double> {
+    static constexpr int value = 2;
+};
 
 // KU = K U on the sliced copy: K (9, npad), U / KU (3, n)
 template <typename M, typename IN, typename OUT>
@@ -526,13 +537,17 @@ __global__ void __launch_bounds__(256, 4) k_cg_persistent(CgArgs<M> a) {
             const int p0 = __ldg(a.sp + s_);
             const int w = (__ldg(a.sp + s_ + 1) - p0) >> 5;
             const int base = p0 + (r & (kSlice - 1));
-            for (int k0 = 0; k0 < w; k0 += kCgUnroll) {
-                typename V4<M>::type g[kCgUnroll];
+            constexpr int U = CgStage<M>::value;
+            const auto zero4 = mk4<M>(M(0), M(0), M(0), M(0));
+            typename V4<M>::type g[U];
 #pragma unroll
-                for (int u = 0; u < kCgUnroll; ++u)
-                    g[u] = (k0 + u < w) ? ldg4(a.G + base + kSlice * (k0 + u)) : mk4<M>(M(0), M(0), M(0), M(0));
+            for (int u = 0; u < U; ++u) g[u] = (u < w) ? ldg4(a.G + base + kSlice * u) : zero4;
+            for (int k0 = 0; k0 < w; k0 += U) {
+                typename V4<M>::type gn[U];  // next stage, loaded before this stage's gathers
 #pragma unroll
-                for (int u = 0; u < kCgUnroll; ++u) {
+                for (int u = 0; u < U; ++u) gn[u] = (k0 + U + u < w) ? ldg4(a.G + base + kSlice * (k0 + U + u)) : zero4;
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
                     if (k0 + u < w) {
                         const double2 rp = a.recA[bits_col(g[u].w)];
                         const double pc = first ? rp.x : rp.x + beta * rp.y;
@@ -541,6 +556,8 @@ __global__ void __launch_bounds__(256, 4) k_cg_persistent(CgArgs<M> a) {
                         a2 = a2 + (double)g[u].z * pc;
                     }
                 }
+#pragma unroll
+                for (int u = 0; u < U; ++u) g[u] = gn[u];
             }
             const double2 rr = a.recA[r];
             const double pr = first ? rr.x : rr.x + beta * rr.y;
@@ -565,12 +582,45 @@ __global__ void __launch_bounds__(256, 4) k_cg_persistent(CgArgs<M> a) {
         double dsum = 0.0;
         for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
             double lp = 0.0, gg = 0.0;
-            CR_SELL_ROW_U(kCgUnroll, a.sp, a.scol, r, {
-                const auto gl = ldg4(a.GL + pos);
-                const auto q = a.recB[c];
-                lp = lp + (double)gl.w * (double)q.w;
-                gg = gg + (double)gl.x * (double)q.x + (double)gl.y * (double)q.y + (double)gl.z * (double)q.z;
-            })
+            {
+                constexpr int U = CgStage<M>::value;
+                const auto zero4 = mk4<M>(M(0), M(0), M(0), M(0));
+                const int s_ = r >> 5;
+                const int p0 = __ldg(a.sp + s_);
+                const int w = (__ldg(a.sp + s_ + 1) - p0) >> 5;
+                const int base = p0 + (r & (kSlice - 1));
+                int cc[U];
+                typename V4<M>::type gl[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    cc[u] = (u < w) ? __ldg(a.scol + base + kSlice * u) : r;
+                    gl[u] = (u < w) ? ldg4(a.GL + base + kSlice * u) : zero4;
+                }
+                for (int k0 = 0; k0 < w; k0 += U) {
+                    int ccn[U];  // next stage
+                    typename V4<M>::type gln[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const bool in = k0 + U + u < w;
+                        ccn[u] = in ? __ldg(a.scol + base + kSlice * (k0 + U + u)) : r;
+                        gln[u] = in ? ldg4(a.GL + base + kSlice * (k0 + U + u)) : zero4;
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        if (k0 + u < w) {
+                            const auto q = a.recB[cc[u]];
+                            lp = lp + (double)gl[u].w * (double)q.w;
+                            gg = gg + (double)gl[u].x * (double)q.x + (double)gl[u].y * (double)q.y +
+                                 (double)gl[u].z * (double)q.z;
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        cc[u] = ccn[u];
+                        gl[u] = gln[u];
+                    }
+                }
+            }
 #pragma unroll
             for (int f = 0; f < NF; ++f)
                 if (f < a.nface) gg += cS[f] * a.z[(size_t)f * n + r];
@@ -1230,9 +1280,21 @@ static int sell_pattern(crimson_lhs* L) {
 }
 
 // NSSOLVER (memLS.f90:1460-1759); R (4, nNo) FP64 in/out; matrices in M.
+// FP64 CSR matrices for the products that enter NSSOLVER's least-squares
+// problem (the A d of every search direction d).  With them the Gram
+// system, the residual estimate and the outer residuals are those of the
+// FP64 operator while the Krylov solvers run on type-M copies.  All null:
+// the type-M matrices serve (the FP64 path).
+struct OuterMats {
+    const double* K = nullptr;
+    const double* G = nullptr;
+    const double* D = nullptr;
+    const double* L = nullptr;
+};
+
 template <typename M, typename B>
 static int nssolver(crimson_lhs* L, crimson_ls* ls, const M* mK, const M* mG, const M* mD, const M* mL, const M* Gt,
-                    double* R) {
+                    double* R, const OuterMats& outer = OuterMats{}) {
     Ctx C{L, L->stream};
     cudaStream_t s = L->stream;
     const int nNo = L->nNo;
@@ -1295,14 +1357,26 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const M* mK, const M* mG, co
         CR_CHECK(cgrad<M>(C, ls->CG, (const typename V4<M>::type*)Gs, (const typename V4<M>::type*)GLs, Pcol(i - 1),
                           cg_nface,
                           cg_coef));
-        C.sv3(mG, (const double*)Pcol(i - 1), MUc(iB - 1));
+        if (outer.G)
+            C.sv3(outer.G, (const double*)Pcol(i - 1), MUc(iB - 1));
+        else
+            C.sv3(mG, (const double*)Pcol(i - 1), MUc(iB - 1));
         launch(k_sub<double, double, double>, grid_for(nv, 256), 256, 0, s, (const double*)L->Rm.p,
                (const double*)MUc(iB - 1), MUc(iBB - 1), nv);
         CR_CHECK((gmres<M, B>(C, ls->GM, (const M*)Ks, MUc(iBB - 1), Ucol(i - 1))));
-        C.vv3s((const M*)Ks, (const double*)Ucol(i - 1), MUc(iBB - 1));
+        if (outer.K)
+            C.vv3(outer.K, (const double*)Ucol(i - 1), MUc(iBB - 1));
+        else
+            C.vv3s((const M*)Ks, (const double*)Ucol(i - 1), MUc(iBB - 1));
         C.addbcmul(0, 3, (const double*)Ucol(i - 1), MUc(iBB - 1));
-        C.ss(mL, (const double*)Pcol(i - 1), MPc(iB - 1));
-        C.vs3(mD, (const double*)Ucol(i - 1), MPc(iBB - 1));
+        if (outer.L)
+            C.ss(outer.L, (const double*)Pcol(i - 1), MPc(iB - 1));
+        else
+            C.ss(mL, (const double*)Pcol(i - 1), MPc(iB - 1));
+        if (outer.D)
+            C.vs3(outer.D, (const double*)Ucol(i - 1), MPc(iBB - 1));
+        else
+            C.vs3(mD, (const double*)Ucol(i - 1), MPc(iBB - 1));
         // Gram matrix entries for columns iB, iBB
         int slot = kSlotGram;
         for (int k = iB; k <= iBB; ++k) {
@@ -1489,10 +1563,12 @@ static int defect64(crimson_lhs* L, const double* R0, const double* x4, double* 
 
 // NSSOLVER on the scaled system in L->R (in/out).  FP64: the reference's
 // arithmetic.  Mixed: FP32 copies of the scaled split matrices drive every
-// inner matvec; each sweep solves A d = D in FP32-matrix arithmetic, adds d
-// to the FP64 solution and forms the FP64 defect D = R0 - A x, until
-// |D| <= refine_tol |R0| (RI.relTol when refine_tol <= 0) or max_refine
-// sweeps.  Every sweep's NSSOLVER stops at its own relative tolerances, so
+// inner matvec (GMRES, CGRAD, the Schur right side); the products A d of the
+// search directions that enter the least-squares problem use the FP64
+// matrices, so a sweep's residual estimate is that of the FP64 operator.
+// Each sweep solves A d = D, adds d to the FP64 solution and forms the FP64
+// defect D = R0 - A x, until |D| <= refine_tol |R0| (RI.relTol when
+// refine_tol <= 0) or max_refine sweeps.  Every sweep's NSSOLVER stops at its own relative tolerances, so
 // the sweeps reach a defect below what one NSSOLVER's estimate can resolve.  Iteration counts are summed
 // over the sweeps.  has_gt: Gt is a separate matrix (host Val path),
 // otherwise mD serves as Gt.
@@ -1538,7 +1614,12 @@ static int solve_scaled(crimson_lhs* L, crimson_ls* ls, bool has_gt) {
     } guard{ls->RI, ls->RI.relTol};
     double sigma = 1.0;
     for (int ref = 0; ref < std::max(ls->max_refine, 1); ++ref) {
-        CR_CHECK((nssolver<float, float>(L, ls, L->mK32.p, L->mG32.p, L->mD32.p, L->mL32.p, Gt32, L->R.p)));
+        OuterMats outer;
+        outer.K = L->mK.p;
+        outer.G = L->mG.p;
+        outer.D = L->mD.p;
+        outer.L = L->mL.p;
+        CR_CHECK((nssolver<float, float>(L, ls, L->mK32.p, L->mG32.p, L->mD32.p, L->mL32.p, Gt32, L->R.p, outer)));
         if (ref == 0) {
             gm = ls->GM;
             cg = ls->CG;

@@ -183,3 +183,35 @@ def test_f32_tangent_converged_steps_match_fp64():
     ep = relerr(y32[:, 3], y64[:, 3])
     print(f"f32 tangent, converged steps: vel {ev:.3e} p {ep:.3e} Pout {abs(p32 - p64) / abs(p64):.3e}")
     assert ev < 1e-6 and ep < 1e-6 and abs(p32 - p64) <= 1e-6 * abs(p64)
+
+def test_mixed_first_sweep_meets_tolerance():
+    """The least-squares products of the mixed NSSOLVER are FP64, so its
+    residual estimate is that of the FP64 operator: one sweep reaches the
+    NSSOLVER tolerance in the FP64 defect, with the iteration counts of the
+    FP64 solve (the FP32 Krylov directions differ only in rounding), and the
+    time steps agree with the FP64 library run far below the tolerance.
+    """
+    inflow = lambda t: 10.0 + 5.0 * np.sin(2 * np.pi * t / 0.8)
+    m = mesh.cylinder(ncross=8, naxial=10)
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        P = FlowParams(rcr=[RCR(srfid=3)], precision=prec, max_refine=8)
+        F = solver.FlowSolver(m, P, inflow=inflow)
+        try:
+            stats = [F.step() for _ in range(3)]
+            runs[prec] = (F.state(), stats, P.epstol_ns)
+        finally:
+            F.close()
+    (y64, _), s64, tol = runs["fp64"]
+    (ym, _), sm, _ = runs["mixed"]
+    for a, b in zip(s64, sm):
+        assert a.nsolves == b.nsolves
+        for i in range(b.nsolves):
+            assert b.refine_steps[i] == 1, (i, b.refine_steps[i], b.refine_rel[i])
+            assert b.refine_rel[i] <= tol
+            assert a.ri_itr[i] == b.ri_itr[i]
+            assert abs(a.cg_itr[i] - b.cg_itr[i]) <= 0.02 * a.cg_itr[i]
+    ev = relerr(ym[:, 0:3], y64[:, 0:3])
+    ep = relerr(ym[:, 3], y64[:, 3])
+    print(f"mixed vs FP64 library after 3 steps: vel {ev:.3e} p {ep:.3e}")
+    assert ev < 1e-7 and ep < 1e-7, (ev, ep)
