@@ -106,6 +106,8 @@ SIGNATURES = {
                                             c_void_p, c_dbl_p, c_void_p]),
     "crimson_launch_count": (ctypes.c_ulonglong, []),
     "crimson_memls_kernel_time": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, c_dbl_p]),
+    "crimson_memls_cg_layout": (ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_longlong)]),
     "crimson_version": (ctypes.c_char_p, []),
     "crimson_last_error": (ctypes.c_char_p, []),
 }

@@ -153,6 +153,14 @@ int crimson_memls_kernel_time(crimson_lhs* L, int which, int reps, double* ms) {
     return memls_kernel_time(L, which, reps, ms);
 }
 const char* crimson_last_error(void) { return g_last_error.c_str(); }
+int crimson_memls_cg_layout(const crimson_lhs* L, int* resident64, int* resident32, long long* smem_bytes) {
+    if (!L) return CRIMSON_ERR_ARG;
+    if (L->cg_res_bytes < 0) return CRIMSON_ERR_STATE;
+    if (resident64) *resident64 = L->cg_grid ? L->cg_res64 : 0;
+    if (resident32) *resident32 = L->cg_grid32 ? L->cg_res32 : 0;
+    if (smem_bytes) *smem_bytes = L->cg_res_bytes;
+    return CRIMSON_OK;
+}
 
 int crimson_ctx_create(crimson_ctx** out, const crimson_params* p, int nshg, int numnp, int nelem, const int* ien,
                        const double* x) {

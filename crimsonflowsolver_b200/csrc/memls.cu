@@ -422,20 +422,23 @@ __global__ void k_sell_cols(const int* __restrict__ rowptr, const int* __restric
     }
 }
 
-// Column index carried in the 4th component of a {G0, G1, G2, col} record
-// (bit pattern, never used in arithmetic).
-__device__ __forceinline__ double col_bits(int c, double) { return __hiloint2double(0, c); }
-__device__ __forceinline__ float col_bits(int c, float) { return __int_as_float(c); }
-__device__ __forceinline__ int bits_col(double w) { return __double2loint(w); }
-__device__ __forceinline__ int bits_col(float w) { return __float_as_int(w); }
+// Largest |col - row| of a CSR pattern (atomicMax into *out).
+__global__ void k_max_offset(const int* __restrict__ rowptr, const int* __restrict__ col, int n, int* out) {
+    int m = 0;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+        for (int j = rowptr[r]; j < rowptr[r + 1]; ++j) m = max(m, abs(col[j] - r));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
 
-// Scaled split matrices (CSR, type M) -> sliced copies: K (9, npad),
-// {G0, G1, G2, col} (npad), {Gt0, Gt1, Gt2, L} (npad).
+// Scaled split matrices (CSR, type M) -> sliced copies: K (9, npad) and G
+// (3, npad) per component, {Gt0, Gt1, Gt2, L} (npad).
 template <typename M>
 __global__ void k_to_sell(const int* __restrict__ rowptr, const int* __restrict__ sp, int n, const M* __restrict__ mK,
                           const M* __restrict__ mG, const M* __restrict__ Gt, const M* __restrict__ mL,
-                          long long npad, M* __restrict__ Ks, typename V4<M>::type* __restrict__ Gs,
-                          typename V4<M>::type* __restrict__ GLs, const int* __restrict__ col) {
+                          long long npad, M* __restrict__ Ks, M* __restrict__ Gs,
+                          typename V4<M>::type* __restrict__ GLs) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         const size_t base = (size_t)sp[r >> 5] + (r & (kSlice - 1));
         const int rs = rowptr[r], re = rowptr[r + 1];
@@ -444,7 +447,8 @@ __global__ void k_to_sell(const int* __restrict__ rowptr, const int* __restrict_
             const size_t jj = (size_t)j;
 #pragma unroll
             for (int q = 0; q < 9; ++q) Ks[q * npad + pos] = mK[9 * jj + q];
-            Gs[pos] = mk4<M>(mG[3 * jj], mG[3 * jj + 1], mG[3 * jj + 2], col_bits(col[jj], M(0)));
+#pragma unroll
+            for (int q = 0; q < 3; ++q) Gs[q * npad + pos] = mG[3 * jj + q];
             GLs[pos] = mk4<M>(Gt[3 * jj], Gt[3 * jj + 1], Gt[3 * jj + 2], mL[jj]);
         }
     }
@@ -463,8 +467,9 @@ __global__ void k_to_sell(const int* __restrict__ rowptr, const int* __restrict_
 // recA = {R, P_prev} (16 B, FP64) read in phase A, recB = {GP, P} read in
 // phase B, stored in the matrix type M (32 B FP64 / 16 B FP32: with FP32
 // matrices the matvec operands are rounded to FP32 as the matrices are,
-// while P itself stays FP64 for the updates); matrix entries
-// {G0, G1, G2, column} and {Gt0, Gt1, Gt2, L}.  Partial sums are written per block
+// while P itself stays FP64 for the updates); matrix entries G per
+// component (three coalesced streams) and {Gt0, Gt1, Gt2, L}; the column
+// indices block-resident in shared memory where they fit (CgCols).  Partial sums are written per block
 // and summed in block order by every block after the barrier
 // (deterministic, identical in all blocks).  Node records written by other
 // blocks in an earlier phase are read with ordinary (L1-cached) loads: the
@@ -483,10 +488,10 @@ constexpr int kCgThreads = 512;
 template <typename M>
 struct CgArgs {
     const int* sp;    // sliced pattern: slice offsets
-    const int* scol;  // sliced pattern: columns
+    const int* scol;  // sliced pattern: columns (read when the columns are not block-resident)
     long long npad;
     int n;
-    const typename V4<M>::type* G;   // sliced (npad) {G0, G1, G2, col}
+    const M* G;                      // sliced G per component: G0 at [0, npad), G1, G2 (stride npad)
     const typename V4<M>::type* GL;  // sliced (npad) {Gt0, Gt1, Gt2, L}
     double* X;
     double2* recA;  // (n) {R, P of the previous iteration}
@@ -511,15 +516,68 @@ __device__ __forceinline__ double sum_partials(const double* part, int k, double
     return block_sum(s, sm);
 }
 
-template <int NF, typename M>
+// Column source of the CG row loops.  Block-resident (kRes): every block
+// copies the columns of its own rows into shared memory once per launch, as
+// 16-bit offsets col - row, and the iterations read no column index from
+// HBM (4 B per entry and phase).  A warp's rows are whole slices (32 rows),
+// so a warp's columns are the concatenation of its slices' column ranges in
+// sliced order; entry k of a row sits at off + 32 k + lane, where off
+// advances by the slice's length after each row.  Otherwise the columns are
+// read from the sliced pattern.
+template <bool kRes>
+struct CgCols {
+    const int* scol;
+    const short* res;  // this warp's resident offsets (kRes)
+    int off;           // offset of the current row's slice within res
+    int lane;
+    __device__ __forceinline__ int col(int r, int base, int k) const {
+        if (kRes) return r + (int)res[off + kSlice * k + lane];
+        return __ldg(scol + base + kSlice * k);
+    }
+    __device__ __forceinline__ void next_row(int w) {
+        if (kRes) off += kSlice * w;
+    }
+};
+
+// Fill this block's resident column offsets; returns this warp's base.
+__device__ int cg_fill_cols(const int* __restrict__ sp, const int* __restrict__ scol, int n, short* res) {
+    __shared__ int woff[kCgThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int s0 = (blockIdx.x * kCgThreads + wid * kSlice) / kSlice;
+    const int sstride = gridDim.x * (kCgThreads / kSlice);
+    const int nsl = (n + kSlice - 1) / kSlice;
+    int tot = 0;
+    for (int s = s0 + lane * sstride; s < nsl; s += 32 * sstride) tot += __ldg(sp + s + 1) - __ldg(sp + s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    if (lane == 0) woff[wid] = tot;
+    __syncthreads();
+    int base = 0;
+    for (int q = 0; q < wid; ++q) base += woff[q];
+    int off = base;
+    for (int s = s0; s < nsl; s += sstride) {
+        const int p0 = __ldg(sp + s), len = __ldg(sp + s + 1) - p0;
+        const int row = s * kSlice + lane;  // position p0 + j belongs to row s*32 + j%32
+        for (int j = lane; j < len; j += 32) res[off + j] = row < n ? (short)(__ldg(scol + p0 + j) - row) : (short)0;
+        off += len;
+    }
+    __syncthreads();
+    return base;
+}
+
+template <int NF, typename M, bool kRes>
 __global__ void __launch_bounds__(kCgThreads, 2) k_cg_persistent(CgArgs<M> a) {
     namespace cgrp = cooperative_groups;
     cgrp::grid_group grid = cgrp::this_grid();
+    extern __shared__ short cg_res[];
     __shared__ double sm[32];
     const int n = a.n;
+    const long long npad = a.npad;
     double* partA = a.part;
     double* partB = a.part + (size_t)gridDim.x * kCgPartStride;
     double* partC = a.part + 2 * (size_t)gridDim.x * kCgPartStride;
+    const int wbase = kRes ? cg_fill_cols(a.sp, a.scol, n, cg_res) : 0;
+    constexpr int U = CgStage<M>::value;
     double err = a.err0, errO = a.err0;
     int suc = 0, i;
     for (i = 1; i <= a.mItr; ++i) {
@@ -534,34 +592,57 @@ __global__ void __launch_bounds__(kCgThreads, 2) k_cg_persistent(CgArgs<M> a) {
         double wp[NF > 0 ? NF : 1];
 #pragma unroll
         for (int f = 0; f < (NF > 0 ? NF : 1); ++f) wp[f] = 0.0;
+        CgCols<kRes> cs{a.scol, cg_res, wbase, (int)(threadIdx.x & 31)};
         for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
             double a0 = 0.0, a1 = 0.0, a2 = 0.0;
             const int s_ = r >> 5;
             const int p0 = __ldg(a.sp + s_);
             const int w = (__ldg(a.sp + s_ + 1) - p0) >> 5;
             const int base = p0 + (r & (kSlice - 1));
-            constexpr int U = CgStage<M>::value;
-            const auto zero4 = mk4<M>(M(0), M(0), M(0), M(0));
-            typename V4<M>::type g[U];
+            // stage: G values and columns of U entries; the next stage is
+            // loaded before this stage's gathers
+            M g0[U], g1[U], g2[U];
+            int cc[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) g[u] = (u < w) ? ldg4(a.G + base + kSlice * u) : zero4;
+            for (int u = 0; u < U; ++u) {
+                const bool in = u < w;
+                const size_t pos = (size_t)base + kSlice * u;
+                g0[u] = in ? __ldg(a.G + pos) : M(0);
+                g1[u] = in ? __ldg(a.G + npad + pos) : M(0);
+                g2[u] = in ? __ldg(a.G + 2 * npad + pos) : M(0);
+                cc[u] = (!kRes && in) ? cs.col(r, base, u) : r;  // resident columns are read at use
+            }
             for (int k0 = 0; k0 < w; k0 += U) {
-                typename V4<M>::type gn[U];  // next stage, loaded before this stage's gathers
+                M n0[U], n1[U], n2[U];
+                int nc[U];
 #pragma unroll
-                for (int u = 0; u < U; ++u) gn[u] = (k0 + U + u < w) ? ldg4(a.G + base + kSlice * (k0 + U + u)) : zero4;
+                for (int u = 0; u < U; ++u) {
+                    const bool in = k0 + U + u < w;
+                    const size_t pos = (size_t)base + kSlice * (k0 + U + u);
+                    n0[u] = in ? __ldg(a.G + pos) : M(0);
+                    n1[u] = in ? __ldg(a.G + npad + pos) : M(0);
+                    n2[u] = in ? __ldg(a.G + 2 * npad + pos) : M(0);
+                    nc[u] = (!kRes && in) ? cs.col(r, base, k0 + U + u) : r;
+                }
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     if (k0 + u < w) {
-                        const double2 rp = a.recA[bits_col(g[u].w)];
+                        const double2 rp = a.recA[kRes ? cs.col(r, base, k0 + u) : cc[u]];
                         const double pc = first ? rp.x : rp.x + beta * rp.y;
-                        a0 = a0 + (double)g[u].x * pc;
-                        a1 = a1 + (double)g[u].y * pc;
-                        a2 = a2 + (double)g[u].z * pc;
+                        a0 = a0 + (double)g0[u] * pc;
+                        a1 = a1 + (double)g1[u] * pc;
+                        a2 = a2 + (double)g2[u] * pc;
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < U; ++u) g[u] = gn[u];
+                for (int u = 0; u < U; ++u) {
+                    g0[u] = n0[u];
+                    g1[u] = n1[u];
+                    g2[u] = n2[u];
+                    cc[u] = nc[u];
+                }
             }
+            cs.next_row(w);
             const double2 rr = a.recA[r];
             const double pr = first ? rr.x : rr.x + beta * rr.y;
             a.recB[r] = mk4<M>((M)a0, (M)a1, (M)a2, (M)pr);
@@ -583,47 +664,46 @@ __global__ void __launch_bounds__(kCgThreads, 2) k_cg_persistent(CgArgs<M> a) {
         for (int f = 0; f < NF; ++f) cS[f] = f < a.nface ? a.coef[f] * sum_partials(partA, f, sm) : 0.0;
         // ---- phase B: SP = L P - Gt GP - sum_f cS_f z_f ; <P, SP> ----
         double dsum = 0.0;
+        CgCols<kRes> cb{a.scol, cg_res, wbase, (int)(threadIdx.x & 31)};
         for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
             double lp = 0.0, gg = 0.0;
-            {
-                constexpr int U = CgStage<M>::value;
-                const auto zero4 = mk4<M>(M(0), M(0), M(0), M(0));
-                const int s_ = r >> 5;
-                const int p0 = __ldg(a.sp + s_);
-                const int w = (__ldg(a.sp + s_ + 1) - p0) >> 5;
-                const int base = p0 + (r & (kSlice - 1));
-                int cc[U];
-                typename V4<M>::type gl[U];
+            const auto zero4 = mk4<M>(M(0), M(0), M(0), M(0));
+            const int s_ = r >> 5;
+            const int p0 = __ldg(a.sp + s_);
+            const int w = (__ldg(a.sp + s_ + 1) - p0) >> 5;
+            const int base = p0 + (r & (kSlice - 1));
+            int cc[U];
+            typename V4<M>::type gl[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                cc[u] = (!kRes && u < w) ? cb.col(r, base, u) : r;
+                gl[u] = (u < w) ? ldg4(a.GL + base + kSlice * u) : zero4;
+            }
+            for (int k0 = 0; k0 < w; k0 += U) {
+                int ccn[U];  // next stage
+                typename V4<M>::type gln[U];
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
-                    cc[u] = (u < w) ? __ldg(a.scol + base + kSlice * u) : r;
-                    gl[u] = (u < w) ? ldg4(a.GL + base + kSlice * u) : zero4;
+                    const bool in = k0 + U + u < w;
+                    ccn[u] = (!kRes && in) ? cb.col(r, base, k0 + U + u) : r;
+                    gln[u] = in ? ldg4(a.GL + base + kSlice * (k0 + U + u)) : zero4;
                 }
-                for (int k0 = 0; k0 < w; k0 += U) {
-                    int ccn[U];  // next stage
-                    typename V4<M>::type gln[U];
 #pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        const bool in = k0 + U + u < w;
-                        ccn[u] = in ? __ldg(a.scol + base + kSlice * (k0 + U + u)) : r;
-                        gln[u] = in ? ldg4(a.GL + base + kSlice * (k0 + U + u)) : zero4;
+                for (int u = 0; u < U; ++u) {
+                    if (k0 + u < w) {
+                        const auto q = a.recB[kRes ? cb.col(r, base, k0 + u) : cc[u]];
+                        lp = lp + (double)gl[u].w * (double)q.w;
+                        gg = gg + (double)gl[u].x * (double)q.x + (double)gl[u].y * (double)q.y +
+                             (double)gl[u].z * (double)q.z;
                     }
+                }
 #pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        if (k0 + u < w) {
-                            const auto q = a.recB[cc[u]];
-                            lp = lp + (double)gl[u].w * (double)q.w;
-                            gg = gg + (double)gl[u].x * (double)q.x + (double)gl[u].y * (double)q.y +
-                                 (double)gl[u].z * (double)q.z;
-                        }
-                    }
-#pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        cc[u] = ccn[u];
-                        gl[u] = gln[u];
-                    }
+                for (int u = 0; u < U; ++u) {
+                    cc[u] = ccn[u];
+                    gl[u] = gln[u];
                 }
             }
+            cb.next_row(w);
 #pragma unroll
             for (int f = 0; f < NF; ++f)
                 if (f < a.nface) gg += cS[f] * a.z[(size_t)f * n + r];
@@ -1093,10 +1173,43 @@ static int cg_faces(Ctx& C, const M* G, const M* Gt, int* nface, double* coef) {
     return CRIMSON_OK;
 }
 
+// Shared memory for block-resident CG columns (CgCols) on a grid of two
+// blocks per SM: 0 when the pattern's column offsets exceed 16 bits; else
+// 2 bytes per sliced entry of the fullest block.  Computed once per pattern.
+static int cg_resident_bytes(crimson_lhs* L, size_t* bytes) {
+    if (L->cg_res_bytes >= 0) {
+        *bytes = (size_t)L->cg_res_bytes;
+        return CRIMSON_OK;
+    }
+    cudaStream_t s = L->stream;
+    const int n = L->nNo;
+    CR_CHECK(L->cg_tmp.alloc(1));
+    CR_CUDA(cudaMemsetAsync(L->cg_tmp.p, 0, sizeof(int), s));
+    launch(k_max_offset, grid_for(n, 256), 256, 0, s, (const int*)L->rowptr, (const int*)L->col, n, L->cg_tmp.p);
+    int maxoff = 0;
+    CR_CUDA(cudaMemcpyAsync(&maxoff, L->cg_tmp.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    std::vector<int> sp((size_t)L->nslice + 1);
+    CR_CUDA(cudaMemcpyAsync(sp.data(), L->sell_ptr.p, sizeof(int) * sp.size(), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    long long best = 0;
+    if (maxoff <= 32767) {
+        const int grid = 2 * sm_count();
+        const int wpb = kCgThreads / kSlice;  // slices (warps) per block
+        std::vector<long long> per((size_t)grid, 0);
+        for (int q = 0; q < L->nslice; ++q) per[(size_t)((q / wpb) % grid)] += sp[q + 1] - sp[q];
+        for (long long v : per) best = std::max(best, v);
+        best = (2 * best + 15) / 16 * 16;
+        if (best == 0) best = 16;
+    }
+    L->cg_res_bytes = best;
+    *bytes = (size_t)best;
+    return CRIMSON_OK;
+}
+
 // CGRAD (memLS.f90:367-430) on the Schur-like operator L P - Gt G P; R in/out (n).
 // Gs / GLs: sliced G and {Gt, L} of this NSSOLVER call.
 template <typename M>
-static int cgrad(Ctx& C, crimson_subls& ls, const typename V4<M>::type* Gs, const typename V4<M>::type* GLs,
+static int cgrad(Ctx& C, crimson_subls& ls, const M* Gs, const typename V4<M>::type* GLs,
                  double* R, int nface,
                  const double* coef) {
     crimson_lhs* L = C.L;
@@ -1112,18 +1225,44 @@ static int cgrad(Ctx& C, crimson_subls& ls, const typename V4<M>::type* Gs, cons
     eps = eps * eps;
     double err = errO;
     err = err * err;
-    const void* kfn = nface == 0 ? (const void*)k_cg_persistent<0, M>
-                      : (nface == 1 ? (const void*)k_cg_persistent<1, M> : (const void*)k_cg_persistent<kMaxCoupled, M>);
+    const void* kres[3] = {(const void*)k_cg_persistent<0, M, true>, (const void*)k_cg_persistent<1, M, true>,
+                           (const void*)k_cg_persistent<kMaxCoupled, M, true>};
+    const void* kglb[3] = {(const void*)k_cg_persistent<0, M, false>, (const void*)k_cg_persistent<1, M, false>,
+                           (const void*)k_cg_persistent<kMaxCoupled, M, false>};
     int& grid = std::is_same<M, float>::value ? L->cg_grid32 : L->cg_grid;
+    int& mode = std::is_same<M, float>::value ? L->cg_res32 : L->cg_res64;
+    size_t rbytes = 0;
+    CR_CHECK(cg_resident_bytes(L, &rbytes));
     if (grid == 0) {
-        int nb0 = 0, nb1 = 0, nb8 = 0;
-        CR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb0, k_cg_persistent<0, M>, kCgThreads, 0));
-        CR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb1, k_cg_persistent<1, M>, kCgThreads, 0));
-        CR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb8, k_cg_persistent<kMaxCoupled, M>, kCgThreads, 0));
-        const int nb = std::min(nb0, std::min(nb1, nb8));
-        if (nb < 1) return CRIMSON_ERR_UNSUPPORTED;
-        grid = sm_count() * std::min(nb, 8);
+        // block-resident columns when two blocks per SM fit with them
+        mode = 0;
+        if (rbytes > 0) {
+            int ok = 1;
+            for (const void* f : kres) {
+                int nb = 0;
+                if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rbytes) != cudaSuccess ||
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, kCgThreads, rbytes) != cudaSuccess || nb < 2)
+                    ok = 0;
+            }
+            (void)cudaGetLastError();  // a refused attribute only selects the other kernel
+            mode = ok;
+        }
+        if (mode) {
+            grid = 2 * sm_count();
+        } else {
+            int nb = 1 << 30;
+            for (const void* f : kglb) {
+                int b = 0;
+                CR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, kCgThreads, 0));
+                nb = std::min(nb, b);
+            }
+            if (nb < 1) return CRIMSON_ERR_UNSUPPORTED;
+            grid = sm_count() * std::min(nb, 8);
+        }
     }
+    const int fi = nface == 0 ? 0 : (nface == 1 ? 1 : 2);
+    const void* kfn = mode ? kres[fi] : kglb[fi];
+    const size_t dyn = mode ? rbytes : 0;
     CR_CHECK(L->cgPart.alloc(3 * (size_t)kCgPartStride * std::max(L->cg_grid, L->cg_grid32)));
     CR_CHECK(L->cgRecA.alloc(2 * (size_t)n));
     CR_CHECK(L->cgRecB.alloc(4 * (size_t)n));
@@ -1154,7 +1293,7 @@ static int cgrad(Ctx& C, crimson_subls& ls, const typename V4<M>::type* Gs, cons
     void* kargs[] = {&a};
     note_launch();
     CR_CUDA(cudaEventRecord(L->ev0, s));
-    CR_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kCgThreads), kargs, 0, s));
+    CR_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kCgThreads), kargs, dyn, s));
     CR_CUDA(cudaEventRecord(L->ev1, s));
     CR_CHECK(C.sync_scal(kSlotCg, 4));
     err = L->hscal[kSlotCg + 0];
@@ -1220,26 +1359,26 @@ static int ge_solve(int N, const double* A, double* B) {
 template <typename M>
 static int sell_alloc(crimson_lhs* L, DBuf<M>& K, DBuf<M>& G, DBuf<M>& GL) {
     const size_t np = (size_t)L->npad + (size_t)kSlice * kSellUnroll;
-    if (K.n == 9 * np && G.n == 4 * np && GL.n == 4 * np) return CRIMSON_OK;
+    if (K.n == 9 * np && G.n == 3 * np && GL.n == 4 * np) return CRIMSON_OK;
     CR_CHECK(K.alloc(9 * np));
-    CR_CHECK(G.alloc(4 * np));
+    CR_CHECK(G.alloc(3 * np));
     CR_CHECK(GL.alloc(4 * np));
     CR_CUDA(cudaMemsetAsync(K.p, 0, sizeof(M) * K.n, L->stream));
     CR_CUDA(cudaMemsetAsync(G.p, 0, sizeof(M) * G.n, L->stream));
     CR_CUDA(cudaMemsetAsync(GL.p, 0, sizeof(M) * GL.n, L->stream));
     return CRIMSON_OK;
 }
-static int sell_mats(crimson_lhs* L, double** K, double4** G, double4** GL) {
+static int sell_mats(crimson_lhs* L, double** K, double** G, double4** GL) {
     CR_CHECK(sell_alloc(L, L->Ks64, L->Gs64, L->GLs64));
     *K = L->Ks64.p;
-    *G = reinterpret_cast<double4*>(L->Gs64.p);
+    *G = L->Gs64.p;
     *GL = reinterpret_cast<double4*>(L->GLs64.p);
     return CRIMSON_OK;
 }
-static int sell_mats(crimson_lhs* L, float** K, float4** G, float4** GL) {
+static int sell_mats(crimson_lhs* L, float** K, float** G, float4** GL) {
     CR_CHECK(sell_alloc(L, L->Ks32, L->Gs32, L->GLs32));
     *K = L->Ks32.p;
-    *G = reinterpret_cast<float4*>(L->Gs32.p);
+    *G = L->Gs32.p;
     *GL = reinterpret_cast<float4*>(L->GLs32.p);
     return CRIMSON_OK;
 }
@@ -1343,11 +1482,11 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const M* mK, const M* mG, co
     double cg_coef[kMaxCoupled];
     CR_CHECK(cg_faces(C, mG, Gt, &cg_nface, cg_coef));
     M* Ks = nullptr;
-    typename V4<M>::type* Gs = nullptr;
+    M* Gs = nullptr;
     typename V4<M>::type* GLs = nullptr;
     CR_CHECK(sell_mats(L, &Ks, &Gs, &GLs));
     launch(k_to_sell<M>, grid_for(nNo, 256), 256, 0, s, L->rowptr, (const int*)L->sell_ptr.p, nNo, mK, mG, Gt, mL,
-           L->npad, Ks, Gs, GLs, L->col);
+           L->npad, Ks, Gs, GLs);
     int i, iBB = 0;
     for (i = 1; i <= ls->RI.mItr; ++i) {
         iB = 2 * i - 1;
@@ -1357,7 +1496,7 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const M* mK, const M* mG, co
         C.vs3(mD, (const double*)Ucol(i - 1), Pcol(i - 1));
         launch(k_sub<double, double, double>, grid_for(nNo, 256), 256, 0, s, (const double*)L->Rc.p,
                (const double*)Pcol(i - 1), Pcol(i - 1), (long long)nNo);
-        CR_CHECK(cgrad<M>(C, ls->CG, (const typename V4<M>::type*)Gs, (const typename V4<M>::type*)GLs, Pcol(i - 1),
+        CR_CHECK(cgrad<M>(C, ls->CG, (const M*)Gs, (const typename V4<M>::type*)GLs, Pcol(i - 1),
                           cg_nface,
                           cg_coef));
         if (outer.G)

@@ -60,6 +60,9 @@ struct crimson_lhs {
     DBuf<double> Ks64, Gs64, GLs64;
     DBuf<float> Ks32, Gs32, GLs32;
     int cg_grid = 0, cg_grid32 = 0;
+    int cg_res64 = 0, cg_res32 = 0;    // CG kernel with block-resident columns (per matrix type)
+    long long cg_res_bytes = -1;       // its shared memory per block (0: offsets exceed 16 bits); -1 unknown
+    DBuf<int> cg_tmp;
     // mixed precision: FP32 copies of the scaled split matrices; FP64 right
     // side and accumulated solution of the iterative refinement
     DBuf<float> mK32, mG32, mD32, mL32, Gt32;

@@ -308,6 +308,15 @@ int crimson_pvsq_noalloc(int nsurf, const int* surf_offsets, const int* d_nodes,
  * Valid after a solve on the lhs. */
 int crimson_memls_kernel_time(crimson_lhs* lhs, int which, int reps, double* ms);
 
+/* Diagnostics: column layout of the persistent CG kernel on this lhs.
+ * resident64 / resident32 = 1 when the kernel with FP64 / FP32 matrices keeps
+ * every block's column indices in shared memory for the whole launch (16-bit
+ * offsets col - row; chosen when the offsets fit and two blocks per SM fit
+ * with them), 0 when it reads them from the sliced pattern each phase;
+ * smem_bytes = shared memory per block of the resident layout (0: offsets
+ * exceed 16 bits).  Valid after a solve on the lhs. */
+int crimson_memls_cg_layout(const crimson_lhs* lhs, int* resident64, int* resident32, long long* smem_bytes);
+
 /* Number of CUDA kernels this library has launched since it was loaded. */
 unsigned long long crimson_launch_count(void);
 
