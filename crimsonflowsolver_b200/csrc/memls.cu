@@ -756,15 +756,16 @@ __global__ void k_face_ext(const int* __restrict__ glob, const double* __restric
 // ---------------------------------------------------------------------------
 template <typename V>
 __global__ void k_face_dot(const int* __restrict__ glob, const double* __restrict__ valM, int fdof, int nsd,
-                           int nNoF, const V* __restrict__ X, int dof, double* out) {
+                           int nNoF, const V* __restrict__ X, int dof, double* part, unsigned int* ticket,
+                           double* out) {
     __shared__ double sm[32];
     double s = 0.0;
-    for (int a = threadIdx.x; a < nNoF; a += blockDim.x) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nNoF; a += gridDim.x * blockDim.x) {
         const int Ac = glob[a];
         for (int i = 0; i < nsd; ++i) s += valM[(size_t)fdof * a + i] * (double)X[(size_t)dof * Ac + i];
     }
     s = block_sum(s, sm);
-    if (threadIdx.x == 0) *out = s;
+    grid_reduce_finish(s, part, ticket, out, sm);
 }
 
 template <typename V>
@@ -1022,7 +1023,11 @@ struct Ctx {
         for (auto& f : L->face) {
             if (f.coupledFlag) {
                 int nsd = std::min(f.dof, dof);
-                launch(k_face_dot<VX>, 1, 512, 0, s, f.glob.p, f.valM.p, f.dof, nsd, f.nNo, X, dof, sc(kSlotFace + k));
+                // a few nodes per thread: the face dot is a chain of gathers
+                int g = (f.nNo + 4 * 128 - 1) / (4 * 128);
+                g = std::max(1, std::min(g, (int)RedScratch::kMaxBlocks));
+                launch(k_face_dot<VX>, g, 128, 0, s, f.glob.p, f.valM.p, f.dof, nsd, f.nNo, X, dof, L->red.part.p,
+                       L->red.ticket.p, sc(kSlotFace + k));
             }
             ++k;
         }
