@@ -384,7 +384,8 @@ struct CgStage<double> {
     static constexpr int value = 2;
 };
 
-// KU = K U on the sliced copy: K (9, npad), U / KU (3, n)
+// KU = K U on the sliced copy: K as {K0..K3} and {K4..K7} 4-vectors (npad
+// each, one 16/32-byte load apiece) and K8 (npad); U / KU (3, n).
 template <typename M, typename IN, typename OUT>
 __global__ void __launch_bounds__(256) k_sell_vv3(const int* __restrict__ sp, const int* __restrict__ scol,
                                                   const M* __restrict__ Ks, long long npad,
@@ -394,10 +395,10 @@ __global__ void __launch_bounds__(256) k_sell_vv3(const int* __restrict__ sp, co
         CR_SELL_ROW(sp, scol, r, {
             const IN* u = U + 3 * (size_t)c;
             const double u0 = (double)__ldg(u), u1 = (double)__ldg(u + 1), u2 = (double)__ldg(u + 2);
-            const double k0 = (double)__ldg(Ks + pos), k1 = (double)__ldg(Ks + npad + pos),
-                         k2 = (double)__ldg(Ks + 2 * npad + pos), k3 = (double)__ldg(Ks + 3 * npad + pos),
-                         k4 = (double)__ldg(Ks + 4 * npad + pos), k5 = (double)__ldg(Ks + 5 * npad + pos),
-                         k6 = (double)__ldg(Ks + 6 * npad + pos), k7 = (double)__ldg(Ks + 7 * npad + pos),
+            const auto ka = ldg4(reinterpret_cast<const typename V4<M>::type*>(Ks) + pos);
+            const auto kb = ldg4(reinterpret_cast<const typename V4<M>::type*>(Ks + 4 * npad) + pos);
+            const double k0 = (double)ka.x, k1 = (double)ka.y, k2 = (double)ka.z, k3 = (double)ka.w,
+                         k4 = (double)kb.x, k5 = (double)kb.y, k6 = (double)kb.z, k7 = (double)kb.w,
                          k8 = (double)__ldg(Ks + 8 * npad + pos);
             a0 = a0 + k0 * u0 + k1 * u1 + k2 * u2;
             a1 = a1 + k3 * u0 + k4 * u1 + k5 * u2;
@@ -432,8 +433,9 @@ __global__ void k_max_offset(const int* __restrict__ rowptr, const int* __restri
     if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
-// Scaled split matrices (CSR, type M) -> sliced copies: K (9, npad) and G
-// (3, npad) per component, {Gt0, Gt1, Gt2, L} (npad).
+// Scaled split matrices (CSR, type M) -> sliced copies: K as two 4-vector
+// arrays and one scalar array (npad each), G (3, npad) per component,
+// {Gt0, Gt1, Gt2, L} (npad).
 template <typename M>
 __global__ void k_to_sell(const int* __restrict__ rowptr, const int* __restrict__ sp, int n, const M* __restrict__ mK,
                           const M* __restrict__ mG, const M* __restrict__ Gt, const M* __restrict__ mL,
@@ -445,8 +447,11 @@ __global__ void k_to_sell(const int* __restrict__ rowptr, const int* __restrict_
         for (int j = rs; j < re; ++j) {
             const size_t pos = base + (size_t)kSlice * (j - rs);
             const size_t jj = (size_t)j;
-#pragma unroll
-            for (int q = 0; q < 9; ++q) Ks[q * npad + pos] = mK[9 * jj + q];
+            reinterpret_cast<typename V4<M>::type*>(Ks)[pos] =
+                mk4<M>(mK[9 * jj], mK[9 * jj + 1], mK[9 * jj + 2], mK[9 * jj + 3]);
+            reinterpret_cast<typename V4<M>::type*>(Ks + 4 * npad)[pos] =
+                mk4<M>(mK[9 * jj + 4], mK[9 * jj + 5], mK[9 * jj + 6], mK[9 * jj + 7]);
+            Ks[8 * npad + pos] = mK[9 * jj + 8];
 #pragma unroll
             for (int q = 0; q < 3; ++q) Gs[q * npad + pos] = mG[3 * jj + q];
             GLs[pos] = mk4<M>(Gt[3 * jj], Gt[3 * jj + 1], Gt[3 * jj + 2], mL[jj]);
@@ -1053,7 +1058,6 @@ static int gmres(Ctx& C, crimson_subls& ls, const M* Ks, const double* R, double
     const long long n = (long long)dof * L->nNo;
     const int sD = ls.sD;
     B* u = reinterpret_cast<B*>(L->basis.p);
-    B* w3 = reinterpret_cast<B*>(L->w3.p);
     auto U = [&](int k) { return u + (size_t)k * n; };
     std::vector<double> h((size_t)(sD + 1) * sD, 0.0), c(sD), sn(sD), err(sD + 1), y(sD);
     auto H = [&](int i, int j) -> double& { return h[(size_t)j * (sD + 1) + i]; };
@@ -1072,10 +1076,7 @@ static int gmres(Ctx& C, crimson_subls& ls, const M* Ks, const double* R, double
             C.addbcmul(0, dof, (const double*)X, U(0));
             launch(k_sub<double, B, B>, grid_for(n, 256), 256, 0, s, R, (const B*)U(0), U(0), n);
         }
-        if (coupled) {
-            CR_CUDA(cudaMemcpyAsync(w3, U(0), sizeof(B) * n, cudaMemcpyDeviceToDevice, s));
-            C.addbcmul(1, dof, (const B*)w3, U(0));
-        }
+        if (coupled) C.addbcmul(1, dof, (const B*)U(0), U(0));  // dots read X before any update: X may alias Y
         C.dot((const B*)U(0), (const B*)U(0), n, kSlotNrm);
         CR_CHECK(C.sync_scal(kSlotNrm, 1));
         err[0] = std::sqrt(L->hscal[kSlotNrm]);
@@ -1097,10 +1098,7 @@ static int gmres(Ctx& C, crimson_subls& ls, const M* Ks, const double* R, double
             B* w = U(i);
             C.vv3s(Ks, (const B*)U(i - 1), w);
             C.addbcmul(0, dof, (const B*)U(i - 1), w);
-            if (coupled) {
-                CR_CUDA(cudaMemcpyAsync(w3, w, sizeof(B) * n, cudaMemcpyDeviceToDevice, s));
-                C.addbcmul(1, dof, (const B*)w3, w);
-            }
+            if (coupled) C.addbcmul(1, dof, (const B*)w, w);
             // fused modified Gram-Schmidt
             for (int j = 1; j <= i; ++j) {
                 const B* uprev = (j == 1) ? nullptr : U(j - 2);
