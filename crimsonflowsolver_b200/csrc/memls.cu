@@ -437,9 +437,9 @@ __global__ void k_max_offset(const int* __restrict__ rowptr, const int* __restri
 // arrays and one scalar array (npad each), G (3, npad) per component,
 // {Gt0, Gt1, Gt2, L} (npad).
 template <typename M>
-__global__ void k_to_sell(const int* __restrict__ rowptr, const int* __restrict__ sp, int n, const M* __restrict__ mK,
-                          const M* __restrict__ mG, const M* __restrict__ Gt, const M* __restrict__ mL,
-                          long long npad, M* __restrict__ Ks, M* __restrict__ Gs,
+__global__ void k_to_sell(const int* __restrict__ rowptr, const int* __restrict__ sp, int n,
+                          const double* __restrict__ mK, const double* __restrict__ mG, const double* __restrict__ Gt,
+                          const double* __restrict__ mL, long long npad, M* __restrict__ Ks, M* __restrict__ Gs,
                           typename V4<M>::type* __restrict__ GLs) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         const size_t base = (size_t)sp[r >> 5] + (r & (kSlice - 1));
@@ -448,13 +448,13 @@ __global__ void k_to_sell(const int* __restrict__ rowptr, const int* __restrict_
             const size_t pos = base + (size_t)kSlice * (j - rs);
             const size_t jj = (size_t)j;
             reinterpret_cast<typename V4<M>::type*>(Ks)[pos] =
-                mk4<M>(mK[9 * jj], mK[9 * jj + 1], mK[9 * jj + 2], mK[9 * jj + 3]);
+                mk4<M>((M)mK[9 * jj], (M)mK[9 * jj + 1], (M)mK[9 * jj + 2], (M)mK[9 * jj + 3]);
             reinterpret_cast<typename V4<M>::type*>(Ks + 4 * npad)[pos] =
-                mk4<M>(mK[9 * jj + 4], mK[9 * jj + 5], mK[9 * jj + 6], mK[9 * jj + 7]);
-            Ks[8 * npad + pos] = mK[9 * jj + 8];
+                mk4<M>((M)mK[9 * jj + 4], (M)mK[9 * jj + 5], (M)mK[9 * jj + 6], (M)mK[9 * jj + 7]);
+            Ks[8 * npad + pos] = (M)mK[9 * jj + 8];
 #pragma unroll
-            for (int q = 0; q < 3; ++q) Gs[q * npad + pos] = mG[3 * jj + q];
-            GLs[pos] = mk4<M>(Gt[3 * jj], Gt[3 * jj + 1], Gt[3 * jj + 2], mL[jj]);
+            for (int q = 0; q < 3; ++q) Gs[q * npad + pos] = (M)mG[3 * jj + q];
+            GLs[pos] = mk4<M>((M)Gt[3 * jj], (M)Gt[3 * jj + 1], (M)Gt[3 * jj + 2], (M)mL[jj]);
         }
     }
 }
@@ -887,10 +887,14 @@ __global__ void k_scale_split_lhs(TangentIn T, const int* __restrict__ rowptr, c
                                   const int* __restrict__ diag, const int* __restrict__ trans,
                                   const double* __restrict__ W, int n, double* __restrict__ mK,
                                   double* __restrict__ mG, double* __restrict__ mD, double* __restrict__ mL) {
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    // 16 lanes per row, one entry per lane: the block reads and writes of a
+    // row are contiguous across the lanes
+    const int sub = threadIdx.x & 15;
+    const int ngroup = (gridDim.x * blockDim.x) >> 4;
+    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; r < n; r += ngroup) {
         const double* wr = W + 4 * (size_t)r;
         const int dg = diag[r];
-        for (int j = rowptr[r]; j < rowptr[r + 1]; ++j) {
+        for (int j = rowptr[r] + sub; j < rowptr[r + 1]; j += 16) {
             const double* wc = W + 4 * (size_t)col[j];
             const size_t jj = (size_t)j, jt = (size_t)trans[j];
             const double Pj[4] = {T.P(jj, 0), T.P(jj, 1), T.P(jj, 2), T.P(jj, 3)};
@@ -1424,22 +1428,16 @@ static int sell_pattern(crimson_lhs* L) {
     return CRIMSON_OK;
 }
 
-// NSSOLVER (memLS.f90:1460-1759); R (4, nNo) FP64 in/out; matrices in M.
-// FP64 CSR matrices for the products that enter NSSOLVER's least-squares
-// problem (the A d of every search direction d).  With them the Gram
-// system, the residual estimate and the outer residuals are those of the
-// FP64 operator while the Krylov solvers run on type-M copies.  All null:
-// the type-M matrices serve (the FP64 path).
-struct OuterMats {
-    const double* K = nullptr;
-    const double* G = nullptr;
-    const double* D = nullptr;
-    const double* L = nullptr;
-};
-
+// NSSOLVER (memLS.f90:1460-1759); R (4, nNo) FP64 in/out.  mK, mG, mD, mL,
+// Gt: the scaled split matrices (FP64 CSR).  GMRES and CGRAD run on sliced
+// copies in M (FP64, or FP32 for the mixed mode) with a type-B GMRES basis;
+// every other product -- the A d of the search directions that enter the
+// least-squares (Gram) problem, the Schur right side D u and the
+// coupled-face vectors -- uses the FP64 matrices, so the Gram system, the
+// residual estimate and the outer residuals are those of the FP64 operator.
 template <typename M, typename B>
-static int nssolver(crimson_lhs* L, crimson_ls* ls, const M* mK, const M* mG, const M* mD, const M* mL, const M* Gt,
-                    double* R, const OuterMats& outer = OuterMats{}) {
+static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const double* mG, const double* mD,
+                    const double* mL, const double* Gt, double* R) {
     Ctx C{L, L->stream};
     cudaStream_t s = L->stream;
     const int nNo = L->nNo;
@@ -1502,26 +1500,17 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const M* mK, const M* mG, co
         CR_CHECK(cgrad<M>(C, ls->CG, (const M*)Gs, (const typename V4<M>::type*)GLs, Pcol(i - 1),
                           cg_nface,
                           cg_coef));
-        if (outer.G)
-            C.sv3(outer.G, (const double*)Pcol(i - 1), MUc(iB - 1));
-        else
-            C.sv3(mG, (const double*)Pcol(i - 1), MUc(iB - 1));
+        C.sv3(mG, (const double*)Pcol(i - 1), MUc(iB - 1));
         launch(k_sub<double, double, double>, grid_for(nv, 256), 256, 0, s, (const double*)L->Rm.p,
                (const double*)MUc(iB - 1), MUc(iBB - 1), nv);
         CR_CHECK((gmres<M, B>(C, ls->GM, (const M*)Ks, MUc(iBB - 1), Ucol(i - 1))));
-        if (outer.K)
-            C.vv3(outer.K, (const double*)Ucol(i - 1), MUc(iBB - 1));
+        if (std::is_same<M, double>::value)
+            C.vv3s((const M*)Ks, (const double*)Ucol(i - 1), MUc(iBB - 1));  // the sliced copy is FP64
         else
-            C.vv3s((const M*)Ks, (const double*)Ucol(i - 1), MUc(iBB - 1));
+            C.vv3(mK, (const double*)Ucol(i - 1), MUc(iBB - 1));
         C.addbcmul(0, 3, (const double*)Ucol(i - 1), MUc(iBB - 1));
-        if (outer.L)
-            C.ss(outer.L, (const double*)Pcol(i - 1), MPc(iB - 1));
-        else
-            C.ss(mL, (const double*)Pcol(i - 1), MPc(iB - 1));
-        if (outer.D)
-            C.vs3(outer.D, (const double*)Ucol(i - 1), MPc(iBB - 1));
-        else
-            C.vs3(mD, (const double*)Ucol(i - 1), MPc(iBB - 1));
+        C.ss(mL, (const double*)Pcol(i - 1), MPc(iB - 1));
+        C.vs3(mD, (const double*)Ucol(i - 1), MPc(iBB - 1));
         // Gram matrix entries for columns iB, iBB
         int slot = kSlotGram;
         for (int k = iB; k <= iBB; ++k) {
@@ -1707,38 +1696,25 @@ static int defect64(crimson_lhs* L, const double* R0, const double* x4, double* 
 }
 
 // NSSOLVER on the scaled system in L->R (in/out).  FP64: the reference's
-// arithmetic.  Mixed: FP32 copies of the scaled split matrices drive every
-// inner matvec (GMRES, CGRAD, the Schur right side); the products A d of the
-// search directions that enter the least-squares problem use the FP64
-// matrices, so a sweep's residual estimate is that of the FP64 operator.
-// Each sweep solves A d = D, adds d to the FP64 solution and forms the FP64
-// defect D = R0 - A x, until |D| <= refine_tol |R0| (RI.relTol when
-// refine_tol <= 0) or max_refine sweeps.  Every sweep's NSSOLVER stops at its own relative tolerances, so
-// the sweeps reach a defect below what one NSSOLVER's estimate can resolve.  Iteration counts are summed
-// over the sweeps.  has_gt: Gt is a separate matrix (host Val path),
+// arithmetic.  Mixed: FP32 sliced copies of the scaled split matrices drive
+// the Krylov matvecs (GMRES, CGRAD); every other product, in particular the
+// A d of the search directions that enter the least-squares problem, uses
+// the FP64 matrices, so a sweep's residual estimate is that of the FP64
+// operator.  Each sweep solves A d = D, adds d to the FP64 solution and
+// forms the FP64 defect D = R0 - A x, until |D| <= refine_tol |R0|
+// (RI.relTol when refine_tol <= 0) or max_refine sweeps.  Every sweep's
+// NSSOLVER stops at its own relative tolerances, so the sweeps reach a
+// defect below what one NSSOLVER's estimate can resolve.  Iteration counts
+// are summed over the sweeps.  has_gt: Gt is a separate matrix (host Val path),
 // otherwise mD serves as Gt.
 static int solve_scaled(crimson_lhs* L, crimson_ls* ls, bool has_gt) {
     cudaStream_t s = L->stream;
     const double* Gt64 = has_gt ? L->Gt.p : L->mD.p;
     if (ls->precision == CRIMSON_FP64)
         return nssolver<double, double>(L, ls, L->mK.p, L->mG.p, L->mD.p, L->mL.p, Gt64, L->R.p);
-    const long long nnz = L->nnz;
     const int n = L->nNo;
-    CR_CHECK(L->mK32.alloc(9 * (size_t)nnz));
-    CR_CHECK(L->mG32.alloc(3 * (size_t)nnz));
-    CR_CHECK(L->mD32.alloc(3 * (size_t)nnz));
-    CR_CHECK(L->mL32.alloc((size_t)nnz));
-    if (has_gt) CR_CHECK(L->Gt32.alloc(3 * (size_t)nnz));
     CR_CHECK(L->R0.alloc(4 * (size_t)n));
     CR_CHECK(L->X4.alloc(4 * (size_t)n));
-    launch(k_convert<float, double>, grid_for(9 * nnz, 256), 256, 0, s, (const double*)L->mK.p, L->mK32.p, 9 * nnz);
-    launch(k_convert<float, double>, grid_for(3 * nnz, 256), 256, 0, s, (const double*)L->mG.p, L->mG32.p, 3 * nnz);
-    launch(k_convert<float, double>, grid_for(3 * nnz, 256), 256, 0, s, (const double*)L->mD.p, L->mD32.p, 3 * nnz);
-    launch(k_convert<float, double>, grid_for(nnz, 256), 256, 0, s, (const double*)L->mL.p, L->mL32.p, nnz);
-    if (has_gt)
-        launch(k_convert<float, double>, grid_for(3 * nnz, 256), 256, 0, s, (const double*)L->Gt.p, L->Gt32.p,
-               3 * nnz);
-    const float* Gt32 = has_gt ? L->Gt32.p : L->mD32.p;
     CR_CUDA(cudaMemcpyAsync(L->R0.p, L->R.p, sizeof(double) * 4 * (size_t)n, cudaMemcpyDeviceToDevice, s));
     CR_CUDA(cudaMemsetAsync(L->X4.p, 0, sizeof(double) * 4 * (size_t)n, s));
     crimson_subls gm{}, cg{}, ri{};
@@ -1759,12 +1735,7 @@ static int solve_scaled(crimson_lhs* L, crimson_ls* ls, bool has_gt) {
     } guard{ls->RI, ls->RI.relTol};
     double sigma = 1.0;
     for (int ref = 0; ref < std::max(ls->max_refine, 1); ++ref) {
-        OuterMats outer;
-        outer.K = L->mK.p;
-        outer.G = L->mG.p;
-        outer.D = L->mD.p;
-        outer.L = L->mL.p;
-        CR_CHECK((nssolver<float, float>(L, ls, L->mK32.p, L->mG32.p, L->mD32.p, L->mL32.p, Gt32, L->R.p, outer)));
+        CR_CHECK((nssolver<float, float>(L, ls, L->mK.p, L->mG.p, L->mD.p, L->mL.p, Gt64, L->R.p)));
         if (ref == 0) {
             gm = ls->GM;
             cg = ls->CG;
@@ -1861,7 +1832,7 @@ int memls_solve_lhs_device(crimson_lhs* L, crimson_ls* ls, const double* d_res, 
     CR_CUDA(cudaMemcpyAsync(L->R.p, d_res, sizeof(double) * 4 * (size_t)L->nNo, cudaMemcpyDeviceToDevice, s));
     launch(k_w_from_lhs, grid_for(L->nNo, 256), 256, 0, s, T, L->diag, L->W.p, L->nNo);
     CR_CHECK(precond_faces(L, false));
-    launch(k_scale_split_lhs, grid_for(L->nNo, 128), 128, 0, s, T, L->rowptr, L->col, L->diag, L->trans,
+    launch(k_scale_split_lhs, grid_for(16LL * L->nNo, 128), 128, 0, s, T, L->rowptr, L->col, L->diag, L->trans,
            (const double*)L->W.p, L->nNo, L->mK.p, L->mG.p, L->mD.p, L->mL.p);
     launch(k_mul, grid_for(4LL * L->nNo, 256), 256, 0, s, L->R.p, (const double*)L->W.p, 4LL * L->nNo);
     CR_CHECK(precond_faces(L, true));

@@ -65,7 +65,6 @@ struct crimson_lhs {
     DBuf<int> cg_tmp;
     // mixed precision: FP32 copies of the scaled split matrices; FP64 right
     // side and accumulated solution of the iterative refinement
-    DBuf<float> mK32, mG32, mD32, mL32, Gt32;
     DBuf<double> R0, X4;
     int refine_steps = 0;
     double refine_rel = 0.0;
