@@ -47,8 +47,8 @@ REFINE_TOL = 0.0      # mixed precision: FP64 defect target (0: the NSSOLVER tol
 # iterations on a 2.07M-tet cylinder (5.3M blocks, matrices and vectors
 # larger than L2); the traffic of a launch grows with blocks x iterations, so
 # the ratio scales the full-size algorithmic bytes to full-size traffic.
-TRAFFIC_PER_ALG_F32 = 0.947
-TRAFFIC_PER_ALG_F64 = 1.001
+TRAFFIC_PER_ALG_F32 = 0.765
+TRAFFIC_PER_ALG_F64 = 0.850
 TRAFFIC_SOURCE = "ncu --set full, k_cg_persistent, 2.07M-tet cylinder, 50 iterations/launch, scaled by blocks"
 # Outer NS iterations and inner GMRES / CG iteration totals per memLS solve on
 # this workload, as counted by the solver on steps 2-5 (identical algorithm
