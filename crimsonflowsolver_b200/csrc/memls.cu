@@ -1065,6 +1065,369 @@ struct Ctx {
     }
 };
 
+// ---------------------------------------------------------------------------
+// One GMRES restart cycle (memLS.f90:715-770) as one persistent cooperative
+// kernel: Arnoldi iterations i = 1..sD with the fused modified Gram-Schmidt
+// order of the launch-per-step path, until |err_i| < eps.  Per iteration:
+// (P1) U(i) = K U(i-1) on the sliced K, with the coupled-face dots
+// S0_f = valM_f . U(i-1) and T_f = valM_f . K U(i-1) of ADDBCMUL; (MGS j)
+// the face terms of ADDBCMUL (op 0, then op 1 with S1_f = T_f + coef0_f S0_f
+// nS_f, exact for node-disjoint faces) folded into the first pass, then
+// U(i) -= h_{j-1} U(j-2) and h_j = <U(i), U(j-1)>; (norm) U(i) -= h_i U(i-1)
+// and |U(i)|^2; every block then applies the Givens rotations to the new
+// Hessenberg column (identical arithmetic in every block, so the exit test
+// agrees) and block 0 stores the column and err; (normalize) U(i) /= h_{i+1}.
+// Every reduction is written per block and summed in block order after the
+// grid barrier (two alternating partial regions).  No host round trip per
+// iteration; the host does the back substitution and X update per cycle.
+// ---------------------------------------------------------------------------
+constexpr int kGmThreads = 512;
+constexpr int kGmMaxSD = 64;
+constexpr int kGmPartStride = 2 * kMaxCoupled + 1;
+
+template <typename M, typename B>
+struct GmArgs {
+    const int* sp;
+    const int* scol;
+    long long npad;
+    int n;
+    const M* Ks;          // sliced K: {K0..K3} (npad), {K4..K7} (npad), K8 (npad)
+    B* u;                 // basis, vector k at u + k n3 (k = 0..sD); u[0] normalized on entry
+    long long n3;
+    int sD;
+    int nface;            // coupled faces (node-disjoint)
+    const int* fidx;      // (n) entry of a coupled-face node, -1 elsewhere
+    const int* fface;     // (entries) face of the entry
+    const double* fval;   // (entries, 3) valM of the entry
+    double coef0[kMaxCoupled], coef1[kMaxCoupled], nS[kMaxCoupled];
+    double err0, eps;
+    double* part;         // 2 regions of kGmPartStride * gridDim
+    double* H;            // (sD + 1, sD) column-major, rotated (written by block 0)
+    double* errv;         // (sD + 1)
+    double* out;          // iterations done, suc
+};
+
+__device__ __forceinline__ double gm_sum(const double* part, int k, double* sm) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += __ldcg(part + (size_t)b * kGmPartStride + k);
+    return block_sum(s, sm);
+}
+
+template <typename M, typename B, int NF>
+__global__ void __launch_bounds__(kGmThreads, 2) k_gmres_cycle(GmArgs<M, B> a) {
+    namespace cgrp = cooperative_groups;
+    cgrp::grid_group grid = cgrp::this_grid();
+    __shared__ double sm[32];
+    __shared__ double sh[kGmMaxSD + 2];  // h_1 .. h_{i+1} of the current column
+    __shared__ double sc[kGmMaxSD], ssn[kGmMaxSD], serr[kGmMaxSD + 1];
+    __shared__ int sdone;
+    const int n = a.n;
+    const long long n3 = a.n3, npad = a.npad;
+    const int tid0 = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    if (threadIdx.x == 0) {
+        serr[0] = a.err0;
+        sdone = 0;
+    }
+    __syncthreads();
+    int bar = 0;  // barrier counter: partial region = bar & 1
+    auto region = [&]() { return a.part + (size_t)(bar & 1) * kGmPartStride * gridDim.x; };
+    int i;
+    for (i = 1; i <= a.sD; ++i) {
+        const B* uin = a.u + (size_t)(i - 1) * n3;
+        B* w = a.u + (size_t)i * n3;
+        // ---- P1: w = K U(i-1); face dots S0_f (on U(i-1)) and T_f (on w) ----
+        double s0[NF > 0 ? NF : 1], tf[NF > 0 ? NF : 1];
+#pragma unroll
+        for (int f = 0; f < (NF > 0 ? NF : 1); ++f) s0[f] = tf[f] = 0.0;
+        for (int r = tid0; r < n; r += nth) {
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+            CR_SELL_ROW_U(4, a.sp, a.scol, r, {
+                const B* uc = uin + 3 * (size_t)c;
+                const double u0 = (double)uc[0], u1 = (double)uc[1], u2 = (double)uc[2];
+                const auto ka = ldcs4(reinterpret_cast<const typename V4<M>::type*>(a.Ks) + pos);
+                const auto kb = ldcs4(reinterpret_cast<const typename V4<M>::type*>(a.Ks + 4 * npad) + pos);
+                const double k8 = (double)__ldcs(a.Ks + 8 * npad + pos);
+                a0 = a0 + (double)ka.x * u0 + (double)ka.y * u1 + (double)ka.z * u2;
+                a1 = a1 + (double)ka.w * u0 + (double)kb.x * u1 + (double)kb.y * u2;
+                a2 = a2 + (double)kb.z * u0 + (double)kb.w * u1 + k8 * u2;
+            })
+            const B w0 = (B)a0, w1 = (B)a1, w2 = (B)a2;
+            w[3 * (size_t)r + 0] = w0;
+            w[3 * (size_t)r + 1] = w1;
+            w[3 * (size_t)r + 2] = w2;
+            if (NF > 0) {
+                const int fe = a.fidx[r];
+                if (fe >= 0) {
+                    const int f = a.fface[fe];
+                    const double* v = a.fval + 3 * (size_t)fe;
+                    const B* ur = uin + 3 * (size_t)r;
+#pragma unroll
+                    for (int q = 0; q < NF; ++q)
+                        if (q == f) {
+                            s0[q] += v[0] * (double)ur[0] + v[1] * (double)ur[1] + v[2] * (double)ur[2];
+                            tf[q] += v[0] * (double)w0 + v[1] * (double)w1 + v[2] * (double)w2;
+                        }
+                }
+            }
+        }
+        double cf[NF > 0 ? NF : 1];
+        if (NF > 0) {
+            double* pr = region();
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                if (f >= a.nface) break;
+                const double x0 = block_sum(s0[f], sm), x1 = block_sum(tf[f], sm);
+                if (threadIdx.x == 0) {
+                    pr[(size_t)blockIdx.x * kGmPartStride + 2 * f] = x0;
+                    pr[(size_t)blockIdx.x * kGmPartStride + 2 * f + 1] = x1;
+                }
+            }
+        }
+        grid.sync();
+        if (NF > 0) {
+            const double* pr = region();
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                cf[f] = 0.0;
+                if (f >= a.nface) continue;
+                const double S0 = gm_sum(pr, 2 * f, sm), T = gm_sum(pr, 2 * f + 1, sm);
+                const double S1 = T + a.coef0[f] * S0 * a.nS[f];
+                cf[f] = a.coef0[f] * S0 + a.coef1[f] * S1;
+            }
+        }
+        ++bar;
+        // ---- MGS passes j = 1..i: h_j = <w, U(j-1)> after w -= h_{j-1} U(j-2) ----
+        for (int j = 1; j <= i; ++j) {
+            const B* uj = a.u + (size_t)(j - 1) * n3;
+            const B* up = j >= 2 ? a.u + (size_t)(j - 2) * n3 : nullptr;
+            const double hp = j >= 2 ? sh[j - 1] : 0.0;
+            double d = 0.0;
+            for (int r = tid0; r < n; r += nth) {
+                int fe = -1;
+                if (NF > 0 && j == 1) fe = a.fidx[r];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const size_t t = 3 * (size_t)r + k;
+                    double wv = (double)w[t];
+                    if (j == 1) {
+                        if (NF > 0 && fe >= 0) {
+                            const int f = a.fface[fe];
+                            double add = 0.0;
+#pragma unroll
+                            for (int q = 0; q < NF; ++q)
+                                if (q == f) add = a.fval[3 * (size_t)fe + k] * cf[q];
+                            wv = (double)(B)(wv + add);
+                            w[t] = (B)wv;
+                        }
+                    } else {
+                        wv = (double)(B)(wv - hp * (double)up[t]);
+                        w[t] = (B)wv;
+                    }
+                    d += wv * (double)__ldcs(uj + t);
+                }
+            }
+            d = block_sum(d, sm);
+            double* pr = region();
+            if (threadIdx.x == 0) pr[(size_t)blockIdx.x * kGmPartStride] = d;
+            grid.sync();
+            const double hj = gm_sum(region(), 0, sm);
+            if (threadIdx.x == 0) sh[j] = hj;
+            ++bar;
+            __syncthreads();
+        }
+        // ---- norm: w -= h_i U(i-1); |w|^2 ----
+        {
+            const double hp = sh[i];
+            double d = 0.0;
+            for (int r = tid0; r < n; r += nth) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const size_t t = 3 * (size_t)r + k;
+                    const double wv = (double)(B)((double)w[t] - hp * (double)uin[t]);
+                    w[t] = (B)wv;
+                    d += wv * wv;
+                }
+            }
+            d = block_sum(d, sm);
+            double* pr = region();
+            if (threadIdx.x == 0) pr[(size_t)blockIdx.x * kGmPartStride] = d;
+            grid.sync();
+            const double hn = gm_sum(region(), 0, sm);
+            ++bar;
+            // ---- Givens (memLS.f90:750-760), identical in every block ----
+            if (threadIdx.x == 0) {
+                double hc[kGmMaxSD + 1];
+                for (int j = 1; j <= i; ++j) hc[j - 1] = sh[j];
+                hc[i] = sqrt(hn);
+                sh[i + 1] = hc[i];
+                double tmp;
+                for (int j = 1; j <= i - 1; ++j) {
+                    tmp = sc[j - 1] * hc[j - 1] + ssn[j - 1] * hc[j];
+                    hc[j] = -ssn[j - 1] * hc[j - 1] + sc[j - 1] * hc[j];
+                    hc[j - 1] = tmp;
+                }
+                tmp = sqrt(hc[i - 1] * hc[i - 1] + hc[i] * hc[i]);
+                sc[i - 1] = hc[i - 1] / tmp;
+                ssn[i - 1] = hc[i] / tmp;
+                hc[i - 1] = tmp;
+                hc[i] = 0.0;
+                serr[i] = -ssn[i - 1] * serr[i - 1];
+                serr[i - 1] = sc[i - 1] * serr[i - 1];
+                if (blockIdx.x == 0) {
+                    for (int j = 0; j <= i; ++j) a.H[(size_t)(i - 1) * (a.sD + 1) + j] = hc[j];
+                    a.errv[i - 1] = serr[i - 1];
+                    a.errv[i] = serr[i];
+                }
+                sdone = fabs(serr[i]) < a.eps ? 1 : 0;
+            }
+            __syncthreads();
+        }
+        if (sdone) break;
+        if (i == a.sD) break;
+        // ---- normalize: U(i) = w / h_{i+1} ----
+        {
+            const double hn = sh[i + 1];
+            for (long long t = tid0; t < n3; t += nth) w[t] = (B)((double)w[t] / hn);
+            grid.sync();
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.out[0] = (double)(i > a.sD ? a.sD : i);
+        a.out[1] = (double)sdone;
+    }
+}
+
+// valM of the coupled faces gathered into (entries, 3): zero past nsd.
+__global__ void k_gm_fval(const double* __restrict__ valM, int fdof, int nsd, int nNoF, double* __restrict__ out) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nNoF; a += gridDim.x * blockDim.x)
+        for (int k = 0; k < 3; ++k) out[3 * (size_t)a + k] = k < nsd ? valM[(size_t)fdof * a + k] : 0.0;
+}
+
+// Coupled-face node map for the persistent cycle: builds it when the set of
+// coupled faces changed; *ok = 0 when two coupled faces share a node (the
+// cycle's closed form of the two ADDBCMUL passes assumes disjoint faces).
+static int gm_face_map(crimson_lhs* L, int* ok) {
+    std::vector<int> cur;
+    for (int k = 0; k < (int)L->face.size(); ++k)
+        if (L->face[k].coupledFlag) cur.push_back(k);
+    if (L->gm_map_ok >= 0 && cur == L->gm_faces) {
+        *ok = L->gm_map_ok;
+        return CRIMSON_OK;
+    }
+    L->gm_faces = cur;
+    L->gm_map_ok = 0;
+    *ok = 0;
+    if ((int)cur.size() > kMaxCoupled) return CRIMSON_OK;
+    cudaStream_t s = L->stream;
+    std::vector<int> fidx((size_t)L->nNo, -1), fface;
+    int entries = 0;
+    for (int q = 0; q < (int)cur.size(); ++q) {
+        const MemlsFace& f = L->face[cur[q]];
+        std::vector<int> g((size_t)f.nNo);
+        CR_CUDA(cudaMemcpyAsync(g.data(), f.glob.p, sizeof(int) * g.size(), cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+        for (int a = 0; a < f.nNo; ++a) {
+            if (g[a] < 0 || g[a] >= L->nNo || fidx[g[a]] >= 0) return CRIMSON_OK;
+            fidx[g[a]] = entries + a;
+            fface.push_back(q);
+        }
+        entries += f.nNo;
+    }
+    CR_CHECK(L->gmFidx.upload(fidx.data(), fidx.size(), s));
+    CR_CHECK(L->gmFface.alloc(std::max<size_t>(1, fface.size())));
+    if (!fface.empty())
+        CR_CUDA(cudaMemcpyAsync(L->gmFface.p, fface.data(), sizeof(int) * fface.size(), cudaMemcpyHostToDevice, s));
+    CR_CHECK(L->gmFval.alloc(3 * (size_t)std::max(1, entries)));
+    CR_CUDA(cudaStreamSynchronize(s));
+    L->gm_map_ok = 1;
+    *ok = 1;
+    return CRIMSON_OK;
+}
+
+// Runs one restart cycle on the device (k_gmres_cycle): U(0) normalized in
+// the basis, err0 = its norm before normalizing.  Returns the iterations
+// done, whether |err_i| < eps was reached, and the rotated Hessenberg
+// columns / err values in the host arrays of gmres().  *used = 0 when the
+// persistent cycle does not apply (sD too large, faces sharing nodes, or no
+// cooperative fit); the caller then runs the launch-per-step loop.
+template <typename M, typename B>
+static int gmres_cycle(Ctx& C, crimson_subls& ls, const M* Ks, double err0, double eps, std::vector<double>& h,
+                       std::vector<double>& err, int* iters, int* suc, int* used) {
+    crimson_lhs* L = C.L;
+    cudaStream_t s = C.s;
+    const int sD = ls.sD;
+    *used = 0;
+    if (sD < 1 || sD > kGmMaxSD) return CRIMSON_OK;
+    int ok = 0;
+    CR_CHECK(gm_face_map(L, &ok));
+    if (!ok) return CRIMSON_OK;
+    const int nface = (int)L->gm_faces.size();
+    const void* fns[3] = {(const void*)k_gmres_cycle<M, B, 0>, (const void*)k_gmres_cycle<M, B, 1>,
+                          (const void*)k_gmres_cycle<M, B, kMaxCoupled>};
+    int& grid = std::is_same<M, float>::value ? L->gm_grid32 : L->gm_grid;
+    if (grid == 0) {
+        int nb = 1 << 30;
+        for (const void* f : fns) {
+            int b = 0;
+            CR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, kGmThreads, 0));
+            nb = std::min(nb, b);
+        }
+        grid = nb >= 1 ? sm_count() * std::min(nb, 2) : -1;
+    }
+    if (grid < 1) return CRIMSON_OK;
+    CR_CHECK(L->gmH.alloc((size_t)(kGmMaxSD + 1) * kGmMaxSD));
+    CR_CHECK(L->gmErr.alloc(kGmMaxSD + 1));
+    CR_CHECK(L->gmOut.alloc(2));
+    CR_CHECK(L->gmPart.alloc(2 * (size_t)kGmPartStride * std::max(L->gm_grid, L->gm_grid32)));
+    GmArgs<M, B> a;
+    a.sp = L->sell_ptr.p;
+    a.scol = L->sell_col.p;
+    a.npad = L->npad;
+    a.n = L->nNo;
+    a.Ks = Ks;
+    a.u = reinterpret_cast<B*>(L->basis.p);
+    a.n3 = 3LL * L->nNo;
+    a.sD = sD;
+    a.nface = nface;
+    a.fidx = L->gmFidx.p;
+    a.fface = L->gmFface.p;
+    a.fval = L->gmFval.p;
+    int off = 0;
+    for (int q = 0; q < nface; ++q) {
+        const MemlsFace& f = L->face[L->gm_faces[q]];
+        launch(k_gm_fval, grid_for(f.nNo, 256), 256, 0, s, (const double*)f.valM.p, f.dof, std::min(f.dof, 3), f.nNo,
+               L->gmFval.p + 3 * (size_t)off);
+        a.coef0[q] = f.res;
+        a.coef1[q] = -f.res / (1.0 + f.res * f.nS);
+        a.nS[q] = f.nS;
+        off += f.nNo;
+    }
+    for (int q = nface; q < kMaxCoupled; ++q) a.coef0[q] = a.coef1[q] = a.nS[q] = 0.0;
+    a.err0 = err0;
+    a.eps = eps;
+    a.part = L->gmPart.p;
+    a.H = L->gmH.p;
+    a.errv = L->gmErr.p;
+    a.out = L->gmOut.p;
+    void* kargs[] = {&a};
+    note_launch();
+    const void* kfn = fns[nface == 0 ? 0 : (nface == 1 ? 1 : 2)];
+    CR_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kGmThreads), kargs, 0, s));
+    double out[2];
+    CR_CUDA(cudaMemcpyAsync(out, L->gmOut.p, sizeof(out), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    const int it = (int)out[0];
+    if (it < 1 || it > sD) return CRIMSON_ERR_STATE;
+    CR_CUDA(cudaMemcpyAsync(h.data(), L->gmH.p, sizeof(double) * (size_t)(sD + 1) * it, cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaMemcpyAsync(err.data(), L->gmErr.p, sizeof(double) * (it + 1), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    CR_CUDA(cudaGetLastError());
+    *iters = it;
+    *suc = out[1] != 0.0 ? 1 : 0;
+    *used = 1;
+    return CRIMSON_OK;
+}
+
 // GMRES (memLS.f90:681-788) on dof = 3; K sliced in M, basis in B, R and X FP64; X may not alias R.
 template <typename M, typename B>
 static int gmres(Ctx& C, crimson_subls& ls, const M* Ks, const double* R, double* X) {
@@ -1109,7 +1472,18 @@ static int gmres(Ctx& C, crimson_subls& ls, const M* Ks, const double* R, double
         }
         ls.dB = ls.fNorm;
         launch(k_divide<B>, grid_for(n, 256), 256, 0, s, (const B*)U(0), (const double*)C.sc(kSlotNrm), U(0), n, 1);
-        for (i = 1; i <= sD; ++i) {
+        // the cycle as one persistent kernel where it applies, else one launch per step
+        int used = 0;
+        {
+            int it = 0, ok = 0;
+            CR_CHECK((gmres_cycle<M, B>(C, ls, Ks, err[0], eps, h, err, &it, &ok, &used)));
+            if (used) {
+                ls.itr = ls.itr + it;
+                i = it;
+                if (ok) ls.suc = 1;
+            }
+        }
+        for (i = used ? i : 1; !used && i <= sD; ++i) {
             ls.itr = ls.itr + 1;
             B* w = U(i);
             C.vv3s(Ks, (const B*)U(i - 1), w);

@@ -63,8 +63,15 @@ struct crimson_lhs {
     int cg_res64 = 0, cg_res32 = 0;    // CG kernel with block-resident columns (per matrix type)
     long long cg_res_bytes = -1;       // its shared memory per block (0: offsets exceed 16 bits); -1 unknown
     DBuf<int> cg_tmp;
-    // mixed precision: FP32 copies of the scaled split matrices; FP64 right
-    // side and accumulated solution of the iterative refinement
+    // persistent GMRES cycle: Hessenberg / err outputs, partial sums and the
+    // coupled-face node map (built for the coupled faces in gm_faces)
+    DBuf<double> gmH, gmErr, gmOut, gmPart, gmFval;
+    DBuf<int> gmFidx, gmFface;
+    std::vector<int> gm_faces;
+    int gm_map_ok = -1;   // 1: map built (faces node-disjoint), 0: not usable, -1: not built
+    int gm_grid = 0, gm_grid32 = 0;
+    // mixed precision: FP64 right side and accumulated solution of the
+    // iterative refinement
     DBuf<double> R0, X4;
     int refine_steps = 0;
     double refine_rel = 0.0;
