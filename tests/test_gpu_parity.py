@@ -209,3 +209,23 @@ def test_reference_mesh_parity(state):
         elm.close()
     for k in ("res", "lhsK", "lhsP"):
         assert relerr(g[k], o[k]) < 1e-12, (k, relerr(g[k], o[k]))
+
+
+def test_time_steps_parity_launch_per_step_gmres():
+    """Krylov space 80 (> 64) runs GMRES through the launch-per-step loop
+    instead of the persistent cycle kernel: the same parity bar."""
+    m = mesh.cylinder(ncross=8, naxial=10)
+    P = FlowParams(rcr=[RCR(srfid=3)], kspace=80)
+    inflow = lambda t: 10.0 + 5.0 * np.sin(2 * np.pi * t / 0.8)
+    F = po.OracleFlow(m, P, inflow=inflow)
+    G = solver.FlowSolver(mesh.cylinder(ncross=8, naxial=10), P, inflow=inflow)
+    try:
+        for _ in range(2):
+            F.step()
+            st = G.step()
+        y, ac = G.state()
+    finally:
+        G.close()
+    assert relerr(y[:, 0:3], F.y[:, 0:3]) < 1e-10, relerr(y[:, 0:3], F.y[:, 0:3])
+    assert relerr(y[:, 3], F.y[:, 3]) < 1e-10, relerr(y[:, 3], F.y[:, 3])
+    assert abs(st.p_out[0] - F.Pn[0]) <= 1e-10 * abs(F.Pn[0])
