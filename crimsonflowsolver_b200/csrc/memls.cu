@@ -393,6 +393,13 @@ template <>
 struct CgStage<double> {
     static constexpr int value = 2;
 };
+// Phase A (G P) of the FP32 kernel holds 5 entries per stage: its three
+// 4-byte component loads per entry put fewer bytes in flight than phase B's
+// one 16-byte record (measured 4% per iteration over 4; 6 spills).
+template <typename M>
+struct CgStageA {
+    static constexpr int value = sizeof(M) == 4 ? 5 : 2;
+};
 
 // KU = K U on the sliced copy: K as {K0..K3} and {K4..K7} 4-vectors (npad
 // each, one 16/32-byte load apiece) and K8 (npad); U / KU (3, n).
@@ -595,6 +602,7 @@ __global__ void __launch_bounds__(kCgThreads, 2) k_cg_persistent(CgArgs<M> a) {
     double* partC = a.part + 2 * (size_t)gridDim.x * kCgPartStride;
     const int wbase = kRes ? cg_fill_cols(a.sp, a.scol, n, cg_res) : 0;
     constexpr int U = CgStage<M>::value;
+    constexpr int UA = CgStageA<M>::value;
     double err = a.err0, errO = a.err0;
     int suc = 0, i;
     for (i = 1; i <= a.mItr; ++i) {
@@ -618,10 +626,10 @@ __global__ void __launch_bounds__(kCgThreads, 2) k_cg_persistent(CgArgs<M> a) {
             const int base = p0 + (r & (kSlice - 1));
             // stage: G values and columns of U entries; the next stage is
             // loaded before this stage's gathers
-            M g0[U], g1[U], g2[U];
-            int cc[U];
+            M g0[UA], g1[UA], g2[UA];
+            int cc[UA];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
+            for (int u = 0; u < UA; ++u) {
                 const bool in = u < w;
                 const size_t pos = (size_t)base + kSlice * u;
                 g0[u] = in ? __ldcs(a.G + pos) : M(0);
@@ -629,20 +637,20 @@ __global__ void __launch_bounds__(kCgThreads, 2) k_cg_persistent(CgArgs<M> a) {
                 g2[u] = in ? __ldcs(a.G + 2 * npad + pos) : M(0);
                 cc[u] = (!kRes && in) ? cs.col(r, base, u) : r;  // resident columns are read at use
             }
-            for (int k0 = 0; k0 < w; k0 += U) {
-                M n0[U], n1[U], n2[U];
-                int nc[U];
+            for (int k0 = 0; k0 < w; k0 += UA) {
+                M n0[UA], n1[UA], n2[UA];
+                int nc[UA];
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const bool in = k0 + U + u < w;
-                    const size_t pos = (size_t)base + kSlice * (k0 + U + u);
+                for (int u = 0; u < UA; ++u) {
+                    const bool in = k0 + UA + u < w;
+                    const size_t pos = (size_t)base + kSlice * (k0 + UA + u);
                     n0[u] = in ? __ldcs(a.G + pos) : M(0);
                     n1[u] = in ? __ldcs(a.G + npad + pos) : M(0);
                     n2[u] = in ? __ldcs(a.G + 2 * npad + pos) : M(0);
-                    nc[u] = (!kRes && in) ? cs.col(r, base, k0 + U + u) : r;
+                    nc[u] = (!kRes && in) ? cs.col(r, base, k0 + UA + u) : r;
                 }
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
+                for (int u = 0; u < UA; ++u) {
                     if (k0 + u < w) {
                         const double2 rp = a.recA[kRes ? cs.col(r, base, k0 + u) : cc[u]];
                         const double pc = first ? rp.x : rp.x + beta * rp.y;
@@ -652,7 +660,7 @@ __global__ void __launch_bounds__(kCgThreads, 2) k_cg_persistent(CgArgs<M> a) {
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
+                for (int u = 0; u < UA; ++u) {
                     g0[u] = n0[u];
                     g1[u] = n1[u];
                     g2[u] = n2[u];
