@@ -383,19 +383,18 @@ constexpr int kSellUnroll = 8;
 #define CR_SELL_ROW(sp, scol, r, ...) CR_SELL_ROW_U(kSellUnroll, sp, scol, r, __VA_ARGS__)
 // Entries per stage of the CG's software-pipelined row loops: the matrix
 // records of the next stage are loaded while the current stage's gathers are
-// in flight (two stages live: 2 x 4 x 16 B FP32, 2 x 2 x 32 B FP64, within
+// in flight (two stages live: 2 x 5 x 16 B FP32, 2 x 2 x 32 B FP64, within
 // the 64 registers of two 512-thread blocks per SM).
 template <typename M>
 struct CgStage {
-    static constexpr int value = 4;
+    static constexpr int value = 5;
 };
 template <>
 struct CgStage<double> {
     static constexpr int value = 2;
 };
-// Phase A (G P) of the FP32 kernel holds 5 entries per stage: its three
-// 4-byte component loads per entry put fewer bytes in flight than phase B's
-// one 16-byte record (measured 4% per iteration over 4; 6 spills).
+// Phase A (G P) uses its own stage width (5 FP32 entries, 2 FP64: FP32
+// measured 4% faster per iteration than 4, 6 spills; FP64 3 spills).
 template <typename M>
 struct CgStageA {
     static constexpr int value = sizeof(M) == 4 ? 5 : 2;
