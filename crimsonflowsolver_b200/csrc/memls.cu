@@ -1078,8 +1078,8 @@ struct Ctx {
 // order of the launch-per-step path, until |err_i| < eps.  Per iteration:
 // (P1) U(i) = K U(i-1) on the sliced K, with the coupled-face dots
 // S0_f = valM_f . U(i-1) and T_f = valM_f . K U(i-1) of ADDBCMUL; (MGS j)
-// the face terms of ADDBCMUL (op 0, then op 1 with S1_f = T_f + coef0_f S0_f
-// nS_f, exact for node-disjoint faces) folded into the first pass, then
+// the face terms of ADDBCMUL (op 0, then op 1 with S1_f = T_f + sum_g
+// coef0_g S0_g (valM_f . valM_g)) folded into the first pass, then
 // U(i) -= h_{j-1} U(j-2) and h_j = <U(i), U(j-1)>; (norm) U(i) -= h_i U(i-1)
 // and |U(i)|^2; every block then applies the Givens rotations to the new
 // Hessenberg column (identical arithmetic in every block, so the exit test
@@ -1102,11 +1102,13 @@ struct GmArgs {
     B* u;                 // basis, vector k at u + k n3 (k = 0..sD); u[0] normalized on entry
     long long n3;
     int sD;
-    int nface;            // coupled faces (node-disjoint)
-    const int* fidx;      // (n) entry of a coupled-face node, -1 elsewhere
+    int nface;            // coupled faces
+    const int* fptr;      // (n + 1) entries of node r: fent[fptr[r] .. fptr[r + 1])
+    const int* fent;      // entry ids grouped by node
     const int* fface;     // (entries) face of the entry
     const double* fval;   // (entries, 3) valM of the entry
-    double coef0[kMaxCoupled], coef1[kMaxCoupled], nS[kMaxCoupled];
+    const double* gram;   // (nface, nface) valM_f . valM_g (diagonal: nS)
+    double coef0[kMaxCoupled], coef1[kMaxCoupled];
     double err0, eps;
     double* part;         // 2 regions of kGmPartStride * gridDim
     double* H;            // (sD + 1, sD) column-major, rotated (written by block 0)
@@ -1163,8 +1165,8 @@ __global__ void __launch_bounds__(kGmThreads, 2) k_gmres_cycle(GmArgs<M, B> a) {
             w[3 * (size_t)r + 1] = w1;
             w[3 * (size_t)r + 2] = w2;
             if (NF > 0) {
-                const int fe = a.fidx[r];
-                if (fe >= 0) {
+                for (int k = a.fptr[r]; k < a.fptr[r + 1]; ++k) {
+                    const int fe = a.fent[k];
                     const int f = a.fface[fe];
                     const double* v = a.fval + 3 * (size_t)fe;
                     const B* ur = uin + 3 * (size_t)r;
@@ -1193,13 +1195,21 @@ __global__ void __launch_bounds__(kGmThreads, 2) k_gmres_cycle(GmArgs<M, B> a) {
         grid.sync();
         if (NF > 0) {
             const double* pr = region();
+            double S0[NF > 0 ? NF : 1], T[NF > 0 ? NF : 1];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                S0[f] = T[f] = 0.0;
+                if (f >= a.nface) continue;
+                S0[f] = gm_sum(pr, 2 * f, sm);
+                T[f] = gm_sum(pr, 2 * f + 1, sm);
+            }
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 cf[f] = 0.0;
                 if (f >= a.nface) continue;
-                const double S0 = gm_sum(pr, 2 * f, sm), T = gm_sum(pr, 2 * f + 1, sm);
-                const double S1 = T + a.coef0[f] * S0 * a.nS[f];
-                cf[f] = a.coef0[f] * S0 + a.coef1[f] * S1;
+                double S1 = T[f];
+                for (int g = 0; g < a.nface; ++g) S1 += a.coef0[g] * S0[g] * a.gram[f * a.nface + g];
+                cf[f] = a.coef0[f] * S0[f] + a.coef1[f] * S1;
             }
         }
         ++bar;
@@ -1210,19 +1220,25 @@ __global__ void __launch_bounds__(kGmThreads, 2) k_gmres_cycle(GmArgs<M, B> a) {
             const double hp = j >= 2 ? sh[j - 1] : 0.0;
             double d = 0.0;
             for (int r = tid0; r < n; r += nth) {
-                int fe = -1;
-                if (NF > 0 && j == 1) fe = a.fidx[r];
+                int k0 = 0, k1 = 0;
+                if (NF > 0 && j == 1) {
+                    k0 = a.fptr[r];
+                    k1 = a.fptr[r + 1];
+                }
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     const size_t t = 3 * (size_t)r + k;
                     double wv = (double)w[t];
                     if (j == 1) {
-                        if (NF > 0 && fe >= 0) {
-                            const int f = a.fface[fe];
+                        if (NF > 0 && k1 > k0) {
                             double add = 0.0;
+                            for (int e = k0; e < k1; ++e) {
+                                const int fe = a.fent[e];
+                                const int f = a.fface[fe];
 #pragma unroll
-                            for (int q = 0; q < NF; ++q)
-                                if (q == f) add = a.fval[3 * (size_t)fe + k] * cf[q];
+                                for (int q = 0; q < NF; ++q)
+                                    if (q == f) add += a.fval[3 * (size_t)fe + k] * cf[q];
+                            }
                             wv = (double)(B)(wv + add);
                             w[t] = (B)wv;
                         }
@@ -1310,9 +1326,11 @@ __global__ void k_gm_fval(const double* __restrict__ valM, int fdof, int nsd, in
         for (int k = 0; k < 3; ++k) out[3 * (size_t)a + k] = k < nsd ? valM[(size_t)fdof * a + k] : 0.0;
 }
 
-// Coupled-face node map for the persistent cycle: builds it when the set of
-// coupled faces changed; *ok = 0 when two coupled faces share a node (the
-// cycle's closed form of the two ADDBCMUL passes assumes disjoint faces).
+// Coupled-face map for the persistent cycle, rebuilt when the set of
+// coupled faces changes: the entries (face node a of coupled face q, in face
+// order) grouped by node (fptr / fent), the face of each entry, and the
+// pairs of entries of different faces at one node (faces that share rim
+// nodes), from which k_gm_gram forms the off-diagonal valM_f . valM_g.
 static int gm_face_map(crimson_lhs* L, int* ok) {
     std::vector<int> cur;
     for (int k = 0; k < (int)L->face.size(); ++k)
@@ -1326,36 +1344,73 @@ static int gm_face_map(crimson_lhs* L, int* ok) {
     *ok = 0;
     if ((int)cur.size() > kMaxCoupled) return CRIMSON_OK;
     cudaStream_t s = L->stream;
-    std::vector<int> fidx((size_t)L->nNo, -1), fface;
-    int entries = 0;
+    const int n = L->nNo;
+    std::vector<int> node_of, fface;
     for (int q = 0; q < (int)cur.size(); ++q) {
         const MemlsFace& f = L->face[cur[q]];
         std::vector<int> g((size_t)f.nNo);
         CR_CUDA(cudaMemcpyAsync(g.data(), f.glob.p, sizeof(int) * g.size(), cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
         for (int a = 0; a < f.nNo; ++a) {
-            if (g[a] < 0 || g[a] >= L->nNo || fidx[g[a]] >= 0) return CRIMSON_OK;
-            fidx[g[a]] = entries + a;
+            if (g[a] < 0 || g[a] >= n) return CRIMSON_OK;
+            node_of.push_back(g[a]);
             fface.push_back(q);
         }
-        entries += f.nNo;
     }
-    CR_CHECK(L->gmFidx.upload(fidx.data(), fidx.size(), s));
+    const int entries = (int)node_of.size();
+    std::vector<int> fptr((size_t)n + 1, 0), fent((size_t)std::max(1, entries));
+    for (int e = 0; e < entries; ++e) ++fptr[(size_t)node_of[e] + 1];
+    for (int r = 0; r < n; ++r) fptr[(size_t)r + 1] += fptr[r];
+    std::vector<int> fill(fptr.begin(), fptr.end() - 1);
+    for (int e = 0; e < entries; ++e) fent[(size_t)fill[node_of[e]]++] = e;
+    std::vector<int> pairs;  // (e1, e2) of different faces at one node
+    for (int r = 0; r < n; ++r)
+        for (int k1 = fptr[r]; k1 < fptr[(size_t)r + 1]; ++k1)
+            for (int k2 = fptr[r]; k2 < fptr[(size_t)r + 1]; ++k2)
+                if (k1 != k2 && fface[fent[k1]] != fface[fent[k2]]) {
+                    pairs.push_back(fent[k1]);
+                    pairs.push_back(fent[k2]);
+                }
+    CR_CHECK(L->gmFptr.upload(fptr.data(), fptr.size(), s));
+    CR_CHECK(L->gmFent.upload(fent.data(), fent.size(), s));
     CR_CHECK(L->gmFface.alloc(std::max<size_t>(1, fface.size())));
     if (!fface.empty())
         CR_CUDA(cudaMemcpyAsync(L->gmFface.p, fface.data(), sizeof(int) * fface.size(), cudaMemcpyHostToDevice, s));
+    L->gm_npairs = (int)pairs.size() / 2;
+    CR_CHECK(L->gmPairs.alloc(std::max<size_t>(2, pairs.size())));
+    if (!pairs.empty())
+        CR_CUDA(cudaMemcpyAsync(L->gmPairs.p, pairs.data(), sizeof(int) * pairs.size(), cudaMemcpyHostToDevice, s));
     CR_CHECK(L->gmFval.alloc(3 * (size_t)std::max(1, entries)));
+    CR_CHECK(L->gmGram.alloc((size_t)kMaxCoupled * kMaxCoupled));
     CR_CUDA(cudaStreamSynchronize(s));
     L->gm_map_ok = 1;
     *ok = 1;
     return CRIMSON_OK;
 }
 
+// valM_f . valM_g of the coupled faces: nS on the diagonal, the shared-node
+// pairs off it (one thread, fixed order).
+struct FaceNorms {
+    double v[kMaxCoupled];
+};
+__global__ void k_gm_gram(const int* __restrict__ pairs, int npairs, const int* __restrict__ fface,
+                          const double* __restrict__ fval, FaceNorms nS, int nface, double* __restrict__ gram) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int f = 0; f < nface; ++f)
+        for (int g = 0; g < nface; ++g) gram[f * nface + g] = f == g ? nS.v[f] : 0.0;
+    for (int p = 0; p < npairs; ++p) {
+        const int e1 = pairs[2 * p], e2 = pairs[2 * p + 1];
+        const double* v1 = fval + 3 * (size_t)e1;
+        const double* v2 = fval + 3 * (size_t)e2;
+        gram[fface[e1] * nface + fface[e2]] += v1[0] * v2[0] + v1[1] * v2[1] + v1[2] * v2[2];
+    }
+}
+
 // Runs one restart cycle on the device (k_gmres_cycle): U(0) normalized in
 // the basis, err0 = its norm before normalizing.  Returns the iterations
 // done, whether |err_i| < eps was reached, and the rotated Hessenberg
 // columns / err values in the host arrays of gmres().  *used = 0 when the
-// persistent cycle does not apply (sD too large, faces sharing nodes, or no
+// persistent cycle does not apply (sD too large, more than 8 coupled faces, or no
 // cooperative fit); the caller then runs the launch-per-step loop.
 template <typename M, typename B>
 static int gmres_cycle(Ctx& C, crimson_subls& ls, const M* Ks, double err0, double eps, std::vector<double>& h,
@@ -1396,9 +1451,12 @@ static int gmres_cycle(Ctx& C, crimson_subls& ls, const M* Ks, double err0, doub
     a.n3 = 3LL * L->nNo;
     a.sD = sD;
     a.nface = nface;
-    a.fidx = L->gmFidx.p;
+    a.fptr = L->gmFptr.p;
+    a.fent = L->gmFent.p;
     a.fface = L->gmFface.p;
     a.fval = L->gmFval.p;
+    a.gram = L->gmGram.p;
+    FaceNorms nsv{};
     int off = 0;
     for (int q = 0; q < nface; ++q) {
         const MemlsFace& f = L->face[L->gm_faces[q]];
@@ -1406,10 +1464,13 @@ static int gmres_cycle(Ctx& C, crimson_subls& ls, const M* Ks, double err0, doub
                L->gmFval.p + 3 * (size_t)off);
         a.coef0[q] = f.res;
         a.coef1[q] = -f.res / (1.0 + f.res * f.nS);
-        a.nS[q] = f.nS;
+        nsv.v[q] = f.nS;
         off += f.nNo;
     }
-    for (int q = nface; q < kMaxCoupled; ++q) a.coef0[q] = a.coef1[q] = a.nS[q] = 0.0;
+    for (int q = nface; q < kMaxCoupled; ++q) a.coef0[q] = a.coef1[q] = 0.0;
+    if (nface > 0)
+        launch(k_gm_gram, 1, 32, 0, s, (const int*)L->gmPairs.p, L->gm_npairs, (const int*)L->gmFface.p,
+               (const double*)L->gmFval.p, nsv, nface, L->gmGram.p);
     a.err0 = err0;
     a.eps = eps;
     a.part = L->gmPart.p;

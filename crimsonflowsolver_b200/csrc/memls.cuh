@@ -65,10 +65,11 @@ struct crimson_lhs {
     DBuf<int> cg_tmp;
     // persistent GMRES cycle: Hessenberg / err outputs, partial sums and the
     // coupled-face node map (built for the coupled faces in gm_faces)
-    DBuf<double> gmH, gmErr, gmOut, gmPart, gmFval;
-    DBuf<int> gmFidx, gmFface;
+    DBuf<double> gmH, gmErr, gmOut, gmPart, gmFval, gmGram;
+    DBuf<int> gmFptr, gmFent, gmFface, gmPairs;
     std::vector<int> gm_faces;
-    int gm_map_ok = -1;   // 1: map built (faces node-disjoint), 0: not usable, -1: not built
+    int gm_npairs = 0;
+    int gm_map_ok = -1;   // 1: map built, 0: not usable (more than 8 coupled faces), -1: not built
     int gm_grid = 0, gm_grid32 = 0;
     // mixed precision: FP64 right side and accumulated solution of the
     // iterative refinement

@@ -229,3 +229,25 @@ def test_time_steps_parity_launch_per_step_gmres():
     assert relerr(y[:, 0:3], F.y[:, 0:3]) < 1e-10, relerr(y[:, 0:3], F.y[:, 0:3])
     assert relerr(y[:, 3], F.y[:, 3]) < 1e-10, relerr(y[:, 3], F.y[:, 3])
     assert abs(st.p_out[0] - F.Pn[0]) <= 1e-10 * abs(F.Pn[0])
+
+
+def test_multi_outlet_time_steps_parity():
+    """Three RCR outlets splitting one cap: the outlet surfaces share their
+    rim nodes, so the two ADDBCMUL passes of every GMRES product couple the
+    faces (the persistent GMRES cycle carries their valM Gram matrix)."""
+    m = mesh.cylinder(ncross=8, naxial=8, n_outlets=3)
+    P = FlowParams(rcr=[RCR(srfid=3), RCR(srfid=4, Rp=120.0, C=1.2e-4), RCR(srfid=5, Rd=900.0)])
+    inflow = lambda t: 10.0 + 5.0 * np.sin(2 * np.pi * t / 0.8)
+    F = po.OracleFlow(m, P, inflow=inflow)
+    G = solver.FlowSolver(mesh.cylinder(ncross=8, naxial=8, n_outlets=3), P, inflow=inflow)
+    try:
+        for _ in range(2):
+            F.step()
+            st = G.step()
+        y, ac = G.state()
+    finally:
+        G.close()
+    assert relerr(y[:, 0:3], F.y[:, 0:3]) < 1e-10, relerr(y[:, 0:3], F.y[:, 0:3])
+    assert relerr(y[:, 3], F.y[:, 3]) < 1e-10, relerr(y[:, 3], F.y[:, 3])
+    for k in range(3):
+        assert abs(st.p_out[k] - F.Pn[k]) <= 1e-10 * abs(F.Pn[k])
