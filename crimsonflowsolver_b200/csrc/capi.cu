@@ -166,6 +166,45 @@ int crimson_ctx_create(crimson_ctx** out, const crimson_params* p, int nshg, int
                        const double* x) {
     if (!out || !ien || !x || nshg <= 0 || numnp < nshg || nelem <= 0) return CRIMSON_ERR_ARG;
     CR_CHECK(check_params(p));
+    // The mesh is checked on the host before any device work: node indices in
+    // range, finite coordinates, and every tet oriented as e3metric assumes,
+    // det[x1 - x4, x2 - x4, x3 - x4] > 0 (a zero or negative volume would give
+    // an infinite or sign-flipped WdetJ).
+    std::vector<double4> hx(numnp);
+    for (int i = 0; i < numnp; ++i) {
+        hx[i] = make_double4(x[i], x[(size_t)numnp + i], x[2 * (size_t)numnp + i], 0.0);
+        if (!std::isfinite(hx[i].x) || !std::isfinite(hx[i].y) || !std::isfinite(hx[i].z)) {
+            set_last_error("non-finite coordinate at node " + std::to_string(i + 1));
+            return CRIMSON_ERR_ARG;
+        }
+    }
+    std::vector<int4> hien(nelem);
+    for (int i = 0; i < nelem; ++i) {
+        int v[4];
+        for (int a = 0; a < 4; ++a) {
+            v[a] = std::abs(ien[(size_t)a * nelem + i]) - 1;
+            if (v[a] < 0 || v[a] >= nshg) {
+                set_last_error("ien out of range at element " + std::to_string(i + 1));
+                return CRIMSON_ERR_ARG;
+            }
+        }
+        const double4 p4 = hx[v[3]];
+        double d[3][3];
+        for (int a = 0; a < 3; ++a) {
+            d[a][0] = hx[v[a]].x - p4.x;
+            d[a][1] = hx[v[a]].y - p4.y;
+            d[a][2] = hx[v[a]].z - p4.z;
+        }
+        const double det = d[0][0] * (d[1][1] * d[2][2] - d[1][2] * d[2][1]) -
+                           d[0][1] * (d[1][0] * d[2][2] - d[1][2] * d[2][0]) +
+                           d[0][2] * (d[1][0] * d[2][1] - d[1][1] * d[2][0]);
+        if (!(det > 0.0)) {
+            set_last_error("element " + std::to_string(i + 1) +
+                           ": zero or negative volume (nodes must satisfy det[x1-x4, x2-x4, x3-x4] > 0)");
+            return CRIMSON_ERR_ARG;
+        }
+        hien[i] = make_int4(v[0], v[1], v[2], v[3]);
+    }
     crimson_ctx* c = new crimson_ctx();
     c->p = *p;
     c->nshg = nshg;
@@ -177,22 +216,6 @@ int crimson_ctx_create(crimson_ctx** out, const crimson_params* p, int nshg, int
         delete c;
         return CRIMSON_ERR_CUDA;
     }
-    std::vector<int4> hien(nelem);
-    for (int i = 0; i < nelem; ++i) {
-        int v[4];
-        for (int a = 0; a < 4; ++a) {
-            v[a] = std::abs(ien[(size_t)a * nelem + i]) - 1;
-            if (v[a] < 0 || v[a] >= nshg) {
-                set_last_error("ien out of range");
-                crimson_ctx_destroy(c);
-                return CRIMSON_ERR_ARG;
-            }
-        }
-        hien[i] = make_int4(v[0], v[1], v[2], v[3]);
-    }
-    std::vector<double4> hx(numnp);
-    for (int i = 0; i < numnp; ++i)
-        hx[i] = make_double4(x[i], x[(size_t)numnp + i], x[2 * (size_t)numnp + i], 0.0);
     int rc = c->ien.upload(hien.data(), hien.size(), c->stream);
     if (rc == CRIMSON_OK) rc = c->x.upload(hx.data(), hx.size(), c->stream);
     std::vector<int> zi(nshg, 0);

@@ -1780,6 +1780,7 @@ static int cgrad(Ctx& C, crimson_subls& ls, const M* Gs, const typename V4<M>::t
 static int ge_solve(int N, const double* A, double* B) {
     if (N == 2) {
         double pivot = A[0] * A[3] - A[1] * A[2];
+        if (pivot == 0.0 || !std::isfinite(pivot)) return CRIMSON_ERR_SINGULAR;
         double saveEl = (B[0] * A[3] - B[1] * A[2]) / pivot;
         B[1] = (B[1] * A[0] - B[0] * A[1]) / pivot;
         B[0] = saveEl;
@@ -1912,6 +1913,10 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
     CR_CHECK(C.sync_scal(0, 2));
     double nv1 = std::sqrt(L->hscal[0]), ns1 = std::sqrt(L->hscal[1]);
     double eps = std::sqrt(std::pow(nv1, 2.0) + std::pow(ns1, 2.0));
+    if (!std::isfinite(eps)) {
+        set_last_error("NSSOLVER: non-finite right-hand side");
+        return CRIMSON_ERR_NONFINITE;
+    }
     ls->RI.iNorm = eps;
     ls->RI.fNorm = eps;
     ls->CG.callD = 0.0;
@@ -1995,6 +2000,11 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
         for (int c = 0; c < iBB; ++c)
             for (int r = 0; r < iBB; ++r) Asub[(size_t)c * iBB + r] = Aa(r, c);
         CR_CHECK(ge_solve(iBB, Asub.data(), xB.data()));
+        for (int t = 0; t < iBB; ++t)
+            if (!std::isfinite(xB[t])) {
+                set_last_error("NSSOLVER: non-finite least-squares coefficients");
+                return CRIMSON_ERR_NONFINITE;
+            }
         double sxb = 0.0;
         for (int t = 0; t < iBB; ++t) sxb = sxb + xB[t] * Bv[t];
         ls->RI.fNorm = std::sqrt(std::pow(ls->RI.iNorm, 2.0) - sxb);
