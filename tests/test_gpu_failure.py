@@ -9,7 +9,16 @@ import numpy as np
 import pytest
 
 from crimsonflowsolver_b200 import FlowParams, RCR, mesh, solver
+from crimsonflowsolver_b200 import _native as N
 from tests.conftest import relerr
+
+
+def _rcr(F, set_to=None):
+    """Read (or write) the RCR history (P_n, Q_n) of a solver's context."""
+    P = np.zeros(1) if set_to is None else np.array(set_to[0], dtype=np.float64)
+    Q = np.zeros(1) if set_to is None else np.array(set_to[1], dtype=np.float64)
+    N.check(N.lib().crimson_rcr_state(F.elm.h, 1, N.dp(P), N.dp(Q), 0 if set_to is None else 1), "crimson_rcr_state")
+    return P.copy(), Q.copy()
 
 pytestmark = pytest.mark.gpu
 
@@ -30,6 +39,7 @@ def test_nonfinite_state_returns_status_and_context_recovers(precision):
             F.step()
         F.set_state(y, ac)
         G.set_state(y, ac)
+        _rcr(G, _rcr(F))   # the failed step left F's outlet history as it was after step 1
         F.istep = G.istep = 1
         F.step()
         G.step()
