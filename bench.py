@@ -389,7 +389,7 @@ def run_ours(args):
                    "parallelism": "replicas" if ws > 1 else "single GPU",
                    "epstol_ns": P.epstol_ns, "epstol_gmres_cg": [P.epstol_mom, P.epstol_cont],
                    "mixed_refine_tol": Pm.refine_tol if Pm.refine_tol > 0 else P.epstol_ns,
-                   "l2": "inputs larger than L2 (FP32 matrices 0.45 GB, FP64 1.3 GB per solve)"},
+                   "l2": "inputs larger than L2 (sliced FP32 matrices 0.66 GB, FP64 1.33 GB per solve)"},
         "fp64": {"value": v64, "unit": "s/timestep", "ms_per_step": t64_ms / args.steps,
                  "solver_iters_per_solve": it64, "gpu_launches": l64, "clocks": clk64},
         "mixed_speedup_vs_fp64": v64 / value,
