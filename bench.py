@@ -131,7 +131,8 @@ def workload_name(args, m) -> str:
         return (f"{m.nelem / 1e6:.1f}M-tet Y-bifurcation ({m.nelem} tets, {m.nshg} nodes; parent R 1 cm, daughters "
                 "R 0.7 cm at +-30 deg, 2 RCR outlets +-20% seeded), pulsatile inflow, dt=1e-3, 3 nonlinear "
                 "iterations/step")
-    return (f"4.0M-tet cylinder ({m.nelem} tets, {m.nshg} nodes), pulsatile inflow, RCR outlet, dt=1e-3, "
+    size = f"{m.nelem / 1e6:.1f}M" if m.nelem >= 1e6 else f"{m.nelem / 1e3:.0f}k"
+    return (f"{size}-tet cylinder ({m.nelem} tets, {m.nshg} nodes), pulsatile inflow, RCR outlet, dt=1e-3, "
             "3 nonlinear iterations/step")
 
 
