@@ -142,9 +142,11 @@ int crimson_memls_ls_create(crimson_ls** ls, int LS_type, int present_mask, doub
 int crimson_memls_ls_free(crimson_ls* ls);
 /* Arithmetic of the NS solve; no counterpart in the reference (memLS is FP64
  * throughout).  CRIMSON_FP64 (default): memLS's arithmetic.  CRIMSON_MIXED:
- * FP32 copies of the scaled block matrices in every inner Krylov matvec and an
- * FP32 GMRES basis; FP64 outer vectors, dot products, Givens rotations, Gram
- * system and CG recurrences; FP64 iterative refinement on the defect
+ * FP32 copies of the scaled block matrices in every GMRES and CG matvec and
+ * an FP32 GMRES basis; FP64 for every other product (the least-squares
+ * products A d, so the NSSOLVER residual estimate is the FP64 operator's),
+ * outer vectors, dot products, Givens rotations, Gram system and CG
+ * recurrences; FP64 iterative refinement on the defect
  * R - A x until |R - A x| <= refine_tol |R| (relTol of memLS_LS_CREATE when
  * refine_tol <= 0) or max_refine sweeps (1..64).
  * Applies to crimson_memls_solve, crimson_solflow_device and crimson_step.
