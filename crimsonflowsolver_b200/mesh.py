@@ -412,7 +412,7 @@ def random_state(nshg: int, seed: int = 5, dtype=np.float64):
 
 
 def cylinder_for_tets(target_tets: int, **kw) -> Mesh:
-    """Cylinder with the cfg1 aspect (ncross:naxial = 24:40) sized to ~target_tets."""
+    """Cylinder with the 60k-tet case's aspect (ncross:naxial = 24:40) sized to ~target_tets."""
     # tets ~= 6 * (pi/4) * ncross^2 * naxial with naxial = 5/3 ncross
     nc = int(round((target_tets / (6 * np.pi / 4 * 5.0 / 3.0)) ** (1.0 / 3.0)))
     return cylinder(ncross=nc, naxial=int(round(nc * 5.0 / 3.0)), **kw)
