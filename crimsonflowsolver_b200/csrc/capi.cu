@@ -437,6 +437,12 @@ int crimson_memls_ls_set_precision(crimson_ls* ls, int precision, int max_refine
     return CRIMSON_OK;
 }
 
+int crimson_memls_ls_set_log(crimson_ls* ls, const char* path) {
+    if (!ls) return CRIMSON_ERR_ARG;
+    ls->log_path = path ? std::string(path) : std::string();
+    return CRIMSON_OK;
+}
+
 int crimson_memls_refine_info(const crimson_lhs* L, int* steps, double* rel) {
     if (!L) return CRIMSON_ERR_ARG;
     if (steps) *steps = L->refine_steps;

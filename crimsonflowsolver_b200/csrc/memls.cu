@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 
 #include "common.cuh"
@@ -2122,6 +2123,35 @@ static int precond_faces(crimson_lhs* L, bool after_scale) {
     return CRIMSON_OK;
 }
 
+// One line per NS solve in the format of memLS's LOGFILE
+// (flowsolver/src/memLS.f90:1720-1757), appended to ls->log_path when set:
+// a header "gnNo nTasks nCoupledFaces" when the file is new, then the
+// success code (100 RI + 10 GM + CG), RI / GM / CG iterations, the time
+// split other / GM / CG in percent, the initial norm, the relative final
+// norm, the wall time, Resm, Resc and dB.
+static void log_solve(const crimson_lhs* L, const crimson_ls* ls) {
+    if (ls->log_path.empty()) return;
+    FILE* probe = std::fopen(ls->log_path.c_str(), "r");
+    const bool exists = probe != nullptr;
+    if (probe) std::fclose(probe);
+    FILE* f = std::fopen(ls->log_path.c_str(), "a");
+    if (!f) return;
+    if (!exists) {
+        int nc = 0;
+        for (const auto& fc : L->face)
+            if (fc.coupledFlag) ++nc;
+        std::fprintf(f, "%12d%12d%12d\n", L->gnNo, 1, nc);
+    }
+    const int code = (ls->RI.suc ? 100 : 0) + (ls->GM.suc ? 10 : 0) + (ls->CG.suc ? 1 : 0);
+    const double t = ls->RI.callD > 0.0 ? ls->RI.callD : 1.0;
+    std::fprintf(f, "%4.3d%3d%4d%5d%4ld%4ld%4ld%9.2E%9.2E%9.2E%4d%4d%4ld\n", code, ls->RI.itr, ls->GM.itr,
+                 ls->CG.itr, std::lround((ls->RI.callD - ls->GM.callD - ls->CG.callD) / t * 1e2),
+                 std::lround(ls->GM.callD / t * 1e2), std::lround(ls->CG.callD / t * 1e2), ls->RI.iNorm,
+                 ls->RI.iNorm != 0.0 ? ls->RI.fNorm / ls->RI.iNorm : 0.0, ls->RI.callD, ls->Resm, ls->Resc,
+                 std::lround(ls->RI.dB));
+    std::fclose(f);
+}
+
 static void copy_stats(const crimson_ls* ls, crimson_ls_stats* st) {
     if (!st) return;
     st->GM = ls->GM;
@@ -2258,6 +2288,7 @@ int memls_solve_val(crimson_lhs* L, crimson_ls* ls, double* Ri, double* Val, con
     CR_CUDA(cudaMemcpyAsync(Val, L->Val.p, sizeof(double) * 16 * (size_t)L->nnz, cudaMemcpyDeviceToHost, s));
     CR_CUDA(cudaStreamSynchronize(s));
     copy_stats(ls, st);
+    log_solve(L, ls);
     return CRIMSON_OK;
 }
 
@@ -2314,6 +2345,7 @@ int memls_solve_lhs_device(crimson_lhs* L, crimson_ls* ls, const double* d_res, 
     CR_CUDA(cudaMemcpyAsync(d_sol, L->R.p, sizeof(double) * 4 * (size_t)L->nNo, cudaMemcpyDeviceToDevice, s));
     CR_CUDA(cudaStreamSynchronize(s));
     copy_stats(ls, st);
+    log_solve(L, ls);
     return CRIMSON_OK;
 }
 

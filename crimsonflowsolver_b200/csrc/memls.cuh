@@ -1,6 +1,7 @@
 // memLS handles shared by memls.cu and capi.cu.
 #pragma once
 
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -94,5 +95,6 @@ struct crimson_ls {
     int precision = CRIMSON_FP64;  // CRIMSON_FP64, CRIMSON_MIXED or CRIMSON_MIXED_F32_TANGENT
     int max_refine = 4;            // FP64 refinement sweeps of the mixed solve
     double refine_tol = 0.0;       // target |R - A x| / |R|; <= 0: RI.relTol
+    std::string log_path;          // per-solve log (memLS_NS.log format); empty: off
 };
 

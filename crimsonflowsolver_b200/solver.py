@@ -204,6 +204,11 @@ class MemLS:
                                                ctypes.byref(st)), "crimson_solflow_device")
         return st
 
+    def set_log(self, path) -> None:
+        """Append one memLS_NS.log-format line per solve to path (None: off)."""
+        N.check(N.lib().crimson_memls_ls_set_log(self.ls, path.encode() if path else None),
+                "crimson_memls_ls_set_log")
+
     def refine_info(self):
         """(sweeps, relative FP64 defect) of the last mixed-precision solve."""
         steps = ctypes.c_int()

@@ -157,6 +157,11 @@ int crimson_memls_ls_free(crimson_ls* ls);
  * (on a small cylinder after 2 steps of 3 iterations: 1e-6 velocity, 4e-5
  * pressure relative to the FP64 tangent). */
 int crimson_memls_ls_set_precision(crimson_ls* ls, int precision, int max_refine, double refine_tol);
+/* Per-solve log in the format of memLS's memLS_NS.log (LOGFILE,
+ * flowsolver/src/memLS.f90:1720-1757), appended to path after every solve
+ * with this ls; path = "memLS_NS.log" gives the reference's file.  NULL or ""
+ * turns it off (the default). */
+int crimson_memls_ls_set_log(crimson_ls* ls, const char* path);
 /* Refinement sweeps taken by the last mixed solve on lhs and its final
  * relative FP64 defect |R - A x| / |R| (scaled system). */
 int crimson_memls_refine_info(const crimson_lhs* lhs, int* steps, double* rel);
