@@ -18,8 +18,17 @@ Multi-GPU: the path does not shard (one GPU, no domain decomposition), so
 ranks and ``value`` counts every rank's time steps (weak scaling).
 
 ``--impl reference`` times the CPU oracle (the reference algorithm restated
-in C++, all host threads) on a bounded sample of the same workload and scales
-it to one time step using the solver's per-iteration costs.
+in C++, all host threads) on the same workload: one complete time step
+(predict, 3 x [ElmGMR + SolFlow pack + full memLS NS solve + correct], RCR
+update), measured, is the value; each of the W + K timed steps is a bounded
+sample (one full-size ElmGMR + pack) so the run stays within minutes.
+
+In this arm (N = 1) the CPU oracle also runs one complete nonlinear
+iteration of the first time step on the full-size mesh (ElmGMR + pack + the
+full memLS solve): 3 x its time is ``cpu_baseline``, and the same system
+solved on the GPU gives the full-size parity figures (``full_size_parity``:
+ElmGMR res/lhsK/lhsP and the FP64 and mixed memLS solutions against the
+oracle, with the iteration counts).
 """
 from __future__ import annotations
 
@@ -40,7 +49,7 @@ sys.path.insert(0, ROOT)
 METRIC = "s/timestep @4M tets (mixed vs FP64 GPU, ≤1e-6 rel err); Melem/s assembly"
 NCROSS, NAXIAL = 80, 133
 NITR = 3
-EPSTOL_NS = 1e-5      # memLS NSSOLVER relative tolerance (epstol(8))
+EPSTOL_NS = 1e-6      # memLS NSSOLVER relative tolerance (epstol(8))
 REFINE_TOL = 0.0      # mixed precision: FP64 defect target (0: the NSSOLVER tolerance)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one persistent
 # CG iteration divided by cg_iter_bytes, from ncu captures of one launch of 50
@@ -50,11 +59,6 @@ REFINE_TOL = 0.0      # mixed precision: FP64 defect target (0: the NSSOLVER tol
 TRAFFIC_PER_ALG_F32 = 0.765
 TRAFFIC_PER_ALG_F64 = 0.850
 TRAFFIC_SOURCE = "ncu --set full, k_cg_persistent, 2.07M-tet cylinder, 50 iterations/launch, scaled by blocks"
-# Outer NS iterations and inner GMRES / CG iteration totals per memLS solve on
-# this workload, as counted by the solver on steps 2-5 (identical algorithm
-# and counts on CPU and GPU, see tests/test_gpu_parity.py).  Used only to
-# scale the CPU sample of --impl reference when it runs without a GPU.
-SOLVE_ITERS = {"ri": 5.7, "gm": 77.0, "cg": 2330.0}
 
 
 def _inflow(t: float) -> float:
@@ -136,76 +140,128 @@ def workload_name(args, m) -> str:
             "3 nonlinear iterations/step")
 
 
-def cpu_sample(m, P, nthreads: int, iters=None):
-    """Time the oracle on one bounded sample of a time step and scale to a step.
-
-    Sample: one ElmGMR (residual + tangent), the SolFlow pack, and one memLS
-    solve cut to a single NSSOLVER outer iteration, at the full workload size.
-    Per-iteration GMRES and CG costs come from the oracle's own callD timers;
-    a full step = nitr x (ElmGMR + pack + outer iterations x (per-outer
-    overhead) + GMRES its x t_gm + CG its x t_cg).
-    """
+def _oracle_first_iteration(m, P, nthreads: int):
+    """The first nonlinear iteration of time step 1 on the CPU oracle, timed:
+    predict, ElmGMR (residual + tangent), SolFlow pack, the full memLS NS
+    solve.  Returns the timings, the oracle's system and solution."""
     from oracle import pyoracle as po
 
-    iters = iters or SOLVE_ITERS
-    colm, rowp = po.genadj(m.ien, m.nshg)
-    elm = po.Elm(m, P, colm, rowp, nthreads=nthreads)
+    F = po.OracleFlow(m, P, nthreads=nthreads, inflow=_inflow)
     m.set_inflow(_inflow(P.Delt))
-    y = np.zeros((m.nshg, 4))
-    full = ((m.iBC >> 3) & 7) == 7
-    y[full, 0:3] = m.BC[full, 2:5]
-    ac = np.zeros_like(y)
-    cc = [po.rcr_coeffs(r.Rp, r.C, r.Rd, r.Pd, r.Pd, 0.0, 0.0, P.alfi * P.Delt) for r in P.rcr]
-    c1 = [c[0] for c in cc]
-    c2 = [c[1] for c in cc]
+    fct = (P.gami - 1.0) / P.gami
+    F.y = F.yold.copy()
+    F.ac = F.acold * fct
+    F._itr_bc(F.y)
+    c1, c2 = F.implicit_coeffs(0, True)
+    yA = F.y.copy()
+    acA = F.ac.copy()
+    yA[:, 0:3] = F.yold[:, 0:3] + P.alfi * (F.y[:, 0:3] - F.yold[:, 0:3])
+    acA[:, 0:3] = F.acold[:, 0:3] + P.almi * (F.ac[:, 0:3] - F.acold[:, 0:3])
+    acA[:, 3] = 0.0
     t0 = time.perf_counter()
-    out = elm(y, ac, srflist=[r.srfid for r in P.rcr], coef1=c1, coef2=c2)
+    out = F.elm(yA, acA, lhs=True, srflist=F.srflist, coef1=c1, coef2=c2)
     t_elm = time.perf_counter() - t0
     t0 = time.perf_counter()
-    Res4, Val4 = po.solflow_pack(m.nshg, colm, rowp, out["res"], out["lhsK"], out["lhsP"])
+    Res4, Val4 = po.solflow_pack(m.nshg, F.colm, F.rowp, out["res"], out["lhsK"], out["lhsP"])
     t_pack = time.perf_counter() - t0
-    from crimsonflowsolver_b200 import FlowParams
-
-    P1 = FlowParams(**{**P.__dict__, "nprjs": 1})
-    ms = po.MemLS(m.nshg, colm, rowp, 1 + len(P.rcr), P1, nthreads=nthreads)
-    nodes, sv = po.dirichlet_face(m)
-    ms.bc_create(1, nodes, 3, 0, sv)
-    for k, r in enumerate(P.rcr):
-        nn, vv = po.neumann_face(m, r.srfid)
-        ms.bc_create(2 + k, nn, 3, 1, vv)
+    faceRes = np.concatenate([[0.0], np.asarray(c1) * P.alfi * P.gami * P.Delt])
+    V = Val4.copy()
     t0 = time.perf_counter()
-    _, st = ms.solve(Res4, Val4, [0.0] + [c * P.alfi * P.gami * P.Delt for c in c1])
+    sol, st = F.memls.solve(Res4, V, faceRes)
     t_solve = time.perf_counter() - t0
-    t_gm = st.GM.callD / max(st.GM.itr, 1)
-    t_cg = st.CG.callD / max(st.CG.itr, 1)
-    t_outer = max(t_solve - st.GM.callD - st.CG.callD, 0.0)
-    t_step = P.nitr * (t_elm + t_pack + iters["ri"] * t_outer + iters["gm"] * t_gm + iters["cg"] * t_cg)
-    sample = (f"full-size ElmGMR {t_elm:.2f}s + pack {t_pack:.2f}s + 1 NSSOLVER outer iteration {t_solve:.2f}s "
-              f"(GM {st.GM.itr} its, CG {st.CG.itr} its); scaled to {P.nitr} solves x ({iters['ri']:.1f} outer, "
-              f"{iters['gm']:.0f} GMRES, {iters['cg']:.0f} CG its)")
-    return t_step, sample, t_elm + t_pack + t_solve
+    return {"t_elm": t_elm, "t_pack": t_pack, "t_solve": t_solve, "stats": st, "F": F, "inputs": (yA, acA, c1, c2),
+            "out": out, "Res4": Res4, "Val4": Val4, "faceRes": faceRes, "sol": sol}
+
+
+def full_size_parity(m, P, nthreads: int):
+    """CPU baseline and full-size parity in one pass (rank 0, N = 1).
+
+    The oracle runs the first nonlinear iteration of time step 1 on the
+    benchmark mesh; 3 x (ElmGMR + pack + solve) is the CPU s/timestep (a
+    measured sample: every nonlinear iteration repeats this work, the first
+    solve being the one from the predicted state).  The GPU then assembles the
+    same ElmGMR inputs and solves the oracle's packed system in FP64 and in
+    mixed precision through the host-pointer C ABI.
+    """
+    from crimsonflowsolver_b200 import FlowParams, solver
+
+    o = _oracle_first_iteration(m, P, nthreads)
+    st = o["stats"]
+    t_iter = o["t_elm"] + o["t_pack"] + o["t_solve"]
+    cpu = {"value": P.nitr * t_iter, "unit": "s/timestep", "cores": nthreads, "kind": "port",
+           "sample": (f"one complete nonlinear iteration of step 1 at full size, measured: ElmGMR {o['t_elm']:.2f}s + "
+                      f"pack {o['t_pack']:.2f}s + full memLS NS solve {o['t_solve']:.2f}s ({st.RI.itr} outer, "
+                      f"{st.GM.itr} GMRES, {st.CG.itr} CG its); x {P.nitr} nonlinear iterations per step")}
+    yA, acA, c1, c2 = o["inputs"]
+    par = {}
+    with solver.ElmGMR(m, P) as elm:
+        colm, rowp = elm.genadj()
+        par["pattern_bit_exact"] = bool(np.array_equal(colm, o["F"].colm) and np.array_equal(rowp, o["F"].rowp))
+        g = elm(yA, acA, c1, c2)
+        for k in ("res", "lhsK", "lhsP"):
+            par[f"elmgmr_{k}_rel_err"] = _relerr(g[k], o["out"][k])
+        del g
+        for prec in ("fp64", "mixed"):
+            Pp = FlowParams(**{**P.__dict__, "precision": prec, "max_refine": 8})
+            ms = solver.MemLS(Pp, 1 + len(P.rcr), nshg=m.nshg, colm=colm, rowp=rowp)
+            nodes, sv = solver.dirichlet_face(m)
+            ms.bc_create(1, nodes, 3, 0, sv)
+            for k, r in enumerate(P.rcr):
+                nn, vv = solver.neumann_face(m, r.srfid)
+                ms.bc_create(2 + k, nn, 3, 1, vv)
+            gsol, gst = ms.solve(o["Res4"], o["Val4"].copy(), o["faceRes"])
+            ms.close()
+            ref = o["sol"]
+            par[f"memls_{prec}"] = {
+                "velocity_rel_err": _relerr(gsol[:, 0:3], ref[:, 0:3]), "pressure_rel_err": _relerr(gsol[:, 3], ref[:, 3]),
+                "iters_gpu": [gst.RI.itr, gst.GM.itr, gst.CG.itr], "iters_oracle": [st.RI.itr, st.GM.itr, st.CG.itr]}
+    par["system"] = (f"first nonlinear iteration of step 1 ({m.nelem} tets, {m.nshg} nodes); ElmGMR on the same "
+                     "y_alpha/a_alpha/RCR coefficients; memLS on the oracle's packed Res4/Val4")
+    return cpu, par
 
 
 def run_reference(args):
+    """The reference algorithm on the CPU (the oracle on all host threads).
+
+    value: one complete time step of the workload, measured.  Each of the
+    W + K steps is a bounded sample of the same workload (one full-size
+    ElmGMR + SolFlow pack, timed), reported in ms_per_step.
+    """
+    from oracle import pyoracle as po
+
     ws, rank = _dist()
     if rank != 0:
         return
     nthreads = os.cpu_count() or 1
     m, P = make_problem(args.ncross, args.naxial, args.epstol_ns, args.workload, args.ybif_h)
-    vals = []
+    F = po.OracleFlow(m, P, nthreads=nthreads, inflow=_inflow)
+    t0 = time.perf_counter()
+    F.step()
+    t_full = time.perf_counter() - t0
+    its = [list(s[:3]) for s in F.stats]
+    y, ac = F.y.copy(), F.ac.copy()
+    cc = F.implicit_coeffs(1, True)
+    samples = []
     for i in range(args.warmup + args.steps):
-        v, sample, wall = cpu_sample(m, P, nthreads)
+        t0 = time.perf_counter()
+        out = F.elm(y, ac, lhs=True, srflist=F.srflist, coef1=cc[0], coef2=cc[1])
+        po.solflow_pack(m.nshg, F.colm, F.rowp, out["res"], out["lhsK"], out["lhsP"])
         if i >= args.warmup:
-            vals.append(v)
-    value = float(np.median(vals))
-    line = {"metric": METRIC, "value": value, "unit": "s/timestep", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+            samples.append(time.perf_counter() - t0)
+        del out
+    sample_s = float(np.median(samples))
+    sample = (f"value: one complete time step measured ({len(its)} nonlinear iterations; outer/GMRES/CG its per "
+              f"solve {its}); each timed step: one full-size ElmGMR (residual + tangent) + SolFlow pack")
+    line = {"metric": METRIC, "value": t_full, "unit": "s/timestep", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sample_s * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": workload_name(args, m) + ", FP64",
-                       "parallelism": "replicas"},
-            "cpu_baseline": {"value": value, "unit": "s/timestep", "cores": nthreads, "kind": "port",
+            "config": {"workload": workload_name(args, m) + ", FP64", "parallelism": "replicas",
+                       "epstol_ns": P.epstol_ns, "epstol_gmres_cg": [P.epstol_mom, P.epstol_cont]},
+            "full_step_measured_s": t_full, "full_step_iters_per_solve": its,
+            "sample_step_s": sample_s,
+            "cpu_baseline": {"value": t_full, "unit": "s/timestep", "cores": nthreads, "kind": "port",
                              "sample": sample},
-            "e2e": {"value": value, "unit": "s/timestep", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": t_full, "unit": "s/timestep", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -323,26 +379,30 @@ def run_ours(args):
            "after_steps": args.warmup + args.steps}
     value = replica_value(tm_ms, args.steps, ws)
     v64 = replica_value(t64_ms, args.steps, ws)
-    # ---- end to end through the host-buffer API (mixed): state in from pinned host, step, state out ----
-    y_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
-    ac_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
-    y0, a0 = FM.state()
-    y_h.copy_(torch.from_numpy(np.ascontiguousarray(y0.T)))
-    ac_h.copy_(torch.from_numpy(np.ascontiguousarray(a0.T)))
-    yp = ctypes.cast(y_h.data_ptr(), N.c_dbl_p)
-    ap = ctypes.cast(ac_h.data_ptr(), N.c_dbl_p)
-    e_steps = max(1, min(args.steps, 3))
-    torch.cuda.synchronize()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    f0.record(sm)
-    for _ in range(e_steps):
-        N.check(L.crimson_state_set(FM.elm.h, yp, ap), "crimson_state_set")
-        FM.step()
-        N.check(L.crimson_state_get(FM.elm.h, yp, ap), "crimson_state_get")
-    f1.record(sm)
-    torch.cuda.synchronize()
-    e2e = f0.elapsed_time(f1) / 1e3 / e_steps
+    # ---- end to end through the host-buffer API: state in from pinned host, step, state out ----
+    def end_to_end(FS, stream):
+        y_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
+        ac_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
+        y0, a0 = FS.state()
+        y_h.copy_(torch.from_numpy(np.ascontiguousarray(y0.T)))
+        ac_h.copy_(torch.from_numpy(np.ascontiguousarray(a0.T)))
+        yp = ctypes.cast(y_h.data_ptr(), N.c_dbl_p)
+        ap = ctypes.cast(ac_h.data_ptr(), N.c_dbl_p)
+        e_steps = max(1, min(args.steps, 3))
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(e_steps):
+            N.check(L.crimson_state_set(FS.elm.h, yp, ap), "crimson_state_set")
+            FS.step()
+            N.check(L.crimson_state_get(FS.elm.h, yp, ap), "crimson_state_get")
+        f1.record(stream)
+        torch.cuda.synchronize()
+        return f0.elapsed_time(f1) / 1e3 / e_steps
+
+    e2e = end_to_end(FM, sm)
+    e2e64 = end_to_end(F64, s64)
     # ---- assembly throughput, timed live on the library stream ----
     dres = torch.zeros((n, 4), dtype=torch.float64, device="cuda")
     nnz = FM.elm._nnz()
@@ -392,6 +452,8 @@ def run_ours(args):
                    "mixed_refine_tol": Pm.refine_tol if Pm.refine_tol > 0 else P.epstol_ns,
                    "l2": "inputs larger than L2 (sliced FP32 matrices 0.66 GB, FP64 1.33 GB per solve)"},
         "fp64": {"value": v64, "unit": "s/timestep", "ms_per_step": t64_ms / args.steps,
+                 "e2e": {"value": e2e64, "unit": "s/timestep", "h2d_bytes_per_step": 2 * 4 * n * 8,
+                         "d2h_bytes_per_step": 2 * 4 * n * 8},
                  "solver_iters_per_solve": it64, "gpu_launches": l64, "clocks": clk64},
         "mixed_speedup_vs_fp64": v64 / value,
         "mixed_rel_err_vs_fp64": acc,
@@ -414,16 +476,14 @@ def run_ours(args):
         "gpu_launches": lm,
         "clocks": clkm,
     }
+    FM.close()
+    F64.close()
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
-            cpu_v, sample, _ = cpu_sample(m, P, os.cpu_count() or 1, it64)
-            line["cpu_baseline"] = {"value": cpu_v, "unit": "s/timestep", "cores": os.cpu_count(), "kind": "port",
-                                    "sample": sample}
+            line["cpu_baseline"], line["full_size_parity"] = full_size_parity(m, P, os.cpu_count() or 1)
         except Exception as ex:  # the CPU baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "unit": "s/timestep", "cores": os.cpu_count(), "kind": "port",
                                     "sample": f"failed: {ex}"}
-    FM.close()
-    F64.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

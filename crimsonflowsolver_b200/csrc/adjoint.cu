@@ -719,22 +719,21 @@ int elmgmr_vjp(crimson_ctx* c, const double* d_y, const double* d_ac, const doub
     const int nc = c->ncoupled;
     std::vector<double> hs(2 * (size_t)std::max(nc, 1), 0.0);
     if (nc > 0) {
-        DBuf<int> doff;
-        CR_CHECK(doff.upload(c->onode_off.data(), c->onode_off.size(), s));
+        const int* doff = c->d_onode_off.p;
         DBuf<double> dc1;
         std::vector<double> h1(nc);
         for (int k = 0; k < nc; ++k) h1[k] = coef1 ? coef1[k] : 0.0;
         CR_CHECK(dc1.upload(h1.data(), nc, s));
         double* sl = c->adj_scal.p + 4;        // s_k = lambda . NABI
         double* qf = c->adj_scal.p + 4 + nc;   // Q_k = y . NABI
-        launch(k_adj_flow, nc, 256, 0, s, (const int*)c->onodes.p, (const int*)doff.p, (const double4*)c->onabi.p, l4,
+        launch(k_adj_flow, nc, 256, 0, s, (const int*)c->onodes.p, doff, (const double4*)c->onabi.p, l4,
                sl);
-        launch(k_adj_flow, nc, 256, 0, s, (const int*)c->onodes.p, (const int*)doff.p, (const double4*)c->onabi.p, y4,
+        launch(k_adj_flow, nc, 256, 0, s, (const int*)c->onodes.p, doff, (const double4*)c->onabi.p, y4,
                qf);
-        launch(k_adj_pvsq, dim3(8, nc), 256, 0, s, (const int*)c->onodes.p, (const int*)doff.p,
+        launch(k_adj_pvsq, dim3(8, nc), 256, 0, s, (const int*)c->onodes.p, doff,
                (const double4*)c->onabi.p, (const double*)sl, (const double*)dc1.p, nc, d_ybar);
         CR_CUDA(cudaMemcpyAsync(hs.data(), sl, sizeof(double) * 2 * nc, cudaMemcpyDeviceToHost, s));
-        CR_CUDA(cudaStreamSynchronize(s));  // doff, dc1 are released at scope exit
+        CR_CUDA(cudaStreamSynchronize(s));  // dc1 is released at scope exit
     }
     double hm = 0.0;
     CR_CUDA(cudaMemcpyAsync(&hm, mub, sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -6,23 +6,35 @@
 //
 // Element kernels use four lanes per linear tet.  In the quadrature phase lane
 // q evaluates quadrature point q (e3ivar/e3stab/e3Res at that point); in the
-// output phase lane a owns row a of the element: rl(a,:) and the four 3x3 +
-// 4 blocks (a, b).  Per-point quantities are exchanged through shared memory.
-// On a linear tet the metrics, gradients and div q are element constants, so
-// they are computed once per element (the reference recomputes them per
-// point with identical inputs), and the sums over quadrature points of the
-// tangent terms are formed algebraically:
-//   K_ij(a,b) = d_ij [ tsFct M_ab + tlW (rho sum_q N_a(q) uBar_q.dN_b
-//                       + 4 mu dN_a.dN_b
-//                       + sum_q (tauM_q rho (u_q.dN_a)(u_q.dN_b)
-//                                + tauBar_q (L_q.dN_a)(L_q.dN_b))) ]
-//               + tlW ( (sum_q tauC_q) dN_b,i dN_a,j + 4 mu dN_b,j dN_a,i )
+// output phase lane a owns row a of the element.  Per-point quantities are
+// exchanged through shared memory.  On a linear tet the metrics, gradients
+// and div q are element constants, so they are computed once per element
+// (the reference recomputes them per point with identical inputs), and the
+// sums over quadrature points of the tangent terms are formed algebraically:
+//   K_ij(a,b) = d_ij Kd(a,b) + tc dN_b,i dN_a,j + tm dN_b,j dN_a,i
+//   Kd(a,b)   = tsFct M_ab + tlW (rho sum_q N_a(q) uBar_q.dN_b + 4 mu dN_a.dN_b
+//                                 + sum_q (tauM_q rho (u_q.dN_a)(u_q.dN_b)
+//                                          + tauBar_q (L_q.dN_a)(L_q.dN_b)))
+//   tc = tlW sum_q tauC_q,  tm = 4 mu tlW
 //   G_i(a,b)  = tlW dN_b,i sum_q N_a(q)
 //   C(a,b)    = tlW/rho (sum_q tauM_q) dN_a.dN_b
 // which equals the reference's per-point accumulation (e3lhs.f90:171-402) in
 // exact arithmetic; the FP64 results agree to rounding (~1e-15 relative).
-// Scatter into the CSR blocks uses FP64 atomics at slots precomputed by the
-// pattern pass (no binary search per element, fillsparse.f90:29-60).
+//
+// Scatter: owner-computes, deterministic.  The element kernel writes one
+// record per element (its residual rows and the tangent's element constants
+// above: 48 doubles); it never writes a global sum.  A node pass then forms,
+// for every node, the residual row and the diagonal tangent block from the
+// records of the elements containing it, and a slot pass forms every
+// off-diagonal CSR block from the records of the elements containing that
+// edge.  Each sum runs over the pattern pass's contribution list of the slot
+// in ascending element order -- the order of the reference's serial
+// scatter (local.f90:64-75, fillsparse.f90:47-60) -- so every result is the
+// same bit for bit on every run.  Records are written once and re-read by
+// the 4 (node pass) and 12 (slot pass) owners of their element, mostly from
+// L2 on banded node numberings.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace crimson {
@@ -80,13 +92,21 @@ static ElmConst make_consts() {
     return k;
 }
 
+// __constant__ memory is per device: upload the tables once for each device
+// that runs an element kernel (the device current on the calling thread,
+// which is the device of the context's stream).  Thread-safe.
 int upload_elm_consts(cudaStream_t s) {
-    static bool done = false;
-    if (done) return CRIMSON_OK;
+    static std::mutex mu;
+    static bool done[256] = {false};
+    int dev = 0;
+    CR_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return CRIMSON_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return CRIMSON_OK;
     ElmConst k = make_consts();
     CR_CUDA(cudaMemcpyToSymbolAsync(c_el, &k, sizeof(k), 0, cudaMemcpyHostToDevice, s));
     CR_CUDA(cudaStreamSynchronize(s));
-    done = true;
+    done[dev] = true;
     return CRIMSON_OK;
 }
 
@@ -141,30 +161,27 @@ __device__ __forceinline__ void elem_metric(const double xl[4][3], double dxidx[
     }
 }
 
+__device__ __forceinline__ double sel4(const double4& v, int a) {
+    return a == 0 ? v.x : (a == 1 ? v.y : (a == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ float sel4(const float4& v, int a) {
+    return a == 0 ? v.x : (a == 1 ? v.y : (a == 2 ? v.z : v.w));
+}
+
 // ---------------------------------------------------------------------------
 // AsIq + e3q: lumped projection of the viscous flux q = mu (grad u + grad u^T)
 // (asiq.f90:52-70, e3q.f90:58-145).  On a linear tet qdi is constant, so
-// ql(a,k) = WdetJ qdi(k) sum_q N_a(q) and rmassl(a) = WdetJ sum_q N_a(q).
-// One thread per element; q node-major (9, nshg).  The lumped mass depends
-// on the geometry only and is accumulated on the first call of a context
-// (rmass != null).  The 4 x 9 contributions of the warp's 32 elements are
-// staged in shared memory and scattered with consecutive lanes on
-// consecutive components of one node (a few sectors per node instead of
-// one per lane).
+// ql(a,k) = WdetJ sum_q N_a(q) qdi(k) and rmassl(a) = WdetJ sum_q N_a(q).
+// k_asiq_rec writes one record per element: {WdetJ, q11, q12, q13, q22, q23,
+// q33, 0} (qdi is symmetric); k_q_node sums, per node, the records of the
+// elements containing it in ascending element order and applies qpbc
+// (qpbc.f90:67-71).  The lumped mass depends on the geometry only: it is
+// summed and inverted on a context's first call and kept (rmass).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_asiq(const int4* __restrict__ ien, const double4* __restrict__ x,
-                                              const double4* __restrict__ y, int nelem, ElmParams P,
-                                              double* __restrict__ qres, double* __restrict__ rmass) {
-    __shared__ double sq9[128][4][9];
-    __shared__ int snode[128][4];
-    const int lane = threadIdx.x & 31, wbase = threadIdx.x & ~31;
-    const int nstride = gridDim.x * blockDim.x;
-    for (int e0 = blockIdx.x * blockDim.x; e0 < nelem; e0 += nstride) {
-        const int e = e0 + threadIdx.x;
-        if (e >= nelem) {
-#pragma unroll
-            for (int a = 0; a < 4; ++a) snode[threadIdx.x][a] = -1;
-        } else {
+__global__ void __launch_bounds__(128) k_asiq_rec(const int4* __restrict__ ien, const double4* __restrict__ x,
+                                                  const double4* __restrict__ y, int nelem, ElmParams P,
+                                                  double* __restrict__ qrec) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
         int4 nn = ien[e];
         int nd[4] = {nn.x, nn.y, nn.z, nn.w};
         double xl[4][3], ul[4][3];
@@ -188,85 +205,74 @@ __global__ void __launch_bounds__(128) k_asiq(const int4* __restrict__ ien, cons
             for (int i = 0; i < 3; ++i)
                 g[k][i] = shg[0][k] * ul[0][i] + shg[1][k] * ul[1][i] + shg[2][k] * ul[2][i] + shg[3][k] * ul[3][i];
         const double mu = P.mu;
-        double qdi[9];
-        qdi[0] = 2.0 * mu * g[0][0];
-        qdi[3] = mu * (g[0][1] + g[1][0]);
-        qdi[6] = mu * (g[0][2] + g[2][0]);
-        qdi[1] = qdi[3];
-        qdi[4] = 2.0 * mu * g[1][1];
-        qdi[7] = mu * (g[1][2] + g[2][1]);
-        qdi[2] = qdi[6];
-        qdi[5] = qdi[7];
-        qdi[8] = 2.0 * mu * g[2][2];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const double wa = W * c_el.SN[a];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) sq9[threadIdx.x][a][k] = wa * qdi[k];
-            snode[threadIdx.x][a] = nd[a];
-            if (rmass) atomicAdd(rmass + nd[a], wa);
-        }
-        }
-        __syncwarp();
-        // 32 elements x 4 nodes x 9 components of this warp
-#pragma unroll 1
-        for (int v = lane; v < 32 * 4 * 9; v += 32) {
-            const int item = v / 9, k = v - 9 * item;
-            const int el = wbase + (item >> 2), a = item & 3;
-            const int node = snode[el][a];
-            if (node >= 0) atomicAdd(qres + 9 * (size_t)node + k, sq9[el][a][k]);
-        }
-        __syncwarp();
+        double4* r = reinterpret_cast<double4*>(qrec + 8 * (size_t)e);
+        r[0] = make_double4(W, 2.0 * mu * g[0][0], mu * (g[0][1] + g[1][0]), mu * (g[0][2] + g[2][0]));
+        r[1] = make_double4(2.0 * mu * g[1][1], mu * (g[1][2] + g[2][1]), 2.0 * mu * g[2][2], 0.0);
     }
 }
 
-// qpbc (qpbc.f90:67-71): rmass <- 1/rmass (first call of a context only),
-// q <- q * rmass
-__global__ void k_qpbc(double* __restrict__ qres, double* __restrict__ rmass, int nshg, int invert) {
+__global__ void __launch_bounds__(256) k_q_node(const int* __restrict__ diag, const int* __restrict__ soff,
+                                                const int* __restrict__ slist, const double* __restrict__ qrec,
+                                                int nshg, int first, double* __restrict__ rmass,
+                                                double* __restrict__ qres) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
-        double r = rmass[i];
-        if (invert) {
-            r = 1.0 / r;
-            rmass[i] = r;
-        }
-        double* q = qres + 9 * (size_t)i;
+        const int d = diag[i];
+        double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, m = 0.0;
+        const int p1 = soff[d + 1];
+        for (int p = soff[d]; p < p1; ++p) {
+            const int t = slist[p];
+            const int e = t >> 4, a = (t >> 2) & 3;
+            const double4* r = reinterpret_cast<const double4*>(qrec + 8 * (size_t)e);
+            const double4 A = r[0], B = r[1];
+            const double wa = A.x * c_el.SN[a];
+            // qdi(1:9) column-major 3x3, symmetric
+            const double qd[9] = {A.y, A.z, A.w, A.z, B.x, B.y, A.w, B.y, B.z};
 #pragma unroll
-        for (int k = 0; k < 9; ++k) q[k] = r * q[k];
+            for (int k = 0; k < 9; ++k) q[k] += wa * qd[k];
+            m += wa;
+        }
+        double r;
+        if (first) {
+            r = 1.0 / m;
+            rmass[i] = r;
+        } else {
+            r = rmass[i];
+        }
+        double* o = qres + 9 * (size_t)i;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) o[k] = r * q[k];
     }
 }
 
 // ---------------------------------------------------------------------------
-// AsIGMR / e3 / e3LHS / fillsparseI, four lanes per element.
+// AsIGMR / e3 / e3LHS, four lanes per element, writing element records.
+//
+// Record of element e (RS doubles at erec + RS e, every group 32-byte aligned):
+//   kLhs == 1 (FP64 tangent), RS = 48:
+//     [0:4)   tc, tm, tlW, cc = tlW/rho sum_q tauM_q
+//     [4:16)  shg transposed: shg[n][k] at 4 + 4k + n
+//     [16:32) Kd(a,b) at 16 + 4a + b
+//     [32:48) rl(a, 0:4) at 32 + 4a  (momentum 1-3, continuity)
+//   kLhs == 2 (FP32 tangent quadrature), RS = 32: rl at [0:16), then 32
+//     floats at double offset 16 with the FP32 layout of [0:32) above.
+//   kLhs == 0 (residual only), RS = 16: rl at [0:16).
 // ---------------------------------------------------------------------------
 constexpr int kQ = 28;   // doubles of per-point data exchanged in shared memory
 
-// FP32 vector reduction (sm_90+): one instruction adds four floats at a
-// 16-byte aligned address.
-__device__ __forceinline__ void red_add_v4(float* p, float a, float b, float c, float d) {
-    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
-                 : "memory");
-}
+template <int kLhs>
+struct RecLayout {
+    static constexpr int RS = kLhs == 1 ? 48 : (kLhs == 2 ? 32 : 16);
+    static constexpr int RO = kLhs == 1 ? 32 : 0;
+};
 
-// Four blocks of 128 threads per SM (128 registers, a few words spilled):
-// measured 14% faster than the unconstrained 168 registers (three blocks).
-// kLhs: 0 residual only; 1 residual + FP64 tangent (lhsK, lhsP); 2 residual
-// (FP64) + FP32 tangent records (16 floats per block: K(9), P(4), 3 zero
-// pads), whose quadrature sums are formed in FP32 and scattered with 4-wide
-// vector reductions.
+// Four blocks of 128 threads per SM (128 registers).
 template <int kLhs>
 __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien, const double4* __restrict__ x,
                                                 const double4* __restrict__ y, const double4* __restrict__ ac,
-                                                const double* __restrict__ qres, const int* __restrict__ epos,
-                                                int nelem, ElmParams P, double* __restrict__ res,
-                                                double* __restrict__ lhsK, double* __restrict__ lhsP,
-                                                float* __restrict__ lhs32) {
+                                                const double* __restrict__ qres, int nelem, ElmParams P,
+                                                double* __restrict__ erec) {
+    constexpr int RS = RecLayout<kLhs>::RS, RO = RecLayout<kLhs>::RO;
     __shared__ double sq[128][kQ];
-    // FP64 tangent staging: per warp the 32 (element, row a) blocks of one
-    // column b, so the scatter can be issued with consecutive lanes on
-    // consecutive values of the same block (3-4 sectors per block instead of
-    // one sector per lane).
-    __shared__ double stg[kLhs == 1 ? 128 : 1][13];
-    __shared__ int stg_slot[kLhs == 1 ? 128 : 1];
     const int lane4 = threadIdx.x & 3;
     const int gbase = threadIdx.x & ~3;   // first thread of this element's group
     const long long ngroups = (long long)gridDim.x * (blockDim.x >> 2);
@@ -294,6 +300,12 @@ __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien,
             yl[a][1] = yv.x;
             yl[a][2] = yv.y;
             yl[a][3] = yv.z;
+        }
+        if (!live) {
+            // a regular tet so that the dead lanes' arithmetic stays finite
+            xl[0][0] = 1.0;
+            xl[1][1] = 1.0;
+            xl[2][2] = 1.0;
         }
         double dxidx[3][3], shg[4][3], WdetJ;
         elem_metric(xl, dxidx, shg, &WdetJ);
@@ -415,17 +427,14 @@ __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien,
         __syncwarp();
         // ---- row a = lane4 ----
         const int a = lane4;
-        const double* S0 = sq[gbase];
-        const double* S1 = sq[gbase + 1];
-        const double* S2 = sq[gbase + 2];
-        const double* S3 = sq[gbase + 3];
-        const double* Sq[4] = {S0, S1, S2, S3};
+        const double* Sq[4] = {sq[gbase], sq[gbase + 1], sq[gbase + 2], sq[gbase + 3]};
         double Na[4];
 #pragma unroll
         for (int qq = 0; qq < 4; ++qq) Na[qq] = c_el.shp[qq][a];
+        double* rec = erec + (size_t)RS * (size_t)(live ? e : 0);
         if (live) {
-            // residual row a
-            double sub[3] = {0.0, 0.0, 0.0}, sG[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, sN[3] = {0, 0, 0};
+            // residual row a (e3res.f90:263-284, unpermuted: momentum 1-3, continuity)
+            double sG[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, sN[3] = {0, 0, 0};
             double div_ub = 0.0;
 #pragma unroll
             for (int qq = 0; qq < 4; ++qq) {
@@ -438,18 +447,49 @@ __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien,
                     for (int j = 0; j < 3; ++j) sG[i][j] += Sx[18 + 3 * i + j];
                 }
             }
-            (void)sub;
-            double* r = res + 4 * (size_t)nd[a];
+            double v[3];
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                double v = sN[i] + shg[a][0] * sG[i][0] + shg[a][1] * sG[i][1] + shg[a][2] * sG[i][2];
-                atomicAdd(r + i, -WdetJ * v);
-            }
-            atomicAdd(r + 3, WdetJ * div_ub);
+            for (int i = 0; i < 3; ++i) v[i] = sN[i] + shg[a][0] * sG[i][0] + shg[a][1] * sG[i][1] + shg[a][2] * sG[i][2];
+            reinterpret_cast<double4*>(rec + RO)[a] = make_double4(-WdetJ * v[0], -WdetJ * v[1], -WdetJ * v[2],
+                                                                   WdetJ * div_ub);
         }
-        if (kLhs == 2) {
-            // FP32 tangent row a: each lane scatters its blocks with 4-wide
-            // vector reductions (4 per 16-float record)
+        if (kLhs == 1 && live) {
+            const double lhsFct = P.alfi * P.gami * P.Delt;
+            const double tlW = lhsFct * WdetJ;
+            const double tsFct = P.almi * WdetJ * rho;
+            double TC = 0.0, TM = 0.0, aqa[4], bqa[4], tMq[4], tBq[4];
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) {
+                const double* Sx = Sq[qq];
+                aqa[qq] = Sx[a];
+                bqa[qq] = Sx[4 + a];
+                tMq[qq] = Sx[12];
+                tBq[qq] = Sx[13];
+                TC += Sx[14];
+                TM += Sx[12];
+            }
+            double Kd[4];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                double conv = 0.0, sym = 0.0;
+#pragma unroll
+                for (int qq = 0; qq < 4; ++qq) {
+                    const double* Sx = Sq[qq];
+                    conv += Na[qq] * Sx[8 + b];
+                    sym += tMq[qq] * rho * aqa[qq] * Sx[b] + tBq[qq] * bqa[qq] * Sx[4 + b];
+                }
+                double grad = shg[a][0] * shg[b][0] + shg[a][1] * shg[b][1] + shg[a][2] * shg[b][2];
+                Kd[b] = tsFct * c_el.M[a][b] + tlW * (rho * conv + 4.0 * mu * grad + sym);
+            }
+            double4* r4 = reinterpret_cast<double4*>(rec);
+            r4[4 + a] = make_double4(Kd[0], Kd[1], Kd[2], Kd[3]);
+            if (a < 3)
+                r4[1 + a] = make_double4(shg[0][a], shg[1][a], shg[2][a], shg[3][a]);
+            else
+                r4[0] = make_double4(tlW * TC, tlW * 4.0 * mu, tlW, tlW / rho * TM);
+        }
+        if (kLhs == 2 && live) {
+            // FP32 element quadrature of the tangent
             const float rhof = (float)rho, muf = (float)mu;
             const float lhsFct = (float)(P.alfi * P.gami * P.Delt);
             const float tlW = lhsFct * (float)WdetJ;
@@ -467,7 +507,7 @@ __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien,
                 Naf[qq] = (float)Na[qq];
             }
             float sga[3] = {(float)shg[a][0], (float)shg[a][1], (float)shg[a][2]};
-            const int* ep = epos + 16 * e + 4 * a;
+            float Kd[4];
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
                 float conv = 0.f, sym = 0.f;
@@ -477,95 +517,163 @@ __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien,
                     conv += Naf[qq] * (float)Sx[8 + b];
                     sym += tMq[qq] * rhof * aqa[qq] * (float)Sx[b] + tBq[qq] * bqa[qq] * (float)Sx[4 + b];
                 }
-                const float sgb[3] = {(float)shg[b][0], (float)shg[b][1], (float)shg[b][2]};
-                const float grad = sga[0] * sgb[0] + sga[1] * sgb[1] + sga[2] * sgb[2];
-                const float Kd = tsFct * (float)c_el.M[a][b] + tlW * (rhof * conv + 4.0f * muf * grad + sym);
-                const float tc = tlW * TC, tm = tlW * 4.0f * muf;
-                float K[9];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j)
-                        K[3 * i + j] = (i == j ? Kd : 0.f) + tc * sgb[i] * sga[j] + tm * sgb[j] * sga[i];
-                const float sn = tlW * (float)c_el.SN[a];
-                if (live) {
-                    float* rec = lhs32 + 16 * (size_t)ep[b];
-                    red_add_v4(rec + 0, K[0], K[1], K[2], K[3]);
-                    red_add_v4(rec + 4, K[4], K[5], K[6], K[7]);
-                    red_add_v4(rec + 8, K[8], sn * sgb[0], sn * sgb[1], sn * sgb[2]);
-                    atomicAdd(rec + 12, tlW / rhof * TM * grad);
-                }
+                const float grad = sga[0] * (float)shg[b][0] + sga[1] * (float)shg[b][1] + sga[2] * (float)shg[b][2];
+                Kd[b] = tsFct * (float)c_el.M[a][b] + tlW * (rhof * conv + 4.0f * muf * grad + sym);
             }
-        }
-        if (kLhs == 1) {
-            // tangent row a of this element, one column b at a time: staged,
-            // then scattered by the whole warp
-            const double lhsFct = P.alfi * P.gami * P.Delt;
-            const double tlW = lhsFct * WdetJ;
-            const double tsFct = P.almi * WdetJ * rho;
-            double TC = 0.0, TM = 0.0, aqa[4], bqa[4], tMq[4], tBq[4];
-#pragma unroll
-            for (int qq = 0; qq < 4; ++qq) {
-                const double* Sx = Sq[qq];
-                aqa[qq] = Sx[a];
-                bqa[qq] = Sx[4 + a];
-                tMq[qq] = Sx[12];
-                tBq[qq] = Sx[13];
-                TC += Sx[14];
-                TM += Sx[12];
-            }
-            const int* ep = epos + 16 * e + 4 * a;
-            const int wbase = threadIdx.x & ~31;
-            const int lane = threadIdx.x & 31;
-#pragma unroll 1
-            for (int b = 0; b < 4; ++b) {
-                double conv = 0.0, sym = 0.0;
-#pragma unroll
-                for (int qq = 0; qq < 4; ++qq) {
-                    const double* Sx = Sq[qq];
-                    conv += Na[qq] * Sx[8 + b];
-                    sym += tMq[qq] * rho * aqa[qq] * Sx[b] + tBq[qq] * bqa[qq] * Sx[4 + b];
-                }
-                double grad = shg[a][0] * shg[b][0] + shg[a][1] * shg[b][1] + shg[a][2] * shg[b][2];
-                double Kd = tsFct * c_el.M[a][b] + tlW * (rho * conv + 4.0 * mu * grad + sym);
-                const double tc = tlW * TC, tm = tlW * 4.0 * mu;
-                double* st = stg[threadIdx.x];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j)
-                        st[3 * i + j] = (i == j ? Kd : 0.0) + tc * shg[b][i] * shg[a][j] + tm * shg[b][j] * shg[a][i];
-                const double sn = tlW * c_el.SN[a];
-                st[9] = sn * shg[b][0];
-                st[10] = sn * shg[b][1];
-                st[11] = sn * shg[b][2];
-                st[12] = tlW / rho * TM * grad;
-                stg_slot[threadIdx.x] = live ? ep[b] : -1;
-                __syncwarp();
-#pragma unroll 1
-                for (int v = lane; v < 32 * 13; v += 32) {
-                    const int blk = v / 13, comp = v - 13 * blk;
-                    const int slot = stg_slot[wbase + blk];
-                    if (slot >= 0) {
-                        double* dst = comp < 9 ? lhsK + 9 * (size_t)slot + comp : lhsP + 4 * (size_t)slot + (comp - 9);
-                        atomicAdd(dst, stg[wbase + blk][comp]);
-                    }
-                }
-                __syncwarp();
-            }
+            float4* r4 = reinterpret_cast<float4*>(rec + 16);
+            r4[4 + a] = make_float4(Kd[0], Kd[1], Kd[2], Kd[3]);
+            if (a < 3)
+                r4[1 + a] = make_float4((float)shg[0][a], (float)shg[1][a], (float)shg[2][a], (float)shg[3][a]);
+            else
+                r4[0] = make_float4(tlW * TC, tlW * 4.0f * muf, tlW, tlW / rhof * TM);
         }
         __syncwarp();
     }
 }
 
 // ---------------------------------------------------------------------------
+// Owner passes: tangent block (a, b) of one element from its record,
+// exactly the expressions of the element-local tangent above.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void pair_block(const T sa[3], const T sb[3], T Kd, T tc, T tm, T sn, T cc, T o[13]) {
+    const T grad = sa[0] * sb[0] + sa[1] * sb[1] + sa[2] * sb[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) o[3 * i + j] = (i == j ? Kd : T(0)) + tc * sb[i] * sa[j] + tm * sb[j] * sa[i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) o[9 + i] = sn * sb[i];
+    o[12] = cc * grad;
+}
+
+// Contribution of element pair (a, b) to its slot, in the record's precision.
+template <int kLhs>
+__device__ __forceinline__ void record_block(const double* __restrict__ rec, int a, int b, double o[13]) {
+    if (kLhs == 1) {
+        const double4* r4 = reinterpret_cast<const double4*>(rec);
+        const double4 sc = r4[0], s0 = r4[1], s1 = r4[2], s2 = r4[3];
+        const double sa[3] = {sel4(s0, a), sel4(s1, a), sel4(s2, a)};
+        const double sb[3] = {sel4(s0, b), sel4(s1, b), sel4(s2, b)};
+        const double Kd = rec[16 + 4 * a + b];
+        pair_block<double>(sa, sb, Kd, sc.x, sc.y, sc.z * c_el.SN[a], sc.w, o);
+    } else {
+        const float* rf = reinterpret_cast<const float*>(rec + 16);
+        const float4* r4 = reinterpret_cast<const float4*>(rf);
+        const float4 sc = r4[0], s0 = r4[1], s1 = r4[2], s2 = r4[3];
+        const float sa[3] = {sel4(s0, a), sel4(s1, a), sel4(s2, a)};
+        const float sb[3] = {sel4(s0, b), sel4(s1, b), sel4(s2, b)};
+        const float Kd = rf[16 + 4 * a + b];
+        float of[13];
+        pair_block<float>(sa, sb, Kd, sc.x, sc.y, sc.z * (float)c_el.SN[a], sc.w, of);
+#pragma unroll
+        for (int k = 0; k < 13; ++k) o[k] = (double)of[k];
+    }
+}
+
+template <int kLhs>
+__device__ __forceinline__ void store_block(long long s, const double acc[13], double* __restrict__ lhsK,
+                                            double* __restrict__ lhsP, float* __restrict__ lhs32) {
+    if (kLhs == 1) {
+        double* k = lhsK + 9 * (size_t)s;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) k[c] = acc[c];
+        double* p = lhsP + 4 * (size_t)s;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) p[c] = acc[9 + c];
+    } else {
+        float4* r = reinterpret_cast<float4*>(lhs32 + 16 * (size_t)s);
+        r[0] = make_float4((float)acc[0], (float)acc[1], (float)acc[2], (float)acc[3]);
+        r[1] = make_float4((float)acc[4], (float)acc[5], (float)acc[6], (float)acc[7]);
+        r[2] = make_float4((float)acc[8], (float)acc[9], (float)acc[10], (float)acc[11]);
+        r[3] = make_float4((float)acc[12], 0.f, 0.f, 0.f);
+    }
+}
+
+// Node pass: residual row and diagonal tangent block of every node.  The
+// elements containing node i are the contributions of its diagonal slot
+// (ascending element order); then the boundary faces at i (ascending face
+// order, AsBMFG after AsIGMR as in elmgmr.f90).  One thread per node.
+template <int kLhs>
+__global__ void __launch_bounds__(256) k_node_pass(const int* __restrict__ diag, const int* __restrict__ soff,
+                                                   const int* __restrict__ slist, const double* __restrict__ erec,
+                                                   const int* __restrict__ fnoff, const int* __restrict__ flist,
+                                                   const double* __restrict__ frec, int nshg,
+                                                   double* __restrict__ res, double* __restrict__ lhsK,
+                                                   double* __restrict__ lhsP, float* __restrict__ lhs32) {
+    constexpr int RS = RecLayout<kLhs>::RS, RO = RecLayout<kLhs>::RO;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
+        const int d = diag[i];
+        double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
+        double acc[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const int p1 = soff[d + 1];
+        for (int p = soff[d]; p < p1; ++p) {
+            const int t = slist[p];
+            const int e = t >> 4, a = (t >> 2) & 3;
+            const double* rec = erec + (size_t)RS * (size_t)e;
+            const double4 rl = reinterpret_cast<const double4*>(rec + RO)[a];
+            r0 += rl.x;
+            r1 += rl.y;
+            r2 += rl.z;
+            r3 += rl.w;
+            if (kLhs) {
+                double o[13];
+                record_block<kLhs == 2 ? 2 : 1>(rec, a, a, o);
+#pragma unroll
+                for (int c = 0; c < 13; ++c) acc[c] += o[c];
+            }
+        }
+        if (fnoff) {
+            const int f1 = fnoff[i + 1];
+            for (int p = fnoff[i]; p < f1; ++p) {
+                const double4 rl = reinterpret_cast<const double4*>(frec)[flist[p]];
+                r0 += rl.x;
+                r1 += rl.y;
+                r2 += rl.z;
+                r3 += rl.w;
+            }
+        }
+        reinterpret_cast<double4*>(res)[i] = make_double4(r0, r1, r2, r3);
+        if (kLhs) store_block<kLhs == 2 ? 2 : 1>(d, acc, lhsK, lhsP, lhs32);
+    }
+}
+
+// Slot pass: every off-diagonal CSR block (i, j) from the elements that
+// contain the edge (ascending element order).  One thread per slot; the
+// diagonal slots (first contribution with a == b) belong to the node pass.
+template <int kLhs>
+__global__ void __launch_bounds__(256) k_slot_pass(const int* __restrict__ soff, const int* __restrict__ slist,
+                                                   const double* __restrict__ erec, long long nnz,
+                                                   double* __restrict__ lhsK, double* __restrict__ lhsP,
+                                                   float* __restrict__ lhs32) {
+    constexpr int RS = RecLayout<kLhs>::RS;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nnz;
+         s += (long long)gridDim.x * blockDim.x) {
+        const int p0 = soff[s], p1 = soff[s + 1];
+        const int t0 = slist[p0];
+        if (((t0 >> 2) & 3) == (t0 & 3)) continue;
+        double acc[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int p = p0; p < p1; ++p) {
+            const int t = p == p0 ? t0 : slist[p];
+            const int e = t >> 4, a = (t >> 2) & 3, b = t & 3;
+            double o[13];
+            record_block<kLhs>(erec + (size_t)RS * (size_t)e, a, b, o);
+#pragma unroll
+            for (int c = 0; c < 13; ++c) acc[c] += o[c];
+        }
+        store_block<kLhs>(s, acc, lhsK, lhsP, lhs32);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // AsBMFG / e3b / e3bvar, rigid wall, one thread per boundary face
 // (e3b.f90:112-470, e3bvar.f90:140-460).  Residual only: for rigid walls the
-// boundary tangent is zero (e3b.f90:338-343).
+// boundary tangent is zero (e3b.f90:338-343).  Writes the face's record
+// rl(n, 0:4) of its three face nodes; the node pass sums them.
 // ---------------------------------------------------------------------------
 __global__ void k_asbmfg(const int4* __restrict__ ienb, const int* __restrict__ iBCB, const double* __restrict__ BCB,
                          const double4* __restrict__ x, const double4* __restrict__ y, int nface, ElmParams P,
-                         double* __restrict__ res) {
+                         double* __restrict__ frec) {
     for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nface; f += gridDim.x * blockDim.x) {
         int4 nn = ienb[f];
         int nd[4] = {nn.x, nn.y, nn.z, nn.w};
@@ -657,19 +765,18 @@ __global__ void k_asbmfg(const int4* __restrict__ ienb, const int* __restrict__ 
 #pragma unroll
                 for (int d = 0; d < 4; ++d) rl[n][d] -= Nb[n] * rNa[d];
         }
+        double4* r4 = reinterpret_cast<double4*>(frec + 12 * (size_t)f);
 #pragma unroll
-        for (int n = 0; n < 3; ++n) {
-            double* r = res + 4 * (size_t)nd[n];
-#pragma unroll
-            for (int d = 0; d < 4; ++d) atomicAdd(r + d, rl[n][d]);
-        }
+        for (int n = 0; n < 3; ++n) r4[n] = make_double4(rl[n][0], rl[n][1], rl[n][2], rl[n][3]);
     }
 }
 
 // ---------------------------------------------------------------------------
 // ElmpvsQ, GRCR branch (elmgmr.f90:1271-1330) with GetFlowQ
 // (boundarydata.f90:1157-1196).  One block per coupled surface reduces
-// Q_k = sum NABI.u over its nodes (fixed order: deterministic).
+// Q_k = sum NABI.u over its nodes (fixed order: deterministic).  The node
+// lists of different surfaces are disjoint (built from ndsurf), so the
+// residual update touches each node once.
 // ---------------------------------------------------------------------------
 __global__ void k_flowq(const int* __restrict__ onodes, const int* __restrict__ off, const double4* __restrict__ onabi,
                         const double4* __restrict__ y, double* __restrict__ q) {
@@ -713,11 +820,6 @@ __global__ void k_bc3res(const int* __restrict__ iBC, int nshg, double* __restri
     }
 }
 
-// device-side offsets for the outlet node groups
-static int upload_offsets(crimson_ctx* c, DBuf<int>& doff) {
-    return doff.upload(c->onode_off.data(), c->onode_off.size(), c->stream);
-}
-
 int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1, const double* coef2,
                   double* d_res, double* d_lhsK, double* d_lhsP, int lhs, float* d_lhs32) {
     cudaStream_t s = c->stream;
@@ -729,50 +831,55 @@ int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const d
     if (c->p.idiff == 1) {
         CR_CHECK(c->qres.alloc((size_t)c->nshg * 9));
         CR_CHECK(c->rmass.alloc((size_t)c->nshg));
-        CR_CUDA(cudaMemsetAsync(c->qres.p, 0, sizeof(double) * 9 * (size_t)c->nshg, s));
+        CR_CHECK(c->qrec.alloc((size_t)c->nelem * 8));
         const bool first = !c->rmass_ready;
-        if (first) CR_CUDA(cudaMemsetAsync(c->rmass.p, 0, sizeof(double) * (size_t)c->nshg, s));
-        launch(k_asiq, grid_for(c->nelem, 128, 16), 128, 0, s, c->ien.p, c->x.p, y4, c->nelem, P, c->qres.p,
-               first ? c->rmass.p : (double*)nullptr);
-        launch(k_qpbc, grid_for(c->nshg, 256), 256, 0, s, c->qres.p, c->rmass.p, c->nshg, first ? 1 : 0);
+        launch(k_asiq_rec, grid_for(c->nelem, 128, 16), 128, 0, s, c->ien.p, c->x.p, y4, c->nelem, P, c->qrec.p);
+        launch(k_q_node, grid_for(c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->qrec.p, c->nshg,
+               first ? 1 : 0, c->rmass.p, c->qres.p);
         c->rmass_ready = true;
     }
-    CR_CUDA(cudaMemsetAsync(d_res, 0, sizeof(double) * 4 * (size_t)c->nshg, s));
-    if (lhs == 2) {
-        CR_CUDA(cudaMemsetAsync(d_lhs32, 0, sizeof(float) * 16 * (size_t)c->nnz, s));
-    } else if (lhs) {
-        CR_CUDA(cudaMemsetAsync(d_lhsK, 0, sizeof(double) * 9 * (size_t)c->nnz, s));
-        CR_CUDA(cudaMemsetAsync(d_lhsP, 0, sizeof(double) * 4 * (size_t)c->nnz, s));
-    }
+    // element records (sized for the FP64 tangent layout, the largest)
+    CR_CHECK(c->erec.alloc((size_t)c->nelem * 48));
     const int blk = 128;
     const int grid = grid_for((long long)c->nelem * 4, blk, 16);
     if (lhs == 2)
-        launch(k_asigmr<2>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
-               nullptr, nullptr, d_lhs32);
+        launch(k_asigmr<2>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->nelem, P, c->erec.p);
     else if (lhs)
-        launch(k_asigmr<1>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
-               d_lhsK, d_lhsP, nullptr);
+        launch(k_asigmr<1>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->nelem, P, c->erec.p);
     else
-        launch(k_asigmr<0>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->epos.p, c->nelem, P, d_res,
-               nullptr, nullptr, nullptr);
+        launch(k_asigmr<0>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->nelem, P, c->erec.p);
     CR_CUDA(cudaGetLastError());
-    if (c->nface > 0)
+    if (c->nface > 0) {
+        CR_CHECK(c->frec.alloc((size_t)c->nface * 12));
         launch(k_asbmfg, grid_for(c->nface, 128), 128, 0, s, c->ienb.p, c->iBCB.p, c->BCB.p, c->x.p, y4, c->nface, P,
-                                                        d_res);
+               c->frec.p);
+    }
+    const int* fno = c->nface > 0 ? c->fnoff.p : nullptr;
+    const int ng = grid_for(c->nshg, 256);
+    const int gs = grid_for(c->nnz, 256);
+    if (lhs == 2) {
+        launch(k_node_pass<2>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p, c->frec.p,
+               c->nshg, d_res, nullptr, nullptr, d_lhs32);
+        launch(k_slot_pass<2>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, nullptr, nullptr, d_lhs32);
+    } else if (lhs) {
+        launch(k_node_pass<1>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p, c->frec.p,
+               c->nshg, d_res, d_lhsK, d_lhsP, nullptr);
+        launch(k_slot_pass<1>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, d_lhsK, d_lhsP, nullptr);
+    } else {
+        launch(k_node_pass<0>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p, c->frec.p,
+               c->nshg, d_res, nullptr, nullptr, nullptr);
+    }
     if (c->ncoupled > 0) {
-        std::vector<double> hc(2 * (size_t)c->ncoupled);
+        double* hc = c->coef_host.data();
         for (int k = 0; k < c->ncoupled; ++k) {
             hc[k] = coef1 ? coef1[k] : 0.0;
             hc[c->ncoupled + k] = coef2 ? coef2[k] : 0.0;
         }
-        CR_CHECK(c->coefs.upload(hc.data(), hc.size(), s));
-        DBuf<int> doff;
-        CR_CHECK(upload_offsets(c, doff));
-        CR_CHECK(c->flowq.alloc((size_t)c->ncoupled));
-        launch(k_flowq, c->ncoupled, 256, 0, s, c->onodes.p, doff.p, c->onabi.p, y4, c->flowq.p);
+        CR_CUDA(cudaMemcpyAsync(c->coefs.p, hc, sizeof(double) * 2 * (size_t)c->ncoupled, cudaMemcpyHostToDevice, s));
+        launch(k_flowq, c->ncoupled, 256, 0, s, c->onodes.p, c->d_onode_off.p, c->onabi.p, y4, c->flowq.p);
         dim3 g2(8, c->ncoupled);
-        launch(k_pvsq_add, g2, 256, 0, s, c->onodes.p, doff.p, c->onabi.p, c->flowq.p, c->coefs.p, c->ncoupled, d_res);
-        CR_CUDA(cudaStreamSynchronize(s));   // doff is released at scope exit
+        launch(k_pvsq_add, g2, 256, 0, s, c->onodes.p, c->d_onode_off.p, c->onabi.p, c->flowq.p, c->coefs.p,
+               c->ncoupled, d_res);
     }
     launch(k_bc3res, grid_for(c->nshg, 256), 256, 0, s, c->iBC.p, c->nshg, d_res);
     CR_CUDA(cudaGetLastError());

@@ -300,9 +300,24 @@ int crimson_set_boundary(crimson_ctx* c, int nface, const int* ienb, const int* 
             for (int n = 0; n < 3; ++n)
                 for (int k = 0; k < 6; ++k) hbcb[18 * (size_t)f + 6 * n + k] = BCB[((size_t)k * 3 + n) * nface + f];
     }
+    // per-node lists of the faces at each face node (ascending face index):
+    // the node pass of ElmGMR sums the face residual records in this order
+    std::vector<int> fnoff((size_t)c->nshg + 1, 0), flist(3 * (size_t)nface);
+    for (int f = 0; f < nface; ++f) {
+        const int v[3] = {hb[f].x, hb[f].y, hb[f].z};
+        for (int n = 0; n < 3; ++n) fnoff[v[n] + 1] += 1;
+    }
+    for (int i = 0; i < c->nshg; ++i) fnoff[i + 1] += fnoff[i];
+    std::vector<int> fill(fnoff.begin(), fnoff.end() - 1);
+    for (int f = 0; f < nface; ++f) {
+        const int v[3] = {hb[f].x, hb[f].y, hb[f].z};
+        for (int n = 0; n < 3; ++n) flist[fill[v[n]]++] = 3 * f + n;
+    }
     CR_CHECK(c->ienb.upload(hb.data(), hb.size(), c->stream));
     CR_CHECK(c->iBCB.upload(hbits.data(), hbits.size(), c->stream));
     CR_CHECK(c->BCB.upload(hbcb.data(), hbcb.size(), c->stream));
+    CR_CHECK(c->fnoff.upload(fnoff.data(), fnoff.size(), c->stream));
+    CR_CHECK(c->flist.upload(flist.data(), flist.size(), c->stream));
     CR_CUDA(cudaStreamSynchronize(c->stream));
     return CRIMSON_OK;
 }
@@ -326,6 +341,10 @@ int crimson_set_outlets(crimson_ctx* c, int ncoupled, const int* srflist, const 
     }
     CR_CHECK(c->onodes.upload(nodes.data(), nodes.size(), c->stream));
     CR_CHECK(c->onabi.upload(nab.data(), nab.size(), c->stream));
+    CR_CHECK(c->d_onode_off.upload(c->onode_off.data(), c->onode_off.size(), c->stream));
+    CR_CHECK(c->flowq.alloc((size_t)ncoupled));
+    CR_CHECK(c->coefs.alloc(2 * (size_t)ncoupled));
+    c->coef_host.assign(2 * (size_t)ncoupled, 0.0);
     CR_CUDA(cudaStreamSynchronize(c->stream));
     c->rcr_Pn.assign(ncoupled, 0.0);
     c->rcr_Qn.assign(ncoupled, 0.0);
@@ -749,13 +768,11 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
     }
     // RCR history update at t_{n+1} (AbstractBoundaryCondition.cxx:55-91)
     if (nc > 0) {
-        DBuf<double> q;
-        CR_CHECK(q.alloc(nc));
         for (int k = 0; k < nc; ++k)
             launch(k_flowq_step, 1, 256, 0, s, c->onodes.p, c->onode_off[k], c->onode_off[k + 1], c->onabi.p,
-                                           reinterpret_cast<const double4*>(c->ycur.p), q.p + k);
+                                           reinterpret_cast<const double4*>(c->ycur.p), c->flowq.p + k);
         std::vector<double> hq(nc);
-        CR_CUDA(cudaMemcpyAsync(hq.data(), q.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaMemcpyAsync(hq.data(), c->flowq.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
         for (int k = 0; k < nc; ++k) {
             double d1, h1;

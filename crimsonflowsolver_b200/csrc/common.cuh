@@ -155,15 +155,20 @@ struct crimson_ctx {
     crimson::DBuf<int4> ienb;       // (nface) 0-based, face nodes first
     crimson::DBuf<int> iBCB;        // (nface) flag bits
     crimson::DBuf<double> BCB;      // (nface, 3, 6) as [f*18 + n*6 + c]
+    crimson::DBuf<int> fnoff;       // (nshg+1) offsets into flist per node
+    crimson::DBuf<int> flist;       // (3 nface) codes 3f + n of the faces at each node, ascending f
+    crimson::DBuf<double> frec;     // (nface, 12) face residual records: rl(n, 0:3) of face node n
 
     // coupled outlets
     int ncoupled = 0;
     std::vector<int> srflist;
     crimson::DBuf<int> onodes;      // outlet node ids grouped by surface
     std::vector<int> onode_off;     // (ncoupled+1) offsets into onodes
+    crimson::DBuf<int> d_onode_off; // device copy of onode_off
     crimson::DBuf<double4> onabi;   // NABI of those nodes
     crimson::DBuf<double> flowq;    // (ncoupled) device scratch for Q
     crimson::DBuf<double> coefs;    // (2*ncoupled) device copy of coef1, coef2
+    std::vector<double> coef_host;  // (2*ncoupled) host staging of coef1, coef2
 
     // pattern (built by crimson_genadj)
     long long nnz = 0;
@@ -171,12 +176,19 @@ struct crimson_ctx {
     crimson::DBuf<int> col;         // (nnz) 0-based
     crimson::DBuf<int> diag;        // (nshg) position of the diagonal block
     crimson::DBuf<int> trans;       // (nnz) position of the transposed block
-    crimson::DBuf<int> epos;        // (nelem*16) CSR position of element pair (a,b)
+    // Contribution lists of the owner-computes scatter: slist holds the
+    // element pairs t = 16 e + 4 a + b grouped by CSR slot, ascending t within
+    // a slot; slot s owns slist[soff[s] .. soff[s+1]).  The diagonal slot of
+    // node i lists exactly the elements containing i (b == a).
+    crimson::DBuf<int> slist;       // (nelem*16)
+    crimson::DBuf<int> soff;        // (nnz+1)
 
     // ElmGMR work space
     crimson::DBuf<double> qres;     // (nshg, 9) node-major: q[9*i + k]
     crimson::DBuf<double> rmass;    // (nshg) 1 / lumped mass (geometry only)
     bool rmass_ready = false;       // rmass holds the inverse lumped mass
+    crimson::DBuf<double> qrec;     // (nelem, 8) AsIq element records {W, q11,q12,q13,q22,q23,q33, 0}
+    crimson::DBuf<double> erec;     // (nelem, 48) element records of the residual and tangent
     crimson::DBuf<double> y4, ac4, res4;   // (4, nshg) staging for host-pointer calls
     crimson::DBuf<double> lhsK, lhsP;      // (9, nnz), (4, nnz)
     crimson::DBuf<float> lhs32;            // (16, nnz) FP32 tangent records (mixed precision)

@@ -61,9 +61,10 @@ __global__ void k_pvsq_apply_noalloc(const int* __restrict__ nodes, const double
     for (int t = a.off[k] + blockIdx.x * blockDim.x + threadIdx.x; t < a.off[k + 1]; t += gridDim.x * blockDim.x) {
         const double* nb = nabi + 3 * (size_t)t;
         double* r = res + 4 * (size_t)(nodes[t] - 1);
-        r[0] += pk * nb[0];
-        r[1] += pk * nb[1];
-        r[2] += pk * nb[2];
+        // atomic: a caller's lists may name a node under several surfaces
+        atomicAdd(r + 0, pk * nb[0]);
+        atomicAdd(r + 1, pk * nb[1]);
+        atomicAdd(r + 2, pk * nb[2]);
     }
 }
 
@@ -99,16 +100,32 @@ extern "C" int crimson_pvsq_noalloc(int nsurf, const int* surf_offsets, const in
     if (nsurf == 0) return CRIMSON_OK;
     PvsqArgs a;
     a.nsurf = nsurf;
+    if (surf_offsets[0] != 0) {
+        set_last_error("crimson_pvsq_noalloc: surf_offsets[0] must be 0");
+        return CRIMSON_ERR_ARG;
+    }
     for (int k = 0; k <= nsurf; ++k) a.off[k] = surf_offsets[k];
     for (int k = 0; k < nsurf; ++k) {
-        if (surf_offsets[k + 1] < surf_offsets[k]) return CRIMSON_ERR_ARG;
+        if (surf_offsets[k + 1] < surf_offsets[k]) {
+            set_last_error("crimson_pvsq_noalloc: surf_offsets must not decrease");
+            return CRIMSON_ERR_ARG;
+        }
         a.coef1[k] = coef1[k];
         a.coef2[k] = coef2[k];
     }
     for (int k = nsurf + 1; k <= kPvsqMaxSurf; ++k) a.off[k] = a.off[nsurf];
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (q_out) {
+        // the copy-back waits for the stream, which a capture forbids
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CR_CUDA(cudaStreamIsCapturing(s, &cs));
+        if (cs != cudaStreamCaptureStatusNone) {
+            set_last_error("crimson_pvsq_noalloc: q_out must be NULL while the stream is being captured");
+            return CRIMSON_ERR_UNSUPPORTED;
+        }
+    }
     double* q = nullptr;
     CR_CHECK(scratch_ptr(&q));
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     launch(k_flowq_noalloc, nsurf, 256, 0, s, d_nodes, d_nabi, d_y, a, q);
     launch(k_pvsq_apply_noalloc, dim3(8, nsurf), 256, 0, s, d_nodes, d_nabi, (const double*)q, a, d_res);
     CR_CUDA(cudaGetLastError());

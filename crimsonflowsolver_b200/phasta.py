@@ -30,6 +30,33 @@ from . import mesh as meshmod
 MAGIC = 362436
 
 
+_HEADER = re.compile(r"(.*?)\s*:\s*<\s*(\d+)\s*>(.*)")
+
+
+def parse_header(line: str) -> Tuple[str, int, list]:
+    """One block header ``key : < nbytes > ints`` -> (key, nbytes, ints)
+    (the grammar cvSolverIO writes and reads, solverio/src/cvSolverIO.cxx)."""
+    m = _HEADER.match(line)
+    if not m:
+        raise ValueError(f"bad header line {line!r}")
+    return m.group(1).strip(), int(m.group(2)), [int(t) for t in m.group(3).split()]
+
+
+def header_lines(path: str) -> list:
+    """The text lines of a PHASTA file (comments and block headers, no data)."""
+    b = open(path, "rb").read()
+    pos, out = 0, []
+    while pos < len(b):
+        e = b.index(b"\n", pos)
+        line = b[pos:e].decode("latin1")
+        pos = e + 1
+        out.append(line)
+        if line.startswith("#") or not line.strip():
+            continue
+        pos += parse_header(line)[1]
+    return out
+
+
 def read_blocks(path: str) -> Tuple[Dict[str, Tuple[list, bytes]], str]:
     """All blocks of a PHASTA file: key -> (header ints, raw data), and the byte order."""
     b = open(path, "rb").read()
@@ -42,10 +69,10 @@ def read_blocks(path: str) -> Tuple[Dict[str, Tuple[list, bytes]], str]:
         pos = e + 1
         if line.startswith("#") or not line.strip():
             continue
-        m = re.match(r"(.*?)\s*:\s*<\s*(\d+)\s*>(.*)", line)
-        if not m:
-            raise ValueError(f"{path}: bad header line {line!r}")
-        key, nb, ints = m.group(1).strip(), int(m.group(2)), [int(t) for t in m.group(3).split()]
+        try:
+            key, nb, ints = parse_header(line)
+        except ValueError:
+            raise ValueError(f"{path}: bad header line {line!r}") from None
         data = b[pos:pos + nb]
         if len(data) != nb:
             raise ValueError(f"{path}: block {key!r} is truncated")

@@ -28,7 +28,10 @@
  * launch on the context's CUDA stream.
  *
  * Threading: one host thread per context; calls on a context are ordered on
- * its stream.  No global mutable state.
+ * its stream.  All mutable state lives in the context and lhs handles,
+ * except two process-wide items: the element kernels' constant tables are
+ * uploaded once per device (guarded by a mutex), and crimson_pvsq_noalloc
+ * keeps its flows in one static device array per device (below).
  */
 #ifndef CRIMSON_B200_H
 #define CRIMSON_B200_H
@@ -292,9 +295,17 @@ void* crimson_ctx_stream(crimson_ctx* ctx);
  * as ElmGMR's outlet coupling does.  Device inputs: d_nodes (1-based node
  * numbers of the surfaces, grouped by surface), d_nabi (3, n) NABI of those
  * nodes, d_y (4, nshg) node-major; d_res (4, nshg) updated in place.  Host
- * inputs: surf_offsets (nsurf+1) into d_nodes, coef1/coef2 (nsurf).  q_out
- * (host, nsurf) receives the flows when not NULL (the call then waits for
- * the stream).  stream is a cudaStream_t (NULL = default stream).
+ * inputs: surf_offsets (nsurf+1) into d_nodes with surf_offsets[0] == 0 and
+ * non-decreasing entries, coef1/coef2 (nsurf).  q_out (host, nsurf) receives
+ * the flows when not NULL (the call then copies them back and waits for the
+ * stream, so q_out must be NULL while the stream is being captured: the call
+ * returns CRIMSON_ERR_UNSUPPORTED otherwise).  stream is a cudaStream_t
+ * (NULL = default stream).
+ * Preconditions the call cannot check (it is given no nshg): every node
+ * number lies in 1..nshg of d_y / d_res.  A node listed under several
+ * surfaces receives each surface's term (the update is atomic per value).
+ * Unlike crimson_elmgmr_device, this call applies no bc3Res afterwards:
+ * zero the constrained rows yourself if the coupling runs after it.
  * At most 64 surfaces: the flows live in a 512-byte static device array
  * shared by every call (overlapping calls on the GPU race on it); the first
  * call on a device looks up that array's address, so make it before any

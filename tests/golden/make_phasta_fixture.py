@@ -1,9 +1,18 @@
-"""Build tests/golden/basic_mesh.npz from the reference's own test case
-testbin/mainTests/basic (geombc.dat.1 + restart.0.1, PHASTA format), with
-the package's PHASTA reader.  Run once where a reference checkout exists:
+"""Build the PHASTA fixtures from the reference's own test case
+testbin/mainTests/basic (geombc.dat.1 + restart.0.1), with the package's
+PHASTA reader.  Run once where a reference checkout exists:
 
-    python tests/golden/make_phasta_fixture.py /path/to/reference
+    python tests/golden/make_phasta_fixture.py /path/to/reference/checkout
+
+Writes
+  basic_mesh.npz      the arrays this path reads (coordinates, connectivity,
+                      boundary codes/values, Dirichlet codes, restart state);
+  basic_headers.json  the text lines (comments and block headers, no binary
+                      data) of both files, so the reader and the writer can
+                      be checked against the reference's header grammar and
+                      block sizes without the reference checkout.
 """
+import json
 import os
 import sys
 
@@ -17,13 +26,19 @@ from crimsonflowsolver_b200 import phasta  # noqa: E402
 
 def main(ref):
     base = os.path.join(ref, "testbin", "mainTests", "basic")
-    m = phasta.read_geombc(os.path.join(base, "geombc.dat.1"))
-    y, ac, _ = phasta.read_restart(os.path.join(base, "restart.0.1"))
+    geo, rst = os.path.join(base, "geombc.dat.1"), os.path.join(base, "restart.0.1")
+    m = phasta.read_geombc(geo)
+    y, ac, _ = phasta.read_restart(rst)
     out = os.path.join(HERE, "basic_mesh.npz")
     np.savez_compressed(out, x=m.x, ien=m.ien, ienb=m.ienb, iBCB=m.iBCB, BCB=m.BCB[:, 0, :], iBC=m.iBC,
                         dirichlet_nodes=m.dirichlet_nodes, dirichlet_values=m.dirichlet_values, y=y, ac=ac)
+    heads = {"geombc.dat.1": phasta.header_lines(geo), "restart.0.1": phasta.header_lines(rst)}
+    with open(os.path.join(HERE, "basic_headers.json"), "w") as f:
+        json.dump(heads, f, indent=1)
     print(out, "nodes", m.nshg, "tets", m.nelem, "boundary", len(m.ienb), "dirichlet", len(m.dirichlet_nodes))
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_phasta_fixture.py /path/to/reference/checkout")
+    main(sys.argv[1])
