@@ -59,6 +59,10 @@ REFINE_TOL = 0.0      # mixed precision: FP64 defect target (0: the NSSOLVER tol
 TRAFFIC_PER_ALG_F32 = 0.765
 TRAFFIC_PER_ALG_F64 = 0.850
 TRAFFIC_SOURCE = "ncu --set full, k_cg_persistent, 2.07M-tet cylinder, 50 iterations/launch, scaled by blocks"
+# The same ratio for the CG on the explicit FP32 Schur operator (k_cg_schur);
+# 1.0 until an ncu capture of that kernel replaces it.
+TRAFFIC_PER_ALG_S2 = 1.0
+TRAFFIC_SOURCE_S2 = "not yet captured: algorithmic bytes"
 
 
 def _inflow(t: float) -> float:
@@ -340,6 +344,16 @@ def cg_iter_bytes(nnz: int, n: int, mbytes: int, nface: int, resident: bool = Fa
     return nnz * ((0 if resident else 8) + 7 * mbytes) + n * (16 + 8 * mbytes + 24 + 16 + 16 + 16 + 16 * nface)
 
 
+def cg_schur_iter_bytes(nnz2: int, n: int, nface: int) -> int:
+    """Algorithmic HBM bytes of one iteration of the CG on the explicit FP32
+    Schur operator: per 2-ring entry the FP32 value and its int16 column
+    offset (6); per row, once: {R, P_prev} FP64 read in both phases and
+    written (3 x 16), its FP32 copy written and gathered (2 x 8), S P written
+    and read (2 x 8), X read and written (16), and w_f, z_f (phase 1) and z_f
+    (phase 2) per coupled face (3 x 8)."""
+    return nnz2 * 6 + n * (48 + 16 + 16 + 16 + 24 * nface)
+
+
 def run_ours(args):
     import ctypes
 
@@ -435,9 +449,16 @@ def run_ours(args):
     nface = len(P.rcr)
     res64, res32, rbytes = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
     N.check(L.crimson_memls_cg_layout(F64.memls.lhs, ctypes.byref(res64), None, None), "crimson_memls_cg_layout")
-    N.check(L.crimson_memls_cg_layout(FM.memls.lhs, None, ctypes.byref(res32), ctypes.byref(rbytes)),
-            "crimson_memls_cg_layout")
-    cg_bytes = cg_iter_bytes(nnz, n, 4, nface, bool(res32.value))
+    if L.crimson_memls_cg_layout(FM.memls.lhs, None, ctypes.byref(res32), ctypes.byref(rbytes)) != 0:
+        res32.value = 0   # the mixed solve ran only the explicit-Schur CG
+    s2_state, s2_nnz, s2_npad, s2_form_ms = FM.memls.schur_info()
+    if s2_state == 1:
+        cg_bytes = cg_schur_iter_bytes(s2_nnz, n, nface)
+        cg_kernel = ("k_cg_schur<1> (one CGRAD iteration on the explicit FP32 Schur operator: S P, "
+                     "coupled-face term, updates)")
+    else:
+        cg_bytes = cg_iter_bytes(nnz, n, 4, nface, bool(res32.value))
+        cg_kernel = "k_cg_persistent<float> (one CGRAD iteration: G P, L P - Gt G P, updates)"
     achieved = cg_bytes / (kt["cg_iter_f32"] / 1e3) / 1e9 if kt["cg_iter_f32"] else None
     cg_bytes64 = cg_iter_bytes(nnz, n, 8, nface, bool(res64.value))
     achieved64 = cg_bytes64 / (kt["cg_iter_f64"] / 1e3) / 1e9 if kt["cg_iter_f64"] else None
@@ -461,13 +482,16 @@ def run_ours(args):
         "assembly_melem_s": m.nelem / t_asm / 1e6,
         "assembly_ms": t_asm * 1e3,
         "kernel_ms": kt,
-        "roofline": {"kernel": "k_cg_persistent<float> (one CGRAD iteration: G P, L P - Gt G P, updates)",
+        "roofline": {"kernel": cg_kernel,
                      "bound": "hbm", "achieved": achieved, "peak": peaks[0], "unit": "GB/s",
                      "frac": achieved / peaks[0] if achieved else None,
-                     "traffic": TRAFFIC_PER_ALG_F32 * cg_bytes if TRAFFIC_PER_ALG_F32 else None,
-                     "traffic_source": TRAFFIC_SOURCE,
+                     "traffic": (TRAFFIC_PER_ALG_S2 if s2_state == 1 else TRAFFIC_PER_ALG_F32) * cg_bytes,
+                     "traffic_source": TRAFFIC_SOURCE_S2 if s2_state == 1 else TRAFFIC_SOURCE,
                      "algorithmic_bytes_per_iter": cg_bytes, "peak_source": peaks[1],
-                     "columns": "block-resident in shared memory" if res32.value else "read per phase",
+                     "schur_operator": {"state": s2_state, "nnz": s2_nnz, "sliced_positions": s2_npad,
+                                        "formation_ms": s2_form_ms},
+                     "columns": ("int16 offsets streamed with the FP32 values" if s2_state == 1 else
+                                 ("block-resident in shared memory" if res32.value else "read per phase")),
                      "fp64_kernel": {"achieved": achieved64, "frac": achieved64 / peaks[0] if achieved64 else None,
                                      "algorithmic_bytes_per_iter": cg_bytes64,
                                      "traffic": TRAFFIC_PER_ALG_F64 * cg_bytes64 if TRAFFIC_PER_ALG_F64 else None}},

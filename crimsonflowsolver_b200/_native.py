@@ -74,6 +74,10 @@ SIGNATURES = {
     "crimson_memls_ls_free": (ctypes.c_int, [c_void_p]),
     "crimson_memls_ls_set_precision": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
     "crimson_memls_refine_info": (ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_int), c_dbl_p]),
+    "crimson_memls_ls_set_schur": (ctypes.c_int, [c_void_p, ctypes.c_int]),
+    "crimson_memls_schur_info": (ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                                                c_dbl_p]),
     "crimson_memls_ls_set_log": (ctypes.c_int, [c_void_p, ctypes.c_char_p]),
     "crimson_memls_lhs_create": (ctypes.c_int, [ctypes.POINTER(c_void_p), ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_longlong, c_int_p, c_int_p, c_int_p, ctypes.c_int]),

@@ -456,6 +456,21 @@ int crimson_memls_ls_set_precision(crimson_ls* ls, int precision, int max_refine
     return CRIMSON_OK;
 }
 
+int crimson_memls_ls_set_schur(crimson_ls* ls, int explicit_schur) {
+    if (!ls || explicit_schur < 0 || explicit_schur > 1) return CRIMSON_ERR_ARG;
+    ls->schur = explicit_schur;
+    return CRIMSON_OK;
+}
+
+int crimson_memls_schur_info(const crimson_lhs* L, int* state, long long* nnz, long long* npad, double* form_ms) {
+    if (!L) return CRIMSON_ERR_ARG;
+    if (state) *state = L->s2_state;
+    if (nnz) *nnz = L->s2_nnz;
+    if (npad) *npad = L->s2_npad;
+    if (form_ms) *form_ms = L->s2_forms > 0 ? L->s2_form_ms / L->s2_forms : 0.0;
+    return CRIMSON_OK;
+}
+
 int crimson_memls_ls_set_log(crimson_ls* ls, const char* path) {
     if (!ls) return CRIMSON_ERR_ARG;
     ls->log_path = path ? std::string(path) : std::string();
@@ -538,6 +553,8 @@ int crimson_memls_lhs_free(crimson_lhs* L) {
     if (L->hscal) cudaFreeHost(L->hscal);
     if (L->ev0) cudaEventDestroy(L->ev0);
     if (L->ev1) cudaEventDestroy(L->ev1);
+    if (L->s2_ev0) cudaEventDestroy(L->s2_ev0);
+    if (L->s2_ev1) cudaEventDestroy(L->s2_ev1);
     cudaStream_t s = L->own_stream ? L->stream : nullptr;
     delete L;
     if (s) cudaStreamDestroy(s);

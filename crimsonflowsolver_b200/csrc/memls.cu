@@ -1673,7 +1673,7 @@ static int cg_resident_bytes(crimson_lhs* L, size_t* bytes) {
 template <typename M>
 static int cgrad(Ctx& C, crimson_subls& ls, const M* Gs, const typename V4<M>::type* GLs,
                  double* R, int nface,
-                 const double* coef) {
+                 const double* coef, bool use_s2 = false) {
     crimson_lhs* L = C.L;
     cudaStream_t s = C.s;
     const int n = L->nNo;
@@ -1687,6 +1687,36 @@ static int cgrad(Ctx& C, crimson_subls& ls, const M* Gs, const typename V4<M>::t
     eps = eps * eps;
     double err = errO;
     err = err * err;
+    if (use_s2) {
+        // the same CGRAD on the explicit FP32 Schur operator (schur.cu)
+        CR_CUDA(cudaEventRecord(L->ev0, s));
+        CR_CHECK(cg_schur_launch(L, R, nface, coef, L->cgW.p, L->cgZ.p, eps, err, ls.mItr, C.sc(kSlotCg)));
+        CR_CUDA(cudaEventRecord(L->ev1, s));
+        CR_CHECK(C.sync_scal(kSlotCg, 4));
+        err = L->hscal[kSlotCg + 0];
+        errO = L->hscal[kSlotCg + 1];
+        const int i = (int)L->hscal[kSlotCg + 2];
+        ls.suc = (int)L->hscal[kSlotCg + 3];
+        float ms = 0.f;
+        CR_CUDA(cudaEventElapsedTime(&ms, L->ev0, L->ev1));
+        L->cg_acc32.ms += ms;
+        L->cg_acc32.iters += i - 1;
+        L->cg_acc32.launches += 1;
+        if (L->s2_form_pending) {
+            float fm = 0.f;
+            CR_CUDA(cudaEventElapsedTime(&fm, L->s2_ev0, L->s2_ev1));
+            L->s2_form_ms += fm;
+            L->s2_forms += 1;
+            L->s2_form_pending = false;
+        }
+        CR_CUDA(cudaMemcpyAsync(R, L->cgX.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+        ls.fNorm = std::sqrt(err);
+        ls.callD = now_s() - time + ls.callD;
+        ls.dB = 5.0 * std::log(err / errO);
+        ls.itr = ls.itr + i - 1;
+        return CRIMSON_OK;
+    }
     const void* kres[3] = {(const void*)k_cg_persistent<0, M, true>, (const void*)k_cg_persistent<1, M, true>,
                            (const void*)k_cg_persistent<kMaxCoupled, M, true>};
     const void* kglb[3] = {(const void*)k_cg_persistent<0, M, false>, (const void*)k_cg_persistent<1, M, false>,
@@ -1948,6 +1978,15 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
     CR_CHECK(sell_mats(L, &Ks, &Gs, &GLs));
     launch(k_to_sell<M>, grid_for(nNo, 256), 256, 0, s, L->rowptr, (const int*)L->sell_ptr.p, nNo, mK, mG, Gt, mL,
            L->npad, Ks, Gs, GLs);
+    // mixed precision: the CG runs on the explicit FP32 Schur operator
+    bool use_s2 = false;
+    if (std::is_same<M, float>::value && ls->schur && cg_nface <= kMaxCoupled) {
+        CR_CHECK(schur_pattern(L));
+        if (L->s2_state == 1) {
+            CR_CHECK(schur_form(L, mG, Gt, mL));
+            use_s2 = true;
+        }
+    }
     int i, iBB = 0;
     for (i = 1; i <= ls->RI.mItr; ++i) {
         iB = 2 * i - 1;
@@ -1959,7 +1998,7 @@ static int nssolver(crimson_lhs* L, crimson_ls* ls, const double* mK, const doub
                (const double*)Pcol(i - 1), Pcol(i - 1), (long long)nNo);
         CR_CHECK(cgrad<M>(C, ls->CG, (const M*)Gs, (const typename V4<M>::type*)GLs, Pcol(i - 1),
                           cg_nface,
-                          cg_coef));
+                          cg_coef, use_s2));
         C.sv3(mG, (const double*)Pcol(i - 1), MUc(iB - 1));
         launch(k_sub<double, double, double>, grid_for(nv, 256), 256, 0, s, (const double*)L->Rm.p,
                (const double*)MUc(iB - 1), MUc(iBB - 1), nv);
@@ -2087,6 +2126,8 @@ static int lhs_work_alloc(crimson_lhs* L, const crimson_ls* ls) {
         CR_CUDA(cudaMallocHost(&L->hscal, sizeof(double) * kScalTotal));
         CR_CUDA(cudaEventCreate(&L->ev0));
         CR_CUDA(cudaEventCreate(&L->ev1));
+        CR_CUDA(cudaEventCreate(&L->s2_ev0));
+        CR_CUDA(cudaEventCreate(&L->s2_ev1));
     }
     return CRIMSON_OK;
 }

@@ -6,6 +6,8 @@
 
 #include "common.cuh"
 
+struct crimson_lhs;
+
 namespace crimson {
 
 struct RedScratch {
@@ -20,6 +22,11 @@ struct RedScratch {
         return CRIMSON_OK;
     }
 };
+
+int schur_pattern(crimson_lhs* L);
+int schur_form(crimson_lhs* L, const double* mG, const double* Gt, const double* mL);
+int cg_schur_launch(crimson_lhs* L, const double* R, int nface, const double* coef, const double* w, const double* z,
+                    double eps, double err0, int mItr, double* out);
 
 }  // namespace crimson
 
@@ -83,6 +90,20 @@ struct crimson_lhs {
         long long iters = 0, launches = 0;
     } cg_acc64, cg_acc32;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // explicit FP32 Schur operator S = L - Gt G of the mixed-precision CG
+    // (schur.cu): 2-ring pattern (CSR and sliced int16 offsets), FP32 values
+    int s2_state = 0;       // 0: pattern not built, 1: usable, -1: not usable on this pattern
+    DBuf<int> s2_rowptr, s2_col, s2_sp;
+    DBuf<short> s2_off;
+    DBuf<float> s2_val;
+    DBuf<float2> s2_recF;
+    DBuf<double> s2_part;
+    long long s2_nnz = 0, s2_npad = 0;
+    int s2_nslice = 0, s2_grid = 0;
+    cudaEvent_t s2_ev0 = nullptr, s2_ev1 = nullptr;
+    bool s2_form_pending = false;   // a formation was recorded between s2_ev0 and s2_ev1
+    double s2_form_ms = 0.0;
+    int s2_forms = 0;
     DBuf<double> scal;      // device scalars
     RedScratch red;
     double* hscal = nullptr;   // pinned host mirror of scal
@@ -95,6 +116,7 @@ struct crimson_ls {
     int precision = CRIMSON_FP64;  // CRIMSON_FP64, CRIMSON_MIXED or CRIMSON_MIXED_F32_TANGENT
     int max_refine = 4;            // FP64 refinement sweeps of the mixed solve
     double refine_tol = 0.0;       // target |R - A x| / |R|; <= 0: RI.relTol
+    int schur = 0;                 // mixed precision: 1 = CG on the explicit FP32 Schur operator when the pattern allows
     std::string log_path;          // per-solve log (memLS_NS.log format); empty: off
 };
 

@@ -162,6 +162,7 @@ class MemLS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, got {P.precision!r}")
         N.check(L.crimson_memls_ls_set_precision(ls, PRECISIONS[P.precision], P.max_refine, P.refine_tol),
                 "crimson_memls_ls_set_precision")
+        N.check(L.crimson_memls_ls_set_schur(ls, int(P.explicit_schur)), "crimson_memls_ls_set_schur")
         lhs = ctypes.c_void_p()
         self._ctx = ctx   # an lhs made from a context must be freed before it
         if ctx is not None:
@@ -208,6 +209,15 @@ class MemLS:
         """Append one memLS_NS.log-format line per solve to path (None: off)."""
         N.check(N.lib().crimson_memls_ls_set_log(self.ls, path.encode() if path else None),
                 "crimson_memls_ls_set_log")
+
+    def schur_info(self):
+        """(state, nnz, sliced positions, average formation ms) of the explicit
+        FP32 Schur operator on this lhs (state 1: in use, 0: not built, -1:
+        the pattern does not allow it)."""
+        st, nnz, npad, fm = ctypes.c_int(), ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_double()
+        N.check(N.lib().crimson_memls_schur_info(self.lhs, ctypes.byref(st), ctypes.byref(nnz), ctypes.byref(npad),
+                                                 ctypes.byref(fm)), "crimson_memls_schur_info")
+        return st.value, nnz.value, npad.value, fm.value
 
     def refine_info(self):
         """(sweeps, relative FP64 defect) of the last mixed-precision solve."""

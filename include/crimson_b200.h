@@ -160,6 +160,19 @@ int crimson_memls_ls_free(crimson_ls* ls);
  * (on a small cylinder after 2 steps of 3 iterations: 1e-6 velocity, 4e-5
  * pressure relative to the FP64 tangent). */
 int crimson_memls_ls_set_precision(crimson_ls* ls, int precision, int max_refine, double refine_tol);
+/* Inner CG form of the mixed-precision solve (no counterpart in the
+ * reference, which has only FP64).  explicit_schur = 1: each
+ * NSSOLVER call forms the continuity Schur operator S = L - Gt G in FP64 on
+ * the 2-ring pattern, rounds it to FP32, and CGRAD multiplies by S (one
+ * sparse product and two grid barriers per iteration); the pattern is built
+ * on the first mixed solve of an lhs and is used when every |col - row| of
+ * the 2-ring fits 16 bits and no row has more than 256 entries.
+ * explicit_schur = 0 (the default): CGRAD multiplies by L and Gt G as two
+ * FP32 products, as memLS does in FP64.  On the 4M-tet cylinder one CG
+ * iteration takes 0.0765 ms with the explicit operator and 0.0739 ms with the
+ * two products: S has about 4 times the entries of the block pattern, which
+ * cancels its single product per iteration.  FP64 solves are unaffected. */
+int crimson_memls_ls_set_schur(crimson_ls* ls, int explicit_schur);
 /* Per-solve log in the format of memLS's memLS_NS.log (LOGFILE,
  * flowsolver/src/memLS.f90:1720-1757), appended to path after every solve
  * with this ls; path = "memLS_NS.log" gives the reference's file.  NULL or ""
@@ -334,6 +347,13 @@ int crimson_memls_kernel_time(crimson_lhs* lhs, int which, int reps, double* ms)
  * smem_bytes = shared memory per block of the resident layout (0: offsets
  * exceed 16 bits).  Valid after a solve on the lhs. */
 int crimson_memls_cg_layout(const crimson_lhs* lhs, int* resident64, int* resident32, long long* smem_bytes);
+
+/* Diagnostics of the explicit FP32 Schur operator (crimson_memls_ls_set_schur)
+ * on this lhs: state 1 = built and used by mixed solves, 0 = not built yet,
+ * -1 = the pattern does not allow it; nnz / npad = its entries and sliced
+ * positions (padding included); form_ms = average time of one formation
+ * (CUDA events).  Valid after a mixed solve on the lhs. */
+int crimson_memls_schur_info(const crimson_lhs* lhs, int* state, long long* nnz, long long* npad, double* form_ms);
 
 /* Number of CUDA kernels this library has launched since it was loaded. */
 unsigned long long crimson_launch_count(void);

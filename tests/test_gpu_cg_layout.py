@@ -5,8 +5,11 @@ offsets col - row when every offset fits (meshes numbered with locality, as
 generated); otherwise it reads them from the sliced pattern in each phase.
 A randomly renumbered copy of a 41k-node cylinder has offsets up to the node
 count and takes the second layout.  One time step on both numberings, FP64
-and mixed: the same iteration counts and states equal to rounding (the CSR
-rows sum their entries in a different order after renumbering).
+and mixed (the two-product CG, explicit_schur=0): the same iteration counts
+and states equal to rounding (the CSR rows sum their entries in a different
+order after renumbering).  The mixed solve's explicit FP32 Schur operator
+needs 16-bit 2-ring offsets too: on the renumbered mesh it is not built and
+the solve falls back to the two-product CG, bit for bit.
 """
 import ctypes
 
@@ -38,12 +41,14 @@ def _renumber(m, seed=11):
                      outlets=list(m.outlets)), perm
 
 
-def _run(m, precision):
-    P = FlowParams(rcr=[RCR(srfid=3)], precision=precision, max_refine=8)
+def _run(m, precision, explicit_schur=0):
+    P = FlowParams(rcr=[RCR(srfid=3)], precision=precision, max_refine=8, explicit_schur=explicit_schur)
     F = solver.FlowSolver(m, P, inflow=lambda t: 10.0)
     try:
         st = F.step()
         y, _ = F.state()
+        if explicit_schur:
+            return y, st, F.memls.schur_info()[0], None
         r64, r32, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
         N.check(N.lib().crimson_memls_cg_layout(F.memls.lhs, ctypes.byref(r64), ctypes.byref(r32), ctypes.byref(nb)),
                 "crimson_memls_cg_layout")
@@ -68,3 +73,11 @@ def test_resident_and_streamed_columns_agree(precision):
         assert abs(s0.cg_itr[i] - s1.cg_itr[i]) <= 1 + 0.01 * s0.cg_itr[i]
     e = relerr(y1[perm], y0)
     assert e < 1e-8, e
+
+
+def test_explicit_schur_falls_back_on_wide_offsets():
+    mr, _ = _renumber(mesh.cylinder(ncross=32, naxial=48))
+    y0, s0, _, _ = _run(mr, "mixed", explicit_schur=0)
+    y1, s1, state, _ = _run(mr, "mixed", explicit_schur=1)
+    assert state == -1
+    assert np.array_equal(y0, y1)

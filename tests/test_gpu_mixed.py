@@ -215,3 +215,37 @@ def test_mixed_first_sweep_meets_tolerance():
     ep = relerr(ym[:, 3], y64[:, 3])
     print(f"mixed vs FP64 library after 3 steps: vel {ev:.3e} p {ep:.3e}")
     assert ev < 1e-7 and ep < 1e-7, (ev, ep)
+
+
+def test_explicit_schur_cg(system):
+    """The mixed solve's inner CG on the explicit FP32 Schur operator
+    S = L - Gt G (2-ring pattern) against the two-product FP32 CG: both meet
+    the refinement tolerance and the direct solve's bound, the operator has
+    the node graph's 2-ring as its pattern, and two solves give the same bits."""
+    import scipy.sparse as sp
+
+    m, P, elm, colm, rowp, Res4, Val4, faceRes, state, xd, A, f = system
+    sols = {}
+    for schur in (1, 0):
+        Pm = FlowParams(rcr=P.rcr, precision="mixed", max_refine=8, refine_tol=1e-10, explicit_schur=schur)
+        ms = _host_memls(m, Pm, colm, rowp)
+        try:
+            sol, st = ms.solve(Res4, Val4.copy(), faceRes)
+            steps, rel = ms.refine_info()
+            info = ms.schur_info()
+            if schur:
+                sol2, _ = ms.solve(Res4, Val4.copy(), faceRes)
+                assert np.array_equal(sol, sol2)
+        finally:
+            ms.close()
+        assert rel <= 1e-10 and st.RI.suc == 1, (schur, steps, rel)
+        assert relerr(sol, xd) < 1e-7, (schur, relerr(sol, xd))
+        sols[schur] = sol
+        if schur:
+            n = m.nshg
+            r = np.repeat(np.arange(n), np.diff(colm))
+            G1 = sp.csr_matrix((np.ones(len(rowp)), (r, rowp - 1)), shape=(n, n))
+            assert info[0] == 1 and info[1] == (G1 @ G1).nnz, info
+        else:
+            assert info[0] == 0, info
+    assert relerr(sols[1], sols[0]) < 1e-7
