@@ -21,14 +21,18 @@
 // which equals the reference's per-point accumulation (e3lhs.f90:171-402) in
 // exact arithmetic; the FP64 results agree to rounding (~1e-15 relative).
 //
-// Scatter: owner-computes, deterministic.  Lane a of an element writes the
-// row record of (element, a) -- its residual row a and what the tangent
-// blocks (a, b) need -- at a node-sorted position (pattern pass); it never
-// writes a global sum.  A row pass then forms, for every node, the residual
-// row and every CSR block of its row from its contiguous records, in
-// ascending element order -- the order of the reference's serial scatter
-// (local.f90:64-75, fillsparse.f90:47-60) -- so every result is the same bit
-// for bit on every run.  Records are written once and streamed once.
+// Scatter: owner-computes, deterministic.  The element kernel writes one
+// record per element (its residual rows and the tangent's element constants
+// above: 48 doubles); it never writes a global sum.  A node pass then forms,
+// for every node, the residual row and the diagonal tangent block from the
+// records of the elements containing it, and a slot pass forms every
+// off-diagonal CSR block from the records of the elements containing that
+// edge.  Each sum runs over the pattern pass's contribution list of the slot
+// in ascending element order -- the order of the reference's serial
+// scatter (local.f90:64-75, fillsparse.f90:47-60) -- so every result is the
+// same bit for bit on every run.  Records are written once and re-read by
+// the 4 (node pass) and 12 (slot pass) owners of their element, mostly from
+// L2 on banded node numberings.
 #include <mutex>
 
 #include "common.cuh"
@@ -170,16 +174,15 @@ __device__ __forceinline__ float sel4(const float4& v, int a) {
 // AsIq + e3q: lumped projection of the viscous flux q = mu (grad u + grad u^T)
 // (asiq.f90:52-70, e3q.f90:58-145).  On a linear tet qdi is constant, so
 // ql(a,k) = WdetJ sum_q N_a(q) qdi(k) and rmassl(a) = WdetJ sum_q N_a(q).
-// k_asiq_rec writes one row record per (element, local node a) at the
-// node-sorted position npos[4 e + a]: {WdetJ sum_q N_a(q), q11, q12, q13,
-// q22, q23, q33, 0} (qdi is symmetric); k_q_rows sums, per node, its
-// contiguous records (ascending element order) and applies qpbc
+// k_asiq_rec writes one record per element: {WdetJ, q11, q12, q13, q22, q23,
+// q33, 0} (qdi is symmetric); k_q_node sums, per node, the records of the
+// elements containing it in ascending element order and applies qpbc
 // (qpbc.f90:67-71).  The lumped mass depends on the geometry only: it is
 // summed and inverted on a context's first call and kept (rmass).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_asiq_rec(const int4* __restrict__ ien, const double4* __restrict__ x,
-                                                  const double4* __restrict__ y, const int* __restrict__ npos,
-                                                  int nelem, ElmParams P, double* __restrict__ qrow) {
+                                                  const double4* __restrict__ y, int nelem, ElmParams P,
+                                                  double* __restrict__ qrec) {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
         int4 nn = ien[e];
         int nd[4] = {nn.x, nn.y, nn.z, nn.w};
@@ -204,29 +207,26 @@ __global__ void __launch_bounds__(128) k_asiq_rec(const int4* __restrict__ ien, 
             for (int i = 0; i < 3; ++i)
                 g[k][i] = shg[0][k] * ul[0][i] + shg[1][k] * ul[1][i] + shg[2][k] * ul[2][i] + shg[3][k] * ul[3][i];
         const double mu = P.mu;
-        const double q11 = 2.0 * mu * g[0][0], q12 = mu * (g[0][1] + g[1][0]), q13 = mu * (g[0][2] + g[2][0]);
-        const double q22 = 2.0 * mu * g[1][1], q23 = mu * (g[1][2] + g[2][1]), q33 = 2.0 * mu * g[2][2];
-        const int4 pp = reinterpret_cast<const int4*>(npos)[e];
-        const int pos[4] = {pp.x, pp.y, pp.z, pp.w};
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            double4* r = reinterpret_cast<double4*>(qrow + 8 * (size_t)pos[a]);
-            r[0] = make_double4(W * c_el.SN[a], q11, q12, q13);
-            r[1] = make_double4(q22, q23, q33, 0.0);
-        }
+        double4* r = reinterpret_cast<double4*>(qrec + 8 * (size_t)e);
+        r[0] = make_double4(W, 2.0 * mu * g[0][0], mu * (g[0][1] + g[1][0]), mu * (g[0][2] + g[2][0]));
+        r[1] = make_double4(2.0 * mu * g[1][1], mu * (g[1][2] + g[2][1]), 2.0 * mu * g[2][2], 0.0);
     }
 }
 
-__global__ void __launch_bounds__(256) k_q_rows(const int* __restrict__ noff, const double* __restrict__ qrow,
+__global__ void __launch_bounds__(256) k_q_node(const int* __restrict__ diag, const int* __restrict__ soff,
+                                                const int* __restrict__ slist, const double* __restrict__ qrec,
                                                 int nshg, int first, double* __restrict__ rmass,
                                                 double* __restrict__ qres) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
+        const int d = diag[i];
         double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, m = 0.0;
-        const int p1 = noff[i + 1];
-        for (int p = noff[i]; p < p1; ++p) {
-            const double4* r = reinterpret_cast<const double4*>(qrow + 8 * (size_t)p);
+        const int p1 = soff[d + 1];
+        for (int p = soff[d]; p < p1; ++p) {
+            const int t = slist[p];
+            const int e = t >> 4, a = (t >> 2) & 3;
+            const double4* r = reinterpret_cast<const double4*>(qrec + 8 * (size_t)e);
             const double4 A = r[0], B = r[1];
-            const double wa = A.x;
+            const double wa = A.x * c_el.SN[a];
             // qdi(1:9) column-major 3x3, symmetric
             const double qd[9] = {A.y, A.z, A.w, A.z, B.x, B.y, A.w, B.y, B.z};
 #pragma unroll
@@ -247,19 +247,17 @@ __global__ void __launch_bounds__(256) k_q_rows(const int* __restrict__ noff, co
 }
 
 // ---------------------------------------------------------------------------
-// AsIGMR / e3 / e3LHS, four lanes per element, writing row records.
+// AsIGMR / e3 / e3LHS, four lanes per element, writing element records.
 //
-// Lane a of element e writes the row record of (e, a) -- everything row
-// n_a of the residual and of the tangent needs from this element -- at
-// erow + RS npos[4 e + a] (node-sorted, every group 32-byte aligned):
-//   kLhs == 1 (FP64 tangent), RS = 24:
-//     [0:4)   rl(a, 0:4)  (momentum 1-3, continuity; unpermuted)
-//     [4:8)   tc, tm, tlW, cc = tlW/rho sum_q tauM_q
-//     [8:20)  shg transposed: shg[n][k] at 8 + 4k + n
-//     [20:24) Kd(a, b), b = 0..3
-//   kLhs == 2 (FP32 tangent quadrature), RS = 16: rl at [0:4), then 20
-//     floats at double offset 4 with the FP32 layout of [4:24) above.
-//   kLhs == 0 (residual only), RS = 4: rl.
+// Record of element e (RS doubles at erec + RS e, every group 32-byte aligned):
+//   kLhs == 1 (FP64 tangent), RS = 48:
+//     [0:4)   tc, tm, tlW, cc = tlW/rho sum_q tauM_q
+//     [4:16)  shg transposed: shg[n][k] at 4 + 4k + n
+//     [16:32) Kd(a,b) at 16 + 4a + b
+//     [32:48) rl(a, 0:4) at 32 + 4a  (momentum 1-3, continuity)
+//   kLhs == 2 (FP32 tangent quadrature), RS = 32: rl at [0:16), then 32
+//     floats at double offset 16 with the FP32 layout of [0:32) above.
+//   kLhs == 0 (residual only), RS = 16: rl at [0:16).
 // ---------------------------------------------------------------------------
 constexpr int kQ = 28;        // doubles of per-point data exchanged in shared memory
 // Shared-memory exchange: element k of a block at k * kQE + q * kQ.  The odd
@@ -270,16 +268,17 @@ constexpr int kQE = 4 * kQ + 1;
 
 template <int kLhs>
 struct RecLayout {
-    static constexpr int RS = kLhs == 1 ? 24 : (kLhs == 2 ? 16 : 4);
+    static constexpr int RS = kLhs == 1 ? 48 : (kLhs == 2 ? 32 : 16);
+    static constexpr int RO = kLhs == 1 ? 32 : 0;
 };
 
 // Four blocks of 128 threads per SM (128 registers).
 template <int kLhs>
 __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien, const double4* __restrict__ x,
                                                 const double4* __restrict__ y, const double4* __restrict__ ac,
-                                                const double* __restrict__ qres, const int* __restrict__ npos,
-                                                int nelem, ElmParams P, double* __restrict__ erow) {
-    constexpr int RS = RecLayout<kLhs>::RS;
+                                                const double* __restrict__ qres, int nelem, ElmParams P,
+                                                double* __restrict__ erec) {
+    constexpr int RS = RecLayout<kLhs>::RS, RO = RecLayout<kLhs>::RO;
     __shared__ double sq[32 * kQE];
     const int lane4 = threadIdx.x & 3;
     double* const sqe = sq + (threadIdx.x >> 2) * kQE;   // this element's per-point data
@@ -439,7 +438,7 @@ __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien,
         double Na[4];
 #pragma unroll
         for (int qq = 0; qq < 4; ++qq) Na[qq] = c_el.shp[qq][a];
-        double* rec = erow + (size_t)RS * (size_t)(live ? npos[4 * e + a] : 0);
+        double* rec = erec + (size_t)RS * (size_t)(live ? e : 0);
         if (live) {
             // residual row a (e3res.f90:263-284, unpermuted: momentum 1-3, continuity)
             double sG[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, sN[3] = {0, 0, 0};
@@ -458,8 +457,8 @@ __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien,
             double v[3];
 #pragma unroll
             for (int i = 0; i < 3; ++i) v[i] = sN[i] + shg[a][0] * sG[i][0] + shg[a][1] * sG[i][1] + shg[a][2] * sG[i][2];
-            reinterpret_cast<double4*>(rec)[0] = make_double4(-WdetJ * v[0], -WdetJ * v[1], -WdetJ * v[2],
-                                                              WdetJ * div_ub);
+            reinterpret_cast<double4*>(rec + RO)[a] = make_double4(-WdetJ * v[0], -WdetJ * v[1], -WdetJ * v[2],
+                                                                   WdetJ * div_ub);
         }
         if (kLhs == 1 && live) {
             const double lhsFct = P.alfi * P.gami * P.Delt;
@@ -490,10 +489,11 @@ __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien,
                 Kd[b] = tsFct * c_el.M[a][b] + tlW * (rho * conv + 4.0 * mu * grad + sym);
             }
             double4* r4 = reinterpret_cast<double4*>(rec);
-            r4[1] = make_double4(tlW * TC, tlW * 4.0 * mu, tlW, tlW / rho * TM);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) r4[2 + k] = make_double4(shg[0][k], shg[1][k], shg[2][k], shg[3][k]);
-            r4[5] = make_double4(Kd[0], Kd[1], Kd[2], Kd[3]);
+            r4[4 + a] = make_double4(Kd[0], Kd[1], Kd[2], Kd[3]);
+            if (a < 3)
+                r4[1 + a] = make_double4(shg[0][a], shg[1][a], shg[2][a], shg[3][a]);
+            else
+                r4[0] = make_double4(tlW * TC, tlW * 4.0 * mu, tlW, tlW / rho * TM);
         }
         if (kLhs == 2 && live) {
             // FP32 element quadrature of the tangent
@@ -527,12 +527,12 @@ __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien,
                 const float grad = sga[0] * (float)shg[b][0] + sga[1] * (float)shg[b][1] + sga[2] * (float)shg[b][2];
                 Kd[b] = tsFct * (float)c_el.M[a][b] + tlW * (rhof * conv + 4.0f * muf * grad + sym);
             }
-            float4* r4 = reinterpret_cast<float4*>(rec + 4);
-            r4[0] = make_float4(tlW * TC, tlW * 4.0f * muf, tlW, tlW / rhof * TM);
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-                r4[1 + k] = make_float4((float)shg[0][k], (float)shg[1][k], (float)shg[2][k], (float)shg[3][k]);
-            r4[4] = make_float4(Kd[0], Kd[1], Kd[2], Kd[3]);
+            float4* r4 = reinterpret_cast<float4*>(rec + 16);
+            r4[4 + a] = make_float4(Kd[0], Kd[1], Kd[2], Kd[3]);
+            if (a < 3)
+                r4[1 + a] = make_float4((float)shg[0][a], (float)shg[1][a], (float)shg[2][a], (float)shg[3][a]);
+            else
+                r4[0] = make_float4(tlW * TC, tlW * 4.0f * muf, tlW, tlW / rhof * TM);
         }
         __syncwarp();
     }
@@ -554,19 +554,25 @@ __device__ __forceinline__ void pair_block(const T sa[3], const T sb[3], T Kd, T
     o[12] = cc * grad;
 }
 
-// Block (a, b) from the row record of (e, a) staged in shared memory.
+// Contribution of element pair (a, b) to its slot, in the record's precision.
 template <int kLhs>
-__device__ __forceinline__ void row_block(const double* __restrict__ rec, int a, int b, double o[13]) {
+__device__ __forceinline__ void record_block(const double* __restrict__ rec, int a, int b, double o[13]) {
     if (kLhs == 1) {
-        const double sa[3] = {rec[8 + a], rec[12 + a], rec[16 + a]};
-        const double sb[3] = {rec[8 + b], rec[12 + b], rec[16 + b]};
-        pair_block<double>(sa, sb, rec[20 + b], rec[4], rec[5], rec[6] * c_el.SN[a], rec[7], o);
+        const double4* r4 = reinterpret_cast<const double4*>(rec);
+        const double4 sc = r4[0], s0 = r4[1], s1 = r4[2], s2 = r4[3];
+        const double sa[3] = {sel4(s0, a), sel4(s1, a), sel4(s2, a)};
+        const double sb[3] = {sel4(s0, b), sel4(s1, b), sel4(s2, b)};
+        const double Kd = rec[16 + 4 * a + b];
+        pair_block<double>(sa, sb, Kd, sc.x, sc.y, sc.z * c_el.SN[a], sc.w, o);
     } else {
-        const float* rf = reinterpret_cast<const float*>(rec + 4);
-        const float sa[3] = {rf[4 + a], rf[8 + a], rf[12 + a]};
-        const float sb[3] = {rf[4 + b], rf[8 + b], rf[12 + b]};
+        const float* rf = reinterpret_cast<const float*>(rec + 16);
+        const float4* r4 = reinterpret_cast<const float4*>(rf);
+        const float4 sc = r4[0], s0 = r4[1], s1 = r4[2], s2 = r4[3];
+        const float sa[3] = {sel4(s0, a), sel4(s1, a), sel4(s2, a)};
+        const float sb[3] = {sel4(s0, b), sel4(s1, b), sel4(s2, b)};
+        const float Kd = rf[16 + 4 * a + b];
         float of[13];
-        pair_block<float>(sa, sb, rf[16 + b], rf[0], rf[1], rf[2] * (float)c_el.SN[a], rf[3], of);
+        pair_block<float>(sa, sb, Kd, sc.x, sc.y, sc.z * (float)c_el.SN[a], sc.w, of);
 #pragma unroll
         for (int k = 0; k < 13; ++k) o[k] = (double)of[k];
     }
@@ -591,79 +597,78 @@ __device__ __forceinline__ void store_block(long long s, const double acc[13], d
     }
 }
 
-// Row pass: one warp per node i forms residual row i and every tangent block
-// of CSR row i.  The row's records (one per element containing i, ascending
-// element order) are contiguous; the warp stages them 32 at a time in
-// shared memory with coalesced loads.  Lane l owns slot l (then l + 32, ...)
-// of the row and adds, record by record in order, the block of every record
-// whose byte b of lsl names slot l; lanes 0..3 sum component l of the
-// residual rows, then the boundary faces at i (ascending face order, AsBMFG
-// after AsIGMR as in elmgmr.f90).  Every sum runs in ascending element
-// order: deterministic.
-constexpr int kRowWarps = 4;
-
+// Node pass: residual row and diagonal tangent block of every node.  The
+// elements containing node i are the contributions of its diagonal slot
+// (ascending element order); then the boundary faces at i (ascending face
+// order, AsBMFG after AsIGMR as in elmgmr.f90).  One thread per node.
 template <int kLhs>
-__global__ void __launch_bounds__(32 * kRowWarps) k_row_pass(const int* __restrict__ rowptr, const int* __restrict__ diag,
-                                                        const int* __restrict__ noff,
-                                                        const unsigned int* __restrict__ lsl,
-                                                        const double* __restrict__ erow, const int* __restrict__ fnoff,
-                                                        const int* __restrict__ flist, const double* __restrict__ frec,
-                                                        int nshg, double* __restrict__ res, double* __restrict__ lhsK,
-                                                        double* __restrict__ lhsP, float* __restrict__ lhs32) {
+__global__ void __launch_bounds__(256) k_node_pass(const int* __restrict__ diag, const int* __restrict__ soff,
+                                                   const int* __restrict__ slist, const double* __restrict__ erec,
+                                                   const int* __restrict__ fnoff, const int* __restrict__ flist,
+                                                   const double* __restrict__ frec, int nshg,
+                                                   double* __restrict__ res, double* __restrict__ lhsK,
+                                                   double* __restrict__ lhsP, float* __restrict__ lhs32) {
+    constexpr int RS = RecLayout<kLhs>::RS, RO = RecLayout<kLhs>::RO;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
+        const int d = diag[i];
+        double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
+        double acc[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const int p1 = soff[d + 1];
+        for (int p = soff[d]; p < p1; ++p) {
+            const int t = slist[p];
+            const int e = t >> 4, a = (t >> 2) & 3;
+            const double* rec = erec + (size_t)RS * (size_t)e;
+            const double4 rl = reinterpret_cast<const double4*>(rec + RO)[a];
+            r0 += rl.x;
+            r1 += rl.y;
+            r2 += rl.z;
+            r3 += rl.w;
+            if (kLhs) {
+                double o[13];
+                record_block<kLhs == 2 ? 2 : 1>(rec, a, a, o);
+#pragma unroll
+                for (int c = 0; c < 13; ++c) acc[c] += o[c];
+            }
+        }
+        if (fnoff) {
+            const int f1 = fnoff[i + 1];
+            for (int p = fnoff[i]; p < f1; ++p) {
+                const double4 rl = reinterpret_cast<const double4*>(frec)[flist[p]];
+                r0 += rl.x;
+                r1 += rl.y;
+                r2 += rl.z;
+                r3 += rl.w;
+            }
+        }
+        reinterpret_cast<double4*>(res)[i] = make_double4(r0, r1, r2, r3);
+        if (kLhs) store_block<kLhs == 2 ? 2 : 1>(d, acc, lhsK, lhsP, lhs32);
+    }
+}
+
+// Slot pass: every off-diagonal CSR block (i, j) from the elements that
+// contain the edge (ascending element order).  One thread per slot; the
+// diagonal slots (first contribution with a == b) belong to the node pass.
+template <int kLhs>
+__global__ void __launch_bounds__(256) k_slot_pass(const int* __restrict__ soff, const int* __restrict__ slist,
+                                                   const double* __restrict__ erec, long long nnz,
+                                                   double* __restrict__ lhsK, double* __restrict__ lhsP,
+                                                   float* __restrict__ lhs32) {
     constexpr int RS = RecLayout<kLhs>::RS;
-    __shared__ __align__(16) double srec[kRowWarps][32 * RS];
-    __shared__ unsigned int slsl[kRowWarps][32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    double* const R = srec[w];
-    const long long nwarps = (long long)gridDim.x * kRowWarps;
-    for (long long iw = (long long)blockIdx.x * kRowWarps + w; iw < nshg; iw += nwarps) {
-        const int i = (int)iw;
-        const int r0 = rowptr[i], len = kLhs ? rowptr[i + 1] - r0 : 0;
-        const unsigned int dl = (unsigned int)(diag[i] - r0);
-        const int n0 = noff[i], nrec = noff[i + 1] - n0;
-        double rsum = 0.0;
-        const int nsb = kLhs ? (len + 31) / 32 : 1;
-        for (int sb = 0; sb < nsb; ++sb) {
-            double acc[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-            const int slot = 32 * sb + lane;
-            for (int rc = 0; rc < nrec; rc += 32) {
-                const int m = min(32, nrec - rc);
-                const double2* src = reinterpret_cast<const double2*>(erow + (size_t)RS * (size_t)(n0 + rc));
-                double2* dst = reinterpret_cast<double2*>(R);
-                for (int q = lane; q < m * (RS / 2); q += 32) dst[q] = src[q];
-                if (kLhs && lane < m) slsl[w][lane] = lsl[n0 + rc + lane];
-                __syncwarp();
-                if (sb == 0 && lane < 4)
-                    for (int j = 0; j < m; ++j) rsum += R[RS * j + lane];
-                if (kLhs && slot < len) {
-                    for (int j = 0; j < m; ++j) {
-                        const unsigned int pk = slsl[w][j];
-                        int a = 0, b = -1;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nnz;
+         s += (long long)gridDim.x * blockDim.x) {
+        const int p0 = soff[s], p1 = soff[s + 1];
+        const int t0 = slist[p0];
+        if (((t0 >> 2) & 3) == (t0 & 3)) continue;
+        double acc[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int p = p0; p < p1; ++p) {
+            const int t = p == p0 ? t0 : slist[p];
+            const int e = t >> 4, a = (t >> 2) & 3, b = t & 3;
+            double o[13];
+            record_block<kLhs>(erec + (size_t)RS * (size_t)e, a, b, o);
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const unsigned int byte = (pk >> (8 * q)) & 0xffu;
-                            if (byte == dl) a = q;
-                            if (byte == (unsigned int)slot) b = q;
-                        }
-                        if (b >= 0) {
-                            double o[13];
-                            row_block<kLhs == 2 ? 2 : 1>(R + RS * j, a, b, o);
-#pragma unroll
-                            for (int c = 0; c < 13; ++c) acc[c] += o[c];
-                        }
-                    }
-                }
-                __syncwarp();
-            }
-            if (kLhs && slot < len) store_block<kLhs == 2 ? 2 : 1>((long long)r0 + slot, acc, lhsK, lhsP, lhs32);
+            for (int c = 0; c < 13; ++c) acc[c] += o[c];
         }
-        if (lane < 4) {
-            if (fnoff) {
-                const int f1 = fnoff[i + 1];
-                for (int p = fnoff[i]; p < f1; ++p) rsum += frec[4 * (size_t)flist[p] + lane];
-            }
-            res[4 * (size_t)i + lane] = rsum;
-        }
+        store_block<kLhs>(s, acc, lhsK, lhsP, lhs32);
     }
 }
 
@@ -825,9 +830,9 @@ __global__ void k_bc3res(const int* __restrict__ iBC, int nshg, double* __restri
 int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1, const double* coef2,
                   double* d_res, double* d_lhsK, double* d_lhsP, int lhs, float* d_lhs32) {
     cudaStream_t s = c->stream;
-    // every pass below reads the pattern's node-sorted record positions
+    // every pass below reads the pattern's contribution lists
     if (c->nnz == 0) CR_CHECK(build_pattern(c));
-    if (!c->noff.p || !c->npos.p || !c->lsl.p) return CRIMSON_ERR_STATE;
+    if (!c->diag.p || !c->soff.p || !c->slist.p) return CRIMSON_ERR_STATE;
     CR_CHECK(upload_elm_consts(s));
     const ElmParams P = elm_params(c->p);
     const double4* y4 = reinterpret_cast<const double4*>(d_y);
@@ -836,24 +841,23 @@ int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const d
     if (c->p.idiff == 1) {
         CR_CHECK(c->qres.alloc((size_t)c->nshg * 9));
         CR_CHECK(c->rmass.alloc((size_t)c->nshg));
-        CR_CHECK(c->qrow.alloc((size_t)c->nelem * 32));
+        CR_CHECK(c->qrec.alloc((size_t)c->nelem * 8));
         const bool first = !c->rmass_ready;
-        launch(k_asiq_rec, grid_for(c->nelem, 128, 16), 128, 0, s, c->ien.p, c->x.p, y4, c->npos.p, c->nelem, P,
-               c->qrow.p);
-        launch(k_q_rows, grid_for(c->nshg, 256), 256, 0, s, c->noff.p, c->qrow.p, c->nshg, first ? 1 : 0, c->rmass.p,
-               c->qres.p);
+        launch(k_asiq_rec, grid_for(c->nelem, 128, 16), 128, 0, s, c->ien.p, c->x.p, y4, c->nelem, P, c->qrec.p);
+        launch(k_q_node, grid_for(c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->qrec.p, c->nshg,
+               first ? 1 : 0, c->rmass.p, c->qres.p);
         c->rmass_ready = true;
     }
-    // row records (sized for the FP64 tangent layout, the largest)
-    CR_CHECK(c->erow.alloc((size_t)c->nelem * 4 * RecLayout<1>::RS));
+    // element records (sized for the FP64 tangent layout, the largest)
+    CR_CHECK(c->erec.alloc((size_t)c->nelem * 48));
     const int blk = 128;
     const int grid = grid_for((long long)c->nelem * 4, blk, 16);
     if (lhs == 2)
-        launch(k_asigmr<2>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->npos.p, c->nelem, P, c->erow.p);
+        launch(k_asigmr<2>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->nelem, P, c->erec.p);
     else if (lhs)
-        launch(k_asigmr<1>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->npos.p, c->nelem, P, c->erow.p);
+        launch(k_asigmr<1>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->nelem, P, c->erec.p);
     else
-        launch(k_asigmr<0>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->npos.p, c->nelem, P, c->erow.p);
+        launch(k_asigmr<0>, grid, blk, 0, s, c->ien.p, c->x.p, y4, a4, c->qres.p, c->nelem, P, c->erec.p);
     CR_CUDA(cudaGetLastError());
     if (c->nface > 0) {
         CR_CHECK(c->frec.alloc((size_t)c->nface * 12));
@@ -861,17 +865,20 @@ int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const d
                c->frec.p);
     }
     const int* fno = c->nface > 0 ? c->fnoff.p : nullptr;
-    const int gr = grid_for((long long)c->nshg * 32, 32 * kRowWarps, 16);
-    const unsigned int* lsl = c->lsl.p;
-    if (lhs == 2)
-        launch(k_row_pass<2>, gr, 32 * kRowWarps, 0, s, c->rowptr.p, c->diag.p, c->noff.p, lsl, c->erow.p, fno,
-               c->flist.p, c->frec.p, c->nshg, d_res, nullptr, nullptr, d_lhs32);
-    else if (lhs)
-        launch(k_row_pass<1>, gr, 32 * kRowWarps, 0, s, c->rowptr.p, c->diag.p, c->noff.p, lsl, c->erow.p, fno,
-               c->flist.p, c->frec.p, c->nshg, d_res, d_lhsK, d_lhsP, nullptr);
-    else
-        launch(k_row_pass<0>, gr, 32 * kRowWarps, 0, s, c->rowptr.p, c->diag.p, c->noff.p, lsl, c->erow.p, fno,
-               c->flist.p, c->frec.p, c->nshg, d_res, nullptr, nullptr, nullptr);
+    const int ng = grid_for(c->nshg, 256);
+    const int gs = grid_for(c->nnz, 256);
+    if (lhs == 2) {
+        launch(k_node_pass<2>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p, c->frec.p,
+               c->nshg, d_res, nullptr, nullptr, d_lhs32);
+        launch(k_slot_pass<2>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, nullptr, nullptr, d_lhs32);
+    } else if (lhs) {
+        launch(k_node_pass<1>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p, c->frec.p,
+               c->nshg, d_res, d_lhsK, d_lhsP, nullptr);
+        launch(k_slot_pass<1>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, d_lhsK, d_lhsP, nullptr);
+    } else {
+        launch(k_node_pass<0>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p, c->frec.p,
+               c->nshg, d_res, nullptr, nullptr, nullptr);
+    }
     if (c->ncoupled > 0) {
         double* hc = c->coef_host.data();
         for (int k = 0; k < c->ncoupled; ++k) {

@@ -176,21 +176,19 @@ struct crimson_ctx {
     crimson::DBuf<int> col;         // (nnz) 0-based
     crimson::DBuf<int> diag;        // (nshg) position of the diagonal block
     crimson::DBuf<int> trans;       // (nnz) position of the transposed block
-    // Row records of the owner-computes scatter: the incidences (element e,
-    // local node a) sorted by node, ascending e within a node.  Node i owns
-    // positions noff[i] .. noff[i+1]); npos[4 e + a] is the position of
-    // (e, a); lsl[position] packs, for b = 0..3, the local slot index
-    // (slot - rowptr[node a]) of block (a, b) in byte b.
-    crimson::DBuf<int> noff;        // (nshg+1)
-    crimson::DBuf<int> npos;        // (nelem*4)
-    crimson::DBuf<unsigned int> lsl;  // (nelem*4)
+    // Contribution lists of the owner-computes scatter: slist holds the
+    // element pairs t = 16 e + 4 a + b grouped by CSR slot, ascending t within
+    // a slot; slot s owns slist[soff[s] .. soff[s+1]).  The diagonal slot of
+    // node i lists exactly the elements containing i (b == a).
+    crimson::DBuf<int> slist;       // (nelem*16)
+    crimson::DBuf<int> soff;        // (nnz+1)
 
     // ElmGMR work space
     crimson::DBuf<double> qres;     // (nshg, 9) node-major: q[9*i + k]
     crimson::DBuf<double> rmass;    // (nshg) 1 / lumped mass (geometry only)
     bool rmass_ready = false;       // rmass holds the inverse lumped mass
-    crimson::DBuf<double> qrow;     // (nelem*4, 8) AsIq row records {W N_a, q11,q12,q13,q22,q23,q33, 0}
-    crimson::DBuf<double> erow;     // (nelem*4, 24) residual / tangent row records
+    crimson::DBuf<double> qrec;     // (nelem, 8) AsIq element records {W, q11,q12,q13,q22,q23,q33, 0}
+    crimson::DBuf<double> erec;     // (nelem, 48) element records of the residual and tangent
     crimson::DBuf<double> y4, ac4, res4;   // (4, nshg) staging for host-pointer calls
     crimson::DBuf<double> lhsK, lhsP;      // (9, nnz), (4, nnz)
     crimson::DBuf<float> lhs32;            // (16, nnz) FP32 tangent records (mixed precision)

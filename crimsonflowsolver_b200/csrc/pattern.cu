@@ -8,13 +8,11 @@
 // sorted, deduplicated rows genadj produces (diagonal included), so the
 // pattern is bit-identical.  The same pass precomputes what the reference
 // searches for at every assembly and solve:
-//   noff/npos/lsl - the (element, local node) incidences sorted by node,
-//                ascending element within a node (the diagonal slot's run of
-//                the stable sort), and for each the local slots of its four
-//                blocks (a, b): ElmGMR's owner-computes scatter sums every
-//                residual row and CSR block in this element order, which is
-//                fillsparseI's serial order (fillsparse.f90:29-60), and needs
-//                no search (sparseloc, fillsparse.f90:210-246)
+//   slist/soff - the element pairs of every CSR slot, ascending t (the
+//                owner-computes scatter of ElmGMR sums them in this order,
+//                which is fillsparseI's serial element order,
+//                fillsparse.f90:29-60; replaces sparseloc's searches,
+//                fillsparse.f90:210-246)
 //   diag  - diagonal slot per row                   (diagPtr, memLS.f90:1121-1131)
 //   trans - slot of the transposed block (j,i)      (solfar.f90:225-232, memLS.f90:1664-1675)
 #include <cub/cub.cuh>
@@ -87,46 +85,6 @@ __global__ void k_diag_trans(const int* __restrict__ rowptr, const int* __restri
     }
 }
 
-// count of incidences per node = run length of its diagonal slot
-__global__ void k_node_counts(const int* __restrict__ diag, const int* __restrict__ soff, int n, int* __restrict__ cnt) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        cnt[i] = soff[diag[i] + 1] - soff[diag[i]];
-}
-
-// npos[4 e + a]: node-sorted position of incidence (e, a), from the
-// diagonal slot's run (pairs t = 16 e + 5 a, ascending e)
-__global__ void k_npos(const int* __restrict__ diag, const int* __restrict__ soff, const int* __restrict__ slist,
-                       const int* __restrict__ noff, int n, int* __restrict__ npos) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int d = diag[i], p0 = soff[d], p1 = soff[d + 1], base = noff[i];
-        for (int p = p0; p < p1; ++p) {
-            const int t = slist[p];
-            npos[4 * (t >> 4) + ((t >> 2) & 3)] = base + (p - p0);
-        }
-    }
-}
-
-// byte b of lsl[npos[4 e + a]] = slot of pair (e, a, b) - rowptr[node a]
-__global__ void k_lsl(const int* __restrict__ soff, const int* __restrict__ slist, const int4* __restrict__ ien,
-                      const int* __restrict__ rowptr, const int* __restrict__ npos, long long nnz,
-                      unsigned char* __restrict__ lsl, int* __restrict__ bad) {
-    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nnz;
-         s += (long long)gridDim.x * blockDim.x) {
-        for (int p = soff[s]; p < soff[s + 1]; ++p) {
-            const int t = slist[p];
-            const int e = t >> 4, a = (t >> 2) & 3, b = t & 3;
-            const int4 nn = ien[e];
-            const int na = a == 0 ? nn.x : (a == 1 ? nn.y : (a == 2 ? nn.z : nn.w));
-            const long long loc = s - rowptr[na];
-            if (loc < 0 || loc > 255) {
-                atomicAdd(bad, 1);
-                continue;
-            }
-            lsl[4 * (size_t)npos[4 * e + a] + b] = (unsigned char)loc;
-        }
-    }
-}
-
 __global__ void k_to_one_based(const int* __restrict__ in, int* __restrict__ out, long long n) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     for (; t < n; t += (long long)gridDim.x * blockDim.x) out[t] = in[t] + 1;
@@ -177,13 +135,12 @@ int build_pattern(crimson_ctx* c) {
     CR_CHECK(c->col.alloc((size_t)hnnz));
     CR_CHECK(c->diag.alloc((size_t)c->nshg));
     CR_CHECK(c->trans.alloc((size_t)hnnz));
-    DBuf<int> soff;
-    CR_CHECK(soff.alloc((size_t)hnnz + 1));
-    // soff = exclusive sum of the run lengths, soff[nnz] = npair; the sorted
-    // pair indices dv.Current() list every slot's pairs in ascending order
+    CR_CHECK(c->soff.alloc((size_t)hnnz + 1));
+    CR_CHECK(c->slist.alloc((size_t)npair));
+    // soff = exclusive sum of the run lengths, soff[nnz] = npair
     CR_CUDA(cudaMemsetAsync(counts.p + hnnz, 0, sizeof(int), s));
-    CR_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tb_scan, counts.p, soff.p, hnnz + 1, s));
-    const int* slist = dv.Current();
+    CR_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tb_scan, counts.p, c->soff.p, hnnz + 1, s));
+    CR_CUDA(cudaMemcpyAsync(c->slist.p, dv.Current(), sizeof(int) * (size_t)npair, cudaMemcpyDeviceToDevice, s));
     CR_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
     launch(k_rowptr_cols, grid_for((long long)hnnz + c->nshg + 1, 256), 256, 0, s, ukeys.p, hnnz, c->nshg, c->rowptr.p,
                                                                               c->col.p);
@@ -196,23 +153,6 @@ int build_pattern(crimson_ctx* c) {
     if (hbad) {
         set_last_error("pattern: missing diagonal / transposed block");
         return CRIMSON_ERR_PATTERN;
-    }
-    // row records: node-sorted incidence positions and local slot bytes
-    CR_CHECK(c->noff.alloc((size_t)c->nshg + 1));
-    CR_CHECK(c->npos.alloc(4 * (size_t)c->nelem));
-    CR_CHECK(c->lsl.alloc(4 * (size_t)c->nelem));
-    launch(k_node_counts, grid_for(c->nshg, 256), 256, 0, s, c->diag.p, soff.p, c->nshg, counts.p);
-    CR_CUDA(cudaMemsetAsync(counts.p + c->nshg, 0, sizeof(int), s));
-    CR_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tb_scan, counts.p, c->noff.p, c->nshg + 1, s));
-    launch(k_npos, grid_for(c->nshg, 256), 256, 0, s, c->diag.p, soff.p, slist, c->noff.p, c->nshg, c->npos.p);
-    launch(k_lsl, grid_for(c->nnz, 256), 256, 0, s, soff.p, slist, c->ien.p, c->rowptr.p, c->npos.p, c->nnz,
-           reinterpret_cast<unsigned char*>(c->lsl.p), bad.p);
-    CR_CUDA(cudaGetLastError());
-    CR_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CR_CUDA(cudaStreamSynchronize(s));
-    if (hbad) {
-        set_last_error("pattern: a node has more than 256 neighbours (row of the CSR pattern longer than 256)");
-        return CRIMSON_ERR_UNSUPPORTED;
     }
     return CRIMSON_OK;
 }

@@ -208,6 +208,40 @@ def test_adjoint_gradient_matches_central_fd():
     assert err.max() < 1e-4, err
 
 
+def _oracle_objective(prob, theta):
+    """J(theta) from the FP64 CPU oracle's own time stepping (the reference
+    algorithm restated), one thread so that every evaluation rounds alike."""
+    from oracle import pyoracle as po
+
+    F = po.OracleFlow(prob.mesh, prob.params(theta), nthreads=1, inflow=prob.inflow)
+    Ps = np.zeros((prob.nsteps, prob.nc))
+    for n in range(prob.nsteps):
+        F.step()
+        Ps[n] = F.Pn
+    return prob._objective(Ps)
+
+
+def test_adjoint_gradient_matches_central_fd_of_oracle():
+    """The GPU adjoint gradient against central differences (relative step
+    1e-6) of the reference solver restated on the CPU, for mu and the 9 RCR
+    parameters: within 1e-4 relative per component (log-sensitivities)."""
+    prob = _problem(ce=2)
+    th = prob.theta0()
+    J, g = prob.gradient(th)
+    J_oracle = _oracle_objective(prob, th)
+    assert abs(J - J_oracle) <= 1e-8 * abs(J_oracle), (J, J_oracle)
+    fd = np.zeros_like(th)
+    for i in range(len(th)):
+        h = 1e-6 * abs(th[i])
+        tp, tm = th.copy(), th.copy()
+        tp[i] += h
+        tm[i] -= h
+        fd[i] = (_oracle_objective(prob, tp) - _oracle_objective(prob, tm)) / (2 * h)
+    err = np.abs(th * g - th * fd) / np.abs(th * fd)
+    print("oracle central FD: J", J_oracle, "\nlog-sensitivities adjoint", th * g, "\nfd", th * fd, "\nerr", err)
+    assert err.max() < 1e-4, err
+
+
 def test_checkpoint_interval_and_autograd():
     import torch
 
