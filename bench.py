@@ -49,7 +49,13 @@ sys.path.insert(0, ROOT)
 METRIC = "s/timestep @4M tets (mixed vs FP64 GPU, ≤1e-6 rel err); Melem/s assembly"
 NCROSS, NAXIAL = 80, 133
 NITR = 3
-EPSTOL_NS = 1e-6      # memLS NSSOLVER relative tolerance (epstol(8))
+# memLS NSSOLVER relative tolerance (epstol(8)).  1e-6 is below what the
+# reference's residual estimate sqrt(|R0|^2 - xB.B) decides reliably: on the
+# 107,520-tet cylinder the CPU oracle's first solve stops after 8 outer
+# iterations with 8 threads and runs to the 10-iteration limit with 1 thread
+# (estimates 6.9e-7 and 1.4e-6 of the initial norm), and the first solve of
+# this workload reaches the 10-iteration limit on CPU and GPU alike.
+EPSTOL_NS = 1e-5
 REFINE_TOL = 0.0      # mixed precision: FP64 defect target (0: the NSSOLVER tolerance)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one persistent
 # CG iteration divided by cg_iter_bytes, from ncu captures of one launch of 50

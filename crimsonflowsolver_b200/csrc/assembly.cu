@@ -597,15 +597,110 @@ __device__ __forceinline__ void store_block(long long s, const double acc[13], d
     }
 }
 
+// ---------------------------------------------------------------------------
+// bc3LHS (bc3lhs.f90:39-198) on one element's 3x3 momentum block K
+// (row-major) for a node with one or two prescribed velocity components
+// (m = ibits(iBC,3,3) in 1..6; coefficients BC(:,4..6) = b4, b5, b6).  The
+// reference projects, per element and node inod in order, the columns of the
+// blocks (i, inod), then the rows of the blocks (inod, i), then sets the
+// constrained diagonal entries of block (inod, inod) to 1; G and C are not
+// touched.  A block (a, b) therefore gets the row operation of node a and the
+// column operation of node b, the one of the smaller local index first.  The
+// two-component case m = 6 keeps the reference's own row update (row 3 from
+// row 1 and entry 6, rows 1-2 zeroed).
+// ---------------------------------------------------------------------------
+struct NodeBC {
+    int m;   // ibits(iBC,3,3)
+    double b4, b5, b6;
+};
+
+__device__ __forceinline__ bool bc_partial(int m) { return m != 0 && m != 7; }
+
+__device__ __forceinline__ NodeBC node_bc(const int* __restrict__ iBC, const double* __restrict__ BC, int ndofBC,
+                                          int n) {
+    NodeBC r;
+    r.m = (iBC[n] >> 3) & 7;
+    r.b4 = r.b5 = r.b6 = 0.0;
+    if (bc_partial(r.m)) {
+        const double* b = BC + (size_t)ndofBC * n;
+        r.b4 = b[3];
+        r.b5 = b[4];
+        r.b6 = b[5];
+    }
+    return r;
+}
+
+__device__ __forceinline__ void bc_colop(const NodeBC& n, double K[9]) {
+    const int m = n.m;
+    if (m == 1 || m == 2 || m == 4) {
+        const int c0 = m == 1 ? 0 : (m == 2 ? 1 : 2), f1 = m == 1 ? 1 : 0, f2 = m == 4 ? 1 : 2;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            K[3 * r + f1] = K[3 * r + f1] - n.b4 * K[3 * r + c0];
+            K[3 * r + f2] = K[3 * r + f2] - n.b5 * K[3 * r + c0];
+            K[3 * r + c0] = 0.0;
+        }
+    } else if (m == 3 || m == 5 || m == 6) {
+        const int f = m == 3 ? 2 : (m == 5 ? 1 : 0), c0 = m == 6 ? 1 : 0, c1 = m == 3 ? 1 : 2;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            K[3 * r + f] = K[3 * r + f] - n.b4 * K[3 * r + c0] - n.b6 * K[3 * r + c1];
+            K[3 * r + c0] = 0.0;
+            K[3 * r + c1] = 0.0;
+        }
+    }
+}
+
+__device__ __forceinline__ void bc_rowop(const NodeBC& n, double K[9]) {
+    const int m = n.m;
+    if (m == 1 || m == 2 || m == 4) {
+        const int c0 = m == 1 ? 0 : (m == 2 ? 1 : 2), f1 = m == 1 ? 1 : 0, f2 = m == 4 ? 1 : 2;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            K[3 * f1 + q] = K[3 * f1 + q] - n.b4 * K[3 * c0 + q];
+            K[3 * f2 + q] = K[3 * f2 + q] - n.b5 * K[3 * c0 + q];
+            K[3 * c0 + q] = 0.0;
+        }
+    } else if (m == 3 || m == 5) {
+        const int f = m == 3 ? 2 : 1, c1 = m == 3 ? 1 : 2;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            K[3 * f + q] = K[3 * f + q] - n.b4 * K[q] - n.b6 * K[3 * c1 + q];
+            K[q] = 0.0;
+            K[3 * c1 + q] = 0.0;
+        }
+    } else if (m == 6) {
+        K[6] = K[6] - n.b4 * K[0];
+        K[7] = K[7] - n.b4 * K[1];
+        K[8] = K[8] - n.b4 * K[2] - n.b6 * K[5];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) K[q] = 0.0;
+    }
+}
+
+// 1 on the constrained diagonal entries (block (inod, inod) only)
+__device__ __forceinline__ void bc_diag(const NodeBC& n, double K[9], double v) {
+    const int m = n.m;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        if ((m >> c) & 1) K[4 * c] = v;
+}
+
 // Node pass: residual row and diagonal tangent block of every node.  The
 // elements containing node i are the contributions of its diagonal slot
 // (ascending element order); then the boundary faces at i (ascending face
-// order, AsBMFG after AsIGMR as in elmgmr.f90).  One thread per node.
+// order, AsBMFG after AsIGMR as in elmgmr.f90).  One thread per node.  For a
+// partially constrained node every element block gets bc3LHS (columns, rows,
+// 1 on the constrained diagonal), and the boundary elements at the node --
+// whose rigid-wall tangent is zero -- add 1 each to those entries, as the
+// reference's bc3LHS + fillsparseI pass over them does (elmgmr.f90:428-438).
 template <int kLhs>
 __global__ void __launch_bounds__(256) k_node_pass(const int* __restrict__ diag, const int* __restrict__ soff,
                                                    const int* __restrict__ slist, const double* __restrict__ erec,
                                                    const int* __restrict__ fnoff, const int* __restrict__ flist,
                                                    const double* __restrict__ frec, int nshg,
+                                                   const int* __restrict__ iBC, const double* __restrict__ BC,
+                                                   int ndofBC, int npartial, const int* __restrict__ bcount,
                                                    double* __restrict__ res, double* __restrict__ lhsK,
                                                    double* __restrict__ lhsP, float* __restrict__ lhs32) {
     constexpr int RS = RecLayout<kLhs>::RS, RO = RecLayout<kLhs>::RO;
@@ -613,6 +708,9 @@ __global__ void __launch_bounds__(256) k_node_pass(const int* __restrict__ diag,
         const int d = diag[i];
         double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
         double acc[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        NodeBC nb{0, 0.0, 0.0, 0.0};
+        if (kLhs && npartial) nb = node_bc(iBC, BC, ndofBC, i);
+        const bool proj = kLhs && bc_partial(nb.m);
         const int p1 = soff[d + 1];
         for (int p = soff[d]; p < p1; ++p) {
             const int t = slist[p];
@@ -626,10 +724,20 @@ __global__ void __launch_bounds__(256) k_node_pass(const int* __restrict__ diag,
             if (kLhs) {
                 double o[13];
                 record_block<kLhs == 2 ? 2 : 1>(rec, a, a, o);
+                if (proj) {
+                    bc_colop(nb, o);
+                    bc_rowop(nb, o);
+                    bc_diag(nb, o, 1.0);
+                }
 #pragma unroll
                 for (int c = 0; c < 13; ++c) acc[c] += o[c];
             }
         }
+        if (proj && bcount)
+            for (int k = 0; k < bcount[i]; ++k)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    if ((nb.m >> c) & 1) acc[4 * c] += 1.0;
         if (fnoff) {
             const int f1 = fnoff[i + 1];
             for (int p = fnoff[i]; p < f1; ++p) {
@@ -651,6 +759,8 @@ __global__ void __launch_bounds__(256) k_node_pass(const int* __restrict__ diag,
 template <int kLhs>
 __global__ void __launch_bounds__(256) k_slot_pass(const int* __restrict__ soff, const int* __restrict__ slist,
                                                    const double* __restrict__ erec, long long nnz,
+                                                   const int4* __restrict__ ien, const int* __restrict__ iBC,
+                                                   const double* __restrict__ BC, int ndofBC, int npartial,
                                                    double* __restrict__ lhsK, double* __restrict__ lhsP,
                                                    float* __restrict__ lhs32) {
     constexpr int RS = RecLayout<kLhs>::RS;
@@ -659,12 +769,30 @@ __global__ void __launch_bounds__(256) k_slot_pass(const int* __restrict__ soff,
         const int p0 = soff[s], p1 = soff[s + 1];
         const int t0 = slist[p0];
         if (((t0 >> 2) & 3) == (t0 & 3)) continue;
+        // bc3LHS: row operation of the row node, column operation of the column node
+        NodeBC ni{0, 0.0, 0.0, 0.0}, nj{0, 0.0, 0.0, 0.0};
+        if (npartial) {
+            const int4 nn = ien[t0 >> 4];
+            const int na[4] = {nn.x, nn.y, nn.z, nn.w};
+            ni = node_bc(iBC, BC, ndofBC, na[(t0 >> 2) & 3]);
+            nj = node_bc(iBC, BC, ndofBC, na[t0 & 3]);
+        }
+        const bool proj = bc_partial(ni.m) || bc_partial(nj.m);
         double acc[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int p = p0; p < p1; ++p) {
             const int t = p == p0 ? t0 : slist[p];
             const int e = t >> 4, a = (t >> 2) & 3, b = t & 3;
             double o[13];
             record_block<kLhs>(erec + (size_t)RS * (size_t)e, a, b, o);
+            if (proj) {
+                if (a < b) {
+                    bc_rowop(ni, o);
+                    bc_colop(nj, o);
+                } else {
+                    bc_colop(nj, o);
+                    bc_rowop(ni, o);
+                }
+            }
 #pragma unroll
             for (int c = 0; c < 13; ++c) acc[c] += o[c];
         }
@@ -813,13 +941,30 @@ __global__ void k_pvsq_add(const int* __restrict__ onodes, const int* __restrict
     }
 }
 
-// bc3Res (bc3res.f90:30-124) for no or all three velocity components
-__global__ void k_bc3res(const int* __restrict__ iBC, int nshg, double* __restrict__ res) {
+// bc3Res (bc3res.f90:30-124): pressure, the velocity components a node's
+// iBC prescribes (one or two through the BC coefficients, or all three), and
+// the plane condition (bit 11)
+__global__ void k_bc3res(const int* __restrict__ iBC, const double* __restrict__ BC, int ndofBC, int nshg,
+                         double* __restrict__ res) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
-        int b = iBC[i];
+        const int bits = iBC[i];
         double* r = res + 4 * (size_t)i;
-        if ((b >> 2) & 1) r[3] = 0.0;
-        if (((b >> 3) & 7) == 7 || ((b >> 11) & 1)) {
+        if ((bits >> 2) & 1) r[3] = 0.0;
+        const int m = (bits >> 3) & 7;
+        if (m != 0) {
+            const double* bc = BC + (size_t)ndofBC * i;
+            const double b4 = bc[3], b5 = bc[4], b6 = bc[5];
+            switch (m) {
+                case 1: r[1] = r[1] - b4 * r[0]; r[2] = r[2] - b5 * r[0]; r[0] = 0.0; break;
+                case 2: r[0] = r[0] - b4 * r[1]; r[2] = r[2] - b5 * r[1]; r[1] = 0.0; break;
+                case 3: r[2] = r[2] - b4 * r[0] - b6 * r[1]; r[0] = 0.0; r[1] = 0.0; break;
+                case 4: r[0] = r[0] - b4 * r[2]; r[1] = r[1] - b5 * r[2]; r[2] = 0.0; break;
+                case 5: r[1] = r[1] - b4 * r[0] - b6 * r[2]; r[0] = 0.0; r[2] = 0.0; break;
+                case 6: r[0] = r[0] - b4 * r[1] - b6 * r[2]; r[1] = 0.0; r[2] = 0.0; break;
+                default: r[0] = 0.0; r[1] = 0.0; r[2] = 0.0; break;
+            }
+        }
+        if ((bits >> 11) & 1) {
             r[0] = 0.0;
             r[1] = 0.0;
             r[2] = 0.0;
@@ -867,17 +1012,21 @@ int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const d
     const int* fno = c->nface > 0 ? c->fnoff.p : nullptr;
     const int ng = grid_for(c->nshg, 256);
     const int gs = grid_for(c->nnz, 256);
+    const int nb = c->p.ndofBC, np = c->npartial;
+    const int* bcnt = c->nface > 0 ? c->bcount.p : nullptr;
     if (lhs == 2) {
         launch(k_node_pass<2>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p, c->frec.p,
-               c->nshg, d_res, nullptr, nullptr, d_lhs32);
-        launch(k_slot_pass<2>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, nullptr, nullptr, d_lhs32);
+               c->nshg, c->iBC.p, c->BC.p, nb, np, bcnt, d_res, nullptr, nullptr, d_lhs32);
+        launch(k_slot_pass<2>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, c->ien.p, c->iBC.p, c->BC.p,
+               nb, np, nullptr, nullptr, d_lhs32);
     } else if (lhs) {
         launch(k_node_pass<1>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p, c->frec.p,
-               c->nshg, d_res, d_lhsK, d_lhsP, nullptr);
-        launch(k_slot_pass<1>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, d_lhsK, d_lhsP, nullptr);
+               c->nshg, c->iBC.p, c->BC.p, nb, np, bcnt, d_res, d_lhsK, d_lhsP, nullptr);
+        launch(k_slot_pass<1>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, c->ien.p, c->iBC.p, c->BC.p,
+               nb, np, d_lhsK, d_lhsP, nullptr);
     } else {
         launch(k_node_pass<0>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p, c->frec.p,
-               c->nshg, d_res, nullptr, nullptr, nullptr);
+               c->nshg, c->iBC.p, c->BC.p, nb, np, bcnt, d_res, nullptr, nullptr, nullptr);
     }
     if (c->ncoupled > 0) {
         double* hc = c->coef_host.data();
@@ -891,7 +1040,7 @@ int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const d
         launch(k_pvsq_add, g2, 256, 0, s, c->onodes.p, c->d_onode_off.p, c->onabi.p, c->flowq.p, c->coefs.p,
                c->ncoupled, d_res);
     }
-    launch(k_bc3res, grid_for(c->nshg, 256), 256, 0, s, c->iBC.p, c->nshg, d_res);
+    launch(k_bc3res, grid_for(c->nshg, 256), 256, 0, s, c->iBC.p, c->BC.p, nb, c->nshg, d_res);
     CR_CUDA(cudaGetLastError());
     return CRIMSON_OK;
 }

@@ -87,14 +87,22 @@ __global__ void k_correct(double* __restrict__ y, double* __restrict__ ac, const
 __global__ void k_itrbc(const int* __restrict__ iBC, const double* __restrict__ BC, int ndofBC, int n,
                         double* __restrict__ y) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        // itrBC (itrbc.f90:33-101): prescribed velocity components (all
+        // three, or one or two through the BC coefficients) and pressure
         const int b = iBC[i];
         const double* bc = BC + (size_t)ndofBC * i;
-        if (((b >> 3) & 7) == 7) {
-            y[4 * (size_t)i + 0] = bc[2];
-            y[4 * (size_t)i + 1] = bc[3];
-            y[4 * (size_t)i + 2] = bc[4];
+        double* v = y + 4 * (size_t)i;
+        switch ((b >> 3) & 7) {
+            case 1: v[0] = bc[2] - bc[3] * v[1] - bc[4] * v[2]; break;
+            case 2: v[1] = bc[2] - bc[3] * v[0] - bc[4] * v[2]; break;
+            case 3: v[0] = bc[2] - bc[3] * v[2]; v[1] = bc[4] - bc[5] * v[2]; break;
+            case 4: v[2] = bc[2] - bc[3] * v[0] - bc[4] * v[1]; break;
+            case 5: v[0] = bc[2] - bc[3] * v[1]; v[2] = bc[4] - bc[5] * v[1]; break;
+            case 6: v[1] = bc[2] - bc[3] * v[0]; v[2] = bc[4] - bc[5] * v[0]; break;
+            case 7: v[0] = bc[2]; v[1] = bc[3]; v[2] = bc[4]; break;
+            default: break;
         }
-        if ((b >> 2) & 1) y[4 * (size_t)i + 3] = bc[0];
+        if ((b >> 2) & 1) v[3] = bc[0];
     }
 }
 __global__ void k_inflow(const int* __restrict__ nodes, const double* __restrict__ prof, int m, double scale,
@@ -262,14 +270,16 @@ int crimson_set_params(crimson_ctx* c, const crimson_params* p) {
 int crimson_set_bc(crimson_ctx* c, const int* iBC, const double* BC) {
     if (!c || !iBC || !BC) return CRIMSON_ERR_ARG;
     const int n = c->nshg, nb = c->p.ndofBC;
-    for (int i = 0; i < n; ++i) {
-        int v = (iBC[i] >> 3) & 7;
-        if (v != 0 && v != 7) {
-            // bc3LHS only acts on partially constrained nodes (bc3lhs.f90:48-49)
-            set_last_error("partially constrained velocity nodes (bc3LHS projection) are not supported");
-            return CRIMSON_ERR_UNSUPPORTED;
-        }
+    if (nb < 6) {
+        set_last_error("ndofBC must be at least 6 (BC(:,4:6) hold the velocity constraint coefficients)");
+        return CRIMSON_ERR_ARG;
     }
+    int np = 0;
+    for (int i = 0; i < n; ++i) {
+        const int v = (iBC[i] >> 3) & 7;
+        if (v != 0 && v != 7) ++np;   // bc3LHS / bc3Res project these (bc3lhs.f90:48-49)
+    }
+    c->npartial = np;
     std::vector<double> nm((size_t)n * nb);
     for (int i = 0; i < n; ++i)
         for (int k = 0; k < nb; ++k) nm[(size_t)nb * i + k] = BC[(size_t)k * n + i];
@@ -316,8 +326,19 @@ int crimson_set_boundary(crimson_ctx* c, int nface, const int* ienb, const int* 
     CR_CHECK(c->ienb.upload(hb.data(), hb.size(), c->stream));
     CR_CHECK(c->iBCB.upload(hbits.data(), hbits.size(), c->stream));
     CR_CHECK(c->BCB.upload(hbcb.data(), hbcb.size(), c->stream));
+    // boundary elements (all four nodes) at each node: bc3LHS puts 1 on the
+    // constrained diagonal entries of a partially constrained node once per
+    // boundary element containing it
+    std::vector<int> bcount((size_t)c->nshg, 0);
+    for (int f = 0; f < nface; ++f) {
+        bcount[hb[f].x] += 1;
+        bcount[hb[f].y] += 1;
+        bcount[hb[f].z] += 1;
+        bcount[hb[f].w] += 1;
+    }
     CR_CHECK(c->fnoff.upload(fnoff.data(), fnoff.size(), c->stream));
     CR_CHECK(c->flist.upload(flist.data(), flist.size(), c->stream));
+    CR_CHECK(c->bcount.upload(bcount.data(), bcount.size(), c->stream));
     CR_CUDA(cudaStreamSynchronize(c->stream));
     return CRIMSON_OK;
 }
@@ -647,6 +668,10 @@ int crimson_elmgmr_vjp(crimson_ctx* c, const double* d_y, const double* d_ac, co
     if (!c || !d_y || !d_ac || !d_lambda || !d_ybar || !d_acbar) return CRIMSON_ERR_ARG;
     if (c->ncoupled > 0 && (!coef1 || !coef2)) return CRIMSON_ERR_ARG;
     CR_CHECK(check_params(&c->p));
+    if (c->npartial > 0) {
+        set_last_error("crimson_elmgmr_vjp: partially constrained velocity nodes are not differentiated");
+        return CRIMSON_ERR_UNSUPPORTED;
+    }
     return elmgmr_vjp(c, d_y, d_ac, coef1, coef2, d_lambda, d_res, d_ybar, d_acbar, mubar, coef1bar, coef2bar);
 }
 

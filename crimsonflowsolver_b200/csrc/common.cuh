@@ -148,6 +148,7 @@ struct crimson_ctx {
     crimson::DBuf<int> iBC;         // (nshg)
     crimson::DBuf<double> BC;       // (ndofBC, nshg) node-major
     std::vector<int> h_iBC;
+    int npartial = 0;               // nodes with one or two prescribed velocity components
     std::vector<double> h_BC;       // reference layout (nshg, ndofBC)
 
     // boundary faces (AsBMFG)
@@ -158,6 +159,7 @@ struct crimson_ctx {
     crimson::DBuf<int> fnoff;       // (nshg+1) offsets into flist per node
     crimson::DBuf<int> flist;       // (3 nface) codes 3f + n of the faces at each node, ascending f
     crimson::DBuf<double> frec;     // (nface, 12) face residual records: rl(n, 0:3) of face node n
+    crimson::DBuf<int> bcount;      // (nshg) boundary elements (all 4 nodes) containing each node
 
     // coupled outlets
     int ncoupled = 0;

@@ -97,7 +97,10 @@ int crimson_ctx_create(crimson_ctx** ctx, const crimson_params* p, int nshg, int
                        const int* ien, const double* x);
 int crimson_ctx_destroy(crimson_ctx* ctx);
 int crimson_set_params(crimson_ctx* ctx, const crimson_params* p);
-/* iBC / BC as passed to ElmGMR (flowsolver/src/elmgmr.f90:1-8) */
+/* iBC / BC as passed to ElmGMR (flowsolver/src/elmgmr.f90:1-8).  Velocity
+ * constraints on none, one, two or all three components (ibits(iBC,3,3)):
+ * itrBC, bc3Res and bc3LHS (itrbc.f90:33-101, bc3res.f90:30-124,
+ * bc3lhs.f90:39-198) use BC(:,3:6) as the reference does; ndofBC >= 6. */
 int crimson_set_bc(crimson_ctx* ctx, const int* iBC, const double* BC);
 /* boundary element blocks mienb / miBCB / mBCB used by AsBMFG
  * (flowsolver/src/elmgmr.f90:325-460) */
@@ -256,7 +259,8 @@ int crimson_solflow_device_transposed(crimson_ctx* ctx, crimson_lhs* lhs, crimso
  *   *mubar = lambda . d res / d mu; coef1bar[k], coef2bar[k] likewise (host).
  * d_res (optional) receives res itself.  Unlike the assembled tangent (the
  * reference's approximate Jacobian), this differentiates tauM, tauC, tauBar,
- * uBar and the flux projection as well. */
+ * uBar and the flux projection as well.  Returns CRIMSON_ERR_UNSUPPORTED when
+ * some node has one or two prescribed velocity components. */
 int crimson_elmgmr_vjp(crimson_ctx* ctx, const double* d_y, const double* d_ac, const double* coef1,
                        const double* coef2, const double* d_lambda, double* d_res, double* d_ybar, double* d_acbar,
                        double* mubar, double* coef1bar, double* coef2bar);

@@ -659,6 +659,95 @@ extern "C" int orc_genadj(int nshg, int nelem, const int* ien, int* colm, int* r
 }
 
 // ===========================================================================
+// bc3LHS (flowsolver/src/bc3lhs.f90:39-198): for every element node with one
+// or two prescribed velocity components (ibits(iBC,3,3) in 1..6), project
+// the constraint out of the element tangent xK (xK[cc*16 + a*4 + b], cc the
+// row-major 3x3 component): the columns of blocks (i, inod), then the rows
+// of blocks (inod, i), then 1 on the constrained diagonal entries of block
+// (inod, inod).  BC column-major (nshg, ndofBC): BC(:,4..6) are k = 3..5.
+// The two-component case ibits = 6 keeps the reference's own row update
+// (row 3 from row 1 and entry 6, rows 1-2 zeroed) exactly as bc3lhs.f90
+// writes it.
+// ===========================================================================
+static void bc3lhs_elem(int nshg, const int* iBC, const double* BC, const int nd[4], double* xK) {
+    for (int inod = 0; inod < 4; ++inod) {
+        const int in = nd[inod];
+        const int m = (iBC[in] >> 3) & 7;
+        if (m == 0 || m == 7) continue;
+        const double b4 = BC[3 * (size_t)nshg + in], b5 = BC[4 * (size_t)nshg + in], b6 = BC[5 * (size_t)nshg + in];
+        auto K = [&](int cc, int a, int b) -> double& { return xK[cc * 16 + a * 4 + b]; };
+        if (m == 1 || m == 2 || m == 4) {
+            const int c0 = m == 1 ? 0 : (m == 2 ? 1 : 2);
+            const int f1 = m == 1 ? 1 : 0, f2 = m == 4 ? 1 : 2;
+            for (int i = 0; i < 4; ++i)
+                for (int r = 0; r < 3; ++r) K(3 * r + f1, i, inod) = K(3 * r + f1, i, inod) - b4 * K(3 * r + c0, i, inod);
+            for (int i = 0; i < 4; ++i)
+                for (int r = 0; r < 3; ++r) K(3 * r + f2, i, inod) = K(3 * r + f2, i, inod) - b5 * K(3 * r + c0, i, inod);
+            for (int i = 0; i < 4; ++i)
+                for (int r = 0; r < 3; ++r) K(3 * r + c0, i, inod) = 0.0;
+            for (int i = 0; i < 4; ++i)
+                for (int q = 0; q < 3; ++q) K(3 * f1 + q, inod, i) = K(3 * f1 + q, inod, i) - b4 * K(3 * c0 + q, inod, i);
+            for (int i = 0; i < 4; ++i)
+                for (int q = 0; q < 3; ++q) K(3 * f2 + q, inod, i) = K(3 * f2 + q, inod, i) - b5 * K(3 * c0 + q, inod, i);
+            for (int i = 0; i < 4; ++i)
+                for (int q = 0; q < 3; ++q) K(3 * c0 + q, inod, i) = 0.0;
+            K(4 * c0, inod, inod) = 1.0;
+        } else {
+            const int f = m == 3 ? 2 : (m == 5 ? 1 : 0);
+            const int c0 = m == 6 ? 1 : 0, c1 = m == 3 ? 1 : 2;
+            for (int i = 0; i < 4; ++i)
+                for (int r = 0; r < 3; ++r)
+                    K(3 * r + f, i, inod) = K(3 * r + f, i, inod) - b4 * K(3 * r + c0, i, inod) - b6 * K(3 * r + c1, i, inod);
+            for (int i = 0; i < 4; ++i)
+                for (int r = 0; r < 3; ++r) {
+                    K(3 * r + c0, i, inod) = 0.0;
+                    K(3 * r + c1, i, inod) = 0.0;
+                }
+            if (m != 6) {
+                for (int i = 0; i < 4; ++i)
+                    for (int q = 0; q < 3; ++q)
+                        K(3 * f + q, inod, i) = K(3 * f + q, inod, i) - b4 * K(3 * c0 + q, inod, i) - b6 * K(3 * c1 + q, inod, i);
+                for (int i = 0; i < 4; ++i)
+                    for (int q = 0; q < 3; ++q) {
+                        K(3 * c0 + q, inod, i) = 0.0;
+                        K(3 * c1 + q, inod, i) = 0.0;
+                    }
+            } else {
+                // bc3lhs.f90:643-672: row 3 updated from row 1 (and entry 6), rows 1-2 zeroed
+                for (int i = 0; i < 4; ++i) {
+                    K(6, inod, i) = K(6, inod, i) - b4 * K(0, inod, i);
+                    K(7, inod, i) = K(7, inod, i) - b4 * K(1, inod, i);
+                    K(8, inod, i) = K(8, inod, i) - b4 * K(2, inod, i) - b6 * K(5, inod, i);
+                }
+                for (int i = 0; i < 4; ++i)
+                    for (int q = 0; q < 6; ++q) K(q, inod, i) = 0.0;
+            }
+            K(4 * c0, inod, inod) = 1.0;
+            K(4 * c1, inod, inod) = 1.0;
+        }
+    }
+}
+
+// bc3Res velocity branches (bc3res.f90:53-103) for node i, res column-major
+static void bc3res_partial(int nshg, const int* iBC, const double* BC, int i, double* res) {
+    const int m = (iBC[i] >> 3) & 7;
+    double* r0 = res + i;
+    double* r1 = res + (size_t)nshg + i;
+    double* r2 = res + 2 * (size_t)nshg + i;
+    const double b4 = BC[3 * (size_t)nshg + i], b5 = BC[4 * (size_t)nshg + i], b6 = BC[5 * (size_t)nshg + i];
+    switch (m) {
+        case 1: *r1 = *r1 - b4 * *r0; *r2 = *r2 - b5 * *r0; *r0 = 0.0; break;
+        case 2: *r0 = *r0 - b4 * *r1; *r2 = *r2 - b5 * *r1; *r1 = 0.0; break;
+        case 3: *r2 = *r2 - b4 * *r0 - b6 * *r1; *r0 = 0.0; *r1 = 0.0; break;
+        case 4: *r0 = *r0 - b4 * *r2; *r1 = *r1 - b5 * *r2; *r2 = 0.0; break;
+        case 5: *r1 = *r1 - b4 * *r0 - b6 * *r2; *r0 = 0.0; *r2 = 0.0; break;
+        case 6: *r0 = *r0 - b4 * *r1 - b6 * *r2; *r1 = 0.0; *r2 = 0.0; break;
+        case 7: *r0 = 0.0; *r1 = 0.0; *r2 = 0.0; break;
+        default: break;
+    }
+}
+
+// ===========================================================================
 // ElmGMR (flowsolver/src/elmgmr.f90:82-555)
 // ===========================================================================
 extern "C" int orc_elmgmr(const orc_params* p, int nshg, int numnp, int nelem, const int* ien, const double* x,
@@ -673,12 +762,6 @@ extern "C" int orc_elmgmr(const orc_params* p, int nshg, int numnp, int nelem, c
     if (p->itau != 0 || p->flmpl != 0.0 || p->flmpr != 0.0 || (p->iconvflow != 1 && p->iconvflow != 2) ||
         (p->idiff != 0 && p->idiff != 1))
         return ORC_ERR_UNSUPPORTED;
-    // bc3LHS acts only on partially constrained (1-2 component) velocity nodes
-    // (bc3lhs.f90:48-49); this path supports none or all three components.
-    for (int i = 0; i < nshg; ++i) {
-        int v = (iBC[i] >> 3) & 7;
-        if (v != 0 && v != 7) return ORC_ERR_UNSUPPORTED;
-    }
     const int ibksiz = p->ibksiz > 0 ? p->ibksiz : 255;
     const int nthr = nthreads_of(p);
     // ---- diffusive-flux reconstruction: AsIq + qpbc (elmgmr.f90:82-118) ----
@@ -791,10 +874,12 @@ extern "C" int orc_elmgmr(const orc_params* p, int nshg, int numnp, int nelem, c
                             res[(size_t)j * nshg + nd] = res[(size_t)j * nshg + nd] + O(e)[a * 4 + j];
                         }
                 if (!lhs) continue;
-                // fillsparseI (fillsparse.f90:29-60)
+                // bc3LHS (elmgmr.f90:224-225), then fillsparseI (fillsparse.f90:29-60)
                 for (int e = e0; e < e1; ++e) {
-                    const double* xK = O(e) + 16;
+                    double* xK = O(e) + 16;
                     const double* xG = O(e) + 16 + 144;
+                    const int ndl[4] = {ien[e] - 1, ien[nelem + e] - 1, ien[2 * nelem + e] - 1, ien[3 * nelem + e] - 1};
+                    bc3lhs_elem(nshg, iBC, BC, ndl, xK);
                     for (int aa = 0; aa < 4; ++aa) {
                         int i = ien[aa * nelem + e];
                         int c = colm[i - 1];
@@ -839,6 +924,27 @@ extern "C" int orc_elmgmr(const orc_params* p, int nshg, int numnp, int nelem, c
                         int nd = ienb[a * nface + f] - 1;
                         res[(size_t)j * nshg + nd] = res[(size_t)j * nshg + nd] + rlb[(size_t)(f - f0) * 16 + a * 4 + j];
                     }
+            // rigid wall: zero boundary tangent; bc3LHS still puts 1 on the
+            // constrained diagonal entries of partially constrained nodes
+            // before fillsparseI (elmgmr.f90:428-438)
+            if (lhs) {
+                for (int f = f0; f < f1; ++f) {
+                    double xK[144] = {0.0};
+                    int ndl[4];
+                    for (int a = 0; a < 4; ++a) ndl[a] = ienb[a * nface + f] - 1;
+                    bc3lhs_elem(nshg, iBC, BC, ndl, xK);
+                    for (int aa = 0; aa < 4; ++aa) {
+                        int i = ndl[aa] + 1;
+                        int c = colm[i - 1];
+                        int n = colm[i] - c;
+                        for (int bb = 0; bb < 4; ++bb) {
+                            long long k = sparseloc(&rowp[c - 1], n, ndl[bb] + 1) + c - 1;
+                            double* K = &lhsK[9 * (k - 1)];
+                            for (int cc = 0; cc < 9; ++cc) K[cc] = K[cc] + xK[cc * 16 + aa * 4 + bb];
+                        }
+                    }
+                }
+            }
         }
     }
     // ---- ElmpvsQ, GRCR branch (elmgmr.f90:1271-1330) with sign = -1 ----
@@ -859,18 +965,13 @@ extern "C" int orc_elmgmr(const orc_params* p, int nshg, int numnp, int nelem, c
     // ---- bc3Res (bc3res.f90:30-124) ----
     for (int i = 0; i < nshg; ++i) {
         if ((iBC[i] >> 2) & 1) res[3 * (size_t)nshg + i] = 0.0;
-        if (((iBC[i] >> 3) & 7) == 7) {
-            res[0 * (size_t)nshg + i] = 0.0;
-            res[1 * (size_t)nshg + i] = 0.0;
-            res[2 * (size_t)nshg + i] = 0.0;
-        }
+        bc3res_partial(nshg, iBC, BC, i, res);
         if ((iBC[i] >> 11) & 1) {
             res[0 * (size_t)nshg + i] = 0.0;
             res[1 * (size_t)nshg + i] = 0.0;
             res[2 * (size_t)nshg + i] = 0.0;
         }
     }
-    (void)BC;
     return ORC_OK;
 }
 
@@ -1646,14 +1747,24 @@ extern "C" void orc_itr_correct(int nshg, double gami, double alfi, double Delt,
 }
 
 extern "C" void orc_itr_bc(int nshg, const int* iBC, const double* BC, double* y) {
-    // itrBC, all-three-components and pressure branches (itrbc.f90:83-101)
+    // itrBC velocity and pressure branches (itrbc.f90:33-101)
     for (int i = 0; i < nshg; ++i) {
-        if (((iBC[i] >> 3) & 7) == 7) {
-            y[0 * (size_t)nshg + i] = BC[2 * (size_t)nshg + i];
-            y[1 * (size_t)nshg + i] = BC[3 * (size_t)nshg + i];
-            y[2 * (size_t)nshg + i] = BC[4 * (size_t)nshg + i];
+        const double* B = BC + i;
+        auto bc = [&](int k) { return B[(size_t)k * nshg]; };   // BC(:, k+1)
+        double* y1 = y + i;
+        double* y2 = y + (size_t)nshg + i;
+        double* y3 = y + 2 * (size_t)nshg + i;
+        switch ((iBC[i] >> 3) & 7) {
+            case 1: *y1 = bc(2) - bc(3) * *y2 - bc(4) * *y3; break;
+            case 2: *y2 = bc(2) - bc(3) * *y1 - bc(4) * *y3; break;
+            case 3: *y1 = bc(2) - bc(3) * *y3; *y2 = bc(4) - bc(5) * *y3; break;
+            case 4: *y3 = bc(2) - bc(3) * *y1 - bc(4) * *y2; break;
+            case 5: *y1 = bc(2) - bc(3) * *y2; *y3 = bc(4) - bc(5) * *y2; break;
+            case 6: *y2 = bc(2) - bc(3) * *y1; *y3 = bc(4) - bc(5) * *y1; break;
+            case 7: *y1 = bc(2); *y2 = bc(3); *y3 = bc(4); break;
+            default: break;
         }
-        if ((iBC[i] >> 2) & 1) y[3 * (size_t)nshg + i] = BC[0 * (size_t)nshg + i];
+        if ((iBC[i] >> 2) & 1) y[3 * (size_t)nshg + i] = bc(0);
     }
 }
 

@@ -86,6 +86,7 @@ def lib():
                                       _c_dbl_p, ctypes.POINTER(OrcLsStats)]
         L.orc_memls_set_threads.argtypes = [ctypes.c_int]
         L.orc_rcr_coeffs.argtypes = [ctypes.c_double] * 8 + [_c_dbl_p, _c_dbl_p]
+        L.orc_itr_bc.argtypes = [ctypes.c_int, _c_int_p, _c_dbl_p, _c_dbl_p]
         _lib = L
     return _lib
 
@@ -244,6 +245,18 @@ class MemLS:
             pass
 
 
+def itr_bc(mesh, y):
+    """itrBC (flowsolver/src/itrbc.f90:33-101) in place on y (nshg, 4): the
+    velocity components a node's iBC prescribes (all three, or one or two
+    through the BC coefficients) and the prescribed pressure."""
+    n = mesh.nshg
+    yF = np.asfortranarray(y)
+    iBC = np.ascontiguousarray(mesh.iBC.astype(np.int32))
+    BCF = np.asfortranarray(mesh.BC)
+    lib().orc_itr_bc(n, _ip(iBC), _dp(BCF), _dp(yF))
+    y[:] = yF
+
+
 def dirichlet_face(mesh):
     """Face 1: nodes with any prescribed velocity, val = 1 on free comps (itrdrv.f90:949-992)."""
     iBC = mesh.iBC
@@ -292,12 +305,8 @@ class OracleFlow:
         self._itr_bc(self.yold)
 
     def _itr_bc(self, y):
-        iBC = self.m.iBC
-        BC = self.m.BC
-        full = ((iBC >> 3) & 7) == 7
-        y[full, 0:3] = BC[full, 2:5]
-        pr = ((iBC >> 2) & 1) == 1
-        y[pr, 3] = BC[pr, 0]
+        """itrBC (itrbc.f90:33-101) in place on y (nshg, 4)."""
+        itr_bc(self.m, y)
 
     def implicit_coeffs(self, n, alpha_form=True):
         P = self.P

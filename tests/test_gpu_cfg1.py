@@ -1,7 +1,10 @@
 """Parity on the plain-method configuration as built: the 24x24 x 40 jittered
 cylinder (107,520 tets, 20,377 nodes), steady parabolic inflow of mean
 10 cm/s, zero-traction outlet, no-slip wall, rho 1.06, mu 0.04, dt 1e-3,
-10 time steps of 3 nonlinear iterations, FP64, NSSOLVER tolerance 1e-6.
+10 time steps of 3 nonlinear iterations, FP64, NSSOLVER tolerance 1e-5 (the
+tightest setting the reference's outer residual estimate decides
+independently of rounding: at 1e-6 the oracle's own first solve takes 8
+outer iterations with 8 threads and 10 with 1).
 
 * FP64 GPU vs the FP64 oracle: identical outer / GMRES / CG iteration counts
   in every one of the 30 solves, velocity and pressure within 1e-10
@@ -24,7 +27,7 @@ NSTEPS = 10
 
 
 def _params(**kw):
-    return FlowParams(epstol_ns=1e-6, **kw)
+    return FlowParams(epstol_ns=1e-5, **kw)
 
 
 @pytest.fixture(scope="module")

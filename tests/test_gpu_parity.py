@@ -251,3 +251,56 @@ def test_multi_outlet_time_steps_parity():
     assert relerr(y[:, 3], F.y[:, 3]) < 1e-10, relerr(y[:, 3], F.y[:, 3])
     for k in range(3):
         assert abs(st.p_out[k] - F.Pn[k]) <= 1e-10 * abs(F.Pn[k])
+
+
+def test_elmgmr_partial_constraints_parity():
+    """Wall nodes with one or two prescribed velocity components (ibits 1-6,
+    random BC(:,4:6) coefficients): bc3LHS on every element block, the
+    boundary elements' unit diagonal entries, and bc3Res -- res, lhsK, lhsP
+    within 1e-12 of the oracle."""
+    from tests.partial_bc import with_partial_constraints
+
+    m = mesh.cylinder(ncross=8, naxial=10)
+    m.set_inflow(10.0)
+    with_partial_constraints(m)
+    P = FlowParams(rcr=[RCR(srfid=3)])
+    elm = solver.ElmGMR(m, P)
+    try:
+        colm, rowp = elm.genadj()
+        rng = np.random.default_rng(21)
+        y = rng.standard_normal((m.nshg, 4))
+        ac = rng.standard_normal((m.nshg, 4))
+        g = elm(y, ac, [80.0], [-4.0])
+        o = po.Elm(m, P, colm, rowp)(y, ac, srflist=[3], coef1=[80.0], coef2=[-4.0])
+    finally:
+        elm.close()
+    for k in ("res", "lhsK", "lhsP"):
+        assert relerr(g[k], o[k]) < 1e-12, (k, relerr(g[k], o[k]))
+
+
+def test_time_steps_partial_constraints_parity():
+    """Two time steps with slip-type constraints (ibits 1-5) on half of the
+    wall nodes: itrBC, bc3Res and bc3LHS in the step against the oracle."""
+    from tests.partial_bc import with_partial_constraints
+
+    inflow = lambda t: 10.0 + 5.0 * np.sin(2 * np.pi * t / 0.8)
+    P = FlowParams(rcr=[RCR(srfid=3)])
+    meshes = []
+    for _ in range(2):
+        m = mesh.cylinder(ncross=8, naxial=10)
+        with_partial_constraints(m, masks=(1, 2, 3, 4, 5))
+        meshes.append(m)
+    F = po.OracleFlow(meshes[0], P, inflow=inflow)
+    G = solver.FlowSolver(meshes[1], P, inflow=inflow)
+    try:
+        its = []
+        for _ in range(2):
+            F.step()
+            st = G.step()
+            its += [(st.ri_itr[i], st.gm_itr[i], st.cg_itr[i]) for i in range(st.nsolves)]
+        y, ac = G.state()
+    finally:
+        G.close()
+    assert its == [s[:3] for s in F.stats]
+    assert relerr(y[:, 0:3], F.y[:, 0:3]) < 1e-10, relerr(y[:, 0:3], F.y[:, 0:3])
+    assert relerr(y[:, 3], F.y[:, 3]) < 1e-10, relerr(y[:, 3], F.y[:, 3])
