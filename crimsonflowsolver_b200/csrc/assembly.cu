@@ -694,7 +694,7 @@ __device__ __forceinline__ void bc_diag(const NodeBC& n, double K[9], double v) 
 // 1 on the constrained diagonal), and the boundary elements at the node --
 // whose rigid-wall tangent is zero -- add 1 each to those entries, as the
 // reference's bc3LHS + fillsparseI pass over them does (elmgmr.f90:428-438).
-template <int kLhs>
+template <int kLhs, bool kProj>
 __global__ void __launch_bounds__(256) k_node_pass(const int* __restrict__ diag, const int* __restrict__ soff,
                                                    const int* __restrict__ slist, const double* __restrict__ erec,
                                                    const int* __restrict__ fnoff, const int* __restrict__ flist,
@@ -709,8 +709,8 @@ __global__ void __launch_bounds__(256) k_node_pass(const int* __restrict__ diag,
         double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
         double acc[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         NodeBC nb{0, 0.0, 0.0, 0.0};
-        if (kLhs && npartial) nb = node_bc(iBC, BC, ndofBC, i);
-        const bool proj = kLhs && bc_partial(nb.m);
+        if (kLhs && kProj) nb = node_bc(iBC, BC, ndofBC, i);
+        const bool proj = kLhs && kProj && bc_partial(nb.m);
         const int p1 = soff[d + 1];
         for (int p = soff[d]; p < p1; ++p) {
             const int t = slist[p];
@@ -756,7 +756,7 @@ __global__ void __launch_bounds__(256) k_node_pass(const int* __restrict__ diag,
 // Slot pass: every off-diagonal CSR block (i, j) from the elements that
 // contain the edge (ascending element order).  One thread per slot; the
 // diagonal slots (first contribution with a == b) belong to the node pass.
-template <int kLhs>
+template <int kLhs, bool kProj>
 __global__ void __launch_bounds__(256) k_slot_pass(const int* __restrict__ soff, const int* __restrict__ slist,
                                                    const double* __restrict__ erec, long long nnz,
                                                    const int4* __restrict__ ien, const int* __restrict__ iBC,
@@ -771,13 +771,13 @@ __global__ void __launch_bounds__(256) k_slot_pass(const int* __restrict__ soff,
         if (((t0 >> 2) & 3) == (t0 & 3)) continue;
         // bc3LHS: row operation of the row node, column operation of the column node
         NodeBC ni{0, 0.0, 0.0, 0.0}, nj{0, 0.0, 0.0, 0.0};
-        if (npartial) {
+        if (kProj) {
             const int4 nn = ien[t0 >> 4];
             const int na[4] = {nn.x, nn.y, nn.z, nn.w};
             ni = node_bc(iBC, BC, ndofBC, na[(t0 >> 2) & 3]);
             nj = node_bc(iBC, BC, ndofBC, na[t0 & 3]);
         }
-        const bool proj = bc_partial(ni.m) || bc_partial(nj.m);
+        const bool proj = kProj && (bc_partial(ni.m) || bc_partial(nj.m));
         double acc[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int p = p0; p < p1; ++p) {
             const int t = p == p0 ? t0 : slist[p];
@@ -972,6 +972,17 @@ __global__ void k_bc3res(const int* __restrict__ iBC, const double* __restrict__
     }
 }
 
+// Grid caps (blocks of 256 per SM) of the owner passes: a grid-stride loop
+// over rows / slots in order, so the cap sets how many rows are in flight.
+#ifndef CRIMSON_NODE_PASS_BLOCKS_PER_SM
+#define CRIMSON_NODE_PASS_BLOCKS_PER_SM 2
+#endif
+#ifndef CRIMSON_SLOT_PASS_BLOCKS_PER_SM
+#define CRIMSON_SLOT_PASS_BLOCKS_PER_SM 32
+#endif
+constexpr int kNodePassBlocksPerSM = CRIMSON_NODE_PASS_BLOCKS_PER_SM;
+constexpr int kSlotPassBlocksPerSM = CRIMSON_SLOT_PASS_BLOCKS_PER_SM;
+
 int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1, const double* coef2,
                   double* d_res, double* d_lhsK, double* d_lhsP, int lhs, float* d_lhs32) {
     cudaStream_t s = c->stream;
@@ -1010,23 +1021,41 @@ int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const d
                c->frec.p);
     }
     const int* fno = c->nface > 0 ? c->fnoff.p : nullptr;
-    const int ng = grid_for(c->nshg, 256);
-    const int gs = grid_for(c->nnz, 256);
+    const int ng = grid_for(c->nshg, 256, kNodePassBlocksPerSM);
+    const int gs = grid_for(c->nnz, 256, kSlotPassBlocksPerSM);
+    // the bc3LHS projection is compiled into separate pass variants, used only
+    // when some node has one or two prescribed velocity components
     const int nb = c->p.ndofBC, np = c->npartial;
     const int* bcnt = c->nface > 0 ? c->bcount.p : nullptr;
     if (lhs == 2) {
-        launch(k_node_pass<2>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p, c->frec.p,
-               c->nshg, c->iBC.p, c->BC.p, nb, np, bcnt, d_res, nullptr, nullptr, d_lhs32);
-        launch(k_slot_pass<2>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, c->ien.p, c->iBC.p, c->BC.p,
-               nb, np, nullptr, nullptr, d_lhs32);
+        if (np)
+            launch(k_node_pass<2, true>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p,
+                   c->frec.p, c->nshg, c->iBC.p, c->BC.p, nb, np, bcnt, d_res, nullptr, nullptr, d_lhs32);
+        else
+            launch(k_node_pass<2, false>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p,
+                   c->frec.p, c->nshg, c->iBC.p, c->BC.p, nb, np, bcnt, d_res, nullptr, nullptr, d_lhs32);
+        if (np)
+            launch(k_slot_pass<2, true>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, c->ien.p, c->iBC.p,
+                   c->BC.p, nb, np, nullptr, nullptr, d_lhs32);
+        else
+            launch(k_slot_pass<2, false>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, c->ien.p, c->iBC.p,
+                   c->BC.p, nb, np, nullptr, nullptr, d_lhs32);
     } else if (lhs) {
-        launch(k_node_pass<1>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p, c->frec.p,
-               c->nshg, c->iBC.p, c->BC.p, nb, np, bcnt, d_res, d_lhsK, d_lhsP, nullptr);
-        launch(k_slot_pass<1>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, c->ien.p, c->iBC.p, c->BC.p,
-               nb, np, d_lhsK, d_lhsP, nullptr);
+        if (np)
+            launch(k_node_pass<1, true>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p,
+                   c->frec.p, c->nshg, c->iBC.p, c->BC.p, nb, np, bcnt, d_res, d_lhsK, d_lhsP, nullptr);
+        else
+            launch(k_node_pass<1, false>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p,
+                   c->frec.p, c->nshg, c->iBC.p, c->BC.p, nb, np, bcnt, d_res, d_lhsK, d_lhsP, nullptr);
+        if (np)
+            launch(k_slot_pass<1, true>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, c->ien.p, c->iBC.p,
+                   c->BC.p, nb, np, d_lhsK, d_lhsP, nullptr);
+        else
+            launch(k_slot_pass<1, false>, gs, 256, 0, s, c->soff.p, c->slist.p, c->erec.p, c->nnz, c->ien.p, c->iBC.p,
+                   c->BC.p, nb, np, d_lhsK, d_lhsP, nullptr);
     } else {
-        launch(k_node_pass<0>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p, c->frec.p,
-               c->nshg, c->iBC.p, c->BC.p, nb, np, bcnt, d_res, nullptr, nullptr, nullptr);
+        launch(k_node_pass<0, false>, ng, 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->erec.p, fno, c->flist.p,
+               c->frec.p, c->nshg, c->iBC.p, c->BC.p, nb, np, bcnt, d_res, nullptr, nullptr, nullptr);
     }
     if (c->ncoupled > 0) {
         double* hc = c->coef_host.data();
