@@ -4,13 +4,13 @@ The CUDA library is built in-tree with :func:`build`; every compute entry point
 runs on the GPU through the C ABI in include/crimson_b200.h.
 """
 from ._native import build, lib  # noqa: F401
-from .problem import RCR, FlowParams, time_params  # noqa: F401
+from .problem import RCR, FlowParams, NetlistBC, time_params  # noqa: F401
 
-__all__ = ["build", "lib", "FlowParams", "RCR", "time_params", "mesh", "solver"]
+__all__ = ["build", "lib", "FlowParams", "RCR", "NetlistBC", "time_params", "mesh", "solver", "netlist"]
 
 
 def __getattr__(name):
-    if name in ("mesh", "solver", "problem"):
+    if name in ("mesh", "solver", "problem", "netlist"):
         import importlib
 
         return importlib.import_module(f".{name}", __name__)

@@ -82,6 +82,8 @@ class AdjointProblem:
                  adj_tol: float = 1e-10, adj_maxit: int = 40):
         if not P.rcr:
             raise ValueError("the objective needs at least one RCR outlet")
+        if P.netlists:
+            raise ValueError("netlist outlets are not differentiated (RCR outlets only)")
         self.mesh = mesh
         self.P0 = P
         self.targets = np.asarray(targets, dtype=np.float64)

@@ -8,6 +8,7 @@
 
 #include "common.cuh"
 #include "memls.cuh"
+#include "netlist.h"
 
 namespace crimson {
 
@@ -369,6 +370,7 @@ int crimson_set_outlets(crimson_ctx* c, int ncoupled, const int* srflist, const 
     CR_CUDA(cudaStreamSynchronize(c->stream));
     c->rcr_Pn.assign(ncoupled, 0.0);
     c->rcr_Qn.assign(ncoupled, 0.0);
+    c->netlists.assign((size_t)ncoupled, nullptr);
     return CRIMSON_OK;
 }
 
@@ -703,6 +705,13 @@ int crimson_set_rcr(crimson_ctx* c, int n, const double* Rp, const double* C, co
     return CRIMSON_OK;
 }
 
+int crimson_set_outlet_netlist(crimson_ctx* c, int k, crimson_netlist* nl) {
+    if (!c || k < 0 || k >= c->ncoupled) return CRIMSON_ERR_ARG;
+    c->netlists.resize((size_t)c->ncoupled, nullptr);
+    c->netlists[(size_t)k] = nl;
+    return CRIMSON_OK;
+}
+
 int crimson_rcr_state(crimson_ctx* c, int n, double* Pn, double* Qn, int set) {
     if (!c || n != c->ncoupled || (n > 0 && (!Pn || !Qn))) return CRIMSON_ERR_ARG;
     if ((int)c->rcr_Pn.size() != n) return CRIMSON_ERR_STATE;
@@ -770,10 +779,24 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
     launch(k_predict, grid_for(4LL * n, 256), 256, 0, s, c->yold.p, c->acold.p, c->ycur.p, c->accur.p, 4LL * n, fct);
     launch(k_itrbc, grid_for(n, 256), 256, 0, s, c->iBC.p, c->BC.p, nb, n, c->ycur.p);
     const int nc = c->ncoupled;
+    c->netlists.resize((size_t)nc, nullptr);
     std::vector<double> c1(nc), c2(nc), faceRes(1 + nc, 0.0);
     for (int k = 0; k < nc; ++k)
-        rcr_coeffs(c->rcr_Rp[k], c->rcr_C[k], c->rcr_Rd[k], c->rcr_Pd[k], c->rcr_Pd[k], c->rcr_Pn[k], c->rcr_Qn[k],
-                   P.alfi * P.Delt, &c1[k], &c2[k]);
+        if (!c->netlists[(size_t)k] && (int)c->rcr_Rp.size() != nc) {
+            set_last_error("crimson_step: coupled surface without an RCR (crimson_set_rcr) or a netlist");
+            return CRIMSON_ERR_STATE;
+        }
+    for (int k = 0; k < nc; ++k) {
+        if (crimson_netlist* nl = c->netlists[(size_t)k]) {
+            // initialiseAtStartOfTimestep, then the implicit coefficients with
+            // alfi*Delt (AbstractBoundaryCondition.cxx:32-53)
+            CR_CHECK(netlist_begin_step(nl));
+            CR_CHECK(crimson_netlist_implicit_coefficients(nl, P.alfi * P.Delt, &c1[k], &c2[k]));
+        } else {
+            rcr_coeffs(c->rcr_Rp[k], c->rcr_C[k], c->rcr_Rd[k], c->rcr_Pd[k], c->rcr_Pd[k], c->rcr_Pn[k],
+                       c->rcr_Qn[k], P.alfi * P.Delt, &c1[k], &c2[k]);
+        }
+    }
     for (int k = 0; k < nc; ++k) faceRes[1 + k] = c1[k] * P.alfi * P.gami * P.Delt;
     std::vector<int> incL(1 + nc, 1);
     if (st) std::memset(st, 0, sizeof(*st));
@@ -817,6 +840,19 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
         CR_CUDA(cudaMemcpyAsync(hq.data(), c->flowq.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
         for (int k = 0; k < nc; ++k) {
+            if (crimson_netlist* nl = c->netlists[(size_t)k]) {
+                // updateLPN with the end-of-step flow, then finalizeLPNAtEndOfTimestep
+                // (itrdrv.f90:1686-1688)
+                CR_CHECK(crimson_netlist_update(nl, P.Delt, hq[k]));
+                CR_CHECK(crimson_netlist_finalize_step(nl));
+                c->rcr_Pn[k] = nl->node[(size_t)nl->iface_node - 1].p;
+                c->rcr_Qn[k] = hq[k];
+                if (st && k < 8) {
+                    st->q_out[k] = hq[k];
+                    st->p_out[k] = c->rcr_Pn[k];
+                }
+                continue;
+            }
             double d1, h1;
             rcr_coeffs(c->rcr_Rp[k], c->rcr_C[k], c->rcr_Rd[k], c->rcr_Pd[k], c->rcr_Pd[k], c->rcr_Pn[k], c->rcr_Qn[k],
                        P.Delt, &d1, &h1);

@@ -211,5 +211,6 @@ struct crimson_ctx {
     crimson::DBuf<double> inlet_profile;   // (ninlet, 3)
     int ninlet = 0;
     std::vector<double> rcr_Rp, rcr_C, rcr_Rd, rcr_Pd, rcr_Pn, rcr_Qn;
+    std::vector<crimson_netlist*> netlists;  // per coupled surface; null: the RCR (not owned)
     int istep = 0;
 };

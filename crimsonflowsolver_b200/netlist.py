@@ -1,0 +1,88 @@
+"""Netlist outlet circuits on the library's C ABI (crimson_netlist_*).
+
+:class:`Netlist` owns one circuit handle built from a :class:`NetlistBC`
+description; the calls mirror NetlistCircuit (flowsolver/src/
+NetlistCircuit.cxx): implicit coefficients at the start of a step, update
+with the end-of-step interface flow, finalisation (histories and diode
+switching).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+from .problem import NetlistBC
+
+KINDS = {"r": 0, "c": 1, "l": 2, "d": 3}
+
+
+class Netlist:
+    def __init__(self, spec: NetlistBC):
+        self.spec = spec
+        comps = spec.components
+        nn = spec.nnodes
+        kind = np.array([KINDS[c[0]] for c in comps], dtype=np.int32)
+        st = np.array([c[1] for c in comps], dtype=np.int32)
+        en = np.array([c[2] for c in comps], dtype=np.int32)
+        val = np.array([c[3] for c in comps], dtype=np.float64)
+        p0 = np.array([spec.initial_pressures.get(i + 1, 0.0) for i in range(nn)], dtype=np.float64)
+        pn = np.array(sorted(spec.prescribed_pressures), dtype=np.int32)
+        pv = np.array([spec.prescribed_pressures[k] for k in pn], dtype=np.float64)
+        fc = [spec.interface_component] + sorted(spec.prescribed_flows)
+        fk = [1] + [0] * len(spec.prescribed_flows)
+        fv = [0.0] + [spec.prescribed_flows[k] for k in sorted(spec.prescribed_flows)]
+        fc, fk, fv = (np.array(fc, dtype=np.int32), np.array(fk, dtype=np.int32), np.array(fv, dtype=np.float64))
+        self.ncomp, self.nnodes = len(comps), nn
+        h = ctypes.c_void_p()
+        N.check(N.lib().crimson_netlist_create(ctypes.byref(h), len(comps), N.ip(kind), N.ip(st), N.ip(en), N.dp(val),
+                                               nn, N.dp(p0), len(pn), N.ip(pn), N.dp(pv), len(fc), N.ip(fc),
+                                               N.ip(fk), N.dp(fv), 1), "crimson_netlist_create")
+        self.h = h
+
+    def flow_permitted(self) -> bool:
+        v = ctypes.c_int()
+        N.check(N.lib().crimson_netlist_flow_permitted(self.h, ctypes.byref(v)), "crimson_netlist_flow_permitted")
+        return bool(v.value)
+
+    def implicit_coefficients(self, alfi_delt: float):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        N.check(N.lib().crimson_netlist_implicit_coefficients(self.h, alfi_delt, ctypes.byref(a), ctypes.byref(b)),
+                "crimson_netlist_implicit_coefficients")
+        return a.value, b.value
+
+    def update(self, delt: float, q: float) -> None:
+        N.check(N.lib().crimson_netlist_update(self.h, delt, q), "crimson_netlist_update")
+
+    def finalize_step(self) -> None:
+        N.check(N.lib().crimson_netlist_finalize_step(self.h), "crimson_netlist_finalize_step")
+
+    def get(self):
+        p = np.zeros(self.nnodes)
+        q = np.zeros(self.ncomp)
+        o = np.zeros(self.ncomp, dtype=np.int32)
+        N.check(N.lib().crimson_netlist_get(self.h, N.dp(p), N.dp(q), N.ip(o)), "crimson_netlist_get")
+        return p, q, o.astype(bool)
+
+    def state(self) -> np.ndarray:
+        n = ctypes.c_int()
+        N.check(N.lib().crimson_netlist_state_size(self.h, ctypes.byref(n)), "crimson_netlist_state_size")
+        buf = np.zeros(n.value)
+        N.check(N.lib().crimson_netlist_state(self.h, N.dp(buf), 0), "crimson_netlist_state")
+        return buf
+
+    def set_state(self, buf: np.ndarray) -> None:
+        buf = np.ascontiguousarray(buf, dtype=np.float64)
+        N.check(N.lib().crimson_netlist_state(self.h, N.dp(buf), 1), "crimson_netlist_state")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            N.lib().crimson_netlist_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -32,7 +32,7 @@ onto this setting (the tightest the reference's estimator can decide).
 from __future__ import annotations
 
 from dataclasses import dataclass, field
-from typing import List
+from typing import Dict, List, Tuple
 
 
 def time_params(rhoinf: float):
@@ -56,6 +56,38 @@ class RCR:
 
 
 @dataclass
+class NetlistBC:
+    """Netlist (0D lumped-parameter) outlet circuit (flowsolver/src/
+    NetlistCircuit.cxx), the input a netlist XML description carries.
+
+    components: (kind, start node, end node, value) with kind "r" (resistor),
+    "c" (capacitor), "l" (inductor) or "d" (diode; value = open resistance);
+    nodes are numbered 1..N and node 1 is the 3D interface node.
+    prescribed_pressures: node -> fixed pressure ('f').
+    prescribed_flows: component (1-based) -> fixed flow ('f').
+    interface_component: the component (1-based) carrying the 3D flow ('t').
+    initial_pressures: node -> initial pressure (default 0).
+    """
+    srfid: int
+    components: List[Tuple[str, int, int, float]]
+    prescribed_pressures: Dict[int, float] = field(default_factory=dict)
+    prescribed_flows: Dict[int, float] = field(default_factory=dict)
+    interface_component: int = 1
+    initial_pressures: Dict[int, float] = field(default_factory=dict)
+
+    @property
+    def nnodes(self) -> int:
+        return max(max(s, e) for _, s, e, _ in self.components)
+
+    @staticmethod
+    def rcr(srfid: int, Rp: float = 100.0, C: float = 1e-4, Rd: float = 1000.0, Pd: float = 0.0) -> "NetlistBC":
+        """The three-element Windkessel as a circuit: 1 -Rp- 2, 2 -C- 3 (ground),
+        2 -Rd- 4 (distal pressure Pd)."""
+        return NetlistBC(srfid=srfid, components=[("r", 1, 2, Rp), ("c", 2, 3, C), ("r", 2, 4, Rd)],
+                         prescribed_pressures={3: 0.0, 4: Pd}, interface_component=1)
+
+
+@dataclass
 class FlowParams:
     rho: float = 1.06
     mu: float = 0.04
@@ -76,6 +108,9 @@ class FlowParams:
     maxiters: int = 500
     nprjs: int = 10
     rcr: List[RCR] = field(default_factory=list)
+    # netlist outlet circuits, coupled after the RCR surfaces (not reference
+    # settings names: the reference reads them from its netlist XML input)
+    netlists: List[NetlistBC] = field(default_factory=list)
     # NS solve arithmetic: "fp64" (memLS's), "mixed" (FP32 matrices in the
     # inner Krylov matvecs, FP64 outer vectors and iterative refinement of at
     # most max_refine sweeps, until the FP64 defect |R - A x| / |R| is at
@@ -90,6 +125,10 @@ class FlowParams:
     # faster on the 4M-tet cylinder, 0.0739 vs 0.0765 ms per CG iteration) on
     # the two FP32 products L P and Gt (G P) (crimson_memls_ls_set_schur).
     explicit_schur: int = 0
+
+    def outlets(self) -> list:
+        """Coupled outlet surfaces in srflist order: the RCRs, then the netlists."""
+        return list(self.rcr) + list(self.netlists)
 
     @property
     def almi(self) -> float:

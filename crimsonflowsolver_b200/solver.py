@@ -61,7 +61,7 @@ class ElmGMR:
             N.check(L.crimson_set_boundary(self.h, ienb.shape[0], N.ip(ienb), N.ip(iBCB), N.dp(BCB)),
                     "crimson_set_boundary")
         if srflist is None:
-            srflist = [r.srfid for r in P.rcr]
+            srflist = [r.srfid for r in P.outlets()]
         self.srflist = list(srflist)
         if self.srflist:
             sl = np.asarray(self.srflist, dtype=np.int32)
@@ -263,7 +263,7 @@ def neumann_face(mesh, srfid: int):
 
 
 class FlowSolver:
-    """Device-resident time stepping (itrdrv_iter_step) with RCR outlets."""
+    """Device-resident time stepping (itrdrv_iter_step) with RCR and netlist outlets."""
 
     def __init__(self, mesh, P: FlowParams, inflow: Optional[Callable[[float], float]] = None):
         self.mesh = mesh
@@ -274,14 +274,25 @@ class FlowSolver:
         self.memls = MemLS(P, 1 + nc, ctx=self.elm)
         nodes, sv = dirichlet_face(mesh)
         self.memls.bc_create(1, nodes, 3, 0, sv)
-        for k, r in enumerate(P.rcr):
+        outlets = P.outlets()
+        for k, r in enumerate(outlets):
             nn, vv = neumann_face(mesh, r.srfid)
             self.memls.bc_create(2 + k, nn, 3, 1, vv)
         L = N.lib()
+        self.netlists = []
         if nc:
-            arr = lambda f: np.ascontiguousarray(np.array([getattr(r, f) for r in P.rcr], dtype=np.float64))
+            # RCR parameters per surface (zeros on netlist surfaces, whose
+            # coefficients come from the circuit)
+            arr = lambda f: np.ascontiguousarray(np.array([getattr(r, f, 0.0) for r in outlets], dtype=np.float64))
             N.check(L.crimson_set_rcr(self.elm.h, nc, N.dp(arr("Rp")), N.dp(arr("C")), N.dp(arr("Rd")),
                                       N.dp(arr("Pd"))), "crimson_set_rcr")
+            from .netlist import Netlist
+
+            for k, r in enumerate(outlets):
+                if hasattr(r, "components"):
+                    nl = Netlist(r)
+                    N.check(L.crimson_set_outlet_netlist(self.elm.h, k, nl.h), "crimson_set_outlet_netlist")
+                    self.netlists.append(nl)
         self.inflow = inflow if inflow is not None else (lambda t: 10.0)
         if mesh.inlet_nodes is not None and len(mesh.inlet_nodes):
             nodes1 = np.ascontiguousarray(mesh.inlet_nodes.astype(np.int64) + 1, dtype=np.int32)
@@ -312,6 +323,9 @@ class FlowSolver:
         if getattr(self, "elm", None) is not None:
             self.elm.close()
             self.elm = None
+        for nl in getattr(self, "netlists", []):
+            nl.close()
+        self.netlists = []
 
     def __del__(self):
         try:

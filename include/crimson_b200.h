@@ -292,6 +292,66 @@ int crimson_set_rcr(crimson_ctx* ctx, int n, const double* Rp, const double* C, 
  * state, flowsolver/src/AbstractBoundaryCondition.cxx:55-91): read (set = 0)
  * or write (set = 1), e.g. to restart from a checkpoint. */
 int crimson_rcr_state(crimson_ctx* ctx, int n, double* Pn, double* Qn, int set);
+/* ---------------------------------------------------------------------------
+ * Netlist (lumped-parameter 0D) outlet circuits: NetlistCircuit
+ * (flowsolver/src/NetlistCircuit.cxx, CircuitData.cxx, CircuitComponent.cxx)
+ * for circuits of resistors, capacitors, inductors and diodes, with fixed
+ * nodal pressures ('f'), fixed component flows ('f') and exactly one
+ * component carrying the 3D interface flow ('t'), coupled to the 3D domain
+ * through p = dp/dQ * Q + H as the ElmpvsQ netlist branch does
+ * (flowsolver/src/elmgmr.f90:1430-1452).  Host-only calls (no GPU needed).
+ *
+ * Nodes are numbered 1..nnodes and each belongs to at least one component;
+ * the 3D interface node is node 1 (the reference reads the coupling
+ * coefficients from the system's first unknown, node 1's pressure) and
+ * belongs to exactly one component.  Diodes start closed and switch at the
+ * end of each step (open while the pressure drop is >= -1e-8 or the flow
+ * >= 1e-8).  A circuit whose closed diodes block every path from the
+ * interface (the reference then switches the surface to a Dirichlet
+ * condition) returns CRIMSON_ERR_UNSUPPORTED.  Volume-tracking chambers,
+ * time-varying prescriptions and Python controllers are not supported.
+ * --------------------------------------------------------------------------- */
+typedef struct crimson_netlist crimson_netlist;
+#define CRIMSON_NETLIST_RESISTOR 0
+#define CRIMSON_NETLIST_CAPACITOR 1
+#define CRIMSON_NETLIST_INDUCTOR 2
+#define CRIMSON_NETLIST_DIODE 3   /* value = open resistance */
+#define CRIMSON_NETLIST_FLOW_FIXED 0
+#define CRIMSON_NETLIST_FLOW_3D 1
+/* createBasicCircuitDescription + initialiseCircuit
+ * (NetlistCircuit.cxx:131-297, 787-834): component j (0-based arrays) joins
+ * start_node[j] -> end_node[j]; initial_pressure (nnodes) is the state the
+ * histories start from. */
+int crimson_netlist_create(crimson_netlist** nl, int ncomp, const int* kind, const int* start_node,
+                           const int* end_node, const double* value, int nnodes, const double* initial_pressure,
+                           int npres, const int* pres_node, const double* pres_value, int nflow, const int* flow_comp,
+                           const int* flow_kind, const double* flow_value, int interface_node);
+void crimson_netlist_free(crimson_netlist* nl);
+/* detectWhetherClosedDiodesStopAllFlowAt3DInterface (CircuitData.cxx:388-470) */
+int crimson_netlist_flow_permitted(crimson_netlist* nl, int* permitted);
+/* computeImplicitCoefficients (NetlistCircuit.cxx:1764-1800) with the
+ * step's alfi*Delt: the interface pressure p = dp_dq * Q + hop. */
+int crimson_netlist_implicit_coefficients(crimson_netlist* nl, double alfi_delt, double* dp_dq, double* hop);
+/* updateLPN (NetlistCircuit.cxx:1582-1594): solve with Delt and the
+ * interface flow at the end of the step. */
+int crimson_netlist_update(crimson_netlist* nl, double delt, double interface_flow);
+/* finalizeLPNAtEndOfTimestep (NetlistCircuit.cxx:732-737): histories and
+ * diode states for the next step. */
+int crimson_netlist_finalize_step(crimson_netlist* nl);
+/* Current nodal pressures (nnodes), component flows (ncomp) and diode
+ * states (ncomp, 1 = open); any pointer may be NULL. */
+int crimson_netlist_get(const crimson_netlist* nl, double* pressures, double* flows, int* open);
+/* Checkpoint of the circuit state: state_size doubles, read (set = 0) or
+ * written (set = 1). */
+int crimson_netlist_state_size(const crimson_netlist* nl, int* n);
+int crimson_netlist_state(crimson_netlist* nl, double* buf, int set);
+/* Couple surface k (0-based, srflist order) through nl instead of its RCR
+ * in crimson_step: the coefficients come from nl at the start of each step,
+ * and nl is updated and finalised with the surface's flow at its end; the
+ * step's p_out is the interface node's pressure.  nl == NULL restores the
+ * RCR.  The context does not own nl: free the context first. */
+int crimson_set_outlet_netlist(crimson_ctx* ctx, int k, crimson_netlist* nl);
+
 /* yold/acold in the reference layout (nshg, 4) */
 int crimson_state_set(crimson_ctx* ctx, const double* y, const double* ac);
 int crimson_state_get(crimson_ctx* ctx, double* y, double* ac);

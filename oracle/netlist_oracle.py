@@ -1,0 +1,144 @@
+"""CPU restatement of the reference's netlist outlet circuits (test infrastructure).
+
+Only the tests, smoke() and bench.py's CPU legs use this module, as the
+checker of the library's crimson_netlist_* calls.  It follows
+flowsolver/src/NetlistCircuit.cxx, CircuitData.cxx and CircuitComponent.cxx:
+
+* the linear system of generateLinearSystemWithoutFactorisation
+  (NetlistCircuit.cxx:1057-1302): unknowns [nodal pressures | history
+  pressures | component flows | history flows]; rows: one per component
+  (resistor p_s - p_e - R q = 0; open diode the same with its resistance,
+  closed diode q = 0; capacitor p_s - p_e - (alfi_delt / C) q - h_s + h_e = 0;
+  inductor p_s - p_e - (L / alfi_delt)(q - q_hist) = 0), one Kirchhoff row
+  per node with more than one incident component (876-917), then identity
+  rows for fixed pressures, history pressures, prescribed flows and history
+  flows (1262-1296), all in ascending index order;
+* the right-hand side of assembleRHS (1370-1580), the 3D flow multiplied by
+  the interface sign (CircuitData.cxx:186-207);
+* the inverse and x = A^-1 b of solveLinearSystem (1723-1733), the
+  coefficients of computeImplicitCoefficients (1764-1800);
+* updateLPN (1582-1594), finalizeLPNAtEndOfTimestep (732-737) with the
+  diode rule of CircuitComponent.cxx:4-17 and the closed-diode start of
+  NetlistBoundaryCondition.cxx:10-35.
+
+numpy's LAPACK inverse stands in for PETSc's dense MatMatSolve.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+class OracleNetlist:
+    def __init__(self, spec):
+        self.comps = [(k, int(s), int(e), float(v)) for k, s, e, v in spec.components]
+        self.np_ = max(max(s, e) for _, s, e, _ in self.comps)
+        self.nc = len(self.comps)
+        self.fixed = {int(k): float(v) for k, v in spec.prescribed_pressures.items()}
+        self.fixed_flow = {int(k): float(v) for k, v in spec.prescribed_flows.items()}
+        self.iface = int(spec.interface_component)
+        self.p = np.array([spec.initial_pressures.get(i + 1, 0.0) for i in range(self.np_)], dtype=float)
+        self.q = np.zeros(self.nc)
+        k, s, e, _ = self.comps[self.iface - 1]
+        self.sign = 1.0 if s == 1 else -1.0
+        cap_nodes = set()
+        for k, s, e, _ in self.comps:
+            if k == "c":
+                cap_nodes.update((s, e))
+        self.hist_nodes = sorted(cap_nodes)
+        self.hist_comps = [j for j, c in enumerate(self.comps) if c[0] == "l"]
+        count = np.zeros(self.np_ + 1, dtype=int)
+        for _, s, e, _ in self.comps:
+            count[s] += 1
+            count[e] += 1
+        self.kirch = [i for i in range(1, self.np_ + 1) if count[i] > 1]
+        self.pp = sorted(self.fixed)
+        self.pf = sorted(set(self.fixed_flow) | {self.iface})
+        self.open = [c[0] != "d" for c in self.comps]  # diodes start closed
+        self.hist_p = {i: self.pressure(i) for i in self.hist_nodes}
+        self.hist_q = {j: self.q[j] for j in self.hist_comps}
+        self.last_q = 0.0
+        self.n = self.np_ + len(self.hist_nodes) + self.nc + len(self.hist_comps)
+
+    def pressure(self, node):
+        return self.fixed.get(node, self.p[node - 1])
+
+    def _system(self, alfi_delt):
+        n, np_, nc = self.n, self.np_, self.nc
+        nhp = len(self.hist_nodes)
+        fq = np_ + nhp          # first flow unknown
+        fhq = fq + nc           # first history-flow unknown
+        hp_col = {node: np_ + i for i, node in enumerate(self.hist_nodes)}
+        hq_col = {j: fhq + i for i, j in enumerate(self.hist_comps)}
+        A = np.zeros((n, n))
+        b = np.zeros(n)
+        r = 0
+        for j, (k, s, e, v) in enumerate(self.comps):
+            if k == "d" and not self.open[j]:
+                A[r, fq + j] = 1.0
+            else:
+                A[r, s - 1] = 1.0
+                A[r, e - 1] = -1.0
+                if k in ("r", "d"):
+                    A[r, fq + j] = -v
+                elif k == "c":
+                    A[r, fq + j] = -alfi_delt / v
+                    A[r, hp_col[s]] = -1.0
+                    A[r, hp_col[e]] = 1.0
+                else:
+                    A[r, fq + j] = -v / alfi_delt
+                    A[r, hq_col[j]] = v / alfi_delt
+            r += 1
+        for node in self.kirch:
+            for j, (_, s, e, _) in enumerate(self.comps):
+                if e == node:
+                    A[r, fq + j] = 1.0
+                if s == node:
+                    A[r, fq + j] = -1.0
+            r += 1
+        for node in self.pp:
+            A[r, node - 1] = 1.0
+            b[r] = self.fixed[node]
+            r += 1
+        for node in self.hist_nodes:
+            A[r, hp_col[node]] = 1.0
+            b[r] = self.hist_p[node]
+            r += 1
+        iface_row = None
+        for comp in self.pf:
+            A[r, fq + comp - 1] = 1.0
+            if comp == self.iface:
+                b[r] = self.last_q * self.sign
+                iface_row = r
+            else:
+                b[r] = self.fixed_flow[comp]
+            r += 1
+        for j in self.hist_comps:
+            A[r, hq_col[j]] = 1.0
+            b[r] = self.hist_q[j]
+            r += 1
+        assert r == n
+        return A, b, iface_row
+
+    def implicit_coefficients(self, alfi_delt):
+        A, b, col = self._system(alfi_delt)
+        Ainv = np.linalg.inv(A)
+        x = Ainv @ b
+        return self.sign * Ainv[0, col], x[0] - Ainv[0, col] * b[col]
+
+    def update(self, delt, q):
+        self.last_q = q
+        A, b, _ = self._system(delt)
+        x = np.linalg.inv(A) @ b
+        self.p = x[:self.np_].copy()
+        fq = self.np_ + len(self.hist_nodes)
+        self.q = x[fq:fq + self.nc].copy()
+
+    def finalize_step(self):
+        self.hist_p = {i: self.pressure(i) for i in self.hist_nodes}
+        self.hist_q = {j: self.q[j] for j in self.hist_comps}
+        for j, (k, s, e, _) in enumerate(self.comps):
+            if k == "d":
+                self.open[j] = (self.pressure(s) - self.pressure(e) >= -1e-8) or (self.q[j] >= 1e-8)
+
+    def interface_pressure(self):
+        return self.pressure(1)

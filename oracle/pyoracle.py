@@ -283,8 +283,12 @@ class OracleFlow:
         self.nthreads = nthreads
         self.colm, self.rowp = genadj(mesh.ien, mesh.nshg)
         self.elm = Elm(mesh, P, self.colm, self.rowp, nthreads)
-        self.rcr = list(P.rcr)
+        # coupled outlets: RCRs, then netlist circuits (netlist_oracle.py)
+        self.rcr = P.outlets() if hasattr(P, "outlets") else list(P.rcr)
         self.srflist = [r.srfid for r in self.rcr]
+        from oracle.netlist_oracle import OracleNetlist
+
+        self.netlists = [OracleNetlist(r) if hasattr(r, "components") else None for r in self.rcr]
         self.memls = MemLS(mesh.nshg, self.colm, self.rowp, 1 + len(self.rcr), P, nthreads)
         nodes, sv = dirichlet_face(mesh)
         self.memls.bc_create(1, nodes, 3, 0, sv)
@@ -313,7 +317,9 @@ class OracleFlow:
         c1 = np.zeros(len(self.rcr))
         c2 = np.zeros(len(self.rcr))
         for k, r in enumerate(self.rcr):
-            if alpha_form:
+            if self.netlists[k] is not None:
+                c1[k], c2[k] = self.netlists[k].implicit_coefficients(P.alfi * P.Delt if alpha_form else P.Delt)
+            elif alpha_form:
                 c1[k], c2[k] = rcr_coeffs(r.Rp, r.C, r.Rd, r.Pd, r.Pd, self.Pn[k], self.Qn[k], P.alfi * P.Delt)
             else:
                 c1[k], c2[k] = rcr_coeffs(r.Rp, r.C, r.Rd, r.Pd, r.Pd, self.Pn[k], self.Qn[k], P.Delt)
@@ -355,11 +361,17 @@ class OracleFlow:
             self.y[:, 3] = self.y[:, 3] + (P.gami * P.alfi * P.Delt) * sol[:, 3]
             self.ac[:, 0:3] = self.ac[:, 0:3] + sol[:, 0:3]
             self._itr_bc(self.y)
-        # RCR history update at n+1
+        # RCR history update at n+1; netlists: updateLPN + finalizeLPNAtEndOfTimestep
         if self.rcr:
             q1 = getflowq(self.m, self.y, self.srflist)
             d1, h1 = self.implicit_coeffs(n, False)
-            self.Pn = d1 * q1 + h1
+            Pn = d1 * q1 + h1
+            for k, nl in enumerate(self.netlists):
+                if nl is not None:
+                    nl.update(P.Delt, q1[k])
+                    nl.finalize_step()
+                    Pn[k] = nl.interface_pressure()
+            self.Pn = Pn
             self.Qn = q1
         self.yold = self.y.copy()
         self.acold = self.ac.copy()

@@ -1,0 +1,74 @@
+"""Netlist outlets in the device time step (crimson_set_outlet_netlist) against
+the oracle's time stepper with the same circuit (OracleFlow +
+oracle/netlist_oracle.py), and the Windkessel written as a netlist against
+the built-in RCR outlet.  Parity bar as for the RCR time steps: velocity,
+pressure and outlet pressure within 1e-10, identical iteration counts."""
+import numpy as np
+import pytest
+
+from crimsonflowsolver_b200 import FlowParams, NetlistBC, RCR, mesh, solver
+from oracle import pyoracle as po
+from tests.conftest import relerr
+
+pytestmark = pytest.mark.gpu
+
+
+def _inflow(t):
+    return 10.0 + 5.0 * np.sin(2 * np.pi * t / 0.8)
+
+
+def test_rcr_netlist_matches_rcr_outlet():
+    """The circuit 1 -Rp- 2, 2 -C- ground, 2 -Rd- Pd coupled through the
+    netlist path gives the RCR outlet's steps (coefficients equal to
+    rounding)."""
+    Pr = FlowParams(rcr=[RCR(srfid=3, Rp=100.0, C=1e-4, Rd=1000.0, Pd=0.0)])
+    Pn = FlowParams(netlists=[NetlistBC.rcr(3, Rp=100.0, C=1e-4, Rd=1000.0, Pd=0.0)])
+    A = solver.FlowSolver(mesh.cylinder(ncross=8, naxial=10), Pr, inflow=_inflow)
+    B = solver.FlowSolver(mesh.cylinder(ncross=8, naxial=10), Pn, inflow=_inflow)
+    try:
+        for _ in range(3):
+            sa = A.step()
+            sb = B.step()
+            assert [sa.cg_itr[i] for i in range(sa.nsolves)] == [sb.cg_itr[i] for i in range(sb.nsolves)]
+        ya, _ = A.state()
+        yb, _ = B.state()
+    finally:
+        A.close()
+        B.close()
+    assert relerr(yb, ya) < 1e-10, relerr(yb, ya)
+    assert abs(sb.p_out[0] - sa.p_out[0]) <= 1e-10 * abs(sa.p_out[0])
+    assert abs(sb.q_out[0] - sa.q_out[0]) <= 1e-10 * abs(sa.q_out[0])
+
+
+def _circuit():
+    # proximal resistance and inertance, a compliance, a diode-guarded
+    # compliant branch and a distal resistance to a venous pressure
+    return NetlistBC(srfid=3, components=[("r", 1, 2, 80.0), ("l", 2, 3, 2.0), ("c", 3, 4, 1.5e-4),
+                                          ("d", 3, 5, 10.0), ("c", 5, 6, 5e-5), ("r", 3, 7, 900.0)],
+                     prescribed_pressures={4: 0.0, 6: 0.0, 7: 5.0}, interface_component=1,
+                     initial_pressures={2: 5.0, 3: 5.0, 5: 0.0})
+
+
+def test_netlist_time_steps_parity():
+    """Three steps with a five-element circuit (inductor, two capacitors, a
+    diode) on the outlet, device vs oracle."""
+    P = FlowParams(netlists=[_circuit()])
+    F = po.OracleFlow(mesh.cylinder(ncross=8, naxial=10), P, inflow=_inflow)
+    G = solver.FlowSolver(mesh.cylinder(ncross=8, naxial=10), P, inflow=_inflow)
+    try:
+        for _ in range(3):
+            F.step()
+            st = G.step()
+        y, _ = G.state()
+        p, q, op = G.netlists[0].get()
+    finally:
+        G.close()
+    its = [(r, g, c) for r, g, c, _, _ in F.stats[-st.nsolves:]]
+    assert its == [(st.ri_itr[i], st.gm_itr[i], st.cg_itr[i]) for i in range(st.nsolves)]
+    assert relerr(y[:, 0:3], F.y[:, 0:3]) < 1e-10, relerr(y[:, 0:3], F.y[:, 0:3])
+    assert relerr(y[:, 3], F.y[:, 3]) < 1e-10, relerr(y[:, 3], F.y[:, 3])
+    o = F.netlists[0]
+    assert abs(st.p_out[0] - F.Pn[0]) <= 1e-10 * abs(F.Pn[0])
+    assert relerr(p, [o.pressure(i + 1) for i in range(len(p))]) < 1e-10
+    assert relerr(q, o.q) < 1e-10
+    assert list(op) == list(o.open)
