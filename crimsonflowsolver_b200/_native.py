@@ -114,14 +114,14 @@ SIGNATURES = {
     "crimson_memls_cg_layout": (ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                                ctypes.POINTER(ctypes.c_longlong)]),
     "crimson_netlist_create": (ctypes.c_int, [ctypes.POINTER(c_void_p), ctypes.c_int, c_int_p, c_int_p, c_int_p,
-                                              c_dbl_p, ctypes.c_int, c_dbl_p, ctypes.c_int, c_int_p, c_dbl_p,
-                                              ctypes.c_int, c_int_p, c_int_p, c_dbl_p, ctypes.c_int]),
+                                              c_dbl_p, c_dbl_p, c_dbl_p, ctypes.c_int, c_dbl_p, ctypes.c_int, c_int_p,
+                                              c_dbl_p, ctypes.c_int, c_int_p, c_int_p, c_dbl_p, ctypes.c_int]),
     "crimson_netlist_free": (None, [c_void_p]),
     "crimson_netlist_flow_permitted": (ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "crimson_netlist_implicit_coefficients": (ctypes.c_int, [c_void_p, ctypes.c_double, c_dbl_p, c_dbl_p]),
     "crimson_netlist_update": (ctypes.c_int, [c_void_p, ctypes.c_double, ctypes.c_double]),
     "crimson_netlist_finalize_step": (ctypes.c_int, [c_void_p]),
-    "crimson_netlist_get": (ctypes.c_int, [c_void_p, c_dbl_p, c_dbl_p, c_int_p]),
+    "crimson_netlist_get": (ctypes.c_int, [c_void_p, c_dbl_p, c_dbl_p, c_int_p, c_dbl_p]),
     "crimson_netlist_state_size": (ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "crimson_netlist_state": (ctypes.c_int, [c_void_p, c_dbl_p, ctypes.c_int]),
     "crimson_set_outlet_netlist": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p]),

@@ -34,24 +34,43 @@ int fail(const char* msg, int code = CRIMSON_ERR_ARG) {
 inline int col_hist_p(const crimson_netlist* nl) { return nl->np; }
 inline int col_flow(const crimson_netlist* nl) { return nl->np + (int)nl->hist_nodes.size(); }
 inline int col_hist_q(const crimson_netlist* nl) { return col_flow(nl) + nl->nc; }
+inline int col_vol(const crimson_netlist* nl) { return col_hist_q(nl) + (int)nl->hist_comps.size(); }
+inline int col_hist_v(const crimson_netlist* nl) { return col_vol(nl) + (int)nl->vol_comps.size(); }
 
 // Pressure of a node as the reference reads it: a fixed-pressure node
 // returns its prescribed value (CircuitPressureNode.cxx:55-66).
 inline double node_pressure(const NetlistNode& d) { return d.fixed ? d.fixed_p : d.p; }
 
 // generateLinearSystemWithoutFactorisation (NetlistCircuit.cxx:1057-1302):
-// one row per component, one Kirchhoff row per node with more than one
-// incident component, then one identity row per prescribed value (fixed
-// pressures, history pressures, prescribed flows, history flows).
+// one row per component (two for a pressure chamber), one Kirchhoff row per
+// node with more than one incident component, then one identity row per
+// prescribed value (fixed pressures, history pressures, prescribed flows,
+// history flows, history volumes).
 void build_system(crimson_netlist* nl, double alfi_delt) {
     const int n = nl->n;
     std::fill(nl->A.begin(), nl->A.end(), 0.0);
     auto a = [&](int r, int c) -> double& { return nl->A[(size_t)r * n + c]; };
     const int cf = col_flow(nl), chp = col_hist_p(nl), chq = col_hist_q(nl);
+    const int cv = col_vol(nl), chv = col_hist_v(nl);
     int row = 0;
     for (int j = 0; j < nl->nc; ++j, ++row) {
         const NetlistComp& c = nl->comp[j];
         switch (c.kind) {
+            case CRIMSON_NETLIST_VOLUME_TRACKING:
+            case CRIMSON_NETLIST_PRESSURE_CHAMBER: {
+                // dV/dt = q: V - V_hist - alfi_delt q = 0
+                const int v = nl->vol_ord[j];
+                a(row, cf + j) = -alfi_delt;
+                a(row, cv + v) = 1.0;
+                a(row, chv + v) = -1.0;
+                if (c.kind == CRIMSON_NETLIST_PRESSURE_CHAMBER) {
+                    // p_start / E - V = -V_unstressed
+                    ++row;
+                    a(row, c.start - 1) = 1.0 / c.value;
+                    a(row, cv + v) = -1.0;
+                }
+                break;
+            }
             case CRIMSON_NETLIST_RESISTOR:
                 a(row, c.start - 1) = 1.0;
                 a(row, c.end - 1) = -1.0;
@@ -93,11 +112,17 @@ void build_system(crimson_netlist* nl, double alfi_delt) {
     for (size_t l = 0; l < nl->hist_nodes.size(); ++l) a(row++, chp + (int)l) = 1.0;
     for (int j : nl->pf_comps) a(row++, cf + j) = 1.0;
     for (size_t l = 0; l < nl->hist_comps.size(); ++l) a(row++, chq + (int)l) = 1.0;
+    for (size_t l = 0; l < nl->vol_comps.size(); ++l) a(row++, chv + (int)l) = 1.0;
+}
+
+// First row of the prescribed values (after the component and Kirchhoff rows).
+inline int first_prescribed_row(const crimson_netlist* nl) {
+    return nl->nc + nl->nchamber + (int)nl->kirch_nodes.size();
 }
 
 // Row of the system that carries the 3D interface flow.
 int iface_row(const crimson_netlist* nl) {
-    int r = nl->nc + (int)nl->kirch_nodes.size() + (int)nl->pp_nodes.size() + (int)nl->hist_nodes.size();
+    int r = first_prescribed_row(nl) + (int)nl->pp_nodes.size() + (int)nl->hist_nodes.size();
     for (int j : nl->pf_comps) {
         if (j == nl->iface_comp) return r;
         ++r;
@@ -108,7 +133,7 @@ int iface_row(const crimson_netlist* nl) {
 // assembleRHS (NetlistCircuit.cxx:1370-1580) in the same row order.
 void assemble_rhs(crimson_netlist* nl) {
     std::fill(nl->b.begin(), nl->b.end(), 0.0);
-    int row = nl->nc + (int)nl->kirch_nodes.size();
+    int row = first_prescribed_row(nl);
     for (int nd : nl->pp_nodes) nl->b[row++] = nl->node[nd - 1].fixed_p;
     for (int nd : nl->hist_nodes) nl->b[row++] = nl->node[nd - 1].hist;
     for (int j : nl->pf_comps) {
@@ -116,6 +141,11 @@ void assemble_rhs(crimson_netlist* nl) {
         nl->b[row++] = c.flow_kind == CRIMSON_NETLIST_FLOW_3D ? nl->last_q * nl->sign : c.flow_fixed;
     }
     for (int j : nl->hist_comps) nl->b[row++] = nl->comp[j].hist_flow;
+    for (int j : nl->vol_comps) nl->b[row++] = nl->comp[j].hist_volume;
+    // a chamber's second row: compliance * pressure = volume - unstressed volume
+    int r = 0;
+    for (int j = 0; j < nl->nc; ++j, ++r)
+        if (nl->comp[j].kind == CRIMSON_NETLIST_PRESSURE_CHAMBER) nl->b[++r] = -nl->comp[j].unstressed;
 }
 
 // solveLinearSystem (NetlistCircuit.cxx:1723-1733): the inverse of the
@@ -204,8 +234,9 @@ int netlist_begin_step(crimson_netlist* nl) {
 extern "C" {
 
 int crimson_netlist_create(crimson_netlist** out, int ncomp, const int* kind, const int* start_node,
-                           const int* end_node, const double* value, int nnodes, const double* initial_pressure,
-                           int npres, const int* pres_node, const double* pres_value, int nflow, const int* flow_comp,
+                           const int* end_node, const double* value, const double* initial_volume,
+                           const double* unstressed_volume, int nnodes, const double* initial_pressure, int npres,
+                           const int* pres_node, const double* pres_value, int nflow, const int* flow_comp,
                            const int* flow_kind, const double* flow_value, int interface_node) {
     if (!out) return CRIMSON_ERR_ARG;
     *out = nullptr;
@@ -231,12 +262,20 @@ int crimson_netlist_create(crimson_netlist** out, int ncomp, const int* kind, co
         c.start = start_node[j];
         c.end = end_node[j];
         c.value = value[j];
-        if (c.kind < CRIMSON_NETLIST_RESISTOR || c.kind > CRIMSON_NETLIST_DIODE)
+        if (c.kind < CRIMSON_NETLIST_RESISTOR || c.kind > CRIMSON_NETLIST_PRESSURE_CHAMBER)
             return bad("netlist: unknown component kind");
         if (c.start < 1 || c.start > nnodes || c.end < 1 || c.end > nnodes || c.start == c.end)
             return bad("netlist: component nodes out of range or equal");
-        if (!std::isfinite(c.value) || (c.kind == CRIMSON_NETLIST_CAPACITOR && c.value == 0.0))
+        if (!std::isfinite(c.value) ||
+            ((c.kind == CRIMSON_NETLIST_CAPACITOR || c.kind == CRIMSON_NETLIST_PRESSURE_CHAMBER) && c.value == 0.0))
             return bad("netlist: bad component value");
+        if (c.kind >= CRIMSON_NETLIST_VOLUME_TRACKING) {
+            if (!initial_volume || !std::isfinite(initial_volume[j]))
+                return bad("netlist: a volume-tracking component needs its initial volume");
+            c.volume = initial_volume[j];
+            c.unstressed = unstressed_volume ? unstressed_volume[j] : 0.0;
+            if (!std::isfinite(c.unstressed)) return bad("netlist: non-finite unstressed volume");
+        }
         uses[c.start - 1] += 1;
         uses[c.end - 1] += 1;
     }
@@ -299,11 +338,21 @@ int crimson_netlist_create(crimson_netlist** out, int ncomp, const int* kind, co
             nl->hist_comp_ord[j] = (int)nl->hist_comps.size();
             nl->hist_comps.push_back(j);
         }
+    // volume-tracking components: a tracked and a history volume each
+    // (NetlistCircuit.cxx:981-1041)
+    nl->vol_ord.assign((size_t)ncomp, -1);
+    for (int j = 0; j < ncomp; ++j)
+        if (nl->comp[j].kind >= CRIMSON_NETLIST_VOLUME_TRACKING) {
+            nl->vol_ord[j] = (int)nl->vol_comps.size();
+            nl->vol_comps.push_back(j);
+            if (nl->comp[j].kind == CRIMSON_NETLIST_PRESSURE_CHAMBER) ++nl->nchamber;
+        }
     for (int i = 0; i < nnodes; ++i)
         if (uses[i] > 1) nl->kirch_nodes.push_back(i + 1);
-    if ((int)(nl->kirch_nodes.size() + nl->pp_nodes.size() + nl->pf_comps.size()) != nnodes)
+    const int nv = (int)nl->vol_comps.size();
+    if (nl->nchamber + (int)(nl->kirch_nodes.size() + nl->pp_nodes.size() + nl->pf_comps.size()) != nnodes + nv)
         return bad("netlist: malformed circuit (the system is not square)");
-    nl->n = nnodes + (int)nl->hist_nodes.size() + ncomp + (int)nl->hist_comps.size();
+    nl->n = nnodes + (int)nl->hist_nodes.size() + ncomp + (int)nl->hist_comps.size() + 2 * nv;
     nl->A.assign((size_t)nl->n * nl->n, 0.0);
     nl->Ainv.assign((size_t)nl->n * nl->n, 0.0);
     nl->b.assign((size_t)nl->n, 0.0);
@@ -326,6 +375,7 @@ int crimson_netlist_create(crimson_netlist** out, int ncomp, const int* kind, co
     for (NetlistNode& d : nl->node)
         if (d.has_hist) d.hist = node_pressure(d);
     for (int j : nl->hist_comps) nl->comp[j].hist_flow = nl->comp[j].flow;
+    for (int j : nl->vol_comps) nl->comp[j].hist_volume = nl->comp[j].volume;
     nl->flow_permitted = detect_flow_permitted(nl);
     *out = nl;
     return CRIMSON_OK;
@@ -369,6 +419,15 @@ int crimson_netlist_update(crimson_netlist* nl, double delt, double interface_fl
     for (int i = 0; i < nl->np; ++i) nl->node[i].p = nl->x[i];
     const int cf = col_flow(nl);
     for (int j = 0; j < nl->nc; ++j) nl->comp[j].flow = nl->x[(size_t)cf + j];
+    // volumes; a chamber passes E (V - V_unstressed) to its start node
+    // (giveComponentsTheirVolumesFromSolutionVector, NetlistCircuit.cxx:
+    // 1636-1660; CircuitComponent.cxx:188-209)
+    const int cv = col_vol(nl);
+    for (int j : nl->vol_comps) {
+        NetlistComp& c = nl->comp[j];
+        c.volume = nl->x[(size_t)cv + nl->vol_ord[j]];
+        if (c.kind == CRIMSON_NETLIST_PRESSURE_CHAMBER) nl->node[(size_t)c.start - 1].p = (c.volume - c.unstressed) * c.value;
+    }
     return CRIMSON_OK;
 }
 
@@ -380,6 +439,7 @@ int crimson_netlist_finalize_step(crimson_netlist* nl) {
     for (NetlistNode& d : nl->node)
         if (d.has_hist) d.hist = node_pressure(d);
     for (int j : nl->hist_comps) nl->comp[j].hist_flow = nl->comp[j].flow;
+    for (int j : nl->vol_comps) nl->comp[j].hist_volume = nl->comp[j].volume;
     const double tol = 1e-8;
     for (NetlistComp& c : nl->comp) {
         if (c.kind != CRIMSON_NETLIST_DIODE) continue;
@@ -390,21 +450,23 @@ int crimson_netlist_finalize_step(crimson_netlist* nl) {
     return CRIMSON_OK;
 }
 
-int crimson_netlist_get(const crimson_netlist* nl, double* pressures, double* flows, int* open) {
+int crimson_netlist_get(const crimson_netlist* nl, double* pressures, double* flows, int* open, double* volumes) {
     if (!nl) return CRIMSON_ERR_ARG;
     for (int i = 0; pressures && i < nl->np; ++i) pressures[i] = node_pressure(nl->node[i]);
     for (int j = 0; flows && j < nl->nc; ++j) flows[j] = nl->comp[j].flow;
     for (int j = 0; open && j < nl->nc; ++j) open[j] = nl->comp[j].open ? 1 : 0;
+    for (int j = 0; volumes && j < nl->nc; ++j) volumes[j] = nl->comp[j].volume;
     return CRIMSON_OK;
 }
 
 int crimson_netlist_state_size(const crimson_netlist* nl, int* n) {
     if (!nl || !n) return CRIMSON_ERR_ARG;
-    *n = 2 * nl->np + 3 * nl->nc + 1;
+    *n = 2 * nl->np + 5 * nl->nc + 1;
     return CRIMSON_OK;
 }
 
-// Checkpoint layout: [p (np), hist (np), flow (nc), hist_flow (nc), open (nc), last_q]
+// Checkpoint layout: [p (np), hist (np), flow (nc), hist_flow (nc), open (nc),
+// volume (nc), hist_volume (nc), last_q]
 int crimson_netlist_state(crimson_netlist* nl, double* buf, int set) {
     if (!nl || !buf) return CRIMSON_ERR_ARG;
     const int np = nl->np, nc = nl->nc;
@@ -417,8 +479,10 @@ int crimson_netlist_state(crimson_netlist* nl, double* buf, int set) {
             nl->comp[j].flow = buf[2 * np + j];
             nl->comp[j].hist_flow = buf[2 * np + nc + j];
             nl->comp[j].open = buf[2 * np + 2 * nc + j] != 0.0;
+            nl->comp[j].volume = buf[2 * np + 3 * nc + j];
+            nl->comp[j].hist_volume = buf[2 * np + 4 * nc + j];
         }
-        nl->last_q = buf[2 * np + 3 * nc];
+        nl->last_q = buf[2 * np + 5 * nc];
         nl->flow_permitted = detect_flow_permitted(nl);
     } else {
         for (int i = 0; i < np; ++i) {
@@ -429,8 +493,10 @@ int crimson_netlist_state(crimson_netlist* nl, double* buf, int set) {
             buf[2 * np + j] = nl->comp[j].flow;
             buf[2 * np + nc + j] = nl->comp[j].hist_flow;
             buf[2 * np + 2 * nc + j] = nl->comp[j].open ? 1.0 : 0.0;
+            buf[2 * np + 3 * nc + j] = nl->comp[j].volume;
+            buf[2 * np + 4 * nc + j] = nl->comp[j].hist_volume;
         }
-        buf[2 * np + 3 * nc] = nl->last_q;
+        buf[2 * np + 5 * nc] = nl->last_q;
     }
     return CRIMSON_OK;
 }

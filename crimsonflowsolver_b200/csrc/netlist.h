@@ -28,6 +28,8 @@ struct NetlistComp {
     double flow = 0.0;       // current flow (start -> end)
     double hist_flow = 0.0;  // flow of the previous step (inductors)
     bool open = true;        // diodes: permits flow
+    // volume-tracking components (value = elastance for a pressure chamber)
+    double volume = 0.0, hist_volume = 0.0, unstressed = 0.0;
 };
 
 }  // namespace crimson
@@ -40,9 +42,13 @@ struct crimson_netlist {
     int iface_comp = -1;  // 0-based
     double sign = 1.0;    // +1: the interface component's start node is the interface node
     // unknown layout of the linear system (NetlistCircuit.cxx:1057-1302):
-    // [pressures (np) | history pressures (nhp) | flows (nc) | history flows (nhf)]
+    // [pressures (np) | history pressures (nhp) | flows (nc) | history flows (nhf)
+    //  | tracked volumes (nv) | history volumes (nv)]
     std::vector<int> hist_nodes;   // ascending node indices with a history pressure
     std::vector<int> hist_comps;   // ascending 0-based inductor indices
+    std::vector<int> vol_comps;    // ascending 0-based volume-tracking components
+    std::vector<int> vol_ord;      // component -> position in vol_comps (-1: none)
+    int nchamber = 0;              // pressure chambers (two rows each)
     std::vector<int> kirch_nodes;  // ascending node indices with more than one incident component
     std::vector<int> pp_nodes;     // ascending prescribed-pressure nodes
     std::vector<int> pf_comps;     // ascending 0-based prescribed-flow components

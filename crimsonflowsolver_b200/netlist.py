@@ -15,7 +15,7 @@ import numpy as np
 from . import _native as N
 from .problem import NetlistBC
 
-KINDS = {"r": 0, "c": 1, "l": 2, "d": 3}
+KINDS = {"r": 0, "c": 1, "l": 2, "i": 2, "d": 3, "t": 4, "v": 5}
 
 
 class Netlist:
@@ -28,6 +28,8 @@ class Netlist:
         en = np.array([c[2] for c in comps], dtype=np.int32)
         val = np.array([c[3] for c in comps], dtype=np.float64)
         p0 = np.array([spec.initial_pressures.get(i + 1, 0.0) for i in range(nn)], dtype=np.float64)
+        v0 = np.array([spec.volumes.get(j + 1, (0.0, 0.0))[0] for j in range(len(comps))], dtype=np.float64)
+        vu = np.array([spec.volumes.get(j + 1, (0.0, 0.0))[1] for j in range(len(comps))], dtype=np.float64)
         pn = np.array(sorted(spec.prescribed_pressures), dtype=np.int32)
         pv = np.array([spec.prescribed_pressures[k] for k in pn], dtype=np.float64)
         fc = [spec.interface_component] + sorted(spec.prescribed_flows)
@@ -37,8 +39,8 @@ class Netlist:
         self.ncomp, self.nnodes = len(comps), nn
         h = ctypes.c_void_p()
         N.check(N.lib().crimson_netlist_create(ctypes.byref(h), len(comps), N.ip(kind), N.ip(st), N.ip(en), N.dp(val),
-                                               nn, N.dp(p0), len(pn), N.ip(pn), N.dp(pv), len(fc), N.ip(fc),
-                                               N.ip(fk), N.dp(fv), 1), "crimson_netlist_create")
+                                               N.dp(v0), N.dp(vu), nn, N.dp(p0), len(pn), N.ip(pn), N.dp(pv), len(fc),
+                                               N.ip(fc), N.ip(fk), N.dp(fv), 1), "crimson_netlist_create")
         self.h = h
 
     def flow_permitted(self) -> bool:
@@ -59,11 +61,13 @@ class Netlist:
         N.check(N.lib().crimson_netlist_finalize_step(self.h), "crimson_netlist_finalize_step")
 
     def get(self):
+        """(nodal pressures, component flows, diode open flags, volumes)."""
         p = np.zeros(self.nnodes)
         q = np.zeros(self.ncomp)
         o = np.zeros(self.ncomp, dtype=np.int32)
-        N.check(N.lib().crimson_netlist_get(self.h, N.dp(p), N.dp(q), N.ip(o)), "crimson_netlist_get")
-        return p, q, o.astype(bool)
+        v = np.zeros(self.ncomp)
+        N.check(N.lib().crimson_netlist_get(self.h, N.dp(p), N.dp(q), N.ip(o), N.dp(v)), "crimson_netlist_get")
+        return p, q, o.astype(bool), v
 
     def state(self) -> np.ndarray:
         n = ctypes.c_int()

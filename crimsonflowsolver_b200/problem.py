@@ -61,12 +61,15 @@ class NetlistBC:
     NetlistCircuit.cxx), the input a netlist XML description carries.
 
     components: (kind, start node, end node, value) with kind "r" (resistor),
-    "c" (capacitor), "l" (inductor) or "d" (diode; value = open resistance);
-    nodes are numbered 1..N and node 1 is the 3D interface node.
+    "c" (capacitor), "l" or "i" (inductor), "d" (diode; value = open
+    resistance), "t" (volume tracking) or "v" (pressure chamber; value =
+    elastance); nodes are numbered 1..N and node 1 is the 3D interface node.
     prescribed_pressures: node -> fixed pressure ('f').
     prescribed_flows: component (1-based) -> fixed flow ('f').
     interface_component: the component (1-based) carrying the 3D flow ('t').
     initial_pressures: node -> initial pressure (default 0).
+    volumes: component (1-based) -> (initial volume, unstressed volume) for
+    the "t" and "v" components.
     """
     srfid: int
     components: List[Tuple[str, int, int, float]]
@@ -74,6 +77,7 @@ class NetlistBC:
     prescribed_flows: Dict[int, float] = field(default_factory=dict)
     interface_component: int = 1
     initial_pressures: Dict[int, float] = field(default_factory=dict)
+    volumes: Dict[int, Tuple[float, float]] = field(default_factory=dict)
 
     @property
     def nnodes(self) -> int:

@@ -299,7 +299,9 @@ int crimson_rcr_state(crimson_ctx* ctx, int n, double* Pn, double* Qn, int set);
  * nodal pressures ('f'), fixed component flows ('f') and exactly one
  * component carrying the 3D interface flow ('t'), coupled to the 3D domain
  * through p = dp/dQ * Q + H as the ElmpvsQ netlist branch does
- * (flowsolver/src/elmgmr.f90:1430-1452).  Host-only calls (no GPU needed).
+ * (flowsolver/src/elmgmr.f90:1430-1452).  Volume-tracking components and
+ * pressure chambers (elastance E, initial and unstressed volume) carry a
+ * volume unknown.  Host-only calls (no GPU needed).
  *
  * Nodes are numbered 1..nnodes and each belongs to at least one component;
  * the 3D interface node is node 1 (the reference reads the coupling
@@ -308,23 +310,29 @@ int crimson_rcr_state(crimson_ctx* ctx, int n, double* Pn, double* Qn, int set);
  * end of each step (open while the pressure drop is >= -1e-8 or the flow
  * >= 1e-8).  A circuit whose closed diodes block every path from the
  * interface (the reference then switches the surface to a Dirichlet
- * condition) returns CRIMSON_ERR_UNSUPPORTED.  Volume-tracking chambers,
- * time-varying prescriptions and Python controllers are not supported.
+ * condition) returns CRIMSON_ERR_UNSUPPORTED.  Left-ventricular pressure
+ * prescriptions, time-varying prescriptions and Python controllers are not
+ * supported.
  * --------------------------------------------------------------------------- */
 typedef struct crimson_netlist crimson_netlist;
 #define CRIMSON_NETLIST_RESISTOR 0
 #define CRIMSON_NETLIST_CAPACITOR 1
 #define CRIMSON_NETLIST_INDUCTOR 2
 #define CRIMSON_NETLIST_DIODE 3   /* value = open resistance */
+#define CRIMSON_NETLIST_VOLUME_TRACKING 4   /* dV/dt = q */
+#define CRIMSON_NETLIST_PRESSURE_CHAMBER 5  /* dV/dt = q, p_start = value * (V - V_unstressed) */
 #define CRIMSON_NETLIST_FLOW_FIXED 0
 #define CRIMSON_NETLIST_FLOW_3D 1
 /* createBasicCircuitDescription + initialiseCircuit
  * (NetlistCircuit.cxx:131-297, 787-834): component j (0-based arrays) joins
- * start_node[j] -> end_node[j]; initial_pressure (nnodes) is the state the
- * histories start from. */
+ * start_node[j] -> end_node[j]; initial_volume / unstressed_volume (ncomp,
+ * read for volume-tracking components only; may be NULL without them, and
+ * unstressed_volume NULL means 0); initial_pressure (nnodes) is the state
+ * the histories start from. */
 int crimson_netlist_create(crimson_netlist** nl, int ncomp, const int* kind, const int* start_node,
-                           const int* end_node, const double* value, int nnodes, const double* initial_pressure,
-                           int npres, const int* pres_node, const double* pres_value, int nflow, const int* flow_comp,
+                           const int* end_node, const double* value, const double* initial_volume,
+                           const double* unstressed_volume, int nnodes, const double* initial_pressure, int npres,
+                           const int* pres_node, const double* pres_value, int nflow, const int* flow_comp,
                            const int* flow_kind, const double* flow_value, int interface_node);
 void crimson_netlist_free(crimson_netlist* nl);
 /* detectWhetherClosedDiodesStopAllFlowAt3DInterface (CircuitData.cxx:388-470) */
@@ -338,9 +346,10 @@ int crimson_netlist_update(crimson_netlist* nl, double delt, double interface_fl
 /* finalizeLPNAtEndOfTimestep (NetlistCircuit.cxx:732-737): histories and
  * diode states for the next step. */
 int crimson_netlist_finalize_step(crimson_netlist* nl);
-/* Current nodal pressures (nnodes), component flows (ncomp) and diode
- * states (ncomp, 1 = open); any pointer may be NULL. */
-int crimson_netlist_get(const crimson_netlist* nl, double* pressures, double* flows, int* open);
+/* Current nodal pressures (nnodes), component flows (ncomp), diode states
+ * (ncomp, 1 = open) and volumes (ncomp, 0 for components without one); any
+ * pointer may be NULL. */
+int crimson_netlist_get(const crimson_netlist* nl, double* pressures, double* flows, int* open, double* volumes);
 /* Checkpoint of the circuit state: state_size doubles, read (set = 0) or
  * written (set = 1). */
 int crimson_netlist_state_size(const crimson_netlist* nl, int* n);

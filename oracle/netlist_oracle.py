@@ -19,7 +19,11 @@ flowsolver/src/NetlistCircuit.cxx, CircuitData.cxx and CircuitComponent.cxx:
   coefficients of computeImplicitCoefficients (1764-1800);
 * updateLPN (1582-1594), finalizeLPNAtEndOfTimestep (732-737) with the
   diode rule of CircuitComponent.cxx:4-17 and the closed-diode start of
-  NetlistBoundaryCondition.cxx:10-35.
+  NetlistBoundaryCondition.cxx:10-35;
+* volume-tracking components (V - V_hist - alfi_delt q = 0) and pressure
+  chambers (the same plus p_start / E - V = -V_unstressed, the start node
+  then taking E (V - V_unstressed), CircuitComponent.cxx:188-209), with the
+  tracked and history volumes after the history flows (1147-1241, 1282-1287).
 
 numpy's LAPACK inverse stands in for PETSc's dense MatMatSolve.
 """
@@ -30,7 +34,7 @@ import numpy as np
 
 class OracleNetlist:
     def __init__(self, spec):
-        self.comps = [(k, int(s), int(e), float(v)) for k, s, e, v in spec.components]
+        self.comps = [("l" if k == "i" else k, int(s), int(e), float(v)) for k, s, e, v in spec.components]
         self.np_ = max(max(s, e) for _, s, e, _ in self.comps)
         self.nc = len(self.comps)
         self.fixed = {int(k): float(v) for k, v in spec.prescribed_pressures.items()}
@@ -46,6 +50,11 @@ class OracleNetlist:
                 cap_nodes.update((s, e))
         self.hist_nodes = sorted(cap_nodes)
         self.hist_comps = [j for j, c in enumerate(self.comps) if c[0] == "l"]
+        self.vol_comps = [j for j, c in enumerate(self.comps) if c[0] in ("t", "v")]
+        self.vol = {j: float(spec.volumes[j + 1][0]) for j in self.vol_comps}
+        self.v0 = {j: float(spec.volumes[j + 1][1]) for j in self.vol_comps}
+        self.hist_v = dict(self.vol)
+        self.nchamber = sum(1 for c in self.comps if c[0] == "v")
         count = np.zeros(self.np_ + 1, dtype=int)
         for _, s, e, _ in self.comps:
             count[s] += 1
@@ -57,7 +66,7 @@ class OracleNetlist:
         self.hist_p = {i: self.pressure(i) for i in self.hist_nodes}
         self.hist_q = {j: self.q[j] for j in self.hist_comps}
         self.last_q = 0.0
-        self.n = self.np_ + len(self.hist_nodes) + self.nc + len(self.hist_comps)
+        self.n = self.np_ + len(self.hist_nodes) + self.nc + len(self.hist_comps) + 2 * len(self.vol_comps)
 
     def pressure(self, node):
         return self.fixed.get(node, self.p[node - 1])
@@ -69,11 +78,23 @@ class OracleNetlist:
         fhq = fq + nc           # first history-flow unknown
         hp_col = {node: np_ + i for i, node in enumerate(self.hist_nodes)}
         hq_col = {j: fhq + i for i, j in enumerate(self.hist_comps)}
+        fv = fhq + len(self.hist_comps)
+        v_col = {j: fv + i for i, j in enumerate(self.vol_comps)}
+        hv_col = {j: fv + len(self.vol_comps) + i for i, j in enumerate(self.vol_comps)}
         A = np.zeros((n, n))
         b = np.zeros(n)
         r = 0
         for j, (k, s, e, v) in enumerate(self.comps):
-            if k == "d" and not self.open[j]:
+            if k in ("t", "v"):
+                A[r, fq + j] = -alfi_delt
+                A[r, v_col[j]] = 1.0
+                A[r, hv_col[j]] = -1.0
+                if k == "v":
+                    r += 1
+                    A[r, s - 1] = 1.0 / v
+                    A[r, v_col[j]] = -1.0
+                    b[r] = -self.v0[j]
+            elif k == "d" and not self.open[j]:
                 A[r, fq + j] = 1.0
             else:
                 A[r, s - 1] = 1.0
@@ -116,6 +137,10 @@ class OracleNetlist:
             A[r, hq_col[j]] = 1.0
             b[r] = self.hist_q[j]
             r += 1
+        for j in self.vol_comps:
+            A[r, hv_col[j]] = 1.0
+            b[r] = self.hist_v[j]
+            r += 1
         assert r == n
         return A, b, iface_row
 
@@ -132,10 +157,17 @@ class OracleNetlist:
         self.p = x[:self.np_].copy()
         fq = self.np_ + len(self.hist_nodes)
         self.q = x[fq:fq + self.nc].copy()
+        fv = fq + self.nc + len(self.hist_comps)
+        for i, j in enumerate(self.vol_comps):
+            self.vol[j] = x[fv + i]
+            k, s, _, v = self.comps[j]
+            if k == "v":
+                self.p[s - 1] = (self.vol[j] - self.v0[j]) * v
 
     def finalize_step(self):
         self.hist_p = {i: self.pressure(i) for i in self.hist_nodes}
         self.hist_q = {j: self.q[j] for j in self.hist_comps}
+        self.hist_v = dict(self.vol)
         for j, (k, s, e, _) in enumerate(self.comps):
             if k == "d":
                 self.open[j] = (self.pressure(s) - self.pressure(e) >= -1e-8) or (self.q[j] >= 1e-8)

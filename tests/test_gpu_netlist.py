@@ -60,7 +60,7 @@ def test_netlist_time_steps_parity():
             F.step()
             st = G.step()
         y, _ = G.state()
-        p, q, op = G.netlists[0].get()
+        p, q, op, _ = G.netlists[0].get()
     finally:
         G.close()
     its = [(r, g, c) for r, g, c, _, _ in F.stats[-st.nsolves:]]

@@ -19,6 +19,8 @@ ALFI, DT = 0.5, 1e-3
 
 def _close(a, b, tol=1e-12):
     a, b = np.asarray(a, float), np.asarray(b, float)
+    if a.size == 0 and b.size == 0:
+        return True
     return np.abs(a - b).max() <= tol * max(1.0, np.abs(b).max())
 
 
@@ -48,16 +50,24 @@ def test_rcr_circuit_matches_reference_rcr(Pd):
 
 def _random_circuit(rng, nextra=6, with_inductor=True, with_diode=True, fixed_flow=True):
     """A random tree from the interface node 1 plus a few cycles; leaves get
-    fixed pressures (or, for one leaf, a fixed flow on its component)."""
+    fixed pressures (or, for one leaf, a fixed flow on its component);
+    pressure chambers end at a fixed-pressure leaf of their own."""
     comps = [("r", 1, 2, float(rng.uniform(50, 150)))]
     nodes = [2]
     nxt = 3
-    kinds = ["r", "c"] + (["l"] if with_inductor else []) + (["d"] if with_diode else [])
+    kinds = ["r", "c", "v"] + (["l"] if with_inductor else []) + (["d"] if with_diode else [])
+    volumes, chamber_leaves = {}, set()
     for _ in range(nextra):
         a = int(rng.choice(nodes))
         k = str(rng.choice(kinds))
         val = {"r": rng.uniform(100, 2000), "c": rng.uniform(1e-5, 1e-3), "l": rng.uniform(1.0, 10.0),
-               "d": rng.uniform(1.0, 20.0)}[k]
+               "d": rng.uniform(1.0, 20.0), "v": rng.uniform(500.0, 5000.0)}[k]
+        if k == "v":
+            comps.append((k, a, nxt, float(val)))
+            volumes[len(comps)] = (float(rng.uniform(20.0, 60.0)), float(rng.uniform(0.0, 10.0)))
+            chamber_leaves.add(nxt)
+            nxt += 1
+            continue
         comps.append((k, a, nxt, float(val)) if rng.random() < 0.7 else (k, nxt, a, float(val)))
         nodes.append(nxt)
         nxt += 1
@@ -75,16 +85,16 @@ def _random_circuit(rng, nextra=6, with_inductor=True, with_diode=True, fixed_fl
     pres, flows = {}, {}
     for i, leaf in enumerate(leaves):
         j = next(j for j, c in enumerate(comps) if leaf in (c[1], c[2]))
-        if fixed_flow and i == 0 and len(leaves) > 1 and comps[j][0] in ("r", "c"):
+        if fixed_flow and i == 0 and len(leaves) > 1 and comps[j][0] in ("r", "c") and leaf not in chamber_leaves:
             flows[j + 1] = float(rng.uniform(-2, 2))
         else:
             pres[leaf] = float(rng.uniform(0, 50)) if rng.random() < 0.5 else 0.0
     init = {i: float(rng.uniform(0, 100)) for i in range(1, nxt)}
     return NetlistBC(srfid=3, components=comps, prescribed_pressures=pres, prescribed_flows=flows,
-                     interface_component=1, initial_pressures=init)
+                     interface_component=1, initial_pressures=init, volumes=volumes)
 
 
-@pytest.mark.parametrize("seed", range(12))
+@pytest.mark.parametrize("seed", range(16))
 def test_random_circuits_match_oracle(seed):
     """Coefficients, nodal pressures, component flows and diode states over
     ten steps of random interface flows, library vs oracle."""
@@ -115,9 +125,10 @@ def test_random_circuits_match_oracle(seed):
         q = float(30.0 * rng.standard_normal())
         g.update(DT, q)
         o.update(DT, q)
-        p, f, op = g.get()
+        p, f, op, vol = g.get()
         assert _close(p, [o.pressure(i + 1) for i in range(len(p))], 1e-10)
         assert _close(f, o.q, 1e-10)
+        assert _close([vol[j] for j in o.vol_comps], [o.vol[j] for j in o.vol_comps], 1e-10)
         g.finalize_step()
         o.finalize_step()
         assert list(g.get()[2]) == list(o.open)
@@ -179,8 +190,9 @@ def test_malformed_circuits_rejected(case):
         fk = np.array([1, 1], np.int32)
         fv = np.zeros(2)
         h = ctypes.c_void_p()
-        rc = N.lib().crimson_netlist_create(ctypes.byref(h), 3, N.ip(kind), N.ip(st), N.ip(en), N.dp(val), 4,
-                                            N.dp(p0), 2, N.ip(pn), N.dp(pv), 2, N.ip(fc), N.ip(fk), N.dp(fv), 1)
+        rc = N.lib().crimson_netlist_create(ctypes.byref(h), 3, N.ip(kind), N.ip(st), N.ip(en), N.dp(val), None,
+                                            None, 4, N.dp(p0), 2, N.ip(pn), N.dp(pv), 2, N.ip(fc), N.ip(fk),
+                                            N.dp(fv), 1)
         assert rc == 1 and not h.value
         return
     if case == "interface_not_node1":
@@ -225,4 +237,26 @@ def test_state_checkpoint_round_trip():
     g.set_state(ck)
     b = run()
     assert a == b
+    g.close()
+
+
+def test_volume_tracking_component_with_fixed_flow():
+    """A volume-tracking component whose flow is prescribed integrates its
+    volume (V = V_hist + Delt q), beside a pressure chamber on the outlet."""
+    spec = NetlistBC(srfid=3, components=[("r", 1, 2, 100.0), ("v", 2, 3, 2000.0), ("t", 2, 4, 0.0),
+                                          ("r", 2, 5, 700.0)],
+                     prescribed_pressures={3: 0.0, 4: 0.0, 5: 0.0}, prescribed_flows={3: 0.5},
+                     interface_component=1, initial_pressures={2: 40.0},
+                     volumes={2: (30.0, 10.0), 3: (5.0, 0.0)})
+    g, o = Netlist(spec), OracleNetlist(spec)
+    for step in range(6):
+        assert _close(g.implicit_coefficients(ALFI * DT), o.implicit_coefficients(ALFI * DT), 1e-12)
+        g.update(DT, 12.0)
+        o.update(DT, 12.0)
+        p, f, _, vol = g.get()
+        assert _close(vol[2], 5.0 + (step + 1) * DT * 0.5, 1e-12)
+        assert _close(p[1], (vol[1] - 10.0) * 2000.0, 1e-12)
+        assert _close(p, [o.pressure(i + 1) for i in range(len(p))], 1e-12)
+        g.finalize_step()
+        o.finalize_step()
     g.close()
