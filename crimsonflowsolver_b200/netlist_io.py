@@ -1,0 +1,168 @@
+"""Readers of the reference's netlist input files into :class:`NetlistBC`.
+
+Two formats, as the reference reads them:
+
+* ``netlist_surfaces.dat`` (NetlistReader, flowsolver/src/fileReaders.cxx:
+  443-760): '#' lines and blank lines are skipped; per circuit the number of
+  components, then per component its type letter (r, c, i, d, t, v), start
+  node, end node and parameter (volume-tracking types add their initial
+  volume on the same line); the prescribed pressures (count, nodes, values,
+  types f/l), the prescribed flows (count, components, values, types f/t),
+  the initial pressures (count, then "node pressure" lines), the 3D
+  interface node, and the component and node control lists.
+* ``netlist_surfaces.xml`` (NetlistXmlReader, flowsolver/src/
+  NetlistXmlReader.cxx:30-460): ``netlistCircuits/circuit`` elements with
+  ``components/component`` (index, type, startNodeIndex, endNodeIndex,
+  parameterValue, initialVolume, initialUnstressedVolume,
+  prescribedFlowType, prescribedFlowValue) and ``nodes/node`` (index,
+  initialPressure, isAt3DInterface, prescribedPressureType; a fixed
+  pressure takes the node's initialPressure).
+
+Each circuit comes back as a dict; :func:`to_netlistbc` turns one into a
+:class:`NetlistBC` for a coupled surface, and raises for what the library
+does not model (left-ventricular pressures, control scripts, an interface
+node other than 1).
+"""
+from __future__ import annotations
+
+import xml.etree.ElementTree as ET
+from typing import Dict, List
+
+from .problem import NetlistBC
+
+_DAT_KINDS = {"r": "r", "c": "c", "i": "l", "d": "d", "t": "t", "v": "v"}
+_XML_KINDS = {"resistor": "r", "capacitor": "c", "inductor": "l", "diode": "d", "volumetracking": "t",
+              "volumetrackingpressurechamber": "v"}
+
+
+def _dat_lines(text: str):
+    """The non-comment, non-blank lines split on whitespace."""
+    for line in text.splitlines():
+        s = line.strip()
+        if s and not s.startswith("#"):
+            yield s.split()
+
+
+def parse_netlist_dat(text: str) -> List[Dict]:
+    lines = _dat_lines(text)
+    out = []
+    for first in lines:
+        c: Dict = {"components": [], "volumes": {}, "prescribed_pressures": {}, "pressure_types": {},
+                   "prescribed_flows": {}, "flow_types": {}, "initial_pressures": {}, "controls": 0}
+        ncomp = int(first[0])
+        for j in range(ncomp):
+            kind = next(lines)[0]
+            if kind not in _DAT_KINDS:
+                raise ValueError(f"unknown netlist component type {kind!r}")
+            st = int(next(lines)[0])
+            en = int(next(lines)[0])
+            par = next(lines)
+            c["components"].append((_DAT_KINDS[kind], st, en, float(par[0])))
+            if kind in ("t", "v"):
+                if len(par) < 2:
+                    raise ValueError("a volume-tracking component needs its initial volume")
+                c["volumes"][j + 1] = (float(par[1]), 0.0)
+        npp = int(next(lines)[0])
+        nodes = [int(next(lines)[0]) for _ in range(npp)]
+        vals = [float(next(lines)[0]) for _ in range(npp)]
+        types = [next(lines)[0] for _ in range(npp)]
+        for nd, v, t in zip(nodes, vals, types):
+            c["prescribed_pressures"][nd] = v
+            c["pressure_types"][nd] = t
+        npf = int(next(lines)[0])
+        comps = [int(next(lines)[0]) for _ in range(npf)]
+        vals = [float(next(lines)[0]) for _ in range(npf)]
+        types = [next(lines)[0] for _ in range(npf)]
+        for j, v, t in zip(comps, vals, types):
+            c["prescribed_flows"][j] = v
+            c["flow_types"][j] = t
+        nn = int(next(lines)[0])
+        for _ in range(nn):
+            t = next(lines)
+            c["initial_pressures"][int(t[0])] = float(t[1])
+        # older files end here: interface node 1, no controls
+        t = next(lines, None)
+        c["interface_node"] = int(t[0]) if t is not None else 1
+        for _ in range(2 if t is not None else 0):  # component controls, then node controls
+            k = int(next(lines)[0])
+            for _ in range(k):
+                next(lines)
+            c["controls"] += k
+        out.append(c)
+    return out
+
+
+def _text(el, tag, default=None):
+    e = el.find(tag)
+    return e.text.strip() if e is not None and e.text is not None else default
+
+
+def parse_netlist_xml(text: str) -> List[Dict]:
+    root = ET.fromstring(text)
+    out = []
+    for circ in root.findall("circuit"):
+        c: Dict = {"components": [], "volumes": {}, "prescribed_pressures": {}, "pressure_types": {},
+                   "prescribed_flows": {}, "flow_types": {}, "initial_pressures": {}, "controls": 0,
+                   "interface_node": None}
+        for j, comp in enumerate(circ.find("components").findall("component")):
+            kind = _text(comp, "type").lower()
+            if kind not in _XML_KINDS:
+                raise ValueError(f"unknown netlist component type {kind!r}")
+            k = _XML_KINDS[kind]
+            c["components"].append((k, int(_text(comp, "startNodeIndex")), int(_text(comp, "endNodeIndex")),
+                                    float(_text(comp, "parameterValue"))))
+            if k in ("t", "v"):
+                v0 = _text(comp, "initialVolume")
+                if v0 is None:
+                    raise ValueError("a volume-tracking component needs its initial volume")
+                c["volumes"][j + 1] = (float(v0), float(_text(comp, "initialUnstressedVolume", "0")))
+            ft = _text(comp, "prescribedFlowType")
+            if ft is not None:
+                t = {"fixed": "f", "threedinterface": "t"}[ft.lower()]
+                c["prescribed_flows"][j + 1] = float(_text(comp, "prescribedFlowValue", "-1")) if t == "f" else -1.0
+                c["flow_types"][j + 1] = t
+            c["controls"] += len(comp.findall("control"))
+        for node in circ.find("nodes").findall("node"):
+            idx = int(_text(node, "index"))
+            p0 = float(_text(node, "initialPressure"))
+            c["initial_pressures"][idx] = p0
+            if (_text(node, "isAt3DInterface") or "").lower() == "true":
+                c["interface_node"] = idx
+            pt = _text(node, "prescribedPressureType")
+            if pt is not None:
+                t = {"fixed": "f", "leftventricular": "l"}[pt.lower()]
+                c["prescribed_pressures"][idx] = p0 if t == "f" else 1.0
+                c["pressure_types"][idx] = t
+            c["controls"] += len(node.findall("control"))
+        out.append(c)
+    return out
+
+
+def to_netlistbc(circuit: Dict, srfid: int, ignore_controls: bool = False) -> NetlistBC:
+    """One parsed circuit as the outlet of surface ``srfid``.  Circuits with
+    control scripts raise, unless ``ignore_controls`` asks for the circuit
+    with its parameters held at their input values."""
+    if circuit["controls"] and not ignore_controls:
+        raise NotImplementedError("netlist control scripts are not supported")
+    if any(t != "f" for t in circuit["pressure_types"].values()):
+        raise NotImplementedError("only fixed nodal pressures are supported")
+    if circuit.get("interface_node") not in (None, 1):
+        raise NotImplementedError("the 3D interface node must be node 1")
+    iface = [j for j, t in circuit["flow_types"].items() if t == "t"]
+    if len(iface) != 1:
+        raise ValueError("exactly one component must carry the 3D interface flow")
+    fixed_flows = {j: v for j, v in circuit["prescribed_flows"].items() if circuit["flow_types"][j] == "f"}
+    return NetlistBC(srfid=srfid, components=list(circuit["components"]),
+                     prescribed_pressures=dict(circuit["prescribed_pressures"]), prescribed_flows=fixed_flows,
+                     interface_component=iface[0], initial_pressures=dict(circuit["initial_pressures"]),
+                     volumes=dict(circuit["volumes"]))
+
+
+def read_netlists(path: str, srfids: List[int]) -> List[NetlistBC]:
+    """Read a netlist_surfaces.dat or .xml; circuit k couples surface srfids[k]."""
+    with open(path) as f:
+        text = f.read()
+    circuits = parse_netlist_xml(text) if path.endswith(".xml") else parse_netlist_dat(text)
+    if len(circuits) != len(srfids):
+        raise ValueError(f"{len(circuits)} circuits in {path}, {len(srfids)} surfaces given")
+    return [to_netlistbc(c, s) for c, s in zip(circuits, srfids)]
