@@ -399,6 +399,23 @@ def run_ours(args):
            "after_steps": args.warmup + args.steps}
     value = replica_value(tm_ms, args.steps, ws)
     v64 = replica_value(t64_ms, args.steps, ws)
+    # ---- mixed with FP32 element quadrature of the tangent (the mixed mode's
+    # second form), same steps from the same state ----
+    Pt = FlowParams(**{**Pm.__dict__, "precision": "mixed_f32_tangent"})
+    FT = solver.FlowSolver(m, Pt, inflow=_inflow)
+    st_ = torch.cuda.ExternalStream(FT.elm.stream_handle)
+    tt_ms, itt, _, _ = _timed_steps(FT, args, st_, local, dist)
+    yt, _ = FT.state()
+    FT.close()
+    del FT
+    vt = replica_value(tt_ms, args.steps, ws)
+    f32_tangent = {"value": vt, "unit": "s/timestep", "speedup_vs_fp64": v64 / vt,
+                   "rel_err_vs_fp64": {"velocity": _relerr(yt[:, 0:3], y64[:, 0:3]),
+                                       "pressure": _relerr(yt[:, 3], y64[:, 3]),
+                                       "outlet_pressure": _relerr(np.array(itt["outlet_p"]),
+                                                                  np.array(it64["outlet_p"])),
+                                       "after_steps": args.warmup + args.steps},
+                   "solver_iters_per_solve": itt}
     # ---- end to end through the host-buffer API: state in from pinned host, step, state out ----
     def end_to_end(FS, stream):
         y_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
@@ -484,6 +501,7 @@ def run_ours(args):
                  "solver_iters_per_solve": it64, "gpu_launches": l64, "clocks": clk64},
         "mixed_speedup_vs_fp64": v64 / value,
         "mixed_rel_err_vs_fp64": acc,
+        "mixed_f32_tangent": f32_tangent,
         "solver_iters_per_solve": itm,
         "assembly_melem_s": m.nelem / t_asm / 1e6,
         "assembly_ms": t_asm * 1e3,
