@@ -704,6 +704,67 @@ def run_microbench(args):
     print(json.dumps(out), flush=True)
 
 
+def run_scale(args):
+    """Large-mesh run, one arm at a time (both at once would not fit beyond
+    ~45M tets): mesh from --ncross / --naxial (170 x 290 gives 39.5M tets),
+    one warm-up step and one timed step per arm, device memory of each arm,
+    the CG iteration time against its algorithmic bytes (columns streamed
+    when they do not fit in shared memory), mixed vs FP64."""
+    import ctypes
+
+    import torch
+
+    from crimsonflowsolver_b200 import FlowParams
+    from crimsonflowsolver_b200 import _native as N
+    from crimsonflowsolver_b200 import solver
+
+    L = N.lib()
+    t0 = time.perf_counter()
+    m, P = make_problem(args.ncross, args.naxial, args.epstol_ns)
+    gen_s = time.perf_counter() - t0
+    peaks = _peaks()
+    free0, total = torch.cuda.mem_get_info()
+    out = {"workload": workload_name(args, m), "tets": m.nelem, "nodes": m.nshg, "mesh_generation_s": gen_s,
+           "device_memory_gb": total / 1e9}
+    y64 = None
+    for prec in ("fp64", "mixed"):
+        Pp = FlowParams(**{**P.__dict__, "precision": prec, "max_refine": 8, "refine_tol": args.refine_tol})
+        F = solver.FlowSolver(m, Pp, inflow=_inflow)
+        F.step()
+        s = torch.cuda.ExternalStream(F.elm.stream_handle)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(s)
+        st = F.step()
+        e1.record(s)
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        ms = ctypes.c_double()
+        N.check(L.crimson_memls_kernel_time(F.memls.lhs, 1 if prec == "fp64" else 4, 1, ctypes.byref(ms)), "kt")
+        r64, r32, rb = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        N.check(L.crimson_memls_cg_layout(F.memls.lhs, ctypes.byref(r64), ctypes.byref(r32), ctypes.byref(rb)),
+                "cg_layout")
+        resident = bool(r64.value if prec == "fp64" else r32.value)
+        nnz = F.elm._nnz()
+        byt = cg_iter_bytes(nnz, m.nshg, 8 if prec == "fp64" else 4, len(P.rcr), resident)
+        y, _ = F.state()
+        if y64 is None:
+            y64 = y
+        out[prec] = {"step_s": e0.elapsed_time(e1) / 1e3, "device_memory_used_gb": (free0 - free1) / 1e9,
+                     "cg_iter_ms": ms.value, "cg_columns_resident": resident,
+                     "cg_algorithmic_bytes_per_iter": byt, "cg_achieved_gbs": byt / ms.value / 1e6,
+                     "cg_frac": byt / ms.value / 1e6 / peaks[0],
+                     "iters_per_solve": [(st.ri_itr[i], st.gm_itr[i], st.cg_itr[i]) for i in range(st.nsolves)],
+                     "rel_err_vs_fp64": _relerr(y, y64)}
+        F.close()
+        del F
+        torch.cuda.synchronize()
+    out["mixed_speedup_vs_fp64"] = out["fp64"]["step_s"] / out["mixed"]["step_s"]
+    out["peak_source"] = peaks[1]
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -732,6 +793,8 @@ def main():
                     help="run the adjoint-gradient workload (multi-outlet cylinder) instead of the benchmark")
     ap.add_argument("--adj-steps", type=int, default=100, help="--adjoint only")
     ap.add_argument("--adj-fd", default="0,1", help="--adjoint only: theta components checked by central FD")
+    ap.add_argument("--scale", action="store_true",
+                    help="large-mesh run of the cylinder, one arm at a time (e.g. --ncross 170 --naxial 290)")
     args = ap.parse_args()
     if args.refine_tol is None:
         args.refine_tol = 1e-8 if args.workload == "ybif" else REFINE_TOL
@@ -741,6 +804,8 @@ def main():
         run_adjoint(args)
     elif args.microbench:
         run_microbench(args)
+    elif args.scale:
+        run_scale(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
