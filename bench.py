@@ -625,7 +625,9 @@ def run_microbench(args):
     ~ N(0, 1) (seeded).  Measures ElmGMR residual + tangent assembly (Melem/s)
     and the 4x4 block SpMV (SPARMULVV, dof 4) on the assembled pattern with
     N(0, 1) blocks, FP64 and FP32, each against the HBM roofline, with CUDA
-    events on the library stream.
+    events on the library stream.  Also ElmGMRSclr (scalar residual +
+    tangent, 768 algorithmic B/elem: gathers 352 + rows 32 + tangent 128 of
+    the interior pass, 256 of the flux projection) on the same mesh.
     """
     import ctypes
 
@@ -685,6 +687,21 @@ def run_microbench(args):
                                      "achieved_gbs": asm32_bytes / t_asm32 / 1e9,
                                      "frac": asm32_bytes / t_asm32 / 1e9 / peak},
            "residual_only_fp64": {"ms": t_res * 1e3, "melem_s": m.nelem / t_res / 1e6}}
+    # ElmGMRSclr on the same mesh: scalar and rate ~ N(0, 1), diffusivity 0.1
+    gs = torch.Generator(device=dev).manual_seed(6)
+    ds = torch.randn(n, dtype=torch.float64, device=dev, generator=gs)
+    dsd = torch.randn(n, dtype=torch.float64, device=dev, generator=gs)
+    rs = torch.empty(n, dtype=torch.float64, device=dev)
+    del K, Pm
+    S = torch.empty(nnz, dtype=torch.float64, device=dev)
+    t_s = timed(lambda: elm.sclr_device(dy, ds, dsd, rs, S, isclr=1, diffus=0.1), 5)
+    t_sr = timed(lambda: elm.sclr_device(dy, ds, dsd, rs, None, isclr=1, diffus=0.1, lhs=False), 5)
+    sclr_bytes = 768 * m.nelem
+    out["assembly_sclr_fp64"] = {"ms": t_s * 1e3, "melem_s": m.nelem / t_s / 1e6,
+                                 "algorithmic_bytes_per_elem": 768, "achieved_gbs": sclr_bytes / t_s / 1e9,
+                                 "frac": sclr_bytes / t_s / 1e9 / peak,
+                                 "residual_only_ms": t_sr * 1e3}
+    del ds, dsd, rs, S
     g = torch.Generator(device=dev).manual_seed(5)
     val = torch.randn((nnz, 16), dtype=torch.float64, device=dev, generator=g)
     u = torch.randn((n, 4), dtype=torch.float64, device=dev, generator=g)

@@ -68,6 +68,10 @@ SIGNATURES = {
                                       ctypes.c_int]),
     "crimson_elmgmr_device": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_dbl_p, c_dbl_p, c_void_p, c_void_p,
                                              c_void_p, ctypes.c_int]),
+    "crimson_elmgmr_sclr": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_double, c_dbl_p, c_dbl_p, c_dbl_p,
+                                           c_dbl_p, c_dbl_p, c_dbl_p, ctypes.c_int]),
+    "crimson_elmgmr_sclr_device": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_double, c_void_p, c_void_p,
+                                                  c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int]),
     "crimson_memls_ls_create": (ctypes.c_int, [ctypes.POINTER(c_void_p), ctypes.c_int, ctypes.c_int,
                                                ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                                c_dbl_p, c_dbl_p, c_int_p]),

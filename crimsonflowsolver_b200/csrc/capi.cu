@@ -29,6 +29,8 @@ int sm_count() {
 
 int build_pattern(crimson_ctx* c);
 int pattern_aux(crimson_lhs* L);
+int elmgmr_sclr_device(crimson_ctx* c, int isclr, double diffus, const double* d_y, const double* d_s,
+                       const double* d_sdot, const double* d_bcbs, double* d_res, double* d_lhsS, int lhs);
 int memls_kernel_time(crimson_lhs* L, int which, int reps, double* ms);
 int pattern_to_host(crimson_ctx* c, int* colm, int* rowp, long long cap);
 int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const double* coef1, const double* coef2,
@@ -326,6 +328,7 @@ int crimson_set_boundary(crimson_ctx* c, int nface, const int* ienb, const int* 
     }
     CR_CHECK(c->ienb.upload(hb.data(), hb.size(), c->stream));
     CR_CHECK(c->iBCB.upload(hbits.data(), hbits.size(), c->stream));
+    c->h_iBCB = hbits;
     CR_CHECK(c->BCB.upload(hbcb.data(), hbcb.size(), c->stream));
     // boundary elements (all four nodes) at each node: bc3LHS puts 1 on the
     // constrained diagonal entries of a partially constrained node once per
@@ -419,6 +422,58 @@ int crimson_elmgmr(crimson_ctx* c, const double* y, const double* ac, const doub
         CR_CUDA(cudaMemcpyAsync(lhsP, c->lhsP.p, sizeof(double) * 4 * (size_t)c->nnz, cudaMemcpyDeviceToHost, s));
     }
     CR_CUDA(cudaStreamSynchronize(s));
+    return CRIMSON_OK;
+}
+
+int crimson_elmgmr_sclr_device(crimson_ctx* c, int isclr, double diffus, const double* d_y, const double* d_s,
+                               const double* d_sdot, const double* d_bcbs, double* d_res, double* d_lhsS, int lhs) {
+    if (!c) return CRIMSON_ERR_ARG;
+    CR_CHECK(check_params(&c->p));
+    if (c->p.flmpl != 0.0 || c->p.flmpr != 0.0 || (c->p.idiff != 0 && c->p.idiff != 1)) {
+        set_last_error("ElmGMRSclr: lumped mass fractions and idiff other than 0 or 1 are not supported");
+        return CRIMSON_ERR_UNSUPPORTED;
+    }
+    if (!d_bcbs && isclr >= 1 && isclr <= 4)
+        for (int f = 0; f < (int)c->h_iBCB.size(); ++f)
+            if ((c->h_iBCB[f] >> (4 + isclr)) & 1) {
+                set_last_error("ElmGMRSclr: a face prescribes the scalar flux (iBCB bit 4+isclr) but bcbs is NULL");
+                return CRIMSON_ERR_ARG;
+            }
+    return elmgmr_sclr_device(c, isclr, diffus, d_y, d_s, d_sdot, d_bcbs, d_res, d_lhsS, lhs);
+}
+
+int crimson_elmgmr_sclr(crimson_ctx* c, int isclr, double diffus, const double* y, const double* s,
+                        const double* sdot, const double* bcbs, double* res, double* lhsS, int lhs) {
+    if (!c || !y || !s || !sdot || !res || (lhs && !lhsS)) return CRIMSON_ERR_ARG;
+    if (c->nnz == 0) CR_CHECK(build_pattern(c));
+    cudaStream_t st = c->stream;
+    const int n = c->nshg;
+    const int nf = c->nface;
+    CR_CHECK(c->y4.alloc(4 * (size_t)n));
+    CR_CHECK(c->sclr_in.alloc(4 * (size_t)n + 3 * (size_t)std::max(nf, 1)));
+    CR_CHECK(c->sclr_res.alloc((size_t)n));
+    if (lhs) CR_CHECK(c->sclr_lhs.alloc((size_t)c->nnz));
+    double* d_stage = c->sclr_in.p;  // y (reference layout), then s, sdot, bcbs
+    CR_CUDA(cudaMemcpyAsync(d_stage, y, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, st));
+    launch(k_soa_to_node4, grid_for(n, 256), 256, 0, st, (const double*)d_stage, n, n, c->y4.p);
+    CR_CUDA(cudaStreamSynchronize(st));
+    CR_CUDA(cudaMemcpyAsync(d_stage, s, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    CR_CUDA(cudaMemcpyAsync(d_stage + n, sdot, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    double* d_b = nullptr;
+    if (bcbs && nf > 0) {
+        // reference layout (nface, 3) -> face-major
+        std::vector<double> hb(3 * (size_t)nf);
+        for (int f = 0; f < nf; ++f)
+            for (int k = 0; k < 3; ++k) hb[3 * (size_t)f + k] = bcbs[(size_t)k * nf + f];
+        d_b = d_stage + 2 * (size_t)n;
+        CR_CUDA(cudaMemcpyAsync(d_b, hb.data(), sizeof(double) * hb.size(), cudaMemcpyHostToDevice, st));
+        CR_CUDA(cudaStreamSynchronize(st));
+    }
+    CR_CHECK(crimson_elmgmr_sclr_device(c, isclr, diffus, c->y4.p, d_stage, d_stage + n, d_b, c->sclr_res.p,
+                                        lhs ? c->sclr_lhs.p : nullptr, lhs));
+    CR_CUDA(cudaMemcpyAsync(res, c->sclr_res.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    if (lhs) CR_CUDA(cudaMemcpyAsync(lhsS, c->sclr_lhs.p, sizeof(double) * (size_t)c->nnz, cudaMemcpyDeviceToHost, st));
+    CR_CUDA(cudaStreamSynchronize(st));
     return CRIMSON_OK;
 }
 

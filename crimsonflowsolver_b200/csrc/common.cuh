@@ -159,6 +159,7 @@ struct crimson_ctx {
     crimson::DBuf<int> fnoff;       // (nshg+1) offsets into flist per node
     crimson::DBuf<int> flist;       // (3 nface) codes 3f + n of the faces at each node, ascending f
     crimson::DBuf<double> frec;     // (nface, 12) face residual records: rl(n, 0:3) of face node n
+    std::vector<int> h_iBCB;        // (nface) flag bits, host copy
     crimson::DBuf<int> bcount;      // (nshg) boundary elements (all 4 nodes) containing each node
 
     // coupled outlets
@@ -194,6 +195,13 @@ struct crimson_ctx {
     crimson::DBuf<double> y4, ac4, res4;   // (4, nshg) staging for host-pointer calls
     crimson::DBuf<double> lhsK, lhsP;      // (9, nnz), (4, nnz)
     crimson::DBuf<float> lhs32;            // (16, nnz) FP32 tangent records (mixed precision)
+
+    // ElmGMRSclr work space (scalar advection-diffusion)
+    crimson::DBuf<double> sclr_qres;       // (nshg, 3) projected diffusive flux, node-major
+    crimson::DBuf<double> sclr_qrec;       // (nelem, 16) projection records
+    crimson::DBuf<double> sclr_erec;       // (nelem, 20) rl(4) + xSebe(4, 4)
+    crimson::DBuf<double> sclr_frec;       // (nface, 3) boundary flux terms
+    crimson::DBuf<double> sclr_in, sclr_res, sclr_lhs;  // staging for host-pointer calls
 
     // time stepping state (crimson_step)
     crimson::DBuf<double> yold, acold, ycur, accur, yalpha, acalpha, solinc, stage;

@@ -1,0 +1,471 @@
+// ElmGMRSclr on the device (flowsolver/src/elmgmr.f90:599-822): residual and
+// tangent of the advection-diffusion equation of one scalar, assembled with
+// the same deterministic owner-computes scheme as ElmGMR.
+//
+//   k_sclr_q      AsIqSclr / e3qSclr (asiq.f90:89-125, e3q.f90:215-300): per
+//                 element the lumped-projection contributions of q =
+//                 diffus grad S and of the lumped mass, per quadrature point
+//   k_sclr_qnode  their sums per node in ascending element order, then
+//                 qpbcSclr (qpbc.f90:118-175): qres = q / rmass
+//   k_sclr_elem   AsIGMRSclr / e3Sclr (asigmr.f90:141-190, e3.f90:183-330):
+//                 per element the residual rows rl(a) and the 4x4 tangent
+//                 xSebe (e3ivarSclr, e3StabSclr, e3ResSclr, e3LHSSclr)
+//   k_sclr_face   AsBSclr / e3bSclr (asbmfg.f90:114-150, e3b.f90:626-720):
+//                 the boundary flux term of each face node
+//   k_sclr_node   per node: residual row (elements, then faces) and the
+//                 diagonal tangent entry; bc3ResSclr (bc3res.f90:138-160)
+//   k_sclr_slot   per off-diagonal CSR entry: fillsparseSclr's sum
+//                 (fillsparse.f90:167-200) in ascending element order
+//
+// Settings as the reference's defaults for a passive scalar: diffusivity
+// scdiff(isclr) (getdiff.f90:145-174), the flow velocity as convection
+// velocity (consrv_sclr_conv_vel = 0), SUPG (ivart = 2), no discontinuity
+// capturing (idcsclr = 0), no source terms (nosource = 1: with nosource = 0
+// the reference reads uninitialised source arrays, its source call being
+// commented out, e3ivar.f90:670-680), Navier = 1, linear tets.
+#include "common.cuh"
+
+namespace crimson {
+
+int build_pattern(crimson_ctx* c);
+
+namespace {
+
+// Quadrature tables built on the host with the oracle's arithmetic
+// (symtet.c / genint.f90:85 interior rule, symtri.c through genshpb.f90
+// boundary rule, shape gradients halved as genshp.f90:35-36).
+struct SclrTables {
+    double shp[4][4];    // [intp][n]
+    double shgl[3][4];   // [dir][n], the same at every point of a linear tet
+    double Qwt[4];
+    double shpb[3][4];   // boundary points
+    double Qwtb[3];
+};
+
+SclrTables sclr_tables() {
+    SclrTables t;
+    const double A4 = 0.5854101966249685, B4 = 0.1381966011250150;
+    const double r4[4][3] = {{A4, B4, B4}, {B4, A4, B4}, {B4, B4, A4}, {B4, B4, B4}};
+    for (int q = 0; q < 4; ++q) {
+        t.shp[q][0] = r4[q][0];
+        t.shp[q][1] = r4[q][1];
+        t.shp[q][2] = r4[q][2];
+        t.shp[q][3] = 1.0e0 - r4[q][0] - r4[q][1] - r4[q][2];
+        t.Qwt[q] = (4.0 / 3.0) * 0.25;
+    }
+    for (int j = 0; j < 3; ++j)
+        for (int n = 0; n < 4; ++n) t.shgl[j][n] = (n == 3 ? -1.0e0 : (n == j ? 1.0e0 : 0.0e0)) / 2.0;
+    const double B3 = 0.666666666666667, C3 = 0.166666666666667, A3 = 0.3333333333333330000000000000000000;
+    const double r3[3][3] = {{B3, C3, C3}, {C3, B3, C3}, {C3, C3, B3}};
+    for (int q = 0; q < 3; ++q) {
+        t.shpb[q][0] = r3[q][0];
+        t.shpb[q][1] = r3[q][1];
+        t.shpb[q][2] = r3[q][2];
+        t.shpb[q][3] = 1.0e0 - r3[q][0] - r3[q][1] - r3[q][2];
+        t.Qwtb[q] = 2.0 * A3;
+    }
+    return t;
+}
+
+struct SclrParams {
+    double alfi, almi, gami, Delt, Dtgl, dtsfct, diffus;
+    int idiff, isclr, lhs;
+};
+
+// e3metric (e3metric.f90:26-81) for a linear tet
+__device__ __forceinline__ void sclr_metric(const double xl[4][3], const double shgl[3][4], double Qwt,
+                                            double dxidx[3][3], double shg[4][3], double* W) {
+    double d[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) d[i][j] = d[i][j] + xl[n][i] * shgl[j][n];
+    dxidx[0][0] = d[1][1] * d[2][2] - d[2][1] * d[1][2];
+    dxidx[0][1] = d[2][1] * d[0][2] - d[0][1] * d[2][2];
+    dxidx[0][2] = d[0][1] * d[1][2] - d[0][2] * d[1][1];
+    const double tmp = 1.0 / (dxidx[0][0] * d[0][0] + dxidx[0][1] * d[1][0] + dxidx[0][2] * d[2][0]);
+    dxidx[0][0] = dxidx[0][0] * tmp;
+    dxidx[0][1] = dxidx[0][1] * tmp;
+    dxidx[0][2] = dxidx[0][2] * tmp;
+    dxidx[1][0] = (d[1][2] * d[2][0] - d[1][0] * d[2][2]) * tmp;
+    dxidx[1][1] = (d[0][0] * d[2][2] - d[2][0] * d[0][2]) * tmp;
+    dxidx[1][2] = (d[1][0] * d[0][2] - d[0][0] * d[1][2]) * tmp;
+    dxidx[2][0] = (d[1][0] * d[2][1] - d[1][1] * d[2][0]) * tmp;
+    dxidx[2][1] = (d[2][0] * d[0][1] - d[0][0] * d[2][1]) * tmp;
+    dxidx[2][2] = (d[0][0] * d[1][1] - d[0][1] * d[1][0]) * tmp;
+    *W = Qwt / tmp;
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            shg[n][k] = shgl[0][n] * dxidx[0][k] + shgl[1][n] * dxidx[1][k] + shgl[2][n] * dxidx[2][k];
+}
+
+// e3gijd, tet branch (e3stab.f90:487-528)
+__device__ __forceinline__ void sclr_gijd(const double dx[3][3], double g[6]) {
+    const double c1 = 1.259921049894873e+00, c2 = 6.299605249474365e-01;
+    double t1 = c1 * dx[0][0] + c2 * (dx[1][0] + dx[2][0]);
+    double t2 = c1 * dx[1][0] + c2 * (dx[0][0] + dx[2][0]);
+    double t3 = c1 * dx[2][0] + c2 * (dx[0][0] + dx[1][0]);
+    g[0] = dx[0][0] * t1 + dx[1][0] * t2 + dx[2][0] * t3;
+    t1 = c1 * dx[0][1] + c2 * (dx[1][1] + dx[2][1]);
+    t2 = c1 * dx[1][1] + c2 * (dx[0][1] + dx[2][1]);
+    t3 = c1 * dx[2][1] + c2 * (dx[0][1] + dx[1][1]);
+    g[1] = dx[0][1] * t1 + dx[1][1] * t2 + dx[2][1] * t3;
+    g[3] = dx[0][0] * t1 + dx[1][0] * t2 + dx[2][0] * t3;
+    t1 = c1 * dx[0][2] + c2 * (dx[1][2] + dx[2][2]);
+    t2 = c1 * dx[1][2] + c2 * (dx[0][2] + dx[2][2]);
+    t3 = c1 * dx[2][2] + c2 * (dx[0][2] + dx[1][2]);
+    g[2] = dx[0][2] * t1 + dx[1][2] * t2 + dx[2][2] * t3;
+    g[4] = dx[0][1] * t1 + dx[1][1] * t2 + dx[2][1] * t3;
+    g[5] = dx[0][0] * t1 + dx[1][0] * t2 + dx[2][0] * t3;
+}
+
+__device__ __forceinline__ void sclr_gather_x(const int4 nn, const double4* __restrict__ x, double xl[4][3]) {
+    const int nd[4] = {nn.x, nn.y, nn.z, nn.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const double4 v = x[nd[a]];
+        xl[a][0] = v.x;
+        xl[a][1] = v.y;
+        xl[a][2] = v.z;
+    }
+}
+
+// Element records of the flux projection: ql(a, 0:3) and rmassl(a), 16 doubles.
+__global__ void __launch_bounds__(128) k_sclr_q(const int4* __restrict__ ien, const double4* __restrict__ x,
+                                                const double* __restrict__ s, int nelem, SclrTables T, SclrParams P,
+                                                double* __restrict__ qrec) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
+        const int4 nn = ien[e];
+        double xl[4][3];
+        sclr_gather_x(nn, x, xl);
+        const double sl[4] = {s[nn.x], s[nn.y], s[nn.z], s[nn.w]};
+        double ql[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, rm[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            double dxidx[3][3], shg[4][3], W;
+            sclr_metric(xl, T.shgl, T.Qwt[q], dxidx, shg, &W);
+            double gT[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int n = 0; n < 4; ++n)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) gT[k] = gT[k] + shg[n][k] * sl[n];
+            const double qdi[3] = {P.diffus * gT[0], P.diffus * gT[1], P.diffus * gT[2]};
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) ql[i][k] = ql[i][k] + T.shp[q][i] * W * qdi[k];
+                rm[i] = rm[i] + T.shp[q][i] * W;
+            }
+        }
+        double4* r = reinterpret_cast<double4*>(qrec + 16 * (size_t)e);
+        r[0] = make_double4(ql[0][0], ql[0][1], ql[0][2], ql[1][0]);
+        r[1] = make_double4(ql[1][1], ql[1][2], ql[2][0], ql[2][1]);
+        r[2] = make_double4(ql[2][2], ql[3][0], ql[3][1], ql[3][2]);
+        r[3] = make_double4(rm[0], rm[1], rm[2], rm[3]);
+    }
+}
+
+// Per node: the projection sums over the elements containing it (the
+// contributions of its diagonal slot, ascending element order), then
+// qres = (1 / rmass) q.
+__global__ void __launch_bounds__(256) k_sclr_qnode(const int* __restrict__ diag, const int* __restrict__ soff,
+                                                    const int* __restrict__ slist, const double* __restrict__ qrec,
+                                                    int nshg, double* __restrict__ qres) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
+        const int d = diag[i];
+        double q0 = 0.0, q1 = 0.0, q2 = 0.0, m = 0.0;
+        const int p1 = soff[d + 1];
+        for (int p = soff[d]; p < p1; ++p) {
+            const int t = slist[p];
+            const int e = t >> 4, a = (t >> 2) & 3;
+            const double* r = qrec + 16 * (size_t)e;
+            q0 += r[3 * a];
+            q1 += r[3 * a + 1];
+            q2 += r[3 * a + 2];
+            m += r[12 + a];
+        }
+        const double rinv = 1.0 / m;
+        qres[3 * (size_t)i] = rinv * q0;
+        qres[3 * (size_t)i + 1] = rinv * q1;
+        qres[3 * (size_t)i + 2] = rinv * q2;
+    }
+}
+
+// e3Sclr per element: record = rl(0:4) then xSebe(a, b) at 4 + 4 a + b (20 doubles).
+__global__ void __launch_bounds__(128) k_sclr_elem(const int4* __restrict__ ien, const double4* __restrict__ x,
+                                                   const double4* __restrict__ y, const double* __restrict__ s,
+                                                   const double* __restrict__ sdot, const double* __restrict__ qres,
+                                                   int nelem, SclrTables T, SclrParams P, double* __restrict__ erec) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
+        const int4 nn = ien[e];
+        const int nd[4] = {nn.x, nn.y, nn.z, nn.w};
+        double xl[4][3], ul[4][3], sl[4], sdl[4], ql[4][3];
+        sclr_gather_x(nn, x, xl);
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const double4 v = y[nd[a]];
+            ul[a][0] = v.x;
+            ul[a][1] = v.y;
+            ul[a][2] = v.z;
+            sl[a] = s[nd[a]];
+            sdl[a] = sdot[nd[a]];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) ql[a][k] = P.idiff >= 1 ? qres[3 * (size_t)nd[a] + k] : 0.0;
+        }
+        double rl[4] = {0, 0, 0, 0};
+        double xS[4][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+        const double lhsFct = P.alfi * P.gami * P.Delt;
+        const double dts = P.Dtgl * P.dtsfct;
+        for (int q = 0; q < 4; ++q) {
+            const double* shp = T.shp[q];
+            // e3ivarSclr
+            double u1 = 0.0, u2 = 0.0, u3 = 0.0;
+#pragma unroll
+            for (int n = 0; n < 4; ++n) {
+                u1 = u1 + shp[n] * ul[n][0];
+                u2 = u2 + shp[n] * ul[n][1];
+                u3 = u3 + shp[n] * ul[n][2];
+            }
+            double Sdot = 0.0;
+#pragma unroll
+            for (int n = 0; n < 4; ++n) Sdot = Sdot + shp[n] * sdl[n];
+            double dxidx[3][3], shg[4][3], W;
+            sclr_metric(xl, T.shgl, T.Qwt[q], dxidx, shg, &W);
+            double gS[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int n = 0; n < 4; ++n)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) gS[k] = gS[k] + shg[n][k] * sl[n];
+            double divS = 0.0;
+            if (P.idiff >= 1)
+#pragma unroll
+                for (int n = 0; n < 4; ++n)
+                    divS = divS + shg[n][0] * ql[n][0] + shg[n][1] * ql[n][1] + shg[n][2] * ql[n][2];
+            const double rLS = (Sdot + (u1 * gS[0] + u2 * gS[1] + u3 * gS[2])) - divS;
+            // e3StabSclr (ivart = 2, ipord = 1, no sources)
+            double g[6];
+            sclr_gijd(dxidx, g);
+            const double tauT = (2.0 * dts) * (2.0 * dts) + 0.0 * 0.0 + u1 * (g[0] * u1 + g[3] * u2 + g[5] * u3) +
+                                u2 * (g[3] * u1 + g[1] * u2 + g[4] * u3) + u3 * (g[5] * u1 + g[4] * u2 + g[2] * u3) +
+                                9.0 * (P.diffus * P.diffus) *
+                                    (g[0] * g[0] + g[1] * g[1] + g[2] * g[2] +
+                                     2.0 * (g[3] * g[3] + g[4] * g[4] + g[5] * g[5]));
+            const double tauS = 1.0 / sqrt(tauT);
+            // e3ResSclr (flmpr = 0)
+            const double rNa = 1.0 * (1.0 * Sdot + u1 * gS[0] + u2 * gS[1] + u3 * gS[2]) - 0.0;
+            const double tmp = 1.0 * tauS * (rLS - 0.0);
+            const double rG0 = P.diffus * gS[0] + u1 * tmp, rG1 = P.diffus * gS[1] + u2 * tmp,
+                         rG2 = P.diffus * gS[2] + u3 * tmp;
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+                rl[a] = rl[a] - W * (shp[a] * rNa + shg[a][0] * rG0 + shg[a][1] * rG1 + shg[a][2] * rG2);
+            if (!P.lhs) continue;
+            // e3LHSSclr (flmpl = 0, no sources)
+            const double tauSl = lhsFct * W * tauS;
+            const double kptmp = lhsFct * W * P.diffus;
+            const double tsFct = P.almi * W * 1.0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const double t1 = W * (u1 * shg[b][0] + u2 * shg[b][1] + u3 * shg[b][2]);
+                const double t2 = t1 * tauS;
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    xS[a][b] = xS[a][b] + shp[a] * shp[b] * (tsFct + 0.0) + shp[a] * lhsFct * t1;
+                    xS[b][a] = xS[b][a] + t2 * shp[a];
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const double tb = tauSl * (u1 * shg[b][0] + u2 * shg[b][1] + u3 * shg[b][2]);
+                const double t0 = kptmp * shg[b][0] + u1 * tb, t1 = kptmp * shg[b][1] + u2 * tb,
+                             t2 = kptmp * shg[b][2] + u3 * tb;
+                xS[b][b] = xS[b][b] + t0 * shg[b][0] + t1 * shg[b][1] + t2 * shg[b][2];
+#pragma unroll
+                for (int a = b + 1; a < 4; ++a) {
+                    const double v = t0 * shg[a][0] + t1 * shg[a][1] + t2 * shg[a][2];
+                    xS[a][b] = xS[a][b] + v;
+                    xS[b][a] = xS[b][a] + v;
+                }
+            }
+        }
+        double4* r = reinterpret_cast<double4*>(erec + 20 * (size_t)e);
+        r[0] = make_double4(rl[0], rl[1], rl[2], rl[3]);
+#pragma unroll
+        for (int a = 0; a < 4; ++a) r[1 + a] = make_double4(xS[a][0], xS[a][1], xS[a][2], xS[a][3]);
+    }
+}
+
+// e3bSclr per face: the flux term of face nodes 0..2 (frec 3 f + n).
+__global__ void __launch_bounds__(128) k_sclr_face(const int4* __restrict__ ienb, const int* __restrict__ iBCB,
+                                                   const double* __restrict__ bcbs, const double4* __restrict__ x,
+                                                   const double* __restrict__ s, int nface, SclrTables T,
+                                                   SclrParams P, double* __restrict__ frec) {
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nface; f += gridDim.x * blockDim.x) {
+        const int4 nn = ienb[f];
+        double xl[4][3];
+        sclr_gather_x(nn, x, xl);
+        const double sl[4] = {s[nn.x], s[nn.y], s[nn.z], s[nn.w]};
+        // the host entry checks that bcbs is given where a face prescribes the flux
+        const bool given = bcbs != nullptr && ((iBCB[f] >> (4 + P.isclr)) & 1);
+        double rl[3] = {0.0, 0.0, 0.0};
+        // the face metric and the gradient are those of the tet: constant
+        // over the face, evaluated at each of the 3 points as the reference does
+        for (int q = 0; q < 3; ++q) {
+            double d[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+            for (int n = 0; n < 4; ++n)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) d[i][j] = d[i][j] + xl[n][i] * T.shgl[j][n];
+            const double v1[3] = {xl[1][0] - xl[0][0], xl[1][1] - xl[0][1], xl[1][2] - xl[0][2]};
+            const double v2[3] = {xl[2][0] - xl[0][0], xl[2][1] - xl[0][1], xl[2][2] - xl[0][2]};
+            const double te1 = v1[1] * v2[2] - v2[1] * v1[2];
+            const double te2 = v2[0] * v1[2] - v1[0] * v2[2];
+            const double te3 = v1[0] * v2[1] - v2[0] * v1[1];
+            const double temp = 1.0 / sqrt(te1 * te1 + te2 * te2 + te3 * te3);
+            const double bn[3] = {te1 * temp, te2 * temp, te3 * temp};
+            const double WdetJb = T.Qwtb[q] / (4.0 * temp);
+            double flux;
+            if (given) {
+                flux = 0.0;
+#pragma unroll
+                for (int n = 0; n < 3; ++n) flux = flux + T.shpb[q][n] * bcbs[3 * (size_t)f + n];
+            } else {
+                double dx[3][3];
+                dx[0][0] = d[1][1] * d[2][2] - d[2][1] * d[1][2];
+                dx[0][1] = d[2][1] * d[0][2] - d[0][1] * d[2][2];
+                dx[0][2] = d[0][1] * d[1][2] - d[0][2] * d[1][1];
+                const double tmp = 1.0 / (dx[0][0] * d[0][0] + dx[0][1] * d[1][0] + dx[0][2] * d[2][0]);
+                dx[0][0] = dx[0][0] * tmp;
+                dx[0][1] = dx[0][1] * tmp;
+                dx[0][2] = dx[0][2] * tmp;
+                dx[1][0] = (d[1][2] * d[2][0] - d[1][0] * d[2][2]) * tmp;
+                dx[1][1] = (d[0][0] * d[2][2] - d[2][0] * d[0][2]) * tmp;
+                dx[1][2] = (d[1][0] * d[0][2] - d[0][0] * d[1][2]) * tmp;
+                dx[2][0] = (d[1][0] * d[2][1] - d[1][1] * d[2][0]) * tmp;
+                dx[2][1] = (d[2][0] * d[0][1] - d[0][0] * d[2][1]) * tmp;
+                dx[2][2] = (d[0][0] * d[1][1] - d[0][1] * d[1][0]) * tmp;
+                double gl[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                for (int n = 0; n < 4; ++n)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) gl[k] = gl[k] + T.shgl[k][n] * sl[n];
+                double gS[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) gS[k] = dx[0][k] * gl[0] + dx[1][k] * gl[1] + dx[2][k] * gl[2];
+                flux = P.diffus * (gS[0] * bn[0] + gS[1] * bn[1] + gS[2] * bn[2]);
+            }
+            const double rNa = -WdetJb * flux;
+#pragma unroll
+            for (int n = 0; n < 3; ++n) rl[n] = rl[n] - T.shpb[q][n] * rNa;
+        }
+#pragma unroll
+        for (int n = 0; n < 3; ++n) frec[3 * (size_t)f + n] = rl[n];
+    }
+}
+
+// Per node: residual row from its elements (ascending) and its boundary
+// faces (ascending), bc3ResSclr, and the diagonal tangent entry.
+__global__ void __launch_bounds__(256) k_sclr_node(const int* __restrict__ diag, const int* __restrict__ soff,
+                                                   const int* __restrict__ slist, const double* __restrict__ erec,
+                                                   const int* __restrict__ fnoff, const int* __restrict__ flist,
+                                                   const double* __restrict__ frec, int nshg,
+                                                   const int* __restrict__ iBC, int isclr, int lhs,
+                                                   double* __restrict__ res, double* __restrict__ lhsS) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
+        const int d = diag[i];
+        double r = 0.0, k = 0.0;
+        const int p1 = soff[d + 1];
+        for (int p = soff[d]; p < p1; ++p) {
+            const int t = slist[p];
+            const int e = t >> 4, a = (t >> 2) & 3;
+            const double* rec = erec + 20 * (size_t)e;
+            r += rec[a];
+            if (lhs) k += rec[4 + 5 * a];
+        }
+        if (fnoff) {
+            const int f1 = fnoff[i + 1];
+            for (int p = fnoff[i]; p < f1; ++p) r += frec[flist[p]];
+        }
+        if ((iBC[i] >> (isclr + 5)) & 1) r = 0.0;
+        res[i] = r;
+        if (lhs) lhsS[d] = k;
+    }
+}
+
+// Per off-diagonal CSR entry: the elements' xSebe(a, b) in ascending element order.
+__global__ void __launch_bounds__(256) k_sclr_slot(const int* __restrict__ soff, const int* __restrict__ slist,
+                                                   const double* __restrict__ erec, long long nnz,
+                                                   double* __restrict__ lhsS) {
+    for (long long sl = (long long)blockIdx.x * blockDim.x + threadIdx.x; sl < nnz;
+         sl += (long long)gridDim.x * blockDim.x) {
+        const int p0 = soff[sl], p1 = soff[sl + 1];
+        const int t0 = slist[p0];
+        if (((t0 >> 2) & 3) == (t0 & 3)) continue;
+        double k = 0.0;
+        for (int p = p0; p < p1; ++p) {
+            const int t = slist[p];
+            const int e = t >> 4, a = (t >> 2) & 3, b = t & 3;
+            k += erec[20 * (size_t)e + 4 + 4 * a + b];
+        }
+        lhsS[sl] = k;
+    }
+}
+
+}  // namespace
+
+// Device entry: d_y (4, nshg) node-major (u, v, w, p), d_s / d_sdot (nshg),
+// d_bcbs (nface, 3) face-major or null; d_res (nshg), d_lhsS (nnz).
+int elmgmr_sclr_device(crimson_ctx* c, int isclr, double diffus, const double* d_y, const double* d_s,
+                       const double* d_sdot, const double* d_bcbs, double* d_res, double* d_lhsS, int lhs) {
+    if (isclr < 1 || isclr > 4 || !(diffus >= 0.0) || !d_y || !d_s || !d_sdot || !d_res || (lhs && !d_lhsS))
+        return CRIMSON_ERR_ARG;
+    cudaStream_t s = c->stream;
+    if (c->nnz == 0) CR_CHECK(build_pattern(c));
+    if (!c->diag.p || !c->soff.p || !c->slist.p) return CRIMSON_ERR_STATE;
+    static const SclrTables T = sclr_tables();
+    SclrParams P;
+    P.alfi = c->p.alfi;
+    P.almi = c->p.almi;
+    P.gami = c->p.gami;
+    P.Delt = c->p.Delt;
+    P.Dtgl = c->p.Dtgl;
+    P.dtsfct = c->p.dtsfct;
+    P.diffus = diffus;
+    P.idiff = c->p.idiff;
+    P.isclr = isclr;
+    P.lhs = lhs ? 1 : 0;
+    CR_CHECK(c->sclr_qres.alloc(3 * (size_t)c->nshg));
+    if (c->p.idiff == 1) {
+        CR_CHECK(c->sclr_qrec.alloc(16 * (size_t)c->nelem));
+        launch(k_sclr_q, grid_for(c->nelem, 128, 16), 128, 0, s, c->ien.p, c->x.p, d_s, c->nelem, T, P,
+               c->sclr_qrec.p);
+        launch(k_sclr_qnode, grid_for(c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->sclr_qrec.p,
+               c->nshg, c->sclr_qres.p);
+    }
+    CR_CHECK(c->sclr_erec.alloc(20 * (size_t)c->nelem));
+    launch(k_sclr_elem, grid_for(c->nelem, 128, 16), 128, 0, s, c->ien.p, c->x.p,
+           reinterpret_cast<const double4*>(d_y), d_s, d_sdot, (const double*)c->sclr_qres.p, c->nelem, T, P,
+           c->sclr_erec.p);
+    const bool faces = c->nface > 0 && c->fnoff.p;
+    if (faces) {
+        CR_CHECK(c->sclr_frec.alloc(3 * (size_t)c->nface));
+        launch(k_sclr_face, grid_for(c->nface, 128, 16), 128, 0, s, c->ienb.p, c->iBCB.p, d_bcbs, c->x.p, d_s,
+               c->nface, T, P, c->sclr_frec.p);
+    }
+    launch(k_sclr_node, grid_for(c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p, c->slist.p,
+           (const double*)c->sclr_erec.p, faces ? (const int*)c->fnoff.p : nullptr, (const int*)c->flist.p,
+           (const double*)c->sclr_frec.p, c->nshg, c->iBC.p, isclr, P.lhs, d_res, d_lhsS);
+    if (lhs)
+        launch(k_sclr_slot, grid_for(c->nnz, 256), 256, 0, s, c->soff.p, c->slist.p, (const double*)c->sclr_erec.p,
+               c->nnz, d_lhsS);
+    CR_CUDA(cudaGetLastError());
+    return CRIMSON_OK;
+}
+
+}  // namespace crimson

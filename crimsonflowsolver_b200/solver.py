@@ -122,6 +122,35 @@ class ElmGMR:
                                               d_lhsP.data_ptr() if lhs else None, 1 if lhs else 0),
                 "crimson_elmgmr_device")
 
+    def sclr(self, y, s, sdot, isclr: int = 1, diffus: float = 0.0, bcbs=None, lhs: bool = True):
+        """ElmGMRSclr (flowsolver/src/elmgmr.f90:599-822) from host arrays:
+        y (nshg, 4) the flow state, s and sdot (nshg) the scalar and its
+        rate, bcbs (nface, 3) the prescribed fluxes of faces whose iBCB bit
+        4 + isclr is set.  Returns res (nshg) and lhsS (nnz)."""
+        nnz = self._nnz()
+        yF = _f(y, np.float64)
+        sv = np.ascontiguousarray(np.asarray(s, dtype=np.float64).reshape(-1))
+        sd = np.ascontiguousarray(np.asarray(sdot, dtype=np.float64).reshape(-1))
+        if yF.shape != (self.nshg, 4) or sv.size != self.nshg or sd.size != self.nshg:
+            raise ValueError("y must be (nshg, 4) and s, sdot (nshg)")
+        bF = _f(bcbs, np.float64) if bcbs is not None else None
+        res = np.zeros(self.nshg)
+        lhsS = np.zeros(nnz) if lhs else None
+        N.check(N.lib().crimson_elmgmr_sclr(self.h, int(isclr), float(diffus), N.dp(yF), N.dp(sv), N.dp(sd),
+                                            N.dp(bF), N.dp(res), N.dp(lhsS), 1 if lhs else 0),
+                "crimson_elmgmr_sclr")
+        return {"res": res, "lhsS": lhsS}
+
+    def sclr_device(self, d_y, d_s, d_sdot, d_res, d_lhsS=None, isclr: int = 1, diffus: float = 0.0, d_bcbs=None,
+                    lhs: bool = True) -> None:
+        """Device-resident ElmGMRSclr on torch tensors: y (nshg, 4), s, sdot,
+        res (nshg), bcbs (nface, 3), lhsS (nnz); on the context's stream."""
+        N.check(N.lib().crimson_elmgmr_sclr_device(self.h, int(isclr), float(diffus), d_y.data_ptr(),
+                                                   d_s.data_ptr(), d_sdot.data_ptr(),
+                                                   d_bcbs.data_ptr() if d_bcbs is not None else None,
+                                                   d_res.data_ptr(), d_lhsS.data_ptr() if lhs else None,
+                                                   1 if lhs else 0), "crimson_elmgmr_sclr_device")
+
     @property
     def stream_handle(self) -> int:
         return N.lib().crimson_ctx_stream(self.h)

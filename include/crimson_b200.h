@@ -292,6 +292,30 @@ int crimson_set_rcr(crimson_ctx* ctx, int n, const double* Rp, const double* C, 
  * state, flowsolver/src/AbstractBoundaryCondition.cxx:55-91): read (set = 0)
  * or write (set = 1), e.g. to restart from a checkpoint. */
 int crimson_rcr_state(crimson_ctx* ctx, int n, double* Pn, double* Qn, int set);
+/* ElmGMRSclr (flowsolver/src/elmgmr.f90:599-822): residual res (nshg) and
+ * tangent lhsS (nnz, the CSR pattern of crimson_genadj) of the
+ * advection-diffusion equation of scalar isclr (1..4) with diffusivity
+ * diffus (scdiff(isclr)), after AsIqSclr/qpbcSclr (the lumped projection of
+ * diffus grad S when idiff = 1), AsIGMRSclr/e3Sclr, fillsparseSclr,
+ * AsBSclr/e3bSclr (the boundary flux term; faces whose iBCB bit 4+isclr is
+ * set take the prescribed flux bcbs (nface, 3) instead, bcbs may be NULL
+ * otherwise) and bc3ResSclr (rows with iBC bit isclr+5 zeroed).  y (nshg, 4)
+ * supplies the velocity; s and sdot (nshg) are the scalar and its rate at
+ * the alpha levels (y(:,5+isclr), ac(:,5+isclr) in the reference).  The
+ * reference's defaults for a passive scalar: SUPG, no discontinuity
+ * capturing, the flow velocity as convection velocity, no source terms
+ * (the reference's source call is commented out; its nosource = 0 reads
+ * uninitialised arrays).  Summation in ascending element order per entry,
+ * bitwise repeatable.  The reference solves this system with ACUSIM
+ * LesLib, which it does not contain; hosts pass res and lhsS to their
+ * own solver.  Returns CRIMSON_ERR_UNSUPPORTED for lumped-mass fractions. */
+int crimson_elmgmr_sclr(crimson_ctx* ctx, int isclr, double diffus, const double* y, const double* s,
+                        const double* sdot, const double* bcbs, double* res, double* lhsS, int lhs);
+/* Device pointers: d_y (4, nshg) node-major, d_s, d_sdot, d_res (nshg),
+ * d_bcbs (nface, 3) face-major or NULL, d_lhsS (nnz); on the context's stream. */
+int crimson_elmgmr_sclr_device(crimson_ctx* ctx, int isclr, double diffus, const double* d_y, const double* d_s,
+                               const double* d_sdot, const double* d_bcbs, double* d_res, double* d_lhsS, int lhs);
+
 /* ---------------------------------------------------------------------------
  * Netlist (lumped-parameter 0D) outlet circuits: NetlistCircuit
  * (flowsolver/src/NetlistCircuit.cxx, CircuitData.cxx, CircuitComponent.cxx)

@@ -975,6 +975,292 @@ extern "C" int orc_elmgmr(const orc_params* p, int nshg, int numnp, int nelem, c
     return ORC_OK;
 }
 
+// ===========================================================================
+// ElmGMRSclr (flowsolver/src/elmgmr.f90:599-822): residual and tangent of the
+// advection-diffusion equation of scalar isclr with diffusivity diffus
+// (getdiffsclr, getdiff.f90:145-174), no sources (nosource = 1: the source
+// call in e3ivarSclr is commented out in the reference, e3ivar.f90:670-680),
+// convective form with the flow velocity (consrv_sclr_conv_vel = 0), SUPG
+// weak form (ivart = 2), no discontinuity capturing (idcsclr = 0).
+//   s, sdot (nshg): the scalar and its time derivative (y(:,5+isclr),
+//   ac(:,5+isclr)); y (nshg, 4) supplies the velocity.
+//   bcbs (nface, 3): prescribed scalar flux per face node, read where
+//   ibits(iBCB(:,1), 4+isclr) is set (e3b.f90:700-715); may be NULL.
+// ===========================================================================
+
+// e3qSclr + e3qvarSclr for one element (e3q.f90:215-300, e3qvar.f90:149-180)
+void e3q_sclr_elem(double diffus, int idiff, const double sl[4], const double xl[4][3], double ql[4][3],
+                   double rm[4]) {
+    const Tables& T = tables();
+    for (int a = 0; a < 4; ++a) {
+        ql[a][0] = ql[a][1] = ql[a][2] = 0.0;
+        rm[a] = 0.0;
+    }
+    for (int intp = 0; intp < 4; ++intp) {
+        const double* shapeVar = T.shp[intp];
+        double dxidx[3][3], shg[4][3], W;
+        e3metric(xl, T.shgl[intp], T.Qwt[intp], dxidx, shg, &W);
+        double gradT[3] = {0.0, 0.0, 0.0};
+        for (int n = 0; n < 4; ++n)
+            for (int k = 0; k < 3; ++k) gradT[k] = gradT[k] + shg[n][k] * sl[n];
+        double qdi[3];
+        for (int k = 0; k < 3; ++k) qdi[k] = diffus * gradT[k];
+        for (int i = 0; i < 4; ++i)
+            for (int k = 0; k < 3; ++k) ql[i][k] = ql[i][k] + shapeVar[i] * W * qdi[k];
+        if (idiff == 1)
+            for (int i = 0; i < 4; ++i) rm[i] = rm[i] + shapeVar[i] * W;
+    }
+}
+
+// e3Sclr for one element (e3.f90:183-330): e3ivarSclr (e3ivar.f90:492-700),
+// e3StabSclr (e3stab.f90:542-600), e3ResSclr (e3res.f90:300-370), e3LHSSclr
+// (e3lhs.f90:416-528).  ul[n] = (u, v, w); rl[a]; xS[a][b] = xSebe(:,a,b).
+void e3_sclr_elem(const orc_params* p, double diffus, const double ul[4][3], const double sl[4],
+                  const double sdl[4], const double xl[4][3], const double ql[4][3], int lhs, double rl[4],
+                  double xS[4][4]) {
+    const Tables& T = tables();
+    for (int intp = 0; intp < 4; ++intp) {
+        const double* shpfun = T.shp[intp];
+        // e3ivarSclr
+        double u1 = 0.0, u2 = 0.0, u3 = 0.0, Sclr = 0.0;
+        for (int n = 0; n < 4; ++n) {
+            u1 = u1 + shpfun[n] * ul[n][0];
+            u2 = u2 + shpfun[n] * ul[n][1];
+            u3 = u3 + shpfun[n] * ul[n][2];
+            Sclr = Sclr + shpfun[n] * sl[n];
+        }
+        double Sdot = 0.0;
+        for (int n = 0; n < 4; ++n) Sdot = Sdot + shpfun[n] * sdl[n];
+        double dxidx[3][3], shg[4][3], W;
+        e3metric(xl, T.shgl[intp], T.Qwt[intp], dxidx, shg, &W);
+        double gradS[3] = {0.0, 0.0, 0.0};
+        for (int n = 0; n < 4; ++n)
+            for (int k = 0; k < 3; ++k) gradS[k] = gradS[k] + shg[n][k] * sl[n];
+        double divS = 0.0;
+        if (p->idiff >= 1)
+            for (int n = 0; n < 4; ++n)
+                divS = divS + shg[n][0] * ql[n][0] + shg[n][1] * ql[n][1] + shg[n][2] * ql[n][2];
+        const double srcR = 0.0, srcL = 0.0, srcRat = 0.0;  // nosource
+        const double rLS = (Sdot + (u1 * gradS[0] + u2 * gradS[1] + u3 * gradS[2])) - divS;
+        // e3StabSclr, ivart = 2, ipord = 1
+        double g[6];
+        e3gijd(dxidx, g);
+        const double fff = 9.0;
+        const double dts = p->Dtgl * p->dtsfct;
+        double tauT = (2.0 * dts) * (2.0 * dts) + srcRat * srcRat + u1 * (g[0] * u1 + g[3] * u2 + g[5] * u3) +
+                      u2 * (g[3] * u1 + g[1] * u2 + g[4] * u3) + u3 * (g[5] * u1 + g[4] * u2 + g[2] * u3) +
+                      fff * (diffus * diffus) *
+                          (g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + 2.0 * (g[3] * g[3] + g[4] * g[4] + g[5] * g[5]));
+        const double tauS = 1.0 / std::sqrt(tauT);
+        // e3ResSclr
+        const double tmps = 1.0 - p->flmpr, rcp = 1.0;
+        const double rNa = rcp * (tmps * Sdot + u1 * gradS[0] + u2 * gradS[1] + u3 * gradS[2]) - srcR;
+        const double tmp = rcp * tauS * (rLS - srcR);
+        const double rGNa[3] = {diffus * gradS[0] + u1 * tmp, diffus * gradS[1] + u2 * tmp, diffus * gradS[2] + u3 * tmp};
+        for (int aa = 0; aa < 4; ++aa)
+            rl[aa] = rl[aa] - W * (shpfun[aa] * rNa + shg[aa][0] * rGNa[0] + shg[aa][1] * rGNa[1] + shg[aa][2] * rGNa[2]);
+        // e3LHSSclr
+        if (!lhs) continue;
+        const double lhsFct = p->alfi * p->gami * p->Delt;
+        const double tauSo = tauS;
+        const double tauSl = lhsFct * W * tauS;
+        const double kptmp = lhsFct * W * diffus;
+        const double tsFct = p->almi * W * (1.0 - p->flmpl);
+        const double src = srcL * W * lhsFct;
+        for (int b = 0; b < 4; ++b) {
+            const double t1 = W * (u1 * shg[b][0] + u2 * shg[b][1] + u3 * shg[b][2]);
+            const double t2 = t1 * tauSo;
+            for (int aa = 0; aa < 4; ++aa) {
+                const double tmp1 = shpfun[aa] * shpfun[b];
+                const double tmp2 = shpfun[aa] * lhsFct;
+                xS[aa][b] = xS[aa][b] + tmp1 * (tsFct + src) + tmp2 * t1;
+                xS[b][aa] = xS[b][aa] + t2 * shpfun[aa];
+            }
+        }
+        for (int b = 0; b < 4; ++b) {
+            const double tb = tauSl * (u1 * shg[b][0] + u2 * shg[b][1] + u3 * shg[b][2]);
+            const double t1[3] = {kptmp * shg[b][0] + u1 * tb, kptmp * shg[b][1] + u2 * tb, kptmp * shg[b][2] + u3 * tb};
+            xS[b][b] = xS[b][b] + t1[0] * shg[b][0] + t1[1] * shg[b][1] + t1[2] * shg[b][2];
+            for (int aa = b + 1; aa < 4; ++aa) {
+                const double v = t1[0] * shg[aa][0] + t1[1] * shg[aa][1] + t1[2] * shg[aa][2];
+                xS[aa][b] = xS[aa][b] + v;
+                xS[b][aa] = xS[b][aa] + v;
+            }
+        }
+    }
+}
+
+// e3bSclr + e3bvarSclr for one linear-tet boundary face (e3b.f90:626-720,
+// e3bvar.f90:1033-1200), Navier = 1; rl[0..2] for the three face nodes.
+void e3b_sclr_face(double diffus, int isclr, const double sl[4], const double xlb[4][3], int ibcb_bits,
+                   const double bcbs[3], double rl[4]) {
+    const Tables& T = tables();
+    for (int intp = 0; intp < 3; ++intp) {
+        const double* shapeVar = T.shpb[intp];
+        double d[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int n = 0; n < 4; ++n)
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) d[i][j] = d[i][j] + xlb[n][i] * T.shglb[intp][j][n];
+        double v1[3], v2[3];
+        for (int i = 0; i < 3; ++i) {
+            v1[i] = xlb[1][i] - xlb[0][i];
+            v2[i] = xlb[2][i] - xlb[0][i];
+        }
+        const double temp1 = v1[1] * v2[2] - v2[1] * v1[2];
+        const double temp2 = v2[0] * v1[2] - v1[0] * v2[2];
+        const double temp3 = v1[0] * v2[1] - v2[0] * v1[1];
+        const double temp = 1.0 / std::sqrt(temp1 * temp1 + temp2 * temp2 + temp3 * temp3);
+        const double bn[3] = {temp1 * temp, temp2 * temp, temp3 * temp};
+        const double WdetJb = T.Qwtb[intp] / (4.0 * temp);
+        double dx[3][3];
+        dx[0][0] = d[1][1] * d[2][2] - d[2][1] * d[1][2];
+        dx[0][1] = d[2][1] * d[0][2] - d[0][1] * d[2][2];
+        dx[0][2] = d[0][1] * d[1][2] - d[0][2] * d[1][1];
+        const double tmp = 1.0 / (dx[0][0] * d[0][0] + dx[0][1] * d[1][0] + dx[0][2] * d[2][0]);
+        dx[0][0] = dx[0][0] * tmp;
+        dx[0][1] = dx[0][1] * tmp;
+        dx[0][2] = dx[0][2] * tmp;
+        dx[1][0] = (d[1][2] * d[2][0] - d[1][0] * d[2][2]) * tmp;
+        dx[1][1] = (d[0][0] * d[2][2] - d[2][0] * d[0][2]) * tmp;
+        dx[1][2] = (d[1][0] * d[0][2] - d[0][0] * d[1][2]) * tmp;
+        dx[2][0] = (d[1][0] * d[2][1] - d[1][1] * d[2][0]) * tmp;
+        dx[2][1] = (d[2][0] * d[0][1] - d[0][0] * d[2][1]) * tmp;
+        dx[2][2] = (d[0][0] * d[1][1] - d[0][1] * d[1][0]) * tmp;
+        double gl[3] = {0.0, 0.0, 0.0};
+        for (int n = 0; n < 4; ++n)
+            for (int k = 0; k < 3; ++k) gl[k] = gl[k] + T.shglb[intp][k][n] * sl[n];
+        double gS[3];
+        for (int k = 0; k < 3; ++k) gS[k] = dx[0][k] * gl[0] + dx[1][k] * gl[1] + dx[2][k] * gl[2];
+        double flux = diffus * (gS[0] * bn[0] + gS[1] * bn[1] + gS[2] * bn[2]);
+        if ((ibcb_bits >> (4 + isclr)) & 1) {
+            flux = 0.0;
+            for (int n = 0; n < 3; ++n) flux = flux + shapeVar[n] * bcbs[n];
+        }
+        const double rNa = -WdetJb * flux;
+        for (int n = 0; n < 3; ++n) rl[n] = rl[n] - shapeVar[n] * rNa;
+    }
+}
+
+extern "C" int orc_elmgmr_sclr(const orc_params* p, int isclr, double diffus, int nshg, int numnp, int nelem,
+                               const int* ien, const double* x, const double* y, const double* s,
+                               const double* sdot, const int* iBC, int nface, const int* ienb, const int* iBCB,
+                               const double* bcbs, const int* colm, const int* rowp, long long nnz, double* res,
+                               double* lhsS, int lhs, double* qres_out) {
+    if (!p || !ien || !x || !y || !s || !sdot || !res || isclr < 1 || isclr > 4) return ORC_ERR_ARG;
+    if (p->flmpl != 0.0 || p->flmpr != 0.0 || (p->idiff != 0 && p->idiff != 1)) return ORC_ERR_UNSUPPORTED;
+    const int ibksiz = p->ibksiz > 0 ? p->ibksiz : 255;
+    const int nblk = (nelem + ibksiz - 1) / ibksiz;
+    auto node = [&](int e, int a) { return ien[a * nelem + e] - 1; };
+    auto gather = [&](int e, double ul[4][3], double sl[4], double sdl[4], double xl[4][3]) {
+        for (int a = 0; a < 4; ++a) {
+            const int nd = node(e, a);
+            for (int d = 0; d < 3; ++d) {
+                ul[a][d] = y[(size_t)d * nshg + nd];
+                xl[a][d] = x[(size_t)d * numnp + nd];
+            }
+            sl[a] = s[nd];
+            sdl[a] = sdot[nd];
+        }
+    };
+    // ---- diffusive flux: AsIqSclr + qpbcSclr (elmgmr.f90:650-683; qpbc.f90:118-175) ----
+    std::vector<double> qres((size_t)nshg * 3, 0.0), rmass(nshg, 0.0);
+    if (p->idiff == 1) {
+        for (int b = 0; b < nblk; ++b) {
+            const int e0 = b * ibksiz, e1 = std::min(nelem, e0 + ibksiz);
+            std::vector<double> qb((size_t)(e1 - e0) * 12), rb((size_t)(e1 - e0) * 4);
+            for (int e = e0; e < e1; ++e) {
+                double ul[4][3], sl[4], sdl[4], xl[4][3], ql[4][3], rm[4];
+                gather(e, ul, sl, sdl, xl);
+                e3q_sclr_elem(diffus, p->idiff, sl, xl, ql, rm);
+                for (int a = 0; a < 4; ++a) {
+                    for (int k = 0; k < 3; ++k) qb[(size_t)(e - e0) * 12 + a * 3 + k] = ql[a][k];
+                    rb[(size_t)(e - e0) * 4 + a] = rm[a];
+                }
+            }
+            // local scatter order: dof k, node a, element e (local.f90:68-75)
+            for (int k = 0; k < 3; ++k)
+                for (int a = 0; a < 4; ++a)
+                    for (int e = e0; e < e1; ++e) {
+                        const int nd = node(e, a);
+                        qres[(size_t)k * nshg + nd] = qres[(size_t)k * nshg + nd] + qb[(size_t)(e - e0) * 12 + a * 3 + k];
+                    }
+            for (int a = 0; a < 4; ++a)
+                for (int e = e0; e < e1; ++e) {
+                    const int nd = node(e, a);
+                    rmass[nd] = rmass[nd] + rb[(size_t)(e - e0) * 4 + a];
+                }
+        }
+        for (int i = 0; i < nshg; ++i) rmass[i] = 1.0 / rmass[i];
+        for (int k = 0; k < 3; ++k)
+            for (int i = 0; i < nshg; ++i) qres[(size_t)k * nshg + i] = rmass[i] * qres[(size_t)k * nshg + i];
+    }
+    if (qres_out) std::memcpy(qres_out, qres.data(), sizeof(double) * (size_t)nshg * 3);
+    // ---- interior elements: AsIGMRSclr + fillsparseSclr (elmgmr.f90:698-745) ----
+    std::fill(res, res + nshg, 0.0);
+    if (lhs) std::fill(lhsS, lhsS + nnz, 0.0);
+    for (int b = 0; b < nblk; ++b) {
+        const int e0 = b * ibksiz, e1 = std::min(nelem, e0 + ibksiz);
+        std::vector<double> rb((size_t)(e1 - e0) * 4), xb((size_t)(e1 - e0) * 16);
+        for (int e = e0; e < e1; ++e) {
+            double ul[4][3], sl[4], sdl[4], xl[4][3], ql[4][3];
+            gather(e, ul, sl, sdl, xl);
+            for (int a = 0; a < 4; ++a)
+                for (int k = 0; k < 3; ++k) ql[a][k] = qres[(size_t)k * nshg + node(e, a)];
+            double rl[4] = {0, 0, 0, 0}, xS[4][4] = {{0}};
+            e3_sclr_elem(p, diffus, ul, sl, sdl, xl, ql, lhs, rl, xS);
+            for (int a = 0; a < 4; ++a) {
+                rb[(size_t)(e - e0) * 4 + a] = rl[a];
+                for (int c = 0; c < 4; ++c) xb[(size_t)(e - e0) * 16 + a * 4 + c] = xS[a][c];
+            }
+        }
+        for (int a = 0; a < 4; ++a)
+            for (int e = e0; e < e1; ++e) {
+                const int nd = node(e, a);
+                res[nd] = res[nd] + rb[(size_t)(e - e0) * 4 + a];
+            }
+        if (!lhs) continue;
+        // fillsparseSclr (fillsparse.f90:167-200)
+        for (int e = e0; e < e1; ++e)
+            for (int aa = 0; aa < 4; ++aa) {
+                const int i = ien[aa * nelem + e];
+                const int c = colm[i - 1];
+                const int n = colm[i] - c;
+                for (int bb = 0; bb < 4; ++bb) {
+                    const long long k = sparseloc(&rowp[c - 1], n, ien[bb * nelem + e]) + c - 1;
+                    lhsS[k - 1] = lhsS[k - 1] + xb[(size_t)(e - e0) * 16 + aa * 4 + bb];
+                }
+            }
+    }
+    // ---- boundary elements: AsBSclr (elmgmr.f90:772-800) ----
+    const int nbblk = (nface + ibksiz - 1) / ibksiz;
+    for (int b = 0; b < nbblk; ++b) {
+        const int f0 = b * ibksiz, f1 = std::min(nface, f0 + ibksiz);
+        std::vector<double> rb((size_t)(f1 - f0) * 4);
+        for (int f = f0; f < f1; ++f) {
+            double sl[4], xlb[4][3], bc[3] = {0.0, 0.0, 0.0};
+            for (int a = 0; a < 4; ++a) {
+                const int nd = ienb[a * nface + f] - 1;
+                sl[a] = s[nd];
+                for (int d = 0; d < 3; ++d) xlb[a][d] = x[(size_t)d * numnp + nd];
+            }
+            if (bcbs)
+                for (int n = 0; n < 3; ++n) bc[n] = bcbs[(size_t)n * nface + f];
+            double rl[4] = {0, 0, 0, 0};
+            e3b_sclr_face(diffus, isclr, sl, xlb, iBCB[f], bc, rl);
+            for (int a = 0; a < 4; ++a) rb[(size_t)(f - f0) * 4 + a] = rl[a];
+        }
+        for (int a = 0; a < 4; ++a)
+            for (int f = f0; f < f1; ++f) {
+                const int nd = ienb[a * nface + f] - 1;
+                res[nd] = res[nd] + rb[(size_t)(f - f0) * 4 + a];
+            }
+    }
+    // ---- bc3ResSclr (bc3res.f90:138-160) ----
+    for (int i = 0; i < nshg; ++i)
+        if ((iBC[i] >> (isclr + 5)) & 1) res[i] = 0.0;
+    return ORC_OK;
+}
+
 extern "C" int orc_getflowq(int nshg, const double* y, int nsrf, const int* srflist, const int* ndsurf,
                             const double* NABI, double* q) {
     for (int k = 0; k < nsrf; ++k) q[k] = 0.0;

@@ -73,6 +73,15 @@ int orc_elmgmr(const orc_params* p, int nshg, int numnp, int nelem, const int* i
                double* qres_out, double* rmass_out);
 
 /* GetFlowQ (flowsolver/src/boundarydata.f90:1157-1196) */
+/* ElmGMRSclr (flowsolver/src/elmgmr.f90:599-822) for scalar isclr (1..4)
+ * with diffusivity diffus: s, sdot (nshg) the scalar and its rate, y (nshg,4)
+ * the velocity, bcbs (nface, 3) prescribed face fluxes (may be NULL);
+ * res (nshg), lhsS (nnz); qres_out (nshg, 3) the projected flux. */
+int orc_elmgmr_sclr(const orc_params* p, int isclr, double diffus, int nshg, int numnp, int nelem,
+                    const int* ien, const double* x, const double* y, const double* s, const double* sdot,
+                    const int* iBC, int nface, const int* ienb, const int* iBCB, const double* bcbs,
+                    const int* colm, const int* rowp, long long nnz, double* res, double* lhsS, int lhs,
+                    double* qres_out);
 int orc_getflowq(int nshg, const double* y, int nsrf, const int* srflist, const int* ndsurf,
                  const double* NABI, double* q);
 

@@ -70,6 +70,10 @@ def lib():
                                  _c_int_p, ctypes.c_longlong, _c_dbl_p, _c_dbl_p, _c_dbl_p, ctypes.c_int, _c_dbl_p,
                                  _c_dbl_p]
         L.orc_getflowq.argtypes = [ctypes.c_int, _c_dbl_p, ctypes.c_int, _c_int_p, _c_int_p, _c_dbl_p, _c_dbl_p]
+        L.orc_elmgmr_sclr.argtypes = [ctypes.POINTER(OrcParams), ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_int, _c_int_p, _c_dbl_p, _c_dbl_p, _c_dbl_p, _c_dbl_p,
+                                      _c_int_p, ctypes.c_int, _c_int_p, _c_int_p, _c_dbl_p, _c_int_p, _c_int_p,
+                                      ctypes.c_longlong, _c_dbl_p, _c_dbl_p, ctypes.c_int, _c_dbl_p]
         L.orc_solflow_pack.argtypes = [ctypes.c_int, ctypes.c_longlong, _c_int_p, _c_int_p, _c_dbl_p, _c_dbl_p,
                                        _c_dbl_p, _c_dbl_p, _c_dbl_p]
         L.orc_memls_ls_create.restype = ctypes.c_void_p
@@ -173,6 +177,28 @@ class Elm:
             out["qres"] = np.ascontiguousarray(qres)
             out["rmass"] = rmass
         return out
+
+
+def elmgmr_sclr(elm, y, s, sdot, isclr=1, diffus=0.2, bcbs=None, lhs=True):
+    """ElmGMRSclr (elmgmr.f90:599-822) on the oracle: res (nshg), lhsS (nnz),
+    qres (nshg, 3).  elm is an :class:`Elm` (mesh arrays and pattern)."""
+    L = lib()
+    m = elm.m
+    nshg = m.nshg
+    yF = np.asfortranarray(y, dtype=np.float64)
+    sv = np.ascontiguousarray(s, dtype=np.float64)
+    sd = np.ascontiguousarray(sdot, dtype=np.float64)
+    res = np.zeros(nshg)
+    lhsS = np.zeros(elm.nnz) if lhs else None
+    qres = np.zeros((nshg, 3), order="F")
+    bF = np.asfortranarray(bcbs, dtype=np.float64) if bcbs is not None else None
+    rc = L.orc_elmgmr_sclr(ctypes.byref(elm.prm), isclr, diffus, nshg, nshg, m.nelem, _ip(elm.ienF), _dp(elm.xF),
+                           _dp(yF), _dp(sv), _dp(sd), _ip(elm.iBC), elm.nface, _ip(elm.ienbF), _ip(elm.iBCBF),
+                           _dp(bF), _ip(elm.colm), _ip(elm.rowp), elm.nnz, _dp(res), _dp(lhsS), 1 if lhs else 0,
+                           _dp(qres))
+    if rc != 0:
+        raise RuntimeError(f"orc_elmgmr_sclr failed rc={rc}")
+    return {"res": res, "lhsS": lhsS, "qres": np.ascontiguousarray(qres)}
 
 
 def getflowq(mesh, y, srflist):
