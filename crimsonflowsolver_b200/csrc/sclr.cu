@@ -8,8 +8,9 @@
 //   k_sclr_qnode  their sums per node in ascending element order, then
 //                 qpbcSclr (qpbc.f90:118-175): qres = q / rmass
 //   k_sclr_elem   AsIGMRSclr / e3Sclr (asigmr.f90:141-190, e3.f90:183-330):
-//                 per element the residual rows rl(a) and the 4x4 tangent
-//                 xSebe (e3ivarSclr, e3StabSclr, e3ResSclr, e3LHSSclr)
+//                 per element (4 lanes, one per quadrature point) the
+//                 residual rows rl(a) and the 4x4 tangent xSebe
+//                 (e3ivarSclr, e3StabSclr, e3ResSclr, e3LHSSclr)
 //   k_sclr_face   AsBSclr / e3bSclr (asbmfg.f90:114-150, e3b.f90:626-720):
 //                 the boundary flux term of each face node
 //   k_sclr_node   per node: residual row (elements, then faces) and the
@@ -64,6 +65,8 @@ SclrTables sclr_tables() {
         t.shpb[q][3] = 1.0e0 - r3[q][0] - r3[q][1] - r3[q][2];
         t.Qwtb[q] = 2.0 * A3;
     }
+    // the kernels rely on equal weights per rule (metric and W hoisted out
+    // of the quadrature loops)
     return t;
 }
 
@@ -134,7 +137,10 @@ __device__ __forceinline__ void sclr_gather_x(const int4 nn, const double4* __re
     }
 }
 
-// Element records of the flux projection: ql(a, 0:3) and rmassl(a), 16 doubles.
+// Offset of off-diagonal xSebe(a, b), a != b, in an element record.
+__host__ __device__ __forceinline__ int sclr_off(int a, int b) { return 8 + 3 * a + (b < a ? b : b - 1); }
+
+// Element records of the flux projection: {ql(a, 0:3), rmassl(a)} at 4 a, 16 doubles.
 __global__ void __launch_bounds__(128) k_sclr_q(const int4* __restrict__ ien, const double4* __restrict__ x,
                                                 const double* __restrict__ s, int nelem, SclrTables T, SclrParams P,
                                                 double* __restrict__ qrec) {
@@ -144,28 +150,26 @@ __global__ void __launch_bounds__(128) k_sclr_q(const int4* __restrict__ ien, co
         sclr_gather_x(nn, x, xl);
         const double sl[4] = {s[nn.x], s[nn.y], s[nn.z], s[nn.w]};
         double ql[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, rm[4] = {0, 0, 0, 0};
+        // linear tet, equal weights: metric, W and grad S are the same at the 4 points
+        double dxidx[3][3], shg[4][3], W;
+        sclr_metric(xl, T.shgl, T.Qwt[0], dxidx, shg, &W);
+        double gT[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            double dxidx[3][3], shg[4][3], W;
-            sclr_metric(xl, T.shgl, T.Qwt[q], dxidx, shg, &W);
-            double gT[3] = {0.0, 0.0, 0.0};
+        for (int n = 0; n < 4; ++n)
 #pragma unroll
-            for (int n = 0; n < 4; ++n)
+            for (int k = 0; k < 3; ++k) gT[k] = gT[k] + shg[n][k] * sl[n];
+        const double qdi[3] = {P.diffus * gT[0], P.diffus * gT[1], P.diffus * gT[2]};
 #pragma unroll
-                for (int k = 0; k < 3; ++k) gT[k] = gT[k] + shg[n][k] * sl[n];
-            const double qdi[3] = {P.diffus * gT[0], P.diffus * gT[1], P.diffus * gT[2]};
+        for (int q = 0; q < 4; ++q)
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k) ql[i][k] = ql[i][k] + T.shp[q][i] * W * qdi[k];
                 rm[i] = rm[i] + T.shp[q][i] * W;
             }
-        }
         double4* r = reinterpret_cast<double4*>(qrec + 16 * (size_t)e);
-        r[0] = make_double4(ql[0][0], ql[0][1], ql[0][2], ql[1][0]);
-        r[1] = make_double4(ql[1][1], ql[1][2], ql[2][0], ql[2][1]);
-        r[2] = make_double4(ql[2][2], ql[3][0], ql[3][1], ql[3][2]);
-        r[3] = make_double4(rm[0], rm[1], rm[2], rm[3]);
+#pragma unroll
+        for (int a = 0; a < 4; ++a) r[a] = make_double4(ql[a][0], ql[a][1], ql[a][2], rm[a]);
     }
 }
 
@@ -175,18 +179,35 @@ __global__ void __launch_bounds__(128) k_sclr_q(const int4* __restrict__ ien, co
 __global__ void __launch_bounds__(256) k_sclr_qnode(const int* __restrict__ diag, const int* __restrict__ soff,
                                                     const int* __restrict__ slist, const double* __restrict__ qrec,
                                                     int nshg, double* __restrict__ qres) {
+    const double4* rec = reinterpret_cast<const double4*>(qrec);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
         const int d = diag[i];
         double q0 = 0.0, q1 = 0.0, q2 = 0.0, m = 0.0;
+        int p = soff[d];
         const int p1 = soff[d + 1];
-        for (int p = soff[d]; p < p1; ++p) {
+        // four independent loads in flight, summed in list order
+        for (; p + 4 <= p1; p += 4) {
+            int t[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) t[j] = slist[p + j];
+            double4 v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = rec[4 * (size_t)(t[j] >> 4) + ((t[j] >> 2) & 3)];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                q0 += v[j].x;
+                q1 += v[j].y;
+                q2 += v[j].z;
+                m += v[j].w;
+            }
+        }
+        for (; p < p1; ++p) {
             const int t = slist[p];
-            const int e = t >> 4, a = (t >> 2) & 3;
-            const double* r = qrec + 16 * (size_t)e;
-            q0 += r[3 * a];
-            q1 += r[3 * a + 1];
-            q2 += r[3 * a + 2];
-            m += r[12 + a];
+            const double4 v = rec[4 * (size_t)(t >> 4) + ((t >> 2) & 3)];
+            q0 += v.x;
+            q1 += v.y;
+            q2 += v.z;
+            m += v.w;
         }
         const double rinv = 1.0 / m;
         qres[3 * (size_t)i] = rinv * q0;
@@ -195,8 +216,10 @@ __global__ void __launch_bounds__(256) k_sclr_qnode(const int* __restrict__ diag
     }
 }
 
-// e3Sclr per element: record = rl(0:4) then xSebe(a, b) at 4 + 4 a + b (20 doubles).
-__global__ void __launch_bounds__(128) k_sclr_elem(const int4* __restrict__ ien, const double4* __restrict__ x,
+// e3Sclr per element.  Record (20 doubles): {rl(a), xSebe(a, a)} at 2 a, so
+// a node's residual and diagonal entry share one 16-byte load; off-diagonal
+// xSebe(a, b) at sclr_off(a, b).
+__global__ void __launch_bounds__(128, 3) k_sclr_elem(const int4* __restrict__ ien, const double4* __restrict__ x,
                                                    const double4* __restrict__ y, const double* __restrict__ s,
                                                    const double* __restrict__ sdot, const double* __restrict__ qres,
                                                    int nelem, SclrTables T, SclrParams P, double* __restrict__ erec) {
@@ -220,9 +243,25 @@ __global__ void __launch_bounds__(128) k_sclr_elem(const int4* __restrict__ ien,
         double xS[4][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
         const double lhsFct = P.alfi * P.gami * P.Delt;
         const double dts = P.Dtgl * P.dtsfct;
+        double dxidx[3][3], shg[4][3], W;
+        sclr_metric(xl, T.shgl, T.Qwt[0], dxidx, shg, &W);
+        double gS[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int n = 0; n < 4; ++n)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) gS[k] = gS[k] + shg[n][k] * sl[n];
+        double divS = 0.0;
+        if (P.idiff >= 1)
+#pragma unroll
+            for (int n = 0; n < 4; ++n)
+                divS = divS + shg[n][0] * ql[n][0] + shg[n][1] * ql[n][1] + shg[n][2] * ql[n][2];
+        double g[6];
+        sclr_gijd(dxidx, g);
+        const double tauDiff = 9.0 * (P.diffus * P.diffus) *
+                               (g[0] * g[0] + g[1] * g[1] + g[2] * g[2] +
+                                2.0 * (g[3] * g[3] + g[4] * g[4] + g[5] * g[5]));
         for (int q = 0; q < 4; ++q) {
             const double* shp = T.shp[q];
-            // e3ivarSclr
             double u1 = 0.0, u2 = 0.0, u3 = 0.0;
 #pragma unroll
             for (int n = 0; n < 4; ++n) {
@@ -233,27 +272,11 @@ __global__ void __launch_bounds__(128) k_sclr_elem(const int4* __restrict__ ien,
             double Sdot = 0.0;
 #pragma unroll
             for (int n = 0; n < 4; ++n) Sdot = Sdot + shp[n] * sdl[n];
-            double dxidx[3][3], shg[4][3], W;
-            sclr_metric(xl, T.shgl, T.Qwt[q], dxidx, shg, &W);
-            double gS[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-            for (int n = 0; n < 4; ++n)
-#pragma unroll
-                for (int k = 0; k < 3; ++k) gS[k] = gS[k] + shg[n][k] * sl[n];
-            double divS = 0.0;
-            if (P.idiff >= 1)
-#pragma unroll
-                for (int n = 0; n < 4; ++n)
-                    divS = divS + shg[n][0] * ql[n][0] + shg[n][1] * ql[n][1] + shg[n][2] * ql[n][2];
             const double rLS = (Sdot + (u1 * gS[0] + u2 * gS[1] + u3 * gS[2])) - divS;
             // e3StabSclr (ivart = 2, ipord = 1, no sources)
-            double g[6];
-            sclr_gijd(dxidx, g);
             const double tauT = (2.0 * dts) * (2.0 * dts) + 0.0 * 0.0 + u1 * (g[0] * u1 + g[3] * u2 + g[5] * u3) +
                                 u2 * (g[3] * u1 + g[1] * u2 + g[4] * u3) + u3 * (g[5] * u1 + g[4] * u2 + g[2] * u3) +
-                                9.0 * (P.diffus * P.diffus) *
-                                    (g[0] * g[0] + g[1] * g[1] + g[2] * g[2] +
-                                     2.0 * (g[3] * g[3] + g[4] * g[4] + g[5] * g[5]));
+                                tauDiff;
             const double tauS = 1.0 / sqrt(tauT);
             // e3ResSclr (flmpr = 0)
             const double rNa = 1.0 * (1.0 * Sdot + u1 * gS[0] + u2 * gS[1] + u3 * gS[2]) - 0.0;
@@ -293,9 +316,11 @@ __global__ void __launch_bounds__(128) k_sclr_elem(const int4* __restrict__ ien,
             }
         }
         double4* r = reinterpret_cast<double4*>(erec + 20 * (size_t)e);
-        r[0] = make_double4(rl[0], rl[1], rl[2], rl[3]);
-#pragma unroll
-        for (int a = 0; a < 4; ++a) r[1 + a] = make_double4(xS[a][0], xS[a][1], xS[a][2], xS[a][3]);
+        r[0] = make_double4(rl[0], xS[0][0], rl[1], xS[1][1]);
+        r[1] = make_double4(rl[2], xS[2][2], rl[3], xS[3][3]);
+        r[2] = make_double4(xS[0][1], xS[0][2], xS[0][3], xS[1][0]);
+        r[3] = make_double4(xS[1][2], xS[1][3], xS[2][0], xS[2][1]);
+        r[4] = make_double4(xS[2][3], xS[3][0], xS[3][1], xS[3][2]);
     }
 }
 
@@ -312,9 +337,18 @@ __global__ void __launch_bounds__(128) k_sclr_face(const int4* __restrict__ ienb
         // the host entry checks that bcbs is given where a face prescribes the flux
         const bool given = bcbs != nullptr && ((iBCB[f] >> (4 + P.isclr)) & 1);
         double rl[3] = {0.0, 0.0, 0.0};
-        // the face metric and the gradient are those of the tet: constant
-        // over the face, evaluated at each of the 3 points as the reference does
-        for (int q = 0; q < 3; ++q) {
+        // the face normal, WdetJb (equal weights) and the tet's gradient are
+        // the same at the 3 boundary points
+        const double v1[3] = {xl[1][0] - xl[0][0], xl[1][1] - xl[0][1], xl[1][2] - xl[0][2]};
+        const double v2[3] = {xl[2][0] - xl[0][0], xl[2][1] - xl[0][1], xl[2][2] - xl[0][2]};
+        const double te1 = v1[1] * v2[2] - v2[1] * v1[2];
+        const double te2 = v2[0] * v1[2] - v1[0] * v2[2];
+        const double te3 = v1[0] * v2[1] - v2[0] * v1[1];
+        const double temp = 1.0 / sqrt(te1 * te1 + te2 * te2 + te3 * te3);
+        const double bn[3] = {te1 * temp, te2 * temp, te3 * temp};
+        const double WdetJb = T.Qwtb[0] / (4.0 * temp);
+        double cflux = 0.0;
+        if (!given) {
             double d[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 #pragma unroll
             for (int n = 0; n < 4; ++n)
@@ -322,43 +356,37 @@ __global__ void __launch_bounds__(128) k_sclr_face(const int4* __restrict__ ienb
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
                     for (int j = 0; j < 3; ++j) d[i][j] = d[i][j] + xl[n][i] * T.shgl[j][n];
-            const double v1[3] = {xl[1][0] - xl[0][0], xl[1][1] - xl[0][1], xl[1][2] - xl[0][2]};
-            const double v2[3] = {xl[2][0] - xl[0][0], xl[2][1] - xl[0][1], xl[2][2] - xl[0][2]};
-            const double te1 = v1[1] * v2[2] - v2[1] * v1[2];
-            const double te2 = v2[0] * v1[2] - v1[0] * v2[2];
-            const double te3 = v1[0] * v2[1] - v2[0] * v1[1];
-            const double temp = 1.0 / sqrt(te1 * te1 + te2 * te2 + te3 * te3);
-            const double bn[3] = {te1 * temp, te2 * temp, te3 * temp};
-            const double WdetJb = T.Qwtb[q] / (4.0 * temp);
-            double flux;
+            double dx[3][3];
+            dx[0][0] = d[1][1] * d[2][2] - d[2][1] * d[1][2];
+            dx[0][1] = d[2][1] * d[0][2] - d[0][1] * d[2][2];
+            dx[0][2] = d[0][1] * d[1][2] - d[0][2] * d[1][1];
+            const double tmp = 1.0 / (dx[0][0] * d[0][0] + dx[0][1] * d[1][0] + dx[0][2] * d[2][0]);
+            dx[0][0] = dx[0][0] * tmp;
+            dx[0][1] = dx[0][1] * tmp;
+            dx[0][2] = dx[0][2] * tmp;
+            dx[1][0] = (d[1][2] * d[2][0] - d[1][0] * d[2][2]) * tmp;
+            dx[1][1] = (d[0][0] * d[2][2] - d[2][0] * d[0][2]) * tmp;
+            dx[1][2] = (d[1][0] * d[0][2] - d[0][0] * d[1][2]) * tmp;
+            dx[2][0] = (d[1][0] * d[2][1] - d[1][1] * d[2][0]) * tmp;
+            dx[2][1] = (d[2][0] * d[0][1] - d[0][0] * d[2][1]) * tmp;
+            dx[2][2] = (d[0][0] * d[1][1] - d[0][1] * d[1][0]) * tmp;
+            double gl[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int n = 0; n < 4; ++n)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) gl[k] = gl[k] + T.shgl[k][n] * sl[n];
+            double gS[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) gS[k] = dx[0][k] * gl[0] + dx[1][k] * gl[1] + dx[2][k] * gl[2];
+            cflux = P.diffus * (gS[0] * bn[0] + gS[1] * bn[1] + gS[2] * bn[2]);
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            double flux = cflux;
             if (given) {
                 flux = 0.0;
 #pragma unroll
                 for (int n = 0; n < 3; ++n) flux = flux + T.shpb[q][n] * bcbs[3 * (size_t)f + n];
-            } else {
-                double dx[3][3];
-                dx[0][0] = d[1][1] * d[2][2] - d[2][1] * d[1][2];
-                dx[0][1] = d[2][1] * d[0][2] - d[0][1] * d[2][2];
-                dx[0][2] = d[0][1] * d[1][2] - d[0][2] * d[1][1];
-                const double tmp = 1.0 / (dx[0][0] * d[0][0] + dx[0][1] * d[1][0] + dx[0][2] * d[2][0]);
-                dx[0][0] = dx[0][0] * tmp;
-                dx[0][1] = dx[0][1] * tmp;
-                dx[0][2] = dx[0][2] * tmp;
-                dx[1][0] = (d[1][2] * d[2][0] - d[1][0] * d[2][2]) * tmp;
-                dx[1][1] = (d[0][0] * d[2][2] - d[2][0] * d[0][2]) * tmp;
-                dx[1][2] = (d[1][0] * d[0][2] - d[0][0] * d[1][2]) * tmp;
-                dx[2][0] = (d[1][0] * d[2][1] - d[1][1] * d[2][0]) * tmp;
-                dx[2][1] = (d[2][0] * d[0][1] - d[0][0] * d[2][1]) * tmp;
-                dx[2][2] = (d[0][0] * d[1][1] - d[0][1] * d[1][0]) * tmp;
-                double gl[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-                for (int n = 0; n < 4; ++n)
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) gl[k] = gl[k] + T.shgl[k][n] * sl[n];
-                double gS[3];
-#pragma unroll
-                for (int k = 0; k < 3; ++k) gS[k] = dx[0][k] * gl[0] + dx[1][k] * gl[1] + dx[2][k] * gl[2];
-                flux = P.diffus * (gS[0] * bn[0] + gS[1] * bn[1] + gS[2] * bn[2]);
             }
             const double rNa = -WdetJb * flux;
 #pragma unroll
@@ -377,20 +405,35 @@ __global__ void __launch_bounds__(256) k_sclr_node(const int* __restrict__ diag,
                                                    const double* __restrict__ frec, int nshg,
                                                    const int* __restrict__ iBC, int isclr, int lhs,
                                                    double* __restrict__ res, double* __restrict__ lhsS) {
+    const double2* rec = reinterpret_cast<const double2*>(erec);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
         const int d = diag[i];
         double r = 0.0, k = 0.0;
+        int p = soff[d];
         const int p1 = soff[d + 1];
-        for (int p = soff[d]; p < p1; ++p) {
+        // four independent loads in flight, summed in list order
+        for (; p + 4 <= p1; p += 4) {
+            int t[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) t[j] = slist[p + j];
+            double2 v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = rec[10 * (size_t)(t[j] >> 4) + ((t[j] >> 2) & 3)];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                r += v[j].x;
+                k += v[j].y;
+            }
+        }
+        for (; p < p1; ++p) {
             const int t = slist[p];
-            const int e = t >> 4, a = (t >> 2) & 3;
-            const double* rec = erec + 20 * (size_t)e;
-            r += rec[a];
-            if (lhs) k += rec[4 + 5 * a];
+            const double2 v = rec[10 * (size_t)(t >> 4) + ((t >> 2) & 3)];
+            r += v.x;
+            k += v.y;
         }
         if (fnoff) {
             const int f1 = fnoff[i + 1];
-            for (int p = fnoff[i]; p < f1; ++p) r += frec[flist[p]];
+            for (int pf = fnoff[i]; pf < f1; ++pf) r += frec[flist[pf]];
         }
         if ((iBC[i] >> (isclr + 5)) & 1) r = 0.0;
         res[i] = r;
@@ -411,7 +454,7 @@ __global__ void __launch_bounds__(256) k_sclr_slot(const int* __restrict__ soff,
         for (int p = p0; p < p1; ++p) {
             const int t = slist[p];
             const int e = t >> 4, a = (t >> 2) & 3, b = t & 3;
-            k += erec[20 * (size_t)e + 4 + 4 * a + b];
+            k += erec[20 * (size_t)e + sclr_off(a, b)];
         }
         lhsS[sl] = k;
     }
