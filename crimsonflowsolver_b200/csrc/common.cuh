@@ -198,7 +198,6 @@ struct crimson_ctx {
 
     // ElmGMRSclr work space (scalar advection-diffusion)
     crimson::DBuf<double> sclr_qres;       // (nshg, 3) projected diffusive flux, node-major
-    crimson::DBuf<double> sclr_qrec;       // (nelem, 16) projection records
     crimson::DBuf<double> sclr_erec;       // (nelem, 20) rl(4) + xSebe(4, 4)
     crimson::DBuf<double> sclr_frec;       // (nface, 3) boundary flux terms
     crimson::DBuf<double> sclr_in, sclr_res, sclr_lhs;  // staging for host-pointer calls

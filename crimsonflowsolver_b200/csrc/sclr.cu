@@ -2,15 +2,14 @@
 // tangent of the advection-diffusion equation of one scalar, assembled with
 // the same deterministic owner-computes scheme as ElmGMR.
 //
-//   k_sclr_q      AsIqSclr / e3qSclr (asiq.f90:89-125, e3q.f90:215-300): per
-//                 element the lumped-projection contributions of q =
-//                 diffus grad S and of the lumped mass, per quadrature point
-//   k_sclr_qnode  their sums per node in ascending element order, then
-//                 qpbcSclr (qpbc.f90:118-175): qres = q / rmass
+//   k_sclr_qnode  AsIqSclr / e3qSclr (asiq.f90:89-125, e3q.f90:215-300) and
+//                 qpbcSclr (qpbc.f90:118-175) per node: the lumped-projection
+//                 contributions of q = diffus grad S and of the lumped mass
+//                 of each element containing the node, summed in ascending
+//                 element order, then qres = q / rmass
 //   k_sclr_elem   AsIGMRSclr / e3Sclr (asigmr.f90:141-190, e3.f90:183-330):
-//                 per element (4 lanes, one per quadrature point) the
-//                 residual rows rl(a) and the 4x4 tangent xSebe
-//                 (e3ivarSclr, e3StabSclr, e3ResSclr, e3LHSSclr)
+//                 per element the residual rows rl(a) and the 4x4 tangent
+//                 xSebe (e3ivarSclr, e3StabSclr, e3ResSclr, e3LHSSclr)
 //   k_sclr_face   AsBSclr / e3bSclr (asbmfg.f90:114-150, e3b.f90:626-720):
 //                 the boundary flux term of each face node
 //   k_sclr_node   per node: residual row (elements, then faces) and the
@@ -140,75 +139,51 @@ __device__ __forceinline__ void sclr_gather_x(const int4 nn, const double4* __re
 // Offset of off-diagonal xSebe(a, b), a != b, in an element record.
 __host__ __device__ __forceinline__ int sclr_off(int a, int b) { return 8 + 3 * a + (b < a ? b : b - 1); }
 
-// Element records of the flux projection: {ql(a, 0:3), rmassl(a)} at 4 a, 16 doubles.
-__global__ void __launch_bounds__(128) k_sclr_q(const int4* __restrict__ ien, const double4* __restrict__ x,
-                                                const double* __restrict__ s, int nelem, SclrTables T, SclrParams P,
-                                                double* __restrict__ qrec) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
-        const int4 nn = ien[e];
-        double xl[4][3];
-        sclr_gather_x(nn, x, xl);
-        const double sl[4] = {s[nn.x], s[nn.y], s[nn.z], s[nn.w]};
-        double ql[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, rm[4] = {0, 0, 0, 0};
-        // linear tet, equal weights: metric, W and grad S are the same at the 4 points
-        double dxidx[3][3], shg[4][3], W;
-        sclr_metric(xl, T.shgl, T.Qwt[0], dxidx, shg, &W);
-        double gT[3] = {0.0, 0.0, 0.0};
+// Per node: the projection sums over the elements containing it (the
+// contributions of its diagonal slot, ascending element order), each
+// element's contribution to this node recomputed from the element's
+// gathers (the metric and grad S are cheap next to a record round trip
+// through memory), then qpbcSclr: qres = (1 / rmass) q.
+__device__ __forceinline__ void sclr_q_contrib(const int4* __restrict__ ien, const double4* __restrict__ x,
+                                               const double* __restrict__ s, const SclrTables& T, double diffus,
+                                               int t, double& q0, double& q1, double& q2, double& m) {
+    const int e = t >> 4, a = (t >> 2) & 3;
+    const int4 nn = ien[e];
+    double xl[4][3];
+    sclr_gather_x(nn, x, xl);
+    const double sl[4] = {s[nn.x], s[nn.y], s[nn.z], s[nn.w]};
+    double dxidx[3][3], shg[4][3], W;
+    sclr_metric(xl, T.shgl, T.Qwt[0], dxidx, shg, &W);
+    double gT[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-        for (int n = 0; n < 4; ++n)
+    for (int n = 0; n < 4; ++n)
 #pragma unroll
-            for (int k = 0; k < 3; ++k) gT[k] = gT[k] + shg[n][k] * sl[n];
-        const double qdi[3] = {P.diffus * gT[0], P.diffus * gT[1], P.diffus * gT[2]};
+        for (int k = 0; k < 3; ++k) gT[k] = gT[k] + shg[n][k] * sl[n];
+    const double qdi[3] = {diffus * gT[0], diffus * gT[1], diffus * gT[2]};
+    double ql[3] = {0.0, 0.0, 0.0}, rm = 0.0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < 4; ++q) {
+        const double sa = T.shp[q][a];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k) ql[i][k] = ql[i][k] + T.shp[q][i] * W * qdi[k];
-                rm[i] = rm[i] + T.shp[q][i] * W;
-            }
-        double4* r = reinterpret_cast<double4*>(qrec + 16 * (size_t)e);
-#pragma unroll
-        for (int a = 0; a < 4; ++a) r[a] = make_double4(ql[a][0], ql[a][1], ql[a][2], rm[a]);
+        for (int k = 0; k < 3; ++k) ql[k] = ql[k] + sa * W * qdi[k];
+        rm = rm + sa * W;
     }
+    q0 += ql[0];
+    q1 += ql[1];
+    q2 += ql[2];
+    m += rm;
 }
 
-// Per node: the projection sums over the elements containing it (the
-// contributions of its diagonal slot, ascending element order), then
-// qres = (1 / rmass) q.
 __global__ void __launch_bounds__(256) k_sclr_qnode(const int* __restrict__ diag, const int* __restrict__ soff,
-                                                    const int* __restrict__ slist, const double* __restrict__ qrec,
-                                                    int nshg, double* __restrict__ qres) {
-    const double4* rec = reinterpret_cast<const double4*>(qrec);
+                                                    const int* __restrict__ slist, const int4* __restrict__ ien,
+                                                    const double4* __restrict__ x, const double* __restrict__ s,
+                                                    int nshg, SclrTables T, double diffus,
+                                                    double* __restrict__ qres) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
         const int d = diag[i];
         double q0 = 0.0, q1 = 0.0, q2 = 0.0, m = 0.0;
-        int p = soff[d];
         const int p1 = soff[d + 1];
-        // four independent loads in flight, summed in list order
-        for (; p + 4 <= p1; p += 4) {
-            int t[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) t[j] = slist[p + j];
-            double4 v[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) v[j] = rec[4 * (size_t)(t[j] >> 4) + ((t[j] >> 2) & 3)];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                q0 += v[j].x;
-                q1 += v[j].y;
-                q2 += v[j].z;
-                m += v[j].w;
-            }
-        }
-        for (; p < p1; ++p) {
-            const int t = slist[p];
-            const double4 v = rec[4 * (size_t)(t >> 4) + ((t >> 2) & 3)];
-            q0 += v.x;
-            q1 += v.y;
-            q2 += v.z;
-            m += v.w;
-        }
+        for (int p = soff[d]; p < p1; ++p) sclr_q_contrib(ien, x, s, T, diffus, slist[p], q0, q1, q2, m);
         const double rinv = 1.0 / m;
         qres[3 * (size_t)i] = rinv * q0;
         qres[3 * (size_t)i + 1] = rinv * q1;
@@ -484,13 +459,9 @@ int elmgmr_sclr_device(crimson_ctx* c, int isclr, double diffus, const double* d
     P.isclr = isclr;
     P.lhs = lhs ? 1 : 0;
     CR_CHECK(c->sclr_qres.alloc(3 * (size_t)c->nshg));
-    if (c->p.idiff == 1) {
-        CR_CHECK(c->sclr_qrec.alloc(16 * (size_t)c->nelem));
-        launch(k_sclr_q, grid_for(c->nelem, 128, 16), 128, 0, s, c->ien.p, c->x.p, d_s, c->nelem, T, P,
-               c->sclr_qrec.p);
-        launch(k_sclr_qnode, grid_for(c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->sclr_qrec.p,
-               c->nshg, c->sclr_qres.p);
-    }
+    if (c->p.idiff == 1)
+        launch(k_sclr_qnode, grid_for(c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->ien.p, c->x.p,
+               d_s, c->nshg, T, diffus, c->sclr_qres.p);
     CR_CHECK(c->sclr_erec.alloc(20 * (size_t)c->nelem));
     launch(k_sclr_elem, grid_for(c->nelem, 128, 16), 128, 0, s, c->ien.p, c->x.p,
            reinterpret_cast<const double4*>(d_y), d_s, d_sdot, (const double*)c->sclr_qres.p, c->nelem, T, P,
