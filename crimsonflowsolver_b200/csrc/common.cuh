@@ -198,7 +198,8 @@ struct crimson_ctx {
 
     // ElmGMRSclr work space (scalar advection-diffusion)
     crimson::DBuf<double> sclr_qres;       // (nshg, 3) projected diffusive flux, node-major
-    crimson::DBuf<double> sclr_erec;       // (nelem, 20) rl(4) + xSebe(4, 4)
+    crimson::DBuf<double> sclr_erec;       // (nelem, 8) {rl(a), xSebe(a, a)}
+    crimson::DBuf<double> sclr_xoff;       // (nelem, 12) off-diagonal xSebe
     crimson::DBuf<double> sclr_frec;       // (nface, 3) boundary flux terms
     crimson::DBuf<double> sclr_in, sclr_res, sclr_lhs;  // staging for host-pointer calls
 

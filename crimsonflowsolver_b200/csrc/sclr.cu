@@ -136,8 +136,8 @@ __device__ __forceinline__ void sclr_gather_x(const int4 nn, const double4* __re
     }
 }
 
-// Offset of off-diagonal xSebe(a, b), a != b, in an element record.
-__host__ __device__ __forceinline__ int sclr_off(int a, int b) { return 8 + 3 * a + (b < a ? b : b - 1); }
+// Offset of off-diagonal xSebe(a, b), a != b, in an element's xoff record.
+__host__ __device__ __forceinline__ int sclr_off(int a, int b) { return 3 * a + (b < a ? b : b - 1); }
 
 // Per node: the projection sums over the elements containing it (the
 // contributions of its diagonal slot, ascending element order), each
@@ -191,13 +191,16 @@ __global__ void __launch_bounds__(256) k_sclr_qnode(const int* __restrict__ diag
     }
 }
 
-// e3Sclr per element.  Record (20 doubles): {rl(a), xSebe(a, a)} at 2 a, so
-// a node's residual and diagonal entry share one 16-byte load; off-diagonal
-// xSebe(a, b) at sclr_off(a, b).
+// e3Sclr per element.  Two records: erec (8 doubles) holds {rl(a),
+// xSebe(a, a)} at 2 a, so a node's residual and diagonal entry are one
+// 16-byte load and the node pass streams only these; xoff (12 doubles, with
+// the tangent only) holds the off-diagonal xSebe(a, b) at sclr_off(a, b)
+// for the slot pass.
 __global__ void __launch_bounds__(128, 3) k_sclr_elem(const int4* __restrict__ ien, const double4* __restrict__ x,
                                                    const double4* __restrict__ y, const double* __restrict__ s,
                                                    const double* __restrict__ sdot, const double* __restrict__ qres,
-                                                   int nelem, SclrTables T, SclrParams P, double* __restrict__ erec) {
+                                                   int nelem, SclrTables T, SclrParams P, double* __restrict__ erec,
+                                                   double* __restrict__ xoff) {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
         const int4 nn = ien[e];
         const int nd[4] = {nn.x, nn.y, nn.z, nn.w};
@@ -290,12 +293,15 @@ __global__ void __launch_bounds__(128, 3) k_sclr_elem(const int4* __restrict__ i
                 }
             }
         }
-        double4* r = reinterpret_cast<double4*>(erec + 20 * (size_t)e);
+        double4* r = reinterpret_cast<double4*>(erec + 8 * (size_t)e);
         r[0] = make_double4(rl[0], xS[0][0], rl[1], xS[1][1]);
         r[1] = make_double4(rl[2], xS[2][2], rl[3], xS[3][3]);
-        r[2] = make_double4(xS[0][1], xS[0][2], xS[0][3], xS[1][0]);
-        r[3] = make_double4(xS[1][2], xS[1][3], xS[2][0], xS[2][1]);
-        r[4] = make_double4(xS[2][3], xS[3][0], xS[3][1], xS[3][2]);
+        if (P.lhs) {
+            double4* o = reinterpret_cast<double4*>(xoff + 12 * (size_t)e);
+            o[0] = make_double4(xS[0][1], xS[0][2], xS[0][3], xS[1][0]);
+            o[1] = make_double4(xS[1][2], xS[1][3], xS[2][0], xS[2][1]);
+            o[2] = make_double4(xS[2][3], xS[3][0], xS[3][1], xS[3][2]);
+        }
     }
 }
 
@@ -393,7 +399,7 @@ __global__ void __launch_bounds__(256) k_sclr_node(const int* __restrict__ diag,
             for (int j = 0; j < 4; ++j) t[j] = slist[p + j];
             double2 v[4];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) v[j] = rec[10 * (size_t)(t[j] >> 4) + ((t[j] >> 2) & 3)];
+            for (int j = 0; j < 4; ++j) v[j] = rec[4 * (size_t)(t[j] >> 4) + ((t[j] >> 2) & 3)];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 r += v[j].x;
@@ -402,7 +408,7 @@ __global__ void __launch_bounds__(256) k_sclr_node(const int* __restrict__ diag,
         }
         for (; p < p1; ++p) {
             const int t = slist[p];
-            const double2 v = rec[10 * (size_t)(t >> 4) + ((t >> 2) & 3)];
+            const double2 v = rec[4 * (size_t)(t >> 4) + ((t >> 2) & 3)];
             r += v.x;
             k += v.y;
         }
@@ -418,7 +424,7 @@ __global__ void __launch_bounds__(256) k_sclr_node(const int* __restrict__ diag,
 
 // Per off-diagonal CSR entry: the elements' xSebe(a, b) in ascending element order.
 __global__ void __launch_bounds__(256) k_sclr_slot(const int* __restrict__ soff, const int* __restrict__ slist,
-                                                   const double* __restrict__ erec, long long nnz,
+                                                   const double* __restrict__ xoff, long long nnz,
                                                    double* __restrict__ lhsS) {
     for (long long sl = (long long)blockIdx.x * blockDim.x + threadIdx.x; sl < nnz;
          sl += (long long)gridDim.x * blockDim.x) {
@@ -429,7 +435,7 @@ __global__ void __launch_bounds__(256) k_sclr_slot(const int* __restrict__ soff,
         for (int p = p0; p < p1; ++p) {
             const int t = slist[p];
             const int e = t >> 4, a = (t >> 2) & 3, b = t & 3;
-            k += erec[20 * (size_t)e + sclr_off(a, b)];
+            k += xoff[12 * (size_t)e + sclr_off(a, b)];
         }
         lhsS[sl] = k;
     }
@@ -462,10 +468,11 @@ int elmgmr_sclr_device(crimson_ctx* c, int isclr, double diffus, const double* d
     if (c->p.idiff == 1)
         launch(k_sclr_qnode, grid_for(c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->ien.p, c->x.p,
                d_s, c->nshg, T, diffus, c->sclr_qres.p);
-    CR_CHECK(c->sclr_erec.alloc(20 * (size_t)c->nelem));
+    CR_CHECK(c->sclr_erec.alloc(8 * (size_t)c->nelem));
+    if (lhs) CR_CHECK(c->sclr_xoff.alloc(12 * (size_t)c->nelem));
     launch(k_sclr_elem, grid_for(c->nelem, 128, 16), 128, 0, s, c->ien.p, c->x.p,
            reinterpret_cast<const double4*>(d_y), d_s, d_sdot, (const double*)c->sclr_qres.p, c->nelem, T, P,
-           c->sclr_erec.p);
+           c->sclr_erec.p, lhs ? c->sclr_xoff.p : nullptr);
     const bool faces = c->nface > 0 && c->fnoff.p;
     if (faces) {
         CR_CHECK(c->sclr_frec.alloc(3 * (size_t)c->nface));
@@ -476,7 +483,7 @@ int elmgmr_sclr_device(crimson_ctx* c, int isclr, double diffus, const double* d
            (const double*)c->sclr_erec.p, faces ? (const int*)c->fnoff.p : nullptr, (const int*)c->flist.p,
            (const double*)c->sclr_frec.p, c->nshg, c->iBC.p, isclr, P.lhs, d_res, d_lhsS);
     if (lhs)
-        launch(k_sclr_slot, grid_for(c->nnz, 256), 256, 0, s, c->soff.p, c->slist.p, (const double*)c->sclr_erec.p,
+        launch(k_sclr_slot, grid_for(c->nnz, 256), 256, 0, s, c->soff.p, c->slist.p, (const double*)c->sclr_xoff.p,
                c->nnz, d_lhsS);
     CR_CUDA(cudaGetLastError());
     return CRIMSON_OK;
