@@ -702,6 +702,24 @@ def run_microbench(args):
                                  "frac": sclr_bytes / t_s / 1e9 / peak,
                                  "residual_only_ms": t_sr * 1e3}
     del ds, dsd, rs, S
+    if not args.no_cpu:
+        # cpu_baseline of the scalar assembly: the oracle restatement, one
+        # thread, on a 40^3-cell lattice (384,000 tets) with the same fields
+        from oracle import pyoracle as po
+
+        ms = mesh.lattice(40, seed=5)
+        cs, rs_ = po.genadj(ms.ien, ms.nshg)
+        oe = po.Elm(ms, P, cs, rs_)
+        rng = np.random.default_rng(6)
+        ys = rng.standard_normal((ms.nshg, 4))
+        s0, s1 = rng.standard_normal(ms.nshg), rng.standard_normal(ms.nshg)
+        po.elmgmr_sclr(oe, ys, s0, s1, isclr=1, diffus=0.1)
+        t0 = time.perf_counter()
+        po.elmgmr_sclr(oe, ys, s0, s1, isclr=1, diffus=0.1)
+        tc = time.perf_counter() - t0
+        out["assembly_sclr_fp64"]["cpu_baseline"] = {"value": ms.nelem / tc / 1e6, "unit": "Melem/s", "cores": 1,
+                                                     "kind": "port",
+                                                     "sample": f"lattice 40^3 x 6 = {ms.nelem} tets, one call"}
     g = torch.Generator(device=dev).manual_seed(5)
     val = torch.randn((nnz, 16), dtype=torch.float64, device=dev, generator=g)
     u = torch.randn((n, 4), dtype=torch.float64, device=dev, generator=g)

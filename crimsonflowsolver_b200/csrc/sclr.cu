@@ -36,6 +36,7 @@ namespace {
 // boundary rule, shape gradients halved as genshp.f90:35-36).
 struct SclrTables {
     double shp[4][4];    // [intp][n]
+    double M[4][4];      // sum over the points of shp[q][a] shp[q][b]
     double shgl[3][4];   // [dir][n], the same at every point of a linear tet
     double Qwt[4];
     double shpb[3][4];   // boundary points
@@ -53,6 +54,11 @@ SclrTables sclr_tables() {
         t.shp[q][3] = 1.0e0 - r4[q][0] - r4[q][1] - r4[q][2];
         t.Qwt[q] = (4.0 / 3.0) * 0.25;
     }
+    for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) {
+            t.M[a][b] = 0.0;
+            for (int q = 0; q < 4; ++q) t.M[a][b] += t.shp[q][a] * t.shp[q][b];
+        }
     for (int j = 0; j < 3; ++j)
         for (int n = 0; n < 4; ++n) t.shgl[j][n] = (n == 3 ? -1.0e0 : (n == j ? 1.0e0 : 0.0e0)) / 2.0;
     const double B3 = 0.666666666666667, C3 = 0.166666666666667, A3 = 0.3333333333333330000000000000000000;
@@ -217,10 +223,10 @@ __global__ void __launch_bounds__(128, 3) k_sclr_elem(const int4* __restrict__ i
 #pragma unroll
             for (int k = 0; k < 3; ++k) ql[a][k] = P.idiff >= 1 ? qres[3 * (size_t)nd[a] + k] : 0.0;
         }
-        double rl[4] = {0, 0, 0, 0};
-        double xS[4][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
         const double lhsFct = P.alfi * P.gami * P.Delt;
         const double dts = P.Dtgl * P.dtsfct;
+        // linear tet, equal weights: metric, W, grad S, div q and g_ij are
+        // the same at the 4 points
         double dxidx[3][3], shg[4][3], W;
         sclr_metric(xl, T.shgl, T.Qwt[0], dxidx, shg, &W);
         double gS[3] = {0.0, 0.0, 0.0};
@@ -238,60 +244,94 @@ __global__ void __launch_bounds__(128, 3) k_sclr_elem(const int4* __restrict__ i
         const double tauDiff = 9.0 * (P.diffus * P.diffus) *
                                (g[0] * g[0] + g[1] * g[1] + g[2] * g[2] +
                                 2.0 * (g[3] * g[3] + g[4] * g[4] + g[5] * g[5]));
+        // Per point only what depends on the interpolated u and Sdot: the
+        // stabilisation tauS (e3StabSclr, ivart = 2, ipord = 1, no sources)
+        // and the sums it enters.  With c_a = u . grad N_a:
+        //   V       = sum_q tauS rLS u           (SUPG residual flux)
+        //   A(a, b) = sum_q tauS c_a N_b         (SUPG mass, e3LHSSclr's flipped term)
+        //   B(a, b) = sum_q tauS c_a c_b         (SUPG convection)
+        double V[3] = {0.0, 0.0, 0.0}, A[4][4], B[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) A[a][b] = B[a][b] = 0.0;
+#pragma unroll
         for (int q = 0; q < 4; ++q) {
             const double* shp = T.shp[q];
-            double u1 = 0.0, u2 = 0.0, u3 = 0.0;
+            double u1 = 0.0, u2 = 0.0, u3 = 0.0, Sdot = 0.0;
 #pragma unroll
             for (int n = 0; n < 4; ++n) {
                 u1 = u1 + shp[n] * ul[n][0];
                 u2 = u2 + shp[n] * ul[n][1];
                 u3 = u3 + shp[n] * ul[n][2];
+                Sdot = Sdot + shp[n] * sdl[n];
             }
-            double Sdot = 0.0;
-#pragma unroll
-            for (int n = 0; n < 4; ++n) Sdot = Sdot + shp[n] * sdl[n];
             const double rLS = (Sdot + (u1 * gS[0] + u2 * gS[1] + u3 * gS[2])) - divS;
-            // e3StabSclr (ivart = 2, ipord = 1, no sources)
-            const double tauT = (2.0 * dts) * (2.0 * dts) + 0.0 * 0.0 + u1 * (g[0] * u1 + g[3] * u2 + g[5] * u3) +
+            const double tauT = (2.0 * dts) * (2.0 * dts) + u1 * (g[0] * u1 + g[3] * u2 + g[5] * u3) +
                                 u2 * (g[3] * u1 + g[1] * u2 + g[4] * u3) + u3 * (g[5] * u1 + g[4] * u2 + g[2] * u3) +
                                 tauDiff;
             const double tauS = 1.0 / sqrt(tauT);
-            // e3ResSclr (flmpr = 0)
-            const double rNa = 1.0 * (1.0 * Sdot + u1 * gS[0] + u2 * gS[1] + u3 * gS[2]) - 0.0;
-            const double tmp = 1.0 * tauS * (rLS - 0.0);
-            const double rG0 = P.diffus * gS[0] + u1 * tmp, rG1 = P.diffus * gS[1] + u2 * tmp,
-                         rG2 = P.diffus * gS[2] + u3 * tmp;
+            const double tmp = tauS * rLS;
+            V[0] = V[0] + tmp * u1;
+            V[1] = V[1] + tmp * u2;
+            V[2] = V[2] + tmp * u3;
+            if (P.lhs) {
+                double c[4];
 #pragma unroll
-            for (int a = 0; a < 4; ++a)
-                rl[a] = rl[a] - W * (shp[a] * rNa + shg[a][0] * rG0 + shg[a][1] * rG1 + shg[a][2] * rG2);
-            if (!P.lhs) continue;
-            // e3LHSSclr (flmpl = 0, no sources)
-            const double tauSl = lhsFct * W * tauS;
-            const double kptmp = lhsFct * W * P.diffus;
-            const double tsFct = P.almi * W * 1.0;
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const double t1 = W * (u1 * shg[b][0] + u2 * shg[b][1] + u3 * shg[b][2]);
-                const double t2 = t1 * tauS;
+                for (int a = 0; a < 4; ++a) c[a] = u1 * shg[a][0] + u2 * shg[a][1] + u3 * shg[a][2];
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
-                    xS[a][b] = xS[a][b] + shp[a] * shp[b] * (tsFct + 0.0) + shp[a] * lhsFct * t1;
-                    xS[b][a] = xS[b][a] + t2 * shp[a];
+                    const double tc = tauS * c[a];
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) A[a][b] = A[a][b] + tc * shp[b];
+#pragma unroll
+                    for (int b = a; b < 4; ++b) B[a][b] = B[a][b] + tc * c[b];
                 }
             }
+        }
+        // the point sums of the q-independent terms: sum_q N_a X_q = (M X)_a
+        double Mu[4][3], Msd[4];
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const double tb = tauSl * (u1 * shg[b][0] + u2 * shg[b][1] + u3 * shg[b][2]);
-                const double t0 = kptmp * shg[b][0] + u1 * tb, t1 = kptmp * shg[b][1] + u2 * tb,
-                             t2 = kptmp * shg[b][2] + u3 * tb;
-                xS[b][b] = xS[b][b] + t0 * shg[b][0] + t1 * shg[b][1] + t2 * shg[b][2];
+        for (int a = 0; a < 4; ++a) {
+            Mu[a][0] = Mu[a][1] = Mu[a][2] = Msd[a] = 0.0;
 #pragma unroll
-                for (int a = b + 1; a < 4; ++a) {
-                    const double v = t0 * shg[a][0] + t1 * shg[a][1] + t2 * shg[a][2];
-                    xS[a][b] = xS[a][b] + v;
-                    xS[b][a] = xS[b][a] + v;
-                }
+            for (int n = 0; n < 4; ++n) {
+                Mu[a][0] = Mu[a][0] + T.M[a][n] * ul[n][0];
+                Mu[a][1] = Mu[a][1] + T.M[a][n] * ul[n][1];
+                Mu[a][2] = Mu[a][2] + T.M[a][n] * ul[n][2];
+                Msd[a] = Msd[a] + T.M[a][n] * sdl[n];
             }
+        }
+        // e3ResSclr summed over the points (flmpr = 0):
+        //   rl(a) = -W [ (M Sdot)_a + (M u)_a . grad S + 4 diffus grad N_a . grad S + grad N_a . V ]
+        double rl[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const double gg = shg[a][0] * gS[0] + shg[a][1] * gS[1] + shg[a][2] * gS[2];
+            const double gv = shg[a][0] * V[0] + shg[a][1] * V[1] + shg[a][2] * V[2];
+            const double mg = Mu[a][0] * gS[0] + Mu[a][1] * gS[1] + Mu[a][2] * gS[2];
+            rl[a] = -W * (Msd[a] + mg + 4.0 * P.diffus * gg + gv);
+        }
+        // e3LHSSclr summed over the points (flmpl = 0, no sources):
+        //   xS(a, b) = almi W M_ab + lhsFct W (M u)_a . grad N_b + W A(a, b)
+        //            + lhsFct W (4 diffus grad N_a . grad N_b + B(a, b))
+        double xS[4][4];
+        if (P.lhs) {
+            const double lw = lhsFct * W, mw = P.almi * W, d4 = 4.0 * P.diffus;
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const double conv = Mu[a][0] * shg[b][0] + Mu[a][1] * shg[b][1] + Mu[a][2] * shg[b][2];
+                    const double gab = shg[a][0] * shg[b][0] + shg[a][1] * shg[b][1] + shg[a][2] * shg[b][2];
+                    const double bab = a <= b ? B[a][b] : B[b][a];
+                    xS[a][b] = mw * T.M[a][b] + lw * conv + W * A[a][b] + lw * (d4 * gab + bab);
+                }
+        } else {
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) xS[a][b] = 0.0;
         }
         double4* r = reinterpret_cast<double4*>(erec + 8 * (size_t)e);
         r[0] = make_double4(rl[0], xS[0][0], rl[1], xS[1][1]);
