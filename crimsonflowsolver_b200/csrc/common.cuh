@@ -198,6 +198,7 @@ struct crimson_ctx {
 
     // ElmGMRSclr work space (scalar advection-diffusion)
     crimson::DBuf<double> sclr_qres;       // (nshg, 3) projected diffusive flux, node-major
+    crimson::DBuf<double> sclr_qrec;       // (nelem, 4) {diffus grad S, W}
     crimson::DBuf<double> sclr_erec;       // (nelem, 8) {rl(a), xSebe(a, a)}
     crimson::DBuf<double> sclr_xoff;       // (nelem, 12) off-diagonal xSebe
     crimson::DBuf<double> sclr_frec;       // (nface, 3) boundary flux terms

@@ -2,11 +2,11 @@
 // tangent of the advection-diffusion equation of one scalar, assembled with
 // the same deterministic owner-computes scheme as ElmGMR.
 //
-//   k_sclr_qnode  AsIqSclr / e3qSclr (asiq.f90:89-125, e3q.f90:215-300) and
-//                 qpbcSclr (qpbc.f90:118-175) per node: the lumped-projection
-//                 contributions of q = diffus grad S and of the lumped mass
-//                 of each element containing the node, summed in ascending
-//                 element order, then qres = q / rmass
+//   k_sclr_q      AsIqSclr / e3qSclr (asiq.f90:89-125, e3q.f90:215-300) per
+//                 element: q = diffus grad S and W, the same at every point
+//   k_sclr_qnode  per node: the lumped-projection contributions of q and of
+//                 the lumped mass of the elements containing it, then
+//                 qpbcSclr (qpbc.f90:118-175): qres = q / rmass
 //   k_sclr_elem   AsIGMRSclr / e3Sclr (asigmr.f90:141-190, e3.f90:183-330):
 //                 per element the residual rows rl(a) and the 4x4 tangent
 //                 xSebe (e3ivarSclr, e3StabSclr, e3ResSclr, e3LHSSclr)
@@ -16,6 +16,10 @@
 //                 diagonal tangent entry; bc3ResSclr (bc3res.f90:138-160)
 //   k_sclr_slot   per off-diagonal CSR entry: fillsparseSclr's sum
 //                 (fillsparse.f90:167-200) in ascending element order
+//
+// The node passes give each node kNodeLanes lanes and combine their sums in
+// a fixed order; the slot pass sums each entry's short list in element
+// order.  Every result is bitwise repeatable.
 //
 // Settings as the reference's defaults for a passive scalar: diffusivity
 // scdiff(isclr) (getdiff.f90:145-174), the flow velocity as convection
@@ -145,55 +149,87 @@ __device__ __forceinline__ void sclr_gather_x(const int4 nn, const double4* __re
 // Offset of off-diagonal xSebe(a, b), a != b, in an element's xoff record.
 __host__ __device__ __forceinline__ int sclr_off(int a, int b) { return 3 * a + (b < a ? b : b - 1); }
 
-// Per node: the projection sums over the elements containing it (the
-// contributions of its diagonal slot, ascending element order), each
-// element's contribution to this node recomputed from the element's
-// gathers (the metric and grad S are cheap next to a record round trip
-// through memory), then qpbcSclr: qres = (1 / rmass) q.
-__device__ __forceinline__ void sclr_q_contrib(const int4* __restrict__ ien, const double4* __restrict__ x,
-                                               const double* __restrict__ s, const SclrTables& T, double diffus,
-                                               int t, double& q0, double& q1, double& q2, double& m) {
-    const int e = t >> 4, a = (t >> 2) & 3;
-    const int4 nn = ien[e];
-    double xl[4][3];
-    sclr_gather_x(nn, x, xl);
-    const double sl[4] = {s[nn.x], s[nn.y], s[nn.z], s[nn.w]};
-    double dxidx[3][3], shg[4][3], W;
-    sclr_metric(xl, T.shgl, T.Qwt[0], dxidx, shg, &W);
-    double gT[3] = {0.0, 0.0, 0.0};
+// Lanes per node in the node passes: the contributions of a node are split
+// round-robin over kNodeLanes lanes (lane l sums entries l, l + kNodeLanes,
+// ... in list order), then combined by a fixed butterfly, so every result is
+// the same bit for bit on every run.
+constexpr int kNodeLanes = 8;
+
+__device__ __forceinline__ double lanes_sum(double v) {
 #pragma unroll
-    for (int n = 0; n < 4; ++n)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) gT[k] = gT[k] + shg[n][k] * sl[n];
-    const double qdi[3] = {diffus * gT[0], diffus * gT[1], diffus * gT[2]};
-    double ql[3] = {0.0, 0.0, 0.0}, rm = 0.0;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const double sa = T.shp[q][a];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) ql[k] = ql[k] + sa * W * qdi[k];
-        rm = rm + sa * W;
-    }
-    q0 += ql[0];
-    q1 += ql[1];
-    q2 += ql[2];
-    m += rm;
+    for (int o = kNodeLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
 
+// AsIqSclr / e3qSclr per element: the point-independent part of the flux
+// projection, {qdi = diffus grad S, W} (32 bytes); a linear tet's metric, W
+// and grad S are the same at the 4 points.
+__global__ void __launch_bounds__(128) k_sclr_q(const int4* __restrict__ ien, const double4* __restrict__ x,
+                                                const double* __restrict__ s, int nelem, SclrTables T,
+                                                double diffus, double4* __restrict__ qrec) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
+        const int4 nn = ien[e];
+        double xl[4][3];
+        sclr_gather_x(nn, x, xl);
+        const double sl[4] = {s[nn.x], s[nn.y], s[nn.z], s[nn.w]};
+        double dxidx[3][3], shg[4][3], W;
+        sclr_metric(xl, T.shgl, T.Qwt[0], dxidx, shg, &W);
+        double gT[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int n = 0; n < 4; ++n)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) gT[k] = gT[k] + shg[n][k] * sl[n];
+        qrec[e] = make_double4(diffus * gT[0], diffus * gT[1], diffus * gT[2], W);
+    }
+}
+
+// Per node: the lumped-projection sums over the elements containing it (the
+// contributions of its diagonal slot), each contribution
+// ql(a) = sum_q N_a(q) W qdi and rmassl(a) = sum_q N_a(q) W as e3qSclr
+// accumulates them, then qpbcSclr: qres = (1 / rmass) q.
 __global__ void __launch_bounds__(256) k_sclr_qnode(const int* __restrict__ diag, const int* __restrict__ soff,
-                                                    const int* __restrict__ slist, const int4* __restrict__ ien,
-                                                    const double4* __restrict__ x, const double* __restrict__ s,
-                                                    int nshg, SclrTables T, double diffus,
-                                                    double* __restrict__ qres) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
+                                                    const int* __restrict__ slist, const double4* __restrict__ qrec,
+                                                    int nshg, SclrTables T, double* __restrict__ qres) {
+    constexpr int NPW = 32 / kNodeLanes;   // nodes per warp and pass
+    const int lane = threadIdx.x & 31, sub = lane % kNodeLanes;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    // warp-uniform loop: the shuffles below always see all 32 lanes
+    for (long long i0 = warp * NPW; i0 < nshg; i0 += nwarp * NPW) {
+        const long long ig = i0 + lane / kNodeLanes;
+        const bool valid = ig < nshg;
+        const int i = valid ? (int)ig : nshg - 1;
         const int d = diag[i];
         double q0 = 0.0, q1 = 0.0, q2 = 0.0, m = 0.0;
         const int p1 = soff[d + 1];
-        for (int p = soff[d]; p < p1; ++p) sclr_q_contrib(ien, x, s, T, diffus, slist[p], q0, q1, q2, m);
-        const double rinv = 1.0 / m;
-        qres[3 * (size_t)i] = rinv * q0;
-        qres[3 * (size_t)i + 1] = rinv * q1;
-        qres[3 * (size_t)i + 2] = rinv * q2;
+        for (int p = soff[d] + sub; p < p1; p += kNodeLanes) {
+            const int t = slist[p];
+            const int a = (t >> 2) & 3;
+            const double4 r = qrec[t >> 4];
+            double ql0 = 0.0, ql1 = 0.0, ql2 = 0.0, rm = 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double sw = T.shp[q][a] * r.w;
+                ql0 = ql0 + sw * r.x;
+                ql1 = ql1 + sw * r.y;
+                ql2 = ql2 + sw * r.z;
+                rm = rm + sw;
+            }
+            q0 += ql0;
+            q1 += ql1;
+            q2 += ql2;
+            m += rm;
+        }
+        q0 = lanes_sum(q0);
+        q1 = lanes_sum(q1);
+        q2 = lanes_sum(q2);
+        m = lanes_sum(m);
+        if (valid && sub == 0) {
+            const double rinv = 1.0 / m;
+            qres[3 * (size_t)i] = rinv * q0;
+            qres[3 * (size_t)i + 1] = rinv * q1;
+            qres[3 * (size_t)i + 2] = rinv * q2;
+        }
     }
 }
 
@@ -426,39 +462,38 @@ __global__ void __launch_bounds__(256) k_sclr_node(const int* __restrict__ diag,
                                                    const double* __restrict__ frec, int nshg,
                                                    const int* __restrict__ iBC, int isclr, int lhs,
                                                    double* __restrict__ res, double* __restrict__ lhsS) {
+    constexpr int NPW = 32 / kNodeLanes;
     const double2* rec = reinterpret_cast<const double2*>(erec);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31, sub = lane % kNodeLanes;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long i0 = warp * NPW; i0 < nshg; i0 += nwarp * NPW) {
+        const long long ig = i0 + lane / kNodeLanes;
+        const bool valid = ig < nshg;
+        const int i = valid ? (int)ig : nshg - 1;
         const int d = diag[i];
         double r = 0.0, k = 0.0;
-        int p = soff[d];
         const int p1 = soff[d + 1];
-        // four independent loads in flight, summed in list order
-        for (; p + 4 <= p1; p += 4) {
-            int t[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) t[j] = slist[p + j];
-            double2 v[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) v[j] = rec[4 * (size_t)(t[j] >> 4) + ((t[j] >> 2) & 3)];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                r += v[j].x;
-                k += v[j].y;
-            }
-        }
-        for (; p < p1; ++p) {
+        for (int p = soff[d] + sub; p < p1; p += kNodeLanes) {
             const int t = slist[p];
             const double2 v = rec[4 * (size_t)(t >> 4) + ((t >> 2) & 3)];
             r += v.x;
             k += v.y;
         }
-        if (fnoff) {
+        // faces after the elements, on the node's first lane
+        if (fnoff && sub == 0) {
+            double rf = 0.0;
             const int f1 = fnoff[i + 1];
-            for (int pf = fnoff[i]; pf < f1; ++pf) r += frec[flist[pf]];
+            for (int pf = fnoff[i]; pf < f1; ++pf) rf += frec[flist[pf]];
+            r = r + rf;
         }
-        if ((iBC[i] >> (isclr + 5)) & 1) r = 0.0;
-        res[i] = r;
-        if (lhs) lhsS[d] = k;
+        r = lanes_sum(r);
+        k = lanes_sum(k);
+        if (valid && sub == 0) {
+            if ((iBC[i] >> (isclr + 5)) & 1) r = 0.0;
+            res[i] = r;
+            if (lhs) lhsS[d] = k;
+        }
     }
 }
 
@@ -505,9 +540,13 @@ int elmgmr_sclr_device(crimson_ctx* c, int isclr, double diffus, const double* d
     P.isclr = isclr;
     P.lhs = lhs ? 1 : 0;
     CR_CHECK(c->sclr_qres.alloc(3 * (size_t)c->nshg));
-    if (c->p.idiff == 1)
-        launch(k_sclr_qnode, grid_for(c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->ien.p, c->x.p,
-               d_s, c->nshg, T, diffus, c->sclr_qres.p);
+    if (c->p.idiff == 1) {
+        CR_CHECK(c->sclr_qrec.alloc(4 * (size_t)c->nelem));
+        double4* qrec = reinterpret_cast<double4*>(c->sclr_qrec.p);
+        launch(k_sclr_q, grid_for(c->nelem, 128, 16), 128, 0, s, c->ien.p, c->x.p, d_s, c->nelem, T, diffus, qrec);
+        launch(k_sclr_qnode, grid_for((long long)kNodeLanes * c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p,
+               c->slist.p, (const double4*)qrec, c->nshg, T, c->sclr_qres.p);
+    }
     CR_CHECK(c->sclr_erec.alloc(8 * (size_t)c->nelem));
     if (lhs) CR_CHECK(c->sclr_xoff.alloc(12 * (size_t)c->nelem));
     launch(k_sclr_elem, grid_for(c->nelem, 128, 16), 128, 0, s, c->ien.p, c->x.p,
@@ -519,7 +558,7 @@ int elmgmr_sclr_device(crimson_ctx* c, int isclr, double diffus, const double* d
         launch(k_sclr_face, grid_for(c->nface, 128, 16), 128, 0, s, c->ienb.p, c->iBCB.p, d_bcbs, c->x.p, d_s,
                c->nface, T, P, c->sclr_frec.p);
     }
-    launch(k_sclr_node, grid_for(c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p, c->slist.p,
+    launch(k_sclr_node, grid_for((long long)kNodeLanes * c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p, c->slist.p,
            (const double*)c->sclr_erec.p, faces ? (const int*)c->fnoff.p : nullptr, (const int*)c->flist.p,
            (const double*)c->sclr_frec.p, c->nshg, c->iBC.p, isclr, P.lhs, d_res, d_lhsS);
     if (lhs)
