@@ -23,13 +23,15 @@
 //
 // Scatter: owner-computes, deterministic.  The element kernel writes one
 // record per element (its residual rows and the tangent's element constants
-// above: 48 doubles); it never writes a global sum.  A node pass then forms,
+// above: 52 doubles); it never writes a global sum.  A node pass then forms,
 // for every node, the residual row and the diagonal tangent block from the
 // records of the elements containing it, and a slot pass forms every
 // off-diagonal CSR block from the records of the elements containing that
-// edge.  Each sum runs over the pattern pass's contribution list of the slot
-// in ascending element order -- the order of the reference's serial
-// scatter (local.f90:64-75, fillsparse.f90:47-60) -- so every result is the
+// edge.  Each sum runs over the pattern pass's contribution list of the
+// slot (ascending element order, the order of the reference's serial
+// scatter, local.f90:64-75, fillsparse.f90:47-60): the slot pass in that
+// order, the node pass over kOwnerLanes lanes per node that take the list
+// round-robin and combine in a fixed butterfly -- so every result is the
 // same bit for bit on every run.  Records are written once and re-read by
 // the 4 (node pass) and 12 (slot pass) owners of their element, mostly from
 // L2 on banded node numberings.
@@ -174,9 +176,22 @@ __device__ __forceinline__ float sel4(const float4& v, int a) {
 // AsIq + e3q: lumped projection of the viscous flux q = mu (grad u + grad u^T)
 // (asiq.f90:52-70, e3q.f90:58-145).  On a linear tet qdi is constant, so
 // ql(a,k) = WdetJ sum_q N_a(q) qdi(k) and rmassl(a) = WdetJ sum_q N_a(q).
+// Lanes per node in the node passes (k_q_node, k_node_pass).
+#ifndef CRIMSON_OWNER_LANES
+#define CRIMSON_OWNER_LANES 4
+#endif
+constexpr int kOwnerLanes = CRIMSON_OWNER_LANES;
+
+// Sum over a node's kOwnerLanes lanes in a fixed butterfly order.
+__device__ __forceinline__ double owner_sum(double v) {
+#pragma unroll
+    for (int o = kOwnerLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // k_asiq_rec writes one record per element: {WdetJ, q11, q12, q13, q22, q23,
 // q33, 0} (qdi is symmetric); k_q_node sums, per node, the records of the
-// elements containing it in ascending element order and applies qpbc
+// elements containing it (kOwnerLanes lanes, fixed combining order) and applies qpbc
 // (qpbc.f90:67-71).  The lumped mass depends on the geometry only: it is
 // summed and inverted on a context's first call and kept (rmass).
 // ---------------------------------------------------------------------------
@@ -217,11 +232,18 @@ __global__ void __launch_bounds__(256) k_q_node(const int* __restrict__ diag, co
                                                 const int* __restrict__ slist, const double* __restrict__ qrec,
                                                 int nshg, int first, double* __restrict__ rmass,
                                                 double* __restrict__ qres) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
+    constexpr int NPW = 32 / kOwnerLanes;
+    const int lane = threadIdx.x & 31, sub = lane % kOwnerLanes;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long i0 = warp * NPW; i0 < nshg; i0 += nwarp * NPW) {
+        const long long ig = i0 + lane / kOwnerLanes;
+        const bool valid = ig < nshg;
+        const int i = valid ? (int)ig : nshg - 1;
         const int d = diag[i];
         double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, m = 0.0;
         const int p1 = soff[d + 1];
-        for (int p = soff[d]; p < p1; ++p) {
+        for (int p = soff[d] + sub; p < p1; p += kOwnerLanes) {
             const int t = slist[p];
             const int e = t >> 4, a = (t >> 2) & 3;
             const double4* r = reinterpret_cast<const double4*>(qrec + 8 * (size_t)e);
@@ -233,6 +255,10 @@ __global__ void __launch_bounds__(256) k_q_node(const int* __restrict__ diag, co
             for (int k = 0; k < 9; ++k) q[k] += wa * qd[k];
             m += wa;
         }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) q[k] = owner_sum(q[k]);
+        m = owner_sum(m);
+        if (!valid || sub != 0) continue;
         double r;
         if (first) {
             r = 1.0 / m;
@@ -250,11 +276,12 @@ __global__ void __launch_bounds__(256) k_q_node(const int* __restrict__ diag, co
 // AsIGMR / e3 / e3LHS, four lanes per element, writing element records.
 //
 // Record of element e (RS doubles at erec + RS e, every group 32-byte aligned):
-//   kLhs == 1 (FP64 tangent), RS = 48:
+//   kLhs == 1 (FP64 tangent), RS = 52:
 //     [0:4)   tc, tm, tlW, cc = tlW/rho sum_q tauM_q
-//     [4:16)  shg transposed: shg[n][k] at 4 + 4k + n
-//     [16:32) Kd(a,b) at 16 + 4a + b
-//     [32:48) rl(a, 0:4) at 32 + 4a  (momentum 1-3, continuity)
+//     [4:20)  grad N_a = (shg[a][0..2], 0) at 4 + 4a: a block (a, b) reads
+//             {tc..cc}, grad N_a, grad N_b and Kd(a,b), four sectors
+//     [20:36) Kd(a,b) at 20 + 4a + b
+//     [36:52) rl(a, 0:4) at 36 + 4a  (momentum 1-3, continuity)
 //   kLhs == 2 (FP32 tangent quadrature), RS = 32: rl at [0:16), then 32
 //     floats at double offset 16 with the FP32 layout of [0:32) above.
 //   kLhs == 0 (residual only), RS = 16: rl at [0:16).
@@ -268,8 +295,8 @@ constexpr int kQE = 4 * kQ + 1;
 
 template <int kLhs>
 struct RecLayout {
-    static constexpr int RS = kLhs == 1 ? 48 : (kLhs == 2 ? 32 : 16);
-    static constexpr int RO = kLhs == 1 ? 32 : 0;
+    static constexpr int RS = kLhs == 1 ? 52 : (kLhs == 2 ? 32 : 16);
+    static constexpr int RO = kLhs == 1 ? 36 : 0;
 };
 
 // Four blocks of 128 threads per SM (128 registers).
@@ -489,11 +516,9 @@ __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien,
                 Kd[b] = tsFct * c_el.M[a][b] + tlW * (rho * conv + 4.0 * mu * grad + sym);
             }
             double4* r4 = reinterpret_cast<double4*>(rec);
-            r4[4 + a] = make_double4(Kd[0], Kd[1], Kd[2], Kd[3]);
-            if (a < 3)
-                r4[1 + a] = make_double4(shg[0][a], shg[1][a], shg[2][a], shg[3][a]);
-            else
-                r4[0] = make_double4(tlW * TC, tlW * 4.0 * mu, tlW, tlW / rho * TM);
+            r4[5 + a] = make_double4(Kd[0], Kd[1], Kd[2], Kd[3]);
+            r4[1 + a] = make_double4(shg[a][0], shg[a][1], shg[a][2], 0.0);
+            if (a == 3) r4[0] = make_double4(tlW * TC, tlW * 4.0 * mu, tlW, tlW / rho * TM);
         }
         if (kLhs == 2 && live) {
             // FP32 element quadrature of the tangent
@@ -559,10 +584,10 @@ template <int kLhs>
 __device__ __forceinline__ void record_block(const double* __restrict__ rec, int a, int b, double o[13]) {
     if (kLhs == 1) {
         const double4* r4 = reinterpret_cast<const double4*>(rec);
-        const double4 sc = r4[0], s0 = r4[1], s1 = r4[2], s2 = r4[3];
-        const double sa[3] = {sel4(s0, a), sel4(s1, a), sel4(s2, a)};
-        const double sb[3] = {sel4(s0, b), sel4(s1, b), sel4(s2, b)};
-        const double Kd = rec[16 + 4 * a + b];
+        const double4 sc = r4[0], ga = r4[1 + a], gb = r4[1 + b];
+        const double sa[3] = {ga.x, ga.y, ga.z};
+        const double sb[3] = {gb.x, gb.y, gb.z};
+        const double Kd = rec[20 + 4 * a + b];
         pair_block<double>(sa, sb, Kd, sc.x, sc.y, sc.z * c_el.SN[a], sc.w, o);
     } else {
         const float* rf = reinterpret_cast<const float*>(rec + 16);
@@ -689,7 +714,10 @@ __device__ __forceinline__ void bc_diag(const NodeBC& n, double K[9], double v) 
 // Node pass: residual row and diagonal tangent block of every node.  The
 // elements containing node i are the contributions of its diagonal slot
 // (ascending element order); then the boundary faces at i (ascending face
-// order, AsBMFG after AsIGMR as in elmgmr.f90).  One thread per node.  For a
+// order, AsBMFG after AsIGMR as in elmgmr.f90).  kOwnerLanes lanes per node
+// split the element contributions round-robin (lane l: entries l,
+// l + kOwnerLanes, ... in list order) and combine them by a fixed butterfly
+// (owner_sum), so the sums are bitwise repeatable; the faces follow.  For a
 // partially constrained node every element block gets bc3LHS (columns, rows,
 // 1 on the constrained diagonal), and the boundary elements at the node --
 // whose rigid-wall tangent is zero -- add 1 each to those entries, as the
@@ -704,7 +732,15 @@ __global__ void __launch_bounds__(256) k_node_pass(const int* __restrict__ diag,
                                                    double* __restrict__ res, double* __restrict__ lhsK,
                                                    double* __restrict__ lhsP, float* __restrict__ lhs32) {
     constexpr int RS = RecLayout<kLhs>::RS, RO = RecLayout<kLhs>::RO;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nshg; i += gridDim.x * blockDim.x) {
+    constexpr int NPW = 32 / kOwnerLanes;  // nodes per warp and pass
+    const int lane = threadIdx.x & 31, sub = lane % kOwnerLanes;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    // warp-uniform loop: the shuffles of owner_sum always see all 32 lanes
+    for (long long i0 = warp * NPW; i0 < nshg; i0 += nwarp * NPW) {
+        const long long ig = i0 + lane / kOwnerLanes;
+        const bool valid = ig < nshg;
+        const int i = valid ? (int)ig : nshg - 1;
         const int d = diag[i];
         double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
         double acc[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -712,7 +748,7 @@ __global__ void __launch_bounds__(256) k_node_pass(const int* __restrict__ diag,
         if (kLhs && kProj) nb = node_bc(iBC, BC, ndofBC, i);
         const bool proj = kLhs && kProj && bc_partial(nb.m);
         const int p1 = soff[d + 1];
-        for (int p = soff[d]; p < p1; ++p) {
+        for (int p = soff[d] + sub; p < p1; p += kOwnerLanes) {
             const int t = slist[p];
             const int e = t >> 4, a = (t >> 2) & 3;
             const double* rec = erec + (size_t)RS * (size_t)e;
@@ -733,6 +769,15 @@ __global__ void __launch_bounds__(256) k_node_pass(const int* __restrict__ diag,
                 for (int c = 0; c < 13; ++c) acc[c] += o[c];
             }
         }
+        r0 = owner_sum(r0);
+        r1 = owner_sum(r1);
+        r2 = owner_sum(r2);
+        r3 = owner_sum(r3);
+        if (kLhs) {
+#pragma unroll
+            for (int c = 0; c < 13; ++c) acc[c] = owner_sum(acc[c]);
+        }
+        if (!valid || sub != 0) continue;
         if (proj && bcount)
             for (int k = 0; k < bcount[i]; ++k)
 #pragma unroll
@@ -975,7 +1020,7 @@ __global__ void k_bc3res(const int* __restrict__ iBC, const double* __restrict__
 // Grid caps (blocks of 256 per SM) of the owner passes: a grid-stride loop
 // over rows / slots in order, so the cap sets how many rows are in flight.
 #ifndef CRIMSON_NODE_PASS_BLOCKS_PER_SM
-#define CRIMSON_NODE_PASS_BLOCKS_PER_SM 2
+#define CRIMSON_NODE_PASS_BLOCKS_PER_SM 8
 #endif
 #ifndef CRIMSON_SLOT_PASS_BLOCKS_PER_SM
 #define CRIMSON_SLOT_PASS_BLOCKS_PER_SM 32
@@ -1000,12 +1045,12 @@ int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const d
         CR_CHECK(c->qrec.alloc((size_t)c->nelem * 8));
         const bool first = !c->rmass_ready;
         launch(k_asiq_rec, grid_for(c->nelem, 128, 16), 128, 0, s, c->ien.p, c->x.p, y4, c->nelem, P, c->qrec.p);
-        launch(k_q_node, grid_for(c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->qrec.p, c->nshg,
+        launch(k_q_node, grid_for((long long)kOwnerLanes * c->nshg, 256), 256, 0, s, c->diag.p, c->soff.p, c->slist.p, c->qrec.p, c->nshg,
                first ? 1 : 0, c->rmass.p, c->qres.p);
         c->rmass_ready = true;
     }
     // element records (sized for the FP64 tangent layout, the largest)
-    CR_CHECK(c->erec.alloc((size_t)c->nelem * 48));
+    CR_CHECK(c->erec.alloc((size_t)c->nelem * RecLayout<1>::RS));
     const int blk = 128;
     const int grid = grid_for((long long)c->nelem * 4, blk, 16);
     if (lhs == 2)
@@ -1021,7 +1066,7 @@ int elmgmr_device(crimson_ctx* c, const double* d_y, const double* d_ac, const d
                c->frec.p);
     }
     const int* fno = c->nface > 0 ? c->fnoff.p : nullptr;
-    const int ng = grid_for(c->nshg, 256, kNodePassBlocksPerSM);
+    const int ng = grid_for((long long)kOwnerLanes * c->nshg, 256, kNodePassBlocksPerSM);
     const int gs = grid_for(c->nnz, 256, kSlotPassBlocksPerSM);
     // the bc3LHS projection is compiled into separate pass variants, used only
     // when some node has one or two prescribed velocity components
