@@ -236,6 +236,8 @@ int crimson_ctx_create(crimson_ctx** out, const crimson_params* p, int nshg, int
     std::vector<double> zb((size_t)nshg * nbc, 0.0);
     c->h_BC.assign(zb.begin(), zb.end());
     c->h_iBC.assign(nshg, 0);
+    c->h_iBC_orig.assign(nshg, 0);
+    c->h_x.assign(x, x + 3 * (size_t)numnp);
     if (rc == CRIMSON_OK) rc = c->BC.upload(zb.data(), zb.size(), c->stream);
     if (rc == CRIMSON_OK) {
         cudaError_t e2 = cudaStreamSynchronize(c->stream);
@@ -287,6 +289,7 @@ int crimson_set_bc(crimson_ctx* c, const int* iBC, const double* BC) {
     for (int i = 0; i < n; ++i)
         for (int k = 0; k < nb; ++k) nm[(size_t)nb * i + k] = BC[(size_t)k * n + i];
     c->h_iBC.assign(iBC, iBC + n);
+    c->h_iBC_orig.assign(iBC, iBC + n);
     c->h_BC.assign(BC, BC + (size_t)n * nb);
     CR_CHECK(c->iBC.upload(iBC, n, c->stream));
     CR_CHECK(c->BC.upload(nm.data(), nm.size(), c->stream));
@@ -297,7 +300,11 @@ int crimson_set_bc(crimson_ctx* c, const int* iBC, const double* BC) {
 int crimson_set_boundary(crimson_ctx* c, int nface, const int* ienb, const int* iBCB, const double* BCB) {
     if (!c || nface < 0 || (nface > 0 && (!ienb || !iBCB))) return CRIMSON_ERR_ARG;
     c->nface = nface;
-    if (nface == 0) return CRIMSON_OK;
+    if (nface == 0) {
+        c->h_iBCB.clear();
+        c->h_ienb.clear();
+        return CRIMSON_OK;
+    }
     std::vector<int4> hb(nface);
     std::vector<int> hbits(nface);
     std::vector<double> hbcb((size_t)nface * 18, 0.0);
@@ -329,6 +336,7 @@ int crimson_set_boundary(crimson_ctx* c, int nface, const int* ienb, const int* 
     CR_CHECK(c->ienb.upload(hb.data(), hb.size(), c->stream));
     CR_CHECK(c->iBCB.upload(hbits.data(), hbits.size(), c->stream));
     c->h_iBCB = hbits;
+    c->h_ienb = hb;
     CR_CHECK(c->BCB.upload(hbcb.data(), hbcb.size(), c->stream));
     // boundary elements (all four nodes) at each node: bc3LHS puts 1 on the
     // constrained diagonal entries of a partially constrained node once per
@@ -347,6 +355,84 @@ int crimson_set_boundary(crimson_ctx* c, int nface, const int* ienb, const int* 
     return CRIMSON_OK;
 }
 
+}  // extern "C"
+
+// NASC (AsBNASC, asbnabi.f90:191-340): per node the integral of its shape
+// function over the boundary faces that carry the natural-pressure bit
+// (iBCB bit 1), with the 3-point triangle rule; faces in ascending order,
+// the points of a face summed first.  The surface integrals of integrScalar
+// (boundarydata.f90:1101-1140) weight nodal values with it.
+static std::vector<double> node_surface_areas(const crimson_ctx* c) {
+    const int n = c->nshg;
+    std::vector<double> nasc((size_t)n, 0.0);
+    if (c->h_ienb.empty() || c->h_x.size() < 3 * (size_t)c->numnp) return nasc;
+    const double B3 = 0.666666666666667, C3 = 0.166666666666667, A3 = 0.3333333333333330000000000000000000;
+    const double r3[3][3] = {{B3, C3, C3}, {C3, B3, C3}, {C3, C3, B3}};
+    const size_t np = (size_t)c->numnp;
+    auto X = [&](int node, int d) { return c->h_x[(size_t)d * np + node]; };
+    for (size_t f = 0; f < c->h_ienb.size(); ++f) {
+        if (!((c->h_iBCB[f] >> 1) & 1)) continue;
+        const int4 e = c->h_ienb[f];
+        const int nd[3] = {e.x, e.y, e.z};
+        double v1[3], v2[3];
+        for (int d = 0; d < 3; ++d) {
+            v1[d] = X(nd[1], d) - X(nd[0], d);
+            v2[d] = X(nd[2], d) - X(nd[0], d);
+        }
+        const double t1 = v1[1] * v2[2] - v2[1] * v1[2];
+        const double t2 = v2[0] * v1[2] - v1[0] * v2[2];
+        const double t3 = v1[0] * v2[1] - v2[0] * v1[1];
+        const double temp = 1.0 / std::sqrt(t1 * t1 + t2 * t2 + t3 * t3);
+        double rl[3] = {0.0, 0.0, 0.0};
+        for (int q = 0; q < 3; ++q) {
+            const double wdetjb = (2.0 * A3) / (4.0 * temp);
+            for (int a = 0; a < 3; ++a) rl[a] = rl[a] + r3[q][a] * wdetjb;
+        }
+        for (int a = 0; a < 3; ++a) nasc[nd[a]] = nasc[nd[a]] + rl[a];
+    }
+    return nasc;
+}
+
+// Puts the effective codes on the device: iBC, its host copy and the count
+// of partially constrained nodes.
+static int upload_codes(crimson_ctx* c, const std::vector<int>& codes) {
+    int np = 0;
+    for (int v : codes) {
+        const int m = (v >> 3) & 7;
+        if (m != 0 && m != 7) ++np;
+    }
+    CR_CHECK(c->iBC.upload(codes.data(), codes.size(), c->stream));
+    CR_CUDA(cudaStreamSynchronize(c->stream));
+    c->h_iBC = codes;
+    c->npartial = np;
+    return CRIMSON_OK;
+}
+
+// memLS face 1 from the codes (itrdrv.f90:949-992): every node with a
+// prescribed velocity component, val 1 on its free components.
+static int rebuild_dirichlet_face(crimson_lhs* L, const std::vector<int>& codes) {
+    std::vector<int> g;
+    std::vector<double> v;
+    for (size_t i = 0; i < codes.size(); ++i) {
+        if (((codes[i] >> 3) & 7) == 0) continue;
+        g.push_back((int)i + 1);
+        for (int d = 0; d < 3; ++d) v.push_back(((codes[i] >> (3 + d)) & 1) ? 0.0 : 1.0);
+    }
+    return crimson_memls_bc_create(L, 1, (int)g.size(), 3, 0, g.data(), v.data());
+}
+
+// Surface integral of the pressure weighted by NASC (integrScalar of y(:,4)).
+__global__ void k_surfp_step(const int* __restrict__ onodes, int beg, int end, const double4* __restrict__ onabi,
+                             const double4* __restrict__ y, double* __restrict__ out) {
+    __shared__ double sm[32];
+    double s = 0.0;
+    for (int t = beg + threadIdx.x; t < end; t += blockDim.x) s += onabi[t].w * y[onodes[t]].w;
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) *out = s;
+}
+
+extern "C" {
+
 int crimson_set_outlets(crimson_ctx* c, int ncoupled, const int* srflist, const int* ndsurf, const double* NABI) {
     if (!c || ncoupled < 0 || (ncoupled > 0 && (!srflist || !ndsurf || !NABI))) return CRIMSON_ERR_ARG;
     if (ncoupled > 8) return CRIMSON_ERR_UNSUPPORTED;
@@ -356,15 +442,19 @@ int crimson_set_outlets(crimson_ctx* c, int ncoupled, const int* srflist, const 
     std::vector<double4> nab;
     c->onode_off.assign(1, 0);
     const int n = c->nshg;
+    const std::vector<double> nasc = node_surface_areas(c);
+    c->oarea.assign((size_t)ncoupled, 0.0);
     for (int k = 0; k < ncoupled; ++k) {
         for (int i = 0; i < n; ++i)
             if (ndsurf[i] == srflist[k]) {
                 nodes.push_back(i);
-                nab.push_back(make_double4(NABI[i], NABI[(size_t)n + i], NABI[2 * (size_t)n + i], 0.0));
+                nab.push_back(make_double4(NABI[i], NABI[(size_t)n + i], NABI[2 * (size_t)n + i], nasc[i]));
+                c->oarea[k] += nasc[i];
             }
         c->onode_off.push_back((int)nodes.size());
     }
     CR_CHECK(c->onodes.upload(nodes.data(), nodes.size(), c->stream));
+    c->h_onodes = nodes;
     CR_CHECK(c->onabi.upload(nab.data(), nab.size(), c->stream));
     CR_CHECK(c->d_onode_off.upload(c->onode_off.data(), c->onode_off.size(), c->stream));
     CR_CHECK(c->flowq.alloc((size_t)ncoupled));
@@ -841,11 +931,36 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
             set_last_error("crimson_step: coupled surface without an RCR (crimson_set_rcr) or a netlist");
             return CRIMSON_ERR_STATE;
         }
+    // Netlists whose closed diodes block the interface (Dirichlet design):
+    // the surface keeps its original Dirichlet codes and is not coupled.
+    std::vector<char> blocked((size_t)nc, 0);
+    for (int k = 0; k < nc; ++k)
+        if (crimson_netlist* nl = c->netlists[(size_t)k]) {
+            CR_CHECK(netlist_begin_step(nl));  // initialiseAtStartOfTimestep
+            blocked[(size_t)k] = nl->flow_permitted ? 0 : 1;
+        }
+    {
+        // iBC = iBC_original with zeros at the nodes of every coupled surface
+        // that takes flow (the binary mask of itrdrv.f90:1114-1133,
+        // BoundaryConditionManager.cxx:797-811); memLS face 1 follows the
+        // codes (rebuildMemLS_lhs, itrdrv.f90:887-1023)
+        std::vector<int> codes(c->h_iBC_orig);
+        for (int k = 0; k < nc; ++k)
+            if (!blocked[(size_t)k])
+                for (int t = c->onode_off[k]; t < c->onode_off[k + 1]; ++t) codes[(size_t)c->h_onodes[t]] = 0;
+        if (codes != c->h_iBC) {
+            CR_CHECK(upload_codes(c, codes));
+            CR_CHECK(rebuild_dirichlet_face(L, codes));
+        }
+    }
     for (int k = 0; k < nc; ++k) {
         if (crimson_netlist* nl = c->netlists[(size_t)k]) {
-            // initialiseAtStartOfTimestep, then the implicit coefficients with
-            // alfi*Delt (AbstractBoundaryCondition.cxx:32-53)
-            CR_CHECK(netlist_begin_step(nl));
+            // the implicit coefficients with alfi*Delt
+            // (AbstractBoundaryCondition.cxx:32-53); none in the Dirichlet design
+            if (blocked[(size_t)k]) {
+                c1[k] = c2[k] = 0.0;
+                continue;
+            }
             CR_CHECK(crimson_netlist_implicit_coefficients(nl, P.alfi * P.Delt, &c1[k], &c2[k]));
         } else {
             rcr_coeffs(c->rcr_Rp[k], c->rcr_C[k], c->rcr_Rd[k], c->rcr_Pd[k], c->rcr_Pd[k], c->rcr_Pn[k],
@@ -891,14 +1006,31 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
         for (int k = 0; k < nc; ++k)
             launch(k_flowq_step, 1, 256, 0, s, c->onodes.p, c->onode_off[k], c->onode_off[k + 1], c->onabi.p,
                                            reinterpret_cast<const double4*>(c->ycur.p), c->flowq.p + k);
-        std::vector<double> hq(nc);
+        // surface pressures of the blocked netlist surfaces (updmultidomaincontainer,
+        // elmgmr.f90:1733-1743: integrScalar of p / area, at t_{n+1})
+        CR_CHECK(c->psurf.alloc((size_t)nc));
+        for (int k = 0; k < nc; ++k)
+            if (blocked[(size_t)k])
+                launch(k_surfp_step, 1, 256, 0, s, c->onodes.p, c->onode_off[k], c->onode_off[k + 1], c->onabi.p,
+                                              reinterpret_cast<const double4*>(c->ycur.p), c->psurf.p + k);
+        std::vector<double> hq(nc), hp(nc, 0.0);
         CR_CUDA(cudaMemcpyAsync(hq.data(), c->flowq.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaMemcpyAsync(hp.data(), c->psurf.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
         for (int k = 0; k < nc; ++k) {
             if (crimson_netlist* nl = c->netlists[(size_t)k]) {
-                // updateLPN with the end-of-step flow, then finalizeLPNAtEndOfTimestep
-                // (itrdrv.f90:1686-1688)
-                CR_CHECK(crimson_netlist_update(nl, P.Delt, hq[k]));
+                // updateLPN with the end-of-step flow (or, blocked, the surface
+                // pressure), then finalizeLPNAtEndOfTimestep (itrdrv.f90:1686-1688)
+                if (blocked[(size_t)k]) {
+                    if (!(c->oarea[(size_t)k] > 0.0)) {
+                        set_last_error("crimson_step: a blocked netlist surface has no area (set the boundary faces "
+                                       "before crimson_set_outlets)");
+                        return CRIMSON_ERR_STATE;
+                    }
+                    CR_CHECK(crimson_netlist_update_pressure(nl, P.Delt, hp[k] / c->oarea[(size_t)k]));
+                } else {
+                    CR_CHECK(crimson_netlist_update(nl, P.Delt, hq[k]));
+                }
                 CR_CHECK(crimson_netlist_finalize_step(nl));
                 c->rcr_Pn[k] = nl->node[(size_t)nl->iface_node - 1].p;
                 c->rcr_Qn[k] = hq[k];

@@ -147,9 +147,12 @@ struct crimson_ctx {
     // Dirichlet data
     crimson::DBuf<int> iBC;         // (nshg)
     crimson::DBuf<double> BC;       // (ndofBC, nshg) node-major
-    std::vector<int> h_iBC;
+    std::vector<int> h_iBC;         // the codes on the device (iBC above)
+    std::vector<int> h_iBC_orig;    // the codes crimson_set_bc received (iBC_original of itrdrv.f90)
     int npartial = 0;               // nodes with one or two prescribed velocity components
     std::vector<double> h_BC;       // reference layout (nshg, ndofBC)
+    std::vector<double> h_x;        // (numnp, 3) reference layout, host copy
+    std::vector<int4> h_ienb;       // (nface) host copy of ienb
 
     // boundary faces (AsBMFG)
     int nface = 0;
@@ -167,6 +170,9 @@ struct crimson_ctx {
     std::vector<int> srflist;
     crimson::DBuf<int> onodes;      // outlet node ids grouped by surface
     std::vector<int> onode_off;     // (ncoupled+1) offsets into onodes
+    std::vector<double> oarea;      // (ncoupled) surface area: sum of NASC over the surface's nodes
+    std::vector<int> h_onodes;      // host copy of onodes
+    crimson::DBuf<double> psurf;    // (ncoupled) surface pressure integrals
     crimson::DBuf<int> d_onode_off; // device copy of onode_off
     crimson::DBuf<double4> onabi;   // NABI of those nodes
     crimson::DBuf<double> flowq;    // (ncoupled) device scratch for Q

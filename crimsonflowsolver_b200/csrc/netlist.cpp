@@ -8,7 +8,11 @@
 // Each time step the circuit is one dense linear system in the reference's
 // unknown order [nodal pressures | history pressures | component flows |
 // history flows]; its inverse gives the implicit coefficients dp/dQ and H of
-// the interface pressure p = dp/dQ * Q + H.
+// the interface pressure p = dp/dQ * Q + H.  When closed diodes block every
+// path from the interface the circuit switches to the reference's Dirichlet
+// design (CircuitData.cxx:482-540): the interface node takes the 3D
+// surface pressure as a prescribed pressure and the interface component's
+// flow is no longer prescribed.
 #include "netlist.h"
 
 #include <algorithm>
@@ -40,6 +44,25 @@ inline int col_hist_v(const crimson_netlist* nl) { return col_vol(nl) + (int)nl-
 // Pressure of a node as the reference reads it: a fixed-pressure node
 // returns its prescribed value (CircuitPressureNode.cxx:55-66).
 inline double node_pressure(const NetlistNode& d) { return d.fixed ? d.fixed_p : d.p; }
+
+// Prescribed-pressure nodes and prescribed-flow components of the current
+// design, ascending: in the Dirichlet design the interface node joins the
+// pressures and the interface component leaves the flows.
+std::vector<int> design_pp(const crimson_netlist* nl) {
+    std::vector<int> pp(nl->pp_nodes);
+    if (!nl->flow_permitted) {
+        pp.push_back(nl->iface_node);
+        std::sort(pp.begin(), pp.end());
+    }
+    return pp;
+}
+
+std::vector<int> design_pf(const crimson_netlist* nl) {
+    std::vector<int> pf;
+    for (int j : nl->pf_comps)
+        if (nl->flow_permitted || j != nl->iface_comp) pf.push_back(j);
+    return pf;
+}
 
 // generateLinearSystemWithoutFactorisation (NetlistCircuit.cxx:1057-1302):
 // one row per component (two for a pressure chamber), one Kirchhoff row per
@@ -108,9 +131,9 @@ void build_system(crimson_netlist* nl, double alfi_delt) {
             if (nl->comp[j].start == nd) a(row, cf + j) = -1.0;
         }
     }
-    for (int nd : nl->pp_nodes) a(row++, nd - 1) = 1.0;
+    for (int nd : design_pp(nl)) a(row++, nd - 1) = 1.0;
     for (size_t l = 0; l < nl->hist_nodes.size(); ++l) a(row++, chp + (int)l) = 1.0;
-    for (int j : nl->pf_comps) a(row++, cf + j) = 1.0;
+    for (int j : design_pf(nl)) a(row++, cf + j) = 1.0;
     for (size_t l = 0; l < nl->hist_comps.size(); ++l) a(row++, chq + (int)l) = 1.0;
     for (size_t l = 0; l < nl->vol_comps.size(); ++l) a(row++, chv + (int)l) = 1.0;
 }
@@ -134,9 +157,11 @@ int iface_row(const crimson_netlist* nl) {
 void assemble_rhs(crimson_netlist* nl) {
     std::fill(nl->b.begin(), nl->b.end(), 0.0);
     int row = first_prescribed_row(nl);
-    for (int nd : nl->pp_nodes) nl->b[row++] = nl->node[nd - 1].fixed_p;
+    // a fixed pressure, or the 3D surface pressure at the interface node
+    // (Pressure_3DInterface, NetlistCircuit.cxx:1386-1410)
+    for (int nd : design_pp(nl)) nl->b[row++] = nl->node[nd - 1].fixed ? nl->node[nd - 1].fixed_p : nl->last_p3d;
     for (int nd : nl->hist_nodes) nl->b[row++] = nl->node[nd - 1].hist;
-    for (int j : nl->pf_comps) {
+    for (int j : design_pf(nl)) {
         const NetlistComp& c = nl->comp[j];
         nl->b[row++] = c.flow_kind == CRIMSON_NETLIST_FLOW_3D ? nl->last_q * nl->sign : c.flow_fixed;
     }
@@ -223,9 +248,6 @@ namespace crimson {
 
 int netlist_begin_step(crimson_netlist* nl) {
     nl->flow_permitted = detect_flow_permitted(nl);
-    if (!nl->flow_permitted)
-        return fail("netlist: closed diodes block every path from the 3D interface (Dirichlet mode is not supported)",
-                    CRIMSON_ERR_UNSUPPORTED);
     return CRIMSON_OK;
 }
 
@@ -394,8 +416,8 @@ int crimson_netlist_flow_permitted(crimson_netlist* nl, int* permitted) {
 int crimson_netlist_implicit_coefficients(crimson_netlist* nl, double alfi_delt, double* dp_dq, double* hop) {
     if (!nl || !dp_dq || !hop || !(alfi_delt > 0.0)) return CRIMSON_ERR_ARG;
     if (!nl->flow_permitted)
-        return fail("netlist: no flow across the 3D interface (Dirichlet mode is not supported)",
-                    CRIMSON_ERR_UNSUPPORTED);
+        return fail("netlist: no flow across the 3D interface (Dirichlet design: no implicit coefficients)",
+                    CRIMSON_ERR_STATE);
     build_system(nl, alfi_delt);
     assemble_rhs(nl);
     const int st = solve(nl);
@@ -408,10 +430,9 @@ int crimson_netlist_implicit_coefficients(crimson_netlist* nl, double alfi_delt,
 }
 
 // updateLPN (NetlistCircuit.cxx:1582-1594): solve with the step's
-// interface flow and take the nodal pressures and component flows.
-int crimson_netlist_update(crimson_netlist* nl, double delt, double interface_flow) {
-    if (!nl || !(delt > 0.0) || !std::isfinite(interface_flow)) return CRIMSON_ERR_ARG;
-    nl->last_q = interface_flow;
+// interface flow (Neumann design) or the 3D surface pressure (Dirichlet
+// design) and take the nodal pressures, component flows and volumes.
+static int netlist_solve_update(crimson_netlist* nl, double delt) {
     build_system(nl, delt);
     assemble_rhs(nl);
     const int st = solve(nl);
@@ -431,6 +452,24 @@ int crimson_netlist_update(crimson_netlist* nl, double delt, double interface_fl
     return CRIMSON_OK;
 }
 
+int crimson_netlist_update(crimson_netlist* nl, double delt, double interface_flow) {
+    if (!nl || !(delt > 0.0) || !std::isfinite(interface_flow)) return CRIMSON_ERR_ARG;
+    if (!nl->flow_permitted)
+        return fail("netlist: the circuit is in the Dirichlet design; update it with the 3D surface pressure",
+                    CRIMSON_ERR_STATE);
+    nl->last_q = interface_flow;
+    return netlist_solve_update(nl, delt);
+}
+
+int crimson_netlist_update_pressure(crimson_netlist* nl, double delt, double interface_pressure) {
+    if (!nl || !(delt > 0.0) || !std::isfinite(interface_pressure)) return CRIMSON_ERR_ARG;
+    if (nl->flow_permitted)
+        return fail("netlist: the circuit is in the Neumann design; update it with the 3D interface flow",
+                    CRIMSON_ERR_STATE);
+    nl->last_p3d = interface_pressure;
+    return netlist_solve_update(nl, delt);
+}
+
 // finalizeLPNAtEndOfTimestep (NetlistCircuit.cxx:732-737): the current
 // pressures and flows become the histories, then the diodes switch
 // (CircuitData.cxx:357-377; rule CircuitComponent.cxx:4-17).
@@ -447,6 +486,9 @@ int crimson_netlist_finalize_step(crimson_netlist* nl) {
         const bool forward = c.flow >= tol;
         c.open = gradient || forward;
     }
+    // detectWhetherClosedDiodesStopAllFlowAt3DInterface for the next step
+    // (initialiseAtStartOfTimestep, NetlistCircuit.cxx:723-728)
+    nl->flow_permitted = detect_flow_permitted(nl);
     return CRIMSON_OK;
 }
 
@@ -461,12 +503,12 @@ int crimson_netlist_get(const crimson_netlist* nl, double* pressures, double* fl
 
 int crimson_netlist_state_size(const crimson_netlist* nl, int* n) {
     if (!nl || !n) return CRIMSON_ERR_ARG;
-    *n = 2 * nl->np + 5 * nl->nc + 1;
+    *n = 2 * nl->np + 5 * nl->nc + 2;
     return CRIMSON_OK;
 }
 
 // Checkpoint layout: [p (np), hist (np), flow (nc), hist_flow (nc), open (nc),
-// volume (nc), hist_volume (nc), last_q]
+// volume (nc), hist_volume (nc), last_q, last_p3d]
 int crimson_netlist_state(crimson_netlist* nl, double* buf, int set) {
     if (!nl || !buf) return CRIMSON_ERR_ARG;
     const int np = nl->np, nc = nl->nc;
@@ -483,6 +525,7 @@ int crimson_netlist_state(crimson_netlist* nl, double* buf, int set) {
             nl->comp[j].hist_volume = buf[2 * np + 4 * nc + j];
         }
         nl->last_q = buf[2 * np + 5 * nc];
+        nl->last_p3d = buf[2 * np + 5 * nc + 1];
         nl->flow_permitted = detect_flow_permitted(nl);
     } else {
         for (int i = 0; i < np; ++i) {
@@ -497,6 +540,7 @@ int crimson_netlist_state(crimson_netlist* nl, double* buf, int set) {
             buf[2 * np + 4 * nc + j] = nl->comp[j].hist_volume;
         }
         buf[2 * np + 5 * nc] = nl->last_q;
+        buf[2 * np + 5 * nc + 1] = nl->last_p3d;
     }
     return CRIMSON_OK;
 }

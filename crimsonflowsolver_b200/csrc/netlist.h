@@ -56,13 +56,14 @@ struct crimson_netlist {
     std::vector<std::vector<int>> nb_start, nb_end;  // neighbouring components at each end
     int n = 0;                                       // system size
     std::vector<double> A, Ainv, b, x;
-    double last_q = 0.0;  // interface flow of the last update (the flow the reference reads from the 3D side)
-    bool flow_permitted = true;
+    double last_q = 0.0;    // interface flow of the last update (the flow the reference reads from the 3D side)
+    double last_p3d = 0.0;  // 3D surface pressure of the last Dirichlet-design update
+    bool flow_permitted = true;  // false: closed diodes block the interface (Dirichlet design)
 };
 
 namespace crimson {
-// initialiseAtStartOfTimestep: CRIMSON_ERR_UNSUPPORTED when closed diodes
-// block every path from the 3D interface (the reference then turns the
-// surface into a Dirichlet boundary).
+// initialiseAtStartOfTimestep: whether closed diodes block every path from
+// the 3D interface (then the circuit takes the Dirichlet design and the
+// surface becomes a Dirichlet boundary of the flow problem).
 int netlist_begin_step(crimson_netlist* nl);
 }  // namespace crimson

@@ -3,8 +3,9 @@
 :class:`Netlist` owns one circuit handle built from a :class:`NetlistBC`
 description; the calls mirror NetlistCircuit (flowsolver/src/
 NetlistCircuit.cxx): implicit coefficients at the start of a step, update
-with the end-of-step interface flow, finalisation (histories and diode
-switching).
+with the end-of-step interface flow -- or, while closed diodes block the
+interface (the Dirichlet design), with the 3D surface pressure --
+finalisation (histories and diode switching).
 """
 from __future__ import annotations
 
@@ -55,7 +56,13 @@ class Netlist:
         return a.value, b.value
 
     def update(self, delt: float, q: float) -> None:
+        """updateLPN with the end-of-step interface flow (Neumann design)."""
         N.check(N.lib().crimson_netlist_update(self.h, delt, q), "crimson_netlist_update")
+
+    def update_pressure(self, delt: float, p: float) -> None:
+        """updateLPN with the 3D surface's mean pressure (Dirichlet design:
+        closed diodes block the interface)."""
+        N.check(N.lib().crimson_netlist_update_pressure(self.h, delt, p), "crimson_netlist_update_pressure")
 
     def finalize_step(self) -> None:
         N.check(N.lib().crimson_netlist_finalize_step(self.h), "crimson_netlist_finalize_step")

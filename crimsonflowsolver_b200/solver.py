@@ -291,6 +291,15 @@ def neumann_face(mesh, srfid: int):
     return nodes, mesh.NABI[nodes]
 
 
+def _with_codes(mesh, iBC):
+    """A view of mesh with other nodal codes."""
+    import copy
+
+    m = copy.copy(mesh)
+    m.iBC = iBC
+    return m
+
+
 class FlowSolver:
     """Device-resident time stepping (itrdrv_iter_step) with RCR and netlist outlets."""
 
@@ -301,9 +310,18 @@ class FlowSolver:
         self.elm._nnz()
         nc = len(self.elm.srflist)
         self.memls = MemLS(P, 1 + nc, ctx=self.elm)
-        nodes, sv = dirichlet_face(mesh)
-        self.memls.bc_create(1, nodes, 3, 0, sv)
         outlets = P.outlets()
+        # a netlist surface starts from zero-velocity Dirichlet codes, which
+        # crimson_step releases while the circuit takes flow and keeps while
+        # its closed diodes block the interface (itrdrv.f90:1114-1133)
+        iBC0 = np.asarray(mesh.iBC, dtype=np.int32).copy()
+        for r in outlets:
+            if hasattr(r, "components"):
+                iBC0[mesh.ndsurf == r.srfid] |= 7 << 3
+        if not np.array_equal(iBC0, mesh.iBC):
+            self.elm.set_bc(iBC0, mesh.BC)
+        nodes, sv = dirichlet_face(_with_codes(mesh, iBC0))
+        self.memls.bc_create(1, nodes, 3, 0, sv)
         for k, r in enumerate(outlets):
             nn, vv = neumann_face(mesh, r.srfid)
             self.memls.bc_create(2 + k, nn, 3, 1, vv)

@@ -332,11 +332,13 @@ int crimson_elmgmr_sclr_device(crimson_ctx* ctx, int isclr, double diffus, const
  * coefficients from the system's first unknown, node 1's pressure) and
  * belongs to exactly one component.  Diodes start closed and switch at the
  * end of each step (open while the pressure drop is >= -1e-8 or the flow
- * >= 1e-8).  A circuit whose closed diodes block every path from the
- * interface (the reference then switches the surface to a Dirichlet
- * condition) returns CRIMSON_ERR_UNSUPPORTED.  Left-ventricular pressure
- * prescriptions, time-varying prescriptions and Python controllers are not
- * supported.
+ * >= 1e-8).  While closed diodes block every path from the interface the
+ * circuit is in the reference's Dirichlet design (CircuitData.cxx:482-540):
+ * the interface node takes the 3D surface pressure as a prescribed pressure
+ * and the interface component's flow is solved for; the flow solver then
+ * holds the surface at its Dirichlet codes (itrdrv.f90:1114-1133).
+ * Left-ventricular pressure prescriptions, time-varying prescriptions and
+ * Python controllers are not supported.
  * --------------------------------------------------------------------------- */
 typedef struct crimson_netlist crimson_netlist;
 #define CRIMSON_NETLIST_RESISTOR 0
@@ -359,14 +361,23 @@ int crimson_netlist_create(crimson_netlist** nl, int ncomp, const int* kind, con
                            const int* pres_node, const double* pres_value, int nflow, const int* flow_comp,
                            const int* flow_kind, const double* flow_value, int interface_node);
 void crimson_netlist_free(crimson_netlist* nl);
-/* detectWhetherClosedDiodesStopAllFlowAt3DInterface (CircuitData.cxx:388-470) */
+/* detectWhetherClosedDiodesStopAllFlowAt3DInterface (CircuitData.cxx:388-470):
+ * 1 in the Neumann design, 0 in the Dirichlet design. */
 int crimson_netlist_flow_permitted(crimson_netlist* nl, int* permitted);
 /* computeImplicitCoefficients (NetlistCircuit.cxx:1764-1800) with the
- * step's alfi*Delt: the interface pressure p = dp_dq * Q + hop. */
+ * step's alfi*Delt: the interface pressure p = dp_dq * Q + hop.
+ * CRIMSON_ERR_STATE in the Dirichlet design (the reference sets them to NaN
+ * there, AbstractBoundaryCondition.cxx:32-53). */
 int crimson_netlist_implicit_coefficients(crimson_netlist* nl, double alfi_delt, double* dp_dq, double* hop);
 /* updateLPN (NetlistCircuit.cxx:1582-1594): solve with Delt and the
- * interface flow at the end of the step. */
+ * interface flow at the end of the step (Neumann design; CRIMSON_ERR_STATE
+ * in the Dirichlet design). */
 int crimson_netlist_update(crimson_netlist* nl, double delt, double interface_flow);
+/* updateLPN in the Dirichlet design: the interface node's prescribed
+ * pressure is the 3D surface's mean pressure at the end of the step
+ * (integrScalar of p over the surface / its area, elmgmr.f90:1733-1743);
+ * CRIMSON_ERR_STATE in the Neumann design. */
+int crimson_netlist_update_pressure(crimson_netlist* nl, double delt, double interface_pressure);
 /* finalizeLPNAtEndOfTimestep (NetlistCircuit.cxx:732-737): histories and
  * diode states for the next step. */
 int crimson_netlist_finalize_step(crimson_netlist* nl);
@@ -381,8 +392,13 @@ int crimson_netlist_state(crimson_netlist* nl, double* buf, int set);
 /* Couple surface k (0-based, srflist order) through nl instead of its RCR
  * in crimson_step: the coefficients come from nl at the start of each step,
  * and nl is updated and finalised with the surface's flow at its end; the
- * step's p_out is the interface node's pressure.  nl == NULL restores the
- * RCR.  The context does not own nl: free the context first. */
+ * step's p_out is the interface node's pressure.  While nl's closed valves
+ * block the interface, the surface keeps the codes crimson_set_bc gave it
+ * (the reference's iBC_original; the coupled surfaces that take flow get
+ * zeros, itrdrv.f90:1114-1133), memLS face 1 of the step's lhs is rebuilt
+ * from the codes when they change, the surface is not coupled, and nl is
+ * updated with the surface's NASC-weighted mean pressure.  nl == NULL
+ * restores the RCR.  The context does not own nl: free the context first. */
 int crimson_set_outlet_netlist(crimson_ctx* ctx, int k, crimson_netlist* nl);
 
 /* yold/acold in the reference layout (nshg, 4) */

@@ -23,7 +23,13 @@ flowsolver/src/NetlistCircuit.cxx, CircuitData.cxx and CircuitComponent.cxx:
 * volume-tracking components (V - V_hist - alfi_delt q = 0) and pressure
   chambers (the same plus p_start / E - V = -V_unstressed, the start node
   then taking E (V - V_unstressed), CircuitComponent.cxx:188-209), with the
-  tracked and history volumes after the history flows (1147-1241, 1282-1287).
+  tracked and history volumes after the history flows (1147-1241, 1282-1287);
+* the search for a path from the interface through flow-permitting
+  components to a free end (CircuitData.cxx:388-470), and the Dirichlet
+  design while none exists (CircuitData.cxx:482-540): the interface node
+  joins the prescribed pressures with the 3D surface pressure
+  (NetlistCircuit.cxx:1386-1410), the interface component leaves the
+  prescribed flows.
 
 numpy's LAPACK inverse stands in for PETSc's dense MatMatSolve.
 """
@@ -63,10 +69,36 @@ class OracleNetlist:
         self.pp = sorted(self.fixed)
         self.pf = sorted(set(self.fixed_flow) | {self.iface})
         self.open = [c[0] != "d" for c in self.comps]  # diodes start closed
+        self.p3d = 0.0
+        self.permitted = self.flow_permitted()
         self.hist_p = {i: self.pressure(i) for i in self.hist_nodes}
         self.hist_q = {j: self.q[j] for j in self.hist_comps}
         self.last_q = 0.0
         self.n = self.np_ + len(self.hist_nodes) + self.nc + len(self.hist_comps) + 2 * len(self.vol_comps)
+
+    def flow_permitted(self):
+        """Whether some flow-permitting path leads from the interface
+        component to a component end no other component touches (other
+        than the interface node)."""
+        touching = {}
+        for j, (_, s, e, _) in enumerate(self.comps):
+            touching.setdefault(s, set()).add(j)
+            touching.setdefault(e, set()).add(j)
+        todo, seen = [self.iface - 1], set()
+        while todo:
+            j = todo.pop()
+            if j in seen:
+                continue
+            seen.add(j)
+            if not self.open[j]:
+                continue
+            _, s, e, _ = self.comps[j]
+            ends = [(s, touching[s] - {j}), (e, touching[e] - {j})]
+            if any(not others and node != 1 for node, others in ends):
+                return True
+            for _, others in ends:
+                todo.extend(others)
+        return False
 
     def pressure(self, node):
         return self.fixed.get(node, self.p[node - 1])
@@ -116,9 +148,10 @@ class OracleNetlist:
                 if s == node:
                     A[r, fq + j] = -1.0
             r += 1
-        for node in self.pp:
+        dirichlet = not self.permitted
+        for node in sorted(set(self.pp) | ({1} if dirichlet else set())):
             A[r, node - 1] = 1.0
-            b[r] = self.fixed[node]
+            b[r] = self.fixed[node] if node in self.fixed else self.p3d
             r += 1
         for node in self.hist_nodes:
             A[r, hp_col[node]] = 1.0
@@ -126,6 +159,8 @@ class OracleNetlist:
             r += 1
         iface_row = None
         for comp in self.pf:
+            if dirichlet and comp == self.iface:
+                continue
             A[r, fq + comp - 1] = 1.0
             if comp == self.iface:
                 b[r] = self.last_q * self.sign
@@ -145,13 +180,23 @@ class OracleNetlist:
         return A, b, iface_row
 
     def implicit_coefficients(self, alfi_delt):
+        assert self.permitted, "no implicit coefficients in the Dirichlet design"
         A, b, col = self._system(alfi_delt)
         Ainv = np.linalg.inv(A)
         x = Ainv @ b
         return self.sign * Ainv[0, col], x[0] - Ainv[0, col] * b[col]
 
     def update(self, delt, q):
+        assert self.permitted
         self.last_q = q
+        self._update(delt)
+
+    def update_pressure(self, delt, p):
+        assert not self.permitted
+        self.p3d = p
+        self._update(delt)
+
+    def _update(self, delt):
         A, b, _ = self._system(delt)
         x = np.linalg.inv(A) @ b
         self.p = x[:self.np_].copy()
@@ -171,6 +216,7 @@ class OracleNetlist:
         for j, (k, s, e, _) in enumerate(self.comps):
             if k == "d":
                 self.open[j] = (self.pressure(s) - self.pressure(e) >= -1e-8) or (self.q[j] >= 1e-8)
+        self.permitted = self.flow_permitted()
 
     def interface_pressure(self):
         return self.pressure(1)

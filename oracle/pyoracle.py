@@ -300,23 +300,75 @@ def neumann_face(mesh, srfid):
     return nodes, mesh.NABI[nodes]
 
 
+def surface_areas(mesh):
+    """NASC (AsBNASC, asbnabi.f90:191-340): per node the integral of its
+    shape function over the faces with the natural-pressure bit, the 3-point
+    triangle rule, faces in order and each face's points summed first."""
+    B3, C3, A3 = 0.666666666666667, 0.166666666666667, 0.3333333333333330
+    r3 = ((B3, C3, C3), (C3, B3, C3), (C3, C3, B3))
+    x = mesh.x
+    nasc = np.zeros(mesh.nshg)
+    for f in range(mesh.ienb.shape[0]):
+        if not (int(mesh.iBCB[f, 0]) >> 1) & 1:
+            continue
+        nd = mesh.ienb[f, :3]
+        v1 = x[nd[1]] - x[nd[0]]
+        v2 = x[nd[2]] - x[nd[0]]
+        t1 = v1[1] * v2[2] - v2[1] * v1[2]
+        t2 = v2[0] * v1[2] - v1[0] * v2[2]
+        t3 = v1[0] * v2[1] - v2[0] * v1[1]
+        temp = 1.0 / np.sqrt(t1 * t1 + t2 * t2 + t3 * t3)
+        rl = [0.0, 0.0, 0.0]
+        for q in range(3):
+            w = (2.0 * A3) / (4.0 * temp)
+            for a in range(3):
+                rl[a] = rl[a] + r3[q][a] * w
+        for a in range(3):
+            nasc[nd[a]] = nasc[nd[a]] + rl[a]
+    return nasc
+
+
+def netlist_surface_codes(mesh, outlets):
+    """The codes a netlist surface starts from: zero-velocity Dirichlet codes
+    on its nodes (ndsurf), released while the circuit takes flow
+    (itrdrv.f90:1114-1133)."""
+    iBC = mesh.iBC.copy()
+    for r in outlets:
+        if hasattr(r, "components"):
+            nodes = np.nonzero(mesh.ndsurf == r.srfid)[0]
+            iBC[nodes] = iBC[nodes] | (7 << 3)
+    return iBC
+
+
 class OracleFlow:
-    """Time stepper over the oracle routines (itrdrv_iter_step + SolFlow)."""
+    """Time stepper over the oracle routines (itrdrv_iter_step + SolFlow).
+
+    Netlist outlets: the surface nodes start from zero-velocity Dirichlet
+    codes; each step the codes are iBC_original with zeros on every coupled
+    surface that takes flow, and memLS's face 1 follows them; a netlist
+    whose closed diodes block the interface is not coupled that step and is
+    updated with the surface's mean pressure (NASC-weighted) at its end."""
 
     def __init__(self, mesh, P, nthreads: int = 1, inflow=None):
-        self.m = mesh
+        import copy
+
         self.P = P
         self.nthreads = nthreads
-        self.colm, self.rowp = genadj(mesh.ien, mesh.nshg)
-        self.elm = Elm(mesh, P, self.colm, self.rowp, nthreads)
         # coupled outlets: RCRs, then netlist circuits (netlist_oracle.py)
         self.rcr = P.outlets() if hasattr(P, "outlets") else list(P.rcr)
         self.srflist = [r.srfid for r in self.rcr]
+        self.m = copy.copy(mesh)
+        self.iBC_orig = netlist_surface_codes(mesh, self.rcr)
+        self.m.iBC = self.iBC_orig.copy()
+        self.colm, self.rowp = genadj(mesh.ien, mesh.nshg)
+        self.elm = Elm(self.m, P, self.colm, self.rowp, nthreads)
         from oracle.netlist_oracle import OracleNetlist
 
         self.netlists = [OracleNetlist(r) if hasattr(r, "components") else None for r in self.rcr]
+        self.onodes = [np.nonzero(mesh.ndsurf == s)[0] for s in self.srflist]
+        self.nasc = surface_areas(mesh) if any(nl is not None for nl in self.netlists) else None
         self.memls = MemLS(mesh.nshg, self.colm, self.rowp, 1 + len(self.rcr), P, nthreads)
-        nodes, sv = dirichlet_face(mesh)
+        nodes, sv = dirichlet_face(self.m)
         self.memls.bc_create(1, nodes, 3, 0, sv)
         for k, r in enumerate(self.rcr):
             nn, vv = neumann_face(mesh, r.srfid)
@@ -338,11 +390,29 @@ class OracleFlow:
         """itrBC (itrbc.f90:33-101) in place on y (nshg, 4)."""
         itr_bc(self.m, y)
 
+    def _blocked(self, k):
+        return self.netlists[k] is not None and not self.netlists[k].permitted
+
+    def _set_codes(self):
+        """iBC = iBC_original, zero on the coupled surfaces that take flow;
+        face 1 rebuilt when the codes change (rebuildMemLS_lhs)."""
+        codes = self.iBC_orig.copy()
+        for k in range(len(self.rcr)):
+            if not self._blocked(k):
+                codes[self.onodes[k]] = 0
+        if not np.array_equal(codes, self.m.iBC):
+            self.m.iBC = codes
+            self.elm.iBC = np.ascontiguousarray(codes.astype(np.int32))
+            nodes, sv = dirichlet_face(self.m)
+            self.memls.bc_create(1, nodes, 3, 0, sv)
+
     def implicit_coeffs(self, n, alpha_form=True):
         P = self.P
         c1 = np.zeros(len(self.rcr))
         c2 = np.zeros(len(self.rcr))
         for k, r in enumerate(self.rcr):
+            if self._blocked(k):
+                continue
             if self.netlists[k] is not None:
                 c1[k], c2[k] = self.netlists[k].implicit_coefficients(P.alfi * P.Delt if alpha_form else P.Delt)
             elif alpha_form:
@@ -377,6 +447,7 @@ class OracleFlow:
         fct = (P.gami - 1.0) / P.gami
         self.y = self.yold.copy()
         self.ac = self.acold * fct
+        self._set_codes()
         self._itr_bc(self.y)
         c1, c2 = self.implicit_coeffs(n, True)
         for _ in range(P.nitr):
@@ -394,7 +465,12 @@ class OracleFlow:
             Pn = d1 * q1 + h1
             for k, nl in enumerate(self.netlists):
                 if nl is not None:
-                    nl.update(P.Delt, q1[k])
+                    if nl.permitted:
+                        nl.update(P.Delt, q1[k])
+                    else:
+                        # integrScalar(p) / area (elmgmr.f90:1733-1743)
+                        w = self.nasc[self.onodes[k]]
+                        nl.update_pressure(P.Delt, float(np.sum(w * self.y[self.onodes[k], 3]) / np.sum(w)))
                     nl.finalize_step()
                     Pn[k] = nl.interface_pressure()
             self.Pn = Pn

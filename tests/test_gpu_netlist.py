@@ -72,3 +72,42 @@ def test_netlist_time_steps_parity():
     assert relerr(p, [o.pressure(i + 1) for i in range(len(p))]) < 1e-10
     assert relerr(q, o.q) < 1e-10
     assert list(op) == list(o.open)
+
+
+def test_valve_switches_surface_between_dirichlet_and_neumann():
+    """A diode on the only path from a netlist outlet (the circuit of the
+    reference's simpleDiodeTest case, a second outlet with an RCR): the
+    valve starts closed, so the surface starts at its Dirichlet codes and
+    the circuit takes the 3D surface pressure; it opens, closes under
+    backflow and opens again within six steps.  Device vs oracle: the
+    design of every step, velocity and pressure within 1e-10, outlet
+    pressures and flows, identical iteration counts."""
+    m = mesh.cylinder(ncross=8, naxial=10, n_outlets=2)
+    spec = NetlistBC(srfid=m.outlets[1], components=[("r", 1, 2, 1.0), ("d", 2, 3, 0.1)],
+                     prescribed_pressures={3: 1250.0}, interface_component=1,
+                     initial_pressures={1: 1058.5, 2: 1058.5, 3: 1250.0})
+    P = FlowParams(rcr=[RCR(srfid=m.outlets[0])], netlists=[spec], nitr=2)
+    F = po.OracleFlow(mesh.cylinder(ncross=8, naxial=10, n_outlets=2), P, inflow=lambda t: 10.0)
+    G = solver.FlowSolver(mesh.cylinder(ncross=8, naxial=10, n_outlets=2), P, inflow=lambda t: 10.0)
+    modes = ""
+    try:
+        for _ in range(6):
+            modes += "N" if F.netlists[1].permitted else "D"
+            assert G.netlists[0].flow_permitted() == F.netlists[1].permitted
+            F.step()
+            st = G.step()
+            its = [(r, g, c) for r, g, c, _, _ in F.stats[-st.nsolves:]]
+            assert its == [(st.ri_itr[i], st.gm_itr[i], st.cg_itr[i]) for i in range(st.nsolves)]
+            for k in range(2):
+                assert abs(st.p_out[k] - F.Pn[k]) <= 1e-9 * abs(F.Pn[k]), (k, st.p_out[k], F.Pn[k])
+                assert abs(st.q_out[k] - F.Qn[k]) <= 1e-9 * max(1.0, abs(F.Qn[k])), (k, st.q_out[k], F.Qn[k])
+        y, _ = G.state()
+        p, q, op, _ = G.netlists[0].get()
+    finally:
+        G.close()
+    assert "DN" in modes and "ND" in modes, modes
+    assert relerr(y[:, 0:3], F.y[:, 0:3]) < 1e-10, relerr(y[:, 0:3], F.y[:, 0:3])
+    assert relerr(y[:, 3], F.y[:, 3]) < 1e-10, relerr(y[:, 3], F.y[:, 3])
+    o = F.netlists[1]
+    assert relerr(p, [o.pressure(i + 1) for i in range(len(p))]) < 1e-10
+    assert list(op) == list(o.open)

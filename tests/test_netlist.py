@@ -156,15 +156,31 @@ def test_diode_opens_and_closes_like_oracle():
 
 
 def test_series_diode_blocks_interface():
-    """Closed diodes on every path from the interface: the reference switches
-    the surface to a Dirichlet condition, which is not supported here."""
+    """Closed diodes on every path from the interface: the circuit takes the
+    Dirichlet design (CircuitData.cxx:482-540).  No implicit coefficients
+    (CRIMSON_ERR_STATE); the update takes the 3D surface pressure, and the
+    diode opens under a positive pressure drop, returning the circuit to the
+    Neumann design -- library vs oracle throughout."""
     spec = NetlistBC(srfid=3, components=[("r", 1, 2, 100.0), ("d", 2, 3, 5.0), ("c", 3, 4, 1e-4)],
                      prescribed_pressures={4: 0.0}, interface_component=1)
-    g = Netlist(spec)
-    assert not g.flow_permitted()
+    g, o = Netlist(spec), OracleNetlist(spec)
+    assert not g.flow_permitted() and not o.permitted
     a, b = ctypes.c_double(), ctypes.c_double()
     rc = N.lib().crimson_netlist_implicit_coefficients(g.h, ALFI * DT, ctypes.byref(a), ctypes.byref(b))
-    assert rc == 2  # CRIMSON_ERR_UNSUPPORTED
+    assert rc == 8  # CRIMSON_ERR_STATE
+    with pytest.raises(RuntimeError):
+        g.update(DT, 1.0)
+    g.update_pressure(DT, 500.0)
+    o.update_pressure(DT, 500.0)
+    p, q, _, _ = g.get()
+    assert _close(p, [o.pressure(i + 1) for i in range(len(p))], 1e-12) and _close(q, o.q, 1e-12)
+    assert p[0] == 500.0 and q[0] == 0.0
+    g.finalize_step()
+    o.finalize_step()
+    assert g.flow_permitted() and o.permitted      # the diode opened
+    with pytest.raises(RuntimeError):
+        g.update_pressure(DT, 500.0)
+    assert _close(g.implicit_coefficients(ALFI * DT), o.implicit_coefficients(ALFI * DT), 1e-12)
     g.close()
 
 

@@ -47,6 +47,17 @@ def test_every_reference_input_parses():
     assert n >= 40
 
 
+def _q3d(step):
+    """Interface flow of the Neumann steps."""
+    return 50.0 + 40.0 * np.sin(2 * np.pi * step / 12)
+
+
+def _p3d(step):
+    """3D surface pressure of the Dirichlet steps: swings both ways, so the
+    heart circuits' valves open and close within twelve steps."""
+    return 20000.0 * np.sin(2 * np.pi * step / 12)
+
+
 def _circuits():
     out = []
     for name, text in sorted(_inputs().items()):
@@ -71,11 +82,13 @@ def _square(c):
 @pytest.mark.parametrize("name,k", _circuits())
 def test_reference_circuit_matches_oracle(name, k):
     """Each circuit of the reference's inputs (control scripts held at their
-    input values) over twelve steps of a pulsatile interface flow: implicit
-    coefficients, pressures, flows, volumes and diode states, library vs
-    oracle.  Circuits of closed-loop cases, whose boundary nodes belong to a
-    downstream circuit in another file, are not square on their own and are
-    rejected, as the reference rejects them without that circuit."""
+    input values) over twelve steps: implicit coefficients, pressures,
+    flows, volumes and diode states, library vs oracle, with a pulsatile
+    interface flow while flow can cross the interface (Neumann design) and
+    a pulsatile 3D surface pressure while closed valves block it (Dirichlet
+    design).  Circuits of closed-loop cases, whose boundary nodes belong to
+    a downstream circuit in another file, are not square on their own and
+    are rejected, as the reference rejects them without that circuit."""
     c = _parse(name, _inputs()[name])[k]
     spec = nio.to_netlistbc(c, 3, ignore_controls=True)
     if not _square(c):
@@ -86,16 +99,20 @@ def test_reference_circuit_matches_oracle(name, k):
     o = OracleNetlist(spec)
     try:
         for step in range(12):
-            if not g.flow_permitted():
-                # closed valves block the interface: the reference would
-                # switch the surface to a Dirichlet condition
-                return
-            a = g.implicit_coefficients(ALFI * DT)
-            b = o.implicit_coefficients(ALFI * DT)
-            assert _close(a, b, 1e-9), (step, a, b)
-            q = 50.0 + 40.0 * np.sin(2 * np.pi * step / 12)
-            g.update(DT, q)
-            o.update(DT, q)
+            assert g.flow_permitted() == o.permitted, step
+            if o.permitted:
+                a = g.implicit_coefficients(ALFI * DT)
+                b = o.implicit_coefficients(ALFI * DT)
+                assert _close(a, b, 1e-9), (step, a, b)
+                q = _q3d(step)
+                g.update(DT, q)
+                o.update(DT, q)
+            else:
+                with pytest.raises(RuntimeError):
+                    g.implicit_coefficients(ALFI * DT)
+                p3d = _p3d(step)
+                g.update_pressure(DT, p3d)
+                o.update_pressure(DT, p3d)
             p, f, _, vol = g.get()
             assert _close(p, [o.pressure(i + 1) for i in range(len(p))], 1e-9)
             assert _close(f, o.q, 1e-9)
@@ -105,6 +122,29 @@ def test_reference_circuit_matches_oracle(name, k):
             assert list(g.get()[2]) == list(o.open)
     finally:
         g.close()
+
+
+def test_designs_switch_both_ways():
+    """The Dirichlet steps above are not idle: 11 of the reference's square
+    circuits start with closed valves blocking the interface, and 9 of them
+    switch to the Neumann design and back within the twelve steps."""
+    starts_blocked = switches = 0
+    for name, text in sorted(_inputs().items()):
+        for c in _parse(name, text):
+            if not _square(c):
+                continue
+            o = OracleNetlist(nio.to_netlistbc(c, 3, ignore_controls=True))
+            modes = ""
+            for step in range(12):
+                modes += "N" if o.permitted else "D"
+                if o.permitted:
+                    o.update(DT, _q3d(step))
+                else:
+                    o.update_pressure(DT, _p3d(step))
+                o.finalize_step()
+            starts_blocked += modes[0] == "D"
+            switches += "DN" in modes and "ND" in modes
+    assert starts_blocked == 11 and switches == 9
 
 
 def test_emulate_rcr_input_is_the_rcr_model():
