@@ -920,9 +920,6 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
     if (c->ninlet > 0)
         launch(k_inflow, grid_for(c->ninlet, 256), 256, 0, s, c->inlet_nodes.p, c->inlet_profile.p, c->ninlet,
                                                           args->inflow_scale, nb, c->BC.p);
-    const double fct = (P.gami - 1.0) / P.gami;
-    launch(k_predict, grid_for(4LL * n, 256), 256, 0, s, c->yold.p, c->acold.p, c->ycur.p, c->accur.p, 4LL * n, fct);
-    launch(k_itrbc, grid_for(n, 256), 256, 0, s, c->iBC.p, c->BC.p, nb, n, c->ycur.p);
     const int nc = c->ncoupled;
     c->netlists.resize((size_t)nc, nullptr);
     std::vector<double> c1(nc), c2(nc), faceRes(1 + nc, 0.0);
@@ -953,6 +950,10 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
             CR_CHECK(rebuild_dirichlet_face(L, codes));
         }
     }
+    // itrPredict (ipred = 1) and itrBC with the step's codes
+    const double fct = (P.gami - 1.0) / P.gami;
+    launch(k_predict, grid_for(4LL * n, 256), 256, 0, s, c->yold.p, c->acold.p, c->ycur.p, c->accur.p, 4LL * n, fct);
+    launch(k_itrbc, grid_for(n, 256), 256, 0, s, c->iBC.p, c->BC.p, nb, n, c->ycur.p);
     for (int k = 0; k < nc; ++k) {
         if (crimson_netlist* nl = c->netlists[(size_t)k]) {
             // the implicit coefficients with alfi*Delt
