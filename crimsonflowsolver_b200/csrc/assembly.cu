@@ -351,15 +351,20 @@ __global__ void __launch_bounds__(128, 4) k_asigmr(const int4* __restrict__ ien,
 #pragma unroll
             for (int d = 0; d < 4; ++d)
                 g[k][d] = shg[0][k] * yl[0][d] + shg[1][k] * yl[1][d] + shg[2][k] * yl[2][d] + shg[3][k] * yl[3][d];
-        // div q (e3ivar.f90:354-368)
+        // div q (e3ivar.f90:354-368): lane a gathers node a's projected flux
+        // and the element's 4 lanes sum their terms (fixed butterfly)
         double divq[3] = {0.0, 0.0, 0.0};
-        if (P.idiff >= 1 && live) {
-#pragma unroll
-            for (int n = 0; n < 4; ++n) {
-                const double* q = qres + 9 * (size_t)nd[n];
+        if (P.idiff >= 1) {
+            if (live) {
+                const double* q = qres + 9 * (size_t)nd[lane4];
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
-                    divq[i] += shg[n][0] * q[i] + shg[n][1] * q[3 + i] + shg[n][2] * q[6 + i];
+                    divq[i] = shg[lane4][0] * q[i] + shg[lane4][1] * q[3 + i] + shg[lane4][2] * q[6 + i];
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                divq[i] += __shfl_xor_sync(0xffffffffu, divq[i], 1);
+                divq[i] += __shfl_xor_sync(0xffffffffu, divq[i], 2);
             }
         }
         // metric tensor, tet branch (e3stab.f90:487-528)
