@@ -125,6 +125,8 @@ SIGNATURES = {
     "crimson_netlist_implicit_coefficients": (ctypes.c_int, [c_void_p, ctypes.c_double, c_dbl_p, c_dbl_p]),
     "crimson_netlist_update": (ctypes.c_int, [c_void_p, ctypes.c_double, ctypes.c_double]),
     "crimson_netlist_update_pressure": (ctypes.c_int, [c_void_p, ctypes.c_double, ctypes.c_double]),
+    "crimson_netlist_get_parameter": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "crimson_netlist_set_parameter": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
     "crimson_netlist_finalize_step": (ctypes.c_int, [c_void_p]),
     "crimson_netlist_get": (ctypes.c_int, [c_void_p, c_dbl_p, c_dbl_p, c_int_p, c_dbl_p]),
     "crimson_netlist_state_size": (ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_int)]),

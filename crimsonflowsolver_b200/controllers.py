@@ -1,0 +1,76 @@
+"""Parameter control systems of netlist circuits.
+
+The reference lets Python scripts adjust circuit parameters between time
+steps (flowsolver/src/ControlSystemsManager.cxx:7-52, ParameterController.cxx:
+242-410, called once per step after the circuits' finalisation,
+itrdrv.f90:2100).  Each script defines a controller with
+``updateControl(currentParameterValue, delt, pressures, flows, volumes)``
+returning the parameter's new value; the dictionaries hold the circuit's
+nodal pressures, component flows and tracked volumes by 1-based index.
+Controllers run in ascending priority, and each may publish values for
+the ones after it (the broadcast dictionaries).
+
+:class:`ParameterController` is a base class with the method names those
+scripts use, so that a script ported to Python 3 runs with little change;
+:func:`run_controllers` is the per-step driver the time stepper calls.
+"""
+from __future__ import annotations
+
+from typing import Dict, Iterable, List, Tuple
+
+
+class ParameterController:
+    """Base class of a control system: override :meth:`updateControl`.
+
+    ``name`` is the key under which this controller's broadcast values reach
+    the others (the reference uses the script's base name);
+    ``controllerPriority`` orders the controllers (lower first)."""
+
+    controllerPriority = 0
+
+    def __init__(self, name: str):
+        self.name = name
+        self._broadcast: Dict[str, float] = {}
+        self._received: Dict[str, Dict[str, float]] = {}
+
+    def updateControl(self, currentParameterValue, delt, dictionaryOfPressuresByNodeIndex,
+                      dictionaryOfFlowsByComponentIndex, dictionaryOfVolumesByComponentIndex):
+        raise NotImplementedError
+
+    def getControllerPriority(self) -> int:
+        return self.controllerPriority
+
+    def addBroadcastVariable(self, key: str, value) -> None:
+        self._broadcast[key] = value
+
+    def clearBroadcastData(self) -> None:
+        self._broadcast = {}
+
+    def getRecievedBroadcastValue(self, controller_name: str, key: str):
+        """A value another controller published this step or before (the
+        spelling is the reference scripts')."""
+        return self._received[controller_name][key]
+
+    def broadcast_data(self) -> Dict[str, Dict[str, float]]:
+        return {self.name: dict(self._broadcast)}
+
+    def receive_broadcast(self, data: Dict[str, Dict[str, float]]) -> None:
+        self._received = {k: dict(v) for k, v in data.items()}
+
+
+def run_controllers(bound: Iterable[Tuple[object, str, int, ParameterController]], delt: float) -> None:
+    """One update of every control system (updateAndPassStateInformation-
+    BetweenPythonParameterControllers): ``bound`` holds (circuit, target,
+    index, controller) with ``circuit`` offering get_parameter /
+    set_parameter / observables.  Controllers run in ascending priority
+    (ties in the given order); each sees the broadcast values of the ones
+    before it, a value published earlier keeping precedence."""
+    items: List = sorted(bound, key=lambda b: b[3].getControllerPriority())
+    gathered: Dict[str, Dict[str, float]] = {}
+    for circuit, target, index, ctl in items:
+        ctl.receive_broadcast(gathered)
+        p, q, v = circuit.observables()
+        new = ctl.updateControl(circuit.get_parameter(target, index), delt, p, q, v)
+        circuit.set_parameter(target, index, float(new))
+        for k, val in ctl.broadcast_data().items():
+            gathered.setdefault(k, val)

@@ -492,6 +492,53 @@ int crimson_netlist_finalize_step(crimson_netlist* nl) {
     return CRIMSON_OK;
 }
 
+// The parameters a control system adjusts between steps
+// (ControlSystemsManager.cxx:125-330): a component's parameter value, a
+// pressure chamber's unstressed volume, a node's pressure (the prescribed
+// value of a fixed-pressure node) or a component's fixed prescribed flow.
+static double* netlist_parameter(crimson_netlist* nl, int what, int index) {
+    switch (what) {
+        case CRIMSON_NETLIST_PARAM_COMPONENT:
+            return index >= 1 && index <= nl->nc ? &nl->comp[(size_t)index - 1].value : nullptr;
+        case CRIMSON_NETLIST_PARAM_UNSTRESSED_VOLUME:
+            return index >= 1 && index <= nl->nc && nl->comp[(size_t)index - 1].kind == CRIMSON_NETLIST_PRESSURE_CHAMBER
+                       ? &nl->comp[(size_t)index - 1].unstressed
+                       : nullptr;
+        case CRIMSON_NETLIST_PARAM_PRESSURE: {
+            if (index < 1 || index > nl->np) return nullptr;
+            NetlistNode& d = nl->node[(size_t)index - 1];
+            return d.fixed ? &d.fixed_p : &d.p;
+        }
+        case CRIMSON_NETLIST_PARAM_FLOW:
+            return index >= 1 && index <= nl->nc && nl->comp[(size_t)index - 1].flow_kind == CRIMSON_NETLIST_FLOW_FIXED
+                       ? &nl->comp[(size_t)index - 1].flow_fixed
+                       : nullptr;
+        default:
+            return nullptr;
+    }
+}
+
+int crimson_netlist_get_parameter(crimson_netlist* nl, int what, int index, double* value) {
+    if (!nl || !value) return CRIMSON_ERR_ARG;
+    const double* v = netlist_parameter(nl, what, index);
+    if (!v) return fail("netlist: no such parameter (kind, index) in this circuit");
+    *value = *v;
+    return CRIMSON_OK;
+}
+
+int crimson_netlist_set_parameter(crimson_netlist* nl, int what, int index, double value) {
+    if (!nl || !std::isfinite(value)) return CRIMSON_ERR_ARG;
+    double* v = netlist_parameter(nl, what, index);
+    if (!v) return fail("netlist: no such parameter (kind, index) in this circuit");
+    if (what == CRIMSON_NETLIST_PARAM_COMPONENT && value == 0.0) {
+        const int k = nl->comp[(size_t)index - 1].kind;
+        if (k == CRIMSON_NETLIST_CAPACITOR || k == CRIMSON_NETLIST_PRESSURE_CHAMBER)
+            return fail("netlist: a capacitance or elastance cannot be 0");
+    }
+    *v = value;
+    return CRIMSON_OK;
+}
+
 int crimson_netlist_get(const crimson_netlist* nl, double* pressures, double* flows, int* open, double* volumes) {
     if (!nl) return CRIMSON_ERR_ARG;
     for (int i = 0; pressures && i < nl->np; ++i) pressures[i] = node_pressure(nl->node[i]);

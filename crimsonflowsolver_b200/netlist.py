@@ -17,6 +17,8 @@ from . import _native as N
 from .problem import NetlistBC
 
 KINDS = {"r": 0, "c": 1, "l": 2, "i": 2, "d": 3, "t": 4, "v": 5}
+# controllable parameters (crimson_netlist_set_parameter)
+TARGETS = {"component": 0, "unstressed_volume": 1, "pressure": 2, "flow": 3}
 
 
 class Netlist:
@@ -75,6 +77,26 @@ class Netlist:
         v = np.zeros(self.ncomp)
         N.check(N.lib().crimson_netlist_get(self.h, N.dp(p), N.dp(q), N.ip(o), N.dp(v)), "crimson_netlist_get")
         return p, q, o.astype(bool), v
+
+    def get_parameter(self, target: str, index: int) -> float:
+        """A controllable parameter: target "component" (R, C, L, a diode's
+        open resistance, a chamber's elastance), "unstressed_volume",
+        "pressure" (node) or "flow" (fixed prescribed flow); index 1-based."""
+        v = ctypes.c_double()
+        N.check(N.lib().crimson_netlist_get_parameter(self.h, TARGETS[target], int(index), ctypes.byref(v)),
+                "crimson_netlist_get_parameter")
+        return v.value
+
+    def set_parameter(self, target: str, index: int, value: float) -> None:
+        N.check(N.lib().crimson_netlist_set_parameter(self.h, TARGETS[target], int(index), float(value)),
+                "crimson_netlist_set_parameter")
+
+    def observables(self):
+        """(pressures by node, flows by component, volumes by volume-tracking
+        component), 1-based dictionaries as control scripts receive them."""
+        p, q, _, v = self.get()
+        vols = {j + 1: float(v[j]) for j, c in enumerate(self.spec.components) if c[0] in ("t", "v")}
+        return ({i + 1: float(x) for i, x in enumerate(p)}, {j + 1: float(x) for j, x in enumerate(q)}, vols)
 
     def state(self) -> np.ndarray:
         n = ctypes.c_int()

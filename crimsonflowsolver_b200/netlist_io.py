@@ -9,19 +9,22 @@ Two formats, as the reference reads them:
   volume on the same line); the prescribed pressures (count, nodes, values,
   types f/l), the prescribed flows (count, components, values, types f/t),
   the initial pressures (count, then "node pressure" lines), the 3D
-  interface node, and the component and node control lists.
+  interface node, and the component and node control lists ("index type
+  script" lines).
 * ``netlist_surfaces.xml`` (NetlistXmlReader, flowsolver/src/
   NetlistXmlReader.cxx:30-460): ``netlistCircuits/circuit`` elements with
   ``components/component`` (index, type, startNodeIndex, endNodeIndex,
   parameterValue, initialVolume, initialUnstressedVolume,
   prescribedFlowType, prescribedFlowValue) and ``nodes/node`` (index,
   initialPressure, isAt3DInterface, prescribedPressureType; a fixed
-  pressure takes the node's initialPressure).
+  pressure takes the node's initialPressure); ``control`` elements (type,
+  source) on components and nodes.
 
 Each circuit comes back as a dict; :func:`to_netlistbc` turns one into a
-:class:`NetlistBC` for a coupled surface, and raises for what the library
-does not model (left-ventricular pressures, control scripts, an interface
-node other than 1).
+:class:`NetlistBC` for a coupled surface, binding its customPython controls
+to the controllers the caller supplies, and raises for what the library
+does not model (left-ventricular pressures, built-in controllers, an
+interface node other than 1).
 """
 from __future__ import annotations
 
@@ -83,10 +86,12 @@ def parse_netlist_dat(text: str) -> List[Dict]:
         # older files end here: interface node 1, no controls
         t = next(lines, None)
         c["interface_node"] = int(t[0]) if t is not None else 1
-        for _ in range(2 if t is not None else 0):  # component controls, then node controls
+        c["control_specs"] = []
+        for item in (("component", "node") if t is not None else ()):  # component controls, then node controls
             k = int(next(lines)[0])
             for _ in range(k):
-                next(lines)
+                f = next(lines)
+                c["control_specs"].append((item, int(f[0]), f[1], f[2] if len(f) > 2 else ""))
             c["controls"] += k
         out.append(c)
     return out
@@ -103,7 +108,7 @@ def parse_netlist_xml(text: str) -> List[Dict]:
     for circ in root.findall("circuit"):
         c: Dict = {"components": [], "volumes": {}, "prescribed_pressures": {}, "pressure_types": {},
                    "prescribed_flows": {}, "flow_types": {}, "initial_pressures": {}, "controls": 0,
-                   "interface_node": None}
+                   "interface_node": None, "control_specs": []}
         for j, comp in enumerate(circ.find("components").findall("component")):
             kind = _text(comp, "type").lower()
             if kind not in _XML_KINDS:
@@ -121,7 +126,9 @@ def parse_netlist_xml(text: str) -> List[Dict]:
                 t = {"fixed": "f", "threedinterface": "t"}[ft.lower()]
                 c["prescribed_flows"][j + 1] = float(_text(comp, "prescribedFlowValue", "-1")) if t == "f" else -1.0
                 c["flow_types"][j + 1] = t
-            c["controls"] += len(comp.findall("control"))
+            for ctl in comp.findall("control"):
+                c["control_specs"].append(("component", j + 1, _text(ctl, "type", ""), _text(ctl, "source", "")))
+                c["controls"] += 1
         for node in circ.find("nodes").findall("node"):
             idx = int(_text(node, "index"))
             p0 = float(_text(node, "initialPressure"))
@@ -133,17 +140,38 @@ def parse_netlist_xml(text: str) -> List[Dict]:
                 t = {"fixed": "f", "leftventricular": "l"}[pt.lower()]
                 c["prescribed_pressures"][idx] = p0 if t == "f" else 1.0
                 c["pressure_types"][idx] = t
-            c["controls"] += len(node.findall("control"))
+            for ctl in node.findall("control"):
+                c["control_specs"].append(("node", idx, _text(ctl, "type", ""), _text(ctl, "source", "")))
+                c["controls"] += 1
         out.append(c)
     return out
 
 
-def to_netlistbc(circuit: Dict, srfid: int, ignore_controls: bool = False) -> NetlistBC:
-    """One parsed circuit as the outlet of surface ``srfid``.  Circuits with
-    control scripts raise, unless ``ignore_controls`` asks for the circuit
-    with its parameters held at their input values."""
+# control types of the inputs (fileReaders.cxx:680-760, NetlistXmlReader.cxx:60-130)
+# that act through a user controller, and the parameter each one drives
+_CONTROL_TARGETS = {("component", "custompython"): "component",
+                    ("component", "custompythonunstressedvolume"): "unstressed_volume",
+                    ("node", "custompython"): "pressure"}
+
+
+def to_netlistbc(circuit: Dict, srfid: int, ignore_controls: bool = False, controllers=None) -> NetlistBC:
+    """One parsed circuit as the outlet of surface ``srfid``.  A circuit's
+    customPython controls (component parameter, unstressed volume, node
+    pressure) take their controller from ``controllers``, a mapping from the
+    script name of the input to a
+    :class:`~crimsonflowsolver_b200.controllers.ParameterController`; with
+    ``ignore_controls`` the parameters stay at their input values.  Other
+    control types (the built-in left-ventricular elastance and bleed
+    controllers, periodic flow / pressure files) raise."""
+    bound = []
     if circuit["controls"] and not ignore_controls:
-        raise NotImplementedError("netlist control scripts are not supported")
+        for item, index, ctype, source in circuit.get("control_specs", []):
+            target = _CONTROL_TARGETS.get((item, ctype.lower()))
+            if target is None:
+                raise NotImplementedError(f"netlist control type {ctype!r} on {item} {index} is not supported")
+            if controllers is None or source not in controllers:
+                raise NotImplementedError(f"no controller given for the control script {source!r}")
+            bound.append((target, index, controllers[source]))
     if any(t != "f" for t in circuit["pressure_types"].values()):
         raise NotImplementedError("only fixed nodal pressures are supported")
     if circuit.get("interface_node") not in (None, 1):
@@ -155,14 +183,15 @@ def to_netlistbc(circuit: Dict, srfid: int, ignore_controls: bool = False) -> Ne
     return NetlistBC(srfid=srfid, components=list(circuit["components"]),
                      prescribed_pressures=dict(circuit["prescribed_pressures"]), prescribed_flows=fixed_flows,
                      interface_component=iface[0], initial_pressures=dict(circuit["initial_pressures"]),
-                     volumes=dict(circuit["volumes"]))
+                     volumes=dict(circuit["volumes"]), controllers=bound)
 
 
-def read_netlists(path: str, srfids: List[int]) -> List[NetlistBC]:
-    """Read a netlist_surfaces.dat or .xml; circuit k couples surface srfids[k]."""
+def read_netlists(path: str, srfids: List[int], controllers=None) -> List[NetlistBC]:
+    """Read a netlist_surfaces.dat or .xml; circuit k couples surface
+    srfids[k]; ``controllers`` maps control script names to controllers."""
     with open(path) as f:
         text = f.read()
     circuits = parse_netlist_xml(text) if path.endswith(".xml") else parse_netlist_dat(text)
     if len(circuits) != len(srfids):
         raise ValueError(f"{len(circuits)} circuits in {path}, {len(srfids)} surfaces given")
-    return [to_netlistbc(c, s) for c, s in zip(circuits, srfids)]
+    return [to_netlistbc(c, s, controllers=controllers) for c, s in zip(circuits, srfids)]

@@ -70,6 +70,11 @@ class NetlistBC:
     initial_pressures: node -> initial pressure (default 0).
     volumes: component (1-based) -> (initial volume, unstressed volume) for
     the "t" and "v" components.
+    controllers: (target, index, controller) triples: a
+    :class:`~crimsonflowsolver_b200.controllers.ParameterController` that
+    sets, after every step, the component value ("component"), a chamber's
+    unstressed volume ("unstressed_volume"), a node's pressure ("pressure")
+    or a component's fixed flow ("flow") of item ``index`` (1-based).
     """
     srfid: int
     components: List[Tuple[str, int, int, float]]
@@ -78,6 +83,7 @@ class NetlistBC:
     interface_component: int = 1
     initial_pressures: Dict[int, float] = field(default_factory=dict)
     volumes: Dict[int, Tuple[float, float]] = field(default_factory=dict)
+    controllers: List[Tuple[str, int, object]] = field(default_factory=list)
 
     @property
     def nnodes(self) -> int:

@@ -387,4 +387,10 @@ class FlowSolver:
         N.check(N.lib().crimson_step(self.elm.h, self.memls.lhs, self.memls.ls, ctypes.byref(args),
                                      ctypes.byref(st)), "crimson_step")
         self.istep += 1
+        # the netlists' control systems, after the step's finalisation (itrdrv.f90:2100)
+        bound = [(nl, t, i, c) for nl in self.netlists for t, i, c in nl.spec.controllers]
+        if bound:
+            from .controllers import run_controllers
+
+            run_controllers(bound, self.P.Delt)
         return st

@@ -337,8 +337,10 @@ int crimson_elmgmr_sclr_device(crimson_ctx* ctx, int isclr, double diffus, const
  * the interface node takes the 3D surface pressure as a prescribed pressure
  * and the interface component's flow is solved for; the flow solver then
  * holds the surface at its Dirichlet codes (itrdrv.f90:1114-1133).
- * Left-ventricular pressure prescriptions, time-varying prescriptions and
- * Python controllers are not supported.
+ * Control systems act through crimson_netlist_set_parameter (the Python
+ * controllers of crimsonflowsolver_b200.controllers drive it); the
+ * reference's built-in left-ventricular elastance and bleed controllers and
+ * left-ventricular pressure prescriptions are not built.
  * --------------------------------------------------------------------------- */
 typedef struct crimson_netlist crimson_netlist;
 #define CRIMSON_NETLIST_RESISTOR 0
@@ -385,6 +387,20 @@ int crimson_netlist_finalize_step(crimson_netlist* nl);
  * (ncomp, 1 = open) and volumes (ncomp, 0 for components without one); any
  * pointer may be NULL. */
 int crimson_netlist_get(const crimson_netlist* nl, double* pressures, double* flows, int* open, double* volumes);
+/* The parameters control systems adjust between steps
+ * (ControlSystemsManager.cxx:125-330; itrdrv.f90:2100 updates them after
+ * the step's finalisation): a component's value (R, C, L, a diode's open
+ * resistance, a chamber's elastance), a pressure chamber's unstressed
+ * volume, a node's pressure (the prescribed value of a fixed-pressure node;
+ * for other nodes the current value, which the next solve replaces) or a
+ * component's fixed prescribed flow.  index is 1-based; CRIMSON_ERR_ARG
+ * when the circuit has no such parameter. */
+#define CRIMSON_NETLIST_PARAM_COMPONENT 0
+#define CRIMSON_NETLIST_PARAM_UNSTRESSED_VOLUME 1
+#define CRIMSON_NETLIST_PARAM_PRESSURE 2
+#define CRIMSON_NETLIST_PARAM_FLOW 3
+int crimson_netlist_get_parameter(crimson_netlist* nl, int what, int index, double* value);
+int crimson_netlist_set_parameter(crimson_netlist* nl, int what, int index, double value);
 /* Checkpoint of the circuit state: state_size doubles, read (set = 0) or
  * written (set = 1). */
 int crimson_netlist_state_size(const crimson_netlist* nl, int* n);

@@ -220,3 +220,59 @@ class OracleNetlist:
 
     def interface_pressure(self):
         return self.pressure(1)
+
+    # ---- control systems (ControlSystemsManager.cxx:125-330) ----
+    def get_parameter(self, target, index):
+        j = index - 1
+        if target == "component":
+            return self.comps[j][3]
+        if target == "unstressed_volume":
+            assert self.comps[j][0] == "v"
+            return self.v0[j]
+        if target == "pressure":
+            return self.fixed[index] if index in self.fixed else float(self.p[j])
+        if target == "flow":
+            return self.fixed_flow[index]
+        raise KeyError(target)
+
+    def set_parameter(self, target, index, value):
+        j = index - 1
+        if target == "component":
+            k, s, e, _ = self.comps[j]
+            self.comps[j] = (k, s, e, float(value))
+        elif target == "unstressed_volume":
+            assert self.comps[j][0] == "v"
+            self.v0[j] = float(value)
+        elif target == "pressure":
+            if index in self.fixed:
+                self.fixed[index] = float(value)
+            else:
+                self.p[j] = float(value)
+        elif target == "flow":
+            assert index in self.fixed_flow
+            self.fixed_flow[index] = float(value)
+        else:
+            raise KeyError(target)
+
+    def observables(self):
+        p = {i + 1: float(self.pressure(i + 1)) for i in range(self.np_)}
+        q = {j + 1: float(self.q[j]) for j in range(self.nc)}
+        v = {j + 1: float(self.vol[j]) for j in self.vol_comps}
+        return p, q, v
+
+
+def run_controllers(bound, delt):
+    """The control systems' update of one step: ascending priority, each
+    controller given the values the earlier ones published (the first
+    publication of a name kept), its return value set as the parameter."""
+    order = sorted(range(len(bound)), key=lambda k: bound[k][3].getControllerPriority())
+    gathered = {}
+    for k in order:
+        circuit, target, index, ctl = bound[k]
+        ctl.receive_broadcast(gathered)
+        p, q, v = circuit.observables()
+        circuit.set_parameter(target, index, float(ctl.updateControl(circuit.get_parameter(target, index), delt,
+                                                                     p, q, v)))
+        for name, data in ctl.broadcast_data().items():
+            if name not in gathered:
+                gathered[name] = data

@@ -478,3 +478,10 @@ class OracleFlow:
         self.yold = self.y.copy()
         self.acold = self.ac.copy()
         self.istep += 1
+        # control systems after the finalisation (itrdrv.f90:2100)
+        bound = [(nl, t, i, c) for nl, r in zip(self.netlists, self.rcr) if nl is not None
+                 for t, i, c in r.controllers]
+        if bound:
+            from oracle.netlist_oracle import run_controllers
+
+            run_controllers(bound, self.P.Delt)

@@ -111,3 +111,53 @@ def test_valve_switches_surface_between_dirichlet_and_neumann():
     o = F.netlists[1]
     assert relerr(p, [o.pressure(i + 1) for i in range(len(p))]) < 1e-10
     assert list(op) == list(o.open)
+
+
+def test_controllers_in_time_steps_parity():
+    """Control systems between steps (itrdrv.f90:2100): a sensor controller
+    publishes a signal from the outlet pressure and a second one scales the
+    distal resistance by it.  Four steps, device vs oracle (each with its
+    own controller instances): state, outlet pressure and the controlled
+    resistance."""
+    from crimsonflowsolver_b200.controllers import ParameterController
+
+    class Sensor(ParameterController):
+        controllerPriority = 1
+
+        def updateControl(self, value, delt, pressures, flows, volumes):
+            self.clearBroadcastData()
+            self.addBroadcastVariable("signal", 1.0 + 1e-4 * pressures[1])
+            return value
+
+    class Distal(ParameterController):
+        controllerPriority = 2
+
+        def __init__(self, name):
+            super().__init__(name)
+            self.base = None
+
+        def updateControl(self, value, delt, pressures, flows, volumes):
+            self.base = value if self.base is None else self.base
+            return self.base * self.getRecievedBroadcastValue("sensor", "signal")
+
+    def spec():
+        s = NetlistBC.rcr(3, Rp=100.0, C=1e-4, Rd=1000.0, Pd=0.0)
+        s.controllers = [("component", 3, Distal("distal")), ("pressure", 1, Sensor("sensor"))]
+        return s
+
+    Pg, Po = FlowParams(netlists=[spec()]), FlowParams(netlists=[spec()])
+    F = po.OracleFlow(mesh.cylinder(ncross=8, naxial=10), Po, inflow=_inflow)
+    G = solver.FlowSolver(mesh.cylinder(ncross=8, naxial=10), Pg, inflow=_inflow)
+    try:
+        for _ in range(4):
+            F.step()
+            st = G.step()
+            assert abs(st.p_out[0] - F.Pn[0]) <= 1e-10 * abs(F.Pn[0])
+            rg = G.netlists[0].get_parameter("component", 3)
+            ro = F.netlists[0].get_parameter("component", 3)
+            assert abs(rg - ro) <= 1e-10 * abs(ro) and rg != 1000.0
+        y, _ = G.state()
+    finally:
+        G.close()
+    assert relerr(y[:, 0:3], F.y[:, 0:3]) < 1e-10, relerr(y[:, 0:3], F.y[:, 0:3])
+    assert relerr(y[:, 3], F.y[:, 3]) < 1e-10, relerr(y[:, 3], F.y[:, 3])
