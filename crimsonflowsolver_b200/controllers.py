@@ -18,6 +18,8 @@ from __future__ import annotations
 
 from typing import Dict, Iterable, List, Tuple
 
+import numpy as np
+
 
 class ParameterController:
     """Base class of a control system: override :meth:`updateControl`.
@@ -56,6 +58,38 @@ class ParameterController:
 
     def receive_broadcast(self, data: Dict[str, Dict[str, float]]) -> None:
         self._received = {k: dict(v) for k, v in data.items()}
+
+
+class PeriodicTableController(ParameterController):
+    """The reference's prescribedPeriodicFlow / prescribedPeriodicPressure
+    controls (its flowPrescriber / pressurePrescriber scripts): a table of
+    (time, value) rows starting at time 0 repeats with the period of its
+    last time; each step advances the periodic time by delt (wrapping once
+    it reaches the period) and returns the table's linear interpolation
+    there."""
+
+    def __init__(self, name: str, times, values):
+        super().__init__(name)
+        self.times = np.asarray(times, dtype=np.float64)
+        self.values = np.asarray(values, dtype=np.float64)
+        if self.times.ndim != 1 or self.times.size < 2 or self.times.shape != self.values.shape:
+            raise ValueError("a periodic table needs two or more (time, value) rows")
+        if self.times[0] != 0.0 or np.any(np.diff(self.times) <= 0.0):
+            raise ValueError("periodic table times must start at 0 and increase")
+        self.period = float(self.times[-1])
+        self.time = 0.0
+
+    @classmethod
+    def from_file(cls, name: str, path: str) -> "PeriodicTableController":
+        """Two plain-text columns (time, value), as the reference's <name>.dat."""
+        data = np.loadtxt(path, ndmin=2)
+        return cls(name, data[:, 0], data[:, 1])
+
+    def updateControl(self, currentParameterValue, delt, *observables):
+        self.time += delt
+        if self.time >= self.period:
+            self.time -= self.period
+        return float(np.interp(self.time, self.times, self.values))
 
 
 def run_controllers(bound: Iterable[Tuple[object, str, int, ParameterController]], delt: float) -> None:

@@ -28,8 +28,9 @@ interface node other than 1).
 """
 from __future__ import annotations
 
+import os
 import xml.etree.ElementTree as ET
-from typing import Dict, List
+from typing import Dict, List, Optional
 
 from .problem import NetlistBC
 
@@ -151,27 +152,39 @@ def parse_netlist_xml(text: str) -> List[Dict]:
 # that act through a user controller, and the parameter each one drives
 _CONTROL_TARGETS = {("component", "custompython"): "component",
                     ("component", "custompythonunstressedvolume"): "unstressed_volume",
-                    ("node", "custompython"): "pressure"}
+                    ("node", "custompython"): "pressure",
+                    ("component", "prescribedperiodicflow"): "flow",
+                    ("node", "prescribedperiodicpressure"): "pressure"}
+_PERIODIC = ("prescribedperiodicflow", "prescribedperiodicpressure")
 
 
-def to_netlistbc(circuit: Dict, srfid: int, ignore_controls: bool = False, controllers=None) -> NetlistBC:
+def to_netlistbc(circuit: Dict, srfid: int, ignore_controls: bool = False, controllers=None,
+                 data_dir: Optional[str] = None) -> NetlistBC:
     """One parsed circuit as the outlet of surface ``srfid``.  A circuit's
     customPython controls (component parameter, unstressed volume, node
     pressure) take their controller from ``controllers``, a mapping from the
     script name of the input to a
-    :class:`~crimsonflowsolver_b200.controllers.ParameterController`; with
-    ``ignore_controls`` the parameters stay at their input values.  Other
-    control types (the built-in left-ventricular elastance and bleed
-    controllers, periodic flow / pressure files) raise."""
+    :class:`~crimsonflowsolver_b200.controllers.ParameterController`; its
+    prescribedPeriodicFlow / prescribedPeriodicPressure controls read the
+    table ``<source>.dat`` from ``data_dir`` (unless ``controllers`` names
+    them); with ``ignore_controls`` the parameters stay at their input
+    values.  The built-in left-ventricular elastance and bleed controllers
+    raise."""
+    from .controllers import PeriodicTableController
+
     bound = []
     if circuit["controls"] and not ignore_controls:
         for item, index, ctype, source in circuit.get("control_specs", []):
             target = _CONTROL_TARGETS.get((item, ctype.lower()))
             if target is None:
                 raise NotImplementedError(f"netlist control type {ctype!r} on {item} {index} is not supported")
-            if controllers is None or source not in controllers:
+            if controllers is not None and source in controllers:
+                bound.append((target, index, controllers[source]))
+            elif ctype.lower() in _PERIODIC and data_dir is not None:
+                path = os.path.join(data_dir, source + ".dat")
+                bound.append((target, index, PeriodicTableController.from_file(source, path)))
+            else:
                 raise NotImplementedError(f"no controller given for the control script {source!r}")
-            bound.append((target, index, controllers[source]))
     if any(t != "f" for t in circuit["pressure_types"].values()):
         raise NotImplementedError("only fixed nodal pressures are supported")
     if circuit.get("interface_node") not in (None, 1):
@@ -194,4 +207,5 @@ def read_netlists(path: str, srfids: List[int], controllers=None) -> List[Netlis
     circuits = parse_netlist_xml(text) if path.endswith(".xml") else parse_netlist_dat(text)
     if len(circuits) != len(srfids):
         raise ValueError(f"{len(circuits)} circuits in {path}, {len(srfids)} surfaces given")
-    return [to_netlistbc(c, s, controllers=controllers) for c, s in zip(circuits, srfids)]
+    return [to_netlistbc(c, s, controllers=controllers, data_dir=os.path.dirname(os.path.abspath(path)))
+            for c, s in zip(circuits, srfids)]

@@ -6,10 +6,13 @@ once where a checkout exists:
     python tests/golden/make_netlist_fixture.py /path/to/reference/checkout
 
 Writes netlist_inputs.json: {path relative to testbin/mainTests: file text},
-one entry per distinct file text.
+one entry per distinct file text; and netlist_periodic_tables.json: the
+(time, value) tables ("<source>.dat" beside the input) that the inputs'
+prescribedPeriodicFlow / prescribedPeriodicPressure controls name.
 """
 import json
 import os
+import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -17,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 def main(ref):
     base = os.path.join(ref, "testbin", "mainTests")
-    seen, out = set(), {}
+    seen, out, tables = set(), {}, {}
     for root, _, files in sorted(os.walk(base)):
         for name in sorted(files):
             if name not in ("netlist_surfaces.dat", "netlist_surfaces.xml"):
@@ -25,13 +28,20 @@ def main(ref):
             path = os.path.join(root, name)
             with open(path) as f:
                 text = f.read()
+            for src in re.findall(r"prescribedPeriodic(?:Flow|Pressure)\s*(?:</type>\s*<source>)?\s*(\w+)", text):
+                tpath = os.path.join(root, src + ".dat")
+                if os.path.exists(tpath):
+                    with open(tpath) as f:
+                        tables[os.path.relpath(tpath, base)] = f.read()
             if text in seen:
                 continue
             seen.add(text)
             out[os.path.relpath(path, base)] = text
     with open(os.path.join(HERE, "netlist_inputs.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
-    print(len(out), "files")
+    with open(os.path.join(HERE, "netlist_periodic_tables.json"), "w") as f:
+        json.dump(tables, f, indent=1, sort_keys=True)
+    print(len(out), "files,", len(tables), "periodic tables")
 
 
 if __name__ == "__main__":

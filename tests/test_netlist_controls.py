@@ -137,7 +137,8 @@ def test_reference_control_declarations_parse_and_bind():
     """The customPython controls of the reference's baroreflex case (the
     .dat's coronary circuit: two component controllers and a node
     controller) bind to user controllers; the built-in LV elastance control
-    and file-driven prescriptions raise."""
+    raises, and so does a file-driven prescription given neither its table's
+    directory nor a controller."""
     coronary = _parse("x.dat", _inputs()["netlist/baroreflexPython/netlist_surfaces.dat"])[1]
     assert coronary["control_specs"] == [("component", 3, "customPython", "coronaryRpController"),
                                          ("component", 5, "customPython", "coronaryRdController"),
@@ -153,4 +154,51 @@ def test_reference_control_declarations_parse_and_bind():
         nio.to_netlistbc(lv, 3, controllers={})  # built-in LV elastance controller
     files = _parse("x.xml", _inputs()["zeroDDomain/pythonFlowPrescriptions/netlist_surfaces.xml"])[2]
     with pytest.raises(NotImplementedError):
-        nio.to_netlistbc(files, 3, controllers={"flowPrescriber": PressureSensor("f")})
+        nio.to_netlistbc(files, 3, controllers={})
+
+
+def _tables():
+    import json
+    import os
+
+    with open(os.path.join(os.path.dirname(__file__), "golden", "netlist_periodic_tables.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("case,target,index", [("pythonFlowPrescriptions", "flow", 2),
+                                               ("pythonPressurePrescriptions", "pressure", 3)])
+def test_periodic_table_controls(tmp_path, case, target, index):
+    """The reference's periodic prescriptions (its zeroDDomain
+    pythonFlowPrescriptions / pythonPressurePrescriptions inputs, third
+    circuit): the table beside the input drives a component's fixed flow or
+    a node's fixed pressure, advancing by delt per step and wrapping at the
+    table's last time; library and oracle take the same values."""
+    name = f"zeroDDomain/{case}/netlist_surfaces.xml"
+    circuit = _parse("x.xml", _inputs()[name])[2]
+    (item, idx, ctype, source), = circuit["control_specs"]
+    assert idx == index and ctype.startswith("prescribedPeriodic")
+    table = _tables()[f"zeroDDomain/{case}/{source}.dat"]
+    (tmp_path / f"{source}.dat").write_text(table)
+    gspec = nio.to_netlistbc(circuit, 3, data_dir=str(tmp_path))
+    ospec = nio.to_netlistbc(circuit, 3, data_dir=str(tmp_path))
+    assert [(t, i) for t, i, _ in gspec.controllers] == [(target, index)]
+    data = np.loadtxt(str(tmp_path / f"{source}.dat"))
+    g, o = Netlist(gspec), OracleNetlist(ospec)
+    time = 0.0
+    for step in range(130):
+        q = 20.0 + 10.0 * np.sin(2 * np.pi * step / 50)
+        g.update(DT, q)
+        o.update(DT, q)
+        g.finalize_step()
+        o.finalize_step()
+        run_controllers([(g, t, i, c) for t, i, c in gspec.controllers], DT)
+        oracle_run_controllers([(o, t, i, c) for t, i, c in ospec.controllers], DT)
+        time += DT
+        if time >= data[-1, 0]:
+            time -= data[-1, 0]
+        want = np.interp(time, data[:, 0], data[:, 1])
+        assert g.get_parameter(target, index) == pytest.approx(want, rel=1e-12, abs=1e-9)
+        assert o.get_parameter(target, index) == pytest.approx(want, rel=1e-12, abs=1e-9)
+        p, f, _, _ = g.get()
+        assert _close(p, [o.pressure(i + 1) for i in range(len(p))], 1e-10) and _close(f, o.q, 1e-10)
+    g.close()
