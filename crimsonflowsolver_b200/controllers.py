@@ -92,6 +92,61 @@ class PeriodicTableController(ParameterController):
         return float(np.interp(self.time, self.times, self.values))
 
 
+class BleedController(ParameterController):
+    """The reference's built-in bleed control (ParameterController.cxx:
+    66-74, timers.cxx): from the trigger step on (1600 steps after the
+    start, counted by its own timer) the controlled resistance or compliance
+    is set to 0.001.  Built-in controllers update after the Python ones
+    (ControlSystemsManager.cxx:7-16), hence the infinite priority."""
+
+    controllerPriority = float("inf")
+
+    def __init__(self, name: str = "bleed", trigger_step: int = 1600, value: float = 0.001):
+        super().__init__(name)
+        self.step = 0
+        self.trigger_step = int(trigger_step)
+        self.value = float(value)
+
+    def updateControl(self, currentParameterValue, delt, *observables):
+        on = self.step >= self.trigger_step
+        self.step += 1
+        return self.value if on else currentParameterValue
+
+
+class LeftVentricularElastanceController(ParameterController):
+    """The reference's built-in left-ventricular elastance control
+    (ParameterController.cxx:11-57): the time-varying elastance of Pope et
+    al., Math. Biosci. Eng. 6 (2009) 93-115 -- a raised cosine from
+    ``e_min`` to ``e_max`` over ``t_max``, back down over ``t_relax``, then
+    ``e_min`` to the end of the period -- on a periodic time advanced by
+    delt each step.  The defaults are the reference's values.  At set-up the
+    controlled elastance takes the value at the starting time
+    (:meth:`elastance`)."""
+
+    controllerPriority = float("inf")
+
+    def __init__(self, name: str = "lvElastance", start_time: float = 0.0, t_max: float = 0.2782,
+                 t_relax: float = 0.1391, e_min: float = 4.10246e-3, e_max: float = 3.0827e-1,
+                 period: float = 0.86):
+        super().__init__(name)
+        self.time = float(start_time)
+        self.t_max, self.t_relax, self.e_min, self.e_max, self.period = t_max, t_relax, e_min, e_max, period
+
+    def elastance(self) -> float:
+        t, de = self.time, self.e_max - self.e_min
+        if t <= self.t_max:
+            return self.e_min + 0.5 * de * (1.0 - np.cos(t * np.pi / self.t_max))
+        if t <= self.t_max + self.t_relax:
+            return self.e_min + 0.5 * de * (1.0 + np.cos((t - self.t_max) * (np.pi / self.t_relax)))
+        return self.e_min
+
+    def updateControl(self, currentParameterValue, delt, *observables):
+        self.time += delt
+        if self.time >= self.period:
+            self.time -= self.period
+        return float(self.elastance())
+
+
 def run_controllers(bound: Iterable[Tuple[object, str, int, ParameterController]], delt: float) -> None:
     """One update of every control system (updateAndPassStateInformation-
     BetweenPythonParameterControllers): ``bound`` holds (circuit, target,

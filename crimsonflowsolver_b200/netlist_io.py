@@ -154,8 +154,15 @@ _CONTROL_TARGETS = {("component", "custompython"): "component",
                     ("component", "custompythonunstressedvolume"): "unstressed_volume",
                     ("node", "custompython"): "pressure",
                     ("component", "prescribedperiodicflow"): "flow",
-                    ("node", "prescribedperiodicpressure"): "pressure"}
+                    ("node", "prescribedperiodicpressure"): "pressure",
+                    ("component", "bleed"): "component",
+                    ("component", "bleedresistance"): "component",
+                    ("component", "bleedcompliance"): "component",
+                    ("component", "l"): "component",
+                    ("component", "leftventricularelastance"): "component"}
 _PERIODIC = ("prescribedperiodicflow", "prescribedperiodicpressure")
+_BLEED = ("bleed", "bleedresistance", "bleedcompliance")
+_LV = ("l", "leftventricularelastance")
 
 
 def to_netlistbc(circuit: Dict, srfid: int, ignore_controls: bool = False, controllers=None,
@@ -168,17 +175,29 @@ def to_netlistbc(circuit: Dict, srfid: int, ignore_controls: bool = False, contr
     prescribedPeriodicFlow / prescribedPeriodicPressure controls read the
     table ``<source>.dat`` from ``data_dir`` (unless ``controllers`` names
     them); with ``ignore_controls`` the parameters stay at their input
-    values.  The built-in left-ventricular elastance and bleed controllers
-    raise."""
-    from .controllers import PeriodicTableController
+    values; bleed and left-ventricular elastance controls take the built-in
+    :class:`~crimsonflowsolver_b200.controllers.BleedController` and
+    :class:`~crimsonflowsolver_b200.controllers.LeftVentricularElastanceController`
+    (the latter sets its chamber's elastance to the starting value)."""
+    from .controllers import BleedController, LeftVentricularElastanceController, PeriodicTableController
 
     bound = []
+    components = list(circuit["components"])
     if circuit["controls"] and not ignore_controls:
         for item, index, ctype, source in circuit.get("control_specs", []):
             target = _CONTROL_TARGETS.get((item, ctype.lower()))
             if target is None:
                 raise NotImplementedError(f"netlist control type {ctype!r} on {item} {index} is not supported")
-            if controllers is not None and source in controllers:
+            if ctype.lower() in _BLEED:
+                bound.append((target, index, BleedController(f"bleed{index}")))
+            elif ctype.lower() in _LV:
+                k, st, en, _ = components[index - 1]
+                if k not in ("t", "v"):
+                    raise ValueError(f"an LV elastance control needs a volume-tracking component, not {k!r}")
+                ctl = LeftVentricularElastanceController(f"lvElastance{index}")
+                components[index - 1] = (k, st, en, ctl.elastance())   # the set-up value
+                bound.append((target, index, ctl))
+            elif controllers is not None and source in controllers:
                 bound.append((target, index, controllers[source]))
             elif ctype.lower() in _PERIODIC and data_dir is not None:
                 path = os.path.join(data_dir, source + ".dat")
@@ -193,7 +212,7 @@ def to_netlistbc(circuit: Dict, srfid: int, ignore_controls: bool = False, contr
     if len(iface) != 1:
         raise ValueError("exactly one component must carry the 3D interface flow")
     fixed_flows = {j: v for j, v in circuit["prescribed_flows"].items() if circuit["flow_types"][j] == "f"}
-    return NetlistBC(srfid=srfid, components=list(circuit["components"]),
+    return NetlistBC(srfid=srfid, components=components,
                      prescribed_pressures=dict(circuit["prescribed_pressures"]), prescribed_flows=fixed_flows,
                      interface_component=iface[0], initial_pressures=dict(circuit["initial_pressures"]),
                      volumes=dict(circuit["volumes"]), controllers=bound)

@@ -136,9 +136,9 @@ def test_controllers_drive_library_and_oracle_alike():
 def test_reference_control_declarations_parse_and_bind():
     """The customPython controls of the reference's baroreflex case (the
     .dat's coronary circuit: two component controllers and a node
-    controller) bind to user controllers; the built-in LV elastance control
-    raises, and so does a file-driven prescription given neither its table's
-    directory nor a controller."""
+    controller) bind to user controllers, the built-in LV elastance control
+    to its built-in controller; a file-driven prescription given neither its
+    table's directory nor a controller raises."""
     coronary = _parse("x.dat", _inputs()["netlist/baroreflexPython/netlist_surfaces.dat"])[1]
     assert coronary["control_specs"] == [("component", 3, "customPython", "coronaryRpController"),
                                          ("component", 5, "customPython", "coronaryRdController"),
@@ -150,8 +150,10 @@ def test_reference_control_declarations_parse_and_bind():
     with pytest.raises(NotImplementedError):
         nio.to_netlistbc(coronary, 4)            # no controllers given
     lv = _parse("x.xml", _inputs()["netlist/heart/netlist_surfaces.xml"])[0]
-    with pytest.raises(NotImplementedError):
-        nio.to_netlistbc(lv, 3, controllers={})  # built-in LV elastance controller
+    spec = nio.to_netlistbc(lv, 3, controllers={})
+    assert [(t, i, type(c).__name__) for t, i, c in spec.controllers] == [
+        ("component", 5, "LeftVentricularElastanceController")]
+    assert spec.components[4][3] == pytest.approx(4.10246e-3)   # the set-up elastance
     files = _parse("x.xml", _inputs()["zeroDDomain/pythonFlowPrescriptions/netlist_surfaces.xml"])[2]
     with pytest.raises(NotImplementedError):
         nio.to_netlistbc(files, 3, controllers={})
@@ -202,3 +204,55 @@ def test_periodic_table_controls(tmp_path, case, target, index):
         p, f, _, _ = g.get()
         assert _close(p, [o.pressure(i + 1) for i in range(len(p))], 1e-10) and _close(f, o.q, 1e-10)
     g.close()
+
+
+def test_bleed_controller_and_builtin_order():
+    """The built-in bleed control sets its component to 0.001 from its
+    trigger step on (1600 steps in the reference), after every Python
+    controller of the step."""
+    from crimsonflowsolver_b200.controllers import BleedController
+
+    seen = []
+
+    class Watch(ParameterController):
+        controllerPriority = 5
+
+        def updateControl(self, value, delt, pressures, flows, volumes):
+            seen.append(g.get_parameter("component", 5))
+            return value
+
+    g = Netlist(_circuit())
+    bound = [(g, "component", 5, BleedController("bleed", trigger_step=3)), (g, "pressure", 1, Watch("w"))]
+    values = []
+    for step in range(6):
+        if g.flow_permitted():
+            g.update(DT, 40.0)
+        else:
+            g.update_pressure(DT, 400.0)
+        g.finalize_step()
+        run_controllers(bound, DT)
+        values.append(g.get_parameter("component", 5))
+    assert values == [900.0, 900.0, 900.0, 0.001, 0.001, 0.001]
+    assert seen == [900.0, 900.0, 900.0, 900.0, 0.001, 0.001]   # the Python controller ran first each step
+    assert BleedController().trigger_step == 1600
+    g.close()
+
+
+def test_lv_elastance_curve():
+    """The built-in LV elastance follows the raised-cosine curve: e_min at
+    the cycle start, e_max at t_max, halfway down at t_max + t_relax / 2,
+    e_min after the relaxation, periodic in the heart period."""
+    from crimsonflowsolver_b200.controllers import LeftVentricularElastanceController as LV
+
+    c = LV()
+    assert c.elastance() == pytest.approx(c.e_min)
+    for t, want in [(c.t_max, c.e_max), (c.t_max + 0.5 * c.t_relax, 0.5 * (c.e_min + c.e_max)),
+                    (c.t_max + c.t_relax + 0.1, c.e_min), (0.25 * c.t_max, c.e_min + 0.5 * (c.e_max - c.e_min)
+                                                          * (1 - np.cos(np.pi / 4)))]:
+        c.time = t
+        assert c.elastance() == pytest.approx(want, rel=1e-12)
+    c = LV()
+    dt = 1e-3
+    vals = [c.updateControl(0.0, dt) for _ in range(2 * 860)]
+    assert vals[859] == pytest.approx(c.e_min, rel=1e-9) and vals[:860] == pytest.approx(vals[860:], rel=1e-9)
+    assert max(vals) == pytest.approx(c.e_max, rel=1e-4)

@@ -168,12 +168,66 @@ def test_emulate_rcr_input_is_the_rcr_model():
 
 
 def test_unsupported_features_raise():
+    """Left-ventricular pressure prescriptions (the reference itself exits
+    on them without its heart model, NetlistCircuit.cxx:1391-1395) and
+    unknown control types raise; the built-in LV elastance control binds."""
     heart = _parse("x.dat", _inputs()["netlist/netlist_surfaces.dat"])[0]
-    with pytest.raises(NotImplementedError):
-        nio.to_netlistbc(heart, 3)
+    spec = nio.to_netlistbc(heart, 3)
+    assert [(t, i, type(c).__name__) for t, i, c in spec.controllers] == [
+        ("component", 5, "LeftVentricularElastanceController")]
     lv = dict(heart, controls=0, pressure_types={6: "l"})
     with pytest.raises(NotImplementedError):
         nio.to_netlistbc(lv, 3)
+    odd = dict(heart, control_specs=[("component", 5, "pc", "")])
+    with pytest.raises(NotImplementedError):
+        nio.to_netlistbc(odd, 3)
+
+
+def _builtin_controlled():
+    out = []
+    for name, text in sorted(_inputs().items()):
+        for k, c in enumerate(_parse(name, text)):
+            types = {t.lower() for _, _, t, _ in c["control_specs"]}
+            if types and types <= {"l", "leftventricularelastance", "bleed", "bleedresistance"} and _square(c):
+                out.append(pytest.param(name, k, id=f"{name}#{k + 1}"))
+    return out
+
+
+@pytest.mark.parametrize("name,k", _builtin_controlled())
+def test_reference_circuit_with_builtin_controls(name, k):
+    """The reference's heart circuits with their built-in LV elastance
+    control bound (the chamber's elastance follows the Pope et al. curve,
+    set after every step): twelve steps through both designs, library vs
+    oracle, each side with its own controller instances."""
+    from crimsonflowsolver_b200.controllers import run_controllers
+    from oracle.netlist_oracle import run_controllers as oracle_run
+
+    c = _parse(name, _inputs()[name])[k]
+    gs, os_ = nio.to_netlistbc(c, 3), nio.to_netlistbc(c, 3)
+    g, o = Netlist(gs), OracleNetlist(os_)
+    gb = [(g, t, i, ctl) for t, i, ctl in gs.controllers]
+    ob = [(o, t, i, ctl) for t, i, ctl in os_.controllers]
+    try:
+        for step in range(12):
+            assert g.flow_permitted() == o.permitted, step
+            if o.permitted:
+                assert _close(g.implicit_coefficients(ALFI * DT), o.implicit_coefficients(ALFI * DT), 1e-9)
+                g.update(DT, _q3d(step))
+                o.update(DT, _q3d(step))
+            else:
+                g.update_pressure(DT, _p3d(step))
+                o.update_pressure(DT, _p3d(step))
+            g.finalize_step()
+            o.finalize_step()
+            run_controllers(gb, DT)
+            oracle_run(ob, DT)
+            p, f, _, vol = g.get()
+            assert _close(p, [o.pressure(i + 1) for i in range(len(p))], 1e-9)
+            assert _close(f, o.q, 1e-9)
+            for t, i, _ in gs.controllers:
+                assert g.get_parameter(t, i) == pytest.approx(o.get_parameter(t, i), rel=1e-12)
+    finally:
+        g.close()
 
 
 def test_read_netlists_assigns_surfaces(tmp_path):
