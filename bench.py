@@ -701,7 +701,28 @@ def run_microbench(args):
                                  "algorithmic_bytes_per_elem": 768, "achieved_gbs": sclr_bytes / t_s / 1e9,
                                  "frac": sclr_bytes / t_s / 1e9 / peak,
                                  "residual_only_ms": t_sr * 1e3}
-    del ds, dsd, rs, S
+    # size-independent checks at full size: two more calls give the same
+    # bits; the patch test (zero velocity, linear scalar) leaves only
+    # rounding on the interior nodes (the lattice has no boundary faces)
+    ref_r, ref_S = rs.clone(), S.clone()
+    elm.sclr_device(dy, ds, dsd, rs, S, isclr=1, diffus=0.1)
+    elm.sclr_device(dy, ds, dsd, rs, S, isclr=1, diffus=0.1)
+    torch.cuda.synchronize()
+    repeatable = bool(torch.equal(rs, ref_r) and torch.equal(S, ref_S))
+    scale = float(ref_r.abs().max())
+    nn1 = args.lattice + 1
+    ijk = np.stack(np.unravel_index(np.arange(n), (nn1, nn1, nn1), order="F"), axis=1)
+    interior = torch.tensor(np.all((ijk > 0) & (ijk < args.lattice), axis=1), device=dev)
+    ds.copy_(torch.tensor(m.x @ np.array([0.3, -1.2, 0.7]) + 2.0, device=dev))
+    dsd.zero_()
+    y0 = torch.zeros_like(dy)
+    elm.sclr_device(y0, ds, dsd, rs, S, isclr=1, diffus=0.1)
+    torch.cuda.synchronize()
+    patch = float(rs[interior].abs().max())
+    out["assembly_sclr_fp64"]["full_size_checks"] = {
+        "repeatable_bitwise": repeatable, "patch_max_interior_res": patch,
+        "patch_rel_to_random_state_res": patch / scale}
+    del ds, dsd, rs, S, y0, ref_r, ref_S
     if not args.no_cpu:
         # cpu_baseline of the scalar assembly: the oracle restatement, one
         # thread, on a 40^3-cell lattice (384,000 tets) with the same fields
