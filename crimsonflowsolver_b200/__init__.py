@@ -4,9 +4,9 @@ The CUDA library is built in-tree with :func:`build`; every compute entry point
 runs on the GPU through the C ABI in include/crimson_b200.h.
 """
 from ._native import build, lib  # noqa: F401
-from .problem import RCR, FlowParams, NetlistBC, time_params  # noqa: F401
+from .problem import RCR, FlowParams, NetlistBC, NetlistLoopBC, time_params  # noqa: F401
 
-__all__ = ["build", "lib", "FlowParams", "RCR", "NetlistBC", "time_params", "mesh", "solver", "netlist"]
+__all__ = ["build", "lib", "FlowParams", "RCR", "NetlistBC", "NetlistLoopBC", "time_params", "mesh", "solver", "netlist"]
 
 
 def __getattr__(name):

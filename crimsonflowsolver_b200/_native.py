@@ -120,6 +120,16 @@ SIGNATURES = {
     "crimson_netlist_create": (ctypes.c_int, [ctypes.POINTER(c_void_p), ctypes.c_int, c_int_p, c_int_p, c_int_p,
                                               c_dbl_p, c_dbl_p, c_dbl_p, ctypes.c_int, c_dbl_p, ctypes.c_int, c_int_p,
                                               c_dbl_p, ctypes.c_int, c_int_p, c_int_p, c_dbl_p, ctypes.c_int]),
+    "crimson_netlist_create_member": (ctypes.c_int, [ctypes.POINTER(c_void_p), ctypes.c_int, c_int_p, c_int_p,
+                                                     c_int_p, c_dbl_p, c_dbl_p, c_dbl_p, ctypes.c_int, c_dbl_p,
+                                                     ctypes.c_int, c_int_p, c_dbl_p, ctypes.c_int, c_int_p, c_int_p,
+                                                     c_dbl_p, ctypes.c_int, ctypes.c_int, c_int_p]),
+    "crimson_netlist_loop_create": (ctypes.c_int, [ctypes.POINTER(c_void_p), ctypes.c_int, ctypes.POINTER(c_void_p),
+                                                   c_void_p, ctypes.c_int, c_int_p, c_int_p, c_int_p]),
+    "crimson_netlist_loop_free": (None, [c_void_p]),
+    "crimson_netlist_loop_implicit_coefficients": (ctypes.c_int, [c_void_p, ctypes.c_double, c_dbl_p, c_dbl_p]),
+    "crimson_netlist_loop_update": (ctypes.c_int, [c_void_p, ctypes.c_double, c_dbl_p, c_dbl_p]),
+    "crimson_netlist_loop_finalize_step": (ctypes.c_int, [c_void_p]),
     "crimson_netlist_free": (None, [c_void_p]),
     "crimson_netlist_flow_permitted": (ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "crimson_netlist_implicit_coefficients": (ctypes.c_int, [c_void_p, ctypes.c_double, c_dbl_p, c_dbl_p]),
@@ -132,6 +142,7 @@ SIGNATURES = {
     "crimson_netlist_state_size": (ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "crimson_netlist_state": (ctypes.c_int, [c_void_p, c_dbl_p, ctypes.c_int]),
     "crimson_set_outlet_netlist": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p]),
+    "crimson_set_outlet_netlist_loop": (ctypes.c_int, [c_void_p, c_void_p, c_int_p]),
     "crimson_version": (ctypes.c_char_p, []),
     "crimson_last_error": (ctypes.c_char_p, []),
 }

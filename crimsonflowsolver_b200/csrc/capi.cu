@@ -853,7 +853,42 @@ int crimson_set_rcr(crimson_ctx* c, int n, const double* Rp, const double* C, co
 int crimson_set_outlet_netlist(crimson_ctx* c, int k, crimson_netlist* nl) {
     if (!c || k < 0 || k >= c->ncoupled) return CRIMSON_ERR_ARG;
     c->netlists.resize((size_t)c->ncoupled, nullptr);
+    c->loop_of.resize((size_t)c->ncoupled, -1);
+    if (c->loop_of[(size_t)k] >= 0) {
+        set_last_error("crimson_set_outlet_netlist: the surface belongs to a closed loop");
+        return CRIMSON_ERR_STATE;
+    }
+    if (nl && !nl->connect_nodes.empty()) {
+        set_last_error("crimson_set_outlet_netlist: a member of a closed loop couples through its loop");
+        return CRIMSON_ERR_ARG;
+    }
     c->netlists[(size_t)k] = nl;
+    return CRIMSON_OK;
+}
+
+int crimson_set_outlet_netlist_loop(crimson_ctx* c, crimson_netlist_loop* loop, const int* surfaces) {
+    if (!c || !loop || !surfaces) return CRIMSON_ERR_ARG;
+    const int nc = c->ncoupled;
+    c->netlists.resize((size_t)nc, nullptr);
+    c->loop_of.resize((size_t)nc, -1);
+    for (crimson_netlist_loop* l : c->loops)
+        if (l == loop) return CRIMSON_ERR_ARG;
+    for (int j = 0; j < loop->nup; ++j) {
+        const int k = surfaces[j];
+        if (k < 0 || k >= nc || c->netlists[(size_t)k] || c->loop_of[(size_t)k] >= 0) {
+            set_last_error("crimson_set_outlet_netlist_loop: a surface is out of range or already coupled");
+            return CRIMSON_ERR_ARG;
+        }
+        for (int e = 0; e < j; ++e)
+            if (surfaces[e] == k) return CRIMSON_ERR_ARG;
+    }
+    const int l = (int)c->loops.size();
+    c->loops.push_back(loop);
+    c->loop_surfaces.emplace_back(surfaces, surfaces + loop->nup);
+    for (int j = 0; j < loop->nup; ++j) {
+        c->netlists[(size_t)surfaces[j]] = loop->member[(size_t)j];
+        c->loop_of[(size_t)surfaces[j]] = l;
+    }
     return CRIMSON_OK;
 }
 
@@ -954,6 +989,17 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
     const double fct = (P.gami - 1.0) / P.gami;
     launch(k_predict, grid_for(4LL * n, 256), 256, 0, s, c->yold.p, c->acold.p, c->ycur.p, c->accur.p, 4LL * n, fct);
     launch(k_itrbc, grid_for(n, 256), 256, 0, s, c->iBC.p, c->BC.p, nb, n, c->ycur.p);
+    c->loop_of.resize((size_t)nc, -1);
+    // closed loops: one solve gives the coefficients of all their surfaces
+    for (size_t l = 0; l < c->loops.size(); ++l) {
+        const std::vector<int>& sf = c->loop_surfaces[l];
+        std::vector<double> a(sf.size()), b(sf.size());
+        CR_CHECK(crimson_netlist_loop_implicit_coefficients(c->loops[l], P.alfi * P.Delt, a.data(), b.data()));
+        for (size_t j = 0; j < sf.size(); ++j) {
+            c1[(size_t)sf[j]] = a[j];
+            c2[(size_t)sf[j]] = b[j];
+        }
+    }
     for (int k = 0; k < nc; ++k) {
         if (crimson_netlist* nl = c->netlists[(size_t)k]) {
             // the implicit coefficients with alfi*Delt
@@ -962,6 +1008,7 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
                 c1[k] = c2[k] = 0.0;
                 continue;
             }
+            if (c->loop_of[(size_t)k] >= 0) continue;
             CR_CHECK(crimson_netlist_implicit_coefficients(nl, P.alfi * P.Delt, &c1[k], &c2[k]));
         } else {
             rcr_coeffs(c->rcr_Rp[k], c->rcr_C[k], c->rcr_Rd[k], c->rcr_Pd[k], c->rcr_Pd[k], c->rcr_Pn[k],
@@ -1018,21 +1065,35 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
         CR_CUDA(cudaMemcpyAsync(hq.data(), c->flowq.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaMemcpyAsync(hp.data(), c->psurf.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
+        for (int k = 0; k < nc; ++k)
+            if (blocked[(size_t)k] && !(c->oarea[(size_t)k] > 0.0)) {
+                set_last_error("crimson_step: a blocked netlist surface has no area (set the boundary faces "
+                               "before crimson_set_outlets)");
+                return CRIMSON_ERR_STATE;
+            }
+        // closed loops: one update of every member with the flows (or, blocked,
+        // the surface pressures) of their surfaces, then the finalisation
+        for (size_t l = 0; l < c->loops.size(); ++l) {
+            const std::vector<int>& sf = c->loop_surfaces[l];
+            std::vector<double> lq(sf.size()), lp(sf.size(), 0.0);
+            for (size_t j = 0; j < sf.size(); ++j) {
+                lq[j] = hq[(size_t)sf[j]];
+                if (blocked[(size_t)sf[j]]) lp[j] = hp[(size_t)sf[j]] / c->oarea[(size_t)sf[j]];
+            }
+            CR_CHECK(crimson_netlist_loop_update(c->loops[l], P.Delt, lq.data(), lp.data()));
+            CR_CHECK(crimson_netlist_loop_finalize_step(c->loops[l]));
+        }
         for (int k = 0; k < nc; ++k) {
             if (crimson_netlist* nl = c->netlists[(size_t)k]) {
                 // updateLPN with the end-of-step flow (or, blocked, the surface
                 // pressure), then finalizeLPNAtEndOfTimestep (itrdrv.f90:1686-1688)
-                if (blocked[(size_t)k]) {
-                    if (!(c->oarea[(size_t)k] > 0.0)) {
-                        set_last_error("crimson_step: a blocked netlist surface has no area (set the boundary faces "
-                                       "before crimson_set_outlets)");
-                        return CRIMSON_ERR_STATE;
-                    }
-                    CR_CHECK(crimson_netlist_update_pressure(nl, P.Delt, hp[k] / c->oarea[(size_t)k]));
-                } else {
-                    CR_CHECK(crimson_netlist_update(nl, P.Delt, hq[k]));
+                if (c->loop_of[(size_t)k] < 0) {
+                    if (blocked[(size_t)k])
+                        CR_CHECK(crimson_netlist_update_pressure(nl, P.Delt, hp[k] / c->oarea[(size_t)k]));
+                    else
+                        CR_CHECK(crimson_netlist_update(nl, P.Delt, hq[k]));
+                    CR_CHECK(crimson_netlist_finalize_step(nl));
                 }
-                CR_CHECK(crimson_netlist_finalize_step(nl));
                 c->rcr_Pn[k] = nl->node[(size_t)nl->iface_node - 1].p;
                 c->rcr_Qn[k] = hq[k];
                 if (st && k < 8) {

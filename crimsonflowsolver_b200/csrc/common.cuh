@@ -227,5 +227,8 @@ struct crimson_ctx {
     int ninlet = 0;
     std::vector<double> rcr_Rp, rcr_C, rcr_Rd, rcr_Pd, rcr_Pn, rcr_Qn;
     std::vector<crimson_netlist*> netlists;  // per coupled surface; null: the RCR (not owned)
+    std::vector<crimson_netlist_loop*> loops;       // closed loops (not owned)
+    std::vector<std::vector<int>> loop_surfaces;    // per loop: the coupled surface of each upstream circuit
+    std::vector<int> loop_of;                       // per coupled surface: its loop, or -1
     int istep = 0;
 };

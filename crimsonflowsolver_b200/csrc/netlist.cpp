@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <new>
 #include <string>
 
@@ -69,10 +70,11 @@ std::vector<int> design_pf(const crimson_netlist* nl) {
 // node with more than one incident component, then one identity row per
 // prescribed value (fixed pressures, history pressures, prescribed flows,
 // history flows, history volumes).
-void build_system(crimson_netlist* nl, double alfi_delt) {
-    const int n = nl->n;
-    std::fill(nl->A.begin(), nl->A.end(), 0.0);
-    auto a = [&](int r, int c) -> double& { return nl->A[(size_t)r * n + c]; };
+// The rows go to M (leading dimension ld, zeroed by the caller) from row r0
+// on, the circuit's unknowns at columns c0..c0 + n - 1; a circuit that shares
+// nodes with another (a closed loop) writes n - (its shared nodes) rows.
+void build_rows(const crimson_netlist* nl, double alfi_delt, double* M, size_t ld, int r0, int c0) {
+    auto a = [&](int r, int c) -> double& { return M[(size_t)(r0 + r) * ld + (size_t)(c0 + c)]; };
     const int cf = col_flow(nl), chp = col_hist_p(nl), chq = col_hist_q(nl);
     const int cv = col_vol(nl), chv = col_hist_v(nl);
     int row = 0;
@@ -138,6 +140,11 @@ void build_system(crimson_netlist* nl, double alfi_delt) {
     for (size_t l = 0; l < nl->vol_comps.size(); ++l) a(row++, chv + (int)l) = 1.0;
 }
 
+void build_system(crimson_netlist* nl, double alfi_delt) {
+    std::fill(nl->A.begin(), nl->A.end(), 0.0);
+    build_rows(nl, alfi_delt, nl->A.data(), (size_t)nl->n, 0, 0);
+}
+
 // First row of the prescribed values (after the component and Kirchhoff rows).
 inline int first_prescribed_row(const crimson_netlist* nl) {
     return nl->nc + nl->nchamber + (int)nl->kirch_nodes.size();
@@ -154,31 +161,35 @@ int iface_row(const crimson_netlist* nl) {
 }
 
 // assembleRHS (NetlistCircuit.cxx:1370-1580) in the same row order.
-void assemble_rhs(crimson_netlist* nl) {
-    std::fill(nl->b.begin(), nl->b.end(), 0.0);
+void rhs_rows(const crimson_netlist* nl, double* b, int r0) {
+    b += r0;
     int row = first_prescribed_row(nl);
     // a fixed pressure, or the 3D surface pressure at the interface node
     // (Pressure_3DInterface, NetlistCircuit.cxx:1386-1410)
-    for (int nd : design_pp(nl)) nl->b[row++] = nl->node[nd - 1].fixed ? nl->node[nd - 1].fixed_p : nl->last_p3d;
-    for (int nd : nl->hist_nodes) nl->b[row++] = nl->node[nd - 1].hist;
+    for (int nd : design_pp(nl)) b[row++] = nl->node[nd - 1].fixed ? nl->node[nd - 1].fixed_p : nl->last_p3d;
+    for (int nd : nl->hist_nodes) b[row++] = nl->node[nd - 1].hist;
     for (int j : design_pf(nl)) {
         const NetlistComp& c = nl->comp[j];
-        nl->b[row++] = c.flow_kind == CRIMSON_NETLIST_FLOW_3D ? nl->last_q * nl->sign : c.flow_fixed;
+        b[row++] = c.flow_kind == CRIMSON_NETLIST_FLOW_3D ? nl->last_q * nl->sign : c.flow_fixed;
     }
-    for (int j : nl->hist_comps) nl->b[row++] = nl->comp[j].hist_flow;
-    for (int j : nl->vol_comps) nl->b[row++] = nl->comp[j].hist_volume;
+    for (int j : nl->hist_comps) b[row++] = nl->comp[j].hist_flow;
+    for (int j : nl->vol_comps) b[row++] = nl->comp[j].hist_volume;
     // a chamber's second row: compliance * pressure = volume - unstressed volume
     int r = 0;
     for (int j = 0; j < nl->nc; ++j, ++r)
-        if (nl->comp[j].kind == CRIMSON_NETLIST_PRESSURE_CHAMBER) nl->b[++r] = -nl->comp[j].unstressed;
+        if (nl->comp[j].kind == CRIMSON_NETLIST_PRESSURE_CHAMBER) b[++r] = -nl->comp[j].unstressed;
+}
+
+void assemble_rhs(crimson_netlist* nl) {
+    std::fill(nl->b.begin(), nl->b.end(), 0.0);
+    rhs_rows(nl, nl->b.data(), 0);
 }
 
 // solveLinearSystem (NetlistCircuit.cxx:1723-1733): the inverse of the
 // system matrix (Gauss-Jordan with partial pivoting), then x = A^-1 b.
-int solve(crimson_netlist* nl) {
-    const int n = nl->n;
-    std::vector<double> m(nl->A);
-    std::vector<double>& inv = nl->Ainv;
+int gj_solve(int n, const std::vector<double>& A, std::vector<double>& inv, const std::vector<double>& b,
+             std::vector<double>& x) {
+    std::vector<double> m(A);
     std::fill(inv.begin(), inv.end(), 0.0);
     for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
     double amax = 0.0;
@@ -211,12 +222,30 @@ int solve(crimson_netlist* nl) {
     }
     for (int i = 0; i < n; ++i) {
         double s = 0.0;
-        for (int c = 0; c < n; ++c) s += inv[(size_t)i * n + c] * nl->b[c];
-        nl->x[i] = s;
+        for (int c = 0; c < n; ++c) s += inv[(size_t)i * n + c] * b[c];
+        x[i] = s;
     }
-    for (double v : nl->x)
+    for (double v : x)
         if (!std::isfinite(v)) return fail("netlist: non-finite circuit solution", CRIMSON_ERR_NONFINITE);
     return CRIMSON_OK;
+}
+
+int solve(crimson_netlist* nl) { return gj_solve(nl->n, nl->A, nl->Ainv, nl->b, nl->x); }
+
+// giveNodesTheirPressuresFromSolutionVector / giveComponentsTheirFlows... /
+// giveComponentsTheirVolumes... (NetlistCircuit.cxx:1596-1660): the
+// circuit's segment xs of a solution; a chamber passes E (V - V_unstressed)
+// to its start node (CircuitComponent.cxx:188-209).
+void take_solution(crimson_netlist* nl, const double* xs) {
+    for (int i = 0; i < nl->np; ++i) nl->node[i].p = xs[i];
+    const int cf = col_flow(nl);
+    for (int j = 0; j < nl->nc; ++j) nl->comp[j].flow = xs[(size_t)cf + j];
+    const int cv = col_vol(nl);
+    for (int j : nl->vol_comps) {
+        NetlistComp& c = nl->comp[j];
+        c.volume = xs[(size_t)cv + nl->vol_ord[j]];
+        if (c.kind == CRIMSON_NETLIST_PRESSURE_CHAMBER) nl->node[(size_t)c.start - 1].p = (c.volume - c.unstressed) * c.value;
+    }
 }
 
 // detectWhetherClosedDiodesStopAllFlowAt3DInterface (CircuitData.cxx:
@@ -224,6 +253,7 @@ int solve(crimson_netlist* nl) {
 // component; flow can cross the interface if one of them has an end with no
 // other component attached (a sink) that is not the interface node.
 bool detect_flow_permitted(const crimson_netlist* nl) {
+    if (nl->iface_comp < 0) return true;  // a loop-closing circuit has no 3D interface
     std::vector<int> stack{nl->iface_comp};
     std::vector<char> seen((size_t)nl->nc, 0);
     while (!stack.empty()) {
@@ -260,13 +290,26 @@ int crimson_netlist_create(crimson_netlist** out, int ncomp, const int* kind, co
                            const double* unstressed_volume, int nnodes, const double* initial_pressure, int npres,
                            const int* pres_node, const double* pres_value, int nflow, const int* flow_comp,
                            const int* flow_kind, const double* flow_value, int interface_node) {
+    if (interface_node != 1) return fail("netlist: the 3D interface node must be node 1");
+    return crimson_netlist_create_member(out, ncomp, kind, start_node, end_node, value, initial_volume,
+                                         unstressed_volume, nnodes, initial_pressure, npres, pres_node, pres_value,
+                                         nflow, flow_comp, flow_kind, flow_value, interface_node, 0, nullptr);
+}
+
+int crimson_netlist_create_member(crimson_netlist** out, int ncomp, const int* kind, const int* start_node,
+                                  const int* end_node, const double* value, const double* initial_volume,
+                                  const double* unstressed_volume, int nnodes, const double* initial_pressure,
+                                  int npres, const int* pres_node, const double* pres_value, int nflow,
+                                  const int* flow_comp, const int* flow_kind, const double* flow_value,
+                                  int interface_node, int nshared, const int* shared_nodes) {
     if (!out) return CRIMSON_ERR_ARG;
     *out = nullptr;
     if (ncomp < 1 || nnodes < 1 || !kind || !start_node || !end_node || !value || !initial_pressure)
         return fail("netlist: need at least one component and one node");
-    if (npres < 0 || nflow < 1 || (npres > 0 && (!pres_node || !pres_value)) || !flow_comp || !flow_kind ||
-        !flow_value)
+    if (npres < 0 || nflow < 0 || (npres > 0 && (!pres_node || !pres_value)) ||
+        (nflow > 0 && (!flow_comp || !flow_kind || !flow_value)))
         return fail("netlist: bad prescribed pressure / flow lists");
+    if (nshared < 0 || (nshared > 0 && !shared_nodes)) return fail("netlist: bad shared-node list");
     crimson_netlist* nl = new (std::nothrow) crimson_netlist;
     if (!nl) return CRIMSON_ERR_OOM;
     auto bad = [&](const char* msg) {
@@ -331,16 +374,36 @@ int crimson_netlist_create(crimson_netlist** out, int ncomp, const int* kind, co
     std::sort(nl->pf_comps.begin(), nl->pf_comps.end());
     // initialiseNodeAndComponentAtInterface (CircuitData.cxx:130-262); the
     // coupling coefficients are read from unknown 0, the pressure of node 1
-    // (NetlistCircuit.cxx:1770-1790), so the interface node is node 1.
-    if (n3d != 1) return bad("netlist: exactly one component must carry the 3D interface flow");
-    if (interface_node != 1) return bad("netlist: the 3D interface node must be node 1");
-    nl->iface_node = interface_node;
-    const NetlistComp& ic = nl->comp[nl->iface_comp];
-    if (ic.start != interface_node && ic.end != interface_node)
-        return bad("netlist: the 3D-flow component does not touch the interface node");
-    if (uses[interface_node - 1] != 1) return bad("netlist: the interface node must belong to exactly one component");
-    if (nl->node[interface_node - 1].fixed) return bad("netlist: the interface node cannot have a prescribed pressure");
-    nl->sign = ic.start == interface_node ? 1.0 : -1.0;
+    // (NetlistCircuit.cxx:1770-1790), so the interface node is node 1.  A
+    // loop-closing circuit (interface_node 0) has none.
+    if (interface_node == 0) {
+        if (n3d != 0) return bad("netlist: a circuit without a 3D interface cannot carry the 3D flow");
+        nl->iface_node = 0;
+        nl->iface_comp = -1;
+    } else {
+        if (n3d != 1) return bad("netlist: exactly one component must carry the 3D interface flow");
+        if (interface_node != 1) return bad("netlist: the 3D interface node must be node 1");
+        nl->iface_node = interface_node;
+        const NetlistComp& ic = nl->comp[nl->iface_comp];
+        if (ic.start != interface_node && ic.end != interface_node)
+            return bad("netlist: the 3D-flow component does not touch the interface node");
+        if (uses[interface_node - 1] != 1)
+            return bad("netlist: the interface node must belong to exactly one component");
+        if (nl->node[interface_node - 1].fixed)
+            return bad("netlist: the interface node cannot have a prescribed pressure");
+        nl->sign = ic.start == interface_node ? 1.0 : -1.0;
+    }
+    // nodes shared with another circuit of a closed loop: their Kirchhoff
+    // equation is the loop's (createListOfNodesWithMultipleIncidentCurrents,
+    // NetlistCircuit.cxx:880-920)
+    for (int k = 0; k < nshared; ++k) {
+        const int nd = shared_nodes[k];
+        if (nd < 1 || nd > nnodes || nd == interface_node) return bad("netlist: bad shared node");
+        nl->connect_nodes.push_back(nd);
+    }
+    std::sort(nl->connect_nodes.begin(), nl->connect_nodes.end());
+    if (std::adjacent_find(nl->connect_nodes.begin(), nl->connect_nodes.end()) != nl->connect_nodes.end())
+        return bad("netlist: a shared node is listed twice");
     // history pressures at capacitor ends, history flows of inductors
     // (NetlistCircuit.cxx:930-979), Kirchhoff nodes (876-917)
     for (const NetlistComp& c : nl->comp)
@@ -370,10 +433,14 @@ int crimson_netlist_create(crimson_netlist** out, int ncomp, const int* kind, co
             if (nl->comp[j].kind == CRIMSON_NETLIST_PRESSURE_CHAMBER) ++nl->nchamber;
         }
     for (int i = 0; i < nnodes; ++i)
-        if (uses[i] > 1) nl->kirch_nodes.push_back(i + 1);
+        if (uses[i] > 1 && !std::binary_search(nl->connect_nodes.begin(), nl->connect_nodes.end(), i + 1))
+            nl->kirch_nodes.push_back(i + 1);
     const int nv = (int)nl->vol_comps.size();
-    if (nl->nchamber + (int)(nl->kirch_nodes.size() + nl->pp_nodes.size() + nl->pf_comps.size()) != nnodes + nv)
-        return bad("netlist: malformed circuit (the system is not square)");
+    if (nl->nchamber + (int)(nl->kirch_nodes.size() + nl->pp_nodes.size() + nl->pf_comps.size()) !=
+        nnodes + nv - (int)nl->connect_nodes.size())
+        return bad(nl->connect_nodes.empty() ? "netlist: malformed circuit (the system is not square)"
+                                             : "netlist: malformed circuit (its rows and its shared nodes do not "
+                                               "make up its unknowns)");
     nl->n = nnodes + (int)nl->hist_nodes.size() + ncomp + (int)nl->hist_comps.size() + 2 * nv;
     nl->A.assign((size_t)nl->n * nl->n, 0.0);
     nl->Ainv.assign((size_t)nl->n * nl->n, 0.0);
@@ -418,6 +485,8 @@ int crimson_netlist_implicit_coefficients(crimson_netlist* nl, double alfi_delt,
     if (!nl->flow_permitted)
         return fail("netlist: no flow across the 3D interface (Dirichlet design: no implicit coefficients)",
                     CRIMSON_ERR_STATE);
+    if (nl->iface_comp < 0 || !nl->connect_nodes.empty())
+        return fail("netlist: no 3D interface, or a member of a closed loop (use the loop)", CRIMSON_ERR_STATE);
     build_system(nl, alfi_delt);
     assemble_rhs(nl);
     const int st = solve(nl);
@@ -433,22 +502,13 @@ int crimson_netlist_implicit_coefficients(crimson_netlist* nl, double alfi_delt,
 // interface flow (Neumann design) or the 3D surface pressure (Dirichlet
 // design) and take the nodal pressures, component flows and volumes.
 static int netlist_solve_update(crimson_netlist* nl, double delt) {
+    if (!nl->connect_nodes.empty())
+        return fail("netlist: a member of a closed loop is solved through its loop", CRIMSON_ERR_STATE);
     build_system(nl, delt);
     assemble_rhs(nl);
     const int st = solve(nl);
     if (st != CRIMSON_OK) return st;
-    for (int i = 0; i < nl->np; ++i) nl->node[i].p = nl->x[i];
-    const int cf = col_flow(nl);
-    for (int j = 0; j < nl->nc; ++j) nl->comp[j].flow = nl->x[(size_t)cf + j];
-    // volumes; a chamber passes E (V - V_unstressed) to its start node
-    // (giveComponentsTheirVolumesFromSolutionVector, NetlistCircuit.cxx:
-    // 1636-1660; CircuitComponent.cxx:188-209)
-    const int cv = col_vol(nl);
-    for (int j : nl->vol_comps) {
-        NetlistComp& c = nl->comp[j];
-        c.volume = nl->x[(size_t)cv + nl->vol_ord[j]];
-        if (c.kind == CRIMSON_NETLIST_PRESSURE_CHAMBER) nl->node[(size_t)c.start - 1].p = (c.volume - c.unstressed) * c.value;
-    }
+    take_solution(nl, nl->x.data());
     return CRIMSON_OK;
 }
 
@@ -589,6 +649,176 @@ int crimson_netlist_state(crimson_netlist* nl, double* buf, int set) {
         buf[2 * np + 5 * nc] = nl->last_q;
         buf[2 * np + 5 * nc + 1] = nl->last_p3d;
     }
+    return CRIMSON_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Closed loops: ClosedLoopDownstreamSubsection (ClosedLoopDownstreamSubsection
+// .cxx:101-500, 609-940).  The upstream circuits' row blocks (each without the
+// Kirchhoff rows of its shared nodes) and the loop-closing circuit's block are
+// tiled along the diagonal in that order, then one Kirchhoff row per shared
+// node of the loop-closing circuit (ascending: the flows of the connected
+// upstream circuits at their mapped nodes, in input order, then its own) and
+// one pressure-equality row per connection (file order: +1 at the upstream
+// node, -1 at the downstream node).  One dense solve gives every member's
+// unknowns; the implicit coefficients of upstream circuit k are read from
+// the inverse at (its node 1, its 3D-flow row).
+// ---------------------------------------------------------------------------
+
+namespace {
+
+void loop_build(crimson_netlist_loop* L, double alfi_delt) {
+    std::fill(L->A.begin(), L->A.end(), 0.0);
+    std::fill(L->b.begin(), L->b.end(), 0.0);
+    const size_t ld = (size_t)L->n;
+    const int nm = (int)L->member.size();
+    for (int m = 0; m < nm; ++m) {
+        build_rows(L->member[m], alfi_delt, L->A.data(), ld, L->row0[m], L->col0[m]);
+        rhs_rows(L->member[m], L->b.data(), L->row0[m]);
+    }
+    int row = L->row0[nm - 1] + L->member[nm - 1]->n - (int)L->member[nm - 1]->connect_nodes.size();
+    auto kirchhoff_part = [&](int m, int node) {
+        const crimson_netlist* nl = L->member[m];
+        const int cf = L->col0[m] + nl->np + (int)nl->hist_nodes.size();
+        for (int j = 0; j < nl->nc; ++j) {
+            if (nl->comp[j].end == node) L->A[(size_t)row * ld + cf + j] = 1.0;
+            if (nl->comp[j].start == node) L->A[(size_t)row * ld + cf + j] = -1.0;
+        }
+    };
+    // appendKirchoffLawsAtInterfacesBetweenCircuits (609-715)
+    for (int d : L->down_nodes) {
+        for (int k = 0; k < L->nup; ++k)
+            for (size_t c = 0; c < L->conn_down.size(); ++c)
+                if (L->conn_down[c] == d && L->conn_up[c] == k) {
+                    kirchhoff_part(k, L->conn_node[c]);
+                    break;
+                }
+        kirchhoff_part(nm - 1, d);
+        ++row;
+    }
+    // enforcePressureEqualityBetweenDuplicatedNodes (770-840)
+    for (size_t c = 0; c < L->conn_down.size(); ++c, ++row) {
+        L->A[(size_t)row * ld + L->col0[L->conn_up[c]] + L->conn_node[c] - 1] = 1.0;
+        L->A[(size_t)row * ld + L->col0[nm - 1] + L->conn_down[c] - 1] = -1.0;
+    }
+}
+
+int loop_solve(crimson_netlist_loop* L, double alfi_delt) {
+    loop_build(L, alfi_delt);
+    return gj_solve(L->n, L->A, L->Ainv, L->b, L->x);
+}
+
+}  // namespace
+
+int crimson_netlist_loop_create(crimson_netlist_loop** out, int nupstream, crimson_netlist* const* upstream,
+                                crimson_netlist* downstream, int nconn, const int* conn_down_node,
+                                const int* conn_upstream, const int* conn_upstream_node) {
+    if (!out) return CRIMSON_ERR_ARG;
+    *out = nullptr;
+    if (nupstream < 1 || !upstream || !downstream || nconn < 1 || !conn_down_node || !conn_upstream ||
+        !conn_upstream_node)
+        return fail("netlist loop: need upstream circuits, a loop-closing circuit and connections");
+    if (downstream->iface_comp >= 0) return fail("netlist loop: the loop-closing circuit has a 3D interface");
+    std::vector<std::vector<int>> up_nodes((size_t)nupstream);
+    std::vector<int> down_nodes;
+    for (int c = 0; c < nconn; ++c) {
+        const int k = conn_upstream[c], u = conn_upstream_node[c], d = conn_down_node[c];
+        if (k < 0 || k >= nupstream || !upstream[k]) return fail("netlist loop: bad upstream circuit index");
+        if (upstream[k]->iface_comp < 0) return fail("netlist loop: an upstream circuit has no 3D interface");
+        if (u < 1 || u > upstream[k]->np || d < 1 || d > downstream->np)
+            return fail("netlist loop: connection node out of range");
+        up_nodes[k].push_back(u);
+        down_nodes.push_back(d);
+        for (int e = 0; e < c; ++e)
+            if (conn_upstream[e] == k && (conn_upstream_node[e] == u || conn_down_node[e] == d))
+                return fail("netlist loop: a connection is listed twice");
+    }
+    for (int k = 0; k < nupstream; ++k) {
+        if (up_nodes[k].empty()) return fail("netlist loop: an upstream circuit without a connection");
+        std::sort(up_nodes[k].begin(), up_nodes[k].end());
+        if (up_nodes[k] != upstream[k]->connect_nodes)
+            return fail("netlist loop: an upstream circuit's shared nodes are not its connections");
+        for (int e = 0; e < k; ++e)
+            if (upstream[e] == upstream[k]) return fail("netlist loop: a circuit is listed twice");
+    }
+    std::sort(down_nodes.begin(), down_nodes.end());
+    down_nodes.erase(std::unique(down_nodes.begin(), down_nodes.end()), down_nodes.end());
+    if (down_nodes != downstream->connect_nodes)
+        return fail("netlist loop: the loop-closing circuit's shared nodes are not its connections");
+    crimson_netlist_loop* L = new (std::nothrow) crimson_netlist_loop;
+    if (!L) return CRIMSON_ERR_OOM;
+    L->nup = nupstream;
+    L->member.assign(upstream, upstream + nupstream);
+    L->member.push_back(downstream);
+    L->conn_down.assign(conn_down_node, conn_down_node + nconn);
+    L->conn_up.assign(conn_upstream, conn_upstream + nconn);
+    L->conn_node.assign(conn_upstream_node, conn_upstream_node + nconn);
+    L->down_nodes = down_nodes;
+    int r = 0, c = 0;
+    for (crimson_netlist* nl : L->member) {
+        L->row0.push_back(r);
+        L->col0.push_back(c);
+        r += nl->n - (int)nl->connect_nodes.size();
+        c += nl->n;
+    }
+    L->n = c;
+    if (r + (int)down_nodes.size() + nconn != c) {
+        delete L;
+        return fail("netlist loop: malformed loop (the system is not square)");
+    }
+    L->A.assign((size_t)c * c, 0.0);
+    L->Ainv.assign((size_t)c * c, 0.0);
+    L->b.assign((size_t)c, 0.0);
+    L->x.assign((size_t)c, 0.0);
+    *out = L;
+    return CRIMSON_OK;
+}
+
+void crimson_netlist_loop_free(crimson_netlist_loop* loop) { delete loop; }
+
+// getImplicitCoefficients (ClosedLoopDownstreamSubsection.cxx:852-888)
+int crimson_netlist_loop_implicit_coefficients(crimson_netlist_loop* L, double alfi_delt, double* dp_dq,
+                                               double* hop) {
+    if (!L || !dp_dq || !hop || !(alfi_delt > 0.0)) return CRIMSON_ERR_ARG;
+    const int st = loop_solve(L, alfi_delt);
+    if (st != CRIMSON_OK) return st;
+    for (int k = 0; k < L->nup; ++k) {
+        const crimson_netlist* nl = L->member[k];
+        if (!nl->flow_permitted) {  // Dirichlet design: the surface is not coupled
+            dp_dq[k] = hop[k] = std::numeric_limits<double>::quiet_NaN();
+            continue;
+        }
+        const size_t row = (size_t)L->col0[k], col = (size_t)(L->row0[k] + iface_row(nl));
+        const double g = L->Ainv[row * L->n + col];
+        dp_dq[k] = nl->sign * g;
+        hop[k] = L->x[row] - g * L->b[col];
+    }
+    return CRIMSON_OK;
+}
+
+// updateLPN of the loop's circuits (NetlistBoundaryCircuitWhenDownstream
+// CircuitsExist.cxx:27-52): one solve with Delt and, per upstream circuit,
+// its interface flow (Neumann design) or its 3D surface pressure (Dirichlet
+// design); every member takes its segment of the solution.
+int crimson_netlist_loop_update(crimson_netlist_loop* L, double delt, const double* interface_flow,
+                                const double* interface_pressure) {
+    if (!L || !(delt > 0.0) || !interface_flow || !interface_pressure) return CRIMSON_ERR_ARG;
+    for (int k = 0; k < L->nup; ++k) {
+        crimson_netlist* nl = L->member[k];
+        const double v = nl->flow_permitted ? interface_flow[k] : interface_pressure[k];
+        if (!std::isfinite(v)) return CRIMSON_ERR_ARG;
+        if (nl->flow_permitted) nl->last_q = v;
+        else nl->last_p3d = v;
+    }
+    const int st = loop_solve(L, delt);
+    if (st != CRIMSON_OK) return st;
+    for (size_t m = 0; m < L->member.size(); ++m) take_solution(L->member[m], L->x.data() + L->col0[m]);
+    return CRIMSON_OK;
+}
+
+int crimson_netlist_loop_finalize_step(crimson_netlist_loop* L) {
+    if (!L) return CRIMSON_ERR_ARG;
+    for (crimson_netlist* nl : L->member) crimson_netlist_finalize_step(nl);
     return CRIMSON_OK;
 }
 

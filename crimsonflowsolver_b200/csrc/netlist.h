@@ -56,9 +56,22 @@ struct crimson_netlist {
     std::vector<std::vector<int>> nb_start, nb_end;  // neighbouring components at each end
     int n = 0;                                       // system size
     std::vector<double> A, Ainv, b, x;
+    std::vector<int> connect_nodes;  // ascending nodes shared with another circuit of a closed loop
     double last_q = 0.0;    // interface flow of the last update (the flow the reference reads from the 3D side)
     double last_p3d = 0.0;  // 3D surface pressure of the last Dirichlet-design update
     bool flow_permitted = true;  // false: closed diodes block the interface (Dirichlet design)
+};
+
+// A closed loop (ClosedLoopDownstreamSubsection): its members and the dense
+// system they share.
+struct crimson_netlist_loop {
+    std::vector<crimson_netlist*> member;  // upstream circuits in input order, then the loop-closing circuit
+    int nup = 0;
+    std::vector<int> conn_down, conn_up, conn_node;  // connections in file order
+    std::vector<int> down_nodes;                     // ascending distinct downstream shared nodes
+    std::vector<int> row0, col0;                     // first row / column of each member's block
+    int n = 0;
+    std::vector<double> A, Ainv, b, x;
 };
 
 namespace crimson {

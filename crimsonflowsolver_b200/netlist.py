@@ -5,7 +5,9 @@ description; the calls mirror NetlistCircuit (flowsolver/src/
 NetlistCircuit.cxx): implicit coefficients at the start of a step, update
 with the end-of-step interface flow -- or, while closed diodes block the
 interface (the Dirichlet design), with the 3D surface pressure --
-finalisation (histories and diode switching).
+finalisation (histories and diode switching).  :class:`NetlistLoop` solves
+a closed loop -- upstream circuits coupled to 3D surfaces joined through a
+loop-closing circuit (ClosedLoopDownstreamSubsection.cxx) -- as one system.
 """
 from __future__ import annotations
 
@@ -14,7 +16,7 @@ import ctypes
 import numpy as np
 
 from . import _native as N
-from .problem import NetlistBC
+from .problem import NetlistBC, NetlistLoopBC
 
 KINDS = {"r": 0, "c": 1, "l": 2, "i": 2, "d": 3, "t": 4, "v": 5}
 # controllable parameters (crimson_netlist_set_parameter)
@@ -35,15 +37,25 @@ class Netlist:
         vu = np.array([spec.volumes.get(j + 1, (0.0, 0.0))[1] for j in range(len(comps))], dtype=np.float64)
         pn = np.array(sorted(spec.prescribed_pressures), dtype=np.int32)
         pv = np.array([spec.prescribed_pressures[k] for k in pn], dtype=np.float64)
-        fc = [spec.interface_component] + sorted(spec.prescribed_flows)
-        fk = [1] + [0] * len(spec.prescribed_flows)
-        fv = [0.0] + [spec.prescribed_flows[k] for k in sorted(spec.prescribed_flows)]
+        iface = int(spec.interface_component)
+        fixed = sorted(spec.prescribed_flows)
+        fc = ([iface] if iface else []) + fixed
+        fk = ([1] if iface else []) + [0] * len(fixed)
+        fv = ([0.0] if iface else []) + [spec.prescribed_flows[k] for k in fixed]
         fc, fk, fv = (np.array(fc, dtype=np.int32), np.array(fk, dtype=np.int32), np.array(fv, dtype=np.float64))
         self.ncomp, self.nnodes = len(comps), nn
         h = ctypes.c_void_p()
-        N.check(N.lib().crimson_netlist_create(ctypes.byref(h), len(comps), N.ip(kind), N.ip(st), N.ip(en), N.dp(val),
-                                               N.dp(v0), N.dp(vu), nn, N.dp(p0), len(pn), N.ip(pn), N.dp(pv), len(fc),
-                                               N.ip(fc), N.ip(fk), N.dp(fv), 1), "crimson_netlist_create")
+        if spec.shared_nodes or not iface:
+            sh = np.array(sorted(spec.shared_nodes), dtype=np.int32)
+            N.check(N.lib().crimson_netlist_create_member(
+                ctypes.byref(h), len(comps), N.ip(kind), N.ip(st), N.ip(en), N.dp(val), N.dp(v0), N.dp(vu), nn,
+                N.dp(p0), len(pn), N.ip(pn), N.dp(pv), len(fc), N.ip(fc), N.ip(fk), N.dp(fv), 1 if iface else 0,
+                len(sh), N.ip(sh)), "crimson_netlist_create_member")
+        else:
+            N.check(N.lib().crimson_netlist_create(ctypes.byref(h), len(comps), N.ip(kind), N.ip(st), N.ip(en),
+                                                   N.dp(val), N.dp(v0), N.dp(vu), nn, N.dp(p0), len(pn), N.ip(pn),
+                                                   N.dp(pv), len(fc), N.ip(fc), N.ip(fk), N.dp(fv), 1),
+                    "crimson_netlist_create")
         self.h = h
 
     def flow_permitted(self) -> bool:
@@ -113,6 +125,67 @@ class Netlist:
         if getattr(self, "h", None):
             N.lib().crimson_netlist_free(self.h)
             self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class NetlistLoop:
+    """A closed loop (:class:`NetlistLoopBC`) on crimson_netlist_loop_*: the
+    member circuits (``upstream`` in input order, ``downstream``) are
+    :class:`Netlist` objects the loop owns."""
+
+    def __init__(self, spec: NetlistLoopBC):
+        self.spec = spec
+        self.upstream = [Netlist(c) for c in spec.upstream]
+        self.downstream = Netlist(spec.downstream)
+        cd = np.array([c[0] for c in spec.connections], dtype=np.int32)
+        ck = np.array([spec.upstream_index(c[1]) for c in spec.connections], dtype=np.int32)
+        cu = np.array([c[2] for c in spec.connections], dtype=np.int32)
+        ups = (ctypes.c_void_p * len(self.upstream))(*[m.h.value for m in self.upstream])
+        h = ctypes.c_void_p()
+        N.check(N.lib().crimson_netlist_loop_create(ctypes.byref(h), len(self.upstream), ups, self.downstream.h,
+                                                    len(cd), N.ip(cd), N.ip(ck), N.ip(cu)),
+                "crimson_netlist_loop_create")
+        self.h = h
+
+    @property
+    def members(self):
+        return self.upstream + [self.downstream]
+
+    def flow_permitted(self):
+        """Per upstream circuit: whether flow can cross its 3D interface."""
+        return [m.flow_permitted() for m in self.upstream]
+
+    def implicit_coefficients(self, alfi_delt: float):
+        """Per upstream circuit (dp_dq, hop); NaN in the Dirichlet design."""
+        n = len(self.upstream)
+        a, b = np.zeros(n), np.zeros(n)
+        N.check(N.lib().crimson_netlist_loop_implicit_coefficients(self.h, alfi_delt, N.dp(a), N.dp(b)),
+                "crimson_netlist_loop_implicit_coefficients")
+        return list(zip(a.tolist(), b.tolist()))
+
+    def update(self, delt: float, flows, pressures=None) -> None:
+        """updateLPN of every member: upstream circuit k takes flows[k] (its
+        end-of-step interface flow) or, in the Dirichlet design,
+        pressures[k] (its 3D surface's mean pressure)."""
+        n = len(self.upstream)
+        q = np.ascontiguousarray(flows, dtype=np.float64).reshape(n)
+        p = np.zeros(n) if pressures is None else np.ascontiguousarray(pressures, dtype=np.float64).reshape(n)
+        N.check(N.lib().crimson_netlist_loop_update(self.h, delt, N.dp(q), N.dp(p)), "crimson_netlist_loop_update")
+
+    def finalize_step(self) -> None:
+        N.check(N.lib().crimson_netlist_loop_finalize_step(self.h), "crimson_netlist_loop_finalize_step")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            N.lib().crimson_netlist_loop_free(self.h)
+            self.h = None
+        for m in getattr(self, "upstream", []) + ([self.downstream] if hasattr(self, "downstream") else []):
+            m.close()
 
     def __del__(self):
         try:

@@ -20,6 +20,11 @@ Two formats, as the reference reads them:
   pressure takes the node's initialPressure); ``control`` elements (type,
   source) on components and nodes.
 
+* ``netlist_closed_loop_downstream.xml`` (NetlistDownstreamXmlReader,
+  NetlistXmlReader.cxx:470-640): loop-closing circuits in the same XML form,
+  whose nodes carry ``upstreamConnectivity/connection`` elements
+  (upstreamCircuitSurfaceIndex, connectsToUpstreamNode).
+
 Each circuit comes back as a dict; :func:`to_netlistbc` turns one into a
 :class:`NetlistBC` for a coupled surface, binding its customPython controls
 to the controllers the caller supplies, and raises for what the library
@@ -32,7 +37,7 @@ import os
 import xml.etree.ElementTree as ET
 from typing import Dict, List, Optional
 
-from .problem import NetlistBC
+from .problem import NetlistBC, NetlistLoopBC
 
 _DAT_KINDS = {"r": "r", "c": "c", "i": "l", "d": "d", "t": "t", "v": "v"}
 _XML_KINDS = {"resistor": "r", "capacitor": "c", "inductor": "l", "diode": "d", "volumetracking": "t",
@@ -109,7 +114,7 @@ def parse_netlist_xml(text: str) -> List[Dict]:
     for circ in root.findall("circuit"):
         c: Dict = {"components": [], "volumes": {}, "prescribed_pressures": {}, "pressure_types": {},
                    "prescribed_flows": {}, "flow_types": {}, "initial_pressures": {}, "controls": 0,
-                   "interface_node": None, "control_specs": []}
+                   "interface_node": None, "control_specs": [], "connections": []}
         for j, comp in enumerate(circ.find("components").findall("component")):
             kind = _text(comp, "type").lower()
             if kind not in _XML_KINDS:
@@ -144,6 +149,9 @@ def parse_netlist_xml(text: str) -> List[Dict]:
             for ctl in node.findall("control"):
                 c["control_specs"].append(("node", idx, _text(ctl, "type", ""), _text(ctl, "source", "")))
                 c["controls"] += 1
+            for conn in node.findall("upstreamConnectivity/connection"):
+                c["connections"].append((idx, int(_text(conn, "upstreamCircuitSurfaceIndex")),
+                                         int(_text(conn, "connectsToUpstreamNode"))))
         out.append(c)
     return out
 
@@ -166,7 +174,7 @@ _LV = ("l", "leftventricularelastance")
 
 
 def to_netlistbc(circuit: Dict, srfid: int, ignore_controls: bool = False, controllers=None,
-                 data_dir: Optional[str] = None) -> NetlistBC:
+                 data_dir: Optional[str] = None, shared_nodes=(), loop_closing: bool = False) -> NetlistBC:
     """One parsed circuit as the outlet of surface ``srfid``.  A circuit's
     customPython controls (component parameter, unstressed volume, node
     pressure) take their controller from ``controllers``, a mapping from the
@@ -178,7 +186,10 @@ def to_netlistbc(circuit: Dict, srfid: int, ignore_controls: bool = False, contr
     values; bleed and left-ventricular elastance controls take the built-in
     :class:`~crimsonflowsolver_b200.controllers.BleedController` and
     :class:`~crimsonflowsolver_b200.controllers.LeftVentricularElastanceController`
-    (the latter sets its chamber's elastance to the starting value)."""
+    (the latter sets its chamber's elastance to the starting value).
+    ``shared_nodes`` and ``loop_closing`` describe a member of a closed loop:
+    the nodes it shares with the loop, and whether it is the loop-closing
+    circuit (no 3D interface)."""
     from .controllers import BleedController, LeftVentricularElastanceController, PeriodicTableController
 
     bound = []
@@ -209,13 +220,55 @@ def to_netlistbc(circuit: Dict, srfid: int, ignore_controls: bool = False, contr
     if circuit.get("interface_node") not in (None, 1):
         raise NotImplementedError("the 3D interface node must be node 1")
     iface = [j for j, t in circuit["flow_types"].items() if t == "t"]
-    if len(iface) != 1:
+    if loop_closing:
+        if iface:
+            raise ValueError("a loop-closing circuit has no 3D interface flow")
+        iface = [0]
+    elif len(iface) != 1:
         raise ValueError("exactly one component must carry the 3D interface flow")
     fixed_flows = {j: v for j, v in circuit["prescribed_flows"].items() if circuit["flow_types"][j] == "f"}
     return NetlistBC(srfid=srfid, components=components,
                      prescribed_pressures=dict(circuit["prescribed_pressures"]), prescribed_flows=fixed_flows,
                      interface_component=iface[0], initial_pressures=dict(circuit["initial_pressures"]),
-                     volumes=dict(circuit["volumes"]), controllers=bound)
+                     volumes=dict(circuit["volumes"]), controllers=bound,
+                     shared_nodes=tuple(sorted(set(int(d) for d in shared_nodes))))
+
+
+def closed_loops(circuits: List[Dict], srfids: List[int], downstream: List[Dict], ignore_controls: bool = False,
+                 controllers=None, data_dir: Optional[str] = None):
+    """The netlist boundary circuits of surfaces ``srfids`` (parsed
+    ``circuits`` in the same order) and the parsed loop-closing circuits
+    ``downstream``: returns (the circuits that connect to no loop-closing
+    circuit, as :class:`NetlistBC`; one :class:`NetlistLoopBC` per
+    loop-closing circuit, its upstream circuits in input order).  A circuit
+    connected to more than one loop-closing circuit is rejected, as the
+    reference asserts (NetlistBoundaryCircuitWhenDownstreamCircuitsExist.cxx:
+    33)."""
+    if len(circuits) != len(srfids):
+        raise ValueError(f"{len(circuits)} circuits, {len(srfids)} surfaces given")
+    owner: Dict[int, int] = {}
+    for li, d in enumerate(downstream):
+        if not d["connections"]:
+            raise ValueError("a loop-closing circuit without connections")
+        for _, srf, _ in d["connections"]:
+            if srf not in srfids:
+                raise ValueError(f"a loop-closing circuit connects to surface {srf}, which has no netlist circuit")
+            if owner.setdefault(srf, li) != li:
+                raise NotImplementedError(f"surface {srf} connects to more than one loop-closing circuit")
+    kw = dict(ignore_controls=ignore_controls, controllers=controllers, data_dir=data_dir)
+    standalone, members = [], {}
+    for c, srf in zip(circuits, srfids):
+        if srf not in owner:
+            standalone.append(to_netlistbc(c, srf, **kw))
+            continue
+        conns = downstream[owner[srf]]["connections"]
+        members[srf] = to_netlistbc(c, srf, shared_nodes=[u for _, s2, u in conns if s2 == srf], **kw)
+    loops = []
+    for d in downstream:
+        ups = [members[s] for s in srfids if s in members and any(s == s2 for _, s2, _ in d["connections"])]
+        down = to_netlistbc(d, 0, shared_nodes=[n for n, _, _ in d["connections"]], loop_closing=True, **kw)
+        loops.append(NetlistLoopBC(upstream=ups, downstream=down, connections=list(d["connections"])))
+    return standalone, loops
 
 
 def read_netlists(path: str, srfids: List[int], controllers=None) -> List[NetlistBC]:
@@ -228,3 +281,25 @@ def read_netlists(path: str, srfids: List[int], controllers=None) -> List[Netlis
         raise ValueError(f"{len(circuits)} circuits in {path}, {len(srfids)} surfaces given")
     return [to_netlistbc(c, s, controllers=controllers, data_dir=os.path.dirname(os.path.abspath(path)))
             for c, s in zip(circuits, srfids)]
+
+
+def netlist_surfaces_of_solver_inp(text: str) -> List[int]:
+    """The "List of Netlist LPN Surfaces" of a solver.inp: the surface each
+    netlist circuit couples, in input order."""
+    for line in text.splitlines():
+        key, _, val = line.partition(":")
+        if key.strip().lower() == "list of netlist lpn surfaces":
+            return [int(t) for t in val.split("#")[0].split()]
+    return []
+
+
+def read_closed_loops(surfaces_path: str, downstream_path: str, srfids: List[int], controllers=None):
+    """Read a netlist_surfaces file and a netlist_closed_loop_downstream.xml:
+    (standalone circuits, loops) as :func:`closed_loops` returns them."""
+    with open(surfaces_path) as f:
+        text = f.read()
+    circuits = parse_netlist_xml(text) if surfaces_path.endswith(".xml") else parse_netlist_dat(text)
+    with open(downstream_path) as f:
+        downstream = parse_netlist_xml(f.read())
+    return closed_loops(circuits, srfids, downstream, controllers=controllers,
+                        data_dir=os.path.dirname(os.path.abspath(surfaces_path)))

@@ -75,6 +75,9 @@ class NetlistBC:
     sets, after every step, the component value ("component"), a chamber's
     unstressed volume ("unstressed_volume"), a node's pressure ("pressure")
     or a component's fixed flow ("flow") of item ``index`` (1-based).
+    shared_nodes: for a member of a closed loop (:class:`NetlistLoopBC`), the
+    nodes it shares with the loop's other circuits; interface_component 0
+    marks the loop-closing circuit, which has no 3D interface.
     """
     srfid: int
     components: List[Tuple[str, int, int, float]]
@@ -84,6 +87,7 @@ class NetlistBC:
     initial_pressures: Dict[int, float] = field(default_factory=dict)
     volumes: Dict[int, Tuple[float, float]] = field(default_factory=dict)
     controllers: List[Tuple[str, int, object]] = field(default_factory=list)
+    shared_nodes: Tuple[int, ...] = ()
 
     @property
     def nnodes(self) -> int:
@@ -121,6 +125,8 @@ class FlowParams:
     # netlist outlet circuits, coupled after the RCR surfaces (not reference
     # settings names: the reference reads them from its netlist XML input)
     netlists: List[NetlistBC] = field(default_factory=list)
+    # closed loops of netlist circuits (NetlistLoopBC)
+    loops: list = field(default_factory=list)
     # NS solve arithmetic: "fp64" (memLS's), "mixed" (FP32 matrices in the
     # inner Krylov matvecs, FP64 outer vectors and iterative refinement of at
     # most max_refine sweeps, until the FP64 defect |R - A x| / |R| is at
@@ -137,8 +143,9 @@ class FlowParams:
     explicit_schur: int = 0
 
     def outlets(self) -> list:
-        """Coupled outlet surfaces in srflist order: the RCRs, then the netlists."""
-        return list(self.rcr) + list(self.netlists)
+        """Coupled outlet surfaces in srflist order: the RCRs, the netlists,
+        then the upstream circuits of each closed loop."""
+        return list(self.rcr) + list(self.netlists) + [c for lp in self.loops for c in lp.upstream]
 
     @property
     def almi(self) -> float:
@@ -155,3 +162,21 @@ class FlowParams:
     @property
     def Dtgl(self) -> float:
         return 1.0 / self.Delt
+
+
+@dataclass
+class NetlistLoopBC:
+    """A closed loop of netlist circuits (flowsolver/src/
+    ClosedLoopDownstreamSubsection.cxx): the upstream circuits coupled to 3D
+    surfaces (input order), one loop-closing circuit (interface_component 0)
+    and the connections (downstream node, upstream surface id, upstream
+    node) in the order of the downstream input."""
+    upstream: List[NetlistBC]
+    downstream: NetlistBC
+    connections: List[Tuple[int, int, int]]
+
+    def upstream_index(self, srfid: int) -> int:
+        for k, c in enumerate(self.upstream):
+            if c.srfid == srfid:
+                return k
+        raise ValueError(f"surface {srfid} is not an upstream circuit of the loop")

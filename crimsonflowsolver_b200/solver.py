@@ -326,20 +326,27 @@ class FlowSolver:
             nn, vv = neumann_face(mesh, r.srfid)
             self.memls.bc_create(2 + k, nn, 3, 1, vv)
         L = N.lib()
-        self.netlists = []
+        self.netlists, self.loops = [], []
         if nc:
             # RCR parameters per surface (zeros on netlist surfaces, whose
             # coefficients come from the circuit)
             arr = lambda f: np.ascontiguousarray(np.array([getattr(r, f, 0.0) for r in outlets], dtype=np.float64))
             N.check(L.crimson_set_rcr(self.elm.h, nc, N.dp(arr("Rp")), N.dp(arr("C")), N.dp(arr("Rd")),
                                       N.dp(arr("Pd"))), "crimson_set_rcr")
-            from .netlist import Netlist
+            from .netlist import Netlist, NetlistLoop
 
+            in_loop = {id(c) for lp in P.loops for c in lp.upstream}
             for k, r in enumerate(outlets):
-                if hasattr(r, "components"):
+                if hasattr(r, "components") and id(r) not in in_loop:
                     nl = Netlist(r)
                     N.check(L.crimson_set_outlet_netlist(self.elm.h, k, nl.h), "crimson_set_outlet_netlist")
                     self.netlists.append(nl)
+            pos = {id(r): k for k, r in enumerate(outlets)}
+            for spec in P.loops:
+                lp = NetlistLoop(spec)
+                sf = np.array([pos[id(c)] for c in spec.upstream], dtype=np.int32)
+                N.check(L.crimson_set_outlet_netlist_loop(self.elm.h, lp.h, N.ip(sf)), "crimson_set_outlet_netlist_loop")
+                self.loops.append(lp)
         self.inflow = inflow if inflow is not None else (lambda t: 10.0)
         if mesh.inlet_nodes is not None and len(mesh.inlet_nodes):
             nodes1 = np.ascontiguousarray(mesh.inlet_nodes.astype(np.int64) + 1, dtype=np.int32)
@@ -370,9 +377,9 @@ class FlowSolver:
         if getattr(self, "elm", None) is not None:
             self.elm.close()
             self.elm = None
-        for nl in getattr(self, "netlists", []):
+        for nl in getattr(self, "netlists", []) + getattr(self, "loops", []):
             nl.close()
-        self.netlists = []
+        self.netlists, self.loops = [], []
 
     def __del__(self):
         try:
@@ -388,7 +395,8 @@ class FlowSolver:
                                      ctypes.byref(st)), "crimson_step")
         self.istep += 1
         # the netlists' control systems, after the step's finalisation (itrdrv.f90:2100)
-        bound = [(nl, t, i, c) for nl in self.netlists for t, i, c in nl.spec.controllers]
+        circuits = self.netlists + [m for lp in self.loops for m in lp.members]
+        bound = [(nl, t, i, c) for nl in circuits for t, i, c in nl.spec.controllers]
         if bound:
             from .controllers import run_controllers
 

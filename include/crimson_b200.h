@@ -337,10 +337,10 @@ int crimson_elmgmr_sclr_device(crimson_ctx* ctx, int isclr, double diffus, const
  * the interface node takes the 3D surface pressure as a prescribed pressure
  * and the interface component's flow is solved for; the flow solver then
  * holds the surface at its Dirichlet codes (itrdrv.f90:1114-1133).
- * Control systems act through crimson_netlist_set_parameter (the Python
- * controllers of crimsonflowsolver_b200.controllers drive it); the
- * reference's built-in left-ventricular elastance and bleed controllers and
- * left-ventricular pressure prescriptions are not built.
+ * Control systems act through crimson_netlist_set_parameter: the Python
+ * controllers of crimsonflowsolver_b200.controllers drive it, the
+ * reference's built-in left-ventricular elastance and bleed controllers
+ * among them; left-ventricular pressure prescriptions are not built.
  * --------------------------------------------------------------------------- */
 typedef struct crimson_netlist crimson_netlist;
 #define CRIMSON_NETLIST_RESISTOR 0
@@ -362,6 +362,21 @@ int crimson_netlist_create(crimson_netlist** nl, int ncomp, const int* kind, con
                            const double* unstressed_volume, int nnodes, const double* initial_pressure, int npres,
                            const int* pres_node, const double* pres_value, int nflow, const int* flow_comp,
                            const int* flow_kind, const double* flow_value, int interface_node);
+/* A member of a closed loop (NetlistBoundaryCircuitWhenDownstreamCircuitsExist,
+ * NetlistClosedLoopDownstreamCircuit): as crimson_netlist_create, with the
+ * nodes shared with the loop's other circuits (shared_nodes, nshared; their
+ * Kirchhoff equations are the loop's) and interface_node 1 for an upstream
+ * circuit coupled to a 3D surface or 0 for the loop-closing (downstream)
+ * circuit, which has no 3D interface and no 3D-flow component.  A member is
+ * solved only through its crimson_netlist_loop; crimson_netlist_get,
+ * _get/_set_parameter, _state and _flow_permitted work on it as on any
+ * circuit. */
+int crimson_netlist_create_member(crimson_netlist** nl, int ncomp, const int* kind, const int* start_node,
+                                  const int* end_node, const double* value, const double* initial_volume,
+                                  const double* unstressed_volume, int nnodes, const double* initial_pressure,
+                                  int npres, const int* pres_node, const double* pres_value, int nflow,
+                                  const int* flow_comp, const int* flow_kind, const double* flow_value,
+                                  int interface_node, int nshared, const int* shared_nodes);
 void crimson_netlist_free(crimson_netlist* nl);
 /* detectWhetherClosedDiodesStopAllFlowAt3DInterface (CircuitData.cxx:388-470):
  * 1 in the Neumann design, 0 in the Dirichlet design. */
@@ -405,6 +420,30 @@ int crimson_netlist_set_parameter(crimson_netlist* nl, int what, int index, doub
  * written (set = 1). */
 int crimson_netlist_state_size(const crimson_netlist* nl, int* n);
 int crimson_netlist_state(crimson_netlist* nl, double* buf, int set);
+/* Closed loops (ClosedLoopDownstreamSubsection.cxx:101-500, 609-940): the
+ * upstream circuits (in input order) and one loop-closing circuit solved as
+ * one system.  Connection c (file order of the downstream input) joins node
+ * conn_down_node[c] of the loop-closing circuit to node conn_upstream_node[c]
+ * of upstream circuit conn_upstream[c] (0-based); each member's shared nodes
+ * must be exactly its connected nodes.  The loop does not own its members:
+ * free the loop first. */
+typedef struct crimson_netlist_loop crimson_netlist_loop;
+int crimson_netlist_loop_create(crimson_netlist_loop** loop, int nupstream, crimson_netlist* const* upstream,
+                                crimson_netlist* downstream, int nconn, const int* conn_down_node,
+                                const int* conn_upstream, const int* conn_upstream_node);
+void crimson_netlist_loop_free(crimson_netlist_loop* loop);
+/* getImplicitCoefficients: per upstream circuit k, p_k = dp_dq[k] * Q_k +
+ * hop[k] from one solve with alfi*Delt; NaN for a circuit in the Dirichlet
+ * design. */
+int crimson_netlist_loop_implicit_coefficients(crimson_netlist_loop* loop, double alfi_delt, double* dp_dq,
+                                               double* hop);
+/* updateLPN for every member: one solve with Delt; upstream circuit k takes
+ * interface_flow[k] in the Neumann design, interface_pressure[k] (the 3D
+ * surface's mean pressure) in the Dirichlet design. */
+int crimson_netlist_loop_update(crimson_netlist_loop* loop, double delt, const double* interface_flow,
+                                const double* interface_pressure);
+/* crimson_netlist_finalize_step of every member. */
+int crimson_netlist_loop_finalize_step(crimson_netlist_loop* loop);
 /* Couple surface k (0-based, srflist order) through nl instead of its RCR
  * in crimson_step: the coefficients come from nl at the start of each step,
  * and nl is updated and finalised with the surface's flow at its end; the
@@ -416,6 +455,15 @@ int crimson_netlist_state(crimson_netlist* nl, double* buf, int set);
  * updated with the surface's NASC-weighted mean pressure.  nl == NULL
  * restores the RCR.  The context does not own nl: free the context first. */
 int crimson_set_outlet_netlist(crimson_ctx* ctx, int k, crimson_netlist* nl);
+
+/* Couple the upstream circuits of loop through it: upstream circuit j
+ * couples surface surfaces[j] (0-based, srflist order).  Each step takes
+ * the loop's implicit coefficients once, updates the loop with the flows
+ * (blocked circuits: the NASC-weighted mean pressures) of its surfaces and
+ * finalises every member; the Dirichlet-design rules of
+ * crimson_set_outlet_netlist hold per upstream circuit.  The context does
+ * not own the loop. */
+int crimson_set_outlet_netlist_loop(crimson_ctx* ctx, crimson_netlist_loop* loop, const int* surfaces);
 
 /* yold/acold in the reference layout (nshg, 4) */
 int crimson_state_set(crimson_ctx* ctx, const double* y, const double* ac);

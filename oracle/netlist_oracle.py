@@ -31,6 +31,15 @@ flowsolver/src/NetlistCircuit.cxx, CircuitData.cxx and CircuitComponent.cxx:
   (NetlistCircuit.cxx:1386-1410), the interface component leaves the
   prescribed flows.
 
+* closed loops (ClosedLoopDownstreamSubsection.cxx:101-500, 609-940): each
+  member circuit leaves out the Kirchhoff rows of the nodes it shares with
+  the loop (NetlistCircuit.cxx:880-920), the blocks of the upstream circuits
+  and then the loop-closing circuit sit on the diagonal, followed by one
+  Kirchhoff row per shared node of the loop-closing circuit and one
+  pressure-equality row per connection; the implicit coefficients of
+  upstream circuit k come from the inverse at (its node 1, its 3D-flow row)
+  (852-888).
+
 numpy's LAPACK inverse stands in for PETSc's dense MatMatSolve.
 """
 from __future__ import annotations
@@ -45,11 +54,11 @@ class OracleNetlist:
         self.nc = len(self.comps)
         self.fixed = {int(k): float(v) for k, v in spec.prescribed_pressures.items()}
         self.fixed_flow = {int(k): float(v) for k, v in spec.prescribed_flows.items()}
-        self.iface = int(spec.interface_component)
+        self.iface = int(spec.interface_component)   # 0: a loop-closing circuit
+        self.shared = set(int(d) for d in getattr(spec, "shared_nodes", ()))
         self.p = np.array([spec.initial_pressures.get(i + 1, 0.0) for i in range(self.np_)], dtype=float)
         self.q = np.zeros(self.nc)
-        k, s, e, _ = self.comps[self.iface - 1]
-        self.sign = 1.0 if s == 1 else -1.0
+        self.sign = 1.0 if not self.iface or self.comps[self.iface - 1][1] == 1 else -1.0
         cap_nodes = set()
         for k, s, e, _ in self.comps:
             if k == "c":
@@ -65,9 +74,9 @@ class OracleNetlist:
         for _, s, e, _ in self.comps:
             count[s] += 1
             count[e] += 1
-        self.kirch = [i for i in range(1, self.np_ + 1) if count[i] > 1]
+        self.kirch = [i for i in range(1, self.np_ + 1) if count[i] > 1 and i not in self.shared]
         self.pp = sorted(self.fixed)
-        self.pf = sorted(set(self.fixed_flow) | {self.iface})
+        self.pf = sorted(set(self.fixed_flow) | ({self.iface} if self.iface else set()))
         self.open = [c[0] != "d" for c in self.comps]  # diodes start closed
         self.p3d = 0.0
         self.permitted = self.flow_permitted()
@@ -80,6 +89,8 @@ class OracleNetlist:
         """Whether some flow-permitting path leads from the interface
         component to a component end no other component touches (other
         than the interface node)."""
+        if not self.iface:
+            return True
         touching = {}
         for j, (_, s, e, _) in enumerate(self.comps):
             touching.setdefault(s, set()).add(j)
@@ -113,8 +124,9 @@ class OracleNetlist:
         fv = fhq + len(self.hist_comps)
         v_col = {j: fv + i for i, j in enumerate(self.vol_comps)}
         hv_col = {j: fv + len(self.vol_comps) + i for i, j in enumerate(self.vol_comps)}
-        A = np.zeros((n, n))
-        b = np.zeros(n)
+        rows = n - len(self.shared)
+        A = np.zeros((rows, n))
+        b = np.zeros(rows)
         r = 0
         for j, (k, s, e, v) in enumerate(self.comps):
             if k in ("t", "v"):
@@ -176,7 +188,7 @@ class OracleNetlist:
             A[r, hv_col[j]] = 1.0
             b[r] = self.hist_v[j]
             r += 1
-        assert r == n
+        assert r == rows
         return A, b, iface_row
 
     def implicit_coefficients(self, alfi_delt):
@@ -198,7 +210,10 @@ class OracleNetlist:
 
     def _update(self, delt):
         A, b, _ = self._system(delt)
-        x = np.linalg.inv(A) @ b
+        self.take(np.linalg.inv(A) @ b)
+
+    def take(self, x):
+        """Pressures, flows and volumes from this circuit's solution segment."""
         self.p = x[:self.np_].copy()
         fq = self.np_ + len(self.hist_nodes)
         self.q = x[fq:fq + self.nc].copy()
@@ -259,6 +274,86 @@ class OracleNetlist:
         q = {j + 1: float(self.q[j]) for j in range(self.nc)}
         v = {j + 1: float(self.vol[j]) for j in self.vol_comps}
         return p, q, v
+
+
+class OracleLoop:
+    """A closed loop: upstream circuits (input order), the loop-closing
+    circuit, and the connections (downstream node, upstream index 0-based,
+    upstream node) in file order."""
+
+    def __init__(self, upstream, downstream, connections):
+        self.up = list(upstream)
+        self.down = downstream
+        self.conn = [(int(d), int(k), int(u)) for d, k, u in connections]
+        self.members = self.up + [self.down]
+
+    def _system(self, alfi_delt):
+        blocks = [m._system(alfi_delt) for m in self.members]
+        n = sum(m.n for m in self.members)
+        A = np.zeros((n, n))
+        b = np.zeros(n)
+        r0, c0 = [], []
+        r = c = 0
+        for m, (Am, bm, _) in zip(self.members, blocks):
+            A[r:r + Am.shape[0], c:c + m.n] = Am
+            b[r:r + Am.shape[0]] = bm
+            r0.append(r)
+            c0.append(c)
+            r += Am.shape[0]
+            c += m.n
+
+        def kirchhoff(row, mi, node):
+            m = self.members[mi]
+            fq = c0[mi] + m.np_ + len(m.hist_nodes)
+            for j, (_, s, e, _) in enumerate(m.comps):
+                if e == node:
+                    A[row, fq + j] = 1.0
+                if s == node:
+                    A[row, fq + j] = -1.0
+
+        for d in sorted({d for d, _, _ in self.conn}):
+            for k in range(len(self.up)):
+                for d2, k2, u in self.conn:
+                    if d2 == d and k2 == k:
+                        kirchhoff(r, k, u)
+                        break
+            kirchhoff(r, len(self.up), d)
+            r += 1
+        for d, k, u in self.conn:
+            A[r, c0[k] + u - 1] = 1.0
+            A[r, c0[-1] + d - 1] = -1.0
+            r += 1
+        assert r == n
+        return A, b, r0, c0, [blk[2] for blk in blocks]
+
+    def implicit_coefficients(self, alfi_delt):
+        A, b, r0, c0, irow = self._system(alfi_delt)
+        Ainv = np.linalg.inv(A)
+        x = Ainv @ b
+        out = []
+        for k, m in enumerate(self.up):
+            if not m.permitted:
+                out.append((float("nan"), float("nan")))
+                continue
+            col = r0[k] + irow[k]
+            g = Ainv[c0[k], col]
+            out.append((m.sign * g, x[c0[k]] - g * b[col]))
+        return out
+
+    def update(self, delt, flows, pressures):
+        for k, m in enumerate(self.up):
+            if m.permitted:
+                m.last_q = flows[k]
+            else:
+                m.p3d = pressures[k]
+        A, b, _, c0, _ = self._system(delt)
+        x = np.linalg.inv(A) @ b
+        for m, c in zip(self.members, c0):
+            m.take(x[c:c + m.n])
+
+    def finalize_step(self):
+        for m in self.members:
+            m.finalize_step()
 
 
 def run_controllers(bound, delt):

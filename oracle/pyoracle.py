@@ -362,9 +362,18 @@ class OracleFlow:
         self.m.iBC = self.iBC_orig.copy()
         self.colm, self.rowp = genadj(mesh.ien, mesh.nshg)
         self.elm = Elm(self.m, P, self.colm, self.rowp, nthreads)
-        from oracle.netlist_oracle import OracleNetlist
+        from oracle.netlist_oracle import OracleLoop, OracleNetlist
 
         self.netlists = [OracleNetlist(r) if hasattr(r, "components") else None for r in self.rcr]
+        # closed loops: their upstream circuits are the outlets' circuits
+        self.loops, self.loop_surfaces = [], []
+        pos = {id(r): k for k, r in enumerate(self.rcr)}
+        for spec in getattr(P, "loops", []):
+            sf = [pos[id(c)] for c in spec.upstream]
+            self.loops.append(OracleLoop([self.netlists[k] for k in sf], OracleNetlist(spec.downstream),
+                                         [(d, spec.upstream_index(s), u) for d, s, u in spec.connections]))
+            self.loop_surfaces.append(sf)
+        self.in_loop = {k for sf in self.loop_surfaces for k in sf}
         self.onodes = [np.nonzero(mesh.ndsurf == s)[0] for s in self.srflist]
         self.nasc = surface_areas(mesh) if any(nl is not None for nl in self.netlists) else None
         self.memls = MemLS(mesh.nshg, self.colm, self.rowp, 1 + len(self.rcr), P, nthreads)
@@ -410,8 +419,14 @@ class OracleFlow:
         P = self.P
         c1 = np.zeros(len(self.rcr))
         c2 = np.zeros(len(self.rcr))
+        for lp, sf in zip(self.loops, self.loop_surfaces):
+            for k, (a, b) in zip(sf, lp.implicit_coefficients(P.alfi * P.Delt if alpha_form else P.Delt)):
+                c1[k], c2[k] = a, b
         for k, r in enumerate(self.rcr):
             if self._blocked(k):
+                c1[k] = c2[k] = 0.0
+                continue
+            if k in self.in_loop:
                 continue
             if self.netlists[k] is not None:
                 c1[k], c2[k] = self.netlists[k].implicit_coefficients(P.alfi * P.Delt if alpha_form else P.Delt)
@@ -463,15 +478,24 @@ class OracleFlow:
             q1 = getflowq(self.m, self.y, self.srflist)
             d1, h1 = self.implicit_coeffs(n, False)
             Pn = d1 * q1 + h1
+
+            def p3d(k):
+                # integrScalar(p) / area (elmgmr.f90:1733-1743)
+                w = self.nasc[self.onodes[k]]
+                return float(np.sum(w * self.y[self.onodes[k], 3]) / np.sum(w))
+
+            for lp, sf in zip(self.loops, self.loop_surfaces):
+                lp.update(P.Delt, [q1[k] for k in sf], [0.0 if lp.up[j].permitted else p3d(k)
+                                                         for j, k in enumerate(sf)])
+                lp.finalize_step()
             for k, nl in enumerate(self.netlists):
                 if nl is not None:
-                    if nl.permitted:
-                        nl.update(P.Delt, q1[k])
-                    else:
-                        # integrScalar(p) / area (elmgmr.f90:1733-1743)
-                        w = self.nasc[self.onodes[k]]
-                        nl.update_pressure(P.Delt, float(np.sum(w * self.y[self.onodes[k], 3]) / np.sum(w)))
-                    nl.finalize_step()
+                    if k not in self.in_loop:
+                        if nl.permitted:
+                            nl.update(P.Delt, q1[k])
+                        else:
+                            nl.update_pressure(P.Delt, p3d(k))
+                        nl.finalize_step()
                     Pn[k] = nl.interface_pressure()
             self.Pn = Pn
             self.Qn = q1
@@ -481,6 +505,8 @@ class OracleFlow:
         # control systems after the finalisation (itrdrv.f90:2100)
         bound = [(nl, t, i, c) for nl, r in zip(self.netlists, self.rcr) if nl is not None
                  for t, i, c in r.controllers]
+        bound += [(lp.down, t, i, c) for lp, spec in zip(self.loops, getattr(P, "loops", []))
+                  for t, i, c in spec.downstream.controllers]
         if bound:
             from oracle.netlist_oracle import run_controllers
 
