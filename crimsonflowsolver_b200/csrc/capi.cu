@@ -464,6 +464,9 @@ int crimson_set_outlets(crimson_ctx* c, int ncoupled, const int* srflist, const 
     c->rcr_Pn.assign(ncoupled, 0.0);
     c->rcr_Qn.assign(ncoupled, 0.0);
     c->netlists.assign((size_t)ncoupled, nullptr);
+    c->loops.clear();
+    c->loop_surfaces.clear();
+    c->loop_of.assign((size_t)ncoupled, -1);
     return CRIMSON_OK;
 }
 

@@ -1,12 +1,13 @@
 """Netlist outlets in the device time step (crimson_set_outlet_netlist) against
 the oracle's time stepper with the same circuit (OracleFlow +
-oracle/netlist_oracle.py), and the Windkessel written as a netlist against
-the built-in RCR outlet.  Parity bar as for the RCR time steps: velocity,
+oracle/netlist_oracle.py), closed loops of circuits
+(crimson_set_outlet_netlist_loop) likewise, and the Windkessel written as a
+netlist against the built-in RCR outlet.  Parity bar as for the RCR time steps: velocity,
 pressure and outlet pressure within 1e-10, identical iteration counts."""
 import numpy as np
 import pytest
 
-from crimsonflowsolver_b200 import FlowParams, NetlistBC, RCR, mesh, solver
+from crimsonflowsolver_b200 import FlowParams, NetlistBC, NetlistLoopBC, RCR, mesh, solver
 from oracle import pyoracle as po
 from tests.conftest import relerr
 
@@ -161,3 +162,57 @@ def test_controllers_in_time_steps_parity():
         G.close()
     assert relerr(y[:, 0:3], F.y[:, 0:3]) < 1e-10, relerr(y[:, 0:3], F.y[:, 0:3])
     assert relerr(y[:, 3], F.y[:, 3]) < 1e-10, relerr(y[:, 3], F.y[:, 3])
+
+
+def _loop(m):
+    """Two outlets joined by a loop-closing circuit: outlet 1 through an
+    RC branch, outlet 2 through a valve (the simpleDiodeTest circuit, which
+    starts closed), both ending at node 1 of a circuit that drains through a
+    compliance and a resistance to a venous pressure."""
+    s0, s1 = m.outlets
+    a = NetlistBC(srfid=s0, components=[("r", 1, 2, 60.0), ("c", 2, 3, 1e-4), ("r", 2, 4, 400.0)],
+                  prescribed_pressures={3: 0.0}, interface_component=1, initial_pressures={2: 5.0, 4: 5.0},
+                  shared_nodes=(4,))
+    b = NetlistBC(srfid=s1, components=[("r", 1, 2, 1.0), ("d", 2, 3, 0.1)], interface_component=1,
+                  initial_pressures={1: 1058.5, 2: 1058.5, 3: 1000.0}, shared_nodes=(3,))
+    d = NetlistBC(srfid=0, components=[("r", 1, 2, 300.0), ("c", 1, 3, 5e-4), ("r", 2, 4, 10.0)],
+                  prescribed_pressures={3: 0.0, 4: 1250.0}, interface_component=0,
+                  initial_pressures={1: 5.0, 2: 1200.0}, shared_nodes=(1,))
+    return NetlistLoopBC(upstream=[a, b], downstream=d, connections=[(1, s0, 4), (1, s1, 3)])
+
+
+def test_closed_loop_time_steps_parity():
+    """A closed loop over both outlets (crimson_set_outlet_netlist_loop):
+    one loop solve gives both surfaces' coefficients, the valved outlet
+    switches between the Dirichlet and the Neumann design, and every step's
+    designs, iteration counts, outlet pressures and flows, and at the end
+    velocity, pressure and every member's state match the oracle's time
+    stepper (OracleFlow with OracleLoop)."""
+    m = mesh.cylinder(ncross=8, naxial=10, n_outlets=2)
+    P = FlowParams(loops=[_loop(m)], nitr=2)
+    F = po.OracleFlow(mesh.cylinder(ncross=8, naxial=10, n_outlets=2), P, inflow=lambda t: 10.0)
+    G = solver.FlowSolver(mesh.cylinder(ncross=8, naxial=10, n_outlets=2), P, inflow=lambda t: 10.0)
+    modes = ""
+    try:
+        for _ in range(6):
+            designs = [u.permitted for u in F.loops[0].up]
+            assert G.loops[0].flow_permitted() == designs
+            modes += "".join("N" if x else "D" for x in designs) + " "
+            F.step()
+            st = G.step()
+            its = [(r, g, c) for r, g, c, _, _ in F.stats[-st.nsolves:]]
+            assert its == [(st.ri_itr[i], st.gm_itr[i], st.cg_itr[i]) for i in range(st.nsolves)]
+            for k in range(2):
+                assert abs(st.p_out[k] - F.Pn[k]) <= 1e-9 * abs(F.Pn[k]), (k, st.p_out[k], F.Pn[k])
+                assert abs(st.q_out[k] - F.Qn[k]) <= 1e-9 * max(1.0, abs(F.Qn[k])), (k, st.q_out[k], F.Qn[k])
+        y, _ = G.state()
+        members = [mm.get() for mm in G.loops[0].members]
+    finally:
+        G.close()
+    assert "ND" in modes and "NN" in modes, modes
+    assert relerr(y[:, 0:3], F.y[:, 0:3]) < 1e-10, relerr(y[:, 0:3], F.y[:, 0:3])
+    assert relerr(y[:, 3], F.y[:, 3]) < 1e-10, relerr(y[:, 3], F.y[:, 3])
+    for (p, q, op, _), o in zip(members, F.loops[0].members):
+        assert relerr(p, [o.pressure(i + 1) for i in range(len(p))]) < 1e-10
+        assert relerr(q, o.q) < 1e-10
+        assert list(op) == list(o.open)
