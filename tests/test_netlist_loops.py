@@ -230,3 +230,70 @@ def test_reader_rejects_circuit_in_two_loops():
         nio.closed_loops(circuits, v["srfids"], down + down, ignore_controls=True)
     with pytest.raises(ValueError):
         nio.closed_loops(circuits, [5, 6, 8], down, ignore_controls=True)
+
+
+def test_closed_loop_heart_with_lv_control():
+    """netlist/closedLoopHeart with its circuits' controls bound (the heart's
+    built-in LV elastance): twelve steps, library vs oracle, each side with
+    its own controller instances run after the finalisation."""
+    from crimsonflowsolver_b200.controllers import run_controllers
+    from oracle.netlist_oracle import run_controllers as oracle_run
+
+    v = _cases()["netlist/closedLoopHeart"]
+
+    def read():
+        return nio.closed_loops(nio.parse_netlist_xml(v["surfaces"]), v["srfids"],
+                                nio.parse_netlist_xml(v["downstream"]))[1][0]
+
+    gs, os_ = read(), read()
+    assert any(c.controllers for c in gs.upstream)
+    g, o = NetlistLoop(gs), _oracle(os_)
+    gb = [(m, t, i, c) for m, spec in zip(g.members, gs.upstream + [gs.downstream]) for t, i, c in spec.controllers]
+    ob = [(m, t, i, c) for m, spec in zip(o.members, os_.upstream + [os_.downstream]) for t, i, c in spec.controllers]
+    try:
+        for step in range(12):
+            assert g.flow_permitted() == [m.permitted for m in o.up]
+            assert _close(g.implicit_coefficients(ALFI * DT), o.implicit_coefficients(ALFI * DT), 1e-9), step
+            q = [2.0 * math.sin(0.9 * step + k) for k in range(3)]
+            p = [9000.0 + 2000.0 * math.cos(0.4 * step + k) for k in range(3)]
+            g.update(DT, q, p)
+            o.update(DT, q, p)
+            g.finalize_step()
+            o.finalize_step()
+            run_controllers(gb, DT)
+            oracle_run(ob, DT)
+            for gm, om in zip(g.members, o.members):
+                pp, f, _, _ = gm.get()
+                assert _close(pp, [om.pressure(j + 1) for j in range(len(pp))], 1e-9), step
+                assert _close(f, om.q, 1e-9), step
+            for (gm, t, i, _), (om, _, _, _) in zip(gb, ob):
+                assert gm.get_parameter(t, i) == pytest.approx(om.get_parameter(t, i), rel=1e-12)
+    finally:
+        g.close()
+
+
+def test_loop_checkpoint_restart():
+    """Every member's state written after five steps and read into a fresh
+    loop: the next five steps of both loops are identical."""
+    spec = _loops("netlist/closedLoopHeart")[1][0]
+    a = NetlistLoop(spec)
+    b = NetlistLoop(spec)
+
+    def run(loop, steps):
+        for step in steps:
+            loop.flow_permitted()
+            loop.implicit_coefficients(ALFI * DT)
+            loop.update(DT, [1.5 * math.sin(step + k) for k in range(3)], [9000.0 + 100.0 * step] * 3)
+            loop.finalize_step()
+
+    try:
+        run(a, range(5))
+        for ma, mb in zip(a.members, b.members):
+            mb.set_state(ma.state())
+        run(a, range(5, 10))
+        run(b, range(5, 10))
+        for ma, mb in zip(a.members, b.members):
+            assert np.array_equal(ma.state(), mb.state())
+    finally:
+        a.close()
+        b.close()
