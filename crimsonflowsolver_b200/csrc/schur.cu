@@ -32,6 +32,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <vector>
 
@@ -287,12 +288,15 @@ int schur_form(crimson_lhs* L, const double* mG, const double* Gt, const double*
     if (L->s2_state != 1) return CRIMSON_ERR_STATE;
     cudaStream_t s = L->stream;
     const size_t smem = 32 * (size_t)kS2Cap * (sizeof(double) + sizeof(int));
-    static bool attr_set[256] = {false};
+    // the attribute is per device; setting it again (two host threads racing
+    // on the first call) is harmless, so a relaxed flag is enough
+    static std::atomic<bool> attr_set[256];
     int dev = 0;
     CR_CUDA(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 256 && !attr_set[dev]) {
+    if (dev < 0 || dev >= 256) return CRIMSON_ERR_UNSUPPORTED;
+    if (!attr_set[dev].load(std::memory_order_relaxed)) {
         CR_CUDA(cudaFuncSetAttribute(k_s2_form, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set[dev] = true;
+        attr_set[dev].store(true, std::memory_order_relaxed);
     }
     CR_CUDA(cudaEventRecord(L->s2_ev0, s));
     launch(k_s2_form, std::min(L->s2_nslice, 2 * sm_count()), kS2Threads, smem, s, L->rowptr, L->col, mG, Gt, mL,
