@@ -1,6 +1,7 @@
-"""Build the PHASTA fixtures from the reference's own test case
-testbin/mainTests/basic (geombc.dat.1 + restart.0.1), with the package's
-PHASTA reader.  Run once where a reference checkout exists:
+"""Build the PHASTA fixtures from the reference's own test cases
+testbin/mainTests/basic and testbin/mainTests/netlist/closedLoopHeart
+(geombc.dat.1 + restart.0.1), with the package's PHASTA reader.  Run once
+where a reference checkout exists:
 
     python tests/golden/make_phasta_fixture.py /path/to/reference/checkout
 
@@ -10,7 +11,10 @@ Writes
   basic_headers.json  the text lines (comments and block headers, no binary
                       data) of both files, so the reader and the writer can
                       be checked against the reference's header grammar and
-                      block sizes without the reference checkout.
+                      block sizes without the reference checkout;
+  closed_loop_heart_mesh.npz  the same arrays for the closedLoopHeart case
+                      (4205 nodes, 18022 tets; outlets 5, 6, 7 coupled
+                      through netlist circuits and a closed loop).
 """
 import json
 import os
@@ -35,6 +39,13 @@ def main(ref):
     heads = {"geombc.dat.1": phasta.header_lines(geo), "restart.0.1": phasta.header_lines(rst)}
     with open(os.path.join(HERE, "basic_headers.json"), "w") as f:
         json.dump(heads, f, indent=1)
+    print(out, "nodes", m.nshg, "tets", m.nelem, "boundary", len(m.ienb), "dirichlet", len(m.dirichlet_nodes))
+    base = os.path.join(ref, "testbin", "mainTests", "netlist", "closedLoopHeart")
+    m = phasta.read_geombc(os.path.join(base, "geombc.dat.1"))
+    y, ac, _ = phasta.read_restart(os.path.join(base, "restart.0.1"))
+    out = os.path.join(HERE, "closed_loop_heart_mesh.npz")
+    np.savez_compressed(out, x=m.x, ien=m.ien, ienb=m.ienb, iBCB=m.iBCB, BCB=m.BCB[:, 0, :], iBC=m.iBC,
+                        dirichlet_nodes=m.dirichlet_nodes, dirichlet_values=m.dirichlet_values, y=y, ac=ac)
     print(out, "nodes", m.nshg, "tets", m.nelem, "boundary", len(m.ienb), "dirichlet", len(m.dirichlet_nodes))
 
 
