@@ -1,0 +1,49 @@
+"""GPU: the reference's closedLoopHeart case (testbin/mainTests/netlist/
+closedLoopHeart; flowsolver/test/testMain.cxx:266-345) through the device
+time step (FlowSolver: crimson_step with the closed loop coupled by
+crimson_set_outlet_netlist_loop), against the oracle's time stepper step by
+step -- the design of each surface, memLS iteration counts, outlet flows and
+pressures, and at the end velocity and pressure within 1e-9 -- and against
+the values the reference's test asserts, with the bars of
+tests/test_reference_closed_loop_heart.py."""
+import numpy as np
+import pytest
+
+from crimsonflowsolver_b200 import solver
+from oracle import pyoracle as po
+from tests.conftest import relerr
+from tests.fixtures import CLOSED_LOOP_HEART_GOLDEN as GOLD
+from tests.fixtures import closed_loop_heart_case
+from tests.test_reference_closed_loop_heart import run_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def test_closed_loop_heart_case_on_device():
+    F, hist = run_oracle()
+    m, y, ac, P = closed_loop_heart_case()
+    y0 = y.copy()
+    po.itr_bc(m, y0)
+    G = solver.FlowSolver(m, P, inflow=lambda t: 0.0)
+    nasc = po.surface_areas(m)
+    onodes = [np.nonzero(m.ndsurf == s)[0] for s in (5, 6, 7)]
+    try:
+        G.set_state(y0, ac)
+        for k in range(5):
+            assert G.loops[0].flow_permitted() == hist[k]["permitted"], k
+            st = G.step()
+            for j in range(3):
+                assert abs(st.q_out[j] - hist[k]["Q"][j]) <= 1e-9 * max(1.0, abs(hist[k]["Q"][j])), (k, j)
+            yk, _ = G.state()
+            p = np.array([np.sum(nasc[o] * yk[o, 3]) / np.sum(nasc[o]) for o in onodes])
+            assert np.all(np.abs(p - hist[k]["p"]) <= 1e-9 * np.abs(hist[k]["p"])), (k, p, hist[k]["p"])
+            down = G.loops[0].downstream.get()[0]
+            assert np.abs(down - hist[k]["down_p"]).max() <= 1e-9 * np.abs(hist[k]["down_p"]).max(), k
+        yG, _ = G.state()
+    finally:
+        G.close()
+    assert relerr(yG[:, 0:3], F.yold[:, 0:3]) < 1e-9, relerr(yG[:, 0:3], F.yold[:, 0:3])
+    assert relerr(yG[:, 3], F.yold[:, 3]) < 1e-9, relerr(yG[:, 3], F.yold[:, 3])
+    gold_q, gold_p = np.array(GOLD["flow_step5"]), np.array(GOLD["pressure_step5"])
+    assert np.all(np.abs(np.array([st.q_out[j] for j in range(3)]) - gold_q) <= 2e-5 * np.abs(gold_q))
+    assert np.all(np.abs(p - gold_p) <= 3e-4 * np.abs(gold_p))

@@ -54,11 +54,12 @@ def run_oracle(steps=5):
     F._itr_bc(F.yold)
     hist = []
     for _ in range(steps):
-        F.step()
         lp = F.loops[0]
+        permitted = [u.permitted for u in lp.up]   # the design the step runs in
+        F.step()
         hist.append({"Q": F.Qn.copy(), "p": surface_mean_pressures(F), "heart_q": float(lp.up[0].q[0]),
                      "down_p": np.array([lp.down.pressure(i + 1) for i in range(lp.down.np_)]),
-                     "permitted": [u.permitted for u in lp.up]})
+                     "permitted": permitted})
     return F, hist
 
 
@@ -72,8 +73,9 @@ def test_case_set_up(oracle_run):
     assert F.srflist == [5, 6, 7]
     assert F.m.nshg == 4205 and F.m.ien.shape == (18022, 4)
     # the heart's valves start closed: its surface is a Dirichlet surface in
-    # step 1 and takes flow from step 2 on
-    assert hist[0]["Q"][0] == 0.0
+    # steps 1 and 2 and takes flow from step 3 on
+    assert [h["permitted"] for h in hist[:3]] == [[False, True, True]] * 2 + [[True, True, True]]
+    assert hist[0]["Q"][0] == 0.0 and hist[1]["Q"][0] == 0.0 and hist[2]["Q"][0] != 0.0
 
 
 def test_loop_closing_circuit_pressures_step4(oracle_run):
