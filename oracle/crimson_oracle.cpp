@@ -10,9 +10,14 @@
 // association explicitly.  Build with -ffp-contract=off so no FMA contraction
 // changes the rounding (the reference build uses plain -O2/-O3 gfortran).
 //
-// Parity status: UNPINNED (no Fortran/MPI toolchain here; no golden vectors at
-// this boundary in the reference's tests).  See tests/test_oracle_*.py for the
-// analytic self-checks that stand in.
+// Parity status: pinned end to end by the values the reference's own test
+// checkClosedLoopWithHeart (flowsolver/test/testMain.cxx:266-345) asserts for
+// testbin/mainTests/netlist/closedLoopHeart, which this restatement, driven
+// by oracle/pyoracle.py's time stepper, reproduces
+// (tests/test_reference_closed_loop_heart.py); no Fortran/MPI toolchain
+// exists here to run the reference itself, and no golden vector exists at the
+// single-call boundary.  tests/test_oracle_*.py hold the analytic
+// self-checks.
 #include "crimson_oracle.h"
 
 #include <algorithm>

@@ -7,11 +7,15 @@
  * the checker for the CUDA path and the timed CPU baseline; the product never
  * links, loads or calls it.
  *
- * Parity status: UNPINNED.  The reference is Fortran 90 + MPI and no Fortran
- * compiler or MPI exists in this environment, and the reference's own tests
- * pin only whole-product history values (deformable walls, netlists, Python
- * controllers), so no golden vector exists at this boundary.  The restatement
- * is checked instead by analytic self-checks (tests/test_oracle_*.py).
+ * Parity status: pinned end to end.  The reference is Fortran 90 + MPI and
+ * no Fortran compiler or MPI exists in this environment, and its own tests
+ * pin only whole-run history values, so no golden vector exists at the
+ * single-call boundary.  One of those whole runs is a rigid-wall memLS case
+ * whose mesh ships with it (testbin/mainTests/netlist/closedLoopHeart,
+ * asserted by flowsolver/test/testMain.cxx:266-345); this restatement,
+ * sequenced by oracle/pyoracle.py, reproduces the asserted flows and
+ * pressures (tests/test_reference_closed_loop_heart.py).  Analytic
+ * self-checks in tests/test_oracle_*.py cover the single calls.
  *
  * Conventions mirror the Fortran arrays: column-major, 1-based node and CSR
  * indices (ien, colm, rowp, ienb, gNodes).
