@@ -43,14 +43,16 @@ class LsStats(ctypes.Structure):
 
 
 class StepArgs(ctypes.Structure):
-    _fields_ = [("nitr", ctypes.c_int), ("inflow_scale", ctypes.c_double)]
+    _fields_ = [("nitr", ctypes.c_int), ("inflow_scale", ctypes.c_double), ("rescontrol", ctypes.c_int),
+                ("res_criteria", ctypes.c_double), ("min_iters", ctypes.c_int)]
 
 
 class StepStats(ctypes.Structure):
     _fields_ = [("nsolves", ctypes.c_int), ("ri_itr", ctypes.c_int * 16), ("gm_itr", ctypes.c_int * 16),
                 ("cg_itr", ctypes.c_int * 16), ("ri_inorm", ctypes.c_double * 16),
                 ("ri_fnorm", ctypes.c_double * 16), ("q_out", ctypes.c_double * 8), ("p_out", ctypes.c_double * 8),
-                ("refine_steps", ctypes.c_int * 16), ("refine_rel", ctypes.c_double * 16)]
+                ("refine_steps", ctypes.c_int * 16), ("refine_rel", ctypes.c_double * 16),
+                ("res_norm", ctypes.c_double * 16)]
 
 
 # name -> (restype, argtypes)

@@ -431,6 +431,54 @@ __global__ void k_surfp_step(const int* __restrict__ onodes, int beg, int end, c
     if (threadIdx.x == 0) *out = s;
 }
 
+// Sum of squares of x (n values) per block, then the block partials summed
+// in block order by one block: deterministic.  rstatic's totres
+// (rstatic.f90:60-118) is sqrt(sum / nshg) over the four dofs of res.
+constexpr int kSumsqBlocks = 296;
+__global__ void k_sumsq_part(const double* __restrict__ x, long long n, double* __restrict__ part) {
+    __shared__ double sm[32];
+    double s = 0.0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        s += x[t] * x[t];
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+__global__ void k_sumsq_final(const double* __restrict__ part, int np, double* __restrict__ out) {
+    __shared__ double sm[32];
+    double s = 0.0;
+    for (int b = threadIdx.x; b < np; b += blockDim.x) s += part[b];
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// Residual control (itrdrv.f90:1516-1522, rstatic.f90:117-124): after the
+// assembly of a nonlinear iteration, totres = sqrt(|res|^2 / nshg); the
+// iteration counter counts the assembled iterations; once totres is below
+// the criterion after at least min_iters of them, the step ends without
+// this iteration's solve and update (the reference solves and then
+// discards the increment) and the counter restarts.  A step that runs all
+// its iterations keeps the count for the next step, as the reference does.
+static int residual_control(crimson_ctx* c, const crimson_step_args* args, crimson_step_stats* st, int it,
+                            bool* done) {
+    *done = false;
+    if (!args->rescontrol) return CRIMSON_OK;
+    cudaStream_t s = c->stream;
+    const long long n4 = 4LL * c->nshg;
+    launch(k_sumsq_part, kSumsqBlocks, 256, 0, s, (const double*)c->res4.p, n4, c->sumsq.p);
+    launch(k_sumsq_final, 1, 256, 0, s, (const double*)c->sumsq.p, kSumsqBlocks, c->sumsq.p + kSumsqBlocks);
+    double ss = 0.0;
+    CR_CUDA(cudaMemcpyAsync(&ss, c->sumsq.p + kSumsqBlocks, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    const double totres = std::sqrt(ss / (double)c->nshg);
+    if (st && it < 16) st->res_norm[it] = totres;
+    c->res_iter += 1;
+    if (totres < args->res_criteria && c->res_iter >= args->min_iters) {
+        c->res_iter = 0;
+        *done = true;
+    }
+    return CRIMSON_OK;
+}
+
 extern "C" {
 
 int crimson_set_outlets(crimson_ctx* c, int ncoupled, const int* srflist, const int* ndsurf, const double* NABI) {
@@ -1021,6 +1069,7 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
     for (int k = 0; k < nc; ++k) faceRes[1 + k] = c1[k] * P.alfi * P.gami * P.Delt;
     std::vector<int> incL(1 + nc, 1);
     if (st) std::memset(st, 0, sizeof(*st));
+    if (args->rescontrol) CR_CHECK(c->sumsq.alloc(kSumsqBlocks + 1));
     for (int it = 0; it < args->nitr; ++it) {
         launch(k_yalpha, grid_for(n, 256), 256, 0, s, c->yold.p, c->acold.p, c->ycur.p, c->accur.p, c->yalpha.p,
                                                   c->acalpha.p, n, P.alfi, P.almi);
@@ -1030,11 +1079,17 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
             CR_CHECK(c->lhs32.alloc(16 * (size_t)c->nnz));
             CR_CHECK(elmgmr_device(c, c->yalpha.p, c->acalpha.p, c1.data(), c2.data(), c->res4.p, nullptr, nullptr, 2,
                                    c->lhs32.p));
+            bool done = false;
+            CR_CHECK(residual_control(c, args, st, it, &done));
+            if (done) break;
             CR_CHECK(memls_solve_lhs_device(L, ls, c->res4.p, nullptr, nullptr, incL.data(), faceRes.data(),
                                             c->solinc.p, &lst, false, c->lhs32.p));
         } else {
             CR_CHECK(elmgmr_device(c, c->yalpha.p, c->acalpha.p, c1.data(), c2.data(), c->res4.p, c->lhsK.p,
                                    c->lhsP.p, 1));
+            bool done = false;
+            CR_CHECK(residual_control(c, args, st, it, &done));
+            if (done) break;
             CR_CHECK(memls_solve_lhs_device(L, ls, c->res4.p, c->lhsK.p, c->lhsP.p, incL.data(), faceRes.data(),
                                             c->solinc.p, &lst));
         }

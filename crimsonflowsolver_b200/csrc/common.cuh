@@ -231,4 +231,6 @@ struct crimson_ctx {
     std::vector<std::vector<int>> loop_surfaces;    // per loop: the coupled surface of each upstream circuit
     std::vector<int> loop_of;                       // per coupled surface: its loop, or -1
     int istep = 0;
+    int res_iter = 0;                 // residual control: iterations since the last early exit
+    crimson::DBuf<double> sumsq;      // residual control: block partials + total
 };

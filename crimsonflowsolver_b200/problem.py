@@ -12,6 +12,8 @@ configs/input.config and the reference test cases):
 * stabflux_coeff             ``Influx Coefficient``
 * ibksiz                     ``Number of Elements Per Block``
 * nitr                       number of solve/update pairs in ``Step Construction``
+* rescontrol, res_criteria,  ``Residual Control`` / ``Residual Criteria`` /
+  min_iters                  ``Minimum Required Iterations``
 * epstol_mom, epstol_cont,   memLS tolerances (epstol(1), epstol(7), epstol(8))
   epstol_ns
 * kspace, ngmres, maxiters,  memLS sizes (Kspace, nGMRES, maxIters, nPrjs)
@@ -114,6 +116,9 @@ class FlowParams:
     stabflux_coeff: float = 0.5
     ibksiz: int = 255
     nitr: int = 3
+    rescontrol: bool = False
+    res_criteria: float = 0.0
+    min_iters: int = 0
     epstol_mom: float = 1e-4
     epstol_cont: float = 1e-4
     epstol_ns: float = 1e-5

@@ -389,7 +389,8 @@ class FlowSolver:
 
     def step(self) -> N.StepStats:
         t1 = self.P.Delt * (self.istep + 1)
-        args = N.StepArgs(nitr=self.P.nitr, inflow_scale=self.inflow(t1))
+        args = N.StepArgs(nitr=self.P.nitr, inflow_scale=self.inflow(t1), rescontrol=int(bool(self.P.rescontrol)),
+                          res_criteria=float(self.P.res_criteria), min_iters=int(self.P.min_iters))
         st = N.StepStats()
         N.check(N.lib().crimson_step(self.elm.h, self.memls.lhs, self.memls.ls, ctypes.byref(args),
                                      ctypes.byref(st)), "crimson_step")

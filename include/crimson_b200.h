@@ -273,6 +273,16 @@ int crimson_elmgmr_vjp(crimson_ctx* ctx, const double* d_y, const double* d_ac, 
 typedef struct {
     int nitr;               /* solve/update pairs per step (Step Construction) */
     double inflow_scale;    /* multiplies the registered inlet profile at t_{n+1} */
+    /* Residual Control / Residual Criteria / Minimum Required Iterations
+     * (itrdrv.f90:1516-1522): with rescontrol != 0 the step ends after the
+     * assembly of the first iteration whose totres = sqrt(|res|^2 / nshg)
+     * (rstatic.f90) is below res_criteria once at least min_iters
+     * iterations have been assembled, without that iteration's solve; the
+     * count carries over a step that ends without such an exit.  Zero
+     * (off) in a zero-initialised struct. */
+    int rescontrol;
+    double res_criteria;
+    int min_iters;
 } crimson_step_args;
 
 typedef struct {
@@ -282,6 +292,7 @@ typedef struct {
     double q_out[8], p_out[8];   /* outlet flow and pressure at t_{n+1} */
     int refine_steps[16];        /* mixed precision: refinement sweeps per solve */
     double refine_rel[16];       /* mixed precision: final |R - A x| / |R| per solve */
+    double res_norm[16];         /* residual control: totres of each assembled iteration */
 } crimson_step_stats;
 
 /* register the inlet profile: BC(node, 3:5) = profile * inflow_scale */

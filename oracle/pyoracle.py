@@ -392,6 +392,8 @@ class OracleFlow:
         self.Pn = np.zeros(len(self.rcr))
         self.Qn = np.zeros(len(self.rcr))
         self.stats = []
+        self.res_iter = 0      # residual control: iterations since the last early exit
+        self.res_norms = []
         mesh.set_inflow(self.inflow(0.0))
         self._itr_bc(self.yold)
 
@@ -436,7 +438,18 @@ class OracleFlow:
                 c1[k], c2[k] = rcr_coeffs(r.Rp, r.C, r.Rd, r.Pd, r.Pd, self.Pn[k], self.Qn[k], P.Delt)
         return c1, c2
 
-    def solflow(self, c1, c2):
+    def _res_control(self, res):
+        """Residual control (itrdrv.f90:1516-1522): totres of rstatic.f90
+        counted per assembled iteration; True ends the step early."""
+        totres = float(np.sqrt(np.sum(np.asarray(res, dtype=float) ** 2) / self.m.nshg))
+        self.res_norms.append(totres)
+        self.res_iter += 1
+        if totres < self.P.res_criteria and self.res_iter >= self.P.min_iters:
+            self.res_iter = 0
+            return True
+        return False
+
+    def solflow(self, c1, c2, stop=None):
         P = self.P
         yA = self.y.copy()
         acA = self.ac.copy()
@@ -446,6 +459,8 @@ class OracleFlow:
         acA[:, 3] = 0.0
         yA[:, 3] = self.y[:, 3]
         out = self.elm(yA, acA, lhs=True, srflist=self.srflist, coef1=c1, coef2=c2)
+        if stop is not None and stop(out["res"]):
+            return None
         Res4, Val4 = solflow_pack(self.m.nshg, self.colm, self.rowp, out["res"], out["lhsK"], out["lhsP"])
         faceRes = np.zeros(1 + len(self.rcr))
         faceRes[1:] = c1
@@ -466,7 +481,10 @@ class OracleFlow:
         self._itr_bc(self.y)
         c1, c2 = self.implicit_coeffs(n, True)
         for _ in range(P.nitr):
-            sol, st, _out = self.solflow(c1, c2)
+            r = self.solflow(c1, c2, stop=self._res_control if getattr(P, "rescontrol", False) else None)
+            if r is None:
+                break
+            sol, st, _out = r
             self.stats.append((st.RI.itr, st.GM.itr, st.CG.itr, st.RI.iNorm, st.RI.fNorm))
             # itrCorrect (itrPC.f90:176-182)
             self.y[:, 0:3] = self.y[:, 0:3] + (P.gami * P.Delt) * sol[:, 0:3]

@@ -50,7 +50,7 @@ def closed_loop_heart_case():
     """(mesh, y, ac, FlowParams) of the closedLoopHeart case: its solver.inp
     (density 0.00106, viscosity 0.004, Delt 1e-3, first-order time
     integration, "0 1" x 5 = five solve/update pairs, influx coefficient
-    0.5, memLS) with configs/input.config's memLS defaults (Kspace 50,
+    0.5, residual control at 1e-3 after at least 2 iterations, memLS) with configs/input.config's memLS defaults (Kspace 50,
     nGMRES 1, maxIters 200, nPrjs 10, epstol 0.01 / 0.2 / 0.4), and its
     netlist inputs: surfaces 5, 6, 7 joined by the loop-closing circuit, the
     heart's LV elastance control bound.  The loop is built afresh on every
@@ -66,5 +66,6 @@ def closed_loop_heart_case():
     _, loops = nio.closed_loops(nio.parse_netlist_xml(v["surfaces"]), v["srfids"],
                                 nio.parse_netlist_xml(v["downstream"]))
     P = FlowParams(rho=0.00106, mu=0.004, rhoinf=-1.0, Delt=1e-3, nitr=5, epstol_mom=0.01, epstol_cont=0.2,
-                   epstol_ns=0.4, kspace=50, ngmres=1, maxiters=200, nprjs=10, stabflux_coeff=0.5, loops=loops)
+                   epstol_ns=0.4, kspace=50, ngmres=1, maxiters=200, nprjs=10, stabflux_coeff=0.5, loops=loops,
+                   rescontrol=True, res_criteria=1e-3, min_iters=2)
     return m, y, ac, P

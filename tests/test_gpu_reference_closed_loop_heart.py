@@ -47,3 +47,34 @@ def test_closed_loop_heart_case_on_device():
     gold_q, gold_p = np.array(GOLD["flow_step5"]), np.array(GOLD["pressure_step5"])
     assert np.all(np.abs(np.array([st.q_out[j] for j in range(3)]) - gold_q) <= 2e-5 * np.abs(gold_q))
     assert np.all(np.abs(p - gold_p) <= 3e-4 * np.abs(gold_p))
+
+
+def test_residual_control_on_device():
+    """Residual control firing (criterion 5, at least two iterations): the
+    device step's totres per assembled iteration, its number of solves per
+    step and the state after three steps match the oracle's."""
+    import dataclasses
+
+    m, y, ac, P = closed_loop_heart_case()
+    P = dataclasses.replace(P, res_criteria=5.0)
+    F = po.OracleFlow(m, P, nthreads=4)
+    F.yold, F.acold = y.copy(), ac.copy()
+    F._itr_bc(F.yold)
+    m2, _, _, P2 = closed_loop_heart_case()
+    G = solver.FlowSolver(m2, dataclasses.replace(P2, res_criteria=5.0), inflow=lambda t: 0.0)
+    y0 = y.copy()
+    po.itr_bc(m2, y0)
+    try:
+        G.set_state(y0, ac)
+        for k in range(3):
+            n0, r0 = len(F.stats), len(F.res_norms)
+            F.step()
+            st = G.step()
+            assert st.nsolves == len(F.stats) - n0, k
+            norms = F.res_norms[r0:]
+            for i, v in enumerate(norms):
+                assert abs(st.res_norm[i] - v) <= 1e-9 * v, (k, i, st.res_norm[i], v)
+        yG, _ = G.state()
+    finally:
+        G.close()
+    assert relerr(yG, F.yold) < 1e-9

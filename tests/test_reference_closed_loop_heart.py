@@ -94,3 +94,30 @@ def test_mean_pressures_step5(oracle_run):
     _, hist = oracle_run
     gold = np.array(GOLD["pressure_step5"])
     assert np.all(np.abs(hist[4]["p"] - gold) <= 3e-4 * np.abs(gold)), hist[4]["p"]
+
+
+def test_residual_control(oracle_run):
+    """The case's residual control (1e-3 after at least two iterations) never
+    fires: totres stays above 0.04, so all 25 iterations run.  With a
+    criterion of 5 it fires in step 2: step 1's five iterations carry over
+    (itrdrv.f90:1516-1522 resets the count only on an exit), so step 2 ends
+    at its first iteration below 5, without that iteration's solve, and
+    the count restarts."""
+    import dataclasses
+
+    F, _ = oracle_run
+    assert len(F.res_norms) == 25 and min(F.res_norms) > 1e-3 and len(F.stats) == 25
+    m, y, ac, P = closed_loop_heart_case()
+    G = po.OracleFlow(m, dataclasses.replace(P, res_criteria=5.0), nthreads=4)
+    G.yold, G.acold = y.copy(), ac.copy()
+    G._itr_bc(G.yold)
+    solves = []
+    for _ in range(3):
+        n0 = len(G.stats)
+        G.step()
+        solves.append(len(G.stats) - n0)
+    r = G.res_norms
+    assert solves[0] == 5
+    first_below = next(i for i in range(5, 10) if r[i] < 5.0)
+    assert solves[1] == first_below - 5 < 5
+    assert all(x >= 5.0 for x in r[5:first_below])
