@@ -145,6 +145,7 @@ SIGNATURES = {
     "crimson_netlist_state": (ctypes.c_int, [c_void_p, c_dbl_p, ctypes.c_int]),
     "crimson_set_outlet_netlist": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p]),
     "crimson_set_outlet_netlist_loop": (ctypes.c_int, [c_void_p, c_void_p, c_int_p]),
+    "crimson_outlet_state": (ctypes.c_int, [c_void_p, ctypes.c_int, c_dbl_p, c_dbl_p]),
     "crimson_version": (ctypes.c_char_p, []),
     "crimson_last_error": (ctypes.c_char_p, []),
 }

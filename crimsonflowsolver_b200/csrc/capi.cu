@@ -973,6 +973,27 @@ int crimson_state_set(crimson_ctx* c, const double* y, const double* ac) {
     return CRIMSON_OK;
 }
 
+// GetFlowQ and integrScalar(p) / area (bctcardio.f90:1021-1040's Updcalc)
+// of every coupled surface for the current state.
+int crimson_outlet_state(crimson_ctx* c, int n, double* q, double* p_mean) {
+    if (!c || n != c->ncoupled || (n > 0 && (!q || !p_mean))) return CRIMSON_ERR_ARG;
+    if (!c->yold.p) return CRIMSON_ERR_STATE;
+    if (n == 0) return CRIMSON_OK;
+    cudaStream_t s = c->stream;
+    CR_CHECK(c->psurf.alloc((size_t)n));
+    for (int k = 0; k < n; ++k) {
+        launch(k_flowq_step, 1, 256, 0, s, c->onodes.p, c->onode_off[k], c->onode_off[k + 1], c->onabi.p,
+               reinterpret_cast<const double4*>(c->yold.p), c->flowq.p + k);
+        launch(k_surfp_step, 1, 256, 0, s, c->onodes.p, c->onode_off[k], c->onode_off[k + 1], c->onabi.p,
+               reinterpret_cast<const double4*>(c->yold.p), c->psurf.p + k);
+    }
+    CR_CUDA(cudaMemcpyAsync(q, c->flowq.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaMemcpyAsync(p_mean, c->psurf.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < n; ++k) p_mean[k] = c->oarea[(size_t)k] > 0.0 ? p_mean[k] / c->oarea[(size_t)k] : 0.0;
+    return CRIMSON_OK;
+}
+
 int crimson_state_get(crimson_ctx* c, double* y, double* ac) {
     if (!c || !c->yold.p || !c->stage.p) return CRIMSON_ERR_STATE;
     const int n = c->nshg;

@@ -369,6 +369,14 @@ class FlowSolver:
         N.check(N.lib().crimson_state_get(self.elm.h, N.dp(y), N.dp(ac)), "crimson_state_get")
         return np.ascontiguousarray(y), np.ascontiguousarray(ac)
 
+    def outlet_state(self):
+        """(flows, mean pressures) of the coupled surfaces for the current
+        state (crimson_outlet_state: GetFlowQ, integrScalar(p) / area)."""
+        n = len(self.elm.srflist)
+        q, p = np.zeros(n), np.zeros(n)
+        N.check(N.lib().crimson_outlet_state(self.elm.h, n, N.dp(q), N.dp(p)), "crimson_outlet_state")
+        return q, p
+
     def close(self) -> None:
         """Free the memLS handles, then the context they borrow from."""
         if getattr(self, "memls", None) is not None:

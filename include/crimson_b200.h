@@ -479,6 +479,12 @@ int crimson_set_outlet_netlist_loop(crimson_ctx* ctx, crimson_netlist_loop* loop
 /* yold/acold in the reference layout (nshg, 4) */
 int crimson_state_set(crimson_ctx* ctx, const double* y, const double* ac);
 int crimson_state_get(crimson_ctx* ctx, double* y, double* ac);
+/* Per coupled surface (n = the number given to crimson_set_outlets) the
+ * flow GetFlowQ and the mean pressure integrScalar(p) / area of the current
+ * state, the values Updcalc writes to FlowHist.dat and PressHist.dat
+ * (bctcardio.f90:1021-1040); the mean pressure is 0 for a surface whose
+ * faces carry no natural-pressure bit. */
+int crimson_outlet_state(crimson_ctx* ctx, int n, double* q, double* p_mean);
 int crimson_step(crimson_ctx* ctx, crimson_lhs* lhs, crimson_ls* ls, const crimson_step_args* args,
                  crimson_step_stats* stats);
 

@@ -27,6 +27,8 @@ def _load(name, label):
     m.iBCB = d["iBCB"].copy()
     m.BCB = np.repeat(d["BCB"][:, None, :], 3, axis=1).copy()   # per face node
     m.iBC = d["iBC"].copy()
+    m.dirichlet_nodes = d["dirichlet_nodes"].copy()
+    m.dirichlet_values = d["dirichlet_values"].copy()
     m.BC = np.zeros((m.nshg, meshmod.NDOFBC))
     m.NABI, m.ndsurf = meshmod.compute_nabi(m.x, m.ienb, m.iBCB, m.nshg)
     m.outlets = sorted(int(s) for s in np.unique(m.iBCB[:, 1]) if s >= meshmod.SRF_OUTLET0)

@@ -11,7 +11,8 @@ one entry per distinct file text; netlist_periodic_tables.json: the
 prescribedPeriodicFlow / prescribedPeriodicPressure controls name; and
 netlist_closed_loops.json: per case directory with a
 netlist_closed_loop_downstream.xml, that file's text, the netlist_surfaces
-file beside it and the "List of Netlist LPN Surfaces" of its solver.inp.
+file beside it, its solver.inp and that file's "List of Netlist LPN
+Surfaces".
 """
 import json
 import os
@@ -53,9 +54,11 @@ def main(ref):
         with open(os.path.join(root, surf[0])) as f:
             surfaces = f.read()
         with open(os.path.join(root, "netlist_closed_loop_downstream.xml")) as f:
+            downstream = f.read()
+        with open(os.path.join(root, "solver.inp")) as f:
             loops[os.path.relpath(root, base)] = {
-                "downstream": f.read(), "surfaces_file": surf[0], "surfaces": surfaces,
-                "srfids": [int(t) for t in lists[0]] if lists else []}
+                "downstream": downstream, "surfaces_file": surf[0], "surfaces": surfaces,
+                "srfids": [int(t) for t in lists[0]] if lists else [], "solver_inp": f.read()}
     with open(os.path.join(HERE, "netlist_closed_loops.json"), "w") as f:
         json.dump(loops, f, indent=1, sort_keys=True)
     with open(os.path.join(HERE, "netlist_inputs.json"), "w") as f:

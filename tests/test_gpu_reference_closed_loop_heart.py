@@ -78,3 +78,28 @@ def test_residual_control_on_device():
     finally:
         G.close()
     assert relerr(yG, F.yold) < 1e-9
+
+
+def test_case_driver_runs_the_reference_case(tmp_path):
+    """crimsonflowsolver_b200.case.Case with closedLoopHeart's own solver.inp
+    (parsed, input.config defaults) and netlist inputs: five steps on the
+    device, the FlowHist.dat / PressHist.dat rows (initial state + 5 steps,
+    from crimson_outlet_state) against the reference test's values."""
+    import json
+    import os
+
+    from crimsonflowsolver_b200 import case
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "netlist_closed_loops.json")) as f:
+        inp = json.load(f)["netlist/closedLoopHeart"]["solver_inp"]
+    m, y, ac, ref = closed_loop_heart_case()
+    c = case.Case(case.parse_solver_inp(inp), m, y, ac, loops=ref.loops)
+    h = c.run(out_dir=str(tmp_path))
+    assert h["flow"].shape == (6, 3) and h["pressure"].shape == (6, 3)
+    gold_q, gold_p = np.array(GOLD["flow_step5"]), np.array(GOLD["pressure_step5"])
+    assert np.all(np.abs(h["flow"][5] - gold_q) <= 2e-5 * np.abs(gold_q)), h["flow"][5]
+    assert np.all(np.abs(h["pressure"][5] - gold_p) <= 3e-4 * np.abs(gold_p)), h["pressure"][5]
+    assert abs(h["pressure"][0][0] - 10664.0) < 1e-6   # the restart's uniform pressure
+    rows = open(tmp_path / "PressHist.dat").read().split("\n")
+    assert int(rows[0]) == 6 and len(rows[6].split()) == 3
