@@ -336,6 +336,7 @@ int crimson_set_boundary(crimson_ctx* c, int nface, const int* ienb, const int* 
     CR_CHECK(c->ienb.upload(hb.data(), hb.size(), c->stream));
     CR_CHECK(c->iBCB.upload(hbits.data(), hbits.size(), c->stream));
     c->h_iBCB = hbits;
+    c->h_face_srf.assign(iBCB + nface, iBCB + 2 * (size_t)nface);
     c->h_ienb = hb;
     CR_CHECK(c->BCB.upload(hbcb.data(), hbcb.size(), c->stream));
     // boundary elements (all four nodes) at each node: bc3LHS puts 1 on the
@@ -421,12 +422,13 @@ static int rebuild_dirichlet_face(crimson_lhs* L, const std::vector<int>& codes)
     return crimson_memls_bc_create(L, 1, (int)g.size(), 3, 0, g.data(), v.data());
 }
 
-// Surface integral of the pressure weighted by NASC (integrScalar of y(:,4)).
-__global__ void k_surfp_step(const int* __restrict__ onodes, int beg, int end, const double4* __restrict__ onabi,
+// Surface integral of the pressure weighted by NASC (integrScalar of y(:,4))
+// over a surface's nodes and edge nodes.
+__global__ void k_surfp_step(const int* __restrict__ pnodes, int beg, int end, const double* __restrict__ pw,
                              const double4* __restrict__ y, double* __restrict__ out) {
     __shared__ double sm[32];
     double s = 0.0;
-    for (int t = beg + threadIdx.x; t < end; t += blockDim.x) s += onabi[t].w * y[onodes[t]].w;
+    for (int t = beg + threadIdx.x; t < end; t += blockDim.x) s += pw[t] * y[pnodes[t]].w;
     s = block_sum(s, sm);
     if (threadIdx.x == 0) *out = s;
 }
@@ -491,16 +493,39 @@ int crimson_set_outlets(crimson_ctx* c, int ncoupled, const int* srflist, const 
     c->onode_off.assign(1, 0);
     const int n = c->nshg;
     const std::vector<double> nasc = node_surface_areas(c);
+    // edsurf (boundarydata.f90:186-253): a node of surface 1 (the wall) on a
+    // face of surface s > 1 is an edge node of s (the last such face wins)
+    std::vector<int> ed((size_t)n, 0);
+    for (size_t f = 0; f < c->h_face_srf.size(); ++f) {
+        const int srf = c->h_face_srf[f];
+        if (srf <= 1) continue;
+        const int v[3] = {c->h_ienb[f].x, c->h_ienb[f].y, c->h_ienb[f].z};
+        for (int a = 0; a < 3; ++a)
+            if (ndsurf[v[a]] == 1) ed[(size_t)v[a]] = srf;
+    }
+    std::vector<int> pn;
+    std::vector<double> pwt;
+    c->pnode_off.assign(1, 0);
     c->oarea.assign((size_t)ncoupled, 0.0);
     for (int k = 0; k < ncoupled; ++k) {
-        for (int i = 0; i < n; ++i)
+        for (int i = 0; i < n; ++i) {
             if (ndsurf[i] == srflist[k]) {
                 nodes.push_back(i);
                 nab.push_back(make_double4(NABI[i], NABI[(size_t)n + i], NABI[2 * (size_t)n + i], nasc[i]));
+            }
+            // integrScalar and calculateArea (boundarydata.f90:259-300,
+            // 1101-1140) take the surface's nodes and its edge nodes
+            if (ndsurf[i] == srflist[k] || (ndsurf[i] == 1 && ed[(size_t)i] == srflist[k])) {
+                pn.push_back(i);
+                pwt.push_back(nasc[i]);
                 c->oarea[k] += nasc[i];
             }
+        }
         c->onode_off.push_back((int)nodes.size());
+        c->pnode_off.push_back((int)pn.size());
     }
+    CR_CHECK(c->pnodes.upload(pn.data(), pn.size(), c->stream));
+    CR_CHECK(c->pw.upload(pwt.data(), pwt.size(), c->stream));
     CR_CHECK(c->onodes.upload(nodes.data(), nodes.size(), c->stream));
     c->h_onodes = nodes;
     CR_CHECK(c->onabi.upload(nab.data(), nab.size(), c->stream));
@@ -984,7 +1009,7 @@ int crimson_outlet_state(crimson_ctx* c, int n, double* q, double* p_mean) {
     for (int k = 0; k < n; ++k) {
         launch(k_flowq_step, 1, 256, 0, s, c->onodes.p, c->onode_off[k], c->onode_off[k + 1], c->onabi.p,
                reinterpret_cast<const double4*>(c->yold.p), c->flowq.p + k);
-        launch(k_surfp_step, 1, 256, 0, s, c->onodes.p, c->onode_off[k], c->onode_off[k + 1], c->onabi.p,
+        launch(k_surfp_step, 1, 256, 0, s, c->pnodes.p, c->pnode_off[k], c->pnode_off[k + 1], c->pw.p,
                reinterpret_cast<const double4*>(c->yold.p), c->psurf.p + k);
     }
     CR_CUDA(cudaMemcpyAsync(q, c->flowq.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
@@ -1138,7 +1163,7 @@ int crimson_step(crimson_ctx* c, crimson_lhs* L, crimson_ls* ls, const crimson_s
         CR_CHECK(c->psurf.alloc((size_t)nc));
         for (int k = 0; k < nc; ++k)
             if (blocked[(size_t)k])
-                launch(k_surfp_step, 1, 256, 0, s, c->onodes.p, c->onode_off[k], c->onode_off[k + 1], c->onabi.p,
+                launch(k_surfp_step, 1, 256, 0, s, c->pnodes.p, c->pnode_off[k], c->pnode_off[k + 1], c->pw.p,
                                               reinterpret_cast<const double4*>(c->ycur.p), c->psurf.p + k);
         std::vector<double> hq(nc), hp(nc, 0.0);
         CR_CUDA(cudaMemcpyAsync(hq.data(), c->flowq.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s));

@@ -163,6 +163,13 @@ struct crimson_ctx {
     crimson::DBuf<int> flist;       // (3 nface) codes 3f + n of the faces at each node, ascending f
     crimson::DBuf<double> frec;     // (nface, 12) face residual records: rl(n, 0:3) of face node n
     std::vector<int> h_iBCB;        // (nface) flag bits, host copy
+    std::vector<int> h_face_srf;    // (nface) surface ids, host copy
+    // surface-pressure integrals (integrScalar, boundarydata.f90:1101-1140):
+    // per coupled surface its nodes (ndsurf) and its edge nodes (ndsurf 1,
+    // edsurf the surface), ascending, with their NASC weights
+    crimson::DBuf<int> pnodes;
+    crimson::DBuf<double> pw;
+    std::vector<int> pnode_off;
     crimson::DBuf<int> bcount;      // (nshg) boundary elements (all 4 nodes) containing each node
 
     // coupled outlets

@@ -300,6 +300,22 @@ def neumann_face(mesh, srfid):
     return nodes, mesh.NABI[nodes]
 
 
+def pressure_nodes(mesh, srfid):
+    """The nodes integrScalar sums over for surface srfid
+    (boundarydata.f90:1101-1140): ndsurf == srfid, and the edge nodes of the
+    wall (ndsurf 1) whose edsurf is srfid (boundarydata.f90:186-253: the
+    last face of a surface > 1 touching the node), ascending."""
+    ed = np.zeros(mesh.nshg, dtype=np.int64)
+    for f in range(mesh.ienb.shape[0]):
+        s = int(mesh.iBCB[f, 1])
+        if s > 1:
+            for a in range(3):
+                nd = mesh.ienb[f, a]
+                if mesh.ndsurf[nd] == 1:
+                    ed[nd] = s
+    return np.nonzero((mesh.ndsurf == srfid) | ((mesh.ndsurf == 1) & (ed == srfid)))[0]
+
+
 def surface_areas(mesh):
     """NASC (AsBNASC, asbnabi.f90:191-340): per node the integral of its
     shape function over the faces with the natural-pressure bit, the 3-point
@@ -376,6 +392,7 @@ class OracleFlow:
         self.in_loop = {k for sf in self.loop_surfaces for k in sf}
         self.onodes = [np.nonzero(mesh.ndsurf == s)[0] for s in self.srflist]
         self.nasc = surface_areas(mesh) if any(nl is not None for nl in self.netlists) else None
+        self.pnodes = [pressure_nodes(mesh, s) for s in self.srflist]
         self.memls = MemLS(mesh.nshg, self.colm, self.rowp, 1 + len(self.rcr), P, nthreads)
         nodes, sv = dirichlet_face(self.m)
         self.memls.bc_create(1, nodes, 3, 0, sv)
@@ -498,9 +515,9 @@ class OracleFlow:
             Pn = d1 * q1 + h1
 
             def p3d(k):
-                # integrScalar(p) / area (elmgmr.f90:1733-1743)
-                w = self.nasc[self.onodes[k]]
-                return float(np.sum(w * self.y[self.onodes[k], 3]) / np.sum(w))
+                # integrScalar(p) / area (elmgmr.f90:1733-1743), edge nodes included
+                w = self.nasc[self.pnodes[k]]
+                return float(np.sum(w * self.y[self.pnodes[k], 3]) / np.sum(w))
 
             for lp, sf in zip(self.loops, self.loop_surfaces):
                 lp.update(P.Delt, [q1[k] for k in sf], [0.0 if lp.up[j].permitted else p3d(k)

@@ -26,7 +26,7 @@ def test_closed_loop_heart_case_on_device():
     po.itr_bc(m, y0)
     G = solver.FlowSolver(m, P, inflow=lambda t: 0.0)
     nasc = po.surface_areas(m)
-    onodes = [np.nonzero(m.ndsurf == s)[0] for s in (5, 6, 7)]
+    onodes = [po.pressure_nodes(m, s) for s in (5, 6, 7)]
     try:
         G.set_state(y0, ac)
         for k in range(5):
@@ -46,7 +46,7 @@ def test_closed_loop_heart_case_on_device():
     assert relerr(yG[:, 3], F.yold[:, 3]) < 1e-9, relerr(yG[:, 3], F.yold[:, 3])
     gold_q, gold_p = np.array(GOLD["flow_step5"]), np.array(GOLD["pressure_step5"])
     assert np.all(np.abs(np.array([st.q_out[j] for j in range(3)]) - gold_q) <= 2e-5 * np.abs(gold_q))
-    assert np.all(np.abs(p - gold_p) <= 3e-4 * np.abs(gold_p))
+    assert np.all(np.abs(p - gold_p) <= 5e-8 * np.abs(gold_p))
 
 
 def test_residual_control_on_device():
@@ -99,7 +99,7 @@ def test_case_driver_runs_the_reference_case(tmp_path):
     assert h["flow"].shape == (6, 3) and h["pressure"].shape == (6, 3)
     gold_q, gold_p = np.array(GOLD["flow_step5"]), np.array(GOLD["pressure_step5"])
     assert np.all(np.abs(h["flow"][5] - gold_q) <= 2e-5 * np.abs(gold_q)), h["flow"][5]
-    assert np.all(np.abs(h["pressure"][5] - gold_p) <= 3e-4 * np.abs(gold_p)), h["pressure"][5]
+    assert np.all(np.abs(h["pressure"][5] - gold_p) <= 5e-8 * np.abs(gold_p)), h["pressure"][5]
     assert abs(h["pressure"][0][0] - 10664.0) < 1e-6   # the restart's uniform pressure
     rows = open(tmp_path / "PressHist.dat").read().split("\n")
     assert int(rows[0]) == 6 and len(rows[6].split()) == 3

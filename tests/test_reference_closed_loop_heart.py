@@ -17,17 +17,18 @@ The oracle's time stepper (OracleFlow with OracleLoop, the restatement the
 GPU path is checked against) reproduces them:
 
 * loop-closing circuit pressures after step 4 within 1e-7 absolute
-  (measured 3e-9 and 1e-8; the reference's own bar is 1e-8);
+  (measured 5e-13 and 1.3e-8; the reference's own bar is 1e-8);
+* surface mean pressures after step 5 within 5e-8 relative (measured
+  2.5e-9, 2.8e-9, 1.1e-8), the surfaces' own nodes and their edge nodes
+  weighted by NASC as integrScalar sums them;
 * surface flows after step 5 within 2e-5 relative (measured 3e-8, 5e-7,
-  7e-6) and the heart's interface flow after step 4 within 2e-5 (4e-7);
-* surface mean pressures after step 5 within 3e-4 relative (measured 4e-6,
-  1.5e-4, 1.3e-4).
+  7e-6) and the heart's interface flow after step 4 within 2e-5 (4e-7).
 
-The solves stop at the case's loose memLS tolerances (0.4 / 0.01 / 0.2), so
-the pressure field, the least converged quantity, carries the largest gap;
-the reference's own test bars (1e-5 .. 1e-8 absolute) are tighter than
-any reimplementation of its iterative solvers can meet, since they only
-hold for the binary that wrote them.
+The solves stop at the case's loose memLS tolerances (0.4 / 0.01 / 0.2);
+solved tightly the same steps give a heart flow of -43.8 instead of
+-307.4, so the values depend on every Krylov iterate, and the gaps above
+are the rounding differences between two implementations of those
+iterations.
 """
 import numpy as np
 import pytest
@@ -39,11 +40,12 @@ from tests.fixtures import closed_loop_heart_case
 
 def surface_mean_pressures(F):
     """PressHist.dat's value: integrScalar(p) / area over each surface
-    (bctcardio.f90:1021-1040, the NASC weights of boundarydata.f90:295-310)."""
+    (bctcardio.f90:1021-1040) over the surface's nodes and its edge nodes,
+    with the NASC weights (boundarydata.f90:259-300, 1101-1140)."""
     out = []
-    for k in range(len(F.onodes)):
-        w = F.nasc[F.onodes[k]]
-        out.append(float(np.sum(w * F.yold[F.onodes[k], 3]) / np.sum(w)))
+    for k in range(len(F.pnodes)):
+        w = F.nasc[F.pnodes[k]]
+        out.append(float(np.sum(w * F.yold[F.pnodes[k], 3]) / np.sum(w)))
     return np.array(out)
 
 
@@ -93,7 +95,7 @@ def test_flows_step5(oracle_run):
 def test_mean_pressures_step5(oracle_run):
     _, hist = oracle_run
     gold = np.array(GOLD["pressure_step5"])
-    assert np.all(np.abs(hist[4]["p"] - gold) <= 3e-4 * np.abs(gold)), hist[4]["p"]
+    assert np.all(np.abs(hist[4]["p"] - gold) <= 5e-8 * np.abs(gold)), hist[4]["p"]
 
 
 def test_residual_control(oracle_run):
