@@ -93,9 +93,9 @@ def flow_params(settings: Dict[str, str], **extra) -> FlowParams:
     for key in ("deformable wall", "time varying boundary conditions from file", "simulate in purely zero dimensions"):
         if _true(_get(s, key)):
             raise NotImplementedError(f"{key} = True is not supported")
-    for key in ("number of rcr surfaces", "number of experimental rcr surfaces"):
-        if int(_get(s, key) or 0) != 0:
-            raise NotImplementedError(f"{key}: give RCR outlets as FlowParams.rcr")
+    nrcr = sum(int(_get(s, key) or 0) for key in ("number of rcr surfaces", "number of experimental rcr surfaces"))
+    if nrcr != len(extra.get("rcr", [])):
+        raise NotImplementedError("RCR surfaces: read rcrt.dat with parse_rcrt and pass them as rcr=")
     steps = _get(s, "step construction").split()
     if len(steps) % 2 or any(steps[i] != "0" or steps[i + 1] != "1" for i in range(0, len(steps), 2)):
         raise NotImplementedError(f"Step Construction {' '.join(steps)!r}: only solve/update pairs '0 1'")
@@ -123,6 +123,28 @@ def flow_params(settings: Dict[str, str], **extra) -> FlowParams:
               min_iters=int(s["minimum required iterations"]) if rescontrol else 0)
     kw.update(extra)
     return FlowParams(**kw)
+
+
+def parse_rcrt(text: str, srfids: List[int]):
+    """rcrt.dat (RcrtReader, fileReaders.cxx:273-380; general_rcrbc.f90:
+    34-60): the largest number of distal-pressure points, then per RCR
+    surface its number of points, Rp, C, Rd and the (time, Pd) points.
+    Returns :class:`~crimsonflowsolver_b200.problem.RCR` outlets; a distal
+    pressure that varies in time is not supported."""
+    from .problem import RCR
+
+    tok = text.split()
+    pos = 1
+    out = []
+    for srf in srfids:
+        npts = int(tok[pos])
+        rp, c, rd = (float(t) for t in tok[pos + 1:pos + 4])
+        pd = [float(tok[pos + 5 + 2 * i]) for i in range(npts)]
+        pos += 4 + 2 * npts
+        if any(v != pd[0] for v in pd):
+            raise NotImplementedError(f"surface {srf}: a time-varying distal pressure is not supported")
+        out.append(RCR(srfid=srf, Rp=rp, C=c, Rd=rd, Pd=pd[0]))
+    return out
 
 
 def _write_hist(path: str, rows: List[np.ndarray]) -> None:
@@ -180,6 +202,11 @@ class Case:
                     downstream = netlist_io.parse_netlist_xml(f.read())
             standalone, loops = netlist_io.closed_loops(circuits, srfids, downstream, controllers=controllers,
                                                         data_dir=path)
+        rcr_srf = [int(t) for key in ("list of rcr surfaces", "list of experimental rcr surfaces")
+                   for t in settings.get(key, "").split()]
+        if rcr_srf and "rcr" not in extra:
+            with open(os.path.join(path, "rcrt.dat")) as f:
+                extra["rcr"] = parse_rcrt(f.read(), rcr_srf)
         return cls(settings, mesh, y, ac, standalone, loops, step0, **extra)
 
     def run(self, steps: Optional[int] = None, out_dir: Optional[str] = None, write_restarts: bool = False):
@@ -199,6 +226,14 @@ class Case:
             y0[full, 0:3] = self.mesh.BC[full, 2:5]
             G.set_state(y0, self.ac0)
             q, p = G.outlet_state()
+            if self.P.rcr and self.step0 == 0:
+                # the RCRs start from the surfaces' initial pressure and flow
+                # (callCPPSetPressureFromFortran, itrdrv.f90:748-760;
+                # AbstractBoundaryCondition.cxx:105-117)
+                from . import _native as N
+
+                pn, qn = np.ascontiguousarray(p), np.ascontiguousarray(q)
+                N.check(N.lib().crimson_rcr_state(G.elm.h, len(pn), N.dp(pn), N.dp(qn), 1), "crimson_rcr_state")
             flows, pressures = [q], [p]
             for k in range(steps):
                 G.step()

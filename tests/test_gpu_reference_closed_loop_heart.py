@@ -103,3 +103,25 @@ def test_case_driver_runs_the_reference_case(tmp_path):
     assert abs(h["pressure"][0][0] - 10664.0) < 1e-6   # the restart's uniform pressure
     rows = open(tmp_path / "PressHist.dat").read().split("\n")
     assert int(rows[0]) == 6 and len(rows[6].split()) == 3
+
+
+def test_case_driver_runs_the_rcrt_case():
+    """legacy/netlistWithRCRTs through crimsonflowsolver_b200.case.Case (RCR
+    outlets from rcrt.dat starting from the initial surface state, the heart
+    circuit on surface 5): five device steps against the oracle's run and the
+    reference test's values, with the bars of
+    tests/test_reference_netlist_rcrt.py."""
+    from crimsonflowsolver_b200 import case
+    from tests import test_reference_netlist_rcrt as T
+
+    _, hist = T.run_oracle()
+    m, y, ac, s, netlists, rcr = T.rcrt_case()
+    c = case.Case(s, m, y, ac, netlists=netlists, rcr=rcr)
+    h = c.run()
+    order = [o.srfid for o in c.P.outlets()]
+    for j, srf in enumerate(order):
+        for k in range(5):
+            assert abs(h["flow"][k + 1][j] - hist[k]["Q"][srf]) <= 1e-9 * abs(hist[k]["Q"][srf]), (k, srf)
+            assert abs(h["pressure"][k + 1][j] - hist[k]["p"][srf]) <= 1e-9 * abs(hist[k]["p"][srf]), (k, srf)
+        assert abs(h["flow"][5][j] - T.GOLD_Q[srf]) <= 1e-6 * abs(T.GOLD_Q[srf])
+        assert abs(h["pressure"][5][j] - T.GOLD_P[srf]) <= 2e-7 * abs(T.GOLD_P[srf])
