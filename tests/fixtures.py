@@ -45,6 +45,7 @@ CLOSED_LOOP_HEART_GOLDEN = {
     "pressure_step5": (553.277617338762, 548.211423767513, 541.282726604241),
     "heart_interface_flow_step4": -287.802631760359,
     "downstream_pressures_step4": (533.100216837156, 533.100216837156, 0.0, 535.821025669528),
+    "downstream_flows_step4": (0.0, 27.2080883237159, -27.2080883237159),
 }
 
 

@@ -61,6 +61,7 @@ def run_oracle(steps=5):
         F.step()
         hist.append({"Q": F.Qn.copy(), "p": surface_mean_pressures(F), "heart_q": float(lp.up[0].q[0]),
                      "down_p": np.array([lp.down.pressure(i + 1) for i in range(lp.down.np_)]),
+                     "down_q": np.array(lp.down.q, dtype=float),
                      "permitted": permitted})
     return F, hist
 
@@ -83,6 +84,15 @@ def test_case_set_up(oracle_run):
 def test_loop_closing_circuit_pressures_step4(oracle_run):
     _, hist = oracle_run
     assert np.abs(hist[3]["down_p"] - np.array(GOLD["downstream_pressures_step4"])).max() < 1e-7
+
+
+def test_loop_closing_circuit_flows_step4(oracle_run):
+    """netlistFlows_downstreamCircuit_0.dat row 5: no flow through the
+    resistor between the two nodes of equal pressure, 27.208 into the
+    compliance and back out through the venous resistor."""
+    _, hist = oracle_run
+    q, gold = hist[3]["down_q"], np.array(GOLD["downstream_flows_step4"])
+    assert abs(q[0]) < 1e-9 and np.all(np.abs(q[1:] - gold[1:]) <= 1e-6 * np.abs(gold[1:])), q
 
 
 def test_flows_step5(oracle_run):
